@@ -1,0 +1,76 @@
+"""Build the CUDA C-ABI library ``anns_fhe_b200/lib/libafhe.so`` for sm_100a.
+
+Plain ``nvcc -shared`` over the sources in ``csrc/``; no torch extension, no
+JIT cache: the library is built in-tree so it travels with the working tree.
+
+    python -m anns_fhe_b200.build [--force] [--ptxas-verbose]
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+LIBDIR = os.path.join(HERE, "lib")
+LIB = os.path.join(LIBDIR, "libafhe.so")
+ROOT = os.path.dirname(HERE)
+INCLUDE = os.path.join(ROOT, "include")
+
+SOURCES = ["api.cu", "driver.cu", "kernels.cu", "tables.cpp"]
+HEADERS = ["internal.h", "lanes.h", "modarith.cuh", "ntt.cuh", "tables.h"]
+
+ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def nvcc_path() -> str:
+    for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found: the CUDA extension cannot be built")
+
+
+def _stale() -> bool:
+    if not os.path.exists(LIB):
+        return True
+    t = os.path.getmtime(LIB)
+    deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS] + [os.path.join(INCLUDE, "afhe.h")]
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def build(force: bool = False, ptxas_verbose: bool = False, quiet: bool = True) -> str:
+    """Compile libafhe.so if missing or older than its sources; return its path."""
+    if not force and not _stale():
+        return LIB
+    os.makedirs(LIBDIR, exist_ok=True)
+    tmp = LIB + ".tmp"
+    cmd = [
+        nvcc_path(), "-O3", "-std=c++17", *ARCH_FLAGS, "-lineinfo",
+        "-Xcompiler", "-fPIC,-O3", "-shared", "--expt-relaxed-constexpr",
+        "-I", INCLUDE, "-I", CSRC,
+        "-o", tmp, *[os.path.join(CSRC, f) for f in SOURCES],
+    ]
+    if ptxas_verbose:
+        cmd.insert(1, "-Xptxas=-v")
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError("nvcc failed:\n" + res.stdout + res.stderr)
+    if not quiet or ptxas_verbose:
+        sys.stdout.write(res.stdout + res.stderr)
+    os.replace(tmp, LIB)
+    return LIB
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("--ptxas-verbose", action="store_true")
+    a = ap.parse_args()
+    print(build(force=a.force, ptxas_verbose=a.ptxas_verbose, quiet=False))
+
+
+if __name__ == "__main__":
+    main()

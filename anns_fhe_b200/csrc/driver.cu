@@ -1,0 +1,402 @@
+// driver.cu -- FHEHostDriver composite operators on the device arenas
+// (cpp_host_model/src/fhe_host_driver.cpp:248-404), plus batched variants.
+//
+// Every composite runs entirely on the context stream; intermediates live in
+// the context-private scratch (one lane per ciphertext of a batch) instead of
+// the reference's fixed SCRATCH_* slots of poly_gmem
+// (cpp_host_model/src/fhe_host_driver.h:63-69), so caller-visible memory is
+// never clobbered. Keys use the full-level layout: digit j, limb i of a key at
+// evk lives at evk + (j * (L + K) + (i < l ? i : L + i - l)) * N, evk_b after
+// all d digits of evk_a (fhe_host_driver.cpp:105-117, fhe_accel_top.cpp:304-305).
+#include <cuda_runtime.h>
+
+#include <cstdlib>
+#include <vector>
+
+#include "internal.h"
+#include "lanes.h"
+#include "tables.h"
+
+using namespace afhe;
+
+namespace {
+
+int check_limbs(afhe_ctx* ctx, uint32_t limbs, uint32_t min_limbs) {
+    if (limbs < min_limbs || limbs > ctx->L) return fail(ctx, AFHE_E_LEVEL, "limb count outside [min, L]");
+    return AFHE_OK;
+}
+
+int check_poly(afhe_ctx* ctx, u64 off, uint32_t limbs) {
+    if (!range_ok(off, (u64)limbs * ctx->n, ctx->prm.poly_words)) return fail(ctx, AFHE_E_RANGE, "operand out of poly_gmem");
+    return AFHE_OK;
+}
+
+int check_key(afhe_ctx* ctx, u64 evk) {
+    u64 words = 2ull * ctx->dnum * (ctx->L + ctx->K) * ctx->n;
+    if (!range_ok(evk, words, ctx->prm.key_words)) return fail(ctx, AFHE_E_RANGE, "key out of key_gmem");
+    return AFHE_OK;
+}
+
+// Key switch nz polynomials (poly_gmem-relative offsets) with one key.
+int ks_batch(afhe_ctx* ctx, const u64* in, const u64* out0, const u64* out1, uint32_t nz, u64 evk, uint32_t limbs) {
+    const u64 n = ctx->n, S = (u64)ctx->L + ctx->K;
+    const OpTabs& t = ctx->lv[limbs];
+    const LevelJobs& lj = ctx->lvjobs[limbs];
+    ZBases zb{};
+    for (uint32_t z = 0; z < nz; ++z) {
+        zb.src[z] = in[z];
+        zb.out[z] = out0[z];
+        zb.aux[z] = out1[z];
+        zb.mid[z] = lane_of(ctx, z).ks;
+    }
+    CK(launch_key_switch(ctx->log_n, t, ctx->jobs_qp, lj.modup, lj.n_modup, ctx->L, limbs, ctx->K, ctx->key, evk,
+                         evk + (u64)ctx->dnum * S * n, (uint32_t)S, ctx->L, ctx->poly, ctx->scr, nz, zb, ctx->st));
+    return AFHE_OK;
+}
+
+// Rescale nz ciphertexts: (in0[z], in1[z]) -> (out0[z], out1[z]), level limbs -> limbs - 1.
+int rescale_batch(afhe_ctx* ctx, const u64* in0, const u64* in1, const u64* out0, const u64* out1, uint32_t nz,
+                  uint32_t limbs) {
+    ZBases zb{};
+    for (uint32_t z = 0; z < nz; ++z) {
+        Lane l = lane_of(ctx, z);
+        for (uint32_t h = 0; h < 2; ++h) {
+            uint32_t zz = 2 * z + h;
+            zb.src[zz] = h ? in1[z] : in0[z];
+            zb.out[zz] = h ? out1[z] : out0[z];
+            zb.mid[zz] = l.resc + (u64)h * ctx->L * ctx->n;
+        }
+    }
+    CK(launch_rescale(ctx->log_n, ctx->lv[limbs], ctx->jobs_qp, limbs, ctx->poly, ctx->scr, 2 * nz, zb, ctx->st));
+    return AFHE_OK;
+}
+
+int ew_batch(afhe_ctx* ctx, ElemOp op, const u64* a, const u64* b, const u64* o, uint32_t nz, uint32_t limbs) {
+    ZBases zb{};
+    for (uint32_t z = 0; z < nz; ++z) {
+        zb.src[z] = a[z];
+        zb.aux[z] = b ? b[z] : a[z];
+        zb.out[z] = o[z];
+    }
+    CK(launch_elementwise(op, ctx->nat.pc, 0, ctx->poly, ctx->n, limbs, nz, zb, ctx->st));
+    return AFHE_OK;
+}
+
+bool overlap(u64 a, u64 aw, u64 b, u64 bw) { return a < b + bw && b < a + aw; }
+
+// eval_mult_relin_rescale on nz ciphertexts (lane z for ciphertext z).
+int mult_relin_rescale_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const afhe_ct_ref* b, const afhe_ct_ref* d,
+                             uint32_t nz, uint32_t limbs) {
+    if (!ctx->has_relin) return fail(ctx, AFHE_E_NOKEY, "no relinearisation key set");
+    TensorArgs ta{};
+    u64 t0[TZMAX], t1[TZMAX], t2[TZMAX], k0[TZMAX], k1[TZMAX], o0[TZMAX], o1[TZMAX];
+    for (uint32_t z = 0; z < nz; ++z) {
+        t0[z] = lane_temp(ctx, z, 0);
+        t1[z] = lane_temp(ctx, z, 1);
+        t2[z] = lane_temp(ctx, z, 2);
+        k0[z] = lane_temp(ctx, z, 3);
+        k1[z] = lane_temp(ctx, z, 4);
+        ta.a0[z] = a[z].c0_offset; ta.a1[z] = a[z].c1_offset;
+        ta.b0[z] = b[z].c0_offset; ta.b1[z] = b[z].c1_offset;
+        ta.d0[z] = t0[z]; ta.d1[z] = t1[z]; ta.d2[z] = t2[z];
+        o0[z] = d[z].c0_offset; o1[z] = d[z].c1_offset;
+    }
+    // 1. tensor product (fhe_host_driver.cpp:280-286)
+    CK(launch_tensor(ctx->nat.pc, ctx->poly, ctx->n, limbs, nz, ta, ctx->st));
+    // 2. relinearise d2 (:288-289)
+    int rc = ks_batch(ctx, t2, k0, k1, nz, ctx->relin_off, limbs);
+    if (rc != AFHE_OK) return rc;
+    // 3. d0 += ks0, d1 += ks1 (:292-293), both in one launch
+    {
+        u64 A[2 * TZMAX], B[2 * TZMAX];
+        for (uint32_t z = 0; z < nz; ++z) {
+            A[2 * z] = t0[z]; B[2 * z] = k0[z];
+            A[2 * z + 1] = t1[z]; B[2 * z + 1] = k1[z];
+        }
+        if ((rc = ew_batch(ctx, EW_ADD, A, B, A, 2 * nz, limbs)) != AFHE_OK) return rc;
+    }
+    // 4. rescale into the destination (:296-305)
+    return rescale_batch(ctx, t0, t1, o0, o1, nz, limbs);
+}
+
+// One rotation step on nz ciphertexts: dst = (auto(c0) + ks0, ks1), KS on auto(c1)
+// (fhe_host_driver.cpp:331-359). Inputs may alias outputs.
+int rotate_step_batch(afhe_ctx* ctx, const u64* in0, const u64* in1, const u64* d0, const u64* d1, uint32_t nz,
+                      int32_t step, uint32_t limbs) {
+    auto it = ctx->rot.find(step);
+    if (it == ctx->rot.end()) return fail(ctx, AFHE_E_NOKEY, "rotation key not found for step " + std::to_string(step));
+    const RotKey& rk = it->second;
+    u64 t0[TZMAX], t1[TZMAX], k0[TZMAX], k1[TZMAX];
+    ZBases zb{};
+    for (uint32_t z = 0; z < nz; ++z) {
+        t0[z] = lane_temp(ctx, z, 0);
+        t1[z] = lane_temp(ctx, z, 1);
+        k0[z] = lane_temp(ctx, z, 3);
+        k1[z] = lane_temp(ctx, z, 4);
+        zb.src[2 * z] = in0[z]; zb.out[2 * z] = t0[z];
+        zb.src[2 * z + 1] = in1[z]; zb.out[2 * z + 1] = t1[z];
+    }
+    CK(launch_automorphism(rk.map, nullptr, ctx->poly, ctx->n, limbs, 2 * nz, zb, ctx->st));
+    int rc = ks_batch(ctx, t1, k0, k1, nz, rk.evk_offset, limbs);
+    if (rc != AFHE_OK) return rc;
+    if ((rc = ew_batch(ctx, EW_ADD, t0, k0, d0, nz, limbs)) != AFHE_OK) return rc;
+    return ew_batch(ctx, EW_COPY, k1, nullptr, d1, nz, limbs);
+}
+
+// eval_rotate on nz ciphertexts by the same amount (fhe_host_driver.cpp:361-404):
+// |r| decomposed into descending powers of two, sign kept.
+int rotate_batch(afhe_ctx* ctx, const afhe_ct_ref* in, const afhe_ct_ref* dst, uint32_t nz, int32_t total,
+                 uint32_t limbs) {
+    u64 i0[TZMAX], i1[TZMAX], o0[TZMAX], o1[TZMAX], c0[TZMAX], c1[TZMAX], x0[TZMAX], x1[TZMAX];
+    for (uint32_t z = 0; z < nz; ++z) {
+        i0[z] = in[z].c0_offset; i1[z] = in[z].c1_offset;
+        o0[z] = dst[z].c0_offset; o1[z] = dst[z].c1_offset;
+        x0[z] = lane_temp(ctx, z, 2);   // chain temporaries (unused by a single step)
+        x1[z] = lane_temp(ctx, z, 5);
+    }
+    if (total == 0) {
+        for (uint32_t z = 0; z < nz; ++z) {
+            CK(cudaMemcpyAsync(ctx->poly + o0[z], ctx->poly + i0[z], (u64)limbs * ctx->n * 8, cudaMemcpyDeviceToDevice, ctx->st));
+            CK(cudaMemcpyAsync(ctx->poly + o1[z], ctx->poly + i1[z], (u64)limbs * ctx->n * 8, cudaMemcpyDeviceToDevice, ctx->st));
+        }
+        return AFHE_OK;
+    }
+    // every step's key must exist before anything is launched
+    long long rem = std::llabs((long long)total);
+    const int sign = total > 0 ? 1 : -1;
+    std::vector<int32_t> steps;
+    while (rem > 0) {
+        long long s = 1;
+        while ((s << 1) <= rem) s <<= 1;
+        steps.push_back((int32_t)(sign * s));
+        rem -= s;
+    }
+    for (int32_t s : steps)
+        if (!ctx->rot.count(s)) return fail(ctx, AFHE_E_NOKEY, "rotation key not found for step " + std::to_string(s));
+    for (uint32_t z = 0; z < nz; ++z) { c0[z] = i0[z]; c1[z] = i1[z]; }
+    for (size_t k = 0; k < steps.size(); ++k) {
+        bool last = k + 1 == steps.size();
+        const u64* n0 = last ? o0 : x0;
+        const u64* n1 = last ? o1 : x1;
+        int rc = rotate_step_batch(ctx, c0, c1, n0, n1, nz, steps[k], limbs);
+        if (rc != AFHE_OK) return rc;
+        for (uint32_t z = 0; z < nz; ++z) { c0[z] = n0[z]; c1[z] = n1[z]; }
+    }
+    return AFHE_OK;
+}
+
+template <class F>
+int for_chunks(uint32_t count, F f) {
+    for (uint32_t s = 0; s < count; s += TZMAX) {
+        uint32_t m = count - s < (uint32_t)TZMAX ? count - s : (uint32_t)TZMAX;
+        int rc = f(s, m);
+        if (rc != AFHE_OK) return rc;
+    }
+    return AFHE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+// ---- key directory ----------------------------------------------------------
+int afhe_set_relin_key(afhe_ctx* ctx, uint64_t evk) {
+    if (!ctx) return fail(nullptr, AFHE_E_ARG, "null context");
+    int rc = check_key(ctx, evk);
+    if (rc != AFHE_OK) return rc;
+    ctx->relin_off = evk;
+    ctx->has_relin = true;
+    return AFHE_OK;
+}
+
+int afhe_add_rotation_key(afhe_ctx* ctx, int32_t step, uint64_t evk) {
+    if (!ctx) return fail(nullptr, AFHE_E_ARG, "null context");
+    int rc = check_key(ctx, evk);
+    if (rc != AFHE_OK) return rc;
+    cudaSetDevice(ctx->device);
+    RotKey rk;
+    rk.step = step;
+    rk.galois = galois_elt_for_step(ctx->log_n, step);
+    rk.evk_offset = evk;
+    std::vector<uint32_t> map(ctx->n);
+    automorphism_map(ctx->log_n, rk.galois, map.data());
+    auto old = ctx->rot.find(step);
+    if (old != ctx->rot.end()) {
+        rk.map = old->second.map;
+    } else {
+        CK(cudaMalloc((void**)&rk.map, ctx->n * sizeof(uint32_t)));
+    }
+    CK(cudaMemcpy(rk.map, map.data(), ctx->n * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    ctx->rot[step] = rk;
+    return AFHE_OK;
+}
+
+int afhe_has_rotation_key(afhe_ctx* ctx, int32_t step) { return ctx && ctx->rot.count(step) ? 1 : 0; }
+
+// ---- primitives (native tables) ------------------------------------------------
+static int ntt_native(afhe_ctx* ctx, bool inv, uint64_t src, uint64_t dst, uint32_t limbs) {
+    if (!ctx) return fail(nullptr, AFHE_E_ARG, "null context");
+    int rc;
+    if ((rc = check_limbs(ctx, limbs, 1)) || (rc = check_poly(ctx, src, limbs)) || (rc = check_poly(ctx, dst, limbs))) return rc;
+    const u64 w = (u64)limbs * ctx->n;
+    u64 s = src;
+    if (src != dst && overlap(src, w, dst, w)) {
+        CK(cudaMemcpyAsync(ctx->scr, ctx->poly + src, w * 8, cudaMemcpyDeviceToDevice, ctx->st));
+        s = ctx->prm.poly_words;
+    }
+    ZBases zb{};
+    zb.src[0] = s; zb.mid[0] = dst; zb.out[0] = dst;
+    CK(launch_ntt_plain(inv, ctx->log_n, ctx->nat.view(), ctx->jobs_qp, limbs, ctx->poly, ctx->poly, 1, zb, ctx->st));
+    return AFHE_OK;
+}
+
+int afhe_ntt(afhe_ctx* ctx, uint64_t src, uint64_t dst, uint32_t limbs) { return ntt_native(ctx, false, src, dst, limbs); }
+int afhe_intt(afhe_ctx* ctx, uint64_t src, uint64_t dst, uint32_t limbs) { return ntt_native(ctx, true, src, dst, limbs); }
+
+static int ew_single(afhe_ctx* ctx, ElemOp op, uint64_t a, uint64_t b, uint64_t dst, uint32_t limbs) {
+    if (!ctx) return fail(nullptr, AFHE_E_ARG, "null context");
+    int rc;
+    if ((rc = check_limbs(ctx, limbs, 1)) || (rc = check_poly(ctx, a, limbs)) || (rc = check_poly(ctx, b, limbs)) ||
+        (rc = check_poly(ctx, dst, limbs)))
+        return rc;
+    const u64 w = (u64)limbs * ctx->n;
+    u64 aa = a, bb = b;
+    if (a != dst && overlap(a, w, dst, w)) {
+        CK(cudaMemcpyAsync(ctx->scr, ctx->poly + a, w * 8, cudaMemcpyDeviceToDevice, ctx->st));
+        aa = ctx->prm.poly_words;
+    }
+    if (b != dst && overlap(b, w, dst, w)) {
+        CK(cudaMemcpyAsync(ctx->scr + w, ctx->poly + b, w * 8, cudaMemcpyDeviceToDevice, ctx->st));
+        bb = ctx->prm.poly_words + w;
+    }
+    return ew_batch(ctx, op, &aa, &bb, &dst, 1, limbs);
+}
+
+int afhe_poly_add(afhe_ctx* c, uint64_t a, uint64_t b, uint64_t d, uint32_t l) { return ew_single(c, EW_ADD, a, b, d, l); }
+int afhe_poly_sub(afhe_ctx* c, uint64_t a, uint64_t b, uint64_t d, uint32_t l) { return ew_single(c, EW_SUB, a, b, d, l); }
+int afhe_poly_mul_ntt(afhe_ctx* c, uint64_t a, uint64_t b, uint64_t d, uint32_t l) { return ew_single(c, EW_MUL, a, b, d, l); }
+
+int afhe_automorphism(afhe_ctx* ctx, uint64_t src, uint32_t galois, uint64_t dst, uint32_t limbs) {
+    if (!ctx) return fail(nullptr, AFHE_E_ARG, "null context");
+    int rc;
+    if ((rc = check_limbs(ctx, limbs, 1)) || (rc = check_poly(ctx, src, limbs)) || (rc = check_poly(ctx, dst, limbs))) return rc;
+    if ((galois & 1u) == 0 || galois >= 2 * ctx->n) return fail(ctx, AFHE_E_ARG, "galois element must be odd and < 2N");
+    std::vector<uint32_t> map(ctx->n);
+    automorphism_map(ctx->log_n, galois, map.data());
+    const u64 w = (u64)limbs * ctx->n;
+    // map in scratch words [0, N/2), the source copy after it (a gather cannot run in place)
+    uint32_t* dmap = (uint32_t*)(ctx->scr);
+    CK(cudaMemcpyAsync(dmap, map.data(), ctx->n * 4, cudaMemcpyHostToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->scr + ctx->n, ctx->poly + src, w * 8, cudaMemcpyDeviceToDevice, ctx->st));
+    ZBases zb{};
+    zb.src[0] = ctx->prm.poly_words + ctx->n;
+    zb.out[0] = dst;
+    CK(launch_automorphism(dmap, nullptr, ctx->poly, ctx->n, limbs, 1, zb, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));   // the host map buffer goes out of scope
+    return AFHE_OK;
+}
+
+int afhe_rescale(afhe_ctx* ctx, uint64_t c0_in, uint64_t c1_in, uint64_t c0_out, uint64_t c1_out, uint32_t limbs) {
+    if (!ctx) return fail(nullptr, AFHE_E_ARG, "null context");
+    int rc;
+    if ((rc = check_limbs(ctx, limbs, 2)) || (rc = check_poly(ctx, c0_in, limbs)) || (rc = check_poly(ctx, c1_in, limbs)) ||
+        (rc = check_poly(ctx, c0_out, limbs - 1)) || (rc = check_poly(ctx, c1_out, limbs - 1)))
+        return rc;
+    // inputs go to lane temps first so that any aliasing with the outputs is safe
+    const u64 w = (u64)limbs * ctx->n;
+    u64 t0 = lane_temp(ctx, 0, 0), t1 = lane_temp(ctx, 0, 1);
+    CK(cudaMemcpyAsync(ctx->poly + t0, ctx->poly + c0_in, w * 8, cudaMemcpyDeviceToDevice, ctx->st));
+    CK(cudaMemcpyAsync(ctx->poly + t1, ctx->poly + c1_in, w * 8, cudaMemcpyDeviceToDevice, ctx->st));
+    return rescale_batch(ctx, &t0, &t1, &c0_out, &c1_out, 1, limbs);
+}
+
+int afhe_key_switch(afhe_ctx* ctx, uint64_t src, uint64_t evk, uint64_t d0, uint64_t d1, uint32_t limbs) {
+    if (!ctx) return fail(nullptr, AFHE_E_ARG, "null context");
+    int rc;
+    if ((rc = check_limbs(ctx, limbs, 1)) || (rc = check_poly(ctx, src, limbs)) || (rc = check_poly(ctx, d0, limbs)) ||
+        (rc = check_poly(ctx, d1, limbs)) || (rc = check_key(ctx, evk)))
+        return rc;
+    const u64 w = (u64)limbs * ctx->n;
+    u64 t = lane_temp(ctx, 0, 2);
+    CK(cudaMemcpyAsync(ctx->poly + t, ctx->poly + src, w * 8, cudaMemcpyDeviceToDevice, ctx->st));
+    return ks_batch(ctx, &t, &d0, &d1, 1, evk, limbs);
+}
+
+// ---- composite operators ------------------------------------------------------
+int afhe_eval_add(afhe_ctx* ctx, uint64_t a0, uint64_t a1, uint64_t b0, uint64_t b1, uint64_t d0, uint64_t d1,
+                  uint32_t limbs) {
+    int rc = afhe_poly_add(ctx, a0, b0, d0, limbs);
+    if (rc != AFHE_OK) return rc;
+    return afhe_poly_add(ctx, a1, b1, d1, limbs);
+}
+
+int afhe_eval_sub_plain(afhe_ctx* ctx, uint64_t a0, uint64_t a1, uint64_t pt, uint64_t d0, uint64_t d1, uint32_t limbs) {
+    int rc = afhe_poly_sub(ctx, a0, pt, d0, limbs);
+    if (rc != AFHE_OK) return rc;
+    if (a1 != d1) {
+        if ((rc = check_poly(ctx, a1, limbs)) || (rc = check_poly(ctx, d1, limbs))) return rc;
+        CK(cudaMemcpyAsync(ctx->poly + d1, ctx->poly + a1, (u64)limbs * ctx->n * 8, cudaMemcpyDeviceToDevice, ctx->st));
+    }
+    return AFHE_OK;
+}
+
+int afhe_eval_mult_relin_rescale_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const afhe_ct_ref* b, const afhe_ct_ref* d,
+                                       uint32_t count, uint32_t limbs) {
+    if (!ctx || (!a && count) || (!b && count) || (!d && count)) return fail(ctx, AFHE_E_ARG, "null argument");
+    int rc;
+    if ((rc = check_limbs(ctx, limbs, 2))) return rc;
+    for (uint32_t i = 0; i < count; ++i)
+        if ((rc = check_poly(ctx, a[i].c0_offset, limbs)) || (rc = check_poly(ctx, a[i].c1_offset, limbs)) ||
+            (rc = check_poly(ctx, b[i].c0_offset, limbs)) || (rc = check_poly(ctx, b[i].c1_offset, limbs)) ||
+            (rc = check_poly(ctx, d[i].c0_offset, limbs - 1)) || (rc = check_poly(ctx, d[i].c1_offset, limbs - 1)))
+            return rc;
+    return for_chunks(count, [&](uint32_t s, uint32_t m) { return mult_relin_rescale_batch(ctx, a + s, b + s, d + s, m, limbs); });
+}
+
+int afhe_eval_mult_relin_rescale(afhe_ctx* ctx, uint64_t a0, uint64_t a1, uint64_t b0, uint64_t b1, uint64_t d0,
+                                 uint64_t d1, uint32_t limbs) {
+    afhe_ct_ref a{a0, a1}, b{b0, b1}, d{d0, d1};
+    return afhe_eval_mult_relin_rescale_batch(ctx, &a, &b, &d, 1, limbs);
+}
+
+int afhe_eval_mult_plain_rescale(afhe_ctx* ctx, uint64_t a0, uint64_t a1, uint64_t pt, uint64_t d0, uint64_t d1,
+                                 uint32_t limbs) {
+    if (!ctx) return fail(nullptr, AFHE_E_ARG, "null context");
+    int rc;
+    if ((rc = check_limbs(ctx, limbs, 2)) || (rc = check_poly(ctx, a0, limbs)) || (rc = check_poly(ctx, a1, limbs)) ||
+        (rc = check_poly(ctx, pt, limbs)) || (rc = check_poly(ctx, d0, limbs - 1)) || (rc = check_poly(ctx, d1, limbs - 1)))
+        return rc;
+    // fhe_host_driver.cpp:308-329: (c0 * pt, c1 * pt), then rescale
+    u64 A[2] = {a0, a1}, B[2] = {pt, pt}, T[2] = {lane_temp(ctx, 0, 0), lane_temp(ctx, 0, 1)};
+    if ((rc = ew_batch(ctx, EW_MUL, A, B, T, 2, limbs)) != AFHE_OK) return rc;
+    return rescale_batch(ctx, &T[0], &T[1], &d0, &d1, 1, limbs);
+}
+
+int afhe_eval_rotate_single_step(afhe_ctx* ctx, uint64_t i0, uint64_t i1, uint64_t d0, uint64_t d1, int32_t step,
+                                 uint32_t limbs) {
+    if (!ctx) return fail(nullptr, AFHE_E_ARG, "null context");
+    int rc;
+    if ((rc = check_limbs(ctx, limbs, 1)) || (rc = check_poly(ctx, i0, limbs)) || (rc = check_poly(ctx, i1, limbs)) ||
+        (rc = check_poly(ctx, d0, limbs)) || (rc = check_poly(ctx, d1, limbs)))
+        return rc;
+    return rotate_step_batch(ctx, &i0, &i1, &d0, &d1, 1, step, limbs);
+}
+
+int afhe_eval_rotate_batch(afhe_ctx* ctx, const afhe_ct_ref* in, const afhe_ct_ref* dst, uint32_t count, int32_t total,
+                           uint32_t limbs) {
+    if (!ctx || (!in && count) || (!dst && count)) return fail(ctx, AFHE_E_ARG, "null argument");
+    int rc;
+    if ((rc = check_limbs(ctx, limbs, 1))) return rc;
+    for (uint32_t i = 0; i < count; ++i)
+        if ((rc = check_poly(ctx, in[i].c0_offset, limbs)) || (rc = check_poly(ctx, in[i].c1_offset, limbs)) ||
+            (rc = check_poly(ctx, dst[i].c0_offset, limbs)) || (rc = check_poly(ctx, dst[i].c1_offset, limbs)))
+            return rc;
+    return for_chunks(count, [&](uint32_t s, uint32_t m) { return rotate_batch(ctx, in + s, dst + s, m, total, limbs); });
+}
+
+int afhe_eval_rotate(afhe_ctx* ctx, uint64_t i0, uint64_t i1, uint64_t d0, uint64_t d1, int32_t total, uint32_t limbs) {
+    afhe_ct_ref in{i0, i1}, d{d0, d1};
+    return afhe_eval_rotate_batch(ctx, &in, &d, 1, total, limbs);
+}
+
+}  // extern "C"

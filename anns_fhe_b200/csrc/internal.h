@@ -1,0 +1,159 @@
+// internal.h -- context state and launch helpers shared by the CUDA sources.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/afhe.h"
+#include "modarith.cuh"
+#include "ntt.cuh"
+
+namespace afhe {
+
+// Table pointers an operator needs at one level (device memory). Every
+// constant that multiplies through Shoup comes with its companion (_sh).
+struct OpTabs {
+    PrimeTables pt;
+    uint32_t p_base;   // table index of special prime 0
+    uint32_t sizeQl;   // level these tables are for
+    uint32_t parts;    // digits at this level
+    uint32_t alpha;
+    const u64* qhat_inv[AFHE_MAX_PARTS];
+    const u64* qhat_inv_sh[AFHE_MAX_PARTS];
+    const u64* qhat_modp[AFHE_MAX_PARTS];
+    const u64* qhat_modp_sh[AFHE_MAX_PARTS];
+    const u64* p_inv_mod_q;
+    const u64* p_inv_mod_q_sh;
+    const u64* phat_inv_modp;
+    const u64* phat_inv_modp_sh;
+    const u64* phat_modq;       // [K][sizeQl]
+    const u64* phat_modq_sh;
+    const u64* qlql;
+    const u64* qlql_sh;
+    const u64* qlinv;
+    const u64* qlinv_sh;
+};
+
+// Owned device storage for one twiddle table set.
+struct DevPrimeSet {
+    PrimeConst* pc = nullptr;
+    u64* tw = nullptr;
+    u64* tw_sh = nullptr;
+    u64* itw = nullptr;
+    u64* itw_sh = nullptr;
+    uint32_t count = 0;
+    PrimeTables view() const { return PrimeTables{pc, tw, tw_sh, itw, itw_sh}; }
+};
+
+struct RotKey {
+    int32_t step;
+    uint32_t galois;
+    u64 evk_offset;
+    uint32_t* map;   // device, N entries
+};
+
+// Key-switch job templates for one level (device arrays).
+struct LevelJobs {
+    LimbJob* modup = nullptr;   // per (digit, complementary limb)
+    uint32_t n_modup = 0;
+};
+
+}  // namespace afhe
+
+struct afhe_ctx {
+    afhe_params prm;
+    int log_n;
+    uint32_t n, L, K, alpha, dnum;
+    int device;
+    cudaStream_t st = nullptr;
+    afhe::u64* poly = nullptr;
+    afhe::u64* key = nullptr;
+
+    // native tables: primes q[0..L), p[0..K) at indices [0, L) and [L, L + K)
+    afhe::DevPrimeSet nat;
+    afhe::u64* lvbuf = nullptr;                 // per-level CRT tables
+    std::vector<afhe::OpTabs> lv;                // index = level (1..L)
+    afhe::LimbJob* jobs_qp = nullptr;            // slot i -> prime i, offsets i*N, for i < L + K
+    std::vector<afhe::LevelJobs> lvjobs;         // index = level
+
+    // tables loaded by OP_LOAD_CONTEXT (dispatch path)
+    bool loaded = false;
+    afhe::DevPrimeSet ld;
+    uint32_t ld_nq = 0, ld_np = 0, ld_alpha = 0, ld_parts = 0;
+    std::vector<afhe::u64> ld_q, ld_p, ld_ninv_q, ld_ninv_p;
+    afhe::u64* ld_crt = nullptr;       // raw CRT tables as loaded (device)
+    afhe::u64* ld_crt_sh = nullptr;    // per-call companions (device)
+    afhe::u64* ld_mod = nullptr;       // per-call moduli for companion prep (device)
+    size_t ld_crt_words = 0;
+    std::vector<size_t> ld_off_qhat_inv, ld_off_qhat_modp;
+    size_t ld_off_pinv = 0, ld_off_phatinv = 0, ld_off_phatmodq = 0, ld_off_qlql = 0, ld_off_qlinv = 0;
+    afhe::LimbJob* ld_jobs = nullptr;  // per-call job list (device)
+    size_t ld_jobs_cap = 0;
+
+    // scratch for composite operators (context-private)
+    afhe::u64* scr = nullptr;
+    size_t scr_words = 0;
+
+    // key directory
+    bool has_relin = false;
+    afhe::u64 relin_off = 0;
+    std::map<int32_t, afhe::RotKey> rot;
+
+    std::string err;
+};
+
+namespace afhe {
+
+// ---- kernel launchers (kernels.cu) -----------------------------------------
+enum ElemOp { EW_ADD = 0, EW_SUB = 1, EW_MUL = 2, EW_COPY = 3 };
+
+// out[l] = a[l] op b[l] for limbs l < limbs, primes from pc[prime0 + l]; z
+// entries with per-z offsets in zb (src = a, aux = b, out = out).
+cudaError_t launch_elementwise(ElemOp op, const PrimeConst* pc, uint32_t prime0, u64* arena, uint32_t n,
+                               uint32_t limbs, uint32_t nz, const ZBases& zb, cudaStream_t st);
+
+// Ciphertext tensor product operands, per z (word offsets into one arena).
+constexpr int TZMAX = 16;
+struct TensorArgs {
+    u64 a0[TZMAX], a1[TZMAX], b0[TZMAX], b1[TZMAX];
+    u64 d0[TZMAX], d1[TZMAX], d2[TZMAX];
+};
+cudaError_t launch_tensor(const PrimeConst* pc, u64* arena, uint32_t n, uint32_t limbs, uint32_t nz,
+                          const TensorArgs& ta, cudaStream_t st);
+
+// out[l][i] = a[l][map[i]]; map as u32[N] (device) or packed pairs in u64.
+cudaError_t launch_automorphism(const uint32_t* map32, const u64* map64, u64* arena, uint32_t n, uint32_t limbs,
+                                uint32_t nz, const ZBases& zb, cudaStream_t st);
+
+// Plain (I)NTT of `limbs` limbs laid out contiguously (limb i at +i*N), table
+// index prime0 + i. src arena -> dst arena, per-z offsets zb.src / zb.out.
+cudaError_t launch_ntt_plain(bool inverse, int log_n, const PrimeTables& pt, const LimbJob* jobs, uint32_t limbs,
+                             u64* src_arena, u64* dst_arena, uint32_t nz, const ZBases& zb, cudaStream_t st);
+
+// Rescale of nz polynomials at level sizeQl: zb.src = input polys (arena),
+// zb.out = outputs (arena), zb.mid = scratch for the last limb's coefficients
+// (scratch arena, N words each), zb.aux = scratch for pass intermediates
+// ((sizeQl - 1) * N words each).
+cudaError_t launch_rescale(int log_n, const OpTabs& t, const LimbJob* jobs_q, uint32_t sizeQl, u64* arena,
+                           u64* scratch, uint32_t nz, const ZBases& zb, cudaStream_t st);
+
+// Key switch of nz polynomials at level sizeQl. Per z: zb.src = input poly
+// (arena), zb.out = ks0 output, zb.aux = ks1 output (arena), zb.mid = scratch
+// region of ks_scratch_words(...) words. Key digit `part`, limb i lives at
+// key + evk_a / evk_b + (part * key_stride + (i < sizeQl ? i : key_pbase + i - sizeQl)) * N.
+size_t ks_scratch_words(uint32_t n, uint32_t L, uint32_t K, uint32_t parts);
+cudaError_t launch_key_switch(int log_n, const OpTabs& t, const LimbJob* jobs_qp, const LimbJob* jobs_modup,
+                              uint32_t n_modup, uint32_t slots_q, uint32_t sizeQl, uint32_t K,
+                              const u64* key, u64 evk_a, u64 evk_b, uint32_t key_stride, uint32_t key_pbase,
+                              u64* arena, u64* scratch, uint32_t nz, const ZBases& zb, cudaStream_t st);
+
+// Companion prep: sh[e] = shoup_companion(v[e] mod m[e], m[e]); v reduced in place.
+cudaError_t launch_companions(u64* v, u64* sh, const u64* m, size_t count, cudaStream_t st);
+// Loaded prime constants: fills pc[i] from q/ninv arrays (device) and itw.
+cudaError_t launch_prime_consts(PrimeConst* pc, const u64* q, const u64* ninv, const u64* itw, uint32_t n,
+                                uint32_t count, cudaStream_t st);
+
+}  // namespace afhe

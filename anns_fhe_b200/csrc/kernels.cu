@@ -1,0 +1,450 @@
+// kernels.cu -- CUDA kernels and launchers for the CKKS evaluation core.
+//
+// Reference functions restated here (paths inside iheydardoost/ANNS_FHE):
+//   poly_add / poly_sub / poly_mul      hardware_fpga_model/hls/src/poly_arith.cpp:3-38
+//   automorphism                        hardware_fpga_model/hls/src/automorphism.cpp:3-12
+//   rescale                             hardware_fpga_model/hls/src/rescale.cpp:3-72
+//   fast_bases_conv / approx_mod_down   hardware_fpga_model/hls/src/key_switch.cpp:7-163
+//   key_switch                          hardware_fpga_model/hls/src/key_switch.cpp:167-439
+// Fusion: the base conversions run as the prologue of the NTT that consumes
+// them; the rescale combine (a_i * q_l^-1 + NTT(...)) and the ModDown combine
+// ((x_Q - y) * P^-1) run as the NTT epilogue; the evaluation-key inner product
+// accumulates all digits of a limb in 128-bit registers and reduces once.
+#include "internal.h"
+
+namespace afhe {
+
+// ---------------------------------------------------------------------------
+// elementwise
+// ---------------------------------------------------------------------------
+template <int OP>
+__global__ void __launch_bounds__(256) elementwise_kernel(const PrimeConst* __restrict__ pc, uint32_t prime0,
+                                                          u64* __restrict__ arena, uint32_t n,
+                                                          const __grid_constant__ ZBases zb) {
+    const uint32_t l = blockIdx.y, z = blockIdx.z;
+    const PrimeConst p = pc[prime0 + l];
+    const u64 off = (u64)l * n;
+    const u64* a = arena + zb.src[z] + off;
+    const u64* b = arena + zb.aux[z] + off;
+    u64* o = arena + zb.out[z] + off;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        u64 x = a[i];
+        u64 r;
+        if (OP == EW_ADD) r = add_mod(x, b[i], p.q);
+        else if (OP == EW_SUB) r = sub_mod(x, b[i], p.q);
+        else if (OP == EW_MUL) r = mul_mod(x, b[i], modconst_of(p));
+        else r = x;
+        o[i] = r;
+    }
+}
+
+cudaError_t launch_elementwise(ElemOp op, const PrimeConst* pc, uint32_t prime0, u64* arena, uint32_t n,
+                               uint32_t limbs, uint32_t nz, const ZBases& zb, cudaStream_t st) {
+    if (limbs == 0 || nz == 0) return cudaSuccess;
+    dim3 grid((n + 255) / 256, limbs, nz);
+    switch (op) {
+    case EW_ADD: elementwise_kernel<EW_ADD><<<grid, 256, 0, st>>>(pc, prime0, arena, n, zb); break;
+    case EW_SUB: elementwise_kernel<EW_SUB><<<grid, 256, 0, st>>>(pc, prime0, arena, n, zb); break;
+    case EW_MUL: elementwise_kernel<EW_MUL><<<grid, 256, 0, st>>>(pc, prime0, arena, n, zb); break;
+    default: elementwise_kernel<EW_COPY><<<grid, 256, 0, st>>>(pc, prime0, arena, n, zb); break;
+    }
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// ciphertext tensor product (fhe_host_driver.cpp:280-286):
+//   d0 = a0*b0, d1 = a0*b1 + a1*b0, d2 = a1*b1  (d1 reduced once from 128 bits)
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) tensor_kernel(const PrimeConst* __restrict__ pc, u64* __restrict__ arena,
+                                                     uint32_t n, const __grid_constant__ TensorArgs ta) {
+    const uint32_t l = blockIdx.y, z = blockIdx.z;
+    const ModConst m = modconst_of(pc[l]);
+    const u64 off = (u64)l * n;
+    const u64* a0 = arena + ta.a0[z] + off;
+    const u64* a1 = arena + ta.a1[z] + off;
+    const u64* b0 = arena + ta.b0[z] + off;
+    const u64* b1 = arena + ta.b1[z] + off;
+    u64* d0 = arena + ta.d0[z] + off;
+    u64* d1 = arena + ta.d1[z] + off;
+    u64* d2 = arena + ta.d2[z] + off;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        u64 x0 = a0[i], x1 = a1[i], y0 = b0[i], y1 = b1[i];
+        Acc128 c;
+        acc_init(c);
+        acc_mad(c, x0, y1);
+        acc_mad(c, x1, y0);
+        d0[i] = mul_mod(x0, y0, m);
+        d1[i] = acc_reduce(c, m);
+        d2[i] = mul_mod(x1, y1, m);
+    }
+}
+
+cudaError_t launch_tensor(const PrimeConst* pc, u64* arena, uint32_t n, uint32_t limbs, uint32_t nz,
+                          const TensorArgs& ta, cudaStream_t st) {
+    if (limbs == 0 || nz == 0) return cudaSuccess;
+    dim3 grid((n + 255) / 256, limbs, nz);
+    tensor_kernel<<<grid, 256, 0, st>>>(pc, arena, n, ta);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// automorphism: out[i] = a[map[i]]
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) automorphism_kernel(const uint32_t* __restrict__ map32,
+                                                           const u64* __restrict__ map64, u64* __restrict__ arena,
+                                                           uint32_t n, const __grid_constant__ ZBases zb) {
+    const uint32_t l = blockIdx.y, z = blockIdx.z;
+    const u64 off = (u64)l * n;
+    const u64* a = arena + zb.src[z] + off;
+    u64* o = arena + zb.out[z] + off;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        uint32_t idx;
+        if (map32) idx = map32[i];
+        else {
+            u64 packed = map64[i >> 1];
+            idx = (i & 1u) ? (uint32_t)(packed >> 32) : (uint32_t)(packed & 0xFFFFFFFFull);
+        }
+        o[i] = idx < n ? a[idx] : 0ull;  // out-of-range map entries read nothing
+    }
+}
+
+cudaError_t launch_automorphism(const uint32_t* map32, const u64* map64, u64* arena, uint32_t n, uint32_t limbs,
+                                uint32_t nz, const ZBases& zb, cudaStream_t st) {
+    if (limbs == 0 || nz == 0) return cudaSuccess;
+    dim3 grid((n + 255) / 256, limbs, nz);
+    automorphism_kernel<<<grid, 256, 0, st>>>(map32, map64, arena, n, zb);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// plain transforms
+// ---------------------------------------------------------------------------
+cudaError_t launch_ntt_plain(bool inverse, int log_n, const PrimeTables& pt, const LimbJob* jobs, uint32_t limbs,
+                             u64* src_arena, u64* dst_arena, uint32_t nz, const ZBases& zb, cudaStream_t st) {
+    LoadPlain pro{src_arena};
+    StorePlain epi{dst_arena};
+    if (inverse) return launch_ntt<true>(log_n, pt, jobs, limbs, nz, dst_arena, zb, pro, epi, st);
+    return launch_ntt<false>(log_n, pt, jobs, limbs, nz, dst_arena, zb, pro, epi, st);
+}
+
+// ---------------------------------------------------------------------------
+// rescale (rescale.cpp:3-72)
+//   step 1: INTT of the last limb -> coefficients in scratch
+//   step 2: NTT over limbs i < L-1 whose prologue is the centred lift of the
+//           last limb times QlQlInvModqlDivqlModq[i], and whose epilogue is
+//           a_i * qlInvModq[i] + NTT(...)
+// ---------------------------------------------------------------------------
+struct RescaleLoad {
+    const u64* scratch;
+    const u64* qlql;
+    const u64* qlql_sh;
+    const PrimeConst* pc_last;   // q_l, the prime being dropped
+    __device__ __forceinline__ u64 operator()(const LimbJob& j, const ZBases& zb, uint32_t z, uint32_t x,
+                                              const PrimeConst& pc) const {
+        const u64 q = pc.q;
+        const u64 ql = pc_last->q, ql_half = ql >> 1;
+        u64 v = scratch[zb.aux[z] + x];                              // last limb coefficient, [0, q_l)
+        u64 vm = csub(mul_shoup_lazy(v, 1, pc.one_sh, q), q);         // v mod q_i
+        u64 qlm = csub(mul_shoup_lazy(ql, 1, pc.one_sh, q), q);       // q_l mod q_i
+        u64 val = (v > ql_half) ? sub_mod(vm, qlm, q) : vm;           // rescale.cpp:50 tie rule
+        return mul_shoup(val, __ldg(qlql + j.aux), __ldg(qlql_sh + j.aux), q);
+    }
+};
+
+struct RescaleStore {
+    u64* arena;
+    const u64* qlinv;
+    const u64* qlinv_sh;
+    __device__ __forceinline__ void operator()(const LimbJob& j, const ZBases& zb, uint32_t z, uint32_t x, u64 v,
+                                               const PrimeConst& pc) const {
+        const u64 q = pc.q;
+        u64 a = arena[zb.src[z] + j.src + x];
+        u64 s = mul_shoup(a, __ldg(qlinv + j.aux), __ldg(qlinv_sh + j.aux), q);
+        arena[zb.out[z] + j.out + x] = add_mod(s, v, q);
+    }
+};
+
+// zb.src = input poly (arena), zb.out = output poly (arena), zb.mid = scratch
+// region of sizeQl * N words per z: words [0, N) hold the last limb's
+// coefficients, words [N, sizeQl * N) the step-2 intermediates.
+cudaError_t launch_rescale(int log_n, const OpTabs& t, const LimbJob* jobs_q, uint32_t sizeQl, u64* arena,
+                           u64* scratch, uint32_t nz, const ZBases& zb_in, cudaStream_t st) {
+    if (sizeQl < 2 || nz == 0) return cudaSuccess;
+    const u64 n = 1ull << log_n;
+    const uint32_t last = sizeQl - 1;
+    // step 1: INTT(last limb). jobs_q[last] has src = dst = out = last * N.
+    ZBases z1 = zb_in;
+    for (uint32_t z = 0; z < nz; ++z) {
+        z1.mid[z] = zb_in.mid[z] - (u64)last * n;   // lands at scratch + mid[z]
+        z1.out[z] = zb_in.mid[z] - (u64)last * n;
+    }
+    cudaError_t e = launch_ntt<true>(log_n, t.pt, jobs_q + last, 1, nz, scratch, z1, LoadPlain{arena},
+                                     StorePlain{scratch}, st);
+    if (e != cudaSuccess) return e;
+    // step 2
+    ZBases z2 = zb_in;
+    for (uint32_t z = 0; z < nz; ++z) {
+        z2.aux[z] = zb_in.mid[z];            // coefficients of the last limb
+        z2.mid[z] = zb_in.mid[z] + n;        // intermediates
+    }
+    RescaleLoad pro{scratch, t.qlql, t.qlql_sh, t.pt.pc + last};
+    RescaleStore epi{arena, t.qlinv, t.qlinv_sh};
+    return launch_ntt<false>(log_n, t.pt, jobs_q, last, nz, scratch, z2, pro, epi, st);
+}
+
+// ---------------------------------------------------------------------------
+// key switch (key_switch.cpp:167-439)
+// ---------------------------------------------------------------------------
+// Scratch layout per polynomial (S = slots_q + K limb slots, Q limb i at slot
+// i, special limb k at slot slots_q + k):
+//   coef   : slots_q * N   INTT of the input's Q limbs
+//   modup  : parts * S * N digit j's complementary limbs, evaluation form
+//   ext0   : S * N         sum_j digit_j * evk_b   (then ModDown input)
+//   ext1   : S * N         sum_j digit_j * evk_a
+//   mid    : 2 * slots_q * N  two-pass intermediates of the ModDown NTTs
+size_t ks_scratch_words(uint32_t n, uint32_t slots_q, uint32_t K, uint32_t parts) {
+    const size_t S = slots_q + K;
+    return (size_t)n * (slots_q + parts * S + 2 * S + 2 * (size_t)slots_q);
+}
+
+// ModUp base conversion as the NTT prologue: job.aux = digit << 16 | k, where
+// k is the output's position among the digit's complementary primes.
+struct ModUpLoad {
+    const u64* scratch;   // coef region at zb.aux[z]
+    OpTabs t;
+    uint32_t K;
+    uint32_t n;
+    __device__ __forceinline__ u64 operator()(const LimbJob& j, const ZBases& zb, uint32_t z, uint32_t x,
+                                              const PrimeConst& pc) const {
+        const uint32_t part = j.aux >> 16, k = j.aux & 0xFFFFu;
+        const uint32_t start = part * t.alpha;
+        const uint32_t size = (part == t.parts - 1) ? t.sizeQl - start : t.alpha;
+        const uint32_t row = t.sizeQl - size + K;   // complementary primes of this digit
+        const u64 p = pc.q, p2 = p << 1;
+        const u64* qi = t.qhat_inv[part];
+        const u64* qish = t.qhat_inv_sh[part];
+        const u64* qm = t.qhat_modp[part];
+        const u64* qmsh = t.qhat_modp_sh[part];
+        u64 s = 0;
+        for (uint32_t i = 0; i < size; ++i) {
+            const uint32_t limb = start + i;
+            const u64 qq = t.pt.pc[limb].q;
+            u64 xv = scratch[zb.aux[z] + (u64)limb * n + x];
+            u64 y = mul_shoup(xv, __ldg(qi + i), __ldg(qish + i), qq);           // [x * qHatInv]_{q_i}
+            u64 w = mul_shoup_lazy(y, __ldg(qm + i * row + k), __ldg(qmsh + i * row + k), p);
+            s += w;
+            s = s >= p2 ? s - p2 : s;
+        }
+        return csub(s, p);
+    }
+};
+
+struct StoreSlot {   // plain store into scratch
+    u64* scratch;
+    __device__ __forceinline__ void operator()(const LimbJob& j, const ZBases& zb, uint32_t z, uint32_t x, u64 v,
+                                               const PrimeConst&) const {
+        scratch[zb.out[z] + j.out + x] = v;
+    }
+};
+
+// Inner product with the evaluation key. One thread per (slot, coefficient).
+// slot s < sizeQl is Q limb s, slot slots_q + k is special limb k.
+__global__ void __launch_bounds__(256) ks_mac_kernel(OpTabs t, uint32_t n, uint32_t slots_q, uint32_t sizeQl,
+                                                     uint32_t K, const u64* __restrict__ key, u64 evk_a, u64 evk_b,
+                                                     uint32_t key_stride, uint32_t key_pbase,
+                                                     const u64* __restrict__ arena, u64* __restrict__ scratch,
+                                                     u64 modup_off, u64 ext0_off, u64 ext1_off,
+                                                     const __grid_constant__ ZBases zb) {
+    const uint32_t sidx = blockIdx.y;   // 0..sizeQl+K-1
+    const uint32_t z = blockIdx.z;
+    const bool isq = sidx < sizeQl;
+    const uint32_t slot = isq ? sidx : slots_q + (sidx - sizeQl);
+    const uint32_t prime = isq ? sidx : t.p_base + (sidx - sizeQl);
+    const uint32_t klimb_in_digit = isq ? sidx : key_pbase + (sidx - sizeQl);
+    const PrimeConst pc = t.pt.pc[prime];
+    const ModConst mc = modconst_of(pc);
+    const u64 S = (u64)slots_q + K;
+    const u64 base_scr = zb.mid[z];
+    const u64* in = arena + zb.src[z] + (u64)sidx * n;   // only valid for Q limbs
+    for (uint32_t x = blockIdx.x * blockDim.x + threadIdx.x; x < n; x += gridDim.x * blockDim.x) {
+        Acc128 ab, aa;
+        acc_init(ab);
+        acc_init(aa);
+        for (uint32_t part = 0; part < t.parts; ++part) {
+            const uint32_t start = part * t.alpha;
+            const uint32_t size = (part == t.parts - 1) ? sizeQl - start : t.alpha;
+            u64 d;
+            if (isq && sidx >= start && sidx < start + size) d = in[x];
+            else d = scratch[base_scr + modup_off + ((u64)part * S + slot) * n + x];
+            const u64 kl = ((u64)part * key_stride + klimb_in_digit) * n + x;
+            acc_mad(ab, d, __ldg(key + evk_b + kl));
+            acc_mad(aa, d, __ldg(key + evk_a + kl));
+        }
+        scratch[base_scr + ext0_off + (u64)slot * n + x] = acc_reduce(ab, mc);
+        scratch[base_scr + ext1_off + (u64)slot * n + x] = acc_reduce(aa, mc);
+    }
+}
+
+// ModDown base conversion P -> Q as the NTT prologue (job = Q limb i).
+struct ModDownLoad {
+    const u64* scratch;  // ext region at zb.aux[z]
+    OpTabs t;
+    uint32_t slots_q, K, n;
+    __device__ __forceinline__ u64 operator()(const LimbJob& j, const ZBases& zb, uint32_t z, uint32_t x,
+                                              const PrimeConst& pc) const {
+        const u64 q = pc.q, q2 = q << 1;
+        const uint32_t i = j.aux;
+        u64 s = 0;
+        for (uint32_t k = 0; k < K; ++k) {
+            const PrimeConst& pk = t.pt.pc[t.p_base + k];
+            u64 xv = scratch[zb.aux[z] + (u64)(slots_q + k) * n + x];
+            u64 y = mul_shoup(xv, __ldg(t.phat_inv_modp + k), __ldg(t.phat_inv_modp_sh + k), pk.q);
+            u64 w = mul_shoup_lazy(y, __ldg(t.phat_modq + k * t.sizeQl + i), __ldg(t.phat_modq_sh + k * t.sizeQl + i), q);
+            s += w;
+            s = s >= q2 ? s - q2 : s;
+        }
+        return csub(s, q);
+    }
+};
+
+// ModDown combine as the NTT epilogue: out = (x_Q - y) * P^-1 mod q_i.
+struct ModDownStore {
+    const u64* scratch;  // ext region at zb.src[z]
+    u64* arena;          // output at zb.out[z]
+    OpTabs t;
+    uint32_t n;
+    __device__ __forceinline__ void operator()(const LimbJob& j, const ZBases& zb, uint32_t z, uint32_t x, u64 v,
+                                               const PrimeConst& pc) const {
+        const u64 q = pc.q;
+        const uint32_t i = j.aux;
+        u64 xq = scratch[zb.src[z] + (u64)i * n + x];
+        u64 d = sub_mod(xq, v, q);
+        arena[zb.out[z] + (u64)i * n + x] = mul_shoup(d, __ldg(t.p_inv_mod_q + i), __ldg(t.p_inv_mod_q_sh + i), q);
+    }
+};
+
+cudaError_t launch_key_switch(int log_n, const OpTabs& t, const LimbJob* jobs_qp, const LimbJob* jobs_modup,
+                              uint32_t n_modup, uint32_t slots_q, uint32_t sizeQl, uint32_t K, const u64* key,
+                              u64 evk_a, u64 evk_b, uint32_t key_stride, uint32_t key_pbase, u64* arena,
+                              u64* scratch, uint32_t nz, const ZBases& zb, cudaStream_t st) {
+    if (nz == 0) return cudaSuccess;
+    if (2 * nz > (uint32_t)ZMAX) return cudaErrorInvalidValue;
+    const u64 n = 1ull << log_n;
+    const u64 S = (u64)slots_q + K;
+    const u64 off_coef = 0;
+    const u64 off_modup = off_coef + (u64)slots_q * n;
+    const u64 off_ext0 = off_modup + (u64)t.parts * S * n;
+    const u64 off_ext1 = off_ext0 + S * n;
+    const u64 off_mid = off_ext1 + S * n;
+    cudaError_t e;
+
+    // 1. INTT of the input's Q limbs -> coef (slot i at coef + i*N)
+    {
+        ZBases a = zb;
+        for (uint32_t z = 0; z < nz; ++z) { a.mid[z] = zb.mid[z] + off_coef; a.out[z] = zb.mid[z] + off_coef; }
+        e = launch_ntt<true>(log_n, t.pt, jobs_qp, sizeQl, nz, scratch, a, LoadPlain{arena}, StorePlain{scratch}, st);
+        if (e != cudaSuccess) return e;
+    }
+    // 2. ModUp: base conversion + NTT for every (digit, complementary limb)
+    {
+        ZBases a = zb;
+        for (uint32_t z = 0; z < nz; ++z) {
+            a.aux[z] = zb.mid[z] + off_coef;
+            a.mid[z] = zb.mid[z] + off_modup;
+            a.out[z] = zb.mid[z] + off_modup;
+        }
+        ModUpLoad pro{scratch, t, K, (uint32_t)n};
+        e = launch_ntt<false>(log_n, t.pt, jobs_modup, n_modup, nz, scratch, a, pro, StoreSlot{scratch}, st);
+        if (e != cudaSuccess) return e;
+    }
+    // 3. inner product with the key
+    {
+        dim3 grid((uint32_t)((n + 255) / 256), sizeQl + K, nz);
+        ks_mac_kernel<<<grid, 256, 0, st>>>(t, (uint32_t)n, slots_q, sizeQl, K, key, evk_a, evk_b, key_stride,
+                                            key_pbase, arena, scratch, off_modup, off_ext0, off_ext1, zb);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    // 4. ModDown of both accumulators: z' = 2z (ext0 -> ks0), 2z + 1 (ext1 -> ks1)
+    {
+        ZBases a{};
+        for (uint32_t z = 0; z < nz; ++z) {
+            for (uint32_t h = 0; h < 2; ++h) {
+                uint32_t zz = 2 * z + h;
+                u64 ext = zb.mid[z] + (h ? off_ext1 : off_ext0);
+                a.src[zz] = ext;
+                a.aux[zz] = ext;
+                a.mid[zz] = ext;
+                a.out[zz] = ext;
+            }
+        }
+        // 4a. INTT of the special limbs, in place
+        e = launch_ntt<true>(log_n, t.pt, jobs_qp + slots_q, K, 2 * nz, scratch, a, LoadPlain{scratch},
+                             StorePlain{scratch}, st);
+        if (e != cudaSuccess) return e;
+        // 4b. NTT over Q limbs with base-conversion prologue and ModDown epilogue
+        ZBases b{};
+        for (uint32_t z = 0; z < nz; ++z) {
+            for (uint32_t h = 0; h < 2; ++h) {
+                uint32_t zz = 2 * z + h;
+                u64 ext = zb.mid[z] + (h ? off_ext1 : off_ext0);
+                b.src[zz] = ext;
+                b.aux[zz] = ext;
+                b.mid[zz] = zb.mid[z] + off_mid + (u64)h * slots_q * n;
+                b.out[zz] = h ? zb.aux[z] : zb.out[z];
+            }
+        }
+        ModDownLoad pro{scratch, t, slots_q, K, (uint32_t)n};
+        ModDownStore epi{scratch, arena, t, (uint32_t)n};
+        e = launch_ntt<false>(log_n, t.pt, jobs_qp, sizeQl, 2 * nz, scratch, b, pro, epi, st);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+// ---------------------------------------------------------------------------
+// table preparation
+// ---------------------------------------------------------------------------
+__global__ void companions_kernel(u64* v, u64* sh, const u64* m, size_t count) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count; i += (size_t)gridDim.x * blockDim.x) {
+        u64 mod = m[i];
+        if (mod == 0) { sh[i] = 0; continue; }
+        u64 w = v[i] % mod;
+        v[i] = w;
+        sh[i] = shoup_companion(w, mod);
+    }
+}
+
+cudaError_t launch_companions(u64* v, u64* sh, const u64* m, size_t count, cudaStream_t st) {
+    if (count == 0) return cudaSuccess;
+    unsigned blocks = (unsigned)((count + 255) / 256);
+    if (blocks > 4096) blocks = 4096;
+    companions_kernel<<<blocks, 256, 0, st>>>(v, sh, m, count);
+    return cudaGetLastError();
+}
+
+__global__ void prime_consts_kernel(PrimeConst* pc, const u64* q, const u64* ninv, const u64* itw, uint32_t n,
+                                    uint32_t count) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    PrimeConst c;
+    c.q = q[i];
+    ModConst m = make_modconst(c.q);
+    c.r64 = m.r64;
+    c.r64_sh = m.r64_sh;
+    c.one_sh = m.one_sh;
+    c.ninv = ninv[i] % c.q;
+    c.ninv_sh = shoup_companion(c.ninv, c.q);
+    c.w1ninv = mul_mod(itw[(u64)i * n + 1] % c.q, c.ninv, m);
+    c.w1ninv_sh = shoup_companion(c.w1ninv, c.q);
+    pc[i] = c;
+}
+
+cudaError_t launch_prime_consts(PrimeConst* pc, const u64* q, const u64* ninv, const u64* itw, uint32_t n,
+                                uint32_t count, cudaStream_t st) {
+    if (count == 0) return cudaSuccess;
+    prime_consts_kernel<<<(count + 63) / 64, 64, 0, st>>>(pc, q, ninv, itw, n, count);
+    return cudaGetLastError();
+}
+
+}  // namespace afhe

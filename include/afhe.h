@@ -1,0 +1,227 @@
+/* afhe.h -- C ABI of the B200-native CKKS evaluation core.
+ *
+ * Drop-in for the accelerator path of iheydardoost/ANNS_FHE:
+ *   * afhe_dispatch() replaces the kernel ABI `extern "C" fhe_accel_top(...)`
+ *     (hardware_fpga_model/hls/src/fhe_accel_top.h:6-56, op codes
+ *     hardware_fpga_model/hls/src/hls_params.h:18-26) with identical op
+ *     semantics over identical 64-bit word offsets into poly_gmem / key_gmem;
+ *   * afhe_eval_*() replace the composite operators of FHEHostDriver
+ *     (cpp_host_model/src/fhe_host_driver.h:78-110) with the same argument
+ *     order (c0/c1 offsets separately, then a limb count);
+ *   * the arenas replace SimMemoryBus (cpp_host_model/src/sim_memory_bus.h:10-34):
+ *     they live in device memory (HBM) and are addressed in 64-bit words.
+ *
+ * Conventions: plain pointers and sizes only; every function returns an
+ * afhe_status and never throws; work is queued on the context's CUDA stream
+ * and ordered; afhe_sync() waits for it. One context is not safe to drive from
+ * two host threads at once; separate contexts are independent.
+ */
+#ifndef AFHE_H
+#define AFHE_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AFHE_MAX_Q 64      /* Q primes (reference: 15 limbs total, hls_params.h:8) */
+#define AFHE_MAX_P 16      /* P primes (reference: 4) */
+#define AFHE_MAX_PARTS 16  /* key-switch digits (reference: 3) */
+
+typedef enum afhe_status {
+    AFHE_OK = 0,
+    AFHE_E_ARG = 1,      /* malformed argument (bad op code, limb count, prime mismatch) */
+    AFHE_E_RANGE = 2,    /* offset + length outside an arena (sim_memory_bus.cpp:13-15) */
+    AFHE_E_NOKEY = 3,    /* no rotation key for a step (fhe_host_driver.cpp:337-339) */
+    AFHE_E_LEVEL = 4,    /* level unsupported by the loaded tables / key */
+    AFHE_E_BUDGET = 5,   /* admission budget exceeded */
+    AFHE_E_TIMEOUT = 6,  /* a bounded device wait gave up */
+    AFHE_E_CUDA = 7,     /* CUDA runtime error (message via afhe_last_error) */
+    AFHE_E_STATE = 8     /* call order violated (e.g. op before context load) */
+} afhe_status;
+
+/* Op codes: hardware_fpga_model/hls/src/hls_params.h:18-26 */
+#define AFHE_OP_NTT 1u
+#define AFHE_OP_INTT 2u
+#define AFHE_OP_POLY_ADD 3u
+#define AFHE_OP_POLY_SUB 4u
+#define AFHE_OP_POLY_MUL_NTT 5u
+#define AFHE_OP_AUTOMORPHISM 6u
+#define AFHE_OP_KEY_SWITCH 7u
+#define AFHE_OP_RESCALE 8u
+#define AFHE_OP_LOAD_CONTEXT 99u
+
+typedef struct afhe_ctx afhe_ctx;
+
+/* Parameters of a context. Replaces FHEContextConfig
+ * (cpp_host_model/src/fhe_host_driver.h:17-53) as a runtime value. */
+typedef struct afhe_params {
+    uint32_t log_n;            /* ring degree N = 2^log_n, 10 <= log_n <= 16 */
+    uint32_t num_q;            /* L, Q primes (ciphertext limbs at the top level) */
+    uint32_t num_p;            /* K, special primes */
+    uint32_t alpha;            /* Q limbs per key-switch digit */
+    uint64_t q[AFHE_MAX_Q];    /* Q chain, q[0] first; each q == 1 mod 2N, < 2^61 */
+    uint64_t p[AFHE_MAX_P];    /* P chain */
+    uint64_t poly_words;       /* poly_gmem size in 64-bit words */
+    uint64_t key_words;        /* key_gmem size in 64-bit words */
+    int32_t device;            /* CUDA device ordinal */
+} afhe_params;
+
+/* Scalar and array registers of fhe_accel_top (fhe_accel_top.h:8-55), with
+ * offsets widened to 64 bits, ap_uint<128> Barrett constants split into
+ * (lo, hi) words, and up to AFHE_MAX_PARTS base-conversion table offsets. */
+typedef struct afhe_accel_args {
+    uint32_t op_code;
+    uint32_t active_limbs;
+    uint64_t src_a_offset, src_b_offset, dst_offset;
+    uint64_t evk_offset;
+    uint32_t prime_idx, galois_elt;         /* unused, as in the reference */
+    uint32_t sizeQl, sizeP, numPartQ, alpha;
+    uint64_t rns_primes[AFHE_MAX_Q];
+    uint64_t p_primes[AFHE_MAX_P];
+    uint64_t barrett_m_q_lo[AFHE_MAX_Q], barrett_m_q_hi[AFHE_MAX_Q];
+    uint32_t barrett_k_q[AFHE_MAX_Q];
+    uint64_t barrett_m_p_lo[AFHE_MAX_P], barrett_m_p_hi[AFHE_MAX_P];
+    uint32_t barrett_k_p[AFHE_MAX_P];
+    uint64_t n_inv_q[AFHE_MAX_Q];
+    uint64_t n_inv_p[AFHE_MAX_P];
+    uint64_t n_inv_mod_q_last;
+    uint64_t twiddles_q_offset, inv_twiddles_q_offset, twiddles_p_offset, inv_twiddles_p_offset;
+    uint64_t qhat_inv_offset[AFHE_MAX_PARTS];   /* qHatInvModq_j_offset */
+    uint64_t qhat_modp_offset[AFHE_MAX_PARTS];  /* qHatModp_j_offset */
+    uint64_t p_inv_mod_q_offset, p_hat_inv_mod_p_offset, p_hat_mod_q_offset;
+    uint64_t qlql_offset, qlinv_offset;         /* QlQlInvModqlDivqlModq, qlInvModq */
+} afhe_accel_args;
+
+/* Where afhe_ctx_write_context_tables() put the context tables in key_gmem.
+ * Same arrangement as FHEHostDriver::initialize_context_from_directory
+ * (fhe_host_driver.cpp:46-86): twiddles Q then P from word 0, inverse twiddles
+ * after them, CRT tables in 64-word-aligned slots, keys 512-word aligned after. */
+typedef struct afhe_context_layout {
+    uint64_t twiddles_q_offset, inv_twiddles_q_offset, twiddles_p_offset, inv_twiddles_p_offset;
+    uint64_t qhat_inv_offset[AFHE_MAX_PARTS];
+    uint64_t qhat_modp_offset[AFHE_MAX_PARTS];
+    uint64_t p_inv_mod_q_offset, p_hat_inv_mod_p_offset, p_hat_mod_q_offset;
+    uint64_t qlql_offset, qlinv_offset;
+    uint64_t first_free_offset;   /* 512-word aligned: where keys may start */
+    uint32_t level;               /* the sizeQl the tables were written for */
+    uint32_t num_parts;
+} afhe_context_layout;
+
+/* One ciphertext in poly_gmem for the batched entry points. */
+typedef struct afhe_ct_ref {
+    uint64_t c0_offset;
+    uint64_t c1_offset;
+} afhe_ct_ref;
+
+/* ---- host-only number theory (no GPU needed) ------------------------------ */
+/* Replaces OpenFHE's parameter generation used by
+ * integration_tools/test_vector_generator.cpp:80-177. */
+int afhe_find_ntt_primes(uint32_t log_n, uint32_t bits, uint32_t count,
+                         const uint64_t* exclude, uint32_t n_exclude, uint64_t* out);
+uint64_t afhe_min_primitive_root(uint32_t log_n, uint64_t q);
+int afhe_gen_twiddles(uint32_t log_n, uint64_t q, uint64_t psi, uint64_t* tw, uint64_t* itw);
+void afhe_barrett_constant(uint64_t q, uint64_t* m_lo, uint64_t* m_hi, uint32_t* k);
+uint64_t afhe_inv_mod(uint64_t a, uint64_t q);
+/* FindAutomorphismIndex (generate_interactive_test_vectors.cpp:297) */
+uint32_t afhe_galois_elt(uint32_t log_n, int32_t step);
+/* AutomorphismTransform's evaluation-form permutation (test_vector_generator.cpp:262-288) */
+int afhe_automorphism_map(uint32_t log_n, uint32_t galois_elt, uint32_t* map);
+/* GetPartQlHatInvModq / GetPartQlHatModp (test_vector_generator.cpp:438-463) */
+int afhe_part_qhat_tables(const uint64_t* q, uint32_t sizeQl, uint32_t alpha, uint32_t part,
+                          const uint64_t* p, uint32_t num_p, uint64_t* qhat_inv, uint64_t* qhat_modp);
+/* GetPInvModq / GetPHatInvModp / GetPHatModq (test_vector_generator.cpp:473-494) */
+int afhe_moddown_tables(const uint64_t* q, uint32_t sizeQl, const uint64_t* p, uint32_t num_p,
+                        uint64_t* p_inv_mod_q, uint64_t* p_hat_inv_mod_p, uint64_t* p_hat_mod_q);
+/* GetQlQlInvModqlDivqlModq / GetqlInvModq (test_vector_generator.cpp:309-310) */
+int afhe_rescale_tables(const uint64_t* q, uint32_t sizeQl, uint64_t* qlql, uint64_t* qlinv);
+
+const char* afhe_status_string(int status);
+const char* afhe_last_error(void);
+
+/* ---- context and arenas --------------------------------------------------- */
+/* Replaces SimMemoryBus construction (sim_memory_bus.cpp:5-10) plus the
+ * FHEHostDriver constructor: allocates poly_gmem / key_gmem in HBM and builds
+ * the per-prime and per-level device tables for the parameter set. */
+int afhe_ctx_create(const afhe_params* params, afhe_ctx** out);
+int afhe_ctx_destroy(afhe_ctx* ctx);
+int afhe_sync(afhe_ctx* ctx);
+/* The context's CUDA stream (a cudaStream_t) and arena base device pointers. */
+void* afhe_stream(afhe_ctx* ctx);
+uint64_t* afhe_poly_gmem(afhe_ctx* ctx);
+uint64_t* afhe_key_gmem(afhe_ctx* ctx);
+
+/* SimMemoryBus::write_poly / read_poly / write_key / read_key
+ * (sim_memory_bus.cpp:12-62): host <-> arena word copies (synchronous). */
+int afhe_write_poly(afhe_ctx* ctx, uint64_t word_offset, const uint64_t* src, uint64_t count);
+int afhe_read_poly(afhe_ctx* ctx, uint64_t word_offset, uint64_t* dst, uint64_t count);
+int afhe_write_key(afhe_ctx* ctx, uint64_t word_offset, const uint64_t* src, uint64_t count);
+int afhe_read_key(afhe_ctx* ctx, uint64_t word_offset, uint64_t* dst, uint64_t count);
+/* Asynchronous variants on the context stream; host buffers should be pinned. */
+int afhe_write_poly_async(afhe_ctx* ctx, uint64_t word_offset, const uint64_t* src, uint64_t count);
+int afhe_read_poly_async(afhe_ctx* ctx, uint64_t word_offset, uint64_t* dst, uint64_t count);
+int afhe_copy_poly(afhe_ctx* ctx, uint64_t dst_offset, uint64_t src_offset, uint64_t count);
+
+/* Writes the context tables for level `level` (twiddles for all Q and P primes,
+ * CRT tables for that level) into key_gmem in the reference's arrangement and
+ * reports the offsets (FHEHostDriver::initialize_context_from_directory,
+ * fhe_host_driver.cpp:18-86). */
+int afhe_ctx_write_context_tables(afhe_ctx* ctx, uint32_t level, afhe_context_layout* out);
+
+/* ---- kernel ABI ------------------------------------------------------------ */
+/* fhe_accel_top (fhe_accel_top.cpp:90-328): one op over the arenas. OP 99 copies
+ * the tables named by the offsets from key_gmem into the context (the reference
+ * keeps them in static on-chip arrays); ops 1-8 use those loaded tables. */
+int afhe_dispatch(afhe_ctx* ctx, const afhe_accel_args* args);
+
+/* ---- key directory (FHEHostDriver m_cfg.relin_key_offset / m_rot_keys) ---- */
+/* Keys are stored at full level: [a_0 .. a_{d-1}][b_0 .. b_{d-1}], each digit
+ * (L + K) * N words, d = ceil(L / alpha) -- the relinearisation-key layout of
+ * fhe_host_driver.cpp:105-117. At level l digit j limb i reads key limb i
+ * (Q limbs) or L + k (P limb k). */
+int afhe_set_relin_key(afhe_ctx* ctx, uint64_t evk_offset);
+/* RotationKeyMeta (fhe_host_driver.h:10-15); the map is computed here. */
+int afhe_add_rotation_key(afhe_ctx* ctx, int32_t step, uint64_t evk_offset);
+int afhe_has_rotation_key(afhe_ctx* ctx, int32_t step);
+
+/* ---- composite operators (FHEHostDriver, fhe_host_driver.cpp:248-404) ---- */
+int afhe_ntt(afhe_ctx* ctx, uint64_t src, uint64_t dst, uint32_t limbs);
+int afhe_intt(afhe_ctx* ctx, uint64_t src, uint64_t dst, uint32_t limbs);
+int afhe_poly_add(afhe_ctx* ctx, uint64_t a, uint64_t b, uint64_t dst, uint32_t limbs);
+int afhe_poly_sub(afhe_ctx* ctx, uint64_t a, uint64_t b, uint64_t dst, uint32_t limbs);
+int afhe_poly_mul_ntt(afhe_ctx* ctx, uint64_t a, uint64_t b, uint64_t dst, uint32_t limbs);
+int afhe_automorphism(afhe_ctx* ctx, uint64_t src, uint32_t galois_elt, uint64_t dst, uint32_t limbs);
+/* rescale c0 and c1 from `limbs` to `limbs - 1` (fhe_host_driver.cpp:362-365) */
+int afhe_rescale(afhe_ctx* ctx, uint64_t c0_in, uint64_t c1_in, uint64_t c0_out, uint64_t c1_out,
+                 uint32_t limbs);
+/* key switch one polynomial with the key at evk_offset (full-level layout):
+ * writes ks0 (sum digit * b) to dst_c0 and ks1 (sum digit * a) to dst_c1 */
+int afhe_key_switch(afhe_ctx* ctx, uint64_t src, uint64_t evk_offset, uint64_t dst_c0,
+                    uint64_t dst_c1, uint32_t limbs);
+
+int afhe_eval_add(afhe_ctx* ctx, uint64_t a_c0, uint64_t a_c1, uint64_t b_c0, uint64_t b_c1,
+                  uint64_t dst_c0, uint64_t dst_c1, uint32_t limbs);
+int afhe_eval_sub_plain(afhe_ctx* ctx, uint64_t a_c0, uint64_t a_c1, uint64_t pt,
+                        uint64_t dst_c0, uint64_t dst_c1, uint32_t limbs);
+int afhe_eval_mult_relin_rescale(afhe_ctx* ctx, uint64_t a_c0, uint64_t a_c1, uint64_t b_c0,
+                                 uint64_t b_c1, uint64_t dst_c0, uint64_t dst_c1, uint32_t in_limbs);
+int afhe_eval_mult_plain_rescale(afhe_ctx* ctx, uint64_t a_c0, uint64_t a_c1, uint64_t pt,
+                                 uint64_t dst_c0, uint64_t dst_c1, uint32_t in_limbs);
+int afhe_eval_rotate_single_step(afhe_ctx* ctx, uint64_t in_c0, uint64_t in_c1, uint64_t dst_c0,
+                                 uint64_t dst_c1, int32_t step, uint32_t limbs);
+int afhe_eval_rotate(afhe_ctx* ctx, uint64_t in_c0, uint64_t in_c1, uint64_t dst_c0,
+                     uint64_t dst_c1, int32_t total_rot, uint32_t limbs);
+
+/* ---- batched composite operators ------------------------------------------ */
+/* The same operator applied to `count` independent ciphertexts in one pass of
+ * launches; each output is bit-identical to the one-at-a-time call. */
+int afhe_eval_mult_relin_rescale_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const afhe_ct_ref* b,
+                                       const afhe_ct_ref* dst, uint32_t count, uint32_t in_limbs);
+int afhe_eval_rotate_batch(afhe_ctx* ctx, const afhe_ct_ref* in, const afhe_ct_ref* dst,
+                           uint32_t count, int32_t total_rot, uint32_t limbs);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AFHE_H */

@@ -1,0 +1,39 @@
+"""Shared test setup: the `gpu` marker, import paths and common fixtures."""
+import os
+import sys
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+
+def pytest_configure(config):
+    config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
+
+
+@pytest.fixture(scope="session")
+def lib():
+    from anns_fhe_b200 import _lib
+    return _lib.load()
+
+
+@pytest.fixture(scope="session")
+def orc():
+    from oracle.oracle import Orc
+    return Orc()
+
+
+@pytest.fixture(scope="session")
+def ref():
+    from oracle.oracle import Ref
+    if not Ref.available():
+        try:
+            from oracle.oracle import build_oracle
+            build_oracle(ref=True)
+        except Exception:
+            pass
+    if not Ref.available():
+        pytest.skip("reference HLS library not built (reference tree absent)")
+    return Ref()
