@@ -1,0 +1,256 @@
+"""Host CKKS layer: encoding, key generation, encryption and decryption.
+
+Replaces the OpenFHE calls of the reference (integration_tools/
+generate_interactive_test_vectors.cpp:161-224 KeyGen / EvalMultKeyGen /
+EvalRotateKeyGen, :383-398 and :443-447 MakeCKKSPackedPlaintext / Encrypt,
+software_golden_model/fhe_core/fhe_context_manager.cpp:81-128 and 460-512).
+Conventions (documented choices; OpenFHE-level parity is not claimed):
+
+* Encoding: slot j of m(X) is m(zeta^(5^j)), zeta = exp(i*pi/N), for
+  j < N/2; the conjugate slots hold the conjugates, so coefficients are real.
+  Rotation by r is the automorphism X -> X^(5^r mod 2N) (slot j <- j + r).
+* Secret: uniform ternary. Errors: rounded Gaussian, sigma = 3.19.
+* Switching key from s' to s (hybrid, dnum digits of alpha limbs), stored at
+  full level as [a_0 .. a_{d-1}][b_0 .. b_{d-1}], each over the L + K primes:
+      b_j = -a_j * s + e_j + [i in digit j] * (P mod q_i) * s'.
+  A rotation key for step r uses s' = sigma_{5^r}(s), matching the reference's
+  order "automorphism first, then key switch" (fhe_host_driver.cpp:331-359).
+* Public-key encryption: (v * b + e0 + m, v * a + e1), v ternary.
+
+All ring arithmetic runs on the device through the C ABI (NTT, products,
+automorphisms); the host samples randomness, encodes and decodes.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from .driver import CkksParams, FheContext, FHEHostDriver
+
+SIGMA = 3.19
+
+
+class Encoder:
+    """Canonical-embedding encoder for N/2 complex slots."""
+
+    def __init__(self, log_n: int):
+        n = 1 << log_n
+        self.n, self.slots = n, n // 2
+        m = 2 * n
+        k = np.array([pow(5, j, m) for j in range(self.slots)], dtype=np.int64)
+        self.t = (k - 1) // 2            # index of zeta^(5^j) among odd powers
+        self.tc = (m - k - 1) // 2       # its conjugate
+        self.zeta = np.exp(1j * np.pi * np.arange(n) / n)
+
+    def encode(self, values, scale: float) -> np.ndarray:
+        """Integer coefficients (int64) of round(scale * embedding^-1(values))."""
+        z = np.zeros(self.slots, dtype=np.complex128)
+        v = np.asarray(values, dtype=np.complex128)
+        z[:v.size] = v
+        M = np.zeros(self.n, dtype=np.complex128)
+        M[self.t] = scale * z
+        M[self.tc] = np.conj(scale * z)
+        y = np.fft.fft(M) / self.n
+        coef = np.rint((y * np.conj(self.zeta)).real)
+        if np.max(np.abs(coef)) >= 2.0**62:
+            raise OverflowError("encoded coefficients exceed 62 bits; lower the scale")
+        return coef.astype(np.int64)
+
+    def decode(self, coeffs, scale: float) -> np.ndarray:
+        y = np.asarray(coeffs, dtype=np.float64) * self.zeta
+        M = self.n * np.fft.ifft(y)
+        return M[self.t] / scale
+
+
+def to_rns(coef: np.ndarray, primes) -> np.ndarray:
+    """Signed integer coefficients -> limb-major residues (uint64)."""
+    out = []
+    for q in primes:
+        out.append(np.mod(coef, np.int64(q)).astype(np.uint64) if coef.dtype == np.int64
+                   else np.array([int(c) % q for c in coef], dtype=np.uint64))
+    return np.concatenate(out)
+
+
+def crt_centered(limbs: np.ndarray, primes) -> np.ndarray:
+    """Limb-major residues -> centred integer coefficients (object array)."""
+    n = limbs.size // len(primes)
+    if len(primes) == 1:
+        q = int(primes[0])
+        v = limbs.astype(object)
+        return np.where(v > q // 2, v - q, v)
+    Q = 1
+    for q in primes:
+        Q *= int(q)
+    acc = np.zeros(n, dtype=object)
+    for i, q in enumerate(primes):
+        q = int(q)
+        Qi = Q // q
+        inv = pow(Qi % q, -1, q)
+        v = limbs[i * n:(i + 1) * n].astype(object)
+        acc = acc + (v * inv % q) * Qi
+    acc = acc % Q
+    return np.where(acc > Q // 2, acc - Q, acc)
+
+
+class Slots:
+    """Bump allocator of polynomial slots ((L + K) * N words each) in poly_gmem."""
+
+    def __init__(self, params: CkksParams, start: int, end: int):
+        self.w = (params.L + params.K) * params.n
+        self.cur, self.end = start, end
+
+    def take(self, count: int = 1) -> list[int]:
+        out = []
+        for _ in range(count):
+            if self.cur + self.w > self.end:
+                raise MemoryError("poly_gmem slots exhausted")
+            out.append(self.cur)
+            self.cur += self.w
+        return out
+
+
+class CkksClient:
+    """Secret-key holder: key generation, encryption, decryption."""
+
+    def __init__(self, ctx: FheContext, slots: Slots, seed: int = 1):
+        self.ctx = ctx
+        self.drv = FHEHostDriver(ctx)
+        self.p = ctx.params
+        self.enc = Encoder(self.p.log_n)
+        self.rng = np.random.default_rng(seed)
+        self.slots = slots
+        n, L, K = self.p.n, self.p.L, self.p.K
+        self.qp = self.p.q + self.p.p
+        (self.s_slot, self.t0, self.t1, self.t2, self.t3, self.pk_b, self.pk_a) = slots.take(7)
+        s = self.rng.integers(-1, 2, n).astype(np.int64)
+        self.s_coef = s
+        self._put_ntt(self.s_slot, s, L + K)
+        # public key over Q: b = -a * s + e, a uniform (evaluation form)
+        a = self._uniform(L)
+        self.ctx.write_poly(self.pk_a, a)
+        self._put_ntt(self.t0, self._gauss(), L)
+        self.drv.poly_mul_ntt(self.pk_a, self.s_slot, self.t1, L)
+        self.drv.poly_sub(self.t0, self.t1, self.pk_b, L)
+
+    # ---- sampling helpers ----
+    def _uniform(self, limbs: int, primes=None) -> np.ndarray:
+        primes = primes or self.qp[:limbs]
+        n = self.p.n
+        return np.concatenate([self.rng.integers(0, int(q), n, dtype=np.uint64) for q in primes])
+
+    def _gauss(self) -> np.ndarray:
+        return np.rint(self.rng.normal(0.0, SIGMA, self.p.n)).astype(np.int64)
+
+    def _put_ntt(self, off: int, coef: np.ndarray, limbs: int) -> None:
+        self.ctx.write_poly(off, to_rns(coef, self.qp[:limbs]))
+        self.drv.ntt(off, off, limbs)
+
+    # ---- keys ----
+    def switch_key(self, sprime_slot: int) -> np.ndarray:
+        """Key from s' (evaluation form over L + K limbs at sprime_slot) to s."""
+        p = self.p
+        n, L, K, d = p.n, p.L, p.K, p.dnum
+        LK = L + K
+        P = 1
+        for x in p.p:
+            P *= x
+        A, B = [], []
+        for j in range(d):
+            a = self._uniform(LK)
+            self.ctx.write_poly(self.t0, a)
+            self._put_ntt(self.t1, self._gauss(), LK)                     # e_j
+            self.drv.poly_mul_ntt(self.t0, self.s_slot, self.t2, LK)       # a_j * s
+            self.drv.poly_sub(self.t1, self.t2, self.t1, LK)               # e_j - a_j s
+            g = np.zeros(LK * n, dtype=np.uint64)
+            for i in range(j * p.alpha, min((j + 1) * p.alpha, L)):
+                g[i * n:(i + 1) * n] = P % p.q[i]
+            self.ctx.write_poly(self.t3, g)
+            self.drv.poly_mul_ntt(self.t3, sprime_slot, self.t2, LK)       # gadget * s'
+            self.drv.poly_add(self.t1, self.t2, self.t1, LK)
+            A.append(a)
+            B.append(self.ctx.read_poly(self.t1, LK * n))
+        return np.concatenate(A + B)
+
+    def relin_key(self) -> np.ndarray:
+        LK = self.p.L + self.p.K
+        tmp = self.slots_tmp()
+        self.drv.poly_mul_ntt(self.s_slot, self.s_slot, tmp, LK)   # s^2
+        return self.switch_key(tmp)
+
+    def slots_tmp(self) -> int:
+        if not hasattr(self, "_tmp"):
+            self._tmp = self.slots.take(1)[0]
+        return self._tmp
+
+    def rotation_key(self, step: int) -> np.ndarray:
+        from .driver import galois_elt
+        LK = self.p.L + self.p.K
+        k = galois_elt(self.p.log_n, step)
+        self.drv.automorphism(self.s_slot, k, self.slots_tmp(), LK)
+        return self.switch_key(self._tmp)
+
+    def install_keys(self, steps, key_base: int = 0) -> int:
+        """Generate the relinearisation key and one rotation key per step,
+        write them to key_gmem from key_base and register them. Returns the
+        first free key word."""
+        kw = self.p.key_words()
+        off = key_base
+        self.ctx.write_key(off, self.relin_key())
+        self.drv.set_relin_key(off)
+        off += kw
+        for s in sorted(set(steps)):
+            self.ctx.write_key(off, self.rotation_key(s))
+            self.drv.add_rotation_key(s, off)
+            off += kw
+        return off
+
+    # ---- encryption ----
+    def encrypt_coef(self, coef: np.ndarray, c0: int, c1: int, level: int | None = None) -> None:
+        """Public-key encryption of integer coefficients into (c0, c1)."""
+        L = level or self.p.L
+        self._put_ntt(self.t0, self.rng.integers(-1, 2, self.p.n).astype(np.int64), L)   # v
+        self._put_ntt(self.t1, self._gauss(), L)                                          # e0
+        self._put_ntt(self.t2, self._gauss(), L)                                          # e1
+        self._put_ntt(self.t3, coef, L)                                                   # m
+        self.drv.poly_mul_ntt(self.t0, self.pk_b, c0, L)
+        self.drv.poly_add(c0, self.t1, c0, L)
+        self.drv.poly_add(c0, self.t3, c0, L)
+        self.drv.poly_mul_ntt(self.t0, self.pk_a, c1, L)
+        self.drv.poly_add(c1, self.t2, c1, L)
+
+    def encrypt(self, values, scale: float, c0: int, c1: int, level: int | None = None) -> None:
+        self.encrypt_coef(self.enc.encode(values, scale), c0, c1, level)
+
+    def decrypt_coef(self, c0: int, c1: int, level: int) -> np.ndarray:
+        self.drv.poly_mul_ntt(c1, self.s_slot, self.t0, level)
+        self.drv.poly_add(c0, self.t0, self.t0, level)
+        self.drv.intt(self.t0, self.t0, level)
+        limbs = self.ctx.read_poly(self.t0, level * self.p.n)
+        return crt_centered(limbs, self.p.q[:level])
+
+    def decrypt(self, c0: int, c1: int, level: int, scale: float) -> np.ndarray:
+        coef = self.decrypt_coef(c0, c1, level).astype(np.float64)
+        return self.enc.decode(coef, scale)
+
+    def decrypt_host(self, c0_limbs: np.ndarray, c1_limbs: np.ndarray, level: int, scale: float) -> np.ndarray:
+        """Decrypt a ciphertext the server returned as host arrays."""
+        n = self.p.n
+        off0, off1 = self.slots_pair()
+        self.ctx.write_poly(off0, c0_limbs[:level * n])
+        self.ctx.write_poly(off1, c1_limbs[:level * n])
+        return self.decrypt(off0, off1, level, scale)
+
+    def slots_pair(self) -> tuple[int, int]:
+        if not hasattr(self, "_pair"):
+            self._pair = tuple(self.slots.take(2))
+        return self._pair
+
+    def plaintext(self, values, scale: float, off: int, level: int) -> None:
+        """Encode `values` into an evaluation-form plaintext at `off` (level limbs)."""
+        self._put_ntt(off, self.enc.encode(values, scale), level)
+
+
+def encode_plaintext(ctx: FheContext, enc: Encoder, values, scale: float, off: int, level: int) -> None:
+    """Server-side plaintext encoding (no secret involved)."""
+    coef = enc.encode(values, scale)
+    ctx.write_poly(off, to_rns(coef, ctx.params.q[:level]))
+    FHEHostDriver(ctx).ntt(off, off, level)

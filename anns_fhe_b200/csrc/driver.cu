@@ -26,6 +26,13 @@ int check_limbs(afhe_ctx* ctx, uint32_t limbs, uint32_t min_limbs) {
     return AFHE_OK;
 }
 
+// Primitive operators also accept "extended" polynomials over all L + K
+// primes (Q limbs then P limbs), as key generation needs.
+int check_limbs_ext(afhe_ctx* ctx, uint32_t limbs) {
+    if (limbs < 1 || limbs > ctx->L + ctx->K) return fail(ctx, AFHE_E_LEVEL, "limb count outside [1, L + K]");
+    return AFHE_OK;
+}
+
 int check_poly(afhe_ctx* ctx, u64 off, uint32_t limbs) {
     if (!range_ok(off, (u64)limbs * ctx->n, ctx->prm.poly_words)) return fail(ctx, AFHE_E_RANGE, "operand out of poly_gmem");
     return AFHE_OK;
@@ -237,7 +244,7 @@ int afhe_has_rotation_key(afhe_ctx* ctx, int32_t step) { return ctx && ctx->rot.
 static int ntt_native(afhe_ctx* ctx, bool inv, uint64_t src, uint64_t dst, uint32_t limbs) {
     if (!ctx) return fail(nullptr, AFHE_E_ARG, "null context");
     int rc;
-    if ((rc = check_limbs(ctx, limbs, 1)) || (rc = check_poly(ctx, src, limbs)) || (rc = check_poly(ctx, dst, limbs))) return rc;
+    if ((rc = check_limbs_ext(ctx, limbs)) || (rc = check_poly(ctx, src, limbs)) || (rc = check_poly(ctx, dst, limbs))) return rc;
     const u64 w = (u64)limbs * ctx->n;
     u64 s = src;
     if (src != dst && overlap(src, w, dst, w)) {
@@ -256,7 +263,7 @@ int afhe_intt(afhe_ctx* ctx, uint64_t src, uint64_t dst, uint32_t limbs) { retur
 static int ew_single(afhe_ctx* ctx, ElemOp op, uint64_t a, uint64_t b, uint64_t dst, uint32_t limbs) {
     if (!ctx) return fail(nullptr, AFHE_E_ARG, "null context");
     int rc;
-    if ((rc = check_limbs(ctx, limbs, 1)) || (rc = check_poly(ctx, a, limbs)) || (rc = check_poly(ctx, b, limbs)) ||
+    if ((rc = check_limbs_ext(ctx, limbs)) || (rc = check_poly(ctx, a, limbs)) || (rc = check_poly(ctx, b, limbs)) ||
         (rc = check_poly(ctx, dst, limbs)))
         return rc;
     const u64 w = (u64)limbs * ctx->n;
@@ -279,7 +286,7 @@ int afhe_poly_mul_ntt(afhe_ctx* c, uint64_t a, uint64_t b, uint64_t d, uint32_t 
 int afhe_automorphism(afhe_ctx* ctx, uint64_t src, uint32_t galois, uint64_t dst, uint32_t limbs) {
     if (!ctx) return fail(nullptr, AFHE_E_ARG, "null context");
     int rc;
-    if ((rc = check_limbs(ctx, limbs, 1)) || (rc = check_poly(ctx, src, limbs)) || (rc = check_poly(ctx, dst, limbs))) return rc;
+    if ((rc = check_limbs_ext(ctx, limbs)) || (rc = check_poly(ctx, src, limbs)) || (rc = check_poly(ctx, dst, limbs))) return rc;
     if ((galois & 1u) == 0 || galois >= 2 * ctx->n) return fail(ctx, AFHE_E_ARG, "galois element must be odd and < 2N");
     std::vector<uint32_t> map(ctx->n);
     automorphism_map(ctx->log_n, galois, map.data());
@@ -392,6 +399,81 @@ int afhe_eval_rotate_batch(afhe_ctx* ctx, const afhe_ct_ref* in, const afhe_ct_r
             (rc = check_poly(ctx, dst[i].c0_offset, limbs)) || (rc = check_poly(ctx, dst[i].c1_offset, limbs)))
             return rc;
     return for_chunks(count, [&](uint32_t s, uint32_t m) { return rotate_batch(ctx, in + s, dst + s, m, total, limbs); });
+}
+
+static int check_cts(afhe_ctx* ctx, const afhe_ct_ref* v, uint32_t count, uint32_t limbs) {
+    int rc;
+    for (uint32_t i = 0; i < count; ++i)
+        if ((rc = check_poly(ctx, v[i].c0_offset, limbs)) || (rc = check_poly(ctx, v[i].c1_offset, limbs))) return rc;
+    return AFHE_OK;
+}
+
+// Batched elementwise composites: ciphertext i of the batch is computed
+// exactly as the single call would; distinct batch entries must not overlap
+// each other's outputs (in-place per entry is fine).
+int afhe_eval_add_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const afhe_ct_ref* b, const afhe_ct_ref* d,
+                        uint32_t count, uint32_t limbs) {
+    if (!ctx || (count && (!a || !b || !d))) return fail(ctx, AFHE_E_ARG, "null argument");
+    int rc;
+    if ((rc = check_limbs(ctx, limbs, 1)) || (rc = check_cts(ctx, a, count, limbs)) ||
+        (rc = check_cts(ctx, b, count, limbs)) || (rc = check_cts(ctx, d, count, limbs)))
+        return rc;
+    return for_chunks(count, [&](uint32_t s, uint32_t m) {
+        u64 A[2 * TZMAX], B[2 * TZMAX], D[2 * TZMAX];
+        for (uint32_t z = 0; z < m; ++z) {
+            A[2 * z] = a[s + z].c0_offset; A[2 * z + 1] = a[s + z].c1_offset;
+            B[2 * z] = b[s + z].c0_offset; B[2 * z + 1] = b[s + z].c1_offset;
+            D[2 * z] = d[s + z].c0_offset; D[2 * z + 1] = d[s + z].c1_offset;
+        }
+        return ew_batch(ctx, EW_ADD, A, B, D, 2 * m, limbs);
+    });
+}
+
+int afhe_eval_sub_plain_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const uint64_t* pt, const afhe_ct_ref* d,
+                              uint32_t count, uint32_t limbs) {
+    if (!ctx || (count && (!a || !pt || !d))) return fail(ctx, AFHE_E_ARG, "null argument");
+    int rc;
+    if ((rc = check_limbs(ctx, limbs, 1)) || (rc = check_cts(ctx, a, count, limbs)) || (rc = check_cts(ctx, d, count, limbs)))
+        return rc;
+    for (uint32_t i = 0; i < count; ++i)
+        if ((rc = check_poly(ctx, pt[i], limbs))) return rc;
+    return for_chunks(count, [&](uint32_t s, uint32_t m) {
+        u64 A[TZMAX], P[TZMAX], D[TZMAX];
+        for (uint32_t z = 0; z < m; ++z) { A[z] = a[s + z].c0_offset; P[z] = pt[s + z]; D[z] = d[s + z].c0_offset; }
+        int r = ew_batch(ctx, EW_SUB, A, P, D, m, limbs);
+        if (r != AFHE_OK) return r;
+        for (uint32_t z = 0; z < m; ++z) { A[z] = a[s + z].c1_offset; D[z] = d[s + z].c1_offset; }
+        uint32_t k = 0;
+        u64 A2[TZMAX], D2[TZMAX];
+        for (uint32_t z = 0; z < m; ++z)
+            if (A[z] != D[z]) { A2[k] = A[z]; D2[k] = D[z]; ++k; }
+        return k ? ew_batch(ctx, EW_COPY, A2, nullptr, D2, k, limbs) : AFHE_OK;
+    });
+}
+
+int afhe_eval_mult_plain_rescale_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const uint64_t* pt, const afhe_ct_ref* d,
+                                       uint32_t count, uint32_t limbs) {
+    if (!ctx || (count && (!a || !pt || !d))) return fail(ctx, AFHE_E_ARG, "null argument");
+    int rc;
+    if ((rc = check_limbs(ctx, limbs, 2)) || (rc = check_cts(ctx, a, count, limbs)) ||
+        (rc = check_cts(ctx, d, count, limbs - 1)))
+        return rc;
+    for (uint32_t i = 0; i < count; ++i)
+        if ((rc = check_poly(ctx, pt[i], limbs))) return rc;
+    return for_chunks(count, [&](uint32_t s, uint32_t m) {
+        u64 A[2 * TZMAX], P[2 * TZMAX], T[2 * TZMAX], t0[TZMAX], t1[TZMAX], o0[TZMAX], o1[TZMAX];
+        for (uint32_t z = 0; z < m; ++z) {
+            t0[z] = lane_temp(ctx, z, 0);
+            t1[z] = lane_temp(ctx, z, 1);
+            A[2 * z] = a[s + z].c0_offset; A[2 * z + 1] = a[s + z].c1_offset;
+            P[2 * z] = pt[s + z]; P[2 * z + 1] = pt[s + z];
+            T[2 * z] = t0[z]; T[2 * z + 1] = t1[z];
+            o0[z] = d[s + z].c0_offset; o1[z] = d[s + z].c1_offset;
+        }
+        int r = ew_batch(ctx, EW_MUL, A, P, T, 2 * m, limbs);
+        if (r != AFHE_OK) return r;
+        return rescale_batch(ctx, t0, t1, o0, o1, m, limbs);
+    });
 }
 
 int afhe_eval_rotate(afhe_ctx* ctx, uint64_t i0, uint64_t i1, uint64_t d0, uint64_t d1, int32_t total, uint32_t limbs) {

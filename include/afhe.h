@@ -186,6 +186,9 @@ int afhe_add_rotation_key(afhe_ctx* ctx, int32_t step, uint64_t evk_offset);
 int afhe_has_rotation_key(afhe_ctx* ctx, int32_t step);
 
 /* ---- composite operators (FHEHostDriver, fhe_host_driver.cpp:248-404) ---- */
+/* The primitives (afhe_ntt .. afhe_automorphism) also accept polynomials over
+ * all L + K primes (Q limbs, then P limbs), as key generation needs; the
+ * ciphertext operators take 1..L limbs. */
 int afhe_ntt(afhe_ctx* ctx, uint64_t src, uint64_t dst, uint32_t limbs);
 int afhe_intt(afhe_ctx* ctx, uint64_t src, uint64_t dst, uint32_t limbs);
 int afhe_poly_add(afhe_ctx* ctx, uint64_t a, uint64_t b, uint64_t dst, uint32_t limbs);
@@ -220,6 +223,13 @@ int afhe_eval_mult_relin_rescale_batch(afhe_ctx* ctx, const afhe_ct_ref* a, cons
                                        const afhe_ct_ref* dst, uint32_t count, uint32_t in_limbs);
 int afhe_eval_rotate_batch(afhe_ctx* ctx, const afhe_ct_ref* in, const afhe_ct_ref* dst,
                            uint32_t count, int32_t total_rot, uint32_t limbs);
+int afhe_eval_add_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const afhe_ct_ref* b, const afhe_ct_ref* dst,
+                        uint32_t count, uint32_t limbs);
+/* pt[i] is the plaintext polynomial offset for ciphertext i */
+int afhe_eval_sub_plain_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const uint64_t* pt, const afhe_ct_ref* dst,
+                              uint32_t count, uint32_t limbs);
+int afhe_eval_mult_plain_rescale_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const uint64_t* pt,
+                                       const afhe_ct_ref* dst, uint32_t count, uint32_t in_limbs);
 
 #ifdef __cplusplus
 }

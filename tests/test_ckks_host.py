@@ -1,0 +1,59 @@
+"""Host-side CKKS pieces that need no GPU: the encoder's round trip, the slot
+rotation convention (X -> X^(5^r) rotates slots left by r), RNS conversion and
+CRT reconstruction, the IVF-PQ index and the rotation-key set of the chain."""
+import numpy as np
+
+from anns_fhe_b200.ckks import Encoder, crt_centered, to_rns
+from anns_fhe_b200.ivfpq import IvfPqIndex, gaussian_mixture, plaintext_search
+from anns_fhe_b200.query import pow2_steps
+
+
+def coef_automorphism(coef: np.ndarray, k: int) -> np.ndarray:
+    n = coef.size
+    out = np.zeros(n, dtype=np.float64)
+    for i, c in enumerate(coef):
+        e = i * k % (2 * n)
+        if e < n:
+            out[e] += c
+        else:
+            out[e - n] -= c
+    return out
+
+
+def test_encoder_roundtrip_and_rotation():
+    enc = Encoder(10)
+    rng = np.random.default_rng(0)
+    z = rng.normal(0, 10, enc.slots)
+    scale = 2.0**30
+    coef = enc.encode(z, scale)
+    assert np.max(np.abs(enc.decode(coef, scale).real - z)) < 1e-6
+    for r in (1, 3, -2):
+        k = pow(5, r % (enc.n // 2), 2 * enc.n)
+        rot = enc.decode(coef_automorphism(coef.astype(np.float64), k), scale).real
+        assert np.max(np.abs(rot - np.roll(z, -r))) < 1e-6
+
+
+def test_rns_crt_roundtrip():
+    q = [1125899906826241, 1125899906629633, 1125899906596865]
+    rng = np.random.default_rng(1)
+    v = rng.integers(-(2**62), 2**62, 64, dtype=np.int64)
+    for k in (1, 2, 3):
+        back = crt_centered(to_rns(v, q[:k]), q[:k])
+        if k >= 2:
+            assert [int(x) for x in back] == [int(x) for x in v]
+        else:
+            assert all((int(a) - int(b)) % q[0] == 0 for a, b in zip(back, v))
+
+
+def test_ivfpq_index_and_plaintext_search():
+    X = gaussian_mixture(2048, 32, 16, 0.1, 5)
+    idx = IvfPqIndex.train(X, n_list=16, M=4, K=32, seed=5, iters=10)
+    assert sum(len(v) for v in idx.lists) == len(X)
+    probes, cand, dist, top = plaintext_search(idx, X[0], nprobe=2, top_k=5)
+    assert len(top) == 5 and idx.assignments[0] in probes
+
+
+def test_pow2_steps():
+    assert pow2_steps(63 * 5) == [256, 32, 16, 8, 2, 1]
+    assert pow2_steps(-6) == [4, 2]
+    assert sum(pow2_steps(12345)) == 12345
