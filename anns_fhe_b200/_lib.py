@@ -118,6 +118,9 @@ SIGNATURES = {
     "afhe_eval_rotate": (C.c_int, [CTX, u64, u64, u64, u64, i32, u32]),
     "afhe_eval_mult_relin_rescale_batch": (C.c_int, [CTX, C.POINTER(CtRef), C.POINTER(CtRef), C.POINTER(CtRef), u32, u32]),
     "afhe_eval_rotate_batch": (C.c_int, [CTX, C.POINTER(CtRef), C.POINTER(CtRef), u32, i32, u32]),
+    "afhe_ntt_batch": (C.c_int, [CTX, P64, u32, u32, C.c_int]),
+    "afhe_kernel_launches": (u64, []),
+    "afhe_eval_rotate_accumulate_batch": (C.c_int, [CTX, C.POINTER(CtRef), C.POINTER(CtRef), u32, i32, u32]),
     "afhe_eval_add_batch": (C.c_int, [CTX, C.POINTER(CtRef), C.POINTER(CtRef), C.POINTER(CtRef), u32, u32]),
     "afhe_eval_sub_plain_batch": (C.c_int, [CTX, C.POINTER(CtRef), P64, C.POINTER(CtRef), u32, u32]),
     "afhe_eval_mult_plain_rescale_batch": (C.c_int, [CTX, C.POINTER(CtRef), P64, C.POINTER(CtRef), u32, u32]),

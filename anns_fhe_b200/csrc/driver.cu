@@ -44,8 +44,10 @@ int check_key(afhe_ctx* ctx, u64 evk) {
     return AFHE_OK;
 }
 
-// Key switch nz polynomials (poly_gmem-relative offsets) with one key.
-int ks_batch(afhe_ctx* ctx, const u64* in, const u64* out0, const u64* out1, uint32_t nz, u64 evk, uint32_t limbs) {
+// Key switch nz polynomials (poly_gmem-relative offsets) with one key, with
+// optional fusion (automorphism gather, c0 add, accumulate; see KsFuse).
+int ks_batch(afhe_ctx* ctx, const u64* in, const u64* out0, const u64* out1, uint32_t nz, u64 evk, uint32_t limbs,
+             const KsFuse* fuse = nullptr) {
     const u64 n = ctx->n, S = (u64)ctx->L + ctx->K;
     const OpTabs& t = ctx->lv[limbs];
     const LevelJobs& lj = ctx->lvjobs[limbs];
@@ -57,7 +59,8 @@ int ks_batch(afhe_ctx* ctx, const u64* in, const u64* out0, const u64* out1, uin
         zb.mid[z] = lane_of(ctx, z).ks;
     }
     CK(launch_key_switch(ctx->log_n, t, ctx->jobs_qp, lj.modup, lj.n_modup, ctx->L, limbs, ctx->K, ctx->key, evk,
-                         evk + (u64)ctx->dnum * S * n, (uint32_t)S, ctx->L, ctx->poly, ctx->scr, nz, zb, ctx->st));
+                         evk + (u64)ctx->dnum * S * n, (uint32_t)S, ctx->L, ctx->poly, ctx->scr, nz, zb, ctx->st,
+                         fuse));
     return AFHE_OK;
 }
 
@@ -110,56 +113,57 @@ int mult_relin_rescale_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const afhe_ct_
     }
     // 1. tensor product (fhe_host_driver.cpp:280-286)
     CK(launch_tensor(ctx->nat.pc, ctx->poly, ctx->n, limbs, nz, ta, ctx->st));
-    // 2. relinearise d2 (:288-289)
-    int rc = ks_batch(ctx, t2, k0, k1, nz, ctx->relin_off, limbs);
+    // 2-3. relinearise d2 and add (:288-293): d0 += ks0, d1 += ks1 in the
+    //      key switch's ModDown epilogue
+    KsFuse f{};
+    f.has_acc = 1;
+    for (uint32_t z = 0; z < nz; ++z) { f.acc0[z] = t0[z]; f.acc1[z] = t1[z]; }
+    int rc = ks_batch(ctx, t2, t0, t1, nz, ctx->relin_off, limbs, &f);
     if (rc != AFHE_OK) return rc;
-    // 3. d0 += ks0, d1 += ks1 (:292-293), both in one launch
-    {
-        u64 A[2 * TZMAX], B[2 * TZMAX];
-        for (uint32_t z = 0; z < nz; ++z) {
-            A[2 * z] = t0[z]; B[2 * z] = k0[z];
-            A[2 * z + 1] = t1[z]; B[2 * z + 1] = k1[z];
-        }
-        if ((rc = ew_batch(ctx, EW_ADD, A, B, A, 2 * nz, limbs)) != AFHE_OK) return rc;
-    }
+    (void)k0; (void)k1;
     // 4. rescale into the destination (:296-305)
     return rescale_batch(ctx, t0, t1, o0, o1, nz, limbs);
 }
 
-// One rotation step on nz ciphertexts: dst = (auto(c0) + ks0, ks1), KS on auto(c1)
-// (fhe_host_driver.cpp:331-359). Inputs may alias outputs.
+// One rotation step on nz ciphertexts (fhe_host_driver.cpp:331-359):
+//   dst = (auto(c0) + ks0, ks1), ks = KS(auto(c1)),
+// or, with acc, dst = acc + that. One fused key switch: the automorphism is
+// applied on the key switch's loads and the additions in its epilogue.
+// Inputs may alias outputs; acc may alias dst.
 int rotate_step_batch(afhe_ctx* ctx, const u64* in0, const u64* in1, const u64* d0, const u64* d1, uint32_t nz,
-                      int32_t step, uint32_t limbs) {
+                      int32_t step, uint32_t limbs, const u64* acc0 = nullptr, const u64* acc1 = nullptr) {
     auto it = ctx->rot.find(step);
     if (it == ctx->rot.end()) return fail(ctx, AFHE_E_NOKEY, "rotation key not found for step " + std::to_string(step));
     const RotKey& rk = it->second;
-    u64 t0[TZMAX], t1[TZMAX], k0[TZMAX], k1[TZMAX];
-    ZBases zb{};
+    KsFuse f{};
+    f.map = rk.map;
+    f.has_c0 = 1;
+    f.has_acc = acc0 != nullptr;
     for (uint32_t z = 0; z < nz; ++z) {
-        t0[z] = lane_temp(ctx, z, 0);
-        t1[z] = lane_temp(ctx, z, 1);
-        k0[z] = lane_temp(ctx, z, 3);
-        k1[z] = lane_temp(ctx, z, 4);
-        zb.src[2 * z] = in0[z]; zb.out[2 * z] = t0[z];
-        zb.src[2 * z + 1] = in1[z]; zb.out[2 * z + 1] = t1[z];
+        f.c0[z] = in0[z];
+        if (acc0) { f.acc0[z] = acc0[z]; f.acc1[z] = acc1[z]; }
     }
-    CK(launch_automorphism(rk.map, nullptr, ctx->poly, ctx->n, limbs, 2 * nz, zb, ctx->st));
-    int rc = ks_batch(ctx, t1, k0, k1, nz, rk.evk_offset, limbs);
-    if (rc != AFHE_OK) return rc;
-    if ((rc = ew_batch(ctx, EW_ADD, t0, k0, d0, nz, limbs)) != AFHE_OK) return rc;
-    return ew_batch(ctx, EW_COPY, k1, nullptr, d1, nz, limbs);
+    return ks_batch(ctx, in1, d0, d1, nz, rk.evk_offset, limbs, &f);
 }
 
 // eval_rotate on nz ciphertexts by the same amount (fhe_host_driver.cpp:361-404):
 // |r| decomposed into descending powers of two, sign kept.
 int rotate_batch(afhe_ctx* ctx, const afhe_ct_ref* in, const afhe_ct_ref* dst, uint32_t nz, int32_t total,
-                 uint32_t limbs) {
+                 uint32_t limbs, bool accumulate = false) {
     u64 i0[TZMAX], i1[TZMAX], o0[TZMAX], o1[TZMAX], c0[TZMAX], c1[TZMAX], x0[TZMAX], x1[TZMAX];
     for (uint32_t z = 0; z < nz; ++z) {
         i0[z] = in[z].c0_offset; i1[z] = in[z].c1_offset;
         o0[z] = dst[z].c0_offset; o1[z] = dst[z].c1_offset;
         x0[z] = lane_temp(ctx, z, 2);   // chain temporaries (unused by a single step)
         x1[z] = lane_temp(ctx, z, 5);
+    }
+    if (total == 0 && accumulate) {   // dst += in
+        u64 A[2 * TZMAX], B[2 * TZMAX];
+        for (uint32_t z = 0; z < nz; ++z) {
+            A[2 * z] = o0[z]; A[2 * z + 1] = o1[z];
+            B[2 * z] = i0[z]; B[2 * z + 1] = i1[z];
+        }
+        return ew_batch(ctx, EW_ADD, A, B, A, 2 * nz, limbs);
     }
     if (total == 0) {
         for (uint32_t z = 0; z < nz; ++z) {
@@ -185,7 +189,8 @@ int rotate_batch(afhe_ctx* ctx, const afhe_ct_ref* in, const afhe_ct_ref* dst, u
         bool last = k + 1 == steps.size();
         const u64* n0 = last ? o0 : x0;
         const u64* n1 = last ? o1 : x1;
-        int rc = rotate_step_batch(ctx, c0, c1, n0, n1, nz, steps[k], limbs);
+        int rc = (last && accumulate) ? rotate_step_batch(ctx, c0, c1, n0, n1, nz, steps[k], limbs, o0, o1)
+                                      : rotate_step_batch(ctx, c0, c1, n0, n1, nz, steps[k], limbs);
         if (rc != AFHE_OK) return rc;
         for (uint32_t z = 0; z < nz; ++z) { c0[z] = n0[z]; c1[z] = n1[z]; }
     }
@@ -473,6 +478,36 @@ int afhe_eval_mult_plain_rescale_batch(afhe_ctx* ctx, const afhe_ct_ref* a, cons
         int r = ew_batch(ctx, EW_MUL, A, P, T, 2 * m, limbs);
         if (r != AFHE_OK) return r;
         return rescale_batch(ctx, t0, t1, o0, o1, m, limbs);
+    });
+}
+
+int afhe_ntt_batch(afhe_ctx* ctx, const uint64_t* polys, uint32_t count, uint32_t limbs, int inverse) {
+    if (!ctx || (count && !polys)) return fail(ctx, AFHE_E_ARG, "null argument");
+    int rc;
+    if ((rc = check_limbs_ext(ctx, limbs))) return rc;
+    for (uint32_t i = 0; i < count; ++i)
+        if ((rc = check_poly(ctx, polys[i], limbs))) return rc;
+    for (uint32_t s = 0; s < count; s += ZMAX) {
+        uint32_t m = count - s < (uint32_t)ZMAX ? count - s : (uint32_t)ZMAX;
+        ZBases zb{};
+        for (uint32_t z = 0; z < m; ++z) zb.src[z] = zb.mid[z] = zb.out[z] = polys[s + z];
+        CK(launch_ntt_plain(inverse != 0, ctx->log_n, ctx->nat.view(), ctx->jobs_qp, limbs, ctx->poly, ctx->poly, m,
+                            zb, ctx->st));
+    }
+    return AFHE_OK;
+}
+
+uint64_t afhe_kernel_launches(void) { return launches_so_far(); }
+
+int afhe_eval_rotate_accumulate_batch(afhe_ctx* ctx, const afhe_ct_ref* in, const afhe_ct_ref* acc, uint32_t count,
+                                      int32_t total, uint32_t limbs) {
+    if (!ctx || (!in && count) || (!acc && count)) return fail(ctx, AFHE_E_ARG, "null argument");
+    int rc;
+    if ((rc = check_limbs(ctx, limbs, 1)) || (rc = check_cts(ctx, in, count, limbs)) ||
+        (rc = check_cts(ctx, acc, count, limbs)))
+        return rc;
+    return for_chunks(count, [&](uint32_t s, uint32_t m) {
+        return rotate_batch(ctx, in + s, acc + s, m, total, limbs, true);
     });
 }
 

@@ -108,6 +108,7 @@ struct afhe_ctx {
 namespace afhe {
 
 // ---- kernel launchers (kernels.cu) -----------------------------------------
+uint64_t launches_so_far();
 enum ElemOp { EW_ADD = 0, EW_SUB = 1, EW_MUL = 2, EW_COPY = 3 };
 
 // out[l] = a[l] op b[l] for limbs l < limbs, primes from pc[prime0 + l]; z
@@ -116,7 +117,7 @@ cudaError_t launch_elementwise(ElemOp op, const PrimeConst* pc, uint32_t prime0,
                                uint32_t limbs, uint32_t nz, const ZBases& zb, cudaStream_t st);
 
 // Ciphertext tensor product operands, per z (word offsets into one arena).
-constexpr int TZMAX = 16;
+constexpr int TZMAX = 64;
 struct TensorArgs {
     u64 a0[TZMAX], a1[TZMAX], b0[TZMAX], b1[TZMAX];
     u64 d0[TZMAX], d1[TZMAX], d2[TZMAX];
@@ -144,11 +145,25 @@ cudaError_t launch_rescale(int log_n, const OpTabs& t, const LimbJob* jobs_q, ui
 // (arena), zb.out = ks0 output, zb.aux = ks1 output (arena), zb.mid = scratch
 // region of ks_scratch_words(...) words. Key digit `part`, limb i lives at
 // key + evk_a / evk_b + (part * key_stride + (i < sizeQl ? i : key_pbase + i - sizeQl)) * N.
+// Optional fusion around a key switch (rotation and accumulation):
+//   * map: the input is read through the automorphism, x -> in[map[x]];
+//   * has_c0: ks0 output += c0[map[x]] (c0 gathered into scratch by the MAC);
+//   * has_acc: ks0 output += acc0[x], ks1 output += acc1[x].
+// So one call computes a whole rotation step, acc + rot(ct), or d + KS(d2).
+struct KsFuse {
+    const uint32_t* map;
+    int has_c0;
+    int has_acc;
+    u64 c0[ZMAX / 2];
+    u64 acc0[ZMAX / 2];
+    u64 acc1[ZMAX / 2];
+};
 size_t ks_scratch_words(uint32_t n, uint32_t L, uint32_t K, uint32_t parts);
 cudaError_t launch_key_switch(int log_n, const OpTabs& t, const LimbJob* jobs_qp, const LimbJob* jobs_modup,
                               uint32_t n_modup, uint32_t slots_q, uint32_t sizeQl, uint32_t K,
                               const u64* key, u64 evk_a, u64 evk_b, uint32_t key_stride, uint32_t key_pbase,
-                              u64* arena, u64* scratch, uint32_t nz, const ZBases& zb, cudaStream_t st);
+                              u64* arena, u64* scratch, uint32_t nz, const ZBases& zb, cudaStream_t st,
+                              const KsFuse* fuse = nullptr);
 
 // Companion prep: sh[e] = shoup_companion(v[e] mod m[e], m[e]); v reduced in place.
 cudaError_t launch_companions(u64* v, u64* sh, const u64* m, size_t count, cudaStream_t st);

@@ -10,9 +10,15 @@
 // them; the rescale combine (a_i * q_l^-1 + NTT(...)) and the ModDown combine
 // ((x_Q - y) * P^-1) run as the NTT epilogue; the evaluation-key inner product
 // accumulates all digits of a limb in 128-bit registers and reduces once.
+#include <atomic>
+
 #include "internal.h"
 
 namespace afhe {
+
+static std::atomic<uint64_t> g_launches{0};
+void count_launches(uint64_t k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
+uint64_t launches_so_far() { return g_launches.load(std::memory_order_relaxed); }
 
 // ---------------------------------------------------------------------------
 // elementwise
@@ -48,6 +54,7 @@ cudaError_t launch_elementwise(ElemOp op, const PrimeConst* pc, uint32_t prime0,
     case EW_MUL: elementwise_kernel<EW_MUL><<<grid, 256, 0, st>>>(pc, prime0, arena, n, zb); break;
     default: elementwise_kernel<EW_COPY><<<grid, 256, 0, st>>>(pc, prime0, arena, n, zb); break;
     }
+    count_launches(1);
     return cudaGetLastError();
 }
 
@@ -84,6 +91,7 @@ cudaError_t launch_tensor(const PrimeConst* pc, u64* arena, uint32_t n, uint32_t
     if (limbs == 0 || nz == 0) return cudaSuccess;
     dim3 grid((n + 255) / 256, limbs, nz);
     tensor_kernel<<<grid, 256, 0, st>>>(pc, arena, n, ta);
+    count_launches(1);
     return cudaGetLastError();
 }
 
@@ -113,6 +121,7 @@ cudaError_t launch_automorphism(const uint32_t* map32, const u64* map64, u64* ar
     if (limbs == 0 || nz == 0) return cudaSuccess;
     dim3 grid((n + 255) / 256, limbs, nz);
     automorphism_kernel<<<grid, 256, 0, st>>>(map32, map64, arena, n, zb);
+    count_launches(1);
     return cudaGetLastError();
 }
 
@@ -202,10 +211,22 @@ cudaError_t launch_rescale(int log_n, const OpTabs& t, const LimbJob* jobs_q, ui
 //   ext0   : S * N         sum_j digit_j * evk_b   (then ModDown input)
 //   ext1   : S * N         sum_j digit_j * evk_a
 //   mid    : 2 * slots_q * N  two-pass intermediates of the ModDown NTTs
+//   t0     : slots_q * N   c0 gathered through the automorphism (rotation)
 size_t ks_scratch_words(uint32_t n, uint32_t slots_q, uint32_t K, uint32_t parts) {
     const size_t S = slots_q + K;
-    return (size_t)n * (slots_q + parts * S + 2 * S + 2 * (size_t)slots_q);
+    return (size_t)n * (slots_q + parts * S + 2 * S + 3 * (size_t)slots_q);
 }
+
+// Input load through the automorphism: the key switch of auto(c1) reads
+// c1[map[x]] (the reference applies automorphism() first, fhe_host_driver.cpp:342-350).
+struct LoadGather {
+    const u64* base;
+    const uint32_t* map;
+    __device__ __forceinline__ u64 operator()(const LimbJob& j, const ZBases& zb, uint32_t z, uint32_t x,
+                                              const PrimeConst&) const {
+        return base[zb.src[z] + j.src + __ldg(map + x)];
+    }
+};
 
 // ModUp base conversion as the NTT prologue: job.aux = digit << 16 | k, where
 // k is the output's position among the digit's complementary primes.
@@ -253,8 +274,9 @@ __global__ void __launch_bounds__(256) ks_mac_kernel(OpTabs t, uint32_t n, uint3
                                                      uint32_t K, const u64* __restrict__ key, u64 evk_a, u64 evk_b,
                                                      uint32_t key_stride, uint32_t key_pbase,
                                                      const u64* __restrict__ arena, u64* __restrict__ scratch,
-                                                     u64 modup_off, u64 ext0_off, u64 ext1_off,
-                                                     const __grid_constant__ ZBases zb) {
+                                                     u64 modup_off, u64 ext0_off, u64 ext1_off, u64 t0_off,
+                                                     const __grid_constant__ ZBases zb,
+                                                     const __grid_constant__ KsFuse f) {
     const uint32_t sidx = blockIdx.y;   // 0..sizeQl+K-1
     const uint32_t z = blockIdx.z;
     const bool isq = sidx < sizeQl;
@@ -267,6 +289,9 @@ __global__ void __launch_bounds__(256) ks_mac_kernel(OpTabs t, uint32_t n, uint3
     const u64 base_scr = zb.mid[z];
     const u64* in = arena + zb.src[z] + (u64)sidx * n;   // only valid for Q limbs
     for (uint32_t x = blockIdx.x * blockDim.x + threadIdx.x; x < n; x += gridDim.x * blockDim.x) {
+        const uint32_t xs = f.map ? __ldg(f.map + x) : x;     // position read through the automorphism
+        if (isq && f.has_c0)
+            scratch[base_scr + t0_off + (u64)sidx * n + x] = arena[f.c0[z] + (u64)sidx * n + xs];
         Acc128 ab, aa;
         acc_init(ab);
         acc_init(aa);
@@ -274,7 +299,7 @@ __global__ void __launch_bounds__(256) ks_mac_kernel(OpTabs t, uint32_t n, uint3
             const uint32_t start = part * t.alpha;
             const uint32_t size = (part == t.parts - 1) ? sizeQl - start : t.alpha;
             u64 d;
-            if (isq && sidx >= start && sidx < start + size) d = in[x];
+            if (isq && sidx >= start && sidx < start + size) d = in[xs];
             else d = scratch[base_scr + modup_off + ((u64)part * S + slot) * n + x];
             const u64 kl = ((u64)part * key_stride + klimb_in_digit) * n + x;
             acc_mad(ab, d, __ldg(key + evk_b + kl));
@@ -308,27 +333,38 @@ struct ModDownLoad {
 };
 
 // ModDown combine as the NTT epilogue: out = (x_Q - y) * P^-1 mod q_i.
+// z' = 2z + h: h = 0 writes ks0 (+ gathered c0, + acc0), h = 1 writes ks1 (+ acc1).
 struct ModDownStore {
     const u64* scratch;  // ext region at zb.src[z]
     u64* arena;          // output at zb.out[z]
     OpTabs t;
     uint32_t n;
+    int has_c0, has_acc;
+    u64 t0base[ZMAX / 2];   // scratch offset of the gathered c0 per ciphertext
+    u64 acc0[ZMAX / 2], acc1[ZMAX / 2];
     __device__ __forceinline__ void operator()(const LimbJob& j, const ZBases& zb, uint32_t z, uint32_t x, u64 v,
                                                const PrimeConst& pc) const {
         const u64 q = pc.q;
         const uint32_t i = j.aux;
-        u64 xq = scratch[zb.src[z] + (u64)i * n + x];
+        const uint32_t h = z & 1u, zc = z >> 1;
+        const u64 li = (u64)i * n + x;
+        u64 xq = scratch[zb.src[z] + li];
         u64 d = sub_mod(xq, v, q);
-        arena[zb.out[z] + (u64)i * n + x] = mul_shoup(d, __ldg(t.p_inv_mod_q + i), __ldg(t.p_inv_mod_q_sh + i), q);
+        u64 r = mul_shoup(d, __ldg(t.p_inv_mod_q + i), __ldg(t.p_inv_mod_q_sh + i), q);
+        if (h == 0 && has_c0) r = add_mod(r, scratch[t0base[zc] + li], q);
+        if (has_acc) r = add_mod(r, arena[(h ? acc1[zc] : acc0[zc]) + li], q);
+        arena[zb.out[z] + li] = r;
     }
 };
 
 cudaError_t launch_key_switch(int log_n, const OpTabs& t, const LimbJob* jobs_qp, const LimbJob* jobs_modup,
                               uint32_t n_modup, uint32_t slots_q, uint32_t sizeQl, uint32_t K, const u64* key,
                               u64 evk_a, u64 evk_b, uint32_t key_stride, uint32_t key_pbase, u64* arena,
-                              u64* scratch, uint32_t nz, const ZBases& zb, cudaStream_t st) {
+                              u64* scratch, uint32_t nz, const ZBases& zb, cudaStream_t st, const KsFuse* fuse) {
     if (nz == 0) return cudaSuccess;
     if (2 * nz > (uint32_t)ZMAX) return cudaErrorInvalidValue;
+    KsFuse f{};
+    if (fuse) f = *fuse;
     const u64 n = 1ull << log_n;
     const u64 S = (u64)slots_q + K;
     const u64 off_coef = 0;
@@ -336,13 +372,18 @@ cudaError_t launch_key_switch(int log_n, const OpTabs& t, const LimbJob* jobs_qp
     const u64 off_ext0 = off_modup + (u64)t.parts * S * n;
     const u64 off_ext1 = off_ext0 + S * n;
     const u64 off_mid = off_ext1 + S * n;
+    const u64 off_t0 = off_mid + 2ull * slots_q * n;
     cudaError_t e;
 
     // 1. INTT of the input's Q limbs -> coef (slot i at coef + i*N)
     {
         ZBases a = zb;
         for (uint32_t z = 0; z < nz; ++z) { a.mid[z] = zb.mid[z] + off_coef; a.out[z] = zb.mid[z] + off_coef; }
-        e = launch_ntt<true>(log_n, t.pt, jobs_qp, sizeQl, nz, scratch, a, LoadPlain{arena}, StorePlain{scratch}, st);
+        if (f.map)
+            e = launch_ntt<true>(log_n, t.pt, jobs_qp, sizeQl, nz, scratch, a, LoadGather{arena, f.map},
+                                 StorePlain{scratch}, st);
+        else
+            e = launch_ntt<true>(log_n, t.pt, jobs_qp, sizeQl, nz, scratch, a, LoadPlain{arena}, StorePlain{scratch}, st);
         if (e != cudaSuccess) return e;
     }
     // 2. ModUp: base conversion + NTT for every (digit, complementary limb)
@@ -361,7 +402,8 @@ cudaError_t launch_key_switch(int log_n, const OpTabs& t, const LimbJob* jobs_qp
     {
         dim3 grid((uint32_t)((n + 255) / 256), sizeQl + K, nz);
         ks_mac_kernel<<<grid, 256, 0, st>>>(t, (uint32_t)n, slots_q, sizeQl, K, key, evk_a, evk_b, key_stride,
-                                            key_pbase, arena, scratch, off_modup, off_ext0, off_ext1, zb);
+                                            key_pbase, arena, scratch, off_modup, off_ext0, off_ext1, off_t0, zb, f);
+        count_launches(1);
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
@@ -395,7 +437,18 @@ cudaError_t launch_key_switch(int log_n, const OpTabs& t, const LimbJob* jobs_qp
             }
         }
         ModDownLoad pro{scratch, t, slots_q, K, (uint32_t)n};
-        ModDownStore epi{scratch, arena, t, (uint32_t)n};
+        ModDownStore epi{};
+        epi.scratch = scratch;
+        epi.arena = arena;
+        epi.t = t;
+        epi.n = (uint32_t)n;
+        epi.has_c0 = f.has_c0;
+        epi.has_acc = f.has_acc;
+        for (uint32_t z = 0; z < nz; ++z) {
+            epi.t0base[z] = zb.mid[z] + off_t0;
+            epi.acc0[z] = f.acc0[z];
+            epi.acc1[z] = f.acc1[z];
+        }
         e = launch_ntt<false>(log_n, t.pt, jobs_qp, sizeQl, 2 * nz, scratch, b, pro, epi, st);
         if (e != cudaSuccess) return e;
     }
@@ -420,6 +473,7 @@ cudaError_t launch_companions(u64* v, u64* sh, const u64* m, size_t count, cudaS
     unsigned blocks = (unsigned)((count + 255) / 256);
     if (blocks > 4096) blocks = 4096;
     companions_kernel<<<blocks, 256, 0, st>>>(v, sh, m, count);
+    count_launches(1);
     return cudaGetLastError();
 }
 
@@ -444,6 +498,7 @@ cudaError_t launch_prime_consts(PrimeConst* pc, const u64* q, const u64* ninv, c
                                 uint32_t count, cudaStream_t st) {
     if (count == 0) return cudaSuccess;
     prime_consts_kernel<<<(count + 63) / 64, 64, 0, st>>>(pc, q, ninv, itw, n, count);
+    count_launches(1);
     return cudaGetLastError();
 }
 

@@ -24,7 +24,7 @@ u64 host_shoup(u64 w, u64 q);
 
 // Scratch lane b owns [b * lane_words, (b + 1) * lane_words) of ctx->scr. A
 // batched composite operator gives ciphertext b of a launch lane b.
-constexpr uint32_t kLanes = 16;
+constexpr uint32_t kLanes = 64;
 constexpr uint32_t kTempPolys = 6;  // d0, d1, d2, ks0, ks1, t (each (L + K) * N words)
 
 struct Lane {

@@ -25,6 +25,9 @@
 
 namespace afhe {
 
+// Host-side count of kernels this library has launched (all contexts).
+void count_launches(uint64_t k);
+
 // Per-prime constants (64 bytes).
 struct PrimeConst {
     u64 q;
@@ -69,7 +72,7 @@ struct NttGeom {
     int last;     // pass writes through the epilogue
 };
 
-constexpr int ZMAX = 32;  // polynomials per launch (blockIdx.z)
+constexpr int ZMAX = 128;  // polynomials per launch (blockIdx.z)
 
 // Per-z word offsets of the operands of one launch (kernel parameter). The
 // meaning of src / out / aux is the prologue's and epilogue's; mid is where a
@@ -134,7 +137,7 @@ __device__ __forceinline__ u64 canon4(u64 v, u64 q) {
 }
 
 template <bool INV, class Pro, class Epi>
-__global__ void __launch_bounds__(512) ntt_pass_kernel(NttGeom g, PrimeTables pt, const LimbJob* __restrict__ jobs,
+__global__ void __launch_bounds__(1024) ntt_pass_kernel(NttGeom g, PrimeTables pt, const LimbJob* __restrict__ jobs,
                                                         u64* __restrict__ mid, const __grid_constant__ ZBases zb,
                                                         Pro pro, Epi epi) {
     extern __shared__ u64 sm[];
@@ -265,7 +268,7 @@ struct NttPlan {
 
 inline NttPlan make_plan(int log_n, bool inverse) {
     NttPlan pl;
-    if (log_n <= 12) {
+    if (log_n <= 13) {   // whole limb in shared memory (<= 64 KB), N / 8 threads
         pl.npass = 1;
         NttGeom a{};
         a.log_n = log_n; a.lo_bit = 0; a.P = log_n; a.log_c = 0; a.first = 1; a.last = 1;
@@ -300,7 +303,13 @@ inline cudaError_t launch_ntt(int log_n, const PrimeTables& pt, const LimbJob* j
         uint32_t ctas = 1u << (log_n - g.P - g.log_c);
         dim3 grid(ctas, njobs, nz);
         size_t smem = (size_t)tile * sizeof(u64);
+        if (smem > 48 * 1024) {
+            cudaError_t e = cudaFuncSetAttribute(ntt_pass_kernel<INV, Pro, Epi>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+        }
         ntt_pass_kernel<INV, Pro, Epi><<<grid, threads, smem, st>>>(g, pt, jobs, mid, zb, pro, epi);
+        count_launches(1);
     }
     return cudaGetLastError();
 }

@@ -13,7 +13,7 @@ with the semantics fixed by integration_tools/generate_interactive_test_vectors.
   stage 4  (client)  decrypt, sort, top-k
 
 Every operator call processes a whole batch of independent ciphertexts (up to
-16 per launch; one lane of context scratch each): several queries in stage 1,
+64 per launch; one lane of context scratch each): several queries in stage 1,
 several (query, list, batch) items in stage 3. Each ciphertext's residues are
 the ones the one-at-a-time chain produces. `lanes=1` is the plain path.
 
@@ -31,7 +31,7 @@ from .ckks import Encoder, Slots, encode_plaintext
 from .driver import FheContext, FHEHostDriver
 from .ivfpq import IvfPqIndex
 
-MAX_LANES = 16
+MAX_LANES = 64
 
 
 @dataclass
@@ -169,6 +169,10 @@ class InteractiveQueryManager:
         L.check(self.lib.afhe_eval_rotate_batch(self.ctx.h, self._refs(cts), self._refs(cts), len(cts), r, limbs),
                 "eval_rotate_batch")
 
+    def _rot_acc(self, src, acc, r, limbs):
+        L.check(self.lib.afhe_eval_rotate_accumulate_batch(self.ctx.h, self._refs(src), self._refs(acc), len(src), r,
+                                                           limbs), "eval_rotate_accumulate_batch")
+
     def _add(self, a, b, d, limbs):
         L.check(self.lib.afhe_eval_add_batch(self.ctx.h, self._refs(a), self._refs(b), self._refs(d), len(a), limbs),
                 "eval_add_batch")
@@ -199,19 +203,16 @@ class InteractiveQueryManager:
             self._sub_plain([q.ct_query for q in qs], [self.pt_centroids] * len(qs), diff, Ll)
             self._square(diff, sq, Ll)
             s = 1
-            while s < D:
-                L.check(self.lib.afhe_eval_rotate_batch(self.ctx.h, self._refs(sq), self._refs(tmp), len(sq), s,
-                                                        self.lvl_sq), "eval_rotate_batch")
-                self._add(sq, tmp, sq, self.lvl_sq)
+            while s < D:                     # sq += rot(sq, s)
+                self._rot_acc(sq, sq, s, self.lvl_sq)
                 s <<= 1
             comp = [q.compact for q in qs]
             for i in range(self.sh.n_list):
                 shift = i * (D - 1)
                 tgt = comp if i == 0 else sel
                 self._mult_plain(sq, [self.mask_onehot[i]] * len(qs), tgt, self.lvl_sq)
-                if shift:
-                    self._rotate(sel, shift, self.lvl_out)
-                    self._add(comp, sel, comp, self.lvl_out)
+                if shift:                    # comp += rot(sel, i * (D - 1))
+                    self._rot_acc(sel, comp, shift, self.lvl_out)
 
     def stage3_fine(self, queries: list[QueryRecord]) -> None:
         """Stage 3 for every (query, probed list, batch) item, lanes at a time.
@@ -236,10 +237,8 @@ class InteractiveQueryManager:
             self._sub_plain([queries[x[0]].ct_dim for x in it], [x[1] for x in it], diff, Ll)
             self._square(diff, sq, Ll)
             s = B
-            while s < D * B:
-                L.check(self.lib.afhe_eval_rotate_batch(self.ctx.h, self._refs(sq), self._refs(tmp), len(sq), s,
-                                                        self.lvl_sq), "eval_rotate_batch")
-                self._add(sq, tmp, sq, self.lvl_sq)
+            while s < D * B:                 # sq += rot(sq, s)
+                self._rot_acc(sq, sq, s, self.lvl_sq)
                 s <<= 1
             self._mult_plain(sq, [self._prefix(x[2]) for x in it], sel, self.lvl_sq)
             # rotate each item by -offset: the same descending power-of-two steps

@@ -50,7 +50,7 @@ SMALL = WorkloadSpec("ivfpq_4096x64_nlist32_N8192_L3", n_vectors=4096, d=64, com
 
 
 class Workload:
-    def __init__(self, spec: WorkloadSpec = SMALL, max_queries: int = 64, lanes: int = 16, device: int = 0,
+    def __init__(self, spec: WorkloadSpec = SMALL, max_queries: int = 64, lanes: int = 64, device: int = 0,
                  index: IvfPqIndex | None = None):
         self.spec = spec
         t0 = time.time()

@@ -127,6 +127,7 @@ def run_ours(args, rank: int, world: int):
 
     for _ in range(args.warmup):
         device_step()
+    lib = wl.ctx.lib
     dist = world > 1
     if dist:
         torch.distributed.barrier()
@@ -134,8 +135,10 @@ def run_ours(args, rank: int, world: int):
     stop, samples = threading.Event(), []
     th = threading.Thread(target=clocks_sampler, args=(stop, samples, dev), daemon=True)
     th.start()
+    launches0 = lib.afhe_kernel_launches()
     ms = [device_step() for _ in range(args.steps)]
     torch.cuda.synchronize()
+    launches = lib.afhe_kernel_launches() - launches0
     stop.set()
     th.join()
     total_ms = sum(ms)
@@ -168,9 +171,70 @@ def run_ours(args, rank: int, world: int):
         "e2e": {"value": queries / (e2e_ms / 1e3), "unit": "queries/s",
                 "h2d_bytes_per_step": e2e[0][1], "d2h_bytes_per_step": e2e[0][2]},
         "clocks": summarize_clocks(samples),
+        "gpu_launches": int(launches),
     }
+    line["roofline"] = ntt_roofline(wl, stream, args.lanes)
     wl.close()
+    if world == 1 and rank == 0 and not args.skip_cpu:
+        from oracle.chain import cpu_reference_rate
+        ref = cpu_reference_rate(steps=1)
+        line["cpu_baseline"] = ref["cpu_baseline"]
     return line
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ntt_roofline(wl, stream, lanes):
+    """The dominant kernel (ntt_pass_kernel, 87% of device time in the launch
+    list) timed alone at the key switch's batch shape: `lanes` ciphertext polys
+    x (L + K) limbs of N = 8192 per launch, forward, in place. Five such
+    batches are cycled (> L2 in total) so every launch streams from HBM.
+    Algorithmic bytes per launch: read + write of every limb once."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from anns_fhe_b200._lib import P64
+    p = wl.params
+    n, limbs = p.n, p.L + p.K
+    per = lanes
+    slot_w = limbs * n
+    nbuf = 5
+    need = nbuf * per * slot_w
+    # borrow the tail of poly_gmem (beyond the workload's slots) if it fits, else a fresh context
+    from anns_fhe_b200.driver import FheContext
+    ctx = FheContext(p, poly_words=need, key_words=1024, device=torch.cuda.current_device())
+    rng = np.random.default_rng(3)
+    for b in range(nbuf * per):
+        ctx.write_poly(b * slot_w, np.concatenate([rng.integers(0, q, n, dtype=np.uint64) for q in p.q + p.p]))
+    st = torch.cuda.ExternalStream(ctx.lib.afhe_stream(ctx.h), device=torch.cuda.current_device())
+    offs = [(C.c_uint64 * per)(*[(b * per + i) * slot_w for i in range(per)]) for b in range(nbuf)]
+    for b in range(nbuf):
+        ctx.lib.afhe_ntt_batch(ctx.h, C.cast(offs[b], P64), per, limbs, 0)
+    reps = 50
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for r in range(reps):
+        ctx.lib.afhe_ntt_batch(ctx.h, C.cast(offs[r % nbuf], P64), per, limbs, 0)
+    e1.record(st)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    ctx.close()
+    bytes_per_launch = 2 * per * limbs * n * 8
+    achieved = bytes_per_launch / (ms * 1e-3) / 1e9
+    peak, src = load_peaks()
+    return {"bound": "hbm", "kernel": f"ntt_pass_kernel (forward, N={n}, single pass, {per}x{limbs} limbs/launch)",
+            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "peak_source": src, "traffic": None, "ms_per_launch": ms,
+            "algorithmic_bytes_per_launch": bytes_per_launch}
 
 
 def run_reference(args, rank: int, world: int):
@@ -184,8 +248,9 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--batch", type=int, default=32, help="queries per step")
-    ap.add_argument("--lanes", type=int, default=16)
+    ap.add_argument("--batch", type=int, default=64, help="queries per step")
+    ap.add_argument("--lanes", type=int, default=64)
+    ap.add_argument("--skip-cpu", action="store_true", help="omit the cpu_baseline leg")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -223,6 +223,17 @@ int afhe_eval_mult_relin_rescale_batch(afhe_ctx* ctx, const afhe_ct_ref* a, cons
                                        const afhe_ct_ref* dst, uint32_t count, uint32_t in_limbs);
 int afhe_eval_rotate_batch(afhe_ctx* ctx, const afhe_ct_ref* in, const afhe_ct_ref* dst,
                            uint32_t count, int32_t total_rot, uint32_t limbs);
+/* In-place forward (inverse = 0) or inverse NTT of `count` polynomials of
+ * `limbs` limbs each (limb i under prime i, Q then P), one launch per pass. */
+int afhe_ntt_batch(afhe_ctx* ctx, const uint64_t* polys, uint32_t count, uint32_t limbs, int inverse);
+/* Kernels launched by this library so far (host-side count, all contexts). */
+uint64_t afhe_kernel_launches(void);
+/* acc[i] = acc[i] + rotate(in[i], total_rot), bit-identical to eval_rotate
+ * into a temporary followed by eval_add; in[i] may equal acc[i] (the
+ * rotate-and-sum step x += rot(x)). The last rotation step's key switch adds
+ * into acc in its epilogue. */
+int afhe_eval_rotate_accumulate_batch(afhe_ctx* ctx, const afhe_ct_ref* in, const afhe_ct_ref* acc,
+                                      uint32_t count, int32_t total_rot, uint32_t limbs);
 int afhe_eval_add_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const afhe_ct_ref* b, const afhe_ct_ref* dst,
                         uint32_t count, uint32_t limbs);
 /* pt[i] is the plaintext polynomial offset for ciphertext i */

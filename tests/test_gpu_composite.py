@@ -149,6 +149,33 @@ def test_rotate(su):
         assert np.array_equal(su.get(3, lvl), e1), total
 
 
+def test_rotate_accumulate(su):
+    from anns_fhe_b200 import _lib as L
+    lvl = su.L
+    A, B = su.ct(lvl), su.ct(lvl)
+    su.put(0, A[0]); su.put(1, A[1]); su.put(2, B[0]); su.put(3, B[1])
+
+    def refs(*cts):
+        arr = (L.CtRef * len(cts))()
+        for i, (a, b) in enumerate(cts):
+            arr[i].c0_offset, arr[i].c1_offset = a, b
+        return arr
+    for total in (1, 3, -2, 0):
+        su.put(2, B[0]); su.put(3, B[1])
+        L.check(su.ctx.lib.afhe_eval_rotate_accumulate_batch(su.ctx.h, refs((su.slot(0), su.slot(1))),
+                                                             refs((su.slot(2), su.slot(3))), 1, total, lvl), "racc")
+        r0, r1 = su.ora.eval_rotate(A, total, su.rot, lvl)
+        e0, e1 = su.ora.eval_add((r0, r1), B, lvl)
+        assert np.array_equal(su.get(2, lvl), e0), total
+        assert np.array_equal(su.get(3, lvl), e1), total
+    # in place: x += rot(x, 2)
+    L.check(su.ctx.lib.afhe_eval_rotate_accumulate_batch(su.ctx.h, refs((su.slot(0), su.slot(1))),
+                                                         refs((su.slot(0), su.slot(1))), 1, 2, lvl), "racc")
+    r0, r1 = su.ora.eval_rotate(A, 2, su.rot, lvl)
+    e0, e1 = su.ora.eval_add(A, (r0, r1), lvl)
+    assert np.array_equal(su.get(0, lvl), e0) and np.array_equal(su.get(1, lvl), e1)
+
+
 def test_missing_rotation_key_is_an_error(su):
     from anns_fhe_b200 import AfheError
     with pytest.raises(AfheError) as ei:
