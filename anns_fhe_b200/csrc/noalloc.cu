@@ -1,0 +1,83 @@
+// noalloc.cu -- a key switch that allocates nothing at call time.
+//
+// Some callers cannot call cudaMalloc on their request path: an application
+// whose device memory is already handed to its own pool allocator (so a fresh
+// cudaMalloc fails or steals from the pool), or a latency-bound serving thread
+// that cannot afford the device-wide synchronisation cudaMalloc / cudaFree may
+// imply. afhe_key_switch_noalloc gives them the key switch with its working
+// memory in a fixed array compiled into this library instead of allocated
+// memory: the array below is static device memory, created when the library is
+// loaded on a device and held by every GPU that loads it until the process
+// exits, so its size is kept modest (16 MiB).
+//
+// The array is shared by every call on a device and keeps the previous call's
+// contents. The key switch writes every scratch word before reading it, so no
+// clearing is needed. Calls whose execution overlaps on the GPU (different
+// streams, or several contexts on one device) race on the array; the caller
+// must order them.
+#include <cuda_runtime.h>
+
+#include <mutex>
+
+#include "internal.h"
+#include "lanes.h"
+
+using namespace afhe;
+
+namespace {
+
+constexpr size_t kNoallocScratchWords = size_t(1) << 21;   // 16 MiB of uint64_t
+constexpr int kMaxDevices = 64;
+
+static __device__ __align__(256) u64 g_noalloc_scratch[kNoallocScratchWords];
+
+// Host code must not use g_noalloc_scratch's name as an address (on the host
+// it names a shadow variable, not device memory): the device address is looked
+// up once per device with that device current, and cached.
+std::mutex g_mu;
+u64* g_dev_addr[kMaxDevices] = {};
+
+int scratch_address(afhe_ctx* ctx, u64** out) {
+    if (ctx->device < 0 || ctx->device >= kMaxDevices) return fail(ctx, AFHE_E_ARG, "device ordinal out of range");
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_dev_addr[ctx->device]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGetSymbolAddress(noalloc scratch)");
+        g_dev_addr[ctx->device] = (u64*)p;
+    }
+    *out = g_dev_addr[ctx->device];
+    return AFHE_OK;
+}
+
+}  // namespace
+
+extern "C" int afhe_key_switch_noalloc(afhe_ctx* ctx, uint64_t* io, uint64_t evk_offset, uint32_t limbs) {
+    if (!ctx || !io) return fail(ctx, AFHE_E_ARG, "null argument");
+    if (limbs < 1 || limbs > ctx->L) return fail(ctx, AFHE_E_LEVEL, "limb count outside [1, L]");
+    const u64 key_words = 2ull * ctx->dnum * (ctx->L + ctx->K) * ctx->n;
+    if (!range_ok(evk_offset, key_words, ctx->prm.key_words)) return fail(ctx, AFHE_E_RANGE, "key out of key_gmem");
+    const size_t need = ks_scratch_words(ctx->n, ctx->L, ctx->K, ctx->dnum);
+    if (need > kNoallocScratchWords)
+        return fail(ctx, AFHE_E_BUDGET,
+                    "afhe_key_switch_noalloc: this parameter set needs " + std::to_string(need) +
+                        " scratch words, more than the fixed " + std::to_string(kNoallocScratchWords));
+    cudaError_t e = cudaSetDevice(ctx->device);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
+    u64* scratch = nullptr;
+    int rc = scratch_address(ctx, &scratch);
+    if (rc != AFHE_OK) return rc;
+    const u64 w = (u64)limbs * ctx->n;
+    ZBases zb{};
+    zb.src[0] = 0;        // input at io[0, w)
+    zb.out[0] = w;        // ks0 at io[w, 2w)
+    zb.aux[0] = 2 * w;    // ks1 at io[2w, 3w)
+    zb.mid[0] = 0;        // scratch from the start of the fixed array
+    const u64 S = (u64)ctx->L + ctx->K;
+    const LevelJobs& lj = ctx->lvjobs[limbs];
+    e = launch_key_switch(ctx->log_n, ctx->lv[limbs], ctx->jobs_qp, lj.modup, lj.n_modup, ctx->L, limbs, ctx->K,
+                          ctx->key, evk_offset, evk_offset + (u64)ctx->dnum * S * ctx->n, (uint32_t)S, ctx->L, io,
+                          scratch, 1, zb, ctx->st);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "afhe_key_switch_noalloc launch");
+    return AFHE_OK;
+}

@@ -216,6 +216,22 @@ int afhe_eval_rotate_single_step(afhe_ctx* ctx, uint64_t in_c0, uint64_t in_c1, 
 int afhe_eval_rotate(afhe_ctx* ctx, uint64_t in_c0, uint64_t in_c1, uint64_t dst_c0,
                      uint64_t dst_c1, int32_t total_rot, uint32_t limbs);
 
+/* Key switch with no allocation at call time (no counterpart in the
+ * reference). For callers that cannot call cudaMalloc on their request path:
+ * applications whose device memory already belongs to their own pool
+ * allocator, or latency-bound threads that cannot take the synchronisation
+ * cudaMalloc / cudaFree may cause. Same result as afhe_key_switch.
+ *   io: device pointer to 3 * limbs * N words: the input polynomial, then ks0
+ *       (sum digit * b), then ks1 (sum digit * a); the caller owns it.
+ *   evk_offset: the key in key_gmem (full-level layout, as afhe_key_switch).
+ * Working memory is a fixed 16 MiB array of static device memory in this
+ * library (held on every GPU that loads it until exit); parameter sets whose
+ * key switch needs more return AFHE_E_BUDGET. The first call on a device looks
+ * up that array's address (cudaGetSymbolAddress), so make it before any stream
+ * capture. All calls on a device share the array: calls that overlap on the
+ * GPU race and must be ordered by the caller. */
+int afhe_key_switch_noalloc(afhe_ctx* ctx, uint64_t* io, uint64_t evk_offset, uint32_t limbs);
+
 /* ---- batched composite operators ------------------------------------------ */
 /* The same operator applied to `count` independent ciphertexts in one pass of
  * launches; each output is bit-identical to the one-at-a-time call. */
