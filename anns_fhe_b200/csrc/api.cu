@@ -146,30 +146,27 @@ int build_native_tables(afhe_ctx* ctx) {
     for (uint32_t i = 0; i < L; ++i) primes[i] = ctx->prm.q[i];
     for (uint32_t k = 0; k < K; ++k) primes[L + k] = ctx->prm.p[k];
 
-    std::vector<u64> tw((size_t)np * n), tws((size_t)np * n), itw((size_t)np * n), itws((size_t)np * n);
+    std::vector<u64> tw(n), itw(n);
+    std::vector<ulonglong2> tw2((size_t)np * n), itw2((size_t)np * n);
     std::vector<PrimeConst> pc(np);
     for (uint32_t i = 0; i < np; ++i) {
         u64 q = primes[i];
         u64 psi = min_primitive_root(ctx->log_n, q);
-        gen_twiddles(ctx->log_n, q, psi, &tw[(size_t)i * n], &itw[(size_t)i * n]);
+        gen_twiddles(ctx->log_n, q, psi, tw.data(), itw.data());
         for (uint32_t j = 0; j < n; ++j) {
-            tws[(size_t)i * n + j] = host_shoup(tw[(size_t)i * n + j], q);
-            itws[(size_t)i * n + j] = host_shoup(itw[(size_t)i * n + j], q);
+            tw2[(size_t)i * n + j] = make_ulonglong2(tw[j], host_shoup(tw[j], q));
+            itw2[(size_t)i * n + j] = make_ulonglong2(itw[j], host_shoup(itw[j], q));
         }
-        pc[i] = host_prime_const(q, inv_mod(n % q, q), itw[(size_t)i * n + 1]);
+        pc[i] = host_prime_const(q, inv_mod(n % q, q), itw[1]);
     }
     DevPrimeSet& s = ctx->nat;
     s.count = np;
     CK(dalloc(&s.pc, np));
-    CK(dalloc(&s.tw, (size_t)np * n));
-    CK(dalloc(&s.tw_sh, (size_t)np * n));
-    CK(dalloc(&s.itw, (size_t)np * n));
-    CK(dalloc(&s.itw_sh, (size_t)np * n));
+    CK(dalloc(&s.tw2, (size_t)np * n));
+    CK(dalloc(&s.itw2, (size_t)np * n));
     CK(cudaMemcpy(s.pc, pc.data(), np * sizeof(PrimeConst), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(s.tw, tw.data(), tw.size() * 8, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(s.tw_sh, tws.data(), tws.size() * 8, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(s.itw, itw.data(), itw.size() * 8, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(s.itw_sh, itws.data(), itws.size() * 8, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(s.tw2, tw2.data(), tw2.size() * sizeof(ulonglong2), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(s.itw2, itw2.data(), itw2.size() * sizeof(ulonglong2), cudaMemcpyHostToDevice));
 
     // per-level CRT tables, each followed by its Shoup companions
     std::vector<u64> buf;
@@ -367,7 +364,7 @@ int afhe_ctx_destroy(afhe_ctx* ctx) {
     auto fr = [](void* p) { if (p) cudaFree(p); };
     fr(ctx->poly); fr(ctx->key); fr(ctx->lvbuf); fr(ctx->jobs_qp);
     for (auto& j : ctx->lvjobs) fr(j.modup);
-    for (DevPrimeSet* s : {&ctx->nat, &ctx->ld}) { fr(s->pc); fr(s->tw); fr(s->tw_sh); fr(s->itw); fr(s->itw_sh); }
+    for (DevPrimeSet* s : {&ctx->nat, &ctx->ld}) { fr(s->pc); fr(s->tw); fr(s->itw); fr(s->tw2); fr(s->itw2); }
     fr(ctx->ld_crt); fr(ctx->ld_crt_sh); fr(ctx->ld_mod); fr(ctx->ld_jobs);
     for (auto& kv : ctx->rot) fr(kv.second.map);
     if (ctx->st) cudaStreamDestroy(ctx->st);
@@ -513,13 +510,13 @@ int load_context(afhe_ctx* ctx, const afhe_accel_args* a) {
     // twiddles: (L + K) rows, Q then P
     DevPrimeSet& s = ctx->ld;
     if (s.count < L + K) {
-        for (void* pp : {(void*)s.pc, (void*)s.tw, (void*)s.tw_sh, (void*)s.itw, (void*)s.itw_sh}) if (pp) cudaFree(pp);
+        for (void* pp : {(void*)s.pc, (void*)s.tw, (void*)s.itw, (void*)s.tw2, (void*)s.itw2}) if (pp) cudaFree(pp);
         s = DevPrimeSet{};
         CK(dalloc(&s.pc, AFHE_MAX_Q + AFHE_MAX_P));
         CK(dalloc(&s.tw, (size_t)(AFHE_MAX_Q + AFHE_MAX_P) * n));
-        CK(dalloc(&s.tw_sh, (size_t)(AFHE_MAX_Q + AFHE_MAX_P) * n));
         CK(dalloc(&s.itw, (size_t)(AFHE_MAX_Q + AFHE_MAX_P) * n));
-        CK(dalloc(&s.itw_sh, (size_t)(AFHE_MAX_Q + AFHE_MAX_P) * n));
+        CK(dalloc(&s.tw2, (size_t)(AFHE_MAX_Q + AFHE_MAX_P) * n));
+        CK(dalloc(&s.itw2, (size_t)(AFHE_MAX_Q + AFHE_MAX_P) * n));
         s.count = AFHE_MAX_Q + AFHE_MAX_P;
     }
     cudaStream_t st = ctx->st;
@@ -527,26 +524,22 @@ int load_context(afhe_ctx* ctx, const afhe_accel_args* a) {
     CK(cudaMemcpyAsync(s.tw + (size_t)L * n, ctx->key + a->twiddles_p_offset, (size_t)K * n * 8, cudaMemcpyDeviceToDevice, st));
     CK(cudaMemcpyAsync(s.itw, ctx->key + a->inv_twiddles_q_offset, (size_t)L * n * 8, cudaMemcpyDeviceToDevice, st));
     CK(cudaMemcpyAsync(s.itw + (size_t)L * n, ctx->key + a->inv_twiddles_p_offset, (size_t)K * n * 8, cudaMemcpyDeviceToDevice, st));
-    std::vector<u64> mods((size_t)(L + K) * n), qv(L + K), ninv(L + K);
+    std::vector<u64> qv(L + K), ninv(L + K);
     for (uint32_t i = 0; i < L + K; ++i) {
         qv[i] = i < L ? a->rns_primes[i] : a->p_primes[i - L];
         ninv[i] = i < L ? a->n_inv_q[i] : a->n_inv_p[i - L];
-        std::fill(mods.begin() + (size_t)i * n, mods.begin() + (size_t)(i + 1) * n, qv[i]);
     }
-    u64* dmods = nullptr;
     u64* dq = nullptr;
     u64* dn = nullptr;
-    CK(dalloc(&dmods, mods.size()));
     CK(dalloc(&dq, L + K));
     CK(dalloc(&dn, L + K));
-    CK(cudaMemcpyAsync(dmods, mods.data(), mods.size() * 8, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(dq, qv.data(), qv.size() * 8, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(dn, ninv.data(), ninv.size() * 8, cudaMemcpyHostToDevice, st));
-    CK(launch_companions(s.tw, s.tw_sh, dmods, mods.size(), st));
-    CK(launch_companions(s.itw, s.itw_sh, dmods, mods.size(), st));
+    CK(launch_interleave(s.tw, dq, s.tw2, L + K, n, st));
+    CK(launch_interleave(s.itw, dq, s.itw2, L + K, n, st));
     CK(launch_prime_consts(s.pc, dq, dn, s.itw, n, L + K, st));
     CK(cudaStreamSynchronize(st));
-    cudaFree(dmods); cudaFree(dq); cudaFree(dn);
+    cudaFree(dq); cudaFree(dn);
 
     // CRT tables, raw
     std::vector<std::pair<u64, u64>> regions;  // (key offset, words) in load order

@@ -37,15 +37,17 @@ struct OpTabs {
     const u64* qlinv_sh;
 };
 
-// Owned device storage for one twiddle table set.
+// Owned device storage for one twiddle table set. tw / itw hold raw tables
+// (only for tables loaded by OP_LOAD_CONTEXT); tw2 / itw2 the (w, companion)
+// pairs the kernels read.
 struct DevPrimeSet {
     PrimeConst* pc = nullptr;
     u64* tw = nullptr;
-    u64* tw_sh = nullptr;
     u64* itw = nullptr;
-    u64* itw_sh = nullptr;
+    ulonglong2* tw2 = nullptr;
+    ulonglong2* itw2 = nullptr;
     uint32_t count = 0;
-    PrimeTables view() const { return PrimeTables{pc, tw, tw_sh, itw, itw_sh}; }
+    PrimeTables view() const { return PrimeTables{pc, tw2, itw2}; }
 };
 
 struct RotKey {
@@ -165,6 +167,9 @@ cudaError_t launch_key_switch(int log_n, const OpTabs& t, const LimbJob* jobs_qp
                               u64* arena, u64* scratch, uint32_t nz, const ZBases& zb, cudaStream_t st,
                               const KsFuse* fuse = nullptr);
 
+// Twiddle pairs: out2[r * n + j] = (w, companion of w), w = raw[r * n + j] mod q[r].
+cudaError_t launch_interleave(const u64* raw, const u64* q, ulonglong2* out2, uint32_t rows, uint32_t n,
+                              cudaStream_t st);
 // Companion prep: sh[e] = shoup_companion(v[e] mod m[e], m[e]); v reduced in place.
 cudaError_t launch_companions(u64* v, u64* sh, const u64* m, size_t count, cudaStream_t st);
 // Loaded prime constants: fills pc[i] from q/ninv arrays (device) and itw.

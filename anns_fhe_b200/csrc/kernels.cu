@@ -477,6 +477,26 @@ cudaError_t launch_companions(u64* v, u64* sh, const u64* m, size_t count, cudaS
     return cudaGetLastError();
 }
 
+__global__ void interleave_kernel(const u64* raw, const u64* q, ulonglong2* out2, uint32_t rows, uint32_t n) {
+    const size_t total = (size_t)rows * n;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < total; i += (size_t)gridDim.x * blockDim.x) {
+        const u64 m = q[i / n];
+        const u64 w = raw[i] % m;
+        out2[i] = make_ulonglong2(w, shoup_companion(w, m));
+    }
+}
+
+cudaError_t launch_interleave(const u64* raw, const u64* q, ulonglong2* out2, uint32_t rows, uint32_t n,
+                              cudaStream_t st) {
+    if (rows == 0) return cudaSuccess;
+    size_t total = (size_t)rows * n;
+    unsigned blocks = (unsigned)((total + 255) / 256);
+    if (blocks > 8192) blocks = 8192;
+    interleave_kernel<<<blocks, 256, 0, st>>>(raw, q, out2, rows, n);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
 __global__ void prime_consts_kernel(PrimeConst* pc, const u64* q, const u64* ninv, const u64* itw, uint32_t n,
                                     uint32_t count) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;

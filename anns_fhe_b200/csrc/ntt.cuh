@@ -36,13 +36,12 @@ struct PrimeConst {
     u64 r64, r64_sh, one_sh;  // reduce128 constants
 };
 
-// One table set: primes [0, count) with twiddles for each.
+// One table set: primes [0, count) with twiddles for each. Twiddles are
+// stored as (w, Shoup companion of w) pairs, one 16-byte load per twiddle.
 struct PrimeTables {
-    const PrimeConst* pc;   // [count]
-    const u64* tw;          // [count][N]
-    const u64* tw_sh;
-    const u64* itw;
-    const u64* itw_sh;
+    const PrimeConst* pc;    // [count]
+    const ulonglong2* tw2;   // [count][N] forward  (psi^bitrev(j), companion)
+    const ulonglong2* itw2;  // [count][N] inverse
 };
 
 AFHE_HD ModConst modconst_of(const PrimeConst& p) {
@@ -100,26 +99,20 @@ struct StorePlain {
     }
 };
 
-__device__ __forceinline__ uint32_t ins_bits(uint32_t rest, int rb, int k, uint32_t j) {
-    uint32_t lo = rest & ((1u << rb) - 1u);
-    uint32_t hi = rest >> rb;
-    return (hi << (rb + k)) | (j << rb) | lo;
-}
-
 // Forward (CT) butterfly, lazy [0, 4q).
-__device__ __forceinline__ void ct_bfly(u64& x, u64& y, u64 w, u64 wsh, u64 q, u64 q2) {
+__device__ __forceinline__ void ct_bfly(u64& x, u64& y, ulonglong2 w, u64 q, u64 q2) {
     u64 a = x >= q2 ? x - q2 : x;
-    u64 t = mul_shoup_lazy(y, w, wsh, q);
+    u64 t = mul_shoup_lazy(y, w.x, w.y, q);
     x = a + t;
     y = a - t + q2;
 }
 
 // Inverse (GS) butterfly, lazy [0, 2q).
-__device__ __forceinline__ void gs_bfly(u64& x, u64& y, u64 w, u64 wsh, u64 q, u64 q2) {
+__device__ __forceinline__ void gs_bfly(u64& x, u64& y, ulonglong2 w, u64 q, u64 q2) {
     u64 u = x + y;
     u64 v = x - y + q2;
     x = u >= q2 ? u - q2 : u;
-    y = mul_shoup_lazy(v, w, wsh, q);
+    y = mul_shoup_lazy(v, w.x, w.y, q);
 }
 
 // Last inverse stage with N^-1 folded in; outputs canonical.
@@ -136,123 +129,134 @@ __device__ __forceinline__ u64 canon4(u64 v, u64 q) {
     return v >= q ? v - q : v;
 }
 
-template <bool INV, class Pro, class Epi>
-__global__ void __launch_bounds__(1024) ntt_pass_kernel(NttGeom g, PrimeTables pt, const LimbJob* __restrict__ jobs,
-                                                        u64* __restrict__ mid, const __grid_constant__ ZBases zb,
-                                                        Pro pro, Epi epi) {
-    extern __shared__ u64 sm[];
-    const LimbJob job = jobs[blockIdx.y];
-    const uint32_t z = blockIdx.z;
-    const u64 zm = zb.mid[z];
-    const PrimeConst pc = pt.pc[job.prime];
+// Shared-memory layout: one pad word per 16 words, so the strided patterns of
+// every round (8-byte elements, strides 1, 2, 8, 16, 64, ...) hit distinct banks.
+__device__ __forceinline__ uint32_t padix(uint32_t e) { return e + (e >> 4); }
+
+// One round: K consecutive stages on bits [RB, RB + K) of the pass index,
+// 8 / 2^K groups of 2^K values per thread, all shapes compile-time.
+template <bool INV, int P, int LOGC, bool COL, int RB, int K>
+__device__ __forceinline__ void ntt_round(u64* sm, const ulonglong2* __restrict__ tw, const PrimeConst& pc,
+                                          uint32_t tile0, int log_n, int lo_bit, bool last_pass) {
+    constexpr uint32_t C = 1u << LOGC;
+    constexpr uint32_t T = (1u << (P + LOGC)) / 8;
+    constexpr uint32_t NK = 1u << K;
+    constexpr uint32_t GROUPS = 8u >> K;
     const u64 q = pc.q, q2 = q << 1;
-    const uint32_t n = 1u << g.log_n;
-    const u64* __restrict__ tw = (INV ? pt.itw : pt.tw) + (u64)job.prime * n;
-    const u64* __restrict__ twsh = (INV ? pt.itw_sh : pt.tw_sh) + (u64)job.prime * n;
-
-    const int P = g.P, logc = g.log_c;
-    const uint32_t C = 1u << logc;
-    const uint32_t tile = 1u << (P + logc);
-    const uint32_t T = blockDim.x;
-    const bool chunk = (g.lo_bit == 0);
-    const uint32_t tile0 = blockIdx.x << logc;   // first chunk (chunk mode) or column (column mode)
-
-    // local index e -> global coefficient index
-    auto gidx = [&](uint32_t e) -> uint32_t {
-        if (chunk) return (tile0 << P) + e;
-        uint32_t b = e >> logc, c = e & (C - 1u);
-        return (b << g.lo_bit) + tile0 + c;
-    };
-
-    // ---- load tile ----
-    for (uint32_t e = threadIdx.x; e < tile; e += T) {
-        uint32_t x = gidx(e);
-        u64 v;
-        if (g.first) v = pro(job, zb, z, x, pc);
-        else v = mid[zm + job.dst + x];
-        sm[e] = v;
-    }
-    __syncthreads();
-
-    // ---- rounds of up to 3 stages ----
-    const int nrounds = (P + 2) / 3;
-    for (int rd = 0; rd < nrounds; ++rd) {
-        int rb, k;
-        if (!INV) {  // forward: high bits first
-            int hi = P - 3 * rd;
-            k = hi >= 3 ? 3 : hi;
-            rb = hi - k;
-        } else {     // inverse: low bits first
-            rb = 3 * rd;
-            k = (P - rb) >= 3 ? 3 : (P - rb);
-        }
-        const uint32_t groups = 8u >> k;
-        const uint32_t nk = 1u << k;
-        for (uint32_t gi = 0; gi < groups; ++gi) {
-            uint32_t r = threadIdx.x + gi * T;
-            uint32_t c, brest;
-            if (chunk) { brest = r & ((1u << (P - k)) - 1u); c = r >> (P - k); }
-            else { c = r & (C - 1u); brest = r >> logc; }
-            uint32_t hb = chunk ? (tile0 + c) : 0u;   // index bits above the pass
-            u64 v[8];
-            uint32_t bj[8];
 #pragma unroll
-            for (uint32_t j = 0; j < 8; ++j) {
-                if (j < nk) {
-                    bj[j] = ins_bits(brest, rb, k, j);
-                    uint32_t e = chunk ? ((c << P) | bj[j]) : ((bj[j] << logc) | c);
-                    v[j] = sm[e];
-                }
-            }
-            if (!INV) {
+    for (uint32_t gi = 0; gi < GROUPS; ++gi) {
+        const uint32_t r = threadIdx.x + gi * T;
+        uint32_t c, brest;
+        if (COL) { c = r & (C - 1u); brest = r >> LOGC; }
+        else { brest = r & ((1u << (P - K)) - 1u); c = r >> (P - K); }
+        const uint32_t base_b = ((brest >> RB) << (RB + K)) | (brest & ((1u << RB) - 1u));
+        const uint32_t base_e = COL ? ((base_b << LOGC) | c) : ((c << P) | base_b);
+        constexpr uint32_t STEP_E = COL ? (1u << (RB + LOGC)) : (1u << RB);
+        const uint32_t hb = COL ? 0u : (tile0 + c);   // index bits above the pass
+        u64 v[NK];
 #pragma unroll
-                for (int s = 2; s >= 0; --s) {
-                    if (s >= k) continue;
-                    const int pb = rb + s;             // bit within pass
-                    const int p = g.lo_bit + pb;       // global bit
+        for (uint32_t j = 0; j < NK; ++j) v[j] = sm[padix(base_e + j * STEP_E)];
+        if (!INV) {
 #pragma unroll
-                    for (uint32_t j = 0; j < 8; ++j) {
-                        if (j >= nk || (j >> s) & 1u) continue;
-                        uint32_t idx = (1u << (g.log_n - 1 - p)) + ((hb << (P - pb - 1)) | (bj[j] >> (pb + 1)));
-                        ct_bfly(v[j], v[j | (1u << s)], __ldg(tw + idx), __ldg(twsh + idx), q, q2);
+            for (int s = K - 1; s >= 0; --s) {
+                const int pb = RB + s;
+                const int p = lo_bit + pb;
+                const uint32_t tb = (1u << (log_n - 1 - p)) + (hb << (P - pb - 1)) + (base_b >> (pb + 1));
+#pragma unroll
+                for (uint32_t m = 0; m < (NK >> (s + 1)); ++m) {
+                    const ulonglong2 w = __ldg(tw + tb + m);
+#pragma unroll
+                    for (uint32_t jj = 0; jj < (1u << s); ++jj) {
+                        const uint32_t j = (m << (s + 1)) | jj;
+                        ct_bfly(v[j], v[j + (1u << s)], w, q, q2);
                     }
                 }
-            } else {
+            }
+        } else {
 #pragma unroll
-                for (int s = 0; s < 3; ++s) {
-                    if (s >= k) continue;
-                    const int pb = rb + s;
-                    const int p = g.lo_bit + pb;
-                    const bool fuse_last = g.last && (p == g.log_n - 1);
+            for (int s = 0; s < K; ++s) {
+                const int pb = RB + s;
+                const int p = lo_bit + pb;
+                if (last_pass && p == log_n - 1) {
 #pragma unroll
-                    for (uint32_t j = 0; j < 8; ++j) {
-                        if (j >= nk || (j >> s) & 1u) continue;
-                        if (fuse_last) {
-                            gs_bfly_last(v[j], v[j | (1u << s)], pc, q2);
-                        } else {
-                            uint32_t idx = (1u << (g.log_n - 1 - p)) + ((hb << (P - pb - 1)) | (bj[j] >> (pb + 1)));
-                            gs_bfly(v[j], v[j | (1u << s)], __ldg(tw + idx), __ldg(twsh + idx), q, q2);
+                    for (uint32_t j = 0; j < (NK >> 1); ++j) gs_bfly_last(v[j], v[j + (NK >> 1)], pc, q2);
+                } else {
+                    const uint32_t tb = (1u << (log_n - 1 - p)) + (hb << (P - pb - 1)) + (base_b >> (pb + 1));
+#pragma unroll
+                    for (uint32_t m = 0; m < (NK >> (s + 1)); ++m) {
+                        const ulonglong2 w = __ldg(tw + tb + m);
+#pragma unroll
+                        for (uint32_t jj = 0; jj < (1u << s); ++jj) {
+                            const uint32_t j = (m << (s + 1)) | jj;
+                            gs_bfly(v[j], v[j + (1u << s)], w, q, q2);
                         }
                     }
                 }
             }
-#pragma unroll
-            for (uint32_t j = 0; j < 8; ++j) {
-                if (j < nk) {
-                    uint32_t e = chunk ? ((c << P) | bj[j]) : ((bj[j] << logc) | c);
-                    sm[e] = v[j];
-                }
-            }
         }
-        __syncthreads();
+#pragma unroll
+        for (uint32_t j = 0; j < NK; ++j) sm[padix(base_e + j * STEP_E)] = v[j];
     }
+}
 
-    // ---- store tile ----
-    for (uint32_t e = threadIdx.x; e < tile; e += T) {
-        uint32_t x = gidx(e);
-        u64 v = sm[e];
+// All rounds of a pass: forward takes bits high to low, inverse low to high,
+// in rounds of three (the remainder round is smaller).
+template <bool INV, int P, int LOGC, bool COL, int RD>
+__device__ __forceinline__ void ntt_rounds(u64* sm, const ulonglong2* tw, const PrimeConst& pc, uint32_t tile0,
+                                           int log_n, int lo_bit, bool last_pass) {
+    constexpr int NR = (P + 2) / 3;
+    if constexpr (RD < NR) {
+        constexpr int HI = P - 3 * RD;                       // forward: bits [.., HI)
+        constexpr int KF = HI >= 3 ? 3 : HI;
+        constexpr int RBF = HI - KF;
+        constexpr int RBI = 3 * RD;                          // inverse: bits [RBI, ..)
+        constexpr int KI = (P - RBI) >= 3 ? 3 : (P - RBI);
+        constexpr int RB = INV ? RBI : RBF;
+        constexpr int K = INV ? KI : KF;
+        ntt_round<INV, P, LOGC, COL, RB, K>(sm, tw, pc, tile0, log_n, lo_bit, last_pass);
+        __syncthreads();
+        ntt_rounds<INV, P, LOGC, COL, RD + 1>(sm, tw, pc, tile0, log_n, lo_bit, last_pass);
+    }
+}
+
+// One pass over 2^(P + LOGC)-word tiles: stage the tile in shared memory
+// (through the prologue on the first pass), run the rounds, write it back
+// (through the epilogue on the last pass, canonical residues).
+template <bool INV, int P, int LOGC, bool COL, class Pro, class Epi>
+__global__ void __launch_bounds__((1u << (P + LOGC)) / 8)
+ntt_kernel(NttGeom g, PrimeTables pt, const LimbJob* __restrict__ jobs, u64* __restrict__ mid,
+           const __grid_constant__ ZBases zb, Pro pro, Epi epi) {
+    extern __shared__ u64 sm[];
+    constexpr uint32_t C = 1u << LOGC;
+    constexpr uint32_t TILE = 1u << (P + LOGC);
+    constexpr uint32_t T = TILE / 8;
+    const LimbJob job = jobs[blockIdx.y];
+    const uint32_t z = blockIdx.z;
+    const u64 zm = zb.mid[z];
+    const PrimeConst pc = pt.pc[job.prime];
+    const uint32_t n = 1u << g.log_n;
+    const ulonglong2* __restrict__ tw = (INV ? pt.itw2 : pt.tw2) + (u64)job.prime * n;
+    const uint32_t tile0 = blockIdx.x << LOGC;
+
+    auto gidx = [&](uint32_t e) -> uint32_t {
+        if (!COL) return (tile0 << P) + e;
+        const uint32_t b = e >> LOGC, c = e & (C - 1u);
+        return (b << g.lo_bit) + tile0 + c;
+    };
+
+#pragma unroll 4
+    for (uint32_t e = threadIdx.x; e < TILE; e += T) {
+        const uint32_t x = gidx(e);
+        sm[padix(e)] = g.first ? pro(job, zb, z, x, pc) : mid[zm + job.dst + x];
+    }
+    __syncthreads();
+    ntt_rounds<INV, P, LOGC, COL, 0>(sm, tw, pc, tile0, g.log_n, g.lo_bit, g.last != 0);
+#pragma unroll 4
+    for (uint32_t e = threadIdx.x; e < TILE; e += T) {
+        const uint32_t x = gidx(e);
+        u64 v = sm[padix(e)];
         if (g.last) {
-            if (!INV) v = canon4(v, q);
+            if (!INV) v = canon4(v, pc.q);
             epi(job, zb, z, x, v, pc);
         } else {
             mid[zm + job.dst + x] = v;
@@ -268,7 +272,7 @@ struct NttPlan {
 
 inline NttPlan make_plan(int log_n, bool inverse) {
     NttPlan pl;
-    if (log_n <= 13) {   // whole limb in shared memory (<= 64 KB), N / 8 threads
+    if (log_n <= 13) {   // whole limb in shared memory (<= 68 KB), N / 8 threads
         pl.npass = 1;
         NttGeom a{};
         a.log_n = log_n; a.lo_bit = 0; a.P = log_n; a.log_c = 0; a.first = 1; a.last = 1;
@@ -278,8 +282,7 @@ inline NttPlan make_plan(int log_n, bool inverse) {
     int pa = (log_n + 1) / 2;     // high (column) pass bits
     int pb = log_n - pa;          // low (chunk) pass bits
     NttGeom col{}, chk{};
-    col.log_n = log_n; col.lo_bit = pb; col.P = pa; col.log_c = 12 - pa < 4 ? 12 - pa : 4;
-    if (col.log_c < 0) col.log_c = 0;
+    col.log_n = log_n; col.lo_bit = pb; col.P = pa; col.log_c = 4;
     chk.log_n = log_n; chk.lo_bit = 0; chk.P = pb; chk.log_c = 12 - pb;
     pl.npass = 2;
     if (!inverse) { pl.g[0] = col; pl.g[1] = chk; }
@@ -287,6 +290,23 @@ inline NttPlan make_plan(int log_n, bool inverse) {
     pl.g[0].first = 1; pl.g[0].last = 0;
     pl.g[1].first = 0; pl.g[1].last = 1;
     return pl;
+}
+
+template <bool INV, int P, int LOGC, bool COL, class Pro, class Epi>
+inline cudaError_t launch_pass(const NttGeom& g, const PrimeTables& pt, const LimbJob* jobs, uint32_t njobs,
+                               uint32_t nz, u64* mid, const ZBases& zb, const Pro& pro, const Epi& epi,
+                               cudaStream_t st) {
+    constexpr uint32_t TILE = 1u << (P + LOGC);
+    const uint32_t ctas = 1u << (g.log_n - P - LOGC);
+    const size_t smem = (size_t)(TILE + TILE / 16) * sizeof(u64);
+    auto kern = ntt_kernel<INV, P, LOGC, COL, Pro, Epi>;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    kern<<<dim3(ctas, njobs, nz), TILE / 8, smem, st>>>(g, pt, jobs, mid, zb, pro, epi);
+    count_launches(1);
+    return cudaSuccess;
 }
 
 // Launch a full transform over `njobs` limbs x `nz` polynomials. Between
@@ -297,19 +317,25 @@ inline cudaError_t launch_ntt(int log_n, const PrimeTables& pt, const LimbJob* j
     if (njobs == 0 || nz == 0) return cudaSuccess;
     NttPlan pl = make_plan(log_n, INV);
     for (int i = 0; i < pl.npass; ++i) {
-        NttGeom g = pl.g[i];
-        uint32_t tile = 1u << (g.P + g.log_c);
-        uint32_t threads = tile / 8;
-        uint32_t ctas = 1u << (log_n - g.P - g.log_c);
-        dim3 grid(ctas, njobs, nz);
-        size_t smem = (size_t)tile * sizeof(u64);
-        if (smem > 48 * 1024) {
-            cudaError_t e = cudaFuncSetAttribute(ntt_pass_kernel<INV, Pro, Epi>,
-                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (e != cudaSuccess) return e;
+        const NttGeom& g = pl.g[i];
+        const bool col = g.lo_bit > 0;
+        cudaError_t e = cudaErrorInvalidValue;
+        if (!col && g.log_c == 0) {
+            switch (g.P) {
+            case 10: e = launch_pass<INV, 10, 0, false>(g, pt, jobs, njobs, nz, mid, zb, pro, epi, st); break;
+            case 11: e = launch_pass<INV, 11, 0, false>(g, pt, jobs, njobs, nz, mid, zb, pro, epi, st); break;
+            case 12: e = launch_pass<INV, 12, 0, false>(g, pt, jobs, njobs, nz, mid, zb, pro, epi, st); break;
+            case 13: e = launch_pass<INV, 13, 0, false>(g, pt, jobs, njobs, nz, mid, zb, pro, epi, st); break;
+            default: break;
+            }
+        } else if (col && g.log_c == 4) {
+            if (g.P == 7) e = launch_pass<INV, 7, 4, true>(g, pt, jobs, njobs, nz, mid, zb, pro, epi, st);
+            else if (g.P == 8) e = launch_pass<INV, 8, 4, true>(g, pt, jobs, njobs, nz, mid, zb, pro, epi, st);
+        } else if (!col) {
+            if (g.P == 7 && g.log_c == 5) e = launch_pass<INV, 7, 5, false>(g, pt, jobs, njobs, nz, mid, zb, pro, epi, st);
+            else if (g.P == 8 && g.log_c == 4) e = launch_pass<INV, 8, 4, false>(g, pt, jobs, njobs, nz, mid, zb, pro, epi, st);
         }
-        ntt_pass_kernel<INV, Pro, Epi><<<grid, threads, smem, st>>>(g, pt, jobs, mid, zb, pro, epi);
-        count_launches(1);
+        if (e != cudaSuccess) return e;
     }
     return cudaGetLastError();
 }
