@@ -120,6 +120,7 @@ SIGNATURES = {
     "afhe_eval_rotate_batch": (C.c_int, [CTX, C.POINTER(CtRef), C.POINTER(CtRef), u32, i32, u32]),
     "afhe_ntt_batch": (C.c_int, [CTX, P64, u32, u32, C.c_int]),
     "afhe_kernel_launches": (u64, []),
+    "afhe_decrypt_batch": (C.c_int, [CTX, C.POINTER(CtRef), u32, u64, u64, u32]),
     "afhe_key_switch_noalloc": (C.c_int, [CTX, C.c_void_p, u64, u32]),
     "afhe_eval_rotate_accumulate_batch": (C.c_int, [CTX, C.POINTER(CtRef), C.POINTER(CtRef), u32, i32, u32]),
     "afhe_eval_add_batch": (C.c_int, [CTX, C.POINTER(CtRef), C.POINTER(CtRef), C.POINTER(CtRef), u32, u32]),

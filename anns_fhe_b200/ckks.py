@@ -60,6 +60,12 @@ class Encoder:
         M = self.n * np.fft.ifft(y)
         return M[self.t] / scale
 
+    def decode_batch(self, coeffs: np.ndarray, scale: float) -> np.ndarray:
+        """decode() for each row of a (count, N) coefficient array."""
+        y = np.asarray(coeffs, dtype=np.float64) * self.zeta[None, :]
+        M = self.n * np.fft.ifft(y, axis=1)
+        return M[:, self.t] / scale
+
 
 def to_rns(coef: np.ndarray, primes) -> np.ndarray:
     """Signed integer coefficients -> limb-major residues (uint64)."""
@@ -243,6 +249,41 @@ class CkksClient:
         if not hasattr(self, "_pair"):
             self._pair = tuple(self.slots.take(2))
         return self._pair
+
+    def _region(self, name: str, words: int) -> int:
+        """A contiguous client work region of at least `words` words (cached)."""
+        have = getattr(self, "_regions", {})
+        self._regions = have
+        if name not in have or have[name][1] < words:
+            k = -(-words // self.slots.w)
+            have[name] = (self.slots.take(k)[0], k * self.slots.w)
+        return have[name][0]
+
+    def decrypt_batch(self, cts, level: int, scale: float) -> np.ndarray:
+        """Decrypt ciphertexts resident in poly_gmem; returns (count, N/2) slot values."""
+        from . import _lib as L
+        n, count = self.p.n, len(cts)
+        out = self._region("dec_out", count * level * n)
+        arr = (L.CtRef * max(count, 1))()
+        for i, (a, b) in enumerate(cts):
+            arr[i].c0_offset, arr[i].c1_offset = a, b
+        L.check(self.ctx.lib.afhe_decrypt_batch(self.ctx.h, arr, count, self.s_slot, out, level), "decrypt_batch")
+        limbs = self.ctx.read_poly(out, count * level * n).reshape(count, level * n)
+        if level == 1:
+            q = np.int64(self.p.q[0])
+            v = limbs.astype(np.int64)
+            coef = np.where(v > q // 2, v - q, v).astype(np.float64)
+        else:
+            coef = np.stack([crt_centered(row, self.p.q[:level]).astype(np.float64) for row in limbs])
+        return self.enc.decode_batch(coef, scale)
+
+    def decrypt_host_batch(self, cts: np.ndarray, level: int, scale: float) -> np.ndarray:
+        """Decrypt ciphertexts received as a host array (count, 2, level * N)."""
+        n, count = self.p.n, cts.shape[0]
+        w = level * n
+        inp = self._region("dec_in", count * 2 * w)
+        self.ctx.write_poly(inp, np.ascontiguousarray(cts).ravel())
+        return self.decrypt_batch([(inp + 2 * i * w, inp + (2 * i + 1) * w) for i in range(count)], level, scale)
 
     def plaintext(self, values, scale: float, off: int, level: int) -> None:
         """Encode `values` into an evaluation-form plaintext at `off` (level limbs)."""

@@ -499,6 +499,34 @@ int afhe_ntt_batch(afhe_ctx* ctx, const uint64_t* polys, uint32_t count, uint32_
 
 uint64_t afhe_kernel_launches(void) { return launches_so_far(); }
 
+int afhe_decrypt_batch(afhe_ctx* ctx, const afhe_ct_ref* cts, uint32_t count, uint64_t s_offset, uint64_t out_offset,
+                       uint32_t limbs) {
+    if (!ctx || (count && !cts)) return fail(ctx, AFHE_E_ARG, "null argument");
+    int rc;
+    if ((rc = check_limbs(ctx, limbs, 1)) || (rc = check_cts(ctx, cts, count, limbs)) ||
+        (rc = check_poly(ctx, s_offset, limbs)))
+        return rc;
+    const u64 w = (u64)limbs * ctx->n;
+    if (!range_ok(out_offset, (u64)count * w, ctx->prm.poly_words)) return fail(ctx, AFHE_E_RANGE, "output out of range");
+    for (uint32_t s0 = 0; s0 < count; s0 += ZMAX) {
+        uint32_t m = count - s0 < (uint32_t)ZMAX ? count - s0 : (uint32_t)ZMAX;
+        u64 A[ZMAX], S[ZMAX], O[ZMAX], C0[ZMAX];
+        for (uint32_t z = 0; z < m; ++z) {
+            A[z] = cts[s0 + z].c1_offset;
+            C0[z] = cts[s0 + z].c0_offset;
+            S[z] = s_offset;
+            O[z] = out_offset + (u64)(s0 + z) * w;
+        }
+        if ((rc = ew_batch(ctx, EW_MUL, A, S, O, m, limbs)) != AFHE_OK) return rc;     // c1 * s
+        if ((rc = ew_batch(ctx, EW_ADD, O, C0, O, m, limbs)) != AFHE_OK) return rc;    // + c0
+        ZBases zb{};
+        for (uint32_t z = 0; z < m; ++z) zb.src[z] = zb.mid[z] = zb.out[z] = O[z];
+        CK(launch_ntt_plain(true, ctx->log_n, ctx->nat.view(), ctx->jobs_qp, limbs, ctx->poly, ctx->poly, m, zb,
+                            ctx->st));
+    }
+    return AFHE_OK;
+}
+
 int afhe_eval_rotate_accumulate_batch(afhe_ctx* ctx, const afhe_ct_ref* in, const afhe_ct_ref* acc, uint32_t count,
                                       int32_t total, uint32_t limbs) {
     if (!ctx || (!in && count) || (!acc && count)) return fail(ctx, AFHE_E_ARG, "null argument");

@@ -153,6 +153,29 @@ class InteractiveQueryManager:
         s = self.slots.take(8)
         return QueryRecord((s[0], s[1]), (s[2], s[3]), (s[4], s[5]), (s[6], s[7]))
 
+    def alloc_queries(self, count: int) -> list[QueryRecord]:
+        """Records whose results (compacted coarse distances, candidate
+        distances; level lvl_out) are packed back to back in two outboxes, so
+        each reaches the host in one copy (read_outbox)."""
+        w = self.lvl_out * self.p.n
+        k = -(-2 * count * w // self.slots.w)
+        comp = self.slots.take(k)[0]
+        dist = self.slots.take(k)[0]
+        recs = []
+        for i in range(count):
+            s = self.slots.take(4)
+            recs.append(QueryRecord((s[0], s[1]), (s[2], s[3]),
+                                    (comp + 2 * i * w, comp + (2 * i + 1) * w),
+                                    (dist + 2 * i * w, dist + (2 * i + 1) * w)))
+        self._outbox = {"compact": comp, "dists": dist}
+        return recs
+
+    def read_outbox(self, kind: str, count: int) -> np.ndarray:
+        """(count, 2, lvl_out * N) result ciphertexts of the first `count`
+        records from alloc_queries, in one device-to-host copy."""
+        w = self.lvl_out * self.p.n
+        return self.ctx.read_poly(self._outbox[kind], 2 * count * w).reshape(count, 2, w)
+
     # ---- batched C-ABI helpers ----
     @staticmethod
     def _refs(cts):

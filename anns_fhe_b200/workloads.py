@@ -64,7 +64,7 @@ class Workload:
         slot_w = (self.params.L + self.params.K) * n
         B = slots // spec.d
         n_batches = sum(-(-len(v) // B) for v in self.index.lists)
-        n_slots = 16 + 1 + spec.n_list + 2 * n_batches + 8 * lanes + 8 * max_queries + 64
+        n_slots = 16 + 1 + spec.n_list + 2 * n_batches + 8 * lanes + 8 * max_queries + 64 + max_queries
         self.ctx = FheContext(self.params, poly_words=n_slots * slot_w,
                               key_words=(2 + 2 * (spec.log_n + 1)) * self.params.key_words() + 4096, device=device)
         self.slots = Slots(self.params, 0, n_slots * slot_w)
@@ -72,7 +72,7 @@ class Workload:
         self.iqm = InteractiveQueryManager(self.ctx, self.index, shape, self.slots, lanes=lanes)
         self.steps = self.iqm.rotation_steps()
         self.client.install_keys(self.steps)
-        self.records = [self.iqm.new_query() for _ in range(max_queries)]
+        self.records = self.iqm.alloc_queries(max_queries)
         self.ctx.sync()
         self.setup_s = time.time() - t0
 
@@ -97,20 +97,30 @@ class Workload:
     def decrypt_slots(self, ct) -> np.ndarray:
         return self.client.decrypt(ct[0], ct[1], self.iqm.lvl_out, self.iqm.out_scale).real
 
+    def decrypt_many(self, cts) -> np.ndarray:
+        return self.client.decrypt_batch(cts, self.iqm.lvl_out, self.iqm.out_scale).real
+
+    def select(self, recs) -> None:
+        """Stage 2 (client): decrypt the compacted coarse distances, keep nprobe lists."""
+        coarse = self.decrypt_many([r.compact for r in recs])[:, :self.spec.n_list]
+        for r, c in zip(recs, coarse):
+            r.probes = list(np.argsort(c, kind="stable")[:self.spec.nprobe])
+
     # ---- protocol ----
     def run(self, Q: np.ndarray, recs: list[QueryRecord] | None = None):
         """Full protocol for a batch of queries; returns per-query dicts."""
         recs = recs or self.records[:len(Q)]
         self.encrypt_queries(Q, recs)
         self.iqm.stage1_coarse(recs)
+        coarse = self.decrypt_many([r.compact for r in recs])[:, :self.spec.n_list]
         out = []
-        for r in recs:
-            coarse = self.decrypt_slots(r.compact)[:self.spec.n_list]
-            r.probes = list(np.argsort(coarse, kind="stable")[:self.spec.nprobe])
-            out.append({"coarse": coarse, "probes": r.probes})
+        for r, c in zip(recs, coarse):
+            r.probes = list(np.argsort(c, kind="stable")[:self.spec.nprobe])
+            out.append({"coarse": c, "probes": r.probes})
         self.iqm.stage3_fine(recs)
-        for r, o in zip(recs, out):
-            d = self.decrypt_slots(r.dists)[:len(r.vids)]
+        dists = self.decrypt_many([r.dists for r in recs])
+        for r, o, d in zip(recs, out, dists):
+            d = d[:len(r.vids)]
             order = np.argsort(d, kind="stable")[:self.spec.top_k]
             o.update(dists=d, vids=list(r.vids), topk=[r.vids[i] for i in order])
         return out

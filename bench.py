@@ -83,9 +83,7 @@ def run_ours(args, rank: int, world: int):
     pinned = [[torch.from_numpy(a).pin_memory() for a in cts] for cts in host_cts]
 
     def select(rs):
-        for r in rs:
-            coarse = wl.decrypt_slots(r.compact)[:wl.spec.n_list]
-            r.probes = list(np.argsort(coarse, kind="stable")[:wl.spec.nprobe])
+        wl.select(rs)
 
     def device_step():
         e0, e1, e2, e3 = (torch.cuda.Event(enable_timing=True) for _ in range(4))
@@ -109,18 +107,19 @@ def run_ours(args, rank: int, world: int):
                 lib.afhe_write_poly_async(wl.ctx.h, off, C.cast(t.data_ptr(), P64), t.numel())
                 h2d += t.numel() * 8
         iqm.stage1_coarse(recs)
-        d2h = 0
-        for r in recs:                    # client receives, decrypts, selects
-            c0, c1 = iqm.read_ct(r.compact)
-            d2h += (c0.size + c1.size) * 8
-            coarse = wl.client.decrypt_host(c0, c1, iqm.lvl_out, iqm.out_scale).real[:wl.spec.n_list]
-            r.probes = list(np.argsort(coarse, kind="stable")[:wl.spec.nprobe])
+        # client receives the compacted coarse distances, decrypts, selects
+        box = iqm.read_outbox("compact", len(recs))
+        d2h = box.nbytes
+        coarse = wl.client.decrypt_host_batch(box, iqm.lvl_out, iqm.out_scale).real[:, :wl.spec.n_list]
+        for r, c in zip(recs, coarse):
+            r.probes = list(np.argsort(c, kind="stable")[:wl.spec.nprobe])
         iqm.stage3_fine(recs)
-        for r in recs:
-            c0, c1 = iqm.read_ct(r.dists)
-            d2h += (c0.size + c1.size) * 8
-            d = wl.client.decrypt_host(c0, c1, iqm.lvl_out, iqm.out_scale).real[:len(r.vids)]
-            np.argsort(d, kind="stable")[:wl.spec.top_k]
+        # client receives the candidate distances, decrypts, ranks
+        box = iqm.read_outbox("dists", len(recs))
+        d2h += box.nbytes
+        dists = wl.client.decrypt_host_batch(box, iqm.lvl_out, iqm.out_scale).real
+        for r, d in zip(recs, dists):
+            np.argsort(d[:len(r.vids)], kind="stable")[:wl.spec.top_k]
         eb.record(stream)
         eb.synchronize()
         return ea.elapsed_time(eb), h2d, d2h

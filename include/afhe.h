@@ -242,6 +242,13 @@ int afhe_eval_rotate_batch(afhe_ctx* ctx, const afhe_ct_ref* in, const afhe_ct_r
 /* In-place forward (inverse = 0) or inverse NTT of `count` polynomials of
  * `limbs` limbs each (limb i under prime i, Q then P), one launch per pass. */
 int afhe_ntt_batch(afhe_ctx* ctx, const uint64_t* polys, uint32_t count, uint32_t limbs, int inverse);
+/* Client-side decryption of `count` ciphertexts at `limbs` limbs with the
+ * secret key s (evaluation form) at s_offset: writes INTT(c0 + c1 * s), the
+ * plaintext's coefficients mod each q_i, to out_offset + i * limbs * N.
+ * Replaces the arithmetic of OpenFHE's Decrypt
+ * (generate_interactive_test_vectors.cpp:443-447); decoding is the caller's. */
+int afhe_decrypt_batch(afhe_ctx* ctx, const afhe_ct_ref* cts, uint32_t count, uint64_t s_offset,
+                       uint64_t out_offset, uint32_t limbs);
 /* Kernels launched by this library so far (host-side count, all contexts). */
 uint64_t afhe_kernel_launches(void);
 /* acc[i] = acc[i] + rotate(in[i], total_rot), bit-identical to eval_rotate
