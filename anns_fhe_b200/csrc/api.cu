@@ -28,6 +28,31 @@ int cuda_fail(afhe_ctx* ctx, cudaError_t e, const char* where) {
 }
 
 u64 host_shoup(u64 w, u64 q) { return (u64)(((unsigned __int128)w << 64) / q); }
+
+int zf_from(afhe_ctx* ctx, const u64* vals, uint32_t n, ZField* out) {
+    if (n == 0) { *out = zf_const(0); return AFHE_OK; }
+    const u64 stride = n > 1 ? vals[1] - vals[0] : 0;
+    bool prog = true;
+    for (uint32_t i = 1; i < n && prog; ++i) prog = (vals[i] - vals[i - 1]) == stride;
+    if (prog) { *out = zf_stride(vals[0], stride); return AFHE_OK; }
+    DescRing& r = ctx->ring;
+    if (n > r.seg_words) return fail(ctx, AFHE_E_ARG, "batch too large for the descriptor ring");
+    if (r.pos + n > r.seg_words) {
+        CK(cudaEventRecord(r.ev[r.cur], ctx->st));
+        r.used[r.cur] = 1;
+        r.cur = (r.cur + 1) % r.nseg;
+        if (r.used[r.cur]) CK(cudaEventSynchronize(r.ev[r.cur]));
+        r.pos = 0;
+    }
+    const size_t at = r.cur * r.seg_words + r.pos;
+    std::memcpy(r.host + at, vals, n * sizeof(u64));
+    CK(cudaMemcpyAsync(r.dev + at, r.host + at, n * sizeof(u64), cudaMemcpyHostToDevice, ctx->st));
+    ZField f{};
+    f.arr = r.dev + at;
+    *out = f;
+    r.pos += (n + 31) & ~(size_t)31;
+    return AFHE_OK;
+}
 }  // namespace afhe
 
 namespace {
@@ -335,7 +360,9 @@ int afhe_ctx_create(const afhe_params* prm, afhe_ctx** out) {
         // poly_gmem and the context-private scratch share one allocation so a
         // kernel can address both from one base: scratch word w is poly word
         // poly_words + w.
-        ctx->scr_words = (size_t)kLanes * lane_words(ctx);
+        ctx->lanes = prm->max_batch ? prm->max_batch : 64;
+        if (ctx->lanes > 4096) { rc = fail(ctx, AFHE_E_ARG, "max_batch must be <= 4096"); break; }
+        ctx->scr_words = (size_t)ctx->lanes * lane_words(ctx);
         e = dalloc(&ctx->poly, prm->poly_words + ctx->scr_words);
         if (e != cudaSuccess) { rc = cuda_fail(ctx, e, "alloc poly_gmem + scratch"); break; }
         ctx->scr = ctx->poly + prm->poly_words;
@@ -346,6 +373,19 @@ int afhe_ctx_create(const afhe_params* prm, afhe_ctx** out) {
         if (e != cudaSuccess) { rc = cuda_fail(ctx, e, "clear arenas"); break; }
         rc = build_native_tables(ctx);
         if (rc != AFHE_OK) break;
+        DescRing& r = ctx->ring;
+        r.seg_words = 1u << 16;
+        r.nseg = 32;
+        e = cudaHostAlloc((void**)&r.host, r.seg_words * r.nseg * sizeof(u64), cudaHostAllocDefault);
+        if (e == cudaSuccess) e = dalloc(&r.dev, r.seg_words * r.nseg);
+        if (e != cudaSuccess) { rc = cuda_fail(ctx, e, "alloc descriptor ring"); break; }
+        r.ev.assign(r.nseg, nullptr);
+        r.used.assign(r.nseg, 0);
+        for (auto& ev : r.ev) {
+            e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+            if (e != cudaSuccess) break;
+        }
+        if (e != cudaSuccess) { rc = cuda_fail(ctx, e, "descriptor ring events"); break; }
     } while (0);
     if (rc != AFHE_OK) {
         std::string msg = ctx->err;
@@ -367,6 +407,9 @@ int afhe_ctx_destroy(afhe_ctx* ctx) {
     for (DevPrimeSet* s : {&ctx->nat, &ctx->ld}) { fr(s->pc); fr(s->tw); fr(s->itw); fr(s->tw2); fr(s->itw2); }
     fr(ctx->ld_crt); fr(ctx->ld_crt_sh); fr(ctx->ld_mod); fr(ctx->ld_jobs);
     for (auto& kv : ctx->rot) fr(kv.second.map);
+    fr(ctx->ring.dev);
+    if (ctx->ring.host) cudaFreeHost(ctx->ring.host);
+    for (auto& ev : ctx->ring.ev) if (ev) cudaEventDestroy(ev);
     if (ctx->st) cudaStreamDestroy(ctx->st);
     delete ctx;
     return AFHE_OK;
@@ -720,9 +763,9 @@ extern "C" int afhe_dispatch(afhe_ctx* ctx, const afhe_accel_args* a) {
         u64 src; bool in_scr;
         if ((rc = stage(ctx, a->src_a_offset, LN, a->dst_offset, LN, 0, &src, &in_scr)) != AFHE_OK) return rc;
         ZBases zb{};
-        zb.src[0] = src;
-        zb.mid[0] = a->dst_offset;
-        zb.out[0] = a->dst_offset;
+        zb.src = zf_const(src);
+        zb.mid = zf_const(a->dst_offset);
+        zb.out = zf_const(a->dst_offset);
         CK(launch_ntt_plain(a->op_code == AFHE_OP_INTT, ctx->log_n, ctx->ld.view(), ctx->ld_jobs, L,
                             in_scr ? ctx->scr : ctx->poly, ctx->poly, 1, zb, st));
         break;
@@ -752,12 +795,12 @@ extern "C" int afhe_dispatch(afhe_ctx* ctx, const afhe_accel_args* a) {
             if (!ia) CK(cudaMemcpyAsync(ctx->scr, ctx->poly + sa, LN * 8, cudaMemcpyDeviceToDevice, st));
             if (!ib) CK(cudaMemcpyAsync(ctx->scr + LN, ctx->poly + sb, LN * 8, cudaMemcpyDeviceToDevice, st));
             ZBases zb{};
-            zb.src[0] = 0; zb.aux[0] = LN; zb.out[0] = 2 * LN;
+            zb.src = zf_const(0); zb.aux = zf_const(LN); zb.out = zf_const(2 * LN);
             CK(launch_elementwise(op, dpc, 0, ctx->scr, n, L, 1, zb, st));
             CK(cudaMemcpyAsync(ctx->poly + a->dst_offset, ctx->scr + 2 * LN, LN * 8, cudaMemcpyDeviceToDevice, st));
         } else {
             ZBases zb{};
-            zb.src[0] = sa; zb.aux[0] = sb; zb.out[0] = a->dst_offset;
+            zb.src = zf_const(sa); zb.aux = zf_const(sb); zb.out = zf_const(a->dst_offset);
             CK(launch_elementwise(op, dpc, 0, ctx->poly, n, L, 1, zb, st));
         }
         CK(cudaStreamSynchronize(st));
@@ -772,7 +815,7 @@ extern "C" int afhe_dispatch(afhe_ctx* ctx, const afhe_accel_args* a) {
         CK(cudaMemcpyAsync(ctx->scr, ctx->poly + a->src_b_offset, (n / 2) * 8, cudaMemcpyDeviceToDevice, st));
         CK(cudaMemcpyAsync(ctx->scr + n, ctx->poly + a->src_a_offset, LN * 8, cudaMemcpyDeviceToDevice, st));
         ZBases zb{};
-        zb.src[0] = n; zb.out[0] = n + LN;
+        zb.src = zf_const(n); zb.out = zf_const(n + LN);
         CK(launch_automorphism(nullptr, ctx->scr, ctx->scr, n, L, 1, zb, st));
         CK(cudaMemcpyAsync(ctx->poly + a->dst_offset, ctx->scr + n + LN, LN * 8, cudaMemcpyDeviceToDevice, st));
         break;
@@ -794,11 +837,9 @@ extern "C" int afhe_dispatch(afhe_ctx* ctx, const afhe_accel_args* a) {
         CK(cudaMemcpyAsync(ctx->scr + s_in, ctx->poly + a->src_a_offset, LN * 8, cudaMemcpyDeviceToDevice, st));
         CK(cudaMemcpyAsync(ctx->scr + s_in + LN, ctx->poly + a->src_b_offset, LN * 8, cudaMemcpyDeviceToDevice, st));
         ZBases zb{};
-        for (int h = 0; h < 2; ++h) {
-            zb.src[h] = s_in + h * LN;
-            zb.out[h] = s_out + h * out;
-            zb.mid[h] = s_tmp + h * LN;
-        }
+        zb.src = zf_stride(s_in, LN);
+        zb.out = zf_stride(s_out, out);
+        zb.mid = zf_stride(s_tmp, LN);
         CK(launch_rescale(ctx->log_n, t, ctx->ld_jobs, L, ctx->scr, ctx->scr, 2, zb, st));
         CK(cudaMemcpyAsync(ctx->poly + a->dst_offset, ctx->scr + s_out, 2 * out * 8, cudaMemcpyDeviceToDevice, st));
         break;
@@ -844,17 +885,15 @@ extern "C" int afhe_dispatch(afhe_ctx* ctx, const afhe_accel_args* a) {
         if (SQ + kw > ctx->scr_words) return fail(ctx, AFHE_E_ARG, "scratch too small for this key switch");
         // input staged into scratch (fhe_accel_top.cpp:299-300 loads it first)
         CK(cudaMemcpyAsync(ctx->scr, ctx->poly + a->src_a_offset, SQ * 8, cudaMemcpyDeviceToDevice, st));
-        ZBases zb{};
-        zb.src[0] = 0;
-        zb.mid[0] = SQ;
-        zb.out[0] = a->dst_offset;        // ks0 at dst
-        zb.aux[0] = a->dst_offset + SQ;   // ks1 at dst + sizeQl * N
         // the kernel reads the input and writes the outputs through one arena
-        // base; the input lives in scratch, so route outputs via scratch too
+        // base; the input lives in scratch, so the outputs go via scratch too
         const u64 o_scr = SQ + kw;
         if (o_scr + 2 * SQ > ctx->scr_words) return fail(ctx, AFHE_E_ARG, "scratch too small for this key switch");
-        zb.out[0] = o_scr;
-        zb.aux[0] = o_scr + SQ;
+        ZBases zb{};
+        zb.src = zf_const(0);
+        zb.mid = zf_const(SQ);
+        zb.out = zf_const(o_scr);        // ks0
+        zb.aux = zf_const(o_scr + SQ);   // ks1
         CK(launch_key_switch(ctx->log_n, t, ctx->ld_jobs, ctx->ld_jobs + sq + K, n_modup, sq, sq, K, ctx->key,
                              a->evk_offset, a->evk_offset + (u64)parts * (sq + K) * n, sq + K, sq, ctx->scr, ctx->scr,
                              1, zb, st));

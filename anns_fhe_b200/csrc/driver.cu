@@ -8,6 +8,10 @@
 // never clobbered. Keys use the full-level layout: digit j, limb i of a key at
 // evk lives at evk + (j * (L + K) + (i < l ? i : L + i - l)) * N, evk_b after
 // all d digits of evk_a (fhe_host_driver.cpp:105-117, fhe_accel_top.cpp:304-305).
+//
+// A batched call processes up to ctx->lanes ciphertexts per launch; the
+// per-ciphertext offsets reach the kernels as ZFields (strided when regular,
+// else a small array staged through the context's descriptor ring).
 #include <cuda_runtime.h>
 
 #include <cstdlib>
@@ -20,6 +24,8 @@
 using namespace afhe;
 
 namespace {
+
+typedef std::vector<u64> Offs;
 
 int check_limbs(afhe_ctx* ctx, uint32_t limbs, uint32_t min_limbs) {
     if (limbs < min_limbs || limbs > ctx->L) return fail(ctx, AFHE_E_LEVEL, "limb count outside [min, L]");
@@ -44,52 +50,71 @@ int check_key(afhe_ctx* ctx, u64 evk) {
     return AFHE_OK;
 }
 
+int check_cts(afhe_ctx* ctx, const afhe_ct_ref* v, uint32_t count, uint32_t limbs) {
+    int rc;
+    for (uint32_t i = 0; i < count; ++i)
+        if ((rc = check_poly(ctx, v[i].c0_offset, limbs)) || (rc = check_poly(ctx, v[i].c1_offset, limbs))) return rc;
+    return AFHE_OK;
+}
+
+#define ZF(dst, vec)                                                                    \
+    do {                                                                                \
+        int _rc = zf_from(ctx, (vec).data(), (uint32_t)(vec).size(), &(dst));           \
+        if (_rc != AFHE_OK) return _rc;                                                 \
+    } while (0)
+
 // Key switch nz polynomials (poly_gmem-relative offsets) with one key, with
 // optional fusion (automorphism gather, c0 add, accumulate; see KsFuse).
-int ks_batch(afhe_ctx* ctx, const u64* in, const u64* out0, const u64* out1, uint32_t nz, u64 evk, uint32_t limbs,
-             const KsFuse* fuse = nullptr) {
+int ks_batch(afhe_ctx* ctx, const ZField& in, const ZField& out0, const ZField& out1, uint32_t nz, u64 evk,
+             uint32_t limbs, const KsFuse* fuse = nullptr) {
     const u64 n = ctx->n, S = (u64)ctx->L + ctx->K;
     const OpTabs& t = ctx->lv[limbs];
     const LevelJobs& lj = ctx->lvjobs[limbs];
     ZBases zb{};
-    for (uint32_t z = 0; z < nz; ++z) {
-        zb.src[z] = in[z];
-        zb.out[z] = out0[z];
-        zb.aux[z] = out1[z];
-        zb.mid[z] = lane_of(ctx, z).ks;
-    }
+    zb.src = in;
+    zb.out = out0;
+    zb.aux = out1;
+    zb.mid = lane_field(ctx, &Lane::ks);
     CK(launch_key_switch(ctx->log_n, t, ctx->jobs_qp, lj.modup, lj.n_modup, ctx->L, limbs, ctx->K, ctx->key, evk,
                          evk + (u64)ctx->dnum * S * n, (uint32_t)S, ctx->L, ctx->poly, ctx->scr, nz, zb, ctx->st,
                          fuse));
     return AFHE_OK;
 }
 
-// Rescale nz ciphertexts: (in0[z], in1[z]) -> (out0[z], out1[z]), level limbs -> limbs - 1.
-int rescale_batch(afhe_ctx* ctx, const u64* in0, const u64* in1, const u64* out0, const u64* out1, uint32_t nz,
+// Rescale nz ciphertexts (in0, in1) -> (out0, out1), level limbs -> limbs - 1.
+// The two polynomials of ciphertext z run as z' = 2z, 2z + 1.
+int rescale_batch(afhe_ctx* ctx, const Offs& in0, const Offs& in1, const Offs& out0, const Offs& out1,
                   uint32_t limbs) {
-    ZBases zb{};
+    const uint32_t nz = (uint32_t)in0.size();
+    Offs src(2 * nz), out(2 * nz);
     for (uint32_t z = 0; z < nz; ++z) {
-        Lane l = lane_of(ctx, z);
-        for (uint32_t h = 0; h < 2; ++h) {
-            uint32_t zz = 2 * z + h;
-            zb.src[zz] = h ? in1[z] : in0[z];
-            zb.out[zz] = h ? out1[z] : out0[z];
-            zb.mid[zz] = l.resc + (u64)h * ctx->L * ctx->n;
-        }
+        src[2 * z] = in0[z]; src[2 * z + 1] = in1[z];
+        out[2 * z] = out0[z]; out[2 * z + 1] = out1[z];
     }
+    ZBases zb{};
+    ZF(zb.src, src);
+    ZF(zb.out, out);
+    zb.mid = zf_pair(lane_field(ctx, &Lane::resc), (u64)ctx->L * ctx->n);
     CK(launch_rescale(ctx->log_n, ctx->lv[limbs], ctx->jobs_qp, limbs, ctx->poly, ctx->scr, 2 * nz, zb, ctx->st));
     return AFHE_OK;
 }
 
-int ew_batch(afhe_ctx* ctx, ElemOp op, const u64* a, const u64* b, const u64* o, uint32_t nz, uint32_t limbs) {
+int ew_fields(afhe_ctx* ctx, ElemOp op, const ZField& a, const ZField& b, const ZField& o, uint32_t nz,
+              uint32_t limbs) {
     ZBases zb{};
-    for (uint32_t z = 0; z < nz; ++z) {
-        zb.src[z] = a[z];
-        zb.aux[z] = b ? b[z] : a[z];
-        zb.out[z] = o[z];
-    }
+    zb.src = a;
+    zb.aux = b;
+    zb.out = o;
     CK(launch_elementwise(op, ctx->nat.pc, 0, ctx->poly, ctx->n, limbs, nz, zb, ctx->st));
     return AFHE_OK;
+}
+
+int ew_batch(afhe_ctx* ctx, ElemOp op, const Offs& a, const Offs* b, const Offs& o, uint32_t limbs) {
+    ZField fa, fb, fo;
+    ZF(fa, a);
+    if (b) ZF(fb, *b); else fb = fa;
+    ZF(fo, o);
+    return ew_fields(ctx, op, fa, fb, fo, (uint32_t)a.size(), limbs);
 }
 
 bool overlap(u64 a, u64 aw, u64 b, u64 bw) { return a < b + bw && b < a + aw; }
@@ -98,31 +123,31 @@ bool overlap(u64 a, u64 aw, u64 b, u64 bw) { return a < b + bw && b < a + aw; }
 int mult_relin_rescale_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const afhe_ct_ref* b, const afhe_ct_ref* d,
                              uint32_t nz, uint32_t limbs) {
     if (!ctx->has_relin) return fail(ctx, AFHE_E_NOKEY, "no relinearisation key set");
-    TensorArgs ta{};
-    u64 t0[TZMAX], t1[TZMAX], t2[TZMAX], k0[TZMAX], k1[TZMAX], o0[TZMAX], o1[TZMAX];
+    Offs a0(nz), a1(nz), b0(nz), b1(nz), o0(nz), o1(nz), t0(nz), t1(nz);
     for (uint32_t z = 0; z < nz; ++z) {
+        a0[z] = a[z].c0_offset; a1[z] = a[z].c1_offset;
+        b0[z] = b[z].c0_offset; b1[z] = b[z].c1_offset;
+        o0[z] = d[z].c0_offset; o1[z] = d[z].c1_offset;
         t0[z] = lane_temp(ctx, z, 0);
         t1[z] = lane_temp(ctx, z, 1);
-        t2[z] = lane_temp(ctx, z, 2);
-        k0[z] = lane_temp(ctx, z, 3);
-        k1[z] = lane_temp(ctx, z, 4);
-        ta.a0[z] = a[z].c0_offset; ta.a1[z] = a[z].c1_offset;
-        ta.b0[z] = b[z].c0_offset; ta.b1[z] = b[z].c1_offset;
-        ta.d0[z] = t0[z]; ta.d1[z] = t1[z]; ta.d2[z] = t2[z];
-        o0[z] = d[z].c0_offset; o1[z] = d[z].c1_offset;
     }
-    // 1. tensor product (fhe_host_driver.cpp:280-286)
+    // 1. tensor product (fhe_host_driver.cpp:280-286) into lane temps 0, 1, 2
+    TensorArgs ta{};
+    ZF(ta.a0, a0); ZF(ta.a1, a1); ZF(ta.b0, b0); ZF(ta.b1, b1);
+    ta.d0 = lane_temp_field(ctx, 0);
+    ta.d1 = lane_temp_field(ctx, 1);
+    ta.d2 = lane_temp_field(ctx, 2);
     CK(launch_tensor(ctx->nat.pc, ctx->poly, ctx->n, limbs, nz, ta, ctx->st));
     // 2-3. relinearise d2 and add (:288-293): d0 += ks0, d1 += ks1 in the
     //      key switch's ModDown epilogue
     KsFuse f{};
     f.has_acc = 1;
-    for (uint32_t z = 0; z < nz; ++z) { f.acc0[z] = t0[z]; f.acc1[z] = t1[z]; }
-    int rc = ks_batch(ctx, t2, t0, t1, nz, ctx->relin_off, limbs, &f);
+    f.acc0 = ta.d0;
+    f.acc1 = ta.d1;
+    int rc = ks_batch(ctx, ta.d2, ta.d0, ta.d1, nz, ctx->relin_off, limbs, &f);
     if (rc != AFHE_OK) return rc;
-    (void)k0; (void)k1;
     // 4. rescale into the destination (:296-305)
-    return rescale_batch(ctx, t0, t1, o0, o1, nz, limbs);
+    return rescale_batch(ctx, t0, t1, o0, o1, limbs);
 }
 
 // One rotation step on nz ciphertexts (fhe_host_driver.cpp:331-359):
@@ -130,40 +155,38 @@ int mult_relin_rescale_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const afhe_ct_
 // or, with acc, dst = acc + that. One fused key switch: the automorphism is
 // applied on the key switch's loads and the additions in its epilogue.
 // Inputs may alias outputs; acc may alias dst.
-int rotate_step_batch(afhe_ctx* ctx, const u64* in0, const u64* in1, const u64* d0, const u64* d1, uint32_t nz,
-                      int32_t step, uint32_t limbs, const u64* acc0 = nullptr, const u64* acc1 = nullptr) {
+int rotate_step_batch(afhe_ctx* ctx, const ZField& in0, const ZField& in1, const ZField& d0, const ZField& d1,
+                      uint32_t nz, int32_t step, uint32_t limbs, const ZField* acc0 = nullptr,
+                      const ZField* acc1 = nullptr) {
     auto it = ctx->rot.find(step);
     if (it == ctx->rot.end()) return fail(ctx, AFHE_E_NOKEY, "rotation key not found for step " + std::to_string(step));
     const RotKey& rk = it->second;
     KsFuse f{};
     f.map = rk.map;
     f.has_c0 = 1;
+    f.c0 = in0;
     f.has_acc = acc0 != nullptr;
-    for (uint32_t z = 0; z < nz; ++z) {
-        f.c0[z] = in0[z];
-        if (acc0) { f.acc0[z] = acc0[z]; f.acc1[z] = acc1[z]; }
-    }
+    if (acc0) { f.acc0 = *acc0; f.acc1 = *acc1; }
     return ks_batch(ctx, in1, d0, d1, nz, rk.evk_offset, limbs, &f);
 }
 
 // eval_rotate on nz ciphertexts by the same amount (fhe_host_driver.cpp:361-404):
-// |r| decomposed into descending powers of two, sign kept.
+// |r| decomposed into descending powers of two, sign kept. With `accumulate`,
+// dst += rotate(in) instead (the last step adds into dst in its epilogue).
 int rotate_batch(afhe_ctx* ctx, const afhe_ct_ref* in, const afhe_ct_ref* dst, uint32_t nz, int32_t total,
                  uint32_t limbs, bool accumulate = false) {
-    u64 i0[TZMAX], i1[TZMAX], o0[TZMAX], o1[TZMAX], c0[TZMAX], c1[TZMAX], x0[TZMAX], x1[TZMAX];
+    Offs i0(nz), i1(nz), o0(nz), o1(nz);
     for (uint32_t z = 0; z < nz; ++z) {
         i0[z] = in[z].c0_offset; i1[z] = in[z].c1_offset;
         o0[z] = dst[z].c0_offset; o1[z] = dst[z].c1_offset;
-        x0[z] = lane_temp(ctx, z, 2);   // chain temporaries (unused by a single step)
-        x1[z] = lane_temp(ctx, z, 5);
     }
     if (total == 0 && accumulate) {   // dst += in
-        u64 A[2 * TZMAX], B[2 * TZMAX];
+        Offs A(2 * nz), B(2 * nz);
         for (uint32_t z = 0; z < nz; ++z) {
             A[2 * z] = o0[z]; A[2 * z + 1] = o1[z];
             B[2 * z] = i0[z]; B[2 * z + 1] = i1[z];
         }
-        return ew_batch(ctx, EW_ADD, A, B, A, 2 * nz, limbs);
+        return ew_batch(ctx, EW_ADD, A, &B, A, limbs);
     }
     if (total == 0) {
         for (uint32_t z = 0; z < nz; ++z) {
@@ -184,23 +207,29 @@ int rotate_batch(afhe_ctx* ctx, const afhe_ct_ref* in, const afhe_ct_ref* dst, u
     }
     for (int32_t s : steps)
         if (!ctx->rot.count(s)) return fail(ctx, AFHE_E_NOKEY, "rotation key not found for step " + std::to_string(s));
-    for (uint32_t z = 0; z < nz; ++z) { c0[z] = i0[z]; c1[z] = i1[z]; }
+    ZField fi0, fi1, fo0, fo1;
+    ZF(fi0, i0); ZF(fi1, i1); ZF(fo0, o0); ZF(fo1, o1);
+    // chain temporaries (lane temps 2 and 5 are unused by a single step)
+    const ZField x0 = lane_temp_field(ctx, 2), x1 = lane_temp_field(ctx, 5);
+    ZField c0 = fi0, c1 = fi1;
     for (size_t k = 0; k < steps.size(); ++k) {
-        bool last = k + 1 == steps.size();
-        const u64* n0 = last ? o0 : x0;
-        const u64* n1 = last ? o1 : x1;
-        int rc = (last && accumulate) ? rotate_step_batch(ctx, c0, c1, n0, n1, nz, steps[k], limbs, o0, o1)
+        const bool last = k + 1 == steps.size();
+        const ZField& n0 = last ? fo0 : x0;
+        const ZField& n1 = last ? fo1 : x1;
+        int rc = (last && accumulate) ? rotate_step_batch(ctx, c0, c1, n0, n1, nz, steps[k], limbs, &fo0, &fo1)
                                       : rotate_step_batch(ctx, c0, c1, n0, n1, nz, steps[k], limbs);
         if (rc != AFHE_OK) return rc;
-        for (uint32_t z = 0; z < nz; ++z) { c0[z] = n0[z]; c1[z] = n1[z]; }
+        c0 = n0;
+        c1 = n1;
     }
     return AFHE_OK;
 }
 
 template <class F>
-int for_chunks(uint32_t count, F f) {
-    for (uint32_t s = 0; s < count; s += TZMAX) {
-        uint32_t m = count - s < (uint32_t)TZMAX ? count - s : (uint32_t)TZMAX;
+int for_chunks(afhe_ctx* ctx, uint32_t count, F f) {
+    const uint32_t w = ctx->lanes;
+    for (uint32_t s = 0; s < count; s += w) {
+        uint32_t m = count - s < w ? count - s : w;
         int rc = f(s, m);
         if (rc != AFHE_OK) return rc;
     }
@@ -257,7 +286,9 @@ static int ntt_native(afhe_ctx* ctx, bool inv, uint64_t src, uint64_t dst, uint3
         s = ctx->prm.poly_words;
     }
     ZBases zb{};
-    zb.src[0] = s; zb.mid[0] = dst; zb.out[0] = dst;
+    zb.src = zf_const(s);
+    zb.mid = zf_const(dst);
+    zb.out = zf_const(dst);
     CK(launch_ntt_plain(inv, ctx->log_n, ctx->nat.view(), ctx->jobs_qp, limbs, ctx->poly, ctx->poly, 1, zb, ctx->st));
     return AFHE_OK;
 }
@@ -281,7 +312,7 @@ static int ew_single(afhe_ctx* ctx, ElemOp op, uint64_t a, uint64_t b, uint64_t 
         CK(cudaMemcpyAsync(ctx->scr + w, ctx->poly + b, w * 8, cudaMemcpyDeviceToDevice, ctx->st));
         bb = ctx->prm.poly_words + w;
     }
-    return ew_batch(ctx, op, &aa, &bb, &dst, 1, limbs);
+    return ew_fields(ctx, op, zf_const(aa), zf_const(bb), zf_const(dst), 1, limbs);
 }
 
 int afhe_poly_add(afhe_ctx* c, uint64_t a, uint64_t b, uint64_t d, uint32_t l) { return ew_single(c, EW_ADD, a, b, d, l); }
@@ -301,8 +332,8 @@ int afhe_automorphism(afhe_ctx* ctx, uint64_t src, uint32_t galois, uint64_t dst
     CK(cudaMemcpyAsync(dmap, map.data(), ctx->n * 4, cudaMemcpyHostToDevice, ctx->st));
     CK(cudaMemcpyAsync(ctx->scr + ctx->n, ctx->poly + src, w * 8, cudaMemcpyDeviceToDevice, ctx->st));
     ZBases zb{};
-    zb.src[0] = ctx->prm.poly_words + ctx->n;
-    zb.out[0] = dst;
+    zb.src = zf_const(ctx->prm.poly_words + ctx->n);
+    zb.out = zf_const(dst);
     CK(launch_automorphism(dmap, nullptr, ctx->poly, ctx->n, limbs, 1, zb, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));   // the host map buffer goes out of scope
     return AFHE_OK;
@@ -319,7 +350,7 @@ int afhe_rescale(afhe_ctx* ctx, uint64_t c0_in, uint64_t c1_in, uint64_t c0_out,
     u64 t0 = lane_temp(ctx, 0, 0), t1 = lane_temp(ctx, 0, 1);
     CK(cudaMemcpyAsync(ctx->poly + t0, ctx->poly + c0_in, w * 8, cudaMemcpyDeviceToDevice, ctx->st));
     CK(cudaMemcpyAsync(ctx->poly + t1, ctx->poly + c1_in, w * 8, cudaMemcpyDeviceToDevice, ctx->st));
-    return rescale_batch(ctx, &t0, &t1, &c0_out, &c1_out, 1, limbs);
+    return rescale_batch(ctx, Offs{t0}, Offs{t1}, Offs{c0_out}, Offs{c1_out}, limbs);
 }
 
 int afhe_key_switch(afhe_ctx* ctx, uint64_t src, uint64_t evk, uint64_t d0, uint64_t d1, uint32_t limbs) {
@@ -331,7 +362,7 @@ int afhe_key_switch(afhe_ctx* ctx, uint64_t src, uint64_t evk, uint64_t d0, uint
     const u64 w = (u64)limbs * ctx->n;
     u64 t = lane_temp(ctx, 0, 2);
     CK(cudaMemcpyAsync(ctx->poly + t, ctx->poly + src, w * 8, cudaMemcpyDeviceToDevice, ctx->st));
-    return ks_batch(ctx, &t, &d0, &d1, 1, evk, limbs);
+    return ks_batch(ctx, zf_const(t), zf_const(d0), zf_const(d1), 1, evk, limbs);
 }
 
 // ---- composite operators ------------------------------------------------------
@@ -356,13 +387,10 @@ int afhe_eval_mult_relin_rescale_batch(afhe_ctx* ctx, const afhe_ct_ref* a, cons
                                        uint32_t count, uint32_t limbs) {
     if (!ctx || (!a && count) || (!b && count) || (!d && count)) return fail(ctx, AFHE_E_ARG, "null argument");
     int rc;
-    if ((rc = check_limbs(ctx, limbs, 2))) return rc;
-    for (uint32_t i = 0; i < count; ++i)
-        if ((rc = check_poly(ctx, a[i].c0_offset, limbs)) || (rc = check_poly(ctx, a[i].c1_offset, limbs)) ||
-            (rc = check_poly(ctx, b[i].c0_offset, limbs)) || (rc = check_poly(ctx, b[i].c1_offset, limbs)) ||
-            (rc = check_poly(ctx, d[i].c0_offset, limbs - 1)) || (rc = check_poly(ctx, d[i].c1_offset, limbs - 1)))
-            return rc;
-    return for_chunks(count, [&](uint32_t s, uint32_t m) { return mult_relin_rescale_batch(ctx, a + s, b + s, d + s, m, limbs); });
+    if ((rc = check_limbs(ctx, limbs, 2)) || (rc = check_cts(ctx, a, count, limbs)) ||
+        (rc = check_cts(ctx, b, count, limbs)) || (rc = check_cts(ctx, d, count, limbs - 1)))
+        return rc;
+    return for_chunks(ctx, count, [&](uint32_t s, uint32_t m) { return mult_relin_rescale_batch(ctx, a + s, b + s, d + s, m, limbs); });
 }
 
 int afhe_eval_mult_relin_rescale(afhe_ctx* ctx, uint64_t a0, uint64_t a1, uint64_t b0, uint64_t b1, uint64_t d0,
@@ -371,17 +399,36 @@ int afhe_eval_mult_relin_rescale(afhe_ctx* ctx, uint64_t a0, uint64_t a1, uint64
     return afhe_eval_mult_relin_rescale_batch(ctx, &a, &b, &d, 1, limbs);
 }
 
+int afhe_eval_mult_plain_rescale_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const uint64_t* pt, const afhe_ct_ref* d,
+                                       uint32_t count, uint32_t limbs) {
+    if (!ctx || (count && (!a || !pt || !d))) return fail(ctx, AFHE_E_ARG, "null argument");
+    int rc;
+    if ((rc = check_limbs(ctx, limbs, 2)) || (rc = check_cts(ctx, a, count, limbs)) ||
+        (rc = check_cts(ctx, d, count, limbs - 1)))
+        return rc;
+    for (uint32_t i = 0; i < count; ++i)
+        if ((rc = check_poly(ctx, pt[i], limbs))) return rc;
+    // fhe_host_driver.cpp:308-329: (c0 * pt, c1 * pt), then rescale
+    return for_chunks(ctx, count, [&](uint32_t s, uint32_t m) {
+        Offs A(2 * m), P(2 * m), T(2 * m), t0(m), t1(m), o0(m), o1(m);
+        for (uint32_t z = 0; z < m; ++z) {
+            t0[z] = lane_temp(ctx, z, 0);
+            t1[z] = lane_temp(ctx, z, 1);
+            A[2 * z] = a[s + z].c0_offset; A[2 * z + 1] = a[s + z].c1_offset;
+            P[2 * z] = pt[s + z]; P[2 * z + 1] = pt[s + z];
+            T[2 * z] = t0[z]; T[2 * z + 1] = t1[z];
+            o0[z] = d[s + z].c0_offset; o1[z] = d[s + z].c1_offset;
+        }
+        int r = ew_batch(ctx, EW_MUL, A, &P, T, limbs);
+        if (r != AFHE_OK) return r;
+        return rescale_batch(ctx, t0, t1, o0, o1, limbs);
+    });
+}
+
 int afhe_eval_mult_plain_rescale(afhe_ctx* ctx, uint64_t a0, uint64_t a1, uint64_t pt, uint64_t d0, uint64_t d1,
                                  uint32_t limbs) {
-    if (!ctx) return fail(nullptr, AFHE_E_ARG, "null context");
-    int rc;
-    if ((rc = check_limbs(ctx, limbs, 2)) || (rc = check_poly(ctx, a0, limbs)) || (rc = check_poly(ctx, a1, limbs)) ||
-        (rc = check_poly(ctx, pt, limbs)) || (rc = check_poly(ctx, d0, limbs - 1)) || (rc = check_poly(ctx, d1, limbs - 1)))
-        return rc;
-    // fhe_host_driver.cpp:308-329: (c0 * pt, c1 * pt), then rescale
-    u64 A[2] = {a0, a1}, B[2] = {pt, pt}, T[2] = {lane_temp(ctx, 0, 0), lane_temp(ctx, 0, 1)};
-    if ((rc = ew_batch(ctx, EW_MUL, A, B, T, 2, limbs)) != AFHE_OK) return rc;
-    return rescale_batch(ctx, &T[0], &T[1], &d0, &d1, 1, limbs);
+    afhe_ct_ref a{a0, a1}, d{d0, d1};
+    return afhe_eval_mult_plain_rescale_batch(ctx, &a, &pt, &d, 1, limbs);
 }
 
 int afhe_eval_rotate_single_step(afhe_ctx* ctx, uint64_t i0, uint64_t i1, uint64_t d0, uint64_t d1, int32_t step,
@@ -391,26 +438,34 @@ int afhe_eval_rotate_single_step(afhe_ctx* ctx, uint64_t i0, uint64_t i1, uint64
     if ((rc = check_limbs(ctx, limbs, 1)) || (rc = check_poly(ctx, i0, limbs)) || (rc = check_poly(ctx, i1, limbs)) ||
         (rc = check_poly(ctx, d0, limbs)) || (rc = check_poly(ctx, d1, limbs)))
         return rc;
-    return rotate_step_batch(ctx, &i0, &i1, &d0, &d1, 1, step, limbs);
+    return rotate_step_batch(ctx, zf_const(i0), zf_const(i1), zf_const(d0), zf_const(d1), 1, step, limbs);
 }
 
 int afhe_eval_rotate_batch(afhe_ctx* ctx, const afhe_ct_ref* in, const afhe_ct_ref* dst, uint32_t count, int32_t total,
                            uint32_t limbs) {
     if (!ctx || (!in && count) || (!dst && count)) return fail(ctx, AFHE_E_ARG, "null argument");
     int rc;
-    if ((rc = check_limbs(ctx, limbs, 1))) return rc;
-    for (uint32_t i = 0; i < count; ++i)
-        if ((rc = check_poly(ctx, in[i].c0_offset, limbs)) || (rc = check_poly(ctx, in[i].c1_offset, limbs)) ||
-            (rc = check_poly(ctx, dst[i].c0_offset, limbs)) || (rc = check_poly(ctx, dst[i].c1_offset, limbs)))
-            return rc;
-    return for_chunks(count, [&](uint32_t s, uint32_t m) { return rotate_batch(ctx, in + s, dst + s, m, total, limbs); });
+    if ((rc = check_limbs(ctx, limbs, 1)) || (rc = check_cts(ctx, in, count, limbs)) ||
+        (rc = check_cts(ctx, dst, count, limbs)))
+        return rc;
+    return for_chunks(ctx, count, [&](uint32_t s, uint32_t m) { return rotate_batch(ctx, in + s, dst + s, m, total, limbs); });
 }
 
-static int check_cts(afhe_ctx* ctx, const afhe_ct_ref* v, uint32_t count, uint32_t limbs) {
+int afhe_eval_rotate_accumulate_batch(afhe_ctx* ctx, const afhe_ct_ref* in, const afhe_ct_ref* acc, uint32_t count,
+                                      int32_t total, uint32_t limbs) {
+    if (!ctx || (!in && count) || (!acc && count)) return fail(ctx, AFHE_E_ARG, "null argument");
     int rc;
-    for (uint32_t i = 0; i < count; ++i)
-        if ((rc = check_poly(ctx, v[i].c0_offset, limbs)) || (rc = check_poly(ctx, v[i].c1_offset, limbs))) return rc;
-    return AFHE_OK;
+    if ((rc = check_limbs(ctx, limbs, 1)) || (rc = check_cts(ctx, in, count, limbs)) ||
+        (rc = check_cts(ctx, acc, count, limbs)))
+        return rc;
+    return for_chunks(ctx, count, [&](uint32_t s, uint32_t m) {
+        return rotate_batch(ctx, in + s, acc + s, m, total, limbs, true);
+    });
+}
+
+int afhe_eval_rotate(afhe_ctx* ctx, uint64_t i0, uint64_t i1, uint64_t d0, uint64_t d1, int32_t total, uint32_t limbs) {
+    afhe_ct_ref in{i0, i1}, d{d0, d1};
+    return afhe_eval_rotate_batch(ctx, &in, &d, 1, total, limbs);
 }
 
 // Batched elementwise composites: ciphertext i of the batch is computed
@@ -423,14 +478,14 @@ int afhe_eval_add_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const afhe_ct_ref* 
     if ((rc = check_limbs(ctx, limbs, 1)) || (rc = check_cts(ctx, a, count, limbs)) ||
         (rc = check_cts(ctx, b, count, limbs)) || (rc = check_cts(ctx, d, count, limbs)))
         return rc;
-    return for_chunks(count, [&](uint32_t s, uint32_t m) {
-        u64 A[2 * TZMAX], B[2 * TZMAX], D[2 * TZMAX];
+    return for_chunks(ctx, count, [&](uint32_t s, uint32_t m) {
+        Offs A(2 * m), B(2 * m), D(2 * m);
         for (uint32_t z = 0; z < m; ++z) {
             A[2 * z] = a[s + z].c0_offset; A[2 * z + 1] = a[s + z].c1_offset;
             B[2 * z] = b[s + z].c0_offset; B[2 * z + 1] = b[s + z].c1_offset;
             D[2 * z] = d[s + z].c0_offset; D[2 * z + 1] = d[s + z].c1_offset;
         }
-        return ew_batch(ctx, EW_ADD, A, B, D, 2 * m, limbs);
+        return ew_batch(ctx, EW_ADD, A, &B, D, limbs);
     });
 }
 
@@ -442,42 +497,17 @@ int afhe_eval_sub_plain_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const uint64_
         return rc;
     for (uint32_t i = 0; i < count; ++i)
         if ((rc = check_poly(ctx, pt[i], limbs))) return rc;
-    return for_chunks(count, [&](uint32_t s, uint32_t m) {
-        u64 A[TZMAX], P[TZMAX], D[TZMAX];
+    return for_chunks(ctx, count, [&](uint32_t s, uint32_t m) {
+        Offs A(m), P(m), D(m), A2, D2;
         for (uint32_t z = 0; z < m; ++z) { A[z] = a[s + z].c0_offset; P[z] = pt[s + z]; D[z] = d[s + z].c0_offset; }
-        int r = ew_batch(ctx, EW_SUB, A, P, D, m, limbs);
+        int r = ew_batch(ctx, EW_SUB, A, &P, D, limbs);
         if (r != AFHE_OK) return r;
-        for (uint32_t z = 0; z < m; ++z) { A[z] = a[s + z].c1_offset; D[z] = d[s + z].c1_offset; }
-        uint32_t k = 0;
-        u64 A2[TZMAX], D2[TZMAX];
         for (uint32_t z = 0; z < m; ++z)
-            if (A[z] != D[z]) { A2[k] = A[z]; D2[k] = D[z]; ++k; }
-        return k ? ew_batch(ctx, EW_COPY, A2, nullptr, D2, k, limbs) : AFHE_OK;
-    });
-}
-
-int afhe_eval_mult_plain_rescale_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const uint64_t* pt, const afhe_ct_ref* d,
-                                       uint32_t count, uint32_t limbs) {
-    if (!ctx || (count && (!a || !pt || !d))) return fail(ctx, AFHE_E_ARG, "null argument");
-    int rc;
-    if ((rc = check_limbs(ctx, limbs, 2)) || (rc = check_cts(ctx, a, count, limbs)) ||
-        (rc = check_cts(ctx, d, count, limbs - 1)))
-        return rc;
-    for (uint32_t i = 0; i < count; ++i)
-        if ((rc = check_poly(ctx, pt[i], limbs))) return rc;
-    return for_chunks(count, [&](uint32_t s, uint32_t m) {
-        u64 A[2 * TZMAX], P[2 * TZMAX], T[2 * TZMAX], t0[TZMAX], t1[TZMAX], o0[TZMAX], o1[TZMAX];
-        for (uint32_t z = 0; z < m; ++z) {
-            t0[z] = lane_temp(ctx, z, 0);
-            t1[z] = lane_temp(ctx, z, 1);
-            A[2 * z] = a[s + z].c0_offset; A[2 * z + 1] = a[s + z].c1_offset;
-            P[2 * z] = pt[s + z]; P[2 * z + 1] = pt[s + z];
-            T[2 * z] = t0[z]; T[2 * z + 1] = t1[z];
-            o0[z] = d[s + z].c0_offset; o1[z] = d[s + z].c1_offset;
-        }
-        int r = ew_batch(ctx, EW_MUL, A, P, T, 2 * m, limbs);
-        if (r != AFHE_OK) return r;
-        return rescale_batch(ctx, t0, t1, o0, o1, m, limbs);
+            if (a[s + z].c1_offset != d[s + z].c1_offset) {
+                A2.push_back(a[s + z].c1_offset);
+                D2.push_back(d[s + z].c1_offset);
+            }
+        return A2.empty() ? AFHE_OK : ew_batch(ctx, EW_COPY, A2, nullptr, D2, limbs);
     });
 }
 
@@ -487,10 +517,13 @@ int afhe_ntt_batch(afhe_ctx* ctx, const uint64_t* polys, uint32_t count, uint32_
     if ((rc = check_limbs_ext(ctx, limbs))) return rc;
     for (uint32_t i = 0; i < count; ++i)
         if ((rc = check_poly(ctx, polys[i], limbs))) return rc;
-    for (uint32_t s = 0; s < count; s += ZMAX) {
-        uint32_t m = count - s < (uint32_t)ZMAX ? count - s : (uint32_t)ZMAX;
+    for (uint32_t s = 0; s < count; s += 4096) {
+        uint32_t m = count - s < 4096u ? count - s : 4096u;
+        Offs v(polys + s, polys + s + m);
         ZBases zb{};
-        for (uint32_t z = 0; z < m; ++z) zb.src[z] = zb.mid[z] = zb.out[z] = polys[s + z];
+        ZF(zb.src, v);
+        zb.mid = zb.src;
+        zb.out = zb.src;
         CK(launch_ntt_plain(inverse != 0, ctx->log_n, ctx->nat.view(), ctx->jobs_qp, limbs, ctx->poly, ctx->poly, m,
                             zb, ctx->st));
     }
@@ -508,40 +541,22 @@ int afhe_decrypt_batch(afhe_ctx* ctx, const afhe_ct_ref* cts, uint32_t count, ui
         return rc;
     const u64 w = (u64)limbs * ctx->n;
     if (!range_ok(out_offset, (u64)count * w, ctx->prm.poly_words)) return fail(ctx, AFHE_E_RANGE, "output out of range");
-    for (uint32_t s0 = 0; s0 < count; s0 += ZMAX) {
-        uint32_t m = count - s0 < (uint32_t)ZMAX ? count - s0 : (uint32_t)ZMAX;
-        u64 A[ZMAX], S[ZMAX], O[ZMAX], C0[ZMAX];
-        for (uint32_t z = 0; z < m; ++z) {
-            A[z] = cts[s0 + z].c1_offset;
-            C0[z] = cts[s0 + z].c0_offset;
-            S[z] = s_offset;
-            O[z] = out_offset + (u64)(s0 + z) * w;
-        }
-        if ((rc = ew_batch(ctx, EW_MUL, A, S, O, m, limbs)) != AFHE_OK) return rc;     // c1 * s
-        if ((rc = ew_batch(ctx, EW_ADD, O, C0, O, m, limbs)) != AFHE_OK) return rc;    // + c0
+    for (uint32_t s0 = 0; s0 < count; s0 += 4096) {
+        uint32_t m = count - s0 < 4096u ? count - s0 : 4096u;
+        Offs C1(m), C0(m);
+        for (uint32_t z = 0; z < m; ++z) { C1[z] = cts[s0 + z].c1_offset; C0[z] = cts[s0 + z].c0_offset; }
+        ZField f1, f0;
+        ZF(f1, C1);
+        ZF(f0, C0);
+        const ZField O = zf_stride(out_offset + (u64)s0 * w, w);
+        if ((rc = ew_fields(ctx, EW_MUL, f1, zf_const(s_offset), O, m, limbs)) != AFHE_OK) return rc;   // c1 * s
+        if ((rc = ew_fields(ctx, EW_ADD, O, f0, O, m, limbs)) != AFHE_OK) return rc;                    // + c0
         ZBases zb{};
-        for (uint32_t z = 0; z < m; ++z) zb.src[z] = zb.mid[z] = zb.out[z] = O[z];
+        zb.src = zb.mid = zb.out = O;
         CK(launch_ntt_plain(true, ctx->log_n, ctx->nat.view(), ctx->jobs_qp, limbs, ctx->poly, ctx->poly, m, zb,
                             ctx->st));
     }
     return AFHE_OK;
-}
-
-int afhe_eval_rotate_accumulate_batch(afhe_ctx* ctx, const afhe_ct_ref* in, const afhe_ct_ref* acc, uint32_t count,
-                                      int32_t total, uint32_t limbs) {
-    if (!ctx || (!in && count) || (!acc && count)) return fail(ctx, AFHE_E_ARG, "null argument");
-    int rc;
-    if ((rc = check_limbs(ctx, limbs, 1)) || (rc = check_cts(ctx, in, count, limbs)) ||
-        (rc = check_cts(ctx, acc, count, limbs)))
-        return rc;
-    return for_chunks(count, [&](uint32_t s, uint32_t m) {
-        return rotate_batch(ctx, in + s, acc + s, m, total, limbs, true);
-    });
-}
-
-int afhe_eval_rotate(afhe_ctx* ctx, uint64_t i0, uint64_t i1, uint64_t d0, uint64_t d1, int32_t total, uint32_t limbs) {
-    afhe_ct_ref in{i0, i1}, d{d0, d1};
-    return afhe_eval_rotate_batch(ctx, &in, &d, 1, total, limbs);
 }
 
 }  // extern "C"

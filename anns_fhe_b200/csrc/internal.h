@@ -50,6 +50,17 @@ struct DevPrimeSet {
     PrimeTables view() const { return PrimeTables{pc, tw2, itw2}; }
 };
 
+// Ring of small per-launch descriptor arrays (ZField::arr): pinned host
+// staging and device memory in segments; a segment is reused only after the
+// event recorded when the stream moved past it has completed.
+struct DescRing {
+    u64* host = nullptr;
+    u64* dev = nullptr;
+    size_t seg_words = 0, nseg = 0, cur = 0, pos = 0;
+    std::vector<cudaEvent_t> ev;
+    std::vector<char> used;
+};
+
 struct RotKey {
     int32_t step;
     uint32_t galois;
@@ -95,9 +106,11 @@ struct afhe_ctx {
     afhe::LimbJob* ld_jobs = nullptr;  // per-call job list (device)
     size_t ld_jobs_cap = 0;
 
-    // scratch for composite operators (context-private)
+    // scratch for composite operators (context-private), `lanes` lanes
     afhe::u64* scr = nullptr;
     size_t scr_words = 0;
+    uint32_t lanes = 64;
+    afhe::DescRing ring;
 
     // key directory
     bool has_relin = false;
@@ -119,10 +132,8 @@ cudaError_t launch_elementwise(ElemOp op, const PrimeConst* pc, uint32_t prime0,
                                uint32_t limbs, uint32_t nz, const ZBases& zb, cudaStream_t st);
 
 // Ciphertext tensor product operands, per z (word offsets into one arena).
-constexpr int TZMAX = 64;
 struct TensorArgs {
-    u64 a0[TZMAX], a1[TZMAX], b0[TZMAX], b1[TZMAX];
-    u64 d0[TZMAX], d1[TZMAX], d2[TZMAX];
+    ZField a0, a1, b0, b1, d0, d1, d2;
 };
 cudaError_t launch_tensor(const PrimeConst* pc, u64* arena, uint32_t n, uint32_t limbs, uint32_t nz,
                           const TensorArgs& ta, cudaStream_t st);
@@ -156,9 +167,7 @@ struct KsFuse {
     const uint32_t* map;
     int has_c0;
     int has_acc;
-    u64 c0[ZMAX / 2];
-    u64 acc0[ZMAX / 2];
-    u64 acc1[ZMAX / 2];
+    ZField c0, acc0, acc1;
 };
 size_t ks_scratch_words(uint32_t n, uint32_t L, uint32_t K, uint32_t parts);
 cudaError_t launch_key_switch(int log_n, const OpTabs& t, const LimbJob* jobs_qp, const LimbJob* jobs_modup,

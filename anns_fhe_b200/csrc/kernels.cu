@@ -25,14 +25,13 @@ uint64_t launches_so_far() { return g_launches.load(std::memory_order_relaxed); 
 // ---------------------------------------------------------------------------
 template <int OP>
 __global__ void __launch_bounds__(256) elementwise_kernel(const PrimeConst* __restrict__ pc, uint32_t prime0,
-                                                          u64* __restrict__ arena, uint32_t n,
-                                                          const __grid_constant__ ZBases zb) {
+                                                          u64* __restrict__ arena, uint32_t n, const ZBases zb) {
     const uint32_t l = blockIdx.y, z = blockIdx.z;
     const PrimeConst p = pc[prime0 + l];
     const u64 off = (u64)l * n;
-    const u64* a = arena + zb.src[z] + off;
-    const u64* b = arena + zb.aux[z] + off;
-    u64* o = arena + zb.out[z] + off;
+    const u64* a = arena + zb.src.at(z) + off;
+    const u64* b = arena + zb.aux.at(z) + off;
+    u64* o = arena + zb.out.at(z) + off;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         u64 x = a[i];
         u64 r;
@@ -63,17 +62,17 @@ cudaError_t launch_elementwise(ElemOp op, const PrimeConst* pc, uint32_t prime0,
 //   d0 = a0*b0, d1 = a0*b1 + a1*b0, d2 = a1*b1  (d1 reduced once from 128 bits)
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) tensor_kernel(const PrimeConst* __restrict__ pc, u64* __restrict__ arena,
-                                                     uint32_t n, const __grid_constant__ TensorArgs ta) {
+                                                     uint32_t n, const TensorArgs ta) {
     const uint32_t l = blockIdx.y, z = blockIdx.z;
     const ModConst m = modconst_of(pc[l]);
     const u64 off = (u64)l * n;
-    const u64* a0 = arena + ta.a0[z] + off;
-    const u64* a1 = arena + ta.a1[z] + off;
-    const u64* b0 = arena + ta.b0[z] + off;
-    const u64* b1 = arena + ta.b1[z] + off;
-    u64* d0 = arena + ta.d0[z] + off;
-    u64* d1 = arena + ta.d1[z] + off;
-    u64* d2 = arena + ta.d2[z] + off;
+    const u64* a0 = arena + ta.a0.at(z) + off;
+    const u64* a1 = arena + ta.a1.at(z) + off;
+    const u64* b0 = arena + ta.b0.at(z) + off;
+    const u64* b1 = arena + ta.b1.at(z) + off;
+    u64* d0 = arena + ta.d0.at(z) + off;
+    u64* d1 = arena + ta.d1.at(z) + off;
+    u64* d2 = arena + ta.d2.at(z) + off;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         u64 x0 = a0[i], x1 = a1[i], y0 = b0[i], y1 = b1[i];
         Acc128 c;
@@ -100,11 +99,11 @@ cudaError_t launch_tensor(const PrimeConst* pc, u64* arena, uint32_t n, uint32_t
 // ---------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) automorphism_kernel(const uint32_t* __restrict__ map32,
                                                            const u64* __restrict__ map64, u64* __restrict__ arena,
-                                                           uint32_t n, const __grid_constant__ ZBases zb) {
+                                                           uint32_t n, const ZBases zb) {
     const uint32_t l = blockIdx.y, z = blockIdx.z;
     const u64 off = (u64)l * n;
-    const u64* a = arena + zb.src[z] + off;
-    u64* o = arena + zb.out[z] + off;
+    const u64* a = arena + zb.src.at(z) + off;
+    u64* o = arena + zb.out.at(z) + off;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         uint32_t idx;
         if (map32) idx = map32[i];
@@ -152,7 +151,7 @@ struct RescaleLoad {
                                               const PrimeConst& pc) const {
         const u64 q = pc.q;
         const u64 ql = pc_last->q, ql_half = ql >> 1;
-        u64 v = scratch[zb.aux[z] + x];                              // last limb coefficient, [0, q_l)
+        u64 v = scratch[zb.aux.at(z) + x];                           // last limb coefficient, [0, q_l)
         u64 vm = csub(mul_shoup_lazy(v, 1, pc.one_sh, q), q);         // v mod q_i
         u64 qlm = csub(mul_shoup_lazy(ql, 1, pc.one_sh, q), q);       // q_l mod q_i
         u64 val = (v > ql_half) ? sub_mod(vm, qlm, q) : vm;           // rescale.cpp:50 tie rule
@@ -167,9 +166,9 @@ struct RescaleStore {
     __device__ __forceinline__ void operator()(const LimbJob& j, const ZBases& zb, uint32_t z, uint32_t x, u64 v,
                                                const PrimeConst& pc) const {
         const u64 q = pc.q;
-        u64 a = arena[zb.src[z] + j.src + x];
+        u64 a = arena[zb.src.at(z) + j.src + x];
         u64 s = mul_shoup(a, __ldg(qlinv + j.aux), __ldg(qlinv_sh + j.aux), q);
-        arena[zb.out[z] + j.out + x] = add_mod(s, v, q);
+        arena[zb.out.at(z) + j.out + x] = add_mod(s, v, q);
     }
 };
 
@@ -181,21 +180,18 @@ cudaError_t launch_rescale(int log_n, const OpTabs& t, const LimbJob* jobs_q, ui
     if (sizeQl < 2 || nz == 0) return cudaSuccess;
     const u64 n = 1ull << log_n;
     const uint32_t last = sizeQl - 1;
-    // step 1: INTT(last limb). jobs_q[last] has src = dst = out = last * N.
+    // step 1: INTT(last limb). jobs_q[last] has src = dst = out = last * N,
+    // so shifting mid / out back by last * N lands it at scratch + mid(z).
     ZBases z1 = zb_in;
-    for (uint32_t z = 0; z < nz; ++z) {
-        z1.mid[z] = zb_in.mid[z] - (u64)last * n;   // lands at scratch + mid[z]
-        z1.out[z] = zb_in.mid[z] - (u64)last * n;
-    }
+    z1.mid = zf_plus(zb_in.mid, (u64)0 - (u64)last * n);
+    z1.out = z1.mid;
     cudaError_t e = launch_ntt<true>(log_n, t.pt, jobs_q + last, 1, nz, scratch, z1, LoadPlain{arena},
                                      StorePlain{scratch}, st);
     if (e != cudaSuccess) return e;
     // step 2
     ZBases z2 = zb_in;
-    for (uint32_t z = 0; z < nz; ++z) {
-        z2.aux[z] = zb_in.mid[z];            // coefficients of the last limb
-        z2.mid[z] = zb_in.mid[z] + n;        // intermediates
-    }
+    z2.aux = zb_in.mid;                      // coefficients of the last limb
+    z2.mid = zf_plus(zb_in.mid, n);          // intermediates
     RescaleLoad pro{scratch, t.qlql, t.qlql_sh, t.pt.pc + last};
     RescaleStore epi{arena, t.qlinv, t.qlinv_sh};
     return launch_ntt<false>(log_n, t.pt, jobs_q, last, nz, scratch, z2, pro, epi, st);
@@ -224,7 +220,7 @@ struct LoadGather {
     const uint32_t* map;
     __device__ __forceinline__ u64 operator()(const LimbJob& j, const ZBases& zb, uint32_t z, uint32_t x,
                                               const PrimeConst&) const {
-        return base[zb.src[z] + j.src + __ldg(map + x)];
+        return base[zb.src.at(z) + j.src + __ldg(map + x)];
     }
 };
 
@@ -250,7 +246,7 @@ struct ModUpLoad {
         for (uint32_t i = 0; i < size; ++i) {
             const uint32_t limb = start + i;
             const u64 qq = t.pt.pc[limb].q;
-            u64 xv = scratch[zb.aux[z] + (u64)limb * n + x];
+            u64 xv = scratch[zb.aux.at(z) + (u64)limb * n + x];
             u64 y = mul_shoup(xv, __ldg(qi + i), __ldg(qish + i), qq);           // [x * qHatInv]_{q_i}
             u64 w = mul_shoup_lazy(y, __ldg(qm + i * row + k), __ldg(qmsh + i * row + k), p);
             s += w;
@@ -264,7 +260,7 @@ struct StoreSlot {   // plain store into scratch
     u64* scratch;
     __device__ __forceinline__ void operator()(const LimbJob& j, const ZBases& zb, uint32_t z, uint32_t x, u64 v,
                                                const PrimeConst&) const {
-        scratch[zb.out[z] + j.out + x] = v;
+        scratch[zb.out.at(z) + j.out + x] = v;
     }
 };
 
@@ -275,8 +271,7 @@ __global__ void __launch_bounds__(256) ks_mac_kernel(OpTabs t, uint32_t n, uint3
                                                      uint32_t key_stride, uint32_t key_pbase,
                                                      const u64* __restrict__ arena, u64* __restrict__ scratch,
                                                      u64 modup_off, u64 ext0_off, u64 ext1_off, u64 t0_off,
-                                                     const __grid_constant__ ZBases zb,
-                                                     const __grid_constant__ KsFuse f) {
+                                                     const ZBases zb, const KsFuse f) {
     const uint32_t sidx = blockIdx.y;   // 0..sizeQl+K-1
     const uint32_t z = blockIdx.z;
     const bool isq = sidx < sizeQl;
@@ -286,12 +281,13 @@ __global__ void __launch_bounds__(256) ks_mac_kernel(OpTabs t, uint32_t n, uint3
     const PrimeConst pc = t.pt.pc[prime];
     const ModConst mc = modconst_of(pc);
     const u64 S = (u64)slots_q + K;
-    const u64 base_scr = zb.mid[z];
-    const u64* in = arena + zb.src[z] + (u64)sidx * n;   // only valid for Q limbs
+    const u64 base_scr = zb.mid.at(z);
+    const u64* in = arena + zb.src.at(z) + (u64)sidx * n;   // only valid for Q limbs
+    const u64 c0_off = f.has_c0 ? f.c0.at(z) : 0;
     for (uint32_t x = blockIdx.x * blockDim.x + threadIdx.x; x < n; x += gridDim.x * blockDim.x) {
         const uint32_t xs = f.map ? __ldg(f.map + x) : x;     // position read through the automorphism
         if (isq && f.has_c0)
-            scratch[base_scr + t0_off + (u64)sidx * n + x] = arena[f.c0[z] + (u64)sidx * n + xs];
+            scratch[base_scr + t0_off + (u64)sidx * n + x] = arena[c0_off + (u64)sidx * n + xs];
         Acc128 ab, aa;
         acc_init(ab);
         acc_init(aa);
@@ -322,7 +318,7 @@ struct ModDownLoad {
         u64 s = 0;
         for (uint32_t k = 0; k < K; ++k) {
             const PrimeConst& pk = t.pt.pc[t.p_base + k];
-            u64 xv = scratch[zb.aux[z] + (u64)(slots_q + k) * n + x];
+            u64 xv = scratch[zb.aux.at(z) + (u64)(slots_q + k) * n + x];
             u64 y = mul_shoup(xv, __ldg(t.phat_inv_modp + k), __ldg(t.phat_inv_modp_sh + k), pk.q);
             u64 w = mul_shoup_lazy(y, __ldg(t.phat_modq + k * t.sizeQl + i), __ldg(t.phat_modq_sh + k * t.sizeQl + i), q);
             s += w;
@@ -335,25 +331,26 @@ struct ModDownLoad {
 // ModDown combine as the NTT epilogue: out = (x_Q - y) * P^-1 mod q_i.
 // z' = 2z + h: h = 0 writes ks0 (+ gathered c0, + acc0), h = 1 writes ks1 (+ acc1).
 struct ModDownStore {
-    const u64* scratch;  // ext region at zb.src[z]
-    u64* arena;          // output at zb.out[z]
+    const u64* scratch;  // ext region at zb.src(z)
+    u64* arena;          // outputs
     OpTabs t;
     uint32_t n;
     int has_c0, has_acc;
-    u64 t0base[ZMAX / 2];   // scratch offset of the gathered c0 per ciphertext
-    u64 acc0[ZMAX / 2], acc1[ZMAX / 2];
+    ZField t0;           // scratch offset of the gathered c0, per ciphertext
+    ZField out0, out1;   // ks0 / ks1 destinations, per ciphertext
+    ZField acc0, acc1;
     __device__ __forceinline__ void operator()(const LimbJob& j, const ZBases& zb, uint32_t z, uint32_t x, u64 v,
                                                const PrimeConst& pc) const {
         const u64 q = pc.q;
         const uint32_t i = j.aux;
         const uint32_t h = z & 1u, zc = z >> 1;
         const u64 li = (u64)i * n + x;
-        u64 xq = scratch[zb.src[z] + li];
+        u64 xq = scratch[zb.src.at(z) + li];
         u64 d = sub_mod(xq, v, q);
         u64 r = mul_shoup(d, __ldg(t.p_inv_mod_q + i), __ldg(t.p_inv_mod_q_sh + i), q);
-        if (h == 0 && has_c0) r = add_mod(r, scratch[t0base[zc] + li], q);
-        if (has_acc) r = add_mod(r, arena[(h ? acc1[zc] : acc0[zc]) + li], q);
-        arena[zb.out[z] + li] = r;
+        if (h == 0 && has_c0) r = add_mod(r, scratch[t0.at(zc) + li], q);
+        if (has_acc) r = add_mod(r, arena[(h ? acc1.at(zc) : acc0.at(zc)) + li], q);
+        arena[(h ? out1.at(zc) : out0.at(zc)) + li] = r;
     }
 };
 
@@ -362,7 +359,7 @@ cudaError_t launch_key_switch(int log_n, const OpTabs& t, const LimbJob* jobs_qp
                               u64 evk_a, u64 evk_b, uint32_t key_stride, uint32_t key_pbase, u64* arena,
                               u64* scratch, uint32_t nz, const ZBases& zb, cudaStream_t st, const KsFuse* fuse) {
     if (nz == 0) return cudaSuccess;
-    if (2 * nz > (uint32_t)ZMAX) return cudaErrorInvalidValue;
+    if (2ull * nz > 65535ull) return cudaErrorInvalidValue;
     KsFuse f{};
     if (fuse) f = *fuse;
     const u64 n = 1ull << log_n;
@@ -378,7 +375,8 @@ cudaError_t launch_key_switch(int log_n, const OpTabs& t, const LimbJob* jobs_qp
     // 1. INTT of the input's Q limbs -> coef (slot i at coef + i*N)
     {
         ZBases a = zb;
-        for (uint32_t z = 0; z < nz; ++z) { a.mid[z] = zb.mid[z] + off_coef; a.out[z] = zb.mid[z] + off_coef; }
+        a.mid = zf_plus(zb.mid, off_coef);
+        a.out = a.mid;
         if (f.map)
             e = launch_ntt<true>(log_n, t.pt, jobs_qp, sizeQl, nz, scratch, a, LoadGather{arena, f.map},
                                  StorePlain{scratch}, st);
@@ -389,11 +387,9 @@ cudaError_t launch_key_switch(int log_n, const OpTabs& t, const LimbJob* jobs_qp
     // 2. ModUp: base conversion + NTT for every (digit, complementary limb)
     {
         ZBases a = zb;
-        for (uint32_t z = 0; z < nz; ++z) {
-            a.aux[z] = zb.mid[z] + off_coef;
-            a.mid[z] = zb.mid[z] + off_modup;
-            a.out[z] = zb.mid[z] + off_modup;
-        }
+        a.aux = zf_plus(zb.mid, off_coef);
+        a.mid = zf_plus(zb.mid, off_modup);
+        a.out = a.mid;
         ModUpLoad pro{scratch, t, K, (uint32_t)n};
         e = launch_ntt<false>(log_n, t.pt, jobs_modup, n_modup, nz, scratch, a, pro, StoreSlot{scratch}, st);
         if (e != cudaSuccess) return e;
@@ -410,32 +406,17 @@ cudaError_t launch_key_switch(int log_n, const OpTabs& t, const LimbJob* jobs_qp
     // 4. ModDown of both accumulators: z' = 2z (ext0 -> ks0), 2z + 1 (ext1 -> ks1)
     {
         ZBases a{};
-        for (uint32_t z = 0; z < nz; ++z) {
-            for (uint32_t h = 0; h < 2; ++h) {
-                uint32_t zz = 2 * z + h;
-                u64 ext = zb.mid[z] + (h ? off_ext1 : off_ext0);
-                a.src[zz] = ext;
-                a.aux[zz] = ext;
-                a.mid[zz] = ext;
-                a.out[zz] = ext;
-            }
-        }
+        a.src = zf_pair(zf_plus(zb.mid, off_ext0), off_ext1 - off_ext0);
+        a.aux = a.src;
+        a.mid = a.src;
+        a.out = a.src;
         // 4a. INTT of the special limbs, in place
         e = launch_ntt<true>(log_n, t.pt, jobs_qp + slots_q, K, 2 * nz, scratch, a, LoadPlain{scratch},
                              StorePlain{scratch}, st);
         if (e != cudaSuccess) return e;
         // 4b. NTT over Q limbs with base-conversion prologue and ModDown epilogue
-        ZBases b{};
-        for (uint32_t z = 0; z < nz; ++z) {
-            for (uint32_t h = 0; h < 2; ++h) {
-                uint32_t zz = 2 * z + h;
-                u64 ext = zb.mid[z] + (h ? off_ext1 : off_ext0);
-                b.src[zz] = ext;
-                b.aux[zz] = ext;
-                b.mid[zz] = zb.mid[z] + off_mid + (u64)h * slots_q * n;
-                b.out[zz] = h ? zb.aux[z] : zb.out[z];
-            }
-        }
+        ZBases b = a;
+        b.mid = zf_pair(zf_plus(zb.mid, off_mid), (u64)slots_q * n);
         ModDownLoad pro{scratch, t, slots_q, K, (uint32_t)n};
         ModDownStore epi{};
         epi.scratch = scratch;
@@ -444,11 +425,11 @@ cudaError_t launch_key_switch(int log_n, const OpTabs& t, const LimbJob* jobs_qp
         epi.n = (uint32_t)n;
         epi.has_c0 = f.has_c0;
         epi.has_acc = f.has_acc;
-        for (uint32_t z = 0; z < nz; ++z) {
-            epi.t0base[z] = zb.mid[z] + off_t0;
-            epi.acc0[z] = f.acc0[z];
-            epi.acc1[z] = f.acc1[z];
-        }
+        epi.t0 = zf_plus(zb.mid, off_t0);
+        epi.out0 = zb.out;
+        epi.out1 = zb.aux;
+        epi.acc0 = f.acc0;
+        epi.acc1 = f.acc1;
         e = launch_ntt<false>(log_n, t.pt, jobs_qp, sizeQl, 2 * nz, scratch, b, pro, epi, st);
         if (e != cudaSuccess) return e;
     }

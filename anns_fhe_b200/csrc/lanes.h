@@ -23,8 +23,8 @@ u64 host_shoup(u64 w, u64 q);
     } while (0)
 
 // Scratch lane b owns [b * lane_words, (b + 1) * lane_words) of ctx->scr. A
-// batched composite operator gives ciphertext b of a launch lane b.
-constexpr uint32_t kLanes = 64;
+// batched composite operator gives ciphertext b of a launch lane b; a context
+// has ctx->lanes lanes (afhe_params.max_batch).
 constexpr uint32_t kTempPolys = 6;  // d0, d1, d2, ks0, ks1, t (each (L + K) * N words)
 
 struct Lane {
@@ -49,5 +49,16 @@ inline Lane lane_of(const afhe_ctx* c, uint32_t b) {
 inline u64 lane_temp(const afhe_ctx* c, uint32_t b, uint32_t t) {
     return c->prm.poly_words + lane_of(c, b).temp + (u64)t * (c->L + c->K) * c->n;
 }
+// the same for lanes 0, 1, 2, ... as a strided field
+inline ZField lane_temp_field(const afhe_ctx* c, uint32_t t) {
+    return zf_stride(lane_temp(c, 0, t), lane_words(c));
+}
+inline ZField lane_field(const afhe_ctx* c, u64 Lane::*member) {
+    return zf_stride(lane_of(c, 0).*member, lane_words(c));
+}
+
+// Field for per-ciphertext offsets vals[0..n): strided when they form an
+// arithmetic progression, else staged through the context's descriptor ring.
+int zf_from(afhe_ctx* ctx, const u64* vals, uint32_t n, ZField* out);
 
 }  // namespace afhe

@@ -69,10 +69,10 @@ extern "C" int afhe_key_switch_noalloc(afhe_ctx* ctx, uint64_t* io, uint64_t evk
     if (rc != AFHE_OK) return rc;
     const u64 w = (u64)limbs * ctx->n;
     ZBases zb{};
-    zb.src[0] = 0;        // input at io[0, w)
-    zb.out[0] = w;        // ks0 at io[w, 2w)
-    zb.aux[0] = 2 * w;    // ks1 at io[2w, 3w)
-    zb.mid[0] = 0;        // scratch from the start of the fixed array
+    zb.src = zf_const(0);        // input at io[0, w)
+    zb.out = zf_const(w);        // ks0 at io[w, 2w)
+    zb.aux = zf_const(2 * w);    // ks1 at io[2w, 3w)
+    zb.mid = zf_const(0);        // scratch from the start of the fixed array
     const u64 S = (u64)ctx->L + ctx->K;
     const LevelJobs& lj = ctx->lvjobs[limbs];
     e = launch_key_switch(ctx->log_n, ctx->lv[limbs], ctx->jobs_qp, lj.modup, lj.n_modup, ctx->L, limbs, ctx->K,

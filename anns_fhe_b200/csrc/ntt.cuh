@@ -71,16 +71,32 @@ struct NttGeom {
     int last;     // pass writes through the epilogue
 };
 
-constexpr int ZMAX = 128;  // polynomials per launch (blockIdx.z)
+// Word offset of one operand for polynomial z of a batched launch:
+//   (arr ? arr[z >> shift] : base + (z >> shift) * stride) + add + (z & low) * hdelta,
+// low = 2^shift - 1. A regular batch (operands at a fixed stride) needs no
+// memory; an irregular one reads a small device array. shift = 1 describes the
+// two polynomials (c0, c1) of ciphertext z >> 1 that differ by hdelta.
+struct ZField {
+    const u64* arr;
+    u64 base, stride, add, hdelta;
+    uint32_t shift;
+    AFHE_HD u64 at(uint32_t z) const {
+        const uint32_t zz = z >> shift;
+        const u64 v = arr ? arr[zz] : base + (u64)zz * stride;
+        return v + add + (u64)(z & ((1u << shift) - 1u)) * hdelta;
+    }
+};
 
-// Per-z word offsets of the operands of one launch (kernel parameter). The
-// meaning of src / out / aux is the prologue's and epilogue's; mid is where a
-// limb lives between the passes of a two-pass transform (in the `mid` arena).
+inline ZField zf_const(u64 v) { ZField f{}; f.base = v; return f; }
+inline ZField zf_stride(u64 base, u64 stride) { ZField f{}; f.base = base; f.stride = stride; return f; }
+inline ZField zf_plus(ZField f, u64 add) { f.add += add; return f; }
+inline ZField zf_pair(ZField f, u64 hdelta) { f.shift = 1; f.hdelta = hdelta; return f; }
+
+// The operands of one batched launch: meaning of src / out / aux is the
+// prologue's and epilogue's; mid is where a limb lives between the passes of
+// a two-pass transform (in the `mid` arena).
 struct ZBases {
-    u64 src[ZMAX];
-    u64 mid[ZMAX];
-    u64 out[ZMAX];
-    u64 aux[ZMAX];
+    ZField src, mid, out, aux;
 };
 
 // Plain prologue / epilogue.
@@ -88,14 +104,14 @@ struct LoadPlain {
     const u64* base;
     __device__ __forceinline__ u64 operator()(const LimbJob& j, const ZBases& zb, uint32_t z, uint32_t x,
                                               const PrimeConst&) const {
-        return base[zb.src[z] + j.src + x];
+        return base[zb.src.at(z) + j.src + x];
     }
 };
 struct StorePlain {
     u64* base;
     __device__ __forceinline__ void operator()(const LimbJob& j, const ZBases& zb, uint32_t z, uint32_t x, u64 v,
                                                const PrimeConst&) const {
-        base[zb.out[z] + j.out + x] = v;
+        base[zb.out.at(z) + j.out + x] = v;
     }
 };
 
@@ -225,14 +241,14 @@ __device__ __forceinline__ void ntt_rounds(u64* sm, const ulonglong2* tw, const 
 template <bool INV, int P, int LOGC, bool COL, class Pro, class Epi>
 __global__ void __launch_bounds__((1u << (P + LOGC)) / 8)
 ntt_kernel(NttGeom g, PrimeTables pt, const LimbJob* __restrict__ jobs, u64* __restrict__ mid,
-           const __grid_constant__ ZBases zb, Pro pro, Epi epi) {
+           const ZBases zb, Pro pro, Epi epi) {
     extern __shared__ u64 sm[];
     constexpr uint32_t C = 1u << LOGC;
     constexpr uint32_t TILE = 1u << (P + LOGC);
     constexpr uint32_t T = TILE / 8;
     const LimbJob job = jobs[blockIdx.y];
     const uint32_t z = blockIdx.z;
-    const u64 zm = zb.mid[z];
+    const u64 zm = zb.mid.at(z);
     const PrimeConst pc = pt.pc[job.prime];
     const uint32_t n = 1u << g.log_n;
     const ulonglong2* __restrict__ tw = (INV ? pt.itw2 : pt.tw2) + (u64)job.prime * n;

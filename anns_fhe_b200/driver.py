@@ -154,7 +154,7 @@ class CkksParams:
 class FheContext:
     """Device context: arenas, tables, key directory (one CUDA stream)."""
 
-    def __init__(self, params: CkksParams, poly_words: int, key_words: int, device: int = 0):
+    def __init__(self, params: CkksParams, poly_words: int, key_words: int, device: int = 0, max_batch: int = 0):
         self.lib = L.load()
         self.params = params
         pr = L.Params()
@@ -164,6 +164,8 @@ class FheContext:
         for i, x in enumerate(params.p):
             pr.p[i] = x
         pr.poly_words, pr.key_words, pr.device = poly_words, key_words, device
+        pr.max_batch = max_batch
+        self.max_batch = max_batch or 64
         h = L.CTX()
         check(self.lib.afhe_ctx_create(C.byref(pr), C.byref(h)), "afhe_ctx_create")
         self.h = h

@@ -13,7 +13,7 @@ with the semantics fixed by integration_tools/generate_interactive_test_vectors.
   stage 4  (client)  decrypt, sort, top-k
 
 Every operator call processes a whole batch of independent ciphertexts (up to
-64 per launch; one lane of context scratch each): several queries in stage 1,
+the context's max_batch per launch; one lane of context scratch each): several queries in stage 1,
 several (query, list, batch) items in stage 3. Each ciphertext's residues are
 the ones the one-at-a-time chain produces. `lanes=1` is the plain path.
 
@@ -31,7 +31,7 @@ from .ckks import Encoder, Slots, encode_plaintext
 from .driver import FheContext, FHEHostDriver
 from .ivfpq import IvfPqIndex
 
-MAX_LANES = 64
+MAX_LANES = 4096
 
 
 @dataclass
@@ -77,7 +77,7 @@ class InteractiveQueryManager:
         self.L = self.p.L
         self.enc = Encoder(self.p.log_n)
         self.slots = slots
-        self.lanes = max(1, min(lanes, MAX_LANES))
+        self.lanes = max(1, min(lanes, MAX_LANES, ctx.max_batch))
         assert shape.n_list * shape.D <= shape.slots, "centroids do not fit one ciphertext"
         L, n = self.L, self.p.n
         self.lvl_sq = L - 1          # after the first rescale

@@ -66,7 +66,8 @@ class Workload:
         n_batches = sum(-(-len(v) // B) for v in self.index.lists)
         n_slots = 16 + 1 + spec.n_list + 2 * n_batches + 8 * lanes + 8 * max_queries + 64 + max_queries
         self.ctx = FheContext(self.params, poly_words=n_slots * slot_w,
-                              key_words=(2 + 2 * (spec.log_n + 1)) * self.params.key_words() + 4096, device=device)
+                              key_words=(2 + 2 * (spec.log_n + 1)) * self.params.key_words() + 4096, device=device,
+                              max_batch=lanes)
         self.slots = Slots(self.params, 0, n_slots * slot_w)
         self.client = CkksClient(self.ctx, self.slots, seed=spec.seed + 7)
         self.iqm = InteractiveQueryManager(self.ctx, self.index, shape, self.slots, lanes=lanes)

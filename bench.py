@@ -247,8 +247,8 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--batch", type=int, default=64, help="queries per step")
-    ap.add_argument("--lanes", type=int, default=64)
+    ap.add_argument("--batch", type=int, default=256, help="queries per step")
+    ap.add_argument("--lanes", type=int, default=256)
     ap.add_argument("--skip-cpu", action="store_true", help="omit the cpu_baseline leg")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -66,6 +66,8 @@ typedef struct afhe_params {
     uint64_t poly_words;       /* poly_gmem size in 64-bit words */
     uint64_t key_words;        /* key_gmem size in 64-bit words */
     int32_t device;            /* CUDA device ordinal */
+    uint32_t max_batch;        /* ciphertexts per batched launch (context scratch lanes);
+                                  0 selects 64 */
 } afhe_params;
 
 /* Scalar and array registers of fhe_accel_top (fhe_accel_top.h:8-55), with
