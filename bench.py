@@ -64,6 +64,7 @@ def run_ours(args, rank: int, world: int):
     import torch
 
     from anns_fhe_b200._lib import P64
+    from anns_fhe_b200.replicas import aggregate, query_seed
     from anns_fhe_b200.workloads import Workload
 
     dev = int(os.environ.get("LOCAL_RANK", 0))
@@ -72,7 +73,7 @@ def run_ours(args, rank: int, world: int):
     stream = torch.cuda.ExternalStream(wl.ctx.lib.afhe_stream(wl.ctx.h), device=dev)
     iqm = wl.iqm
     recs = wl.records[:args.batch]
-    Q = wl.queries(args.batch, seed=1000 + rank)
+    Q = wl.queries(args.batch, seed=query_seed(1000, rank))
     # client work done once: encrypted queries on the host (pinned) for e2e
     wl.encrypt_queries(Q, recs)
     n = wl.params.n
@@ -145,11 +146,9 @@ def run_ours(args, rank: int, world: int):
         e2e_step()
     e2e = [e2e_step() for _ in range(args.steps)]
     e2e_ms = sum(x[0] for x in e2e)
-    if dist:
-        t = torch.tensor([total_ms, e2e_ms], device=f"cuda:{dev}")
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms, e2e_ms = float(t[0]), float(t[1])
-    queries = args.batch * args.steps * world
+    # replicas: all ranks' queries over the slowest rank's time
+    total_ms, queries = aggregate(total_ms, args.batch * args.steps)
+    e2e_ms, _ = aggregate(e2e_ms, args.batch * args.steps)
     line = {
         "metric": "encrypted IVF-PQ queries/s (batched server, interactive protocol)",
         "value": queries / (total_ms / 1e3),
@@ -236,9 +235,68 @@ def ntt_roofline(wl, stream, lanes):
             "algorithmic_bytes_per_launch": bytes_per_launch}
 
 
+def profile_step(nq: int):
+    """Profiling driver: one warm step, then one measured step of `nq` queries.
+    Prints the kernel-launch counts an ncu launch list needs (-s / -c)."""
+    import numpy as np  # noqa: F401
+
+    from anns_fhe_b200.workloads import Workload
+    wl = Workload(max_queries=nq, lanes=nq)
+    lib = wl.ctx.lib
+    recs = wl.records[:nq]
+    wl.encrypt_queries(wl.queries(nq, seed=7), recs)
+
+    def step():
+        wl.iqm.stage1_coarse(recs)
+        wl.select(recs)
+        wl.iqm.stage3_fine(recs)
+        wl.ctx.sync()
+    step()
+    a = lib.afhe_kernel_launches()
+    t = time.time()
+    step()
+    print(f"WARM_LAUNCHES={a} STEP_LAUNCHES={lib.afhe_kernel_launches() - a} step_s={time.time() - t:.3f}")
+    wl.close()
+
+
+def profile_ntt(polys: int, log_n: int = 13, reps: int = 10):
+    """Profiling driver: batched in-place NTT / INTT over `polys` polynomials of
+    4 limbs (the key switch's shape), forward then inverse, `reps` each."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from anns_fhe_b200._lib import P64
+    from anns_fhe_b200.driver import CkksParams, FheContext
+    prm = CkksParams.generate(log_n, 3, 50, 1, 60, 1)
+    n, limbs = prm.n, 4
+    ctx = FheContext(prm, poly_words=polys * limbs * n, key_words=1024)
+    rng = np.random.default_rng(1)
+    limb_data = np.concatenate([rng.integers(0, q, n, dtype=np.uint64) for q in prm.q + prm.p])
+    for b in range(polys):
+        ctx.write_poly(b * limbs * n, limb_data)
+    offs = (C.c_uint64 * polys)(*[b * limbs * n for b in range(polys)])
+    lib = ctx.lib
+    st = torch.cuda.ExternalStream(lib.afhe_stream(ctx.h))
+    for inv in (0, 1):
+        lib.afhe_ntt_batch(ctx.h, C.cast(offs, P64), polys, limbs, inv)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(reps):
+            lib.afhe_ntt_batch(ctx.h, C.cast(offs, P64), polys, limbs, inv)
+        e1.record(st)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        gb = 2 * polys * limbs * n * 8 / 1e9
+        print(f"log_n={log_n} inverse={inv} {polys}x{limbs} limbs: {ms * 1e3:.1f} us per launch, {gb / (ms * 1e-3):.0f} GB/s")
+    ctx.close()
+
+
 def run_reference(args, rank: int, world: int):
     from oracle.chain import cpu_reference_rate
-    return cpu_reference_rate(steps=args.steps, warmup=args.warmup)
+    # one untimed query per worker at most: each takes seconds on a core
+    return cpu_reference_rate(steps=args.steps, warmup=min(args.warmup, 1), n_gpus=args.gpus)
 
 
 def main():
@@ -250,7 +308,14 @@ def main():
     ap.add_argument("--batch", type=int, default=256, help="queries per step")
     ap.add_argument("--lanes", type=int, default=256)
     ap.add_argument("--skip-cpu", action="store_true", help="omit the cpu_baseline leg")
+    ap.add_argument("--profile-step", type=int, default=0, help="profiling driver: queries per step")
+    ap.add_argument("--profile-ntt", type=int, default=0, help="profiling driver: polynomials per NTT launch")
+    ap.add_argument("--log-n", type=int, default=13, help="ring degree for --profile-ntt")
     args = ap.parse_args()
+    if args.profile_step:
+        return profile_step(args.profile_step)
+    if args.profile_ntt:
+        return profile_ntt(args.profile_ntt, args.log_n)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if args.impl == "reference":

@@ -119,13 +119,17 @@ def one_query(st, counts) -> float:
 
 
 def _worker(args):
-    seed, counts, nq = args
+    seed, counts, nq, warm = args
     st = _setup(seed)
+    for _ in range(warm):
+        one_query(st, counts)
     return [one_query(st, counts) for _ in range(nq)]
 
 
-def cpu_reference_rate(steps: int = 1, warmup: int = 0, workers: int | None = None, queries_per_worker: int = 1):
-    """Queries/s of the chain on all host cores: `steps` rounds of one query per worker."""
+def cpu_reference_rate(steps: int = 1, warmup: int = 0, workers: int | None = None, queries_per_worker: int = 1,
+                       n_gpus: int = 0):
+    """Queries/s of the chain on all host cores: `warmup` untimed, then `steps`
+    timed rounds of one query per worker process."""
     spec = _config()
     B = (1 << spec.log_n) // 2 // spec.d
     counts = _items(spec, B)
@@ -133,7 +137,7 @@ def cpu_reference_rate(steps: int = 1, warmup: int = 0, workers: int | None = No
     ctx = mp.get_context("spawn")
     with ctx.Pool(workers) as pool:
         t0 = time.perf_counter()
-        per = pool.map(_worker, [(11 + w, counts, queries_per_worker * max(1, steps)) for w in range(workers)])
+        per = pool.map(_worker, [(11 + w, counts, queries_per_worker * max(1, steps), warmup) for w in range(workers)])
         wall = time.perf_counter() - t0
     per_query = [x for p in per for x in p]
     done = len(per_query)
@@ -146,7 +150,7 @@ def cpu_reference_rate(steps: int = 1, warmup: int = 0, workers: int | None = No
         "metric": "encrypted IVF-PQ queries/s (batched server, interactive protocol)",
         "value": rate,
         "unit": "queries/s",
-        "n_gpus": 0,
+        "n_gpus": n_gpus,
         "steps": steps,
         "warmup": warmup,
         "ms_per_step": chain_s * 1e3,
