@@ -4,6 +4,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -361,6 +362,10 @@ int afhe_ctx_create(const afhe_params* prm, afhe_ctx** out) {
         // kernel can address both from one base: scratch word w is poly word
         // poly_words + w.
         ctx->lanes = prm->max_batch ? prm->max_batch : 64;
+        {
+            const char* v = std::getenv("AFHE_KS_FUSED");
+            ctx->ks_fused = key_switch_fused_supported(ctx->log_n) && !(v && v[0] == '0');
+        }
         if (ctx->lanes > 4096) { rc = fail(ctx, AFHE_E_ARG, "max_batch must be <= 4096"); break; }
         ctx->scr_words = (size_t)ctx->lanes * lane_words(ctx);
         e = dalloc(&ctx->poly, prm->poly_words + ctx->scr_words);

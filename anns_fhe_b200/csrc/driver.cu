@@ -14,6 +14,7 @@
 // else a small array staged through the context's descriptor ring).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdlib>
 #include <vector>
 
@@ -65,8 +66,10 @@ int check_cts(afhe_ctx* ctx, const afhe_ct_ref* v, uint32_t count, uint32_t limb
 
 // Key switch nz polynomials (poly_gmem-relative offsets) with one key, with
 // optional fusion (automorphism gather, c0 add, accumulate; see KsFuse).
+// `fused_ok` is false when an entry's outputs may overlap another entry's
+// inputs, which the one-kernel key switch cannot order.
 int ks_batch(afhe_ctx* ctx, const ZField& in, const ZField& out0, const ZField& out1, uint32_t nz, u64 evk,
-             uint32_t limbs, const KsFuse* fuse = nullptr) {
+             uint32_t limbs, const KsFuse* fuse = nullptr, bool fused_ok = true) {
     const u64 n = ctx->n, S = (u64)ctx->L + ctx->K;
     const OpTabs& t = ctx->lv[limbs];
     const LevelJobs& lj = ctx->lvjobs[limbs];
@@ -75,6 +78,11 @@ int ks_batch(afhe_ctx* ctx, const ZField& in, const ZField& out0, const ZField& 
     zb.out = out0;
     zb.aux = out1;
     zb.mid = lane_field(ctx, &Lane::ks);
+    if (ctx->ks_fused && fused_ok) {
+        CK(launch_key_switch_fused(ctx->log_n, t, limbs, ctx->K, ctx->key, evk, evk + (u64)ctx->dnum * S * n,
+                                   (uint32_t)S, ctx->L, ctx->poly, ctx->scr, nz, zb, ctx->st, fuse));
+        return AFHE_OK;
+    }
     CK(launch_key_switch(ctx->log_n, t, ctx->jobs_qp, lj.modup, lj.n_modup, ctx->L, limbs, ctx->K, ctx->key, evk,
                          evk + (u64)ctx->dnum * S * n, (uint32_t)S, ctx->L, ctx->poly, ctx->scr, nz, zb, ctx->st,
                          fuse));
@@ -157,7 +165,7 @@ int mult_relin_rescale_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const afhe_ct_
 // Inputs may alias outputs; acc may alias dst.
 int rotate_step_batch(afhe_ctx* ctx, const ZField& in0, const ZField& in1, const ZField& d0, const ZField& d1,
                       uint32_t nz, int32_t step, uint32_t limbs, const ZField* acc0 = nullptr,
-                      const ZField* acc1 = nullptr) {
+                      const ZField* acc1 = nullptr, bool fused_ok = true) {
     auto it = ctx->rot.find(step);
     if (it == ctx->rot.end()) return fail(ctx, AFHE_E_NOKEY, "rotation key not found for step " + std::to_string(step));
     const RotKey& rk = it->second;
@@ -167,7 +175,32 @@ int rotate_step_batch(afhe_ctx* ctx, const ZField& in0, const ZField& in1, const
     f.c0 = in0;
     f.has_acc = acc0 != nullptr;
     if (acc0) { f.acc0 = *acc0; f.acc1 = *acc1; }
-    return ks_batch(ctx, in1, d0, d1, nz, rk.evk_offset, limbs, &f);
+    return ks_batch(ctx, in1, d0, d1, nz, rk.evk_offset, limbs, &f, fused_ok);
+}
+
+// Whether the one-kernel key switch may run a rotation batch: its entries run
+// concurrently and each reads input limb i up to the point where it writes
+// output limb i, so every input polynomial must either be disjoint from every
+// output polynomial or coincide exactly with an output of its own entry (all
+// polynomials span w words).
+bool fused_rotation_safe(const Offs& i0, const Offs& i1, const Offs& o0, const Offs& o1, u64 w) {
+    const size_t nz = i0.size();
+    std::vector<std::pair<u64, uint32_t>> outs;
+    outs.reserve(2 * nz);
+    for (uint32_t z = 0; z < nz; ++z) {
+        outs.emplace_back(o0[z], z);
+        outs.emplace_back(o1[z], z);
+    }
+    std::sort(outs.begin(), outs.end());
+    for (uint32_t z = 0; z < nz; ++z)
+        for (u64 a : {i0[z], i1[z]}) {
+            // outputs starting in (a - w, a + w) overlap [a, a + w)
+            const u64 lo = a >= w ? a - w + 1 : 0;
+            auto it = std::lower_bound(outs.begin(), outs.end(), std::make_pair(lo, 0u));
+            for (; it != outs.end() && it->first < a + w; ++it)
+                if (it->second != z || it->first != a) return false;
+        }
+    return true;
 }
 
 // eval_rotate on nz ciphertexts by the same amount (fhe_host_driver.cpp:361-404):
@@ -207,6 +240,7 @@ int rotate_batch(afhe_ctx* ctx, const afhe_ct_ref* in, const afhe_ct_ref* dst, u
     }
     for (int32_t s : steps)
         if (!ctx->rot.count(s)) return fail(ctx, AFHE_E_NOKEY, "rotation key not found for step " + std::to_string(s));
+    const bool fused_ok = fused_rotation_safe(i0, i1, o0, o1, (u64)limbs * ctx->n);
     ZField fi0, fi1, fo0, fo1;
     ZF(fi0, i0); ZF(fi1, i1); ZF(fo0, o0); ZF(fo1, o1);
     // chain temporaries (lane temps 2 and 5 are unused by a single step)
@@ -216,8 +250,9 @@ int rotate_batch(afhe_ctx* ctx, const afhe_ct_ref* in, const afhe_ct_ref* dst, u
         const bool last = k + 1 == steps.size();
         const ZField& n0 = last ? fo0 : x0;
         const ZField& n1 = last ? fo1 : x1;
-        int rc = (last && accumulate) ? rotate_step_batch(ctx, c0, c1, n0, n1, nz, steps[k], limbs, &fo0, &fo1)
-                                      : rotate_step_batch(ctx, c0, c1, n0, n1, nz, steps[k], limbs);
+        int rc = (last && accumulate)
+                     ? rotate_step_batch(ctx, c0, c1, n0, n1, nz, steps[k], limbs, &fo0, &fo1, fused_ok)
+                     : rotate_step_batch(ctx, c0, c1, n0, n1, nz, steps[k], limbs, nullptr, nullptr, fused_ok);
         if (rc != AFHE_OK) return rc;
         c0 = n0;
         c1 = n1;
@@ -438,7 +473,9 @@ int afhe_eval_rotate_single_step(afhe_ctx* ctx, uint64_t i0, uint64_t i1, uint64
     if ((rc = check_limbs(ctx, limbs, 1)) || (rc = check_poly(ctx, i0, limbs)) || (rc = check_poly(ctx, i1, limbs)) ||
         (rc = check_poly(ctx, d0, limbs)) || (rc = check_poly(ctx, d1, limbs)))
         return rc;
-    return rotate_step_batch(ctx, zf_const(i0), zf_const(i1), zf_const(d0), zf_const(d1), 1, step, limbs);
+    const bool fused_ok = fused_rotation_safe(Offs{i0}, Offs{i1}, Offs{d0}, Offs{d1}, (u64)limbs * ctx->n);
+    return rotate_step_batch(ctx, zf_const(i0), zf_const(i1), zf_const(d0), zf_const(d1), 1, step, limbs, nullptr,
+                             nullptr, fused_ok);
 }
 
 int afhe_eval_rotate_batch(afhe_ctx* ctx, const afhe_ct_ref* in, const afhe_ct_ref* dst, uint32_t count, int32_t total,

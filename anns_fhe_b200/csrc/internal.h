@@ -111,6 +111,7 @@ struct afhe_ctx {
     size_t scr_words = 0;
     uint32_t lanes = 64;
     afhe::DescRing ring;
+    bool ks_fused = true;   // one-kernel key switch where supported (AFHE_KS_FUSED=0 turns it off)
 
     // key directory
     bool has_relin = false;
@@ -175,6 +176,18 @@ cudaError_t launch_key_switch(int log_n, const OpTabs& t, const LimbJob* jobs_qp
                               const u64* key, u64 evk_a, u64 evk_b, uint32_t key_stride, uint32_t key_pbase,
                               u64* arena, u64* scratch, uint32_t nz, const ZBases& zb, cudaStream_t st,
                               const KsFuse* fuse = nullptr);
+
+// The same key switch as one kernel per polynomial (N <= 2^13): each CTA
+// keeps the limb being transformed and both accumulators in shared memory
+// and needs ks_fused_scratch_words(...) words of scratch at zb.mid (the INTT
+// of the input's limbs and of the special accumulators). Entries of one
+// launch run concurrently, so an entry's outputs must not overlap another
+// entry's inputs (in place within an entry is fine).
+bool key_switch_fused_supported(int log_n);
+size_t ks_fused_scratch_words(uint32_t n, uint32_t sizeQl, uint32_t K);
+cudaError_t launch_key_switch_fused(int log_n, const OpTabs& t, uint32_t sizeQl, uint32_t K, const u64* key, u64 evk_a,
+                                    u64 evk_b, uint32_t key_stride, uint32_t key_pbase, u64* arena, u64* scratch,
+                                    uint32_t nz, const ZBases& zb, cudaStream_t st, const KsFuse* fuse = nullptr);
 
 // Twiddle pairs: out2[r * n + j] = (w, companion of w), w = raw[r * n + j] mod q[r].
 cudaError_t launch_interleave(const u64* raw, const u64* q, ulonglong2* out2, uint32_t rows, uint32_t n,
