@@ -90,6 +90,7 @@ SIGNATURES = {
     "afhe_stream": (C.c_void_p, [CTX]),
     "afhe_poly_gmem": (C.c_void_p, [CTX]),
     "afhe_key_gmem": (C.c_void_p, [CTX]),
+    "afhe_scratch_words": (u64, [CTX]),
     "afhe_write_poly": (C.c_int, [CTX, u64, P64, u64]),
     "afhe_read_poly": (C.c_int, [CTX, u64, P64, u64]),
     "afhe_write_key": (C.c_int, [CTX, u64, P64, u64]),

@@ -23,6 +23,7 @@ automorphisms); the host samples randomness, encodes and decodes.
 from __future__ import annotations
 
 import numpy as np
+import scipy.fft as _sfft
 
 from .driver import CkksParams, FheContext, FHEHostDriver
 
@@ -60,11 +61,13 @@ class Encoder:
         M = self.n * np.fft.ifft(y)
         return M[self.t] / scale
 
-    def decode_batch(self, coeffs: np.ndarray, scale: float) -> np.ndarray:
-        """decode() for each row of a (count, N) coefficient array."""
+    def decode_batch(self, coeffs: np.ndarray, scale: float, slots: int | None = None) -> np.ndarray:
+        """decode() for each row of a (count, N) coefficient array, the first
+        `slots` slots (all by default); the transforms run on every host core."""
         y = np.asarray(coeffs, dtype=np.float64) * self.zeta[None, :]
-        M = self.n * np.fft.ifft(y, axis=1)
-        return M[:, self.t] / scale
+        M = _sfft.ifft(y, axis=1, norm="forward", workers=-1)    # = N * ifft(y)
+        t = self.t if slots is None else self.t[:slots]
+        return M[:, t] / scale
 
 
 def to_rns(coef: np.ndarray, primes) -> np.ndarray:
@@ -259,8 +262,9 @@ class CkksClient:
             have[name] = (self.slots.take(k)[0], k * self.slots.w)
         return have[name][0]
 
-    def decrypt_batch(self, cts, level: int, scale: float) -> np.ndarray:
-        """Decrypt ciphertexts resident in poly_gmem; returns (count, N/2) slot values."""
+    def decrypt_batch(self, cts, level: int, scale: float, slots: int | None = None) -> np.ndarray:
+        """Decrypt ciphertexts resident in poly_gmem; returns (count, slots) slot
+        values (all N/2 slots by default)."""
         from . import _lib as L
         n, count = self.p.n, len(cts)
         out = self._region("dec_out", count * level * n)
@@ -269,21 +273,23 @@ class CkksClient:
             arr[i].c0_offset, arr[i].c1_offset = a, b
         L.check(self.ctx.lib.afhe_decrypt_batch(self.ctx.h, arr, count, self.s_slot, out, level), "decrypt_batch")
         limbs = self.ctx.read_poly(out, count * level * n).reshape(count, level * n)
-        if level == 1:
-            q = np.int64(self.p.q[0])
-            v = limbs.astype(np.int64)
-            coef = np.where(v > q // 2, v - q, v).astype(np.float64)
+        if level == 1 and self.p.q[0] < 2**53:
+            # residues below 2^53 convert to float64 exactly; centre in place
+            q = float(self.p.q[0])
+            coef = limbs.astype(np.float64)
+            coef -= q * (coef > q // 2)
         else:
             coef = np.stack([crt_centered(row, self.p.q[:level]).astype(np.float64) for row in limbs])
-        return self.enc.decode_batch(coef, scale)
+        return self.enc.decode_batch(coef, scale, slots)
 
-    def decrypt_host_batch(self, cts: np.ndarray, level: int, scale: float) -> np.ndarray:
+    def decrypt_host_batch(self, cts: np.ndarray, level: int, scale: float, slots: int | None = None) -> np.ndarray:
         """Decrypt ciphertexts received as a host array (count, 2, level * N)."""
         n, count = self.p.n, cts.shape[0]
         w = level * n
         inp = self._region("dec_in", count * 2 * w)
         self.ctx.write_poly(inp, np.ascontiguousarray(cts).ravel())
-        return self.decrypt_batch([(inp + 2 * i * w, inp + (2 * i + 1) * w) for i in range(count)], level, scale)
+        return self.decrypt_batch([(inp + 2 * i * w, inp + (2 * i + 1) * w) for i in range(count)], level, scale,
+                                  slots)
 
     def plaintext(self, values, scale: float, off: int, level: int) -> None:
         """Encode `values` into an evaluation-form plaintext at `off` (level limbs)."""

@@ -412,6 +412,7 @@ int afhe_ctx_destroy(afhe_ctx* ctx) {
     for (DevPrimeSet* s : {&ctx->nat, &ctx->ld}) { fr(s->pc); fr(s->tw); fr(s->itw); fr(s->tw2); fr(s->itw2); }
     fr(ctx->ld_crt); fr(ctx->ld_crt_sh); fr(ctx->ld_mod); fr(ctx->ld_jobs);
     for (auto& kv : ctx->rot) fr(kv.second.map);
+    free_key_preps(ctx);
     fr(ctx->ring.dev);
     if (ctx->ring.host) cudaFreeHost(ctx->ring.host);
     for (auto& ev : ctx->ring.ev) if (ev) cudaEventDestroy(ev);
@@ -429,6 +430,7 @@ int afhe_sync(afhe_ctx* ctx) {
 void* afhe_stream(afhe_ctx* ctx) { return ctx ? (void*)ctx->st : nullptr; }
 uint64_t* afhe_poly_gmem(afhe_ctx* ctx) { return ctx ? ctx->poly : nullptr; }
 uint64_t* afhe_key_gmem(afhe_ctx* ctx) { return ctx ? ctx->key : nullptr; }
+uint64_t afhe_scratch_words(afhe_ctx* ctx) { return ctx ? (uint64_t)ctx->scr_words : 0; }
 
 static int arena_copy(afhe_ctx* ctx, bool poly, bool to_dev, u64 off, void* host, u64 count, bool async) {
     if (!ctx) return fail(nullptr, AFHE_E_ARG, "null context");
@@ -439,6 +441,10 @@ static int arena_copy(afhe_ctx* ctx, bool poly, bool to_dev, u64 off, void* host
     cudaError_t e = to_dev ? cudaMemcpyAsync(base, host, count * 8, cudaMemcpyHostToDevice, ctx->st)
                            : cudaMemcpyAsync(host, base, count * 8, cudaMemcpyDeviceToHost, ctx->st);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "arena copy");
+    if (!poly && to_dev) {
+        int rc = refresh_key_preps(ctx, off, count);
+        if (rc != AFHE_OK) return rc;
+    }
     if (!async) CK(cudaStreamSynchronize(ctx->st));
     return AFHE_OK;
 }

@@ -69,7 +69,7 @@ int check_cts(afhe_ctx* ctx, const afhe_ct_ref* v, uint32_t count, uint32_t limb
 // `fused_ok` is false when an entry's outputs may overlap another entry's
 // inputs, which the one-kernel key switch cannot order.
 int ks_batch(afhe_ctx* ctx, const ZField& in, const ZField& out0, const ZField& out1, uint32_t nz, u64 evk,
-             uint32_t limbs, const KsFuse* fuse = nullptr, bool fused_ok = true) {
+             uint32_t limbs, const KsFuse* fuse = nullptr, bool fused_ok = true, const ulonglong2* prep = nullptr) {
     const u64 n = ctx->n, S = (u64)ctx->L + ctx->K;
     const OpTabs& t = ctx->lv[limbs];
     const LevelJobs& lj = ctx->lvjobs[limbs];
@@ -80,7 +80,7 @@ int ks_batch(afhe_ctx* ctx, const ZField& in, const ZField& out0, const ZField& 
     zb.mid = lane_field(ctx, &Lane::ks);
     if (ctx->ks_fused && fused_ok) {
         CK(launch_key_switch_fused(ctx->log_n, t, limbs, ctx->K, ctx->key, evk, evk + (u64)ctx->dnum * S * n,
-                                   (uint32_t)S, ctx->L, ctx->poly, ctx->scr, nz, zb, ctx->st, fuse));
+                                   (uint32_t)S, ctx->L, ctx->poly, ctx->scr, nz, zb, ctx->st, fuse, prep));
         return AFHE_OK;
     }
     CK(launch_key_switch(ctx->log_n, t, ctx->jobs_qp, lj.modup, lj.n_modup, ctx->L, limbs, ctx->K, ctx->key, evk,
@@ -152,7 +152,7 @@ int mult_relin_rescale_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const afhe_ct_
     f.has_acc = 1;
     f.acc0 = ta.d0;
     f.acc1 = ta.d1;
-    int rc = ks_batch(ctx, ta.d2, ta.d0, ta.d1, nz, ctx->relin_off, limbs, &f);
+    int rc = ks_batch(ctx, ta.d2, ta.d0, ta.d1, nz, ctx->relin_off, limbs, &f, true, ctx->relin_prep);
     if (rc != AFHE_OK) return rc;
     // 4. rescale into the destination (:296-305)
     return rescale_batch(ctx, t0, t1, o0, o1, limbs);
@@ -175,7 +175,7 @@ int rotate_step_batch(afhe_ctx* ctx, const ZField& in0, const ZField& in1, const
     f.c0 = in0;
     f.has_acc = acc0 != nullptr;
     if (acc0) { f.acc0 = *acc0; f.acc1 = *acc1; }
-    return ks_batch(ctx, in1, d0, d1, nz, rk.evk_offset, limbs, &f, fused_ok);
+    return ks_batch(ctx, in1, d0, d1, nz, rk.evk_offset, limbs, &f, fused_ok, rk.prep);
 }
 
 // Whether the one-kernel key switch may run a rotation batch: its entries run
@@ -260,6 +260,18 @@ int rotate_batch(afhe_ctx* ctx, const afhe_ct_ref* in, const afhe_ct_ref* dst, u
     return AFHE_OK;
 }
 
+u64 key_region_words(const afhe_ctx* ctx) { return 2ull * ctx->dnum * (ctx->L + ctx->K) * ctx->n; }
+
+// The one-kernel key switch reads a registered key through a prepared copy:
+// (k mod q, Shoup companion) per key word, derived on the device.
+int prep_key(afhe_ctx* ctx, u64 evk, ulonglong2** prep) {
+    if (!ctx->ks_fused) return AFHE_OK;
+    const u64 words = key_region_words(ctx);
+    if (!*prep) CK(cudaMalloc((void**)prep, words * sizeof(ulonglong2)));
+    CK(launch_key_prep(ctx->key + evk, *prep, ctx->nat.pc, ctx->n, ctx->L + ctx->K, words, ctx->st));
+    return AFHE_OK;
+}
+
 template <class F>
 int for_chunks(afhe_ctx* ctx, uint32_t count, F f) {
     const uint32_t w = ctx->lanes;
@@ -273,6 +285,27 @@ int for_chunks(afhe_ctx* ctx, uint32_t count, F f) {
 
 }  // namespace
 
+int afhe::refresh_key_preps(afhe_ctx* ctx, u64 off, u64 count) {
+    const u64 words = key_region_words(ctx);
+    auto hit = [&](u64 evk) { return count && off < evk + words && evk < off + count; };
+    int rc;
+    if (ctx->has_relin && ctx->relin_prep && hit(ctx->relin_off))
+        if ((rc = prep_key(ctx, ctx->relin_off, &ctx->relin_prep)) != AFHE_OK) return rc;
+    for (auto& kv : ctx->rot)
+        if (kv.second.prep && hit(kv.second.evk_offset))
+            if ((rc = prep_key(ctx, kv.second.evk_offset, &kv.second.prep)) != AFHE_OK) return rc;
+    return AFHE_OK;
+}
+
+void afhe::free_key_preps(afhe_ctx* ctx) {
+    if (ctx->relin_prep) cudaFree(ctx->relin_prep);
+    ctx->relin_prep = nullptr;
+    for (auto& kv : ctx->rot) {
+        if (kv.second.prep) cudaFree(kv.second.prep);
+        kv.second.prep = nullptr;
+    }
+}
+
 extern "C" {
 
 // ---- key directory ----------------------------------------------------------
@@ -280,6 +313,8 @@ int afhe_set_relin_key(afhe_ctx* ctx, uint64_t evk) {
     if (!ctx) return fail(nullptr, AFHE_E_ARG, "null context");
     int rc = check_key(ctx, evk);
     if (rc != AFHE_OK) return rc;
+    cudaSetDevice(ctx->device);
+    if ((rc = prep_key(ctx, evk, &ctx->relin_prep)) != AFHE_OK) return rc;
     ctx->relin_off = evk;
     ctx->has_relin = true;
     return AFHE_OK;
@@ -299,12 +334,14 @@ int afhe_add_rotation_key(afhe_ctx* ctx, int32_t step, uint64_t evk) {
     auto old = ctx->rot.find(step);
     if (old != ctx->rot.end()) {
         rk.map = old->second.map;
+        rk.prep = old->second.prep;
     } else {
         CK(cudaMalloc((void**)&rk.map, ctx->n * sizeof(uint32_t)));
     }
     CK(cudaMemcpy(rk.map, map.data(), ctx->n * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    rc = prep_key(ctx, evk, &rk.prep);
     ctx->rot[step] = rk;
-    return AFHE_OK;
+    return rc;
 }
 
 int afhe_has_rotation_key(afhe_ctx* ctx, int32_t step) { return ctx && ctx->rot.count(step) ? 1 : 0; }
@@ -397,7 +434,12 @@ int afhe_key_switch(afhe_ctx* ctx, uint64_t src, uint64_t evk, uint64_t d0, uint
     const u64 w = (u64)limbs * ctx->n;
     u64 t = lane_temp(ctx, 0, 2);
     CK(cudaMemcpyAsync(ctx->poly + t, ctx->poly + src, w * 8, cudaMemcpyDeviceToDevice, ctx->st));
-    return ks_batch(ctx, zf_const(t), zf_const(d0), zf_const(d1), 1, evk, limbs);
+    // a registered key at this offset brings its prepared copy
+    const ulonglong2* prep = nullptr;
+    if (ctx->has_relin && ctx->relin_off == evk) prep = ctx->relin_prep;
+    for (const auto& kv : ctx->rot)
+        if (!prep && kv.second.evk_offset == evk) prep = kv.second.prep;
+    return ks_batch(ctx, zf_const(t), zf_const(d0), zf_const(d1), 1, evk, limbs, nullptr, true, prep);
 }
 
 // ---- composite operators ------------------------------------------------------

@@ -65,7 +65,8 @@ struct RotKey {
     int32_t step;
     uint32_t galois;
     u64 evk_offset;
-    uint32_t* map;   // device, N entries
+    uint32_t* map;              // device, N entries
+    ulonglong2* prep = nullptr;  // (k mod q, Shoup companion) per key word, for the one-kernel key switch
 };
 
 // Key-switch job templates for one level (device arrays).
@@ -116,6 +117,7 @@ struct afhe_ctx {
     // key directory
     bool has_relin = false;
     afhe::u64 relin_off = 0;
+    ulonglong2* relin_prep = nullptr;
     std::map<int32_t, afhe::RotKey> rot;
 
     std::string err;
@@ -183,11 +185,19 @@ cudaError_t launch_key_switch(int log_n, const OpTabs& t, const LimbJob* jobs_qp
 // of the input's limbs and of the special accumulators). Entries of one
 // launch run concurrently, so an entry's outputs must not overlap another
 // entry's inputs (in place within an entry is fine).
+// `prep`, when given, holds the key (evk_a digits then evk_b digits, the key
+// region's word order) as (k mod q, Shoup companion) pairs; the inner product
+// then multiplies with Shoup's method instead of a full 128-bit reduction.
 bool key_switch_fused_supported(int log_n);
 size_t ks_fused_scratch_words(uint32_t n, uint32_t sizeQl, uint32_t K);
 cudaError_t launch_key_switch_fused(int log_n, const OpTabs& t, uint32_t sizeQl, uint32_t K, const u64* key, u64 evk_a,
                                     u64 evk_b, uint32_t key_stride, uint32_t key_pbase, u64* arena, u64* scratch,
-                                    uint32_t nz, const ZBases& zb, cudaStream_t st, const KsFuse* fuse = nullptr);
+                                    uint32_t nz, const ZBases& zb, cudaStream_t st, const KsFuse* fuse = nullptr,
+                                    const ulonglong2* prep = nullptr);
+// prep[w] = (k mod q, companion) for k = key[w], w < words, where word w
+// belongs to key limb slot (w / n) mod S and slot i uses prime pc[i].
+cudaError_t launch_key_prep(const u64* key, ulonglong2* prep, const PrimeConst* pc, uint32_t n, uint32_t S, u64 words,
+                            cudaStream_t st);
 
 // Twiddle pairs: out2[r * n + j] = (w, companion of w), w = raw[r * n + j] mod q[r].
 cudaError_t launch_interleave(const u64* raw, const u64* q, ulonglong2* out2, uint32_t rows, uint32_t n,

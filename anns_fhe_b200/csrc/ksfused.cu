@@ -18,11 +18,13 @@
 //
 // Shared memory: three padded limb buffers (W for transforms, A0 / A1 for the
 // two accumulators), 3 * (N + N/16) words = 204 KB at N = 8192. The key limbs
-// every CTA of a launch reads are the same, so they come from L2.
+// every CTA of a launch reads are the same, so they come from L2. A registered
+// key comes as a prepared copy of (k mod q, Shoup companion) pairs, so each
+// inner-product term is one Shoup multiplication.
 //
 // In place is safe: input limb i is read only while slot i is processed, and
 // output limb i is written after every read of input limb i and of the
-// gathered c0 limb i (they are staged in shared memory first).
+// gathered c0 limb i (staged in shared memory behind a barrier).
 #include "internal.h"
 
 namespace afhe {
@@ -39,6 +41,8 @@ struct KsFusedArgs {
     u64* scratch;
     ZField in, out0, out1, mid;
     KsFuse f;
+    const ulonglong2* prep;   // prepared key (evk_a digits, then evk_b digits), or null
+    u64 prep_b;               // offset of the evk_b digits in prep
 };
 
 // digit j of a level-l key switch: limbs [start, start + size)
@@ -59,12 +63,24 @@ __device__ __noinline__ void inv_ntt(u64* buf, const PrimeTables pt, uint32_t pr
     ntt_rounds<true, LOGN, 0, false, 0>(buf, pt.itw2 + ((u64)prime << LOGN), pc, 0u, LOGN, 0, true);
 }
 
+// Every element-wise pass below gives each thread the positions
+// x_k = threadIdx.x + k * N/8, k < 8, and issues a chunk's global loads before
+// its arithmetic, so several L2 round trips are in flight per thread.
+constexpr uint32_t kPer = 8;     // positions per thread
+constexpr uint32_t kChunk = 4;   // positions whose loads are issued together
+
+template <int LOGN>
+__device__ __forceinline__ uint32_t pos(uint32_t k) { return threadIdx.x + k * ((1u << LOGN) / 8); }
+
+// gathered position of x: the automorphism's source index, or x itself
+__device__ __forceinline__ uint32_t gpos(const uint32_t* map, uint32_t x) { return map ? __ldg(map + x) : x; }
+
 // Inner product for one slot (Q limb `s` < l, or special limb s - l) into A0 / A1:
 // A0 = sum_j d_j * evk_b[j], A1 = sum_j d_j * evk_a[j] (mod the slot's prime).
-template <int LOGN>
-__device__ void mac_slot(const KsFusedArgs& a, uint32_t z, uint32_t s, u64* W, u64* A0, u64* A1,
-                         const u64* __restrict__ in, const u64* __restrict__ coef) {
-    constexpr uint32_t N = 1u << LOGN, T = N / 8;
+template <int LOGN, bool PREP>
+__device__ void mac_slot(const KsFusedArgs& a, uint32_t s, u64* W, u64* A0, u64* A1, const u64* __restrict__ in,
+                         const u64* __restrict__ coef) {
+    constexpr uint32_t N = 1u << LOGN;
     const OpTabs& t = a.t;
     const uint32_t l = a.sizeQl;
     const bool isq = s < l;
@@ -72,57 +88,106 @@ __device__ void mac_slot(const KsFusedArgs& a, uint32_t z, uint32_t s, u64* W, u
     const uint32_t klimb = isq ? s : a.key_pbase + (s - l);
     const PrimeConst pc = t.pt.pc[prime];
     const ModConst mc = modconst_of(pc);
-    const u64 p2 = pc.q << 1;
+    const u64 q = pc.q, p2 = q << 1;
+    const uint32_t* map = a.f.map;
     for (uint32_t j = 0; j < t.parts; ++j) {
         uint32_t start, size;
         digit_range(t, j, start, size);
         const bool own = isq && s >= start && s < start + size;
-        const u64* kb = a.key + a.evk_b + ((u64)j * a.key_stride + klimb) * N;
-        const u64* ka = a.key + a.evk_a + ((u64)j * a.key_stride + klimb) * N;
+        const u64 kofs = ((u64)j * a.key_stride + klimb) * N;
+        const u64* kb = a.key + a.evk_b + kofs;
+        const u64* ka = a.key + a.evk_a + kofs;
+        const ulonglong2* pb2 = PREP ? a.prep + a.prep_b + kofs : nullptr;
+        const ulonglong2* pa2 = PREP ? a.prep + kofs : nullptr;
         if (!own) {
             // W = BConv_j(coef) at this slot's prime, then NTT
             const uint32_t row = l - size + a.K;
             const uint32_t kpos = isq ? (s < start ? s : s - size) : (l - size) + (s - l);
-            const u64* qi = t.qhat_inv[j];
-            const u64* qish = t.qhat_inv_sh[j];
-            const u64* qm = t.qhat_modp[j];
-            const u64* qmsh = t.qhat_modp_sh[j];
-#pragma unroll 2
-            for (uint32_t x = threadIdx.x; x < N; x += T) {
-                u64 acc = 0;
-                for (uint32_t i = 0; i < size; ++i) {
-                    const uint32_t limb = start + i;
-                    const u64 qq = t.pt.pc[limb].q;
-                    u64 y = mul_shoup(coef[((u64)limb << LOGN) + x], __ldg(qi + i), __ldg(qish + i), qq);
-                    acc += mul_shoup_lazy(y, __ldg(qm + i * row + kpos), __ldg(qmsh + i * row + kpos), pc.q);
-                    acc = acc >= p2 ? acc - p2 : acc;
+            u64 acc[kPer];
+#pragma unroll
+            for (uint32_t k = 0; k < kPer; ++k) acc[k] = 0;
+            for (uint32_t i = 0; i < size; ++i) {
+                const uint32_t limb = start + i;
+                const u64 qq = t.pt.pc[limb].q;
+                const u64 w0 = __ldg(t.qhat_inv[j] + i), w0s = __ldg(t.qhat_inv_sh[j] + i);
+                const u64 w1 = __ldg(t.qhat_modp[j] + i * row + kpos), w1s = __ldg(t.qhat_modp_sh[j] + i * row + kpos);
+                const u64* src = coef + ((u64)limb << LOGN);
+                u64 v[kPer];
+#pragma unroll
+                for (uint32_t k = 0; k < kPer; ++k) v[k] = src[pos<LOGN>(k)];
+#pragma unroll
+                for (uint32_t k = 0; k < kPer; ++k) {
+                    acc[k] += mul_shoup_lazy(mul_shoup(v[k], w0, w0s, qq), w1, w1s, q);
+                    acc[k] = acc[k] >= p2 ? acc[k] - p2 : acc[k];
                 }
-                W[padix(x)] = csub(acc, pc.q);
             }
+#pragma unroll
+            for (uint32_t k = 0; k < kPer; ++k) W[padix(pos<LOGN>(k))] = csub(acc[k], q);
             __syncthreads();
             fwd_ntt<LOGN>(W, t.pt, prime, pc);
         }
-#pragma unroll 2
-        for (uint32_t x = threadIdx.x; x < N; x += T) {
-            u64 d;
-            if (own) d = in[((u64)s << LOGN) + (a.f.map ? __ldg(a.f.map + x) : x)];
-            else d = canon4(W[padix(x)], pc.q);
-            u64 pb = mul_mod(d, __ldg(kb + x), mc);
-            u64 pa = mul_mod(d, __ldg(ka + x), mc);
-            if (j > 0) {
-                pb = add_mod(pb, A0[padix(x)], pc.q);
-                pa = add_mod(pa, A1[padix(x)], pc.q);
+        const u64* src = in + ((u64)s << LOGN);
+        if (PREP) {
+            // Shoup products with the prepared key; the accumulators stay lazy
+            // in [0, 2q) (both consumers accept that range)
+#pragma unroll
+            for (uint32_t c = 0; c < kPer; c += kChunk) {
+                u64 d[kChunk];
+                ulonglong2 vb[kChunk], va[kChunk];
+#pragma unroll
+                for (uint32_t k = 0; k < kChunk; ++k) {
+                    const uint32_t x = pos<LOGN>(c + k);
+                    vb[k] = __ldg(pb2 + x);
+                    va[k] = __ldg(pa2 + x);
+                    d[k] = own ? src[gpos(map, x)] : W[padix(x)];   // any d < 2^64 is valid for Shoup
+                }
+#pragma unroll
+                for (uint32_t k = 0; k < kChunk; ++k) {
+                    const uint32_t e = padix(pos<LOGN>(c + k));
+                    u64 pb = mul_shoup_lazy(d[k], vb[k].x, vb[k].y, q);
+                    u64 pa = mul_shoup_lazy(d[k], va[k].x, va[k].y, q);
+                    if (j > 0) {
+                        pb += A0[e];
+                        pa += A1[e];
+                        pb = pb >= p2 ? pb - p2 : pb;
+                        pa = pa >= p2 ? pa - p2 : pa;
+                    }
+                    A0[e] = pb;
+                    A1[e] = pa;
+                }
             }
-            A0[padix(x)] = pb;
-            A1[padix(x)] = pa;
+        } else {
+#pragma unroll
+            for (uint32_t c = 0; c < kPer; c += kChunk) {
+                u64 d[kChunk], vb[kChunk], va[kChunk];
+#pragma unroll
+                for (uint32_t k = 0; k < kChunk; ++k) {
+                    const uint32_t x = pos<LOGN>(c + k);
+                    vb[k] = __ldg(kb + x);
+                    va[k] = __ldg(ka + x);
+                    d[k] = own ? src[gpos(map, x)] : canon4(W[padix(x)], q);
+                }
+#pragma unroll
+                for (uint32_t k = 0; k < kChunk; ++k) {
+                    const uint32_t e = padix(pos<LOGN>(c + k));
+                    u64 pb = mul_mod(d[k], vb[k], mc);
+                    u64 pa = mul_mod(d[k], va[k], mc);
+                    if (j > 0) {
+                        pb = add_mod(pb, A0[e], q);
+                        pa = add_mod(pa, A1[e], q);
+                    }
+                    A0[e] = pb;
+                    A1[e] = pa;
+                }
+            }
         }
         __syncthreads();
     }
 }
 
-template <int LOGN>
+template <int LOGN, bool PREP>
 __global__ void __launch_bounds__((1u << LOGN) / 8, 1) ks_fused_kernel(const KsFusedArgs a) {
-    constexpr uint32_t N = 1u << LOGN, T = N / 8;
+    constexpr uint32_t N = 1u << LOGN;
     constexpr uint32_t PADN = N + N / 16;
     extern __shared__ u64 smem[];
     u64* W = smem;
@@ -131,6 +196,7 @@ __global__ void __launch_bounds__((1u << LOGN) / 8, 1) ks_fused_kernel(const KsF
     const uint32_t z = blockIdx.x;
     const OpTabs& t = a.t;
     const uint32_t l = a.sizeQl, K = a.K;
+    const uint32_t* map = a.f.map;
     const u64* in = a.arena + a.in.at(z);
     u64* coef = a.scratch + a.mid.at(z);          // l limbs
     u64* pcoef = coef + ((u64)l << LOGN);         // 2K limbs: INTT of the special accumulators
@@ -138,26 +204,37 @@ __global__ void __launch_bounds__((1u << LOGN) / 8, 1) ks_fused_kernel(const KsF
     // phase 0: coefficients of the input's limbs (read through the automorphism)
     for (uint32_t i = 0; i < l; ++i) {
         const PrimeConst pc = t.pt.pc[i];
-#pragma unroll 2
-        for (uint32_t x = threadIdx.x; x < N; x += T)
-            W[padix(x)] = in[((u64)i << LOGN) + (a.f.map ? __ldg(a.f.map + x) : x)];
+        const u64* src = in + ((u64)i << LOGN);
+        {
+            uint32_t g[kPer];
+            u64 v[kPer];
+#pragma unroll
+            for (uint32_t k = 0; k < kPer; ++k) g[k] = gpos(map, pos<LOGN>(k));
+#pragma unroll
+            for (uint32_t k = 0; k < kPer; ++k) v[k] = src[g[k]];
+#pragma unroll
+            for (uint32_t k = 0; k < kPer; ++k) W[padix(pos<LOGN>(k))] = v[k];
+        }
         __syncthreads();
         inv_ntt<LOGN>(W, t.pt, i, pc);
-#pragma unroll 2
-        for (uint32_t x = threadIdx.x; x < N; x += T) coef[((u64)i << LOGN) + x] = W[padix(x)];
+#pragma unroll
+        for (uint32_t k = 0; k < kPer; ++k) coef[((u64)i << LOGN) + pos<LOGN>(k)] = W[padix(pos<LOGN>(k))];
         __syncthreads();
     }
     // phase 1: special slots -> INTT of both accumulators
     for (uint32_t k = 0; k < K; ++k) {
-        mac_slot<LOGN>(a, z, l + k, W, A0, A1, in, coef);
+        mac_slot<LOGN, PREP>(a, l + k, W, A0, A1, in, coef);
         const uint32_t prime = t.p_base + k;
         const PrimeConst pc = t.pt.pc[prime];
         inv_ntt<LOGN>(A0, t.pt, prime, pc);
         inv_ntt<LOGN>(A1, t.pt, prime, pc);
-#pragma unroll 2
-        for (uint32_t x = threadIdx.x; x < N; x += T) {
-            pcoef[((u64)(2 * k) << LOGN) + x] = A0[padix(x)];
-            pcoef[((u64)(2 * k + 1) << LOGN) + x] = A1[padix(x)];
+        u64* d0 = pcoef + ((u64)(2 * k) << LOGN);
+        u64* d1 = pcoef + ((u64)(2 * k + 1) << LOGN);
+#pragma unroll
+        for (uint32_t e = 0; e < kPer; ++e) {
+            const uint32_t x = pos<LOGN>(e);
+            d0[x] = A0[padix(x)];
+            d1[x] = A1[padix(x)];
         }
         __syncthreads();
     }
@@ -166,58 +243,108 @@ __global__ void __launch_bounds__((1u << LOGN) / 8, 1) ks_fused_kernel(const KsF
     const u64 c0 = a.f.has_c0 ? a.f.c0.at(z) : 0;
     const u64 ac0 = a.f.has_acc ? a.f.acc0.at(z) : 0, ac1 = a.f.has_acc ? a.f.acc1.at(z) : 0;
     for (uint32_t i = 0; i < l; ++i) {
-        mac_slot<LOGN>(a, z, i, W, A0, A1, in, coef);
+        mac_slot<LOGN, PREP>(a, i, W, A0, A1, in, coef);
         const PrimeConst pc = t.pt.pc[i];
         const u64 q = pc.q, q2 = q << 1;
         const u64 pinv = __ldg(t.p_inv_mod_q + i), pinv_sh = __ldg(t.p_inv_mod_q_sh + i);
         for (uint32_t h = 0; h < 2; ++h) {
             u64* A = h ? A1 : A0;
             // W = BConv of the special limbs to q_i (approx_mod_down's fast_bases_conv), then NTT
-#pragma unroll 2
-            for (uint32_t x = threadIdx.x; x < N; x += T) {
-                u64 acc = 0;
+            {
+                u64 acc[kPer];
+#pragma unroll
+                for (uint32_t e = 0; e < kPer; ++e) acc[e] = 0;
                 for (uint32_t k = 0; k < K; ++k) {
-                    const PrimeConst& pk = t.pt.pc[t.p_base + k];
-                    u64 y = mul_shoup(pcoef[((u64)(2 * k + h) << LOGN) + x], __ldg(t.phat_inv_modp + k),
-                                      __ldg(t.phat_inv_modp_sh + k), pk.q);
-                    acc += mul_shoup_lazy(y, __ldg(t.phat_modq + k * l + i), __ldg(t.phat_modq_sh + k * l + i), q);
-                    acc = acc >= q2 ? acc - q2 : acc;
+                    const u64 pq = t.pt.pc[t.p_base + k].q;
+                    const u64 w0 = __ldg(t.phat_inv_modp + k), w0s = __ldg(t.phat_inv_modp_sh + k);
+                    const u64 w1 = __ldg(t.phat_modq + k * l + i), w1s = __ldg(t.phat_modq_sh + k * l + i);
+                    const u64* src = pcoef + ((u64)(2 * k + h) << LOGN);
+                    u64 v[kPer];
+#pragma unroll
+                    for (uint32_t e = 0; e < kPer; ++e) v[e] = src[pos<LOGN>(e)];
+#pragma unroll
+                    for (uint32_t e = 0; e < kPer; ++e) {
+                        acc[e] += mul_shoup_lazy(mul_shoup(v[e], w0, w0s, pq), w1, w1s, q);
+                        acc[e] = acc[e] >= q2 ? acc[e] - q2 : acc[e];
+                    }
                 }
-                W[padix(x)] = csub(acc, q);
+#pragma unroll
+                for (uint32_t e = 0; e < kPer; ++e) W[padix(pos<LOGN>(e))] = csub(acc[e], q);
             }
             __syncthreads();
             fwd_ntt<LOGN>(W, t.pt, i, pc);
-            // (x_Q - y) * P^-1, then the fused extras, staged in A before any store
-#pragma unroll 2
-            for (uint32_t x = threadIdx.x; x < N; x += T) {
-                u64 r = mul_shoup(sub_mod(A[padix(x)], canon4(W[padix(x)], q), q), pinv, pinv_sh, q);
-                if (h == 0 && a.f.has_c0)
-                    r = add_mod(r, a.arena[c0 + ((u64)i << LOGN) + (a.f.map ? __ldg(a.f.map + x) : x)], q);
-                A[padix(x)] = r;
-            }
-            __syncthreads();
+            // (x_Q - y) * P^-1 plus the fused extras. The gathered c0 limb i
+            // is staged in A and stored after a barrier (c0 may alias out0);
+            // every other output goes straight out (each element is read and
+            // written by the same thread).
+            const bool stage = h == 0 && a.f.has_c0;
             const u64 ob = (h ? o1 : o0) + ((u64)i << LOGN);
             const u64 ab = (h ? ac1 : ac0) + ((u64)i << LOGN);
-#pragma unroll 2
-            for (uint32_t x = threadIdx.x; x < N; x += T) {
-                u64 r = A[padix(x)];
-                if (a.f.has_acc) r = add_mod(r, a.arena[ab + x], q);
-                a.arena[ob + x] = r;
+            const u64* cb = a.arena + c0 + ((u64)i << LOGN);
+#pragma unroll
+            for (uint32_t c = 0; c < kPer; c += kChunk) {
+                u64 ex[kChunk];
+#pragma unroll
+                for (uint32_t e = 0; e < kChunk; ++e) {
+                    const uint32_t x = pos<LOGN>(c + e);
+                    ex[e] = stage ? cb[gpos(map, x)] : (a.f.has_acc ? a.arena[ab + x] : 0);
+                }
+#pragma unroll
+                for (uint32_t e = 0; e < kChunk; ++e) {
+                    const uint32_t x = pos<LOGN>(c + e);
+                    // A may be lazy in [0, 2q): the difference is then in
+                    // [0, 2q) and mul_shoup returns it canonical
+                    u64 r = mul_shoup(sub_mod(A[padix(x)], canon4(W[padix(x)], q), q), pinv, pinv_sh, q);
+                    if (stage || a.f.has_acc) r = add_mod(r, ex[e], q);
+                    if (stage) A[padix(x)] = r;
+                    else a.arena[ob + x] = r;
+                }
+            }
+            if (stage) {
+                __syncthreads();
+#pragma unroll
+                for (uint32_t c = 0; c < kPer; c += kChunk) {
+                    u64 ex[kChunk];
+#pragma unroll
+                    for (uint32_t e = 0; e < kChunk; ++e) ex[e] = a.f.has_acc ? a.arena[ab + pos<LOGN>(c + e)] : 0;
+#pragma unroll
+                    for (uint32_t e = 0; e < kChunk; ++e) {
+                        const uint32_t x = pos<LOGN>(c + e);
+                        u64 r = A[padix(x)];
+                        if (a.f.has_acc) r = add_mod(r, ex[e], q);
+                        a.arena[ob + x] = r;
+                    }
+                }
             }
             __syncthreads();
         }
     }
 }
 
-template <int LOGN>
-cudaError_t launch_fused(const KsFusedArgs& a, uint32_t nz, cudaStream_t st) {
+template <int LOGN, bool PREP>
+cudaError_t launch_fused_v(const KsFusedArgs& a, uint32_t nz, cudaStream_t st) {
     constexpr uint32_t N = 1u << LOGN;
     const size_t smem = 3ull * (N + N / 16) * sizeof(u64);
-    cudaError_t e = cudaFuncSetAttribute(ks_fused_kernel<LOGN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    auto kern = ks_fused_kernel<LOGN, PREP>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    ks_fused_kernel<LOGN><<<nz, N / 8, smem, st>>>(a);
+    kern<<<nz, N / 8, smem, st>>>(a);
     count_launches(1);
     return cudaGetLastError();
+}
+
+template <int LOGN>
+cudaError_t launch_fused(const KsFusedArgs& a, uint32_t nz, cudaStream_t st) {
+    return a.prep ? launch_fused_v<LOGN, true>(a, nz, st) : launch_fused_v<LOGN, false>(a, nz, st);
+}
+
+__global__ void key_prep_kernel(const u64* __restrict__ key, ulonglong2* __restrict__ prep,
+                                const PrimeConst* __restrict__ pc, uint32_t n, uint32_t S, u64 words) {
+    for (u64 w = blockIdx.x * (u64)blockDim.x + threadIdx.x; w < words; w += (u64)gridDim.x * blockDim.x) {
+        const u64 q = pc[(w / n) % S].q;
+        const u64 k = key[w] % q;
+        prep[w] = make_ulonglong2(k, shoup_companion(k, q));
+    }
 }
 
 }  // namespace
@@ -226,9 +353,20 @@ bool key_switch_fused_supported(int log_n) { return log_n >= 10 && log_n <= 13; 
 
 size_t ks_fused_scratch_words(uint32_t n, uint32_t sizeQl, uint32_t K) { return (size_t)n * (sizeQl + 2 * K); }
 
+cudaError_t launch_key_prep(const u64* key, ulonglong2* prep, const PrimeConst* pc, uint32_t n, uint32_t S, u64 words,
+                            cudaStream_t st) {
+    if (words == 0) return cudaSuccess;
+    u64 blocks = (words + 255) / 256;
+    if (blocks > 4096) blocks = 4096;
+    key_prep_kernel<<<(unsigned)blocks, 256, 0, st>>>(key, prep, pc, n, S, words);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_key_switch_fused(int log_n, const OpTabs& t, uint32_t sizeQl, uint32_t K, const u64* key, u64 evk_a,
                                     u64 evk_b, uint32_t key_stride, uint32_t key_pbase, u64* arena, u64* scratch,
-                                    uint32_t nz, const ZBases& zb, cudaStream_t st, const KsFuse* fuse) {
+                                    uint32_t nz, const ZBases& zb, cudaStream_t st, const KsFuse* fuse,
+                                    const ulonglong2* prep) {
     if (nz == 0) return cudaSuccess;
     KsFusedArgs a{};
     a.t = t;
@@ -246,6 +384,8 @@ cudaError_t launch_key_switch_fused(int log_n, const OpTabs& t, uint32_t sizeQl,
     a.out1 = zb.aux;
     a.mid = zb.mid;
     if (fuse) a.f = *fuse;
+    a.prep = prep;
+    a.prep_b = evk_b - evk_a;
     switch (log_n) {
     case 10: return launch_fused<10>(a, nz, st);
     case 11: return launch_fused<11>(a, nz, st);

@@ -15,6 +15,10 @@ extern thread_local std::string g_last_error;
 int fail(afhe_ctx* ctx, int code, const std::string& msg);
 int cuda_fail(afhe_ctx* ctx, cudaError_t e, const char* where);
 u64 host_shoup(u64 w, u64 q);
+// Re-derive the prepared copies of registered keys that overlap key words
+// [off, off + count) after they were overwritten (driver.cu).
+int refresh_key_preps(afhe_ctx* ctx, u64 off, u64 count);
+void free_key_preps(afhe_ctx* ctx);
 
 #define CK(expr)                                                        \
     do {                                                                \

@@ -208,6 +208,10 @@ class FheContext:
         check(self.lib.afhe_read_key(self.h, off, _p64(a), count), "read_key")
         return a
 
+    def scratch_bytes(self) -> int:
+        """Bytes of context-private device scratch (all lanes)."""
+        return int(self.lib.afhe_scratch_words(self.h)) * 8
+
     def sync(self) -> None:
         check(self.lib.afhe_sync(self.h), "sync")
 

@@ -69,6 +69,12 @@ def run_ours(args, rank: int, world: int):
 
     dev = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(dev)
+    if args.batch <= 0:
+        # the key switch runs one CTA per ciphertext and one CTA per SM at a
+        # time: two full waves per launch
+        args.batch = 2 * torch.cuda.get_device_properties(dev).multi_processor_count
+    if args.lanes <= 0:
+        args.lanes = args.batch
     wl = Workload(max_queries=args.batch, lanes=args.lanes, device=dev)
     stream = torch.cuda.ExternalStream(wl.ctx.lib.afhe_stream(wl.ctx.h), device=dev)
     iqm = wl.iqm
@@ -111,14 +117,14 @@ def run_ours(args, rank: int, world: int):
         # client receives the compacted coarse distances, decrypts, selects
         box = iqm.read_outbox("compact", len(recs))
         d2h = box.nbytes
-        coarse = wl.client.decrypt_host_batch(box, iqm.lvl_out, iqm.out_scale).real[:, :wl.spec.n_list]
+        coarse = wl.client.decrypt_host_batch(box, iqm.lvl_out, iqm.out_scale, wl.spec.n_list).real
         for r, c in zip(recs, coarse):
             r.probes = list(np.argsort(c, kind="stable")[:wl.spec.nprobe])
         iqm.stage3_fine(recs)
         # client receives the candidate distances, decrypts, ranks
         box = iqm.read_outbox("dists", len(recs))
         d2h += box.nbytes
-        dists = wl.client.decrypt_host_batch(box, iqm.lvl_out, iqm.out_scale).real
+        dists = wl.client.decrypt_host_batch(box, iqm.lvl_out, iqm.out_scale, max(len(r.vids) for r in recs)).real
         for r, d in zip(recs, dists):
             np.argsort(d[:len(r.vids)], kind="stable")[:wl.spec.top_k]
         eb.record(stream)
@@ -165,13 +171,15 @@ def run_ours(args, rank: int, world: int):
         "config": {"workload": wl.spec.name, "queries_per_step": args.batch, "lanes": args.lanes,
                    "nprobe": wl.spec.nprobe, "n_list": wl.spec.n_list, "ring_degree": n,
                    "q_limbs": wl.params.L, "p_limbs": wl.params.K,
-                   "l2": "working set (< 126 MB) stays L2-resident; no flush: the metric is a serving rate"},
+                   "l2": f"no flush; inputs larger than L2: {args.batch * 2 * Lw * 8 / 1e6:.0f} MB of query "
+                         f"ciphertexts and {wl.ctx.scratch_bytes() / 1e9:.1f} GB of lane scratch per step "
+                         f"(L2 126 MB)"},
         "e2e": {"value": queries / (e2e_ms / 1e3), "unit": "queries/s",
                 "h2d_bytes_per_step": e2e[0][1], "d2h_bytes_per_step": e2e[0][2]},
         "clocks": summarize_clocks(samples),
         "gpu_launches": int(launches),
     }
-    line["roofline"] = ntt_roofline(wl, stream, args.lanes)
+    line["roofline"] = ks_roofline(wl.params, args.lanes)
     wl.close()
     if world == 1 and rank == 0 and not args.skip_cpu:
         from oracle.chain import cpu_reference_rate
@@ -189,50 +197,73 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
-def ntt_roofline(wl, stream, lanes):
-    """The dominant kernel (ntt_pass_kernel, 87% of device time in the launch
-    list) timed alone at the key switch's batch shape: `lanes` ciphertext polys
-    x (L + K) limbs of N = 8192 per launch, forward, in place. Five such
-    batches are cycled (> L2 in total) so every launch streams from HBM.
-    Algorithmic bytes per launch: read + write of every limb once."""
+def ks_roofline(params, lanes: int, reps: int = 20):
+    """The dominant kernel (ks_fused_kernel: the one-kernel key switch, ~88% of
+    device time in the launch list) timed alone: one rotation step of `lanes`
+    ciphertexts at the top level per launch (one launch per call), five batches
+    cycled so the inputs (> L2 in total) stream from HBM.
+    Algorithmic bytes per launch: per ciphertext c0 and c1 read and both
+    outputs written (4 x L limbs of N words), plus the rotation key read once
+    (2 x dnum x (L + K) limbs)."""
     import ctypes as C
 
     import numpy as np
     import torch
 
-    from anns_fhe_b200._lib import P64
-    p = wl.params
-    n, limbs = p.n, p.L + p.K
-    per = lanes
-    slot_w = limbs * n
-    nbuf = 5
-    need = nbuf * per * slot_w
-    # borrow the tail of poly_gmem (beyond the workload's slots) if it fits, else a fresh context
+    from anns_fhe_b200._lib import CtRef
     from anns_fhe_b200.driver import FheContext
-    ctx = FheContext(p, poly_words=need, key_words=1024, device=torch.cuda.current_device())
+    p = params
+    n, L, K = p.n, p.L, p.K
+    w = L * n
+    nbuf = 5
+    kw = p.key_words()
+    ctx = FheContext(p, poly_words=(nbuf + 1) * lanes * 2 * w, key_words=kw, max_batch=lanes,
+                     device=torch.cuda.current_device())
     rng = np.random.default_rng(3)
-    for b in range(nbuf * per):
-        ctx.write_poly(b * slot_w, np.concatenate([rng.integers(0, q, n, dtype=np.uint64) for q in p.q + p.p]))
+    allp = p.q + p.p
+    key = np.concatenate([rng.integers(0, q, n, dtype=np.uint64) for _ in range(2 * p.dnum) for q in allp])
+    ctx.write_key(0, key)
+    ctx.lib.afhe_add_rotation_key(ctx.h, 1, 0)
+    limb = np.concatenate([rng.integers(0, q, n, dtype=np.uint64) for q in p.q])
+    for i in range((nbuf + 1) * lanes * 2):
+        ctx.write_poly(i * w, limb)
+
+    def refs(first):
+        arr = (CtRef * lanes)()
+        for i in range(lanes):
+            arr[i].c0_offset, arr[i].c1_offset = (first + 2 * i) * w, (first + 2 * i + 1) * w
+        return arr
+    ins = [refs(b * lanes * 2) for b in range(nbuf)]
+    out = refs(nbuf * lanes * 2)
     st = torch.cuda.ExternalStream(ctx.lib.afhe_stream(ctx.h), device=torch.cuda.current_device())
-    offs = [(C.c_uint64 * per)(*[(b * per + i) * slot_w for i in range(per)]) for b in range(nbuf)]
     for b in range(nbuf):
-        ctx.lib.afhe_ntt_batch(ctx.h, C.cast(offs[b], P64), per, limbs, 0)
-    reps = 50
+        ctx.lib.afhe_eval_rotate_batch(ctx.h, ins[b], out, lanes, 1, L)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = ctx.lib.afhe_kernel_launches()
     e0.record(st)
     for r in range(reps):
-        ctx.lib.afhe_ntt_batch(ctx.h, C.cast(offs[r % nbuf], P64), per, limbs, 0)
+        ctx.lib.afhe_eval_rotate_batch(ctx.h, ins[r % nbuf], out, lanes, 1, L)
     e1.record(st)
     e1.synchronize()
-    ms = e0.elapsed_time(e1) / reps
+    launches = ctx.lib.afhe_kernel_launches() - l0
+    ms = e0.elapsed_time(e1) / launches
     ctx.close()
-    bytes_per_launch = 2 * per * limbs * n * 8
+    bytes_per_launch = lanes * 4 * w * 8 + 2 * p.dnum * (L + K) * n * 8
     achieved = bytes_per_launch / (ms * 1e-3) / 1e9
     peak, src = load_peaks()
-    return {"bound": "hbm", "kernel": f"ntt_pass_kernel (forward, N={n}, single pass, {per}x{limbs} limbs/launch)",
+    return {"bound": "hbm", "kernel": f"ks_fused_kernel (rotation key switch, N={n}, level {L}, {lanes} ciphertexts/launch)",
             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "peak_source": src, "traffic": None, "ms_per_launch": ms,
             "algorithmic_bytes_per_launch": bytes_per_launch}
+
+
+def profile_ks(lanes: int):
+    """Profiling driver: the roofline measurement of the key-switch kernel alone
+    (six warm-up launches, then 20 measured)."""
+    from anns_fhe_b200.driver import CkksParams
+    from anns_fhe_b200.workloads import SMALL as spec
+    p = CkksParams.generate(spec.log_n, spec.num_q, spec.q_bits, spec.num_p, spec.p_bits, spec.alpha)
+    print(json.dumps(ks_roofline(p, lanes)))
 
 
 def profile_step(nq: int):
@@ -305,17 +336,20 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--batch", type=int, default=256, help="queries per step")
-    ap.add_argument("--lanes", type=int, default=256)
+    ap.add_argument("--batch", type=int, default=0, help="queries per step (default: 2 x the SM count)")
+    ap.add_argument("--lanes", type=int, default=0, help="ciphertexts per launch (default: the batch)")
     ap.add_argument("--skip-cpu", action="store_true", help="omit the cpu_baseline leg")
     ap.add_argument("--profile-step", type=int, default=0, help="profiling driver: queries per step")
     ap.add_argument("--profile-ntt", type=int, default=0, help="profiling driver: polynomials per NTT launch")
+    ap.add_argument("--profile-ks", type=int, default=0, help="profiling driver: ciphertexts per key-switch launch")
     ap.add_argument("--log-n", type=int, default=13, help="ring degree for --profile-ntt")
     args = ap.parse_args()
     if args.profile_step:
         return profile_step(args.profile_step)
     if args.profile_ntt:
         return profile_ntt(args.profile_ntt, args.log_n)
+    if args.profile_ks:
+        return profile_ks(args.profile_ks)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if args.impl == "reference":

@@ -153,6 +153,10 @@ int afhe_sync(afhe_ctx* ctx);
 void* afhe_stream(afhe_ctx* ctx);
 uint64_t* afhe_poly_gmem(afhe_ctx* ctx);
 uint64_t* afhe_key_gmem(afhe_ctx* ctx);
+/* Words of context-private device scratch (max_batch lanes) allocated after
+ * poly_gmem; no counterpart in the reference (its composites use fixed
+ * SCRATCH_* slots inside poly_gmem, fhe_host_driver.h:63-69). */
+uint64_t afhe_scratch_words(afhe_ctx* ctx);
 
 /* SimMemoryBus::write_poly / read_poly / write_key / read_key
  * (sim_memory_bus.cpp:12-62): host <-> arena word copies (synchronous). */

@@ -58,7 +58,7 @@ class Pair:
         self.rot = {s: self.keys[i + 1] for i, s in enumerate(STEPS)}
         self.ctxs = []
         for fused in (True, False):
-            ctx = make_ctx(self.prm, fused, 16 * self.PW, (1 + len(STEPS)) * kw)
+            ctx = make_ctx(self.prm, fused, 16 * self.PW, (2 + len(STEPS)) * kw)
             drv = FHEHostDriver(ctx)
             for i, (a, b) in enumerate(self.keys):
                 ctx.write_key(i * kw, np.concatenate([a, b]))
@@ -197,3 +197,57 @@ def test_rotate_batch_entries_chained(pr):
     for g in both(pr, run):
         assert np.array_equal(g[0], ex[0]) and np.array_equal(g[1], ex[1])
         assert np.array_equal(g[2], ey[0]) and np.array_equal(g[3], ey[1])
+
+
+def test_unregistered_key_and_rewritten_key(pr):
+    """A key switch with a key offset that was never registered, and a
+    registered key whose words are overwritten after registration: both use
+    the key words as they are at call time."""
+    lvl = pr.L
+    x = pr.ct(lvl)[0]
+    allp = pr.prm.q + pr.prm.p
+    new_a = np.concatenate([uniform_residues(pr.rng, allp, pr.n) for _ in range(pr.prm.dnum)])
+    new_b = np.concatenate([uniform_residues(pr.rng, allp, pr.n) for _ in range(pr.prm.dnum)])
+    e0, e1 = pr.ora.key_switch(x, new_a, new_b, lvl)
+
+    def run(ctx, drv):
+        ctx.write_poly(pr.slot(0), x)
+        # overwrite the registered relinearisation key (offset 0) ...
+        ctx.write_key(0, np.concatenate([new_a, new_b]))
+        drv.key_switch(pr.slot(0), 0, pr.slot(1), pr.slot(2), lvl)
+        got = [ctx.read_poly(pr.slot(1), lvl * pr.n), ctx.read_poly(pr.slot(2), lvl * pr.n)]
+        # ... and check the relinearisation itself picked the new key up
+        A, B = pr.ct(lvl), pr.ct(lvl)
+        for i, v in enumerate(A + B):
+            ctx.write_poly(pr.slot(3 + i), v)
+        drv.eval_mult_relin_rescale(pr.slot(3), pr.slot(4), pr.slot(5), pr.slot(6), pr.slot(7), pr.slot(8), lvl)
+        m0, m1 = pr.ora.eval_mult_relin_rescale(A, B, (new_a, new_b), lvl)
+        got.append(np.array_equal(ctx.read_poly(pr.slot(7), (lvl - 1) * pr.n), m0)
+                   and np.array_equal(ctx.read_poly(pr.slot(8), (lvl - 1) * pr.n), m1))
+        # restore the original relinearisation key for the other tests
+        a, b = pr.keys[0]
+        ctx.write_key(0, np.concatenate([a, b]))
+        return got
+    for g0, g1, mult_ok in both(pr, run):
+        assert np.array_equal(g0, e0) and np.array_equal(g1, e1)
+        assert mult_ok
+
+
+def test_key_switch_with_unregistered_offset(pr):
+    """Key words written past every registered key and never registered."""
+    lvl = pr.L
+    kw = pr.prm.key_words()
+    off = (1 + len(STEPS)) * kw
+    x = pr.ct(lvl)[0]
+    allp = pr.prm.q + pr.prm.p
+    ka = np.concatenate([uniform_residues(pr.rng, allp, pr.n) for _ in range(pr.prm.dnum)])
+    kb = np.concatenate([uniform_residues(pr.rng, allp, pr.n) for _ in range(pr.prm.dnum)])
+    e0, e1 = pr.ora.key_switch(x, ka, kb, lvl)
+
+    def run(ctx, drv):
+        ctx.write_key(off, np.concatenate([ka, kb]))
+        ctx.write_poly(pr.slot(0), x)
+        drv.key_switch(pr.slot(0), off, pr.slot(1), pr.slot(2), lvl)
+        return ctx.read_poly(pr.slot(1), lvl * pr.n), ctx.read_poly(pr.slot(2), lvl * pr.n)
+    for g0, g1 in both(pr, run):
+        assert np.array_equal(g0, e0) and np.array_equal(g1, e1)
