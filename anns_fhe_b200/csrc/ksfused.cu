@@ -63,6 +63,14 @@ __device__ __noinline__ void inv_ntt(u64* buf, const PrimeTables pt, uint32_t pr
     ntt_rounds<true, LOGN, 0, false, 0>(buf, pt.itw2 + ((u64)prime << LOGN), pc, 0u, LOGN, 0, true);
 }
 
+// Two limbs of the same prime transformed together (shared twiddles).
+template <bool INV, int LOGN>
+__device__ __noinline__ void ntt2(u64* b0, u64* b1, const PrimeTables pt, uint32_t prime, const PrimeConst pc) {
+    u64* const bufs[2] = {b0, b1};
+    ntt_rounds_n<INV, LOGN, 0, false, 0, 8, 2>(bufs, (INV ? pt.itw2 : pt.tw2) + ((u64)prime << LOGN), pc, 0u, LOGN,
+                                                0, true);
+}
+
 // Every element-wise pass below gives each thread the positions
 // x_k = threadIdx.x + k * N/8, k < 8, and issues a chunk's global loads before
 // its arithmetic, so several L2 round trips are in flight per thread.
@@ -185,6 +193,188 @@ __device__ void mac_slot(const KsFusedArgs& a, uint32_t s, u64* W, u64* A0, u64*
     }
 }
 
+// The key switch at one Q limb with one special prime (a single digit):
+// nothing leaves shared memory between the input load and the output store.
+//   W = INTT_q0(in), W = BConv(W) to P, W = NTT_P(W); A_h = W * key_h[P];
+//   (A0, A1) = INTT_P; BConv to q0 in place; (A0, A1) = NTT_q0;
+//   out_h = (in * key_h[q0] - A_h) * P^-1 (+ extras), the own digit's product
+//   computed in the same pass. Same residues as the general path.
+template <int LOGN, bool PREP>
+__device__ __forceinline__ void ks_one_limb(const KsFusedArgs& a, u64* W, u64* A0, u64* A1) {
+    constexpr uint32_t N = 1u << LOGN;
+    const uint32_t z = blockIdx.x;
+    const OpTabs& t = a.t;
+    const uint32_t* map = a.f.map;
+    const u64* in = a.arena + a.in.at(z);
+    const PrimeConst pq = t.pt.pc[0], pp = t.pt.pc[t.p_base];
+    const u64 q = pq.q, p = pp.q;
+    // W = INTT_q0(input through the automorphism)
+    {
+        uint32_t g[kPer];
+        u64 v[kPer];
+#pragma unroll
+        for (uint32_t k = 0; k < kPer; ++k) g[k] = gpos(map, pos<LOGN>(k));
+#pragma unroll
+        for (uint32_t k = 0; k < kPer; ++k) v[k] = in[g[k]];
+#pragma unroll
+        for (uint32_t k = 0; k < kPer; ++k) W[padix(pos<LOGN>(k))] = v[k];
+    }
+    __syncthreads();
+    inv_ntt<LOGN>(W, t.pt, 0, pq);
+    // BConv q0 -> P in place (digit 0's only limb), then NTT_P
+    {
+        const u64 w0 = __ldg(t.qhat_inv[0]), w0s = __ldg(t.qhat_inv_sh[0]);
+        const u64 w1 = __ldg(t.qhat_modp[0]), w1s = __ldg(t.qhat_modp_sh[0]);
+#pragma unroll
+        for (uint32_t k = 0; k < kPer; ++k) {
+            const uint32_t e = padix(pos<LOGN>(k));
+            W[e] = csub(mul_shoup_lazy(mul_shoup(W[e], w0, w0s, q), w1, w1s, p), p);
+        }
+    }
+    __syncthreads();
+    fwd_ntt<LOGN>(W, t.pt, t.p_base, pp);
+    // inner product at P
+    {
+        const u64 kofs = (u64)a.key_pbase * N;
+        const ModConst mc = modconst_of(pp);
+#pragma unroll 1
+        for (uint32_t c = 0; c < kPer; c += kChunk) {
+            u64 d[kChunk], rb[kChunk], ra[kChunk];
+#pragma unroll
+            for (uint32_t k = 0; k < kChunk; ++k) d[k] = W[padix(pos<LOGN>(c + k))];
+            if (PREP) {
+                ulonglong2 vb[kChunk], va[kChunk];
+#pragma unroll
+                for (uint32_t k = 0; k < kChunk; ++k) {
+                    const uint32_t x = pos<LOGN>(c + k);
+                    vb[k] = __ldg(a.prep + a.prep_b + kofs + x);
+                    va[k] = __ldg(a.prep + kofs + x);
+                }
+#pragma unroll
+                for (uint32_t k = 0; k < kChunk; ++k) {
+                    rb[k] = mul_shoup_lazy(d[k], vb[k].x, vb[k].y, p);
+                    ra[k] = mul_shoup_lazy(d[k], va[k].x, va[k].y, p);
+                }
+            } else {
+                u64 vb[kChunk], va[kChunk];
+#pragma unroll
+                for (uint32_t k = 0; k < kChunk; ++k) {
+                    const uint32_t x = pos<LOGN>(c + k);
+                    vb[k] = __ldg(a.key + a.evk_b + kofs + x);
+                    va[k] = __ldg(a.key + a.evk_a + kofs + x);
+                }
+#pragma unroll
+                for (uint32_t k = 0; k < kChunk; ++k) {
+                    rb[k] = mul_mod(canon4(d[k], p), vb[k], mc);
+                    ra[k] = mul_mod(canon4(d[k], p), va[k], mc);
+                }
+            }
+#pragma unroll
+            for (uint32_t k = 0; k < kChunk; ++k) {
+                const uint32_t e = padix(pos<LOGN>(c + k));
+                A0[e] = rb[k];
+                A1[e] = ra[k];
+            }
+        }
+    }
+    __syncthreads();
+    ntt2<true, LOGN>(A0, A1, t.pt, t.p_base, pp);
+    // BConv P -> q0 in place on both, then NTT_q0 of both
+    {
+        const u64 w0 = __ldg(t.phat_inv_modp), w0s = __ldg(t.phat_inv_modp_sh);
+        const u64 w1 = __ldg(t.phat_modq), w1s = __ldg(t.phat_modq_sh);
+#pragma unroll
+        for (uint32_t k = 0; k < kPer; ++k) {
+            const uint32_t e = padix(pos<LOGN>(k));
+            A0[e] = csub(mul_shoup_lazy(mul_shoup(A0[e], w0, w0s, p), w1, w1s, q), q);
+            A1[e] = csub(mul_shoup_lazy(mul_shoup(A1[e], w0, w0s, p), w1, w1s, q), q);
+        }
+    }
+    __syncthreads();
+    ntt2<false, LOGN>(A0, A1, t.pt, 0, pq);
+    // out_h = (in * key_h[q0] - A_h) * P^-1, staged in A_h: the input and the
+    // gathered c0 may alias the outputs
+    {
+        const ModConst mc = modconst_of(pq);
+        const u64 pinv = __ldg(t.p_inv_mod_q), pinv_sh = __ldg(t.p_inv_mod_q_sh);
+        const u64* cb = a.arena + (a.f.has_c0 ? a.f.c0.at(z) : 0);
+#pragma unroll 1
+        for (uint32_t c = 0; c < kPer; c += kChunk) {
+            u64 d[kChunk], cv[kChunk], rb[kChunk], ra[kChunk];
+#pragma unroll
+            for (uint32_t k = 0; k < kChunk; ++k) {
+                const uint32_t g = gpos(map, pos<LOGN>(c + k));
+                d[k] = in[g];
+                cv[k] = a.f.has_c0 ? cb[g] : 0;
+            }
+            if (PREP) {
+                ulonglong2 vb[kChunk], va[kChunk];
+#pragma unroll
+                for (uint32_t k = 0; k < kChunk; ++k) {
+                    const uint32_t x = pos<LOGN>(c + k);
+                    vb[k] = __ldg(a.prep + a.prep_b + x);
+                    va[k] = __ldg(a.prep + x);
+                }
+#pragma unroll
+                for (uint32_t k = 0; k < kChunk; ++k) {
+                    rb[k] = mul_shoup_lazy(d[k], vb[k].x, vb[k].y, q);
+                    ra[k] = mul_shoup_lazy(d[k], va[k].x, va[k].y, q);
+                }
+            } else {
+                u64 vb[kChunk], va[kChunk];
+#pragma unroll
+                for (uint32_t k = 0; k < kChunk; ++k) {
+                    const uint32_t x = pos<LOGN>(c + k);
+                    vb[k] = __ldg(a.key + a.evk_b + x);
+                    va[k] = __ldg(a.key + a.evk_a + x);
+                }
+#pragma unroll
+                for (uint32_t k = 0; k < kChunk; ++k) {
+                    rb[k] = mul_mod(d[k], vb[k], mc);
+                    ra[k] = mul_mod(d[k], va[k], mc);
+                }
+            }
+#pragma unroll
+            for (uint32_t k = 0; k < kChunk; ++k) {
+                const uint32_t e = padix(pos<LOGN>(c + k));
+                u64 r0 = mul_shoup(sub_mod(rb[k], canon4(A0[e], q), q), pinv, pinv_sh, q);
+                const u64 r1 = mul_shoup(sub_mod(ra[k], canon4(A1[e], q), q), pinv, pinv_sh, q);
+                if (a.f.has_c0) r0 = add_mod(r0, cv[k], q);
+                A0[e] = r0;
+                A1[e] = r1;
+            }
+        }
+    }
+    __syncthreads();
+    {
+        u64* o0 = a.arena + a.out0.at(z);
+        u64* o1 = a.arena + a.out1.at(z);
+        const u64* x0 = a.arena + (a.f.has_acc ? a.f.acc0.at(z) : 0);
+        const u64* x1 = a.arena + (a.f.has_acc ? a.f.acc1.at(z) : 0);
+#pragma unroll 1
+        for (uint32_t c = 0; c < kPer; c += kChunk) {
+            u64 e0[kChunk], e1[kChunk];
+#pragma unroll
+            for (uint32_t k = 0; k < kChunk; ++k) {
+                const uint32_t x = pos<LOGN>(c + k);
+                e0[k] = a.f.has_acc ? x0[x] : 0;
+                e1[k] = a.f.has_acc ? x1[x] : 0;
+            }
+#pragma unroll
+            for (uint32_t k = 0; k < kChunk; ++k) {
+                const uint32_t x = pos<LOGN>(c + k);
+                u64 r0 = A0[padix(x)], r1 = A1[padix(x)];
+                if (a.f.has_acc) {
+                    r0 = add_mod(r0, e0[k], q);
+                    r1 = add_mod(r1, e1[k], q);
+                }
+                o0[x] = r0;
+                o1[x] = r1;
+            }
+        }
+    }
+}
+
 template <int LOGN, bool PREP>
 __global__ void __launch_bounds__((1u << LOGN) / 8, 1) ks_fused_kernel(const KsFusedArgs a) {
     constexpr uint32_t N = 1u << LOGN;
@@ -197,6 +387,10 @@ __global__ void __launch_bounds__((1u << LOGN) / 8, 1) ks_fused_kernel(const KsF
     const OpTabs& t = a.t;
     const uint32_t l = a.sizeQl, K = a.K;
     const uint32_t* map = a.f.map;
+    if (l == 1 && K == 1) {
+        ks_one_limb<LOGN, PREP>(a, W, A0, A1);
+        return;
+    }
     const u64* in = a.arena + a.in.at(z);
     u64* coef = a.scratch + a.mid.at(z);          // l limbs
     u64* pcoef = coef + ((u64)l << LOGN);         // 2K limbs: INTT of the special accumulators
@@ -226,8 +420,7 @@ __global__ void __launch_bounds__((1u << LOGN) / 8, 1) ks_fused_kernel(const KsF
         mac_slot<LOGN, PREP>(a, l + k, W, A0, A1, in, coef);
         const uint32_t prime = t.p_base + k;
         const PrimeConst pc = t.pt.pc[prime];
-        inv_ntt<LOGN>(A0, t.pt, prime, pc);
-        inv_ntt<LOGN>(A1, t.pt, prime, pc);
+        ntt2<true, LOGN>(A0, A1, t.pt, prime, pc);
         u64* d0 = pcoef + ((u64)(2 * k) << LOGN);
         u64* d1 = pcoef + ((u64)(2 * k + 1) << LOGN);
 #pragma unroll

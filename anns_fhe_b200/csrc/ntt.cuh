@@ -149,40 +149,38 @@ __device__ __forceinline__ u64 canon4(u64 v, u64 q) {
 // every round (8-byte elements, strides 1, 2, 8, 16, 64, ...) hit distinct banks.
 __device__ __forceinline__ uint32_t padix(uint32_t e) { return e + (e >> 4); }
 
-// One round: K consecutive stages on bits [RB, RB + K) of the pass index,
-// 8 / 2^K groups of 2^K values per thread, all shapes compile-time. The
-// round's twiddles are fetched into registers by fetch() before the barrier
-// that precedes the round, so their latency overlaps the barrier wait.
-template <bool INV, int P, int LOGC, bool COL, int RB, int K>
+// One round: K consecutive stages on bits [RB, RB + K) of the pass index.
+// Each of the TILE / EPT threads holds EPT values per round, as EPT / 2^K
+// groups of 2^K; all shapes are compile-time.
+template <bool INV, int P, int LOGC, bool COL, int RB, int K, int EPT>
 struct NttRound {
     static constexpr uint32_t C = 1u << LOGC;
-    static constexpr uint32_t T = (1u << (P + LOGC)) / 8;
+    static constexpr uint32_t T = (1u << (P + LOGC)) / EPT;
     static constexpr uint32_t NK = 1u << K;
-    static constexpr uint32_t GROUPS = 8u >> K;
-    static constexpr uint32_t PER_G = NK - 1;        // twiddles per group: NK >> (s + 1) for stage s
-    static constexpr uint32_t NTW = GROUPS * PER_G;
+    static constexpr uint32_t GROUPS = EPT >> K;
     static constexpr uint32_t STEP_E = COL ? (1u << (RB + LOGC)) : (1u << RB);
 
-    // slot of twiddle m of stage s within a group
+    // slot of twiddle m of stage s among a group's NK - 1 twiddles
     __device__ static constexpr uint32_t slot(int s, uint32_t m) { return (NK >> (s + 1)) - 1 + m; }
 
-    __device__ __forceinline__ static void geo(uint32_t gi, uint32_t tile0, uint32_t& base_b, uint32_t& base_e,
-                                               uint32_t& hb) {
-        const uint32_t r = threadIdx.x + gi * T;
-        uint32_t c, brest;
-        if (COL) { c = r & (C - 1u); brest = r >> LOGC; }
-        else { brest = r & ((1u << (P - K)) - 1u); c = r >> (P - K); }
-        base_b = ((brest >> RB) << (RB + K)) | (brest & ((1u << RB) - 1u));
-        base_e = COL ? ((base_b << LOGC) | c) : ((c << P) | base_b);
-        hb = COL ? 0u : (tile0 + c);   // index bits above the pass
-    }
-
-    __device__ __forceinline__ static void fetch(const ulonglong2* __restrict__ tw, uint32_t tile0, int log_n,
-                                                 int lo_bit, bool last_pass, ulonglong2 (&w)[NTW]) {
+    // Rounds over NB buffers of the same prime at once: each group's
+    // twiddles and addresses are computed once and applied to every buffer.
+    template <int NB>
+    __device__ __forceinline__ static void run_n(u64* const (&sms)[NB], const ulonglong2* __restrict__ tw,
+                                                 const PrimeConst& pc, uint32_t tile0, int log_n, int lo_bit,
+                                                 bool last_pass) {
+        const u64 q = pc.q, q2 = q << 1;
 #pragma unroll
         for (uint32_t gi = 0; gi < GROUPS; ++gi) {
-            uint32_t base_b, base_e, hb;
-            geo(gi, tile0, base_b, base_e, hb);
+            const uint32_t r = threadIdx.x + gi * T;
+            uint32_t c, brest;
+            if (COL) { c = r & (C - 1u); brest = r >> LOGC; }
+            else { brest = r & ((1u << (P - K)) - 1u); c = r >> (P - K); }
+            const uint32_t base_b = ((brest >> RB) << (RB + K)) | (brest & ((1u << RB) - 1u));
+            const uint32_t base_e = COL ? ((base_b << LOGC) | c) : ((c << P) | base_b);
+            const uint32_t hb = COL ? 0u : (tile0 + c);   // index bits above the pass
+            // the group's twiddles, issued before its values are read
+            ulonglong2 w[NK - 1];
 #pragma unroll
             for (int s = 0; s < K; ++s) {
                 const int pb = RB + s;
@@ -190,116 +188,101 @@ struct NttRound {
                 if (INV && last_pass && p == log_n - 1) continue;   // N^-1 stage: constants, no table
                 const uint32_t tb = (1u << (log_n - 1 - p)) + (hb << (P - pb - 1)) + (base_b >> (pb + 1));
 #pragma unroll
-                for (uint32_t m = 0; m < (NK >> (s + 1)); ++m) w[gi * PER_G + slot(s, m)] = __ldg(tw + tb + m);
+                for (uint32_t m = 0; m < (NK >> (s + 1)); ++m) w[slot(s, m)] = __ldg(tw + tb + m);
             }
-        }
-    }
-
-    __device__ __forceinline__ static void run(u64* sm, const PrimeConst& pc, uint32_t tile0, int log_n, int lo_bit,
-                                               bool last_pass, const ulonglong2 (&w)[NTW]) {
-        const u64 q = pc.q, q2 = q << 1;
 #pragma unroll
-        for (uint32_t gi = 0; gi < GROUPS; ++gi) {
-            uint32_t base_b, base_e, hb;
-            geo(gi, tile0, base_b, base_e, hb);
-            // base_e has zeros where j * STEP_E has ones, so
-            // padix(base_e + j * STEP_E) = padix(base_e) + padix(j * STEP_E):
-            // one address per group, compile-time offsets per element
-            u64* const sp = sm + padix(base_e);
-            u64 v[NK];
+            for (int b = 0; b < NB; ++b) {
+                // base_e has zeros where j * STEP_E has ones, so
+                // padix(base_e + j * STEP_E) = padix(base_e) + padix(j * STEP_E):
+                // one address per group, compile-time offsets per element
+                u64* const sp = sms[b] + padix(base_e);
+                u64 v[NK];
 #pragma unroll
-            for (uint32_t j = 0; j < NK; ++j) v[j] = sp[padix(j * STEP_E)];
-            if (!INV) {
+                for (uint32_t j = 0; j < NK; ++j) v[j] = sp[padix(j * STEP_E)];
+                if (!INV) {
 #pragma unroll
-                for (int s = K - 1; s >= 0; --s) {
-#pragma unroll
-                    for (uint32_t m = 0; m < (NK >> (s + 1)); ++m) {
-                        const ulonglong2 ww = w[gi * PER_G + slot(s, m)];
-#pragma unroll
-                        for (uint32_t jj = 0; jj < (1u << s); ++jj) {
-                            const uint32_t j = (m << (s + 1)) | jj;
-                            ct_bfly(v[j], v[j + (1u << s)], ww, q, q2);
-                        }
-                    }
-                }
-            } else {
-#pragma unroll
-                for (int s = 0; s < K; ++s) {
-                    const int p = lo_bit + RB + s;
-                    if (last_pass && p == log_n - 1) {
-#pragma unroll
-                        for (uint32_t j = 0; j < (NK >> 1); ++j) gs_bfly_last(v[j], v[j + (NK >> 1)], pc, q2);
-                    } else {
+                    for (int s = K - 1; s >= 0; --s) {
 #pragma unroll
                         for (uint32_t m = 0; m < (NK >> (s + 1)); ++m) {
-                            const ulonglong2 ww = w[gi * PER_G + slot(s, m)];
+                            const ulonglong2 ww = w[slot(s, m)];
 #pragma unroll
                             for (uint32_t jj = 0; jj < (1u << s); ++jj) {
                                 const uint32_t j = (m << (s + 1)) | jj;
-                                gs_bfly(v[j], v[j + (1u << s)], ww, q, q2);
+                                ct_bfly(v[j], v[j + (1u << s)], ww, q, q2);
+                            }
+                        }
+                    }
+                } else {
+#pragma unroll
+                    for (int s = 0; s < K; ++s) {
+                        const int p = lo_bit + RB + s;
+                        if (last_pass && p == log_n - 1) {
+#pragma unroll
+                            for (uint32_t j = 0; j < (NK >> 1); ++j) gs_bfly_last(v[j], v[j + (NK >> 1)], pc, q2);
+                        } else {
+#pragma unroll
+                            for (uint32_t m = 0; m < (NK >> (s + 1)); ++m) {
+                                const ulonglong2 ww = w[slot(s, m)];
+#pragma unroll
+                                for (uint32_t jj = 0; jj < (1u << s); ++jj) {
+                                    const uint32_t j = (m << (s + 1)) | jj;
+                                    gs_bfly(v[j], v[j + (1u << s)], ww, q, q2);
+                                }
                             }
                         }
                     }
                 }
-            }
 #pragma unroll
-            for (uint32_t j = 0; j < NK; ++j) sp[padix(j * STEP_E)] = v[j];
+                for (uint32_t j = 0; j < NK; ++j) sp[padix(j * STEP_E)] = v[j];
+            }
         }
     }
 };
 
-// Round RD of a pass: forward takes bits high to low, inverse low to high, in
-// rounds of three (the remainder round is smaller).
-template <bool INV, int P, int LOGC, bool COL, int RD>
-struct NttRoundAt {
-    static constexpr int NR = (P + 2) / 3;
-    static constexpr int HI = P - 3 * RD;                       // forward: bits [.., HI)
-    static constexpr int KF = HI >= 3 ? 3 : HI;
-    static constexpr int RBF = HI - KF;
-    static constexpr int RBI = 3 * RD;                          // inverse: bits [RBI, ..)
-    static constexpr int KI = (P - RBI) >= 3 ? 3 : (P - RBI);
-    using R = NttRound<INV, P, LOGC, COL, INV ? RBI : RBF, INV ? KI : KF>;
-};
-
-template <bool INV, int P, int LOGC, bool COL, int RD>
-__device__ __forceinline__ void ntt_rounds_from(u64* sm, const ulonglong2* tw, const PrimeConst& pc, uint32_t tile0,
-                                                int log_n, int lo_bit, bool last_pass,
-                                                const ulonglong2 (&w)[NttRoundAt<INV, P, LOGC, COL, RD>::R::NTW]) {
-    using A = NttRoundAt<INV, P, LOGC, COL, RD>;
-    A::R::run(sm, pc, tile0, log_n, lo_bit, last_pass, w);
-    if constexpr (RD + 1 < A::NR) {
-        using R2 = typename NttRoundAt<INV, P, LOGC, COL, RD + 1>::R;
-        ulonglong2 w2[R2::NTW];
-        R2::fetch(tw, tile0, log_n, lo_bit, last_pass, w2);
+// All rounds of a pass over NB tiles in shared memory (same prime), each
+// round followed by a barrier: forward takes bits high to low, inverse low to
+// high, in rounds of three (the remainder round is smaller).
+template <bool INV, int P, int LOGC, bool COL, int RD, int EPT, int NB>
+__device__ __forceinline__ void ntt_rounds_n(u64* const (&sms)[NB], const ulonglong2* tw, const PrimeConst& pc,
+                                             uint32_t tile0, int log_n, int lo_bit, bool last_pass) {
+    constexpr int NR = (P + 2) / 3;
+    if constexpr (RD < NR) {
+        constexpr int HI = P - 3 * RD;                       // forward: bits [.., HI)
+        constexpr int KF = HI >= 3 ? 3 : HI;
+        constexpr int RBF = HI - KF;
+        constexpr int RBI = 3 * RD;                          // inverse: bits [RBI, ..)
+        constexpr int KI = (P - RBI) >= 3 ? 3 : (P - RBI);
+        NttRound<INV, P, LOGC, COL, INV ? RBI : RBF, INV ? KI : KF, EPT>::template run_n<NB>(
+            sms, tw, pc, tile0, log_n, lo_bit, last_pass);
         __syncthreads();
-        ntt_rounds_from<INV, P, LOGC, COL, RD + 1>(sm, tw, pc, tile0, log_n, lo_bit, last_pass, w2);
-    } else {
-        __syncthreads();
+        ntt_rounds_n<INV, P, LOGC, COL, RD + 1, EPT, NB>(sms, tw, pc, tile0, log_n, lo_bit, last_pass);
     }
 }
 
-// All rounds of a pass over the tile in shared memory (ends with a barrier).
-template <bool INV, int P, int LOGC, bool COL, int RD>
+// One tile.
+template <bool INV, int P, int LOGC, bool COL, int RD, int EPT = 8>
 __device__ __forceinline__ void ntt_rounds(u64* sm, const ulonglong2* tw, const PrimeConst& pc, uint32_t tile0,
                                            int log_n, int lo_bit, bool last_pass) {
-    static_assert(RD == 0, "a pass starts at round 0");
-    using R0 = typename NttRoundAt<INV, P, LOGC, COL, 0>::R;
-    ulonglong2 w[R0::NTW];
-    R0::fetch(tw, tile0, log_n, lo_bit, last_pass, w);
-    ntt_rounds_from<INV, P, LOGC, COL, 0>(sm, tw, pc, tile0, log_n, lo_bit, last_pass, w);
+    u64* const one[1] = {sm};
+    ntt_rounds_n<INV, P, LOGC, COL, RD, EPT, 1>(one, tw, pc, tile0, log_n, lo_bit, last_pass);
 }
 
 // One pass over 2^(P + LOGC)-word tiles: stage the tile in shared memory
 // (through the prologue on the first pass), run the rounds, write it back
 // (through the epilogue on the last pass, canonical residues).
+// Values per thread: 16 for 8192-word tiles (512 threads, two CTAs per SM
+// whose barriers interleave), else 8.
+constexpr int ntt_ept(int P, int LOGC) { return P + LOGC >= 13 ? 16 : 8; }
+
 template <bool INV, int P, int LOGC, bool COL, class Pro, class Epi>
-__global__ void __launch_bounds__((1u << (P + LOGC)) / 8)
+__global__ void __launch_bounds__((1u << (P + LOGC)) / ntt_ept(P, LOGC), ntt_ept(P, LOGC) == 16 ? 2 : 1)
 ntt_kernel(NttGeom g, PrimeTables pt, const LimbJob* __restrict__ jobs, u64* __restrict__ mid,
            const ZBases zb, Pro pro, Epi epi) {
     extern __shared__ u64 sm[];
     constexpr uint32_t C = 1u << LOGC;
     constexpr uint32_t TILE = 1u << (P + LOGC);
-    constexpr uint32_t T = TILE / 8;
+    constexpr int EPT = ntt_ept(P, LOGC);
+    constexpr uint32_t T = TILE / EPT;
     const LimbJob job = jobs[blockIdx.y];
     const uint32_t z = blockIdx.z;
     const u64 zm = zb.mid.at(z);
@@ -320,7 +303,7 @@ ntt_kernel(NttGeom g, PrimeTables pt, const LimbJob* __restrict__ jobs, u64* __r
         sm[padix(e)] = g.first ? pro(job, zb, z, x, pc) : mid[zm + job.dst + x];
     }
     __syncthreads();
-    ntt_rounds<INV, P, LOGC, COL, 0>(sm, tw, pc, tile0, g.log_n, g.lo_bit, g.last != 0);
+    ntt_rounds<INV, P, LOGC, COL, 0, EPT>(sm, tw, pc, tile0, g.log_n, g.lo_bit, g.last != 0);
 #pragma unroll 4
     for (uint32_t e = threadIdx.x; e < TILE; e += T) {
         const uint32_t x = gidx(e);
@@ -374,7 +357,7 @@ inline cudaError_t launch_pass(const NttGeom& g, const PrimeTables& pt, const Li
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
-    kern<<<dim3(ctas, njobs, nz), TILE / 8, smem, st>>>(g, pt, jobs, mid, zb, pro, epi);
+    kern<<<dim3(ctas, njobs, nz), TILE / ntt_ept(P, LOGC), smem, st>>>(g, pt, jobs, mid, zb, pro, epi);
     count_launches(1);
     return cudaSuccess;
 }

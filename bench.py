@@ -197,7 +197,7 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
-def ks_roofline(params, lanes: int, reps: int = 20):
+def ks_roofline(params, lanes: int, reps: int = 20, level: int = 0):
     """The dominant kernel (ks_fused_kernel: the one-kernel key switch, ~88% of
     device time in the launch list) timed alone: one rotation step of `lanes`
     ciphertexts at the top level per launch (one launch per call), five batches
@@ -213,7 +213,8 @@ def ks_roofline(params, lanes: int, reps: int = 20):
     from anns_fhe_b200._lib import CtRef
     from anns_fhe_b200.driver import FheContext
     p = params
-    n, L, K = p.n, p.L, p.K
+    n, K = p.n, p.K
+    L = level or p.L
     w = L * n
     nbuf = 5
     kw = p.key_words()
@@ -224,7 +225,7 @@ def ks_roofline(params, lanes: int, reps: int = 20):
     key = np.concatenate([rng.integers(0, q, n, dtype=np.uint64) for _ in range(2 * p.dnum) for q in allp])
     ctx.write_key(0, key)
     ctx.lib.afhe_add_rotation_key(ctx.h, 1, 0)
-    limb = np.concatenate([rng.integers(0, q, n, dtype=np.uint64) for q in p.q])
+    limb = np.concatenate([rng.integers(0, q, n, dtype=np.uint64) for q in p.q[:L]])
     for i in range((nbuf + 1) * lanes * 2):
         ctx.write_poly(i * w, limb)
 
@@ -251,19 +252,19 @@ def ks_roofline(params, lanes: int, reps: int = 20):
     bytes_per_launch = lanes * 4 * w * 8 + 2 * p.dnum * (L + K) * n * 8
     achieved = bytes_per_launch / (ms * 1e-3) / 1e9
     peak, src = load_peaks()
-    return {"bound": "hbm", "kernel": f"ks_fused_kernel (rotation key switch, N={n}, level {L}, {lanes} ciphertexts/launch)",
+    return {"bound": "hbm", "kernel": f"ks_fused_kernel (rotation key switch, N={n}, {L} limbs, {lanes} ciphertexts/launch)",
             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "peak_source": src, "traffic": None, "ms_per_launch": ms,
             "algorithmic_bytes_per_launch": bytes_per_launch}
 
 
-def profile_ks(lanes: int):
+def profile_ks(lanes: int, level: int = 0):
     """Profiling driver: the roofline measurement of the key-switch kernel alone
-    (six warm-up launches, then 20 measured)."""
+    (five warm-up launches, then 20 measured) at `level` limbs (default: all)."""
     from anns_fhe_b200.driver import CkksParams
     from anns_fhe_b200.workloads import SMALL as spec
     p = CkksParams.generate(spec.log_n, spec.num_q, spec.q_bits, spec.num_p, spec.p_bits, spec.alpha)
-    print(json.dumps(ks_roofline(p, lanes)))
+    print(json.dumps(ks_roofline(p, lanes, level=level)))
 
 
 def profile_step(nq: int):
@@ -342,6 +343,7 @@ def main():
     ap.add_argument("--profile-step", type=int, default=0, help="profiling driver: queries per step")
     ap.add_argument("--profile-ntt", type=int, default=0, help="profiling driver: polynomials per NTT launch")
     ap.add_argument("--profile-ks", type=int, default=0, help="profiling driver: ciphertexts per key-switch launch")
+    ap.add_argument("--level", type=int, default=0, help="limbs for --profile-ks (default: all)")
     ap.add_argument("--log-n", type=int, default=13, help="ring degree for --profile-ntt")
     args = ap.parse_args()
     if args.profile_step:
@@ -349,7 +351,7 @@ def main():
     if args.profile_ntt:
         return profile_ntt(args.profile_ntt, args.log_n)
     if args.profile_ks:
-        return profile_ks(args.profile_ks)
+        return profile_ks(args.profile_ks, args.level)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if args.impl == "reference":
