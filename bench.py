@@ -188,6 +188,12 @@ def run_ours(args, rank: int, world: int):
     return line
 
 
+# ncu --set full of ks_fused_kernel, 148 ciphertexts of N = 8192, 3 + 1 limbs
+# per launch (summary under profiles/)
+KS_TRAFFIC_148 = 107.2e6 + 70.4e6
+KS_FMAHEAVY_FRAC_148 = 0.588
+
+
 def load_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     try:
@@ -249,13 +255,22 @@ def ks_roofline(params, lanes: int, reps: int = 20, level: int = 0):
     launches = ctx.lib.afhe_kernel_launches() - l0
     ms = e0.elapsed_time(e1) / launches
     ctx.close()
-    bytes_per_launch = lanes * 4 * w * 8 + 2 * p.dnum * (L + K) * n * 8
+    key_bytes = 2 * p.dnum * (L + K) * n * 8
+    bytes_per_launch = lanes * 4 * w * 8 + key_bytes
     achieved = bytes_per_launch / (ms * 1e-3) / 1e9
     peak, src = load_peaks()
+    traffic = None
+    if (n, L, K) == (8192, 3, 1):
+        # DRAM read + write of one 148-ciphertext launch from the ncu capture
+        # of this shape under profiles/: 177.6 MB, of which the key (read
+        # once) is key_bytes; the rest grows with the ciphertexts.
+        traffic = (KS_TRAFFIC_148 - key_bytes) * lanes / 148 + key_bytes
     return {"bound": "hbm", "kernel": f"ks_fused_kernel (rotation key switch, N={n}, {L} limbs, {lanes} ciphertexts/launch)",
             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "peak_source": src, "traffic": None, "ms_per_launch": ms,
-            "algorithmic_bytes_per_launch": bytes_per_launch}
+            "peak_source": src, "traffic": traffic, "ms_per_launch": ms,
+            "algorithmic_bytes_per_launch": bytes_per_launch,
+            # the kernel is bound by the integer multiply pipe, not HBM (same capture)
+            "int_pipe": {"pipe": "fmaheavy (IMAD)", "frac": KS_FMAHEAVY_FRAC_148}}
 
 
 def profile_ks(lanes: int, level: int = 0):
