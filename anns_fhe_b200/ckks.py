@@ -258,7 +258,9 @@ class CkksClient:
         have = getattr(self, "_regions", {})
         self._regions = have
         if name not in have or have[name][1] < words:
-            k = -(-words // self.slots.w)
+            # grow at least twofold, so that slowly rising batch sizes do not
+            # leave a trail of outgrown regions behind
+            k = max(-(-words // self.slots.w), 2 * (have[name][1] // self.slots.w if name in have else 0))
             have[name] = (self.slots.take(k)[0], k * self.slots.w)
         return have[name][0]
 

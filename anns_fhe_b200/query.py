@@ -122,6 +122,18 @@ class InteractiveQueryManager:
         for _ in range(self.lanes):
             s = slots.take(8)
             self.work.append(dict(diff=(s[0], s[1]), sq=(s[2], s[3]), tmp=(s[4], s[5]), sel=(s[6], s[7])))
+        # stage 1b: the n_list - 1 masked ciphertexts of each lane's query,
+        # rotated side by side (lvl_out limbs each, packed)
+        w = self.lvl_out * n
+        per_lane = 2 * (shape.n_list - 1) * w
+        base = slots.take(self.compaction_slots(shape.n_list, L, n, slots.w, self.lanes))[0] if per_lane else 0
+        self.cmp = [[(base + k * per_lane + 2 * i * w, base + k * per_lane + (2 * i + 1) * w)
+                     for i in range(shape.n_list - 1)] for k in range(self.lanes)]
+
+    @staticmethod
+    def compaction_slots(n_list: int, L: int, n: int, slot_w: int, lanes: int) -> int:
+        """Slots of the stage-1b buffers: n_list - 1 ciphertexts at L - 2 limbs per lane."""
+        return -(-lanes * 2 * (n_list - 1) * (L - 2) * n // slot_w)
 
     def _prefix(self, count: int) -> int:
         if count not in self.mask_prefix:
@@ -229,13 +241,56 @@ class InteractiveQueryManager:
             while s < D:                     # sq += rot(sq, s)
                 self._rot_acc(sq, sq, s, self.lvl_sq)
                 s <<= 1
-            comp = [q.compact for q in qs]
-            for i in range(self.sh.n_list):
-                shift = i * (D - 1)
-                tgt = comp if i == 0 else sel
-                self._mult_plain(sq, [self.mask_onehot[i]] * len(qs), tgt, self.lvl_sq)
-                if shift:                    # comp += rot(sel, i * (D - 1))
-                    self._rot_acc(sel, comp, shift, self.lvl_out)
+            self._compact(qs, sq)
+
+    def _compact(self, qs: list[QueryRecord], sq) -> None:
+        """Stage 1b for a chunk of queries: compact = sum over i of
+        rot(rescale(sq * mask_i), i * (D - 1)).
+
+        The reference runs the lists one after another, each rotation as
+        eval_rotate's descending power-of-two steps, accumulating as it goes.
+        Here every (query, list) term is masked in one batched operator. The
+        rotations run step by step from the highest power of two down: each
+        step rotates, in one batched launch, every term whose shift has that
+        bit. So each term sees exactly its eval_rotate steps, in the same
+        order, and its residues are the reference's. The terms are then
+        summed pairwise. Modular addition is exact and commutative, so the
+        sum equals the reference's running accumulation word for word. The
+        depth is log2(max shift) rotations plus log2(n_list) additions,
+        instead of one eval_rotate after another."""
+        D, nl = self.sh.D, self.sh.n_list
+        comp = [q.compact for q in qs]
+        src, pts, dst = [], [], []
+        for k in range(len(qs)):
+            for i in range(nl):
+                src.append(sq[k])
+                pts.append(self.mask_onehot[i])
+                dst.append(comp[k] if i == 0 else self.cmp[k][i - 1])
+        self._mult_plain(src, pts, dst, self.lvl_sq)
+        if nl == 1:
+            return
+        terms = [(self.cmp[k][i - 1], i * (D - 1)) for k in range(len(qs)) for i in range(1, nl)]
+        top = max(s for _, s in terms).bit_length()
+        for b in range(top - 1, -1, -1):
+            sub = [ct for ct, s in terms if (s >> b) & 1]
+            if sub:
+                self._rotate(sub, 1 << b, self.lvl_out)
+        # per query: comp += sum of its n_list - 1 rotated terms
+        groups = [[comp[k]] + self.cmp[k] for k in range(len(qs))]
+        self._sum_groups(groups, self.lvl_out)
+
+    def _sum_groups(self, groups, limbs: int) -> None:
+        """groups[g][0] += groups[g][1] + ... , all groups side by side, by
+        pairwise batched additions (depth log2 of the largest group)."""
+        live = [list(g) for g in groups]
+        while any(len(g) > 1 for g in live):
+            a, b = [], []
+            for g in live:
+                for j in range(0, len(g) - 1, 2):
+                    a.append(g[j])
+                    b.append(g[j + 1])
+            self._add(a, b, a, limbs)
+            live = [g[0::2] for g in live]
 
     def stage3_fine(self, queries: list[QueryRecord]) -> None:
         """Stage 3 for every (query, probed list, batch) item, lanes at a time.
@@ -271,24 +326,24 @@ class InteractiveQueryManager:
                 sub = [sel[k] for k, x in enumerate(it) if (x[3] >> b) & 1]
                 if sub:
                     self._rotate(sub, -(1 << b), self.lvl_out)
-            # accumulate: the item at offset 0 starts its query's sum
-            pending = []
-            n = self.p.n
+            # accumulate: each query's items of this chunk are summed pairwise
+            # (exact modular additions, so the order does not change a word);
+            # the chunk holding the query's offset-0 item starts its sum.
+            byq: dict[int, list[int]] = {}
             for k, x in enumerate(it):
-                dst = queries[x[0]].dists
-                if x[3] == 0:
-                    w_ = self.lvl_out * n
-                    L.check(self.lib.afhe_copy_poly(self.ctx.h, dst[0], sel[k][0], w_), "copy_poly")
-                    L.check(self.lib.afhe_copy_poly(self.ctx.h, dst[1], sel[k][1], w_), "copy_poly")
+                byq.setdefault(x[0], []).append(k)
+            self._sum_groups([[sel[k] for k in ks] for ks in byq.values()], self.lvl_out)
+            w_ = self.lvl_out * self.p.n
+            adds = []
+            for qi, ks in byq.items():
+                dst, head = queries[qi].dists, sel[ks[0]]
+                if any(it[k][3] == 0 for k in ks):
+                    L.check(self.lib.afhe_copy_poly(self.ctx.h, dst[0], head[0], w_), "copy_poly")
+                    L.check(self.lib.afhe_copy_poly(self.ctx.h, dst[1], head[1], w_), "copy_poly")
                 else:
-                    pending.append((dst, sel[k]))
-            while pending:
-                seen, now, later = set(), [], []
-                for dst, src in pending:
-                    (later if dst in seen else now).append((dst, src))
-                    seen.add(dst)
-                self._add([d for d, _ in now], [s_ for _, s_ in now], [d for d, _ in now], self.lvl_out)
-                pending = later
+                    adds.append((dst, head))
+            if adds:
+                self._add([d for d, _ in adds], [h for _, h in adds], [d for d, _ in adds], self.lvl_out)
 
     # ---- result transfer ----
     def read_ct(self, ct: tuple[int, int]) -> tuple[np.ndarray, np.ndarray]:

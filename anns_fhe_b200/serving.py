@@ -1,0 +1,287 @@
+"""Serving loop for encrypted IVF-PQ queries: continuous batching on one GPU.
+
+The reference runs one query at a time through InteractiveQueryManager::
+execute_interactive_query (cpp_host_model/src/interactive_query_manager.cpp:
+279-303): stage 1/1b on the server, stage 2 on the client, stage 3 on the
+server, stage 4 on the client. Here many queries are in flight. The
+protocol is the one in docs/interactive_search_protocol.md:13-55.
+
+* Admission. A request that has arrived takes a free query record. A record
+  holds the device-resident ciphertexts of one query: the two encrypted
+  queries at the top level and the two result ciphertexts. The number of
+  records in use is capped by an HBM budget (`budget_bytes` / bytes per
+  query), so a request waits on the host while the budget is spent. Evaluation
+  keys and the index's plaintexts are resident for the loop's whole life.
+* Ticks. Each tick launches, as batched operators on the context stream:
+  - stage 1/1b for the requests admitted since the last tick;
+  - stage 3 for the queries whose lists the client selected at the end of
+    the previous tick.
+  Then the tick copies both kinds of results to the host, and the client
+  decrypts them. Coarse results give each query its lists, and the query
+  runs stage 3 in the next tick. Candidate results give its top-k, and the
+  query's record is freed. A request that arrives while a tick is on the GPU
+  is admitted at the next tick. Its stage 1 then runs in the same launches
+  window as other queries' stage 3.
+* Results are independent of the mix. Each ciphertext's residues are those
+  of the one-ciphertext-at-a-time chain, whatever else shares its launches,
+  so a query's result ciphertexts are bit-identical alone and in any mix.
+* The plain path is the same loop with one lane and one query in flight.
+  That is one ciphertext per launch and one query at a time, as the
+  reference runs it.
+
+Latency is measured on the host from a request's arrival time to the moment
+its top-k is known, with `time.perf_counter`.
+"""
+from __future__ import annotations
+
+import math
+import time
+from collections import deque
+from dataclasses import dataclass, field
+
+import numpy as np
+
+
+@dataclass
+class Request:
+    qid: int
+    arrival: float          # seconds from the start of the trace
+    payload: int            # index into the backend's encrypted-query pool
+
+
+@dataclass
+class Completion:
+    qid: int
+    arrival: float
+    admitted: float
+    done: float
+    probes: list = field(default_factory=list)
+    topk: list = field(default_factory=list)
+    result: np.ndarray | None = None    # (2, lvl_out * N) candidate-distance ciphertext, if kept
+
+    @property
+    def latency(self) -> float:
+        return self.done - self.arrival
+
+    @property
+    def service(self) -> float:
+        """Time from admission to the top-k (no queueing)."""
+        return self.done - self.admitted
+
+
+def poisson_arrivals(rate: float, duration: float, seed: int) -> np.ndarray:
+    """Arrival times (seconds) of a seeded Poisson process of `rate` per second."""
+    rng = np.random.default_rng(seed)
+    n = max(1, int(rate * duration * 1.2) + 16)
+    t = np.cumsum(rng.exponential(1.0 / rate, n))
+    while t[-1] < duration:
+        t = np.concatenate([t, t[-1] + np.cumsum(rng.exponential(1.0 / rate, n))])
+    return t[t < duration]
+
+
+def make_trace(arrivals: np.ndarray, pool: int, seed: int = 0) -> list[Request]:
+    rng = np.random.default_rng(seed)
+    return [Request(i, float(t), int(rng.integers(0, pool))) for i, t in enumerate(arrivals)]
+
+
+def percentile(xs, p: float) -> float:
+    """Nearest-rank percentile (p in [0, 100])."""
+    if not len(xs):
+        return float("nan")
+    s = sorted(xs)
+    k = max(0, min(len(s) - 1, int(math.ceil(p / 100.0 * len(s))) - 1))
+    return float(s[k])
+
+
+class WorkloadBackend:
+    """The server and client of a `workloads.Workload`, driven through the C ABI.
+
+    The encrypted-query pool is held on the host. The client encrypts each
+    distinct query once, and a request's admission copies its four ciphertexts
+    into the record on the context stream. Results come back to the host with
+    one copy per contiguous run of records. The client decrypts them with its
+    secret key, as in the bench's end-to-end step.
+    """
+
+    def __init__(self, wl, Q: np.ndarray | None = None, lanes: int | None = None,
+                 pool: list[list[np.ndarray]] | None = None):
+        """Q: query vectors the client encrypts into the pool; or `pool`:
+        ciphertexts already encrypted, four host arrays (ct_query c0, c1,
+        ct_dim c0, c1) per query."""
+        self.wl = wl
+        self.iqm = wl.iqm
+        self.lib = wl.ctx.lib
+        self.h = wl.ctx.h
+        self.lanes = lanes or wl.iqm.lanes
+        self.records = wl.records
+        self.n = wl.params.n
+        Lw = wl.params.L * self.n
+        self.pool: list[list[np.ndarray]] = list(pool or [])
+        chunk = len(wl.records)
+        for c0 in range(0, 0 if Q is None else len(Q), chunk):
+            part = Q[c0:c0 + chunk]
+            recs = wl.records[:len(part)]
+            wl.encrypt_queries(part, recs)
+            for r in recs:
+                self.pool.append([wl.ctx.read_poly(o, Lw) for o in (*r.ct_query, *r.ct_dim)])
+        w = self.iqm.lvl_out * self.n
+        self.rec_words = 2 * w
+        # device bytes one in-flight query holds: two encrypted queries at L
+        # limbs and two result ciphertexts at lvl_out limbs
+        self.bytes_per_query = (4 * Lw + 2 * self.rec_words) * 8
+
+    def with_lanes(self, lanes: int) -> "WorkloadBackend":
+        """The same server and encrypted-query pool, `lanes` ciphertexts per launch."""
+        other = object.__new__(WorkloadBackend)
+        other.__dict__.update(self.__dict__)
+        other.lanes = lanes
+        return other
+
+    def upload(self, rec, payload: int) -> None:
+        from . import _lib as L
+        for off, a in zip((*rec.ct_query, *rec.ct_dim), self.pool[payload]):
+            L.check(self.lib.afhe_write_poly_async(self.h, off, a.ctypes.data_as(L.P64), a.size), "write_poly_async")
+
+    def coarse(self, recs) -> None:
+        lanes = self.iqm.lanes
+        try:
+            self.iqm.lanes = self.lanes
+            self.iqm.stage1_coarse(recs)
+        finally:
+            self.iqm.lanes = lanes
+
+    def fine(self, recs) -> None:
+        lanes = self.iqm.lanes
+        try:
+            self.iqm.lanes = self.lanes
+            self.iqm.stage3_fine(recs)
+        finally:
+            self.iqm.lanes = lanes
+
+    def fetch(self, kind: str, recs) -> np.ndarray:
+        """(len(recs), 2, lvl_out * N) result ciphertexts, copied to the host."""
+        base = self.iqm._outbox[kind]
+        idx = [(getattr(r, "compact" if kind == "compact" else "dists")[0] - base) // self.rec_words for r in recs]
+        out = np.empty((len(recs), 2, self.rec_words // 2), dtype=np.uint64)
+        order = np.argsort(idx)
+        i = 0
+        while i < len(order):                # one copy per contiguous run of records
+            j = i
+            while j + 1 < len(order) and idx[order[j + 1]] == idx[order[j]] + 1:
+                j += 1
+            first = idx[order[i]]
+            block = self.wl.ctx.read_poly(base + first * self.rec_words, (j - i + 1) * self.rec_words)
+            block = block.reshape(j - i + 1, 2, -1)
+            for k in range(i, j + 1):
+                out[order[k]] = block[k - i]
+            i = j + 1
+        return out
+
+    def select(self, recs, box: np.ndarray) -> None:
+        wl = self.wl
+        coarse = wl.client.decrypt_host_batch(box, self.iqm.lvl_out, self.iqm.out_scale, wl.spec.n_list).real
+        for r, c in zip(recs, coarse):
+            r.probes = list(np.argsort(c, kind="stable")[:wl.spec.nprobe])
+
+    def topk(self, recs, box: np.ndarray) -> list[list[int]]:
+        wl = self.wl
+        m = max(len(r.vids) for r in recs)
+        d = wl.client.decrypt_host_batch(box, self.iqm.lvl_out, self.iqm.out_scale, m).real
+        out = []
+        for r, row in zip(recs, d):
+            order = np.argsort(row[:len(r.vids)], kind="stable")[:wl.spec.top_k]
+            out.append([r.vids[i] for i in order])
+        return out
+
+
+class ServingLoop:
+    """Continuous batching over a backend (see the module docstring).
+
+    backend: an object with `records`, `bytes_per_query`, `upload(rec,
+    payload)`, `coarse(recs)`, `fine(recs)`, `fetch(kind, recs)`,
+    `select(recs, box)` and `topk(recs, box)`; `WorkloadBackend` drives the
+    GPU.
+    budget_bytes: HBM the in-flight queries may hold (None: every record).
+    max_inflight: a further cap on queries in flight (None: no cap).
+    max_admit: queries admitted per tick (None: the backend's lanes).
+    keep_results: keep each query's candidate-distance ciphertext.
+    """
+
+    def __init__(self, backend, budget_bytes: int | None = None, max_inflight: int | None = None,
+                 max_admit: int | None = None, keep_results: bool = False):
+        self.b = backend
+        cap = len(backend.records)
+        if budget_bytes is not None:
+            cap = min(cap, int(budget_bytes // backend.bytes_per_query))
+        if max_inflight is not None:
+            cap = min(cap, max_inflight)
+        if cap < 1:
+            raise ValueError("the HBM budget does not hold one query")
+        self.capacity = cap
+        self.max_admit = max_admit or getattr(backend, "lanes", cap)
+        self.keep = keep_results
+        self.ticks = 0
+        self.tick_log: list[tuple[int, int]] = []      # (admitted, finishing) per tick
+
+    def run(self, trace: list[Request], realtime: bool = True, clock=time.perf_counter) -> list[Completion]:
+        """Serve `trace` (sorted by arrival). With realtime=False every request
+        counts as arrived at once (the order and mixing of a saturated
+        server, used by tests); latencies are then measured from the start."""
+        free = deque(self.b.records[:self.capacity])
+        pending = deque(sorted(trace, key=lambda r: r.arrival))
+        waiting: deque = deque()
+        selected: list = []          # (req, rec, admitted) with probes chosen
+        done: list[Completion] = []
+        t0 = clock()
+        now = lambda: clock() - t0  # noqa: E731
+        while pending or waiting or selected:
+            t = now()
+            while pending and (not realtime or pending[0].arrival <= t):
+                waiting.append(pending.popleft())
+            admit = []
+            while waiting and free and len(admit) < self.max_admit:
+                req = waiting.popleft()
+                admit.append((req, free.popleft(), now()))
+            if not admit and not selected:
+                # idle: wait for the next arrival
+                if pending:
+                    dt = pending[0].arrival - now()
+                    if dt > 0:
+                        time.sleep(min(dt, 0.005))
+                continue
+            self.ticks += 1
+            self.tick_log.append((len(admit), len(selected)))
+            for req, rec, _ in admit:
+                self.b.upload(rec, req.payload)
+            arecs = [rec for _, rec, _ in admit]
+            srecs = [rec for _, rec, _ in selected]
+            if arecs:
+                self.b.coarse(arecs)
+            if srecs:
+                self.b.fine(srecs)
+            cbox = self.b.fetch("compact", arecs) if arecs else None
+            dbox = self.b.fetch("dists", srecs) if srecs else None
+            finishing = selected
+            if arecs:
+                self.b.select(arecs, cbox)
+            if finishing:
+                tops = self.b.topk(srecs, dbox)
+                t_done = now()
+                for k, ((req, rec, adm), top) in enumerate(zip(finishing, tops)):
+                    done.append(Completion(req.qid, req.arrival if realtime else 0.0, adm, t_done,
+                                           list(rec.probes), top, dbox[k].copy() if self.keep else None))
+                    free.append(rec)
+            selected = admit
+        return done
+
+
+def summarize(done: list[Completion], duration: float | None = None) -> dict:
+    """p50/p99 latency (ms) and throughput of a served trace."""
+    if not done:
+        return {"completed": 0}
+    lat = [c.latency * 1e3 for c in done]
+    first = min(c.arrival for c in done)
+    last = max(c.done for c in done)
+    span = duration if duration is not None else max(last - first, 1e-9)
+    return {"completed": len(done), "qps": len(done) / max(last - first, 1e-9), "offered_span_s": span,
+            "p50_ms": percentile(lat, 50), "p99_ms": percentile(lat, 99), "max_ms": max(lat)}

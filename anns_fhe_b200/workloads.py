@@ -64,7 +64,12 @@ class Workload:
         slot_w = (self.params.L + self.params.K) * n
         B = slots // spec.d
         n_batches = sum(-(-len(v) // B) for v in self.index.lists)
-        n_slots = 16 + 1 + spec.n_list + 2 * n_batches + 8 * lanes + 8 * max_queries + 64 + max_queries
+        w_out = (self.params.L - 2) * n
+        most = max(max_queries, lanes)
+        dec_slots = -(-most * 2 * w_out // slot_w) + -(-most * w_out // slot_w)
+        n_slots = (16 + 1 + spec.n_list + 2 * n_batches + 8 * lanes + 8 * max_queries + 64 + max_queries
+                   + InteractiveQueryManager.compaction_slots(spec.n_list, self.params.L, n, slot_w, lanes)
+                   + dec_slots)
         self.ctx = FheContext(self.params, poly_words=n_slots * slot_w,
                               key_words=(2 + 2 * (spec.log_n + 1)) * self.params.key_words() + 4096, device=device,
                               max_batch=lanes)
@@ -74,6 +79,9 @@ class Workload:
         self.steps = self.iqm.rotation_steps()
         self.client.install_keys(self.steps)
         self.records = self.iqm.alloc_queries(max_queries)
+        # the client's decryption staging, sized once for the largest batch
+        self.client._region("dec_in", most * 2 * w_out)
+        self.client._region("dec_out", most * w_out)
         self.ctx.sync()
         self.setup_s = time.time() - t0
 

@@ -179,6 +179,7 @@ def run_ours(args, rank: int, world: int):
         "clocks": summarize_clocks(samples),
         "gpu_launches": int(launches),
     }
+    line["serving"] = serve_leg(args, wl, host_cts, rank)
     line["roofline"] = ks_roofline(wl.params, args.lanes)
     wl.close()
     if world == 1 and rank == 0 and not args.skip_cpu:
@@ -186,6 +187,68 @@ def run_ours(args, rank: int, world: int):
         ref = cpu_reference_rate(steps=1)
         line["cpu_baseline"] = ref["cpu_baseline"]
     return line
+
+
+def serve_leg(args, wl, host_cts, rank: int):
+    """Latency beside throughput: the plain path (one ciphertext per launch,
+    one query at a time) and the continuous-batching server on a seeded
+    Poisson trace, both from the same encrypted queries through the C ABI,
+    host buffers in and out, client decryption included."""
+    from anns_fhe_b200.serving import (Request, ServingLoop, WorkloadBackend, make_trace, percentile,
+                                       poisson_arrivals, summarize)
+    be = WorkloadBackend(wl, pool=host_cts)
+    plain = be.with_lanes(1)
+    nplain = max(1, args.plain_queries)
+    ServingLoop(plain, max_inflight=1).run([Request(0, 0.0, 0)], realtime=False)     # warm-up
+    svc = []
+    for i in range(nplain):
+        c = ServingLoop(plain, max_inflight=1).run([Request(i, 0.0, i % len(host_cts))], realtime=False)[0]
+        svc.append(c.service * 1e3)
+    plain_qps = 1e3 * nplain / sum(svc)
+    rate = args.serve_rate or 10.0 * plain_qps
+    warm = make_trace(poisson_arrivals(rate, 0.3, seed=query_seed_base(rank) + 1), pool=len(host_cts), seed=1)
+    ServingLoop(be).run(warm)
+    trace = make_trace(poisson_arrivals(rate, args.serve_seconds, seed=query_seed_base(rank) + 2),
+                       pool=len(host_cts), seed=2)
+    loop = ServingLoop(be)
+    done = loop.run(trace)
+    s = summarize(done)
+    return {"plain": {"queries_per_s": plain_qps, "p50_ms": percentile(svc, 50), "p99_ms": percentile(svc, 99),
+                      "queries": nplain, "lanes": 1, "inflight": 1},
+            "served": {"offered_qps": rate, "queries_per_s": s["qps"], "p50_ms": s["p50_ms"], "p99_ms": s["p99_ms"],
+                       "completed": s["completed"], "offered": len(trace), "seconds": args.serve_seconds,
+                       "ticks": loop.ticks, "lanes": be.lanes, "max_inflight": loop.capacity,
+                       "trace": f"seeded Poisson arrivals at {rate:.0f} queries/s (10x the plain path's rate "
+                                f"unless --serve-rate is given)"}}
+
+
+def serve_sweep(rates, seconds: float, batch: int):
+    """Serving driver: the plain path's latency and rate, then the served loop
+    at each offered rate for `seconds` (seeded Poisson arrivals); one JSON
+    line per rate."""
+    from anns_fhe_b200.serving import (Request, ServingLoop, WorkloadBackend, make_trace, percentile,
+                                       poisson_arrivals, summarize)
+    from anns_fhe_b200.workloads import Workload
+    wl = Workload(max_queries=batch, lanes=batch)
+    be = WorkloadBackend(wl, wl.queries(batch, seed=77))
+    plain = be.with_lanes(1)
+    ServingLoop(plain, max_inflight=1).run([Request(0, 0.0, 0)], realtime=False)
+    svc = [ServingLoop(plain, max_inflight=1).run([Request(i, 0.0, i)], realtime=False)[0].service * 1e3
+           for i in range(32)]
+    print(json.dumps({"path": "plain", "queries_per_s": 1e3 * len(svc) / sum(svc),
+                      "p50_ms": percentile(svc, 50), "p99_ms": percentile(svc, 99)}), flush=True)
+    ServingLoop(be).run(make_trace(poisson_arrivals(200.0, 0.5, seed=1), pool=batch, seed=1))
+    for r in rates:
+        trace = make_trace(poisson_arrivals(r, seconds, seed=int(r)), pool=batch, seed=int(r) + 1)
+        loop = ServingLoop(be)
+        s = summarize(loop.run(trace))
+        s.update(path="served", offered_qps=r, offered=len(trace), ticks=loop.ticks, seconds=seconds)
+        print(json.dumps(s), flush=True)
+    wl.close()
+
+
+def query_seed_base(rank: int) -> int:
+    return 5000 + 1000 * rank
 
 
 # ncu --set full of ks_fused_kernel, 148 ciphertexts of N = 8192, 3 + 1 limbs
@@ -355,12 +418,18 @@ def main():
     ap.add_argument("--batch", type=int, default=0, help="queries per step (default: 2 x the SM count)")
     ap.add_argument("--lanes", type=int, default=0, help="ciphertexts per launch (default: the batch)")
     ap.add_argument("--skip-cpu", action="store_true", help="omit the cpu_baseline leg")
+    ap.add_argument("--plain-queries", type=int, default=16, help="queries timed on the plain path")
+    ap.add_argument("--serve-rate", type=float, default=0.0, help="served trace rate (default: 10x plain)")
+    ap.add_argument("--serve-seconds", type=float, default=5.0, help="served trace length")
+    ap.add_argument("--serve-sweep", default="", help="serving driver: comma-separated offered rates (queries/s)")
     ap.add_argument("--profile-step", type=int, default=0, help="profiling driver: queries per step")
     ap.add_argument("--profile-ntt", type=int, default=0, help="profiling driver: polynomials per NTT launch")
     ap.add_argument("--profile-ks", type=int, default=0, help="profiling driver: ciphertexts per key-switch launch")
     ap.add_argument("--level", type=int, default=0, help="limbs for --profile-ks (default: all)")
     ap.add_argument("--log-n", type=int, default=13, help="ring degree for --profile-ntt")
     args = ap.parse_args()
+    if args.serve_sweep:
+        return serve_sweep([float(x) for x in args.serve_sweep.split(",")], args.serve_seconds, args.batch or 296)
     if args.profile_step:
         return profile_step(args.profile_step)
     if args.profile_ntt:

@@ -1,0 +1,105 @@
+"""The GPU query chain equals the reference's chain, residue for residue.
+
+The server chain (anns_fhe_b200/query.py) batches ciphertexts across queries,
+lists and candidate batches. It runs the stage-1b rotations step by step across
+all lists, and sums terms pairwise. The reference runs it one ciphertext at a
+time: interactive_query_manager.cpp:85-303, with the semantics of
+generate_interactive_test_vectors.cpp:383-541. For each list, mask, rescale,
+eval_rotate by i (D - 1) and eval_add into a running sum; for each candidate
+batch, the same with -offset.
+
+This test replays that sequential chain on the CPU oracle (the C restatement
+of the reference's HLS kernels) with the very keys, plaintexts and
+encrypted queries the GPU used, read back from the device. It then requires
+the compacted coarse ciphertext and the candidate-distance ciphertext of
+every query to be identical word for word. A small ring (N = 2^10, 8 lists of
+8 dimensions) keeps the oracle fast. The bench's configuration (N = 2^13) runs
+for one query, through the one-kernel key switch.
+"""
+import numpy as np
+import pytest
+
+from anns_fhe_b200.workloads import SMALL, Workload, WorkloadSpec
+from oracle.composite import OracleCKKS
+
+pytestmark = pytest.mark.gpu
+
+TINY = WorkloadSpec("ivfpq_512x8_nlist8_N1024_L3", n_vectors=512, d=8, components=8, sigma=0.1, n_list=8, M=2, K=16,
+                    nprobe=2, top_k=4, log_n=10, num_q=3, q_bits=50, num_p=1, p_bits=60, alpha=1, log_scale=40)
+
+
+def reference_chain(wl, ora, ct, ct_dim, probes):
+    """One query through the reference's sequential chain on the oracle."""
+    iqm, p = wl.iqm, wl.params
+    n, L = p.n, p.L
+    D, B, nl = iqm.sh.D, iqm.sh.B, iqm.sh.n_list
+    kw = p.key_words()
+    half = kw // 2
+
+    def key(off):
+        k = wl.ctx.read_key(off, kw)
+        return k[:half], k[half:]
+    relin = key(0)
+    rot = {s: key(kw * (1 + i)) for i, s in enumerate(sorted(wl.steps))}
+
+    def pt(off, limbs):
+        return wl.ctx.read_poly(off, limbs * n)
+    # stage 1 / 1b
+    diff = ora.eval_sub_plain(ct, pt(iqm.pt_centroids, L), L)
+    sq = ora.eval_mult_relin_rescale(diff, diff, relin, L)
+    s = 1
+    while s < D:
+        sq = ora.eval_add(sq, ora.eval_rotate(sq, s, rot, L - 1), L - 1)
+        s <<= 1
+    comp = None
+    for i in range(nl):
+        sel = ora.eval_mult_plain_rescale(sq, pt(iqm.mask_onehot[i], L - 1), L - 1)
+        if i:
+            sel = ora.eval_rotate(sel, i * (D - 1), rot, L - 2)
+        comp = sel if comp is None else ora.eval_add(comp, sel, L - 2)
+    # stage 3
+    off, acc = 0, None
+    for c in probes:
+        for pt_off, cnt, _ in iqm.batches[c]:
+            diff = ora.eval_sub_plain(ct_dim, pt(pt_off, L), L)
+            sq = ora.eval_mult_relin_rescale(diff, diff, relin, L)
+            s = B
+            while s < D * B:
+                sq = ora.eval_add(sq, ora.eval_rotate(sq, s, rot, L - 1), L - 1)
+                s <<= 1
+            sel = ora.eval_mult_plain_rescale(sq, pt(iqm.mask_prefix[cnt], L - 1), L - 1)
+            if off:
+                sel = ora.eval_rotate(sel, -off, rot, L - 2)
+            acc = sel if acc is None else ora.eval_add(acc, sel, L - 2)
+            off += cnt
+    return comp, acc
+
+
+def run_and_compare(spec, nq, lanes, orc):
+    wl = Workload(spec, max_queries=nq, lanes=lanes)
+    try:
+        p = wl.params
+        n, L = p.n, p.L
+        recs = wl.records[:nq]
+        wl.encrypt_queries(wl.queries(nq, seed=21), recs)
+        ins = [((wl.ctx.read_poly(r.ct_query[0], L * n), wl.ctx.read_poly(r.ct_query[1], L * n)),
+                (wl.ctx.read_poly(r.ct_dim[0], L * n), wl.ctx.read_poly(r.ct_dim[1], L * n))) for r in recs]
+        wl.iqm.stage1_coarse(recs)
+        wl.select(recs)
+        wl.iqm.stage3_fine(recs)
+        ora = OracleCKKS(p.log_n, p.q, p.p, p.alpha, orc)
+        for r, (ct, ct_dim) in zip(recs, ins):
+            comp, acc = reference_chain(wl, ora, ct, ct_dim, r.probes)
+            got_c, got_d = wl.iqm.read_ct(r.compact), wl.iqm.read_ct(r.dists)
+            assert np.array_equal(got_c[0], comp[0]) and np.array_equal(got_c[1], comp[1]), "stage 1b differs"
+            assert np.array_equal(got_d[0], acc[0]) and np.array_equal(got_d[1], acc[1]), "stage 3 differs"
+    finally:
+        wl.close()
+
+
+def test_chain_matches_reference_small_ring(orc):
+    run_and_compare(TINY, nq=3, lanes=4, orc=orc)
+
+
+def test_chain_matches_reference_bench_configuration(orc):
+    run_and_compare(SMALL, nq=1, lanes=8, orc=orc)

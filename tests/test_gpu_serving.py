@@ -1,0 +1,68 @@
+"""Serving loop on the GPU (small configuration: N = 2^13, 4,096 x 64
+database, n_list 32, nprobe 4).
+
+* Each query's result is the same alone and in the mix: the candidate-distance
+  ciphertext a query gets back from the continuous-batching server (several
+  queries admitted per tick, stage 1 of new queries beside stage 3 of earlier
+  ones, 8 ciphertexts per launch) is bit-identical to the one it gets when it
+  is served alone on the plain path (one ciphertext per launch, one query in
+  flight). Decrypted, the two are therefore equal, far inside the CKKS
+  tolerance of 1e-2 used for the plaintext comparison.
+* Probes and top-k equal the plaintext IVF-PQ search.
+* A short real-time Poisson trace completes every request.
+"""
+import numpy as np
+import pytest
+
+from anns_fhe_b200.serving import (Request, ServingLoop, WorkloadBackend, make_trace, poisson_arrivals,
+                                   summarize)
+from anns_fhe_b200.workloads import Workload
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def served():
+    wl = Workload(max_queries=12, lanes=8)
+    Q = wl.queries(10, seed=11)
+    be = WorkloadBackend(wl, Q)
+    yield wl, Q, be
+    wl.close()
+
+
+def test_result_same_alone_and_in_mix(served):
+    wl, Q, be = served
+    trace = [Request(i, 0.0, i) for i in range(len(Q))]
+    loop = ServingLoop(be, max_admit=3, keep_results=True)
+    mix = {c.qid: c for c in loop.run(trace, realtime=False)}
+    assert sorted(mix) == list(range(len(Q)))
+    assert any(a and f for a, f in loop.tick_log), "no tick mixed stage 1 and stage 3"
+    plain = be.with_lanes(1)
+    for req in trace:
+        alone = ServingLoop(plain, max_inflight=1, keep_results=True).run([req], realtime=False)
+        assert len(alone) == 1
+        a, m = alone[0], mix[req.qid]
+        assert a.probes == m.probes
+        assert a.topk == m.topk
+        assert np.array_equal(a.result, m.result), f"query {req.qid}: result differs alone and in the mix"
+
+
+def test_served_topk_matches_plaintext(served):
+    wl, Q, be = served
+    done = ServingLoop(be, max_admit=4).run([Request(i, 0.0, i) for i in range(len(Q))], realtime=False)
+    for c in done:
+        _, probes, _, _, top = wl.plaintext(Q[c.qid])
+        assert c.probes == list(probes)
+        assert c.topk == list(top)
+
+
+def test_realtime_trace_completes(served):
+    wl, Q, be = served
+    trace = make_trace(poisson_arrivals(200.0, 0.5, seed=2), pool=len(Q), seed=3)
+    done = ServingLoop(be).run(trace, realtime=True)
+    assert len(done) == len(trace)
+    s = summarize(done)
+    assert s["p99_ms"] >= s["p50_ms"] > 0
+    for c in done:
+        _, _, _, _, top = wl.plaintext(Q[trace[c.qid].payload])
+        assert c.topk == list(top)

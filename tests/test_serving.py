@@ -1,0 +1,118 @@
+"""Serving loop scheduling on the CPU, with a fake backend that records calls.
+
+Checks the properties the GPU serving path relies on: every request
+completes once; a query runs stage 1 in the tick that admits it and stage 3
+in the next one; the HBM budget caps the queries in flight; arrivals are
+admitted in order; requests that arrive while others are in flight share
+their ticks (the mix); the Poisson trace has the requested rate.
+"""
+import numpy as np
+import pytest
+
+from anns_fhe_b200.serving import (Request, ServingLoop, make_trace, percentile, poisson_arrivals, summarize)
+
+
+class Rec:
+    def __init__(self, i):
+        self.i = i
+        self.probes = []
+        self.vids = []
+
+
+class FakeBackend:
+    def __init__(self, records=8, lanes=4, bytes_per_query=100):
+        self.records = [Rec(i) for i in range(records)]
+        self.lanes = lanes
+        self.bytes_per_query = bytes_per_query
+        self.log = []
+        self.payload = {}
+
+    def upload(self, rec, payload):
+        self.payload[rec.i] = payload
+
+    def coarse(self, recs):
+        self.log.append(("coarse", [r.i for r in recs]))
+
+    def fine(self, recs):
+        self.log.append(("fine", [r.i for r in recs]))
+        assert all(r.probes for r in recs), "stage 3 before selection"
+
+    def ticks(self):
+        """The log grouped by tick: a tick runs stage 1 (if any) then stage 3 (if any)."""
+        out = []
+        for kind, ids in self.log:
+            if kind == "fine" and out and "coarse" in out[-1] and "fine" not in out[-1]:
+                out[-1]["fine"] = ids
+            else:
+                out.append({kind: ids})
+        return out
+
+    def fetch(self, kind, recs):
+        return np.zeros((len(recs), 2, 4), dtype=np.uint64)
+
+    def select(self, recs, box):
+        for r in recs:
+            r.probes = [self.payload[r.i]]
+
+    def topk(self, recs, box):
+        return [[self.payload[r.i]] for r in recs]
+
+
+def test_every_request_completes_in_two_ticks():
+    be = FakeBackend(records=6, lanes=3)
+    loop = ServingLoop(be)
+    trace = [Request(i, 0.0, 100 + i) for i in range(10)]
+    done = loop.run(trace, realtime=False)
+    assert sorted(c.qid for c in done) == list(range(10))
+    # the result is the request's own (payload carried through the record)
+    assert all(c.topk == [100 + c.qid] for c in done)
+    # admission in arrival order, at most `lanes` per tick, in flight <= records
+    admitted = [a for a, _ in loop.tick_log]
+    assert all(a <= 3 for a in admitted) and sum(admitted) == 10
+    assert all(a + f <= 6 for a, f in loop.tick_log)
+    # a query admitted at tick t finishes at tick t + 1
+    assert loop.tick_log[0] == (3, 0)
+    assert all(f == a for (a, _), (_, f) in zip(loop.tick_log, loop.tick_log[1:]))
+
+
+def test_budget_caps_inflight():
+    be = FakeBackend(records=16, lanes=16, bytes_per_query=1000)
+    loop = ServingLoop(be, budget_bytes=4500)
+    assert loop.capacity == 4
+    done = loop.run([Request(i, 0.0, i) for i in range(9)], realtime=False)
+    assert len(done) == 9
+    assert all(a + f <= 4 for a, f in loop.tick_log)
+    with pytest.raises(ValueError):
+        ServingLoop(be, budget_bytes=10)
+
+
+def test_mix_stage1_and_stage3_share_ticks():
+    be = FakeBackend(records=8, lanes=2)
+    loop = ServingLoop(be)
+    loop.run([Request(i, 0.0, i) for i in range(6)], realtime=False)
+    ticks = be.ticks()
+    assert len(ticks) == loop.ticks
+    mixed = [k for k in ticks if "coarse" in k and "fine" in k]
+    assert mixed, "no tick ran stage 1 of new queries beside stage 3 of earlier ones"
+    for k in mixed:
+        assert not set(k["coarse"]) & set(k["fine"])
+
+
+def test_realtime_latency_and_order():
+    be = FakeBackend(records=4, lanes=4)
+    loop = ServingLoop(be)
+    arr = np.array([0.0, 0.001, 0.002, 0.010, 0.011])
+    done = loop.run(make_trace(arr, pool=3, seed=1), realtime=True)
+    assert len(done) == 5
+    for c in done:
+        assert c.done >= c.arrival and c.admitted >= c.arrival - 1e-9
+    s = summarize(done)
+    assert s["completed"] == 5 and s["p99_ms"] >= s["p50_ms"] >= 0
+
+
+def test_poisson_rate_and_percentile():
+    t = poisson_arrivals(200.0, 20.0, seed=4)
+    assert np.all(np.diff(t) > 0) and t[-1] < 20.0
+    assert abs(len(t) / 20.0 - 200.0) < 15.0
+    assert np.array_equal(t, poisson_arrivals(200.0, 20.0, seed=4))
+    assert percentile([1, 2, 3, 4], 50) == 2 and percentile([1, 2, 3, 4], 99) == 4
