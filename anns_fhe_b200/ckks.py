@@ -267,6 +267,12 @@ class CkksClient:
     def decrypt_batch(self, cts, level: int, scale: float, slots: int | None = None) -> np.ndarray:
         """Decrypt ciphertexts resident in poly_gmem; returns (count, slots) slot
         values (all N/2 slots by default)."""
+        return self.enc.decode_batch(self.decrypt_batch_coef(cts, level), scale, slots)
+
+    def decrypt_batch_coef(self, cts, level: int) -> np.ndarray:
+        """The device part of decryption: m = c0 + c1 s, INTT, centred CRT
+        lift on the host; returns (count, N) float64 coefficients (decode
+        them with `enc.decode_batch`)."""
         from . import _lib as L
         n, count = self.p.n, len(cts)
         out = self._region("dec_out", count * level * n)
@@ -282,16 +288,19 @@ class CkksClient:
             coef -= q * (coef > q // 2)
         else:
             coef = np.stack([crt_centered(row, self.p.q[:level]).astype(np.float64) for row in limbs])
-        return self.enc.decode_batch(coef, scale, slots)
+        return coef
 
     def decrypt_host_batch(self, cts: np.ndarray, level: int, scale: float, slots: int | None = None) -> np.ndarray:
         """Decrypt ciphertexts received as a host array (count, 2, level * N)."""
+        return self.enc.decode_batch(self.decrypt_host_batch_coef(cts, level), scale, slots)
+
+    def decrypt_host_batch_coef(self, cts: np.ndarray, level: int) -> np.ndarray:
+        """The device part of `decrypt_host_batch`: (count, N) float64 coefficients."""
         n, count = self.p.n, cts.shape[0]
         w = level * n
         inp = self._region("dec_in", count * 2 * w)
         self.ctx.write_poly(inp, np.ascontiguousarray(cts).ravel())
-        return self.decrypt_batch([(inp + 2 * i * w, inp + (2 * i + 1) * w) for i in range(count)], level, scale,
-                                  slots)
+        return self.decrypt_batch_coef([(inp + 2 * i * w, inp + (2 * i + 1) * w) for i in range(count)], level)
 
     def plaintext(self, values, scale: float, off: int, level: int) -> None:
         """Encode `values` into an evaluation-form plaintext at `off` (level limbs)."""

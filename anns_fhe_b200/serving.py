@@ -14,14 +14,15 @@ protocol is the one in docs/interactive_search_protocol.md:13-55.
   keys and the index's plaintexts are resident for the loop's whole life.
 * Ticks. Each tick launches, as batched operators on the context stream:
   - stage 1/1b for the requests admitted since the last tick;
-  - stage 3 for the queries whose lists the client selected at the end of
-    the previous tick.
-  Then the tick copies both kinds of results to the host, and the client
-  decrypts them. Coarse results give each query its lists, and the query
-  runs stage 3 in the next tick. Candidate results give its top-k, and the
-  query's record is freed. A request that arrives while a tick is on the GPU
-  is admitted at the next tick. Its stage 1 then runs in the same launches
-  window as other queries' stage 3.
+  - stage 3 for the queries whose lists the client selected from the
+    previous tick's results.
+  The client's host work for the previous tick (decoding, list selection,
+  top-k) runs while this tick's stage 1 is on the GPU. Then both kinds of
+  results are copied to the host, and the device part of the client's
+  decryption runs. A query's record is freed once its candidate distances
+  are on the host. A request that arrives while a tick is on the GPU is
+  admitted at the next tick. Its stage 1 then shares the GPU with other
+  queries' stage 3.
 * Results are independent of the mix. Each ciphertext's residues are those
   of the one-ciphertext-at-a-time chain, whatever else shares its launches,
   so a query's result ciphertexts are bit-identical alone and in any mix.
@@ -177,20 +178,33 @@ class WorkloadBackend:
             i = j + 1
         return out
 
-    def select(self, recs, box: np.ndarray) -> None:
+    def receive(self, kind: str, recs) -> dict:
+        """Results of `recs` to the client: the result ciphertexts to the host
+        ("box", (count, 2, lvl_out * N)), then the device part of the
+        client's decryption ("coef", (count, N) coefficients). Synchronous."""
+        box = self.fetch(kind, recs)
+        got = {"box": box, "coef": self.wl.client.decrypt_host_batch_coef(box, self.iqm.lvl_out)}
+        if kind == "dists":     # the record may be reused before the top-k is decoded
+            got["vids"] = [list(r.vids) for r in recs]
+        return got
+
+    def select(self, recs, got: dict) -> None:
+        """Stage 2 on the host: decode the coarse distances, keep the nprobe nearest lists."""
         wl = self.wl
-        coarse = wl.client.decrypt_host_batch(box, self.iqm.lvl_out, self.iqm.out_scale, wl.spec.n_list).real
+        coarse = wl.client.enc.decode_batch(got["coef"], self.iqm.out_scale, wl.spec.n_list).real
         for r, c in zip(recs, coarse):
             r.probes = list(np.argsort(c, kind="stable")[:wl.spec.nprobe])
 
-    def topk(self, recs, box: np.ndarray) -> list[list[int]]:
+    def topk(self, recs, got: dict) -> list[list[int]]:
+        """Stage 4 on the host: decode the candidate distances, rank them."""
         wl = self.wl
-        m = max(len(r.vids) for r in recs)
-        d = wl.client.decrypt_host_batch(box, self.iqm.lvl_out, self.iqm.out_scale, m).real
+        vids = got["vids"]
+        m = max(len(v) for v in vids)
+        d = wl.client.enc.decode_batch(got["coef"], self.iqm.out_scale, m).real
         out = []
-        for r, row in zip(recs, d):
-            order = np.argsort(row[:len(r.vids)], kind="stable")[:wl.spec.top_k]
-            out.append([r.vids[i] for i in order])
+        for v, row in zip(vids, d):
+            order = np.argsort(row[:len(v)], kind="stable")[:wl.spec.top_k]
+            out.append([v[i] for i in order])
         return out
 
 
@@ -198,13 +212,20 @@ class ServingLoop:
     """Continuous batching over a backend (see the module docstring).
 
     backend: an object with `records`, `bytes_per_query`, `upload(rec,
-    payload)`, `coarse(recs)`, `fine(recs)`, `fetch(kind, recs)`,
-    `select(recs, box)` and `topk(recs, box)`; `WorkloadBackend` drives the
+    payload)`, `coarse(recs)`, `fine(recs)`, `receive(kind, recs)`,
+    `select(recs, got)` and `topk(recs, got)`; `WorkloadBackend` drives the
     GPU.
     budget_bytes: HBM the in-flight queries may hold (None: every record).
     max_inflight: a further cap on queries in flight (None: no cap).
     max_admit: queries admitted per tick (None: the backend's lanes).
     keep_results: keep each query's candidate-distance ciphertext.
+
+    A tick, in order: admit arrived requests and launch their stage 1; decode,
+    on the host, the results the previous tick received, while that stage 1
+    runs on the GPU (selections, and the top-k of finished queries); launch
+    stage 3 for the queries just selected; receive this tick's results
+    (device to host, client decryption on the device). A record is freed as
+    soon as its query's candidate distances are on the host.
     """
 
     def __init__(self, backend, budget_bytes: int | None = None, max_inflight: int | None = None,
@@ -221,7 +242,7 @@ class ServingLoop:
         self.max_admit = max_admit or getattr(backend, "lanes", cap)
         self.keep = keep_results
         self.ticks = 0
-        self.tick_log: list[tuple[int, int]] = []      # (admitted, finishing) per tick
+        self.tick_log: list[tuple[int, int]] = []      # (stage-1 queries, stage-3 queries) per tick
 
     def run(self, trace: list[Request], realtime: bool = True, clock=time.perf_counter) -> list[Completion]:
         """Serve `trace` (sorted by arrival). With realtime=False every request
@@ -230,11 +251,12 @@ class ServingLoop:
         free = deque(self.b.records[:self.capacity])
         pending = deque(sorted(trace, key=lambda r: r.arrival))
         waiting: deque = deque()
-        selected: list = []          # (req, rec, admitted) with probes chosen
+        coarse_got = None      # (entries, received) of the last tick's stage 1
+        fine_got = None        # (entries, received) of the last tick's stage 3
         done: list[Completion] = []
         t0 = clock()
         now = lambda: clock() - t0  # noqa: E731
-        while pending or waiting or selected:
+        while pending or waiting or coarse_got or fine_got:
             t = now()
             while pending and (not realtime or pending[0].arrival <= t):
                 waiting.append(pending.popleft())
@@ -242,36 +264,40 @@ class ServingLoop:
             while waiting and free and len(admit) < self.max_admit:
                 req = waiting.popleft()
                 admit.append((req, free.popleft(), now()))
-            if not admit and not selected:
-                # idle: wait for the next arrival
-                if pending:
+            if not admit and not coarse_got and not fine_got:
+                if pending:                      # idle: wait for the next arrival
                     dt = pending[0].arrival - now()
                     if dt > 0:
                         time.sleep(min(dt, 0.005))
                 continue
-            self.ticks += 1
-            self.tick_log.append((len(admit), len(selected)))
+            arecs = [rec for _, rec, _ in admit]
             for req, rec, _ in admit:
                 self.b.upload(rec, req.payload)
-            arecs = [rec for _, rec, _ in admit]
-            srecs = [rec for _, rec, _ in selected]
             if arecs:
                 self.b.coarse(arecs)
+            # host work of the previous tick, overlapping the stage 1 just launched
+            selected = []
+            if coarse_got:
+                entries, got = coarse_got
+                self.b.select([rec for _, rec, _ in entries], got)
+                selected = [(req, rec, adm, list(rec.probes)) for req, rec, adm in entries]
+            if fine_got:
+                entries, got = fine_got
+                tops = self.b.topk([rec for _, rec, _, _ in entries], got)
+                t_done = now()
+                for k, ((req, rec, adm, probes), top) in enumerate(zip(entries, tops)):
+                    done.append(Completion(req.qid, req.arrival if realtime else 0.0, adm, t_done,
+                                           probes, top, got["box"][k].copy() if self.keep else None))
+            srecs = [rec for _, rec, _, _ in selected]
             if srecs:
                 self.b.fine(srecs)
-            cbox = self.b.fetch("compact", arecs) if arecs else None
-            dbox = self.b.fetch("dists", srecs) if srecs else None
-            finishing = selected
-            if arecs:
-                self.b.select(arecs, cbox)
-            if finishing:
-                tops = self.b.topk(srecs, dbox)
-                t_done = now()
-                for k, ((req, rec, adm), top) in enumerate(zip(finishing, tops)):
-                    done.append(Completion(req.qid, req.arrival if realtime else 0.0, adm, t_done,
-                                           list(rec.probes), top, dbox[k].copy() if self.keep else None))
-                    free.append(rec)
-            selected = admit
+            if arecs or srecs:
+                self.ticks += 1
+                self.tick_log.append((len(arecs), len(srecs)))
+            coarse_got = (admit, self.b.receive("compact", arecs)) if arecs else None
+            fine_got = (selected, self.b.receive("dists", srecs)) if srecs else None
+            for rec in srecs:                    # results are on the host: the record is free
+                free.append(rec)
         return done
 
 

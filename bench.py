@@ -75,7 +75,9 @@ def run_ours(args, rank: int, world: int):
         args.batch = 2 * torch.cuda.get_device_properties(dev).multi_processor_count
     if args.lanes <= 0:
         args.lanes = args.batch
-    wl = Workload(max_queries=args.batch, lanes=args.lanes, device=dev)
+    # twice the records of a step: the serving leg keeps one tick's queries
+    # in flight while admitting the next
+    wl = Workload(max_queries=2 * args.batch, lanes=args.lanes, device=dev)
     stream = torch.cuda.ExternalStream(wl.ctx.lib.afhe_stream(wl.ctx.h), device=dev)
     iqm = wl.iqm
     recs = wl.records[:args.batch]
@@ -179,7 +181,7 @@ def run_ours(args, rank: int, world: int):
         "clocks": summarize_clocks(samples),
         "gpu_launches": int(launches),
     }
-    line["serving"] = serve_leg(args, wl, host_cts, rank)
+    line["serving"] = serve_leg(args, wl, [[t.numpy() for t in cts] for cts in pinned], rank)
     line["roofline"] = ks_roofline(wl.params, args.lanes)
     wl.close()
     if world == 1 and rank == 0 and not args.skip_cpu:
@@ -229,8 +231,10 @@ def serve_sweep(rates, seconds: float, batch: int):
     from anns_fhe_b200.serving import (Request, ServingLoop, WorkloadBackend, make_trace, percentile,
                                        poisson_arrivals, summarize)
     from anns_fhe_b200.workloads import Workload
-    wl = Workload(max_queries=batch, lanes=batch)
-    be = WorkloadBackend(wl, wl.queries(batch, seed=77))
+    import torch
+    wl = Workload(max_queries=2 * batch, lanes=batch)
+    pool = WorkloadBackend(wl, wl.queries(batch, seed=77)).pool
+    be = WorkloadBackend(wl, pool=[[torch.from_numpy(a).pin_memory().numpy() for a in cts] for cts in pool])
     plain = be.with_lanes(1)
     ServingLoop(plain, max_inflight=1).run([Request(0, 0.0, 0)], realtime=False)
     svc = [ServingLoop(plain, max_inflight=1).run([Request(i, 0.0, i)], realtime=False)[0].service * 1e3

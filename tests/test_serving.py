@@ -26,8 +26,11 @@ class FakeBackend:
         self.bytes_per_query = bytes_per_query
         self.log = []
         self.payload = {}
+        self.busy = set()      # records whose query's results are not yet on the host
 
     def upload(self, rec, payload):
+        assert rec.i not in self.busy, "record reused while its query is in flight"
+        self.busy.add(rec.i)
         self.payload[rec.i] = payload
 
     def coarse(self, recs):
@@ -41,21 +44,29 @@ class FakeBackend:
         """The log grouped by tick: a tick runs stage 1 (if any) then stage 3 (if any)."""
         out = []
         for kind, ids in self.log:
+            if kind.startswith("receive"):
+                continue
             if kind == "fine" and out and "coarse" in out[-1] and "fine" not in out[-1]:
                 out[-1]["fine"] = ids
             else:
                 out.append({kind: ids})
         return out
 
-    def fetch(self, kind, recs):
-        return np.zeros((len(recs), 2, 4), dtype=np.uint64)
+    def receive(self, kind, recs):
+        self.log.append(("receive-" + kind, [r.i for r in recs]))
+        if kind == "dists":
+            self.busy -= {r.i for r in recs}
+        return {"box": np.zeros((len(recs), 2, 4), dtype=np.uint64), "ids": [r.i for r in recs],
+                "payload": [self.payload[r.i] for r in recs]}
 
-    def select(self, recs, box):
+    def select(self, recs, got):
+        assert got["ids"] == [r.i for r in recs]
         for r in recs:
             r.probes = [self.payload[r.i]]
 
-    def topk(self, recs, box):
-        return [[self.payload[r.i]] for r in recs]
+    def topk(self, recs, got):
+        assert got["ids"] == [r.i for r in recs]
+        return [[p] for p in got["payload"]]
 
 
 def test_every_request_completes_in_two_ticks():
