@@ -502,6 +502,29 @@ int afhe_eval_mult_plain_rescale_batch(afhe_ctx* ctx, const afhe_ct_ref* a, cons
     });
 }
 
+int afhe_rescale_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const afhe_ct_ref* d, uint32_t count, uint32_t limbs) {
+    if (!ctx || (count && (!a || !d))) return fail(ctx, AFHE_E_ARG, "null argument");
+    int rc;
+    if ((rc = check_limbs(ctx, limbs, 2)) || (rc = check_cts(ctx, a, count, limbs)) ||
+        (rc = check_cts(ctx, d, count, limbs - 1)))
+        return rc;
+    // OP 8 on both polynomials (fhe_accel_top.cpp:286-292); the inputs go to
+    // lane temps first, so outputs may alias any input
+    return for_chunks(ctx, count, [&](uint32_t s, uint32_t m) {
+        Offs A(2 * m), T(2 * m), t0(m), t1(m), o0(m), o1(m);
+        for (uint32_t z = 0; z < m; ++z) {
+            t0[z] = lane_temp(ctx, z, 0);
+            t1[z] = lane_temp(ctx, z, 1);
+            A[2 * z] = a[s + z].c0_offset; A[2 * z + 1] = a[s + z].c1_offset;
+            T[2 * z] = t0[z]; T[2 * z + 1] = t1[z];
+            o0[z] = d[s + z].c0_offset; o1[z] = d[s + z].c1_offset;
+        }
+        int r = ew_batch(ctx, EW_COPY, A, nullptr, T, limbs);
+        if (r != AFHE_OK) return r;
+        return rescale_batch(ctx, t0, t1, o0, o1, limbs);
+    });
+}
+
 int afhe_eval_mult_plain_rescale(afhe_ctx* ctx, uint64_t a0, uint64_t a1, uint64_t pt, uint64_t d0, uint64_t d1,
                                  uint32_t limbs) {
     afhe_ct_ref a{a0, a1}, d{d0, d1};

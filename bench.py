@@ -407,6 +407,69 @@ def profile_ntt(polys: int, log_n: int = 13, reps: int = 10):
     ctx.close()
 
 
+def ntt_config(reps: int = 5):
+    """Primitive microbenchmark: forward and inverse NTT over 64 ciphertexts x
+    2 polynomials x 24 limbs at N = 2^16 (one batched call each), CUDA events
+    on the context stream; algorithmic bytes = every limb read and written once."""
+    import torch
+
+    from anns_fhe_b200.primitives import NttBatch
+    wl = NttBatch()
+    st = torch.cuda.ExternalStream(wl.ctx.lib.afhe_stream(wl.ctx.h))
+    peak, src = load_peaks()
+    out = {"workload": "ntt_64ct_x2_x24limbs_N65536", "algorithmic_bytes_per_call": wl.algorithmic_bytes(),
+           "butterflies_per_call": wl.butterflies()}
+    for inv in (False, True):
+        for _ in range(2):
+            wl.transform(inv)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = wl.ctx.lib.afhe_kernel_launches()
+        e0.record(st)
+        for _ in range(reps):
+            wl.transform(inv)
+        e1.record(st)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        gbs = wl.algorithmic_bytes() / (ms * 1e-3) / 1e9
+        out["inverse" if inv else "forward"] = {
+            "ms_per_call": ms, "launches_per_call": (wl.ctx.lib.afhe_kernel_launches() - l0) / reps,
+            "achieved_gbs": gbs, "frac_hbm": gbs / peak, "peak_gbs": peak, "peak_source": src,
+            "gbutterflies_per_s": wl.butterflies() / (ms * 1e-3) / 1e9}
+    wl.close()
+    print(json.dumps(out))
+
+
+def ks_config(reps: int = 3):
+    """Batched hybrid key switching and rotation at N = 2^16 (24 + 8 limbs,
+    dnum 3): 32 ciphertexts at seeded levels 8-24, rotate-and-sum by 2^0..2^14,
+    then rescale; one batched call per level group and step."""
+    import torch
+
+    from anns_fhe_b200.primitives import KeySwitchBatch
+    wl = KeySwitchBatch()
+    st = torch.cuda.ExternalStream(wl.ctx.lib.afhe_stream(wl.ctx.h))
+    wl.run()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = wl.ctx.lib.afhe_kernel_launches()
+    e0.record(st)
+    for _ in range(reps):
+        wl.run()
+    e1.record(st)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    peak, src = load_peaks()
+    byts = wl.algorithmic_bytes_per_step() * len(wl.steps)
+    gbs = byts / (ms * 1e-3) / 1e9
+    print(json.dumps({"workload": "ks_rotate_sum_32ct_N65536_L24_K8_dnum3", "levels": wl.levels,
+                      "level_groups": len(wl.groups()), "ms_per_chain": ms,
+                      "key_switches_per_chain": wl.key_switch_count(),
+                      "key_switches_per_s": wl.key_switch_count() / (ms * 1e-3),
+                      "launches_per_chain": (wl.ctx.lib.afhe_kernel_launches() - l0) / reps,
+                      "algorithmic_bytes_per_chain": byts, "achieved_gbs": gbs, "frac_hbm": gbs / peak,
+                      "peak_gbs": peak, "peak_source": src}))
+    wl.close()
+
+
 def run_reference(args, rank: int, world: int):
     from oracle.chain import cpu_reference_rate
     # one untimed query per worker at most: each takes seconds on a core
@@ -426,12 +489,18 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=0.0, help="served trace rate (default: 10x plain)")
     ap.add_argument("--serve-seconds", type=float, default=5.0, help="served trace length")
     ap.add_argument("--serve-sweep", default="", help="serving driver: comma-separated offered rates (queries/s)")
+    ap.add_argument("--ntt-config", action="store_true", help="NTT microbenchmark driver (64 ct x 2 x 24 limbs, N=2^16)")
+    ap.add_argument("--ks-config", action="store_true", help="batched key-switch driver (32 ct, N=2^16, dnum 3)")
     ap.add_argument("--profile-step", type=int, default=0, help="profiling driver: queries per step")
     ap.add_argument("--profile-ntt", type=int, default=0, help="profiling driver: polynomials per NTT launch")
     ap.add_argument("--profile-ks", type=int, default=0, help="profiling driver: ciphertexts per key-switch launch")
     ap.add_argument("--level", type=int, default=0, help="limbs for --profile-ks (default: all)")
     ap.add_argument("--log-n", type=int, default=13, help="ring degree for --profile-ntt")
     args = ap.parse_args()
+    if args.ntt_config:
+        return ntt_config()
+    if args.ks_config:
+        return ks_config()
     if args.serve_sweep:
         return serve_sweep([float(x) for x in args.serve_sweep.split(",")], args.serve_seconds, args.batch or 296)
     if args.profile_step:

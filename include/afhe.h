@@ -270,6 +270,11 @@ int afhe_eval_sub_plain_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const uint64_
                               uint32_t count, uint32_t limbs);
 int afhe_eval_mult_plain_rescale_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const uint64_t* pt,
                                        const afhe_ct_ref* dst, uint32_t count, uint32_t in_limbs);
+/* Rescale of `count` ciphertexts, in_limbs -> in_limbs - 1: OP 8 (RESCALE) on
+ * c0 and c1 of each (fhe_accel_top.cpp:286-292, FHEHostDriver::rescale at
+ * fhe_host_driver.cpp:239-242), with this level's tables. dst may alias a. */
+int afhe_rescale_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const afhe_ct_ref* dst, uint32_t count,
+                       uint32_t in_limbs);
 
 #ifdef __cplusplus
 }
