@@ -275,7 +275,7 @@ __device__ __forceinline__ void ntt_rounds(u64* sm, const ulonglong2* tw, const 
 constexpr int ntt_ept(int P, int LOGC) { return P + LOGC >= 13 ? 16 : 8; }
 
 template <bool INV, int P, int LOGC, bool COL, class Pro, class Epi>
-__global__ void __launch_bounds__((1u << (P + LOGC)) / ntt_ept(P, LOGC), ntt_ept(P, LOGC) == 16 ? 2 : 1)
+__global__ void __launch_bounds__((1u << (P + LOGC)) / ntt_ept(P, LOGC), 2)
 ntt_kernel(NttGeom g, PrimeTables pt, const LimbJob* __restrict__ jobs, u64* __restrict__ mid,
            const ZBases zb, Pro pro, Epi epi) {
     extern __shared__ u64 sm[];
