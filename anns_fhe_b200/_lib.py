@@ -98,6 +98,7 @@ SIGNATURES = {
     "afhe_write_poly_async": (C.c_int, [CTX, u64, P64, u64]),
     "afhe_read_poly_async": (C.c_int, [CTX, u64, P64, u64]),
     "afhe_copy_poly": (C.c_int, [CTX, u64, u64, u64]),
+    "afhe_read_poly_rows": (C.c_int, [CTX, u64, u64, u64, u64, P64]),
     "afhe_ctx_write_context_tables": (C.c_int, [CTX, u32, C.POINTER(ContextLayout)]),
     "afhe_dispatch": (C.c_int, [CTX, C.POINTER(AccelArgs)]),
     "afhe_set_relin_key": (C.c_int, [CTX, u64]),
@@ -128,6 +129,7 @@ SIGNATURES = {
     "afhe_eval_sub_plain_batch": (C.c_int, [CTX, C.POINTER(CtRef), P64, C.POINTER(CtRef), u32, u32]),
     "afhe_eval_mult_plain_rescale_batch": (C.c_int, [CTX, C.POINTER(CtRef), P64, C.POINTER(CtRef), u32, u32]),
     "afhe_rescale_batch": (C.c_int, [CTX, C.POINTER(CtRef), C.POINTER(CtRef), u32, u32]),
+    "afhe_eval_copy_batch": (C.c_int, [CTX, C.POINTER(CtRef), C.POINTER(CtRef), u32, u32]),
 }
 
 _lib = None

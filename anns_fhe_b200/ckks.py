@@ -56,6 +56,18 @@ class Encoder:
             raise OverflowError("encoded coefficients exceed 62 bits; lower the scale")
         return coef.astype(np.int64)
 
+    def encode_batch(self, values: np.ndarray, scale: float) -> np.ndarray:
+        """encode() for each row of a (count, <= N/2) real array; (count, N) int64."""
+        v = np.asarray(values, dtype=np.complex128)
+        M = np.zeros((v.shape[0], self.n), dtype=np.complex128)
+        M[:, self.t[:v.shape[1]]] = scale * v
+        M[:, self.tc[:v.shape[1]]] = np.conj(scale * v)
+        y = _sfft.fft(M, axis=1, workers=-1) / self.n
+        coef = np.rint((y * np.conj(self.zeta)[None, :]).real)
+        if np.max(np.abs(coef)) >= 2.0**62:
+            raise OverflowError("encoded coefficients exceed 62 bits; lower the scale")
+        return coef.astype(np.int64)
+
     def decode(self, coeffs, scale: float) -> np.ndarray:
         y = np.asarray(coeffs, dtype=np.float64) * self.zeta
         M = self.n * np.fft.ifft(y)
@@ -305,6 +317,22 @@ class CkksClient:
     def plaintext(self, values, scale: float, off: int, level: int) -> None:
         """Encode `values` into an evaluation-form plaintext at `off` (level limbs)."""
         self._put_ntt(off, self.enc.encode(values, scale), level)
+
+
+def encode_plaintexts(ctx: FheContext, enc: Encoder, values: np.ndarray, scale: float, offs, level: int,
+                      chunk: int = 256) -> None:
+    """Server-side encoding of many plaintexts: row i of `values` into the
+    evaluation-form polynomial at offs[i] (level limbs); host FFTs in chunks,
+    one batched NTT per chunk on the device."""
+    from . import _lib as L
+    primes = [np.int64(q) for q in ctx.params.q[:level]]
+    for c0 in range(0, len(offs), chunk):
+        rows = enc.encode_batch(values[c0:c0 + chunk], scale)
+        part = list(offs[c0:c0 + chunk])
+        for coef, off in zip(rows, part):
+            ctx.write_poly(off, np.concatenate([np.mod(coef, q).astype(np.uint64) for q in primes]))
+        arr = (L.u64 * len(part))(*part)
+        L.check(ctx.lib.afhe_ntt_batch(ctx.h, arr, len(part), level, 0), "ntt_batch")
 
 
 def encode_plaintext(ctx: FheContext, enc: Encoder, values, scale: float, off: int, level: int) -> None:

@@ -456,6 +456,20 @@ int afhe_read_key(afhe_ctx* c, uint64_t o, uint64_t* d, uint64_t n) { return are
 int afhe_write_poly_async(afhe_ctx* c, uint64_t o, const uint64_t* s, uint64_t n) { return arena_copy(c, true, true, o, (void*)s, n, true); }
 int afhe_read_poly_async(afhe_ctx* c, uint64_t o, uint64_t* d, uint64_t n) { return arena_copy(c, true, false, o, d, n, true); }
 
+int afhe_read_poly_rows(afhe_ctx* ctx, uint64_t off, uint64_t stride, uint64_t rows, uint64_t row_words,
+                        uint64_t* dst) {
+    if (!ctx || (rows && !dst)) return fail(ctx, AFHE_E_ARG, "null argument");
+    if (rows == 0 || row_words == 0) return AFHE_OK;
+    if (stride < row_words) return fail(ctx, AFHE_E_ARG, "row stride shorter than a row");
+    if (rows > 1 && stride > (~0ull - row_words) / (rows - 1)) return fail(ctx, AFHE_E_RANGE, "rows out of range");
+    const u64 span = (rows - 1) * stride + row_words;
+    if (!range_ok(off, span, ctx->prm.poly_words)) return fail(ctx, AFHE_E_RANGE, "rows out of poly_gmem");
+    CK(cudaMemcpy2DAsync(dst, row_words * 8, ctx->poly + off, stride * 8, row_words * 8, rows,
+                         cudaMemcpyDeviceToHost, ctx->st));
+    CK(cudaStreamSynchronize(ctx->st));
+    return AFHE_OK;
+}
+
 int afhe_copy_poly(afhe_ctx* ctx, uint64_t dst, uint64_t src, uint64_t count) {
     if (!ctx) return fail(nullptr, AFHE_E_ARG, "null context");
     if (!range_ok(src, count, ctx->prm.poly_words) || !range_ok(dst, count, ctx->prm.poly_words))

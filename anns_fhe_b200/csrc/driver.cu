@@ -591,6 +591,21 @@ int afhe_eval_add_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const afhe_ct_ref* 
     });
 }
 
+int afhe_eval_copy_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const afhe_ct_ref* d, uint32_t count, uint32_t limbs) {
+    if (!ctx || (count && (!a || !d))) return fail(ctx, AFHE_E_ARG, "null argument");
+    int rc;
+    if ((rc = check_limbs(ctx, limbs, 1)) || (rc = check_cts(ctx, a, count, limbs)) || (rc = check_cts(ctx, d, count, limbs)))
+        return rc;
+    return for_chunks(ctx, count, [&](uint32_t s, uint32_t m) {
+        Offs A(2 * m), D(2 * m);
+        for (uint32_t z = 0; z < m; ++z) {
+            A[2 * z] = a[s + z].c0_offset; A[2 * z + 1] = a[s + z].c1_offset;
+            D[2 * z] = d[s + z].c0_offset; D[2 * z + 1] = d[s + z].c1_offset;
+        }
+        return ew_batch(ctx, EW_COPY, A, nullptr, D, limbs);
+    });
+}
+
 int afhe_eval_sub_plain_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const uint64_t* pt, const afhe_ct_ref* d,
                               uint32_t count, uint32_t limbs) {
     if (!ctx || (count && (!a || !pt || !d))) return fail(ctx, AFHE_E_ARG, "null argument");

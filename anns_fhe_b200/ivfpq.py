@@ -27,17 +27,56 @@ def gaussian_mixture(n: int, d: int, components: int, sigma: float, seed: int) -
     return (centers[lab] + rng.normal(0.0, sigma, (n, d))).astype(np.float32)
 
 
-def kmeans(X: np.ndarray, k: int, iters: int, seed: int, tol: float = 1e-5) -> np.ndarray:
+def _sqdist_argmin(X: np.ndarray, C: np.ndarray, chunk: int = 65536) -> np.ndarray:
+    """argmin_j ||x_i - c_j||^2 in float64, in row chunks (bounded memory)."""
+    X = np.asarray(X)
+    C = C.astype(np.float64)
+    cc = (C * C).sum(1)[None, :]
+    out = np.empty(len(X), dtype=np.int64)
+    for s in range(0, len(X), chunk):
+        x = X[s:s + chunk].astype(np.float64)
+        d2 = (x * x).sum(1)[:, None] + cc - 2 * x @ C.T
+        out[s:s + chunk] = np.argmin(d2, axis=1)
+    return out
+
+
+def farthest_init(X: np.ndarray, k: int, rng) -> np.ndarray:
+    """Farthest-point seeding: a random first centre, then each next centre is
+    the point farthest from the centres chosen so far. On a well-separated
+    mixture with k components it puts one centre in every component."""
+    # float32 on a sample of at most 32 points per centre is plenty to seed
+    if len(X) > 32 * k:
+        X = X[np.sort(rng.choice(len(X), 32 * k, replace=False))]
+    X = X.astype(np.float32)
+    C = np.empty((k, X.shape[1]), dtype=np.float32)
+    xx = (X * X).sum(1)
+    C[0] = X[rng.integers(len(X))]
+    d2 = xx + C[0] @ C[0] - 2 * X @ C[0]
+    for i in range(1, k):
+        C[i] = X[int(np.argmax(d2))]
+        d2 = np.minimum(d2, xx + C[i] @ C[i] - 2 * X @ C[i])
+    return C.astype(np.float64)
+
+
+def kmeans(X: np.ndarray, k: int, iters: int, seed: int, tol: float = 1e-5, init: str = "random") -> np.ndarray:
+    """Lloyd's k-means: seeded random-choice initialisation (the reference's,
+    ivf_quantizer.py:19-82) or farthest-point seeding; empty clusters
+    reseeded from a random point."""
     rng = np.random.default_rng(seed)
     X = X.astype(np.float64)
-    C = X[rng.choice(len(X), size=k, replace=False)].copy()
+    if init == "farthest":
+        C = farthest_init(X, k, rng)
+    else:
+        C = X[rng.choice(len(X), size=k, replace=False)].copy()
     for _ in range(iters):
-        d2 = (X * X).sum(1)[:, None] + (C * C).sum(1)[None, :] - 2 * X @ C.T
-        lab = np.argmin(d2, axis=1)
+        lab = _sqdist_argmin(X, C)
+        cnt = np.bincount(lab, minlength=k)
         newC = np.zeros_like(C)
-        for i in range(k):
-            m = lab == i
-            newC[i] = X[m].mean(0) if m.any() else X[rng.integers(len(X))]
+        np.add.at(newC, lab, X) if len(X) < 4096 else _scatter_sum(newC, lab, X)
+        for i in np.nonzero(cnt == 0)[0]:
+            newC[i] = X[rng.integers(len(X))]
+        nz = cnt > 0
+        newC[nz] /= cnt[nz, None]
         done = np.allclose(C, newC, atol=tol)
         C = newC
         if done:
@@ -45,11 +84,17 @@ def kmeans(X: np.ndarray, k: int, iters: int, seed: int, tol: float = 1e-5) -> n
     return C.astype(np.float32)
 
 
+def _scatter_sum(out: np.ndarray, lab: np.ndarray, X: np.ndarray) -> None:
+    """out[lab[i]] += X[i], by sorting (faster than np.add.at for large inputs)."""
+    order = np.argsort(lab, kind="stable")
+    ls = lab[order]
+    starts = np.concatenate([[0], np.nonzero(np.diff(ls))[0] + 1])
+    sums = np.add.reduceat(X[order], starts, axis=0)
+    out[ls[starts]] = sums
+
+
 def assign(X: np.ndarray, C: np.ndarray) -> np.ndarray:
-    X = X.astype(np.float64)
-    C = C.astype(np.float64)
-    d2 = (X * X).sum(1)[:, None] + (C * C).sum(1)[None, :] - 2 * X @ C.T
-    return np.argmin(d2, axis=1).astype(np.int32)
+    return _sqdist_argmin(X, C).astype(np.int32)
 
 
 @dataclass
@@ -77,19 +122,33 @@ class IvfPqIndex:
         return rec
 
     @classmethod
-    def train(cls, X: np.ndarray, n_list: int, M: int, K: int, seed: int, iters: int = 25) -> "IvfPqIndex":
-        C = kmeans(X, n_list, iters, seed)
+    def train(cls, X: np.ndarray, n_list: int, M: int, K: int, seed: int, iters: int = 25,
+              train_sample: int | None = None, pq_sample: int | None = None,
+              init: str = "random") -> "IvfPqIndex":
+        """IVF k-means, then residual PQ. With `train_sample` (`pq_sample`),
+        the IVF (PQ) k-means run on a seeded sample of that many vectors;
+        every vector is then assigned and encoded (training on a sample, as
+        large IVF-PQ builds do)."""
+        T = X
+        if train_sample and train_sample < len(X):
+            T = X[np.sort(np.random.default_rng(seed + 99).choice(len(X), train_sample, replace=False))]
+        C = kmeans(T, n_list, iters, seed, init=init)
         lab = assign(X, C)
+        tlab = lab if T is X else assign(T, C)
         R = X - C[lab]
+        RT = R if T is X else T - C[tlab]
+        if pq_sample and pq_sample < len(RT):
+            RT = RT[np.sort(np.random.default_rng(seed + 98).choice(len(RT), pq_sample, replace=False))]
         d = X.shape[1]
         sd = d // M
         books = np.zeros((M, K, sd), dtype=np.float32)
         codes = np.zeros((len(X), M), dtype=np.uint8)
         for m in range(M):
-            sub = R[:, m * sd:(m + 1) * sd]
-            books[m] = kmeans(sub, K, iters, seed + 1 + m)
-            codes[:, m] = assign(sub, books[m])
-        lists = [np.nonzero(lab == c)[0].tolist() for c in range(n_list)]
+            books[m] = kmeans(RT[:, m * sd:(m + 1) * sd], K, iters, seed + 1 + m)
+            codes[:, m] = assign(R[:, m * sd:(m + 1) * sd], books[m])
+        order = np.argsort(lab, kind="stable")
+        bounds = np.searchsorted(lab[order], np.arange(n_list + 1))
+        lists = [order[bounds[c]:bounds[c + 1]].tolist() for c in range(n_list)]
         return cls(C, books, lab, codes, lists)
 
 

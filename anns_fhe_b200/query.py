@@ -17,6 +17,19 @@ the context's max_batch per launch; one lane of context scratch each): several q
 several (query, list, batch) items in stage 3. Each ciphertext's residues are
 the ones the one-at-a-time chain produces. `lanes=1` is the plain path.
 
+Two compactions:
+  * "reference": the chain above, verbatim, for indexes whose centroids fit
+    one ciphertext (n_list * D <= slots);
+  * "packed", for larger indexes: the centroids span n_coarse = n_list /
+    (slots / D) ciphertexts, centroid k * (slots / D) + c at slot c * D of
+    coarse ciphertext k. Each coarse ciphertext's tree sum is masked at every
+    slot c * D at once, rescaled, rotated right by k and summed, so one
+    ciphertext returns all n_list distances (list k * (slots / D) + c at slot
+    c * D + k). That takes n_coarse key switches per query instead of the
+    reference's sum over lists of popcount(i * (D - 1)).
+Candidate distances past `slots` continue in further result ciphertexts
+(candidate p at slot p mod slots of result p // slots).
+
 Phase-3 candidate plaintexts depend only on the index, so they are encoded
 once and stay resident in HBM (poly_gmem), as do the masks.
 """
@@ -27,7 +40,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _lib as L
-from .ckks import Encoder, Slots, encode_plaintext
+from .ckks import Encoder, Slots, encode_plaintext, encode_plaintexts
 from .driver import FheContext, FHEHostDriver
 from .ivfpq import IvfPqIndex
 
@@ -42,10 +55,26 @@ class QueryShape:
     nprobe: int
     top_k: int
     scale: float
+    compaction: str = "reference"
 
     @property
     def B(self) -> int:
         return self.slots // self.D
+
+    @property
+    def per_ct(self) -> int:
+        """Centroids per coarse ciphertext (one every D slots)."""
+        return self.slots // self.D
+
+    @property
+    def n_coarse(self) -> int:
+        return -(-self.n_list // self.per_ct)
+
+    def coarse_slot(self, lst: int) -> int:
+        """Slot of list `lst`'s distance in the compacted coarse ciphertext."""
+        if self.compaction == "reference":
+            return lst
+        return (lst % self.per_ct) * self.D + lst // self.per_ct
 
 
 @dataclass
@@ -53,9 +82,10 @@ class QueryRecord:
     ct_query: tuple[int, int]
     ct_dim: tuple[int, int]
     compact: tuple[int, int]
-    dists: tuple[int, int]
+    dists: tuple[int, int]                          # the first result ciphertext
     probes: list = field(default_factory=list)
-    vids: list = field(default_factory=list)       # slot -> vector id (stage 3 order)
+    vids: list = field(default_factory=list)       # candidate position -> vector id (stage 3 order)
+    results: list = field(default_factory=list)    # every result ciphertext (dists first)
 
 
 def pow2_steps(x: int) -> list[int]:
@@ -78,62 +108,90 @@ class InteractiveQueryManager:
         self.enc = Encoder(self.p.log_n)
         self.slots = slots
         self.lanes = max(1, min(lanes, MAX_LANES, ctx.max_batch))
-        assert shape.n_list * shape.D <= shape.slots, "centroids do not fit one ciphertext"
+        if shape.compaction == "reference":
+            assert shape.n_list * shape.D <= shape.slots, "centroids do not fit one ciphertext"
+        else:
+            assert shape.compaction == "packed" and shape.n_coarse <= shape.D, "unsupported compaction"
         L, n = self.L, self.p.n
         self.lvl_sq = L - 1          # after the first rescale
         self.lvl_out = L - 2         # after the mask rescale
         # scale of the results: Delta^2 / q_{L-1}; masks carry q_{L-2} so the second rescale keeps it
         self.out_scale = shape.scale * shape.scale / self.p.q[L - 1]
         mask_scale = float(self.p.q[L - 2])
-        D = shape.D
-        # ---- resident plaintexts ----
-        self.pt_centroids = slots.take(1)[0]
-        vals = np.zeros(shape.slots)
-        for c in range(index.n_list):
-            vals[c * D:(c + 1) * D] = index.centroids[c]
-        encode_plaintext(ctx, self.enc, vals, shape.scale, self.pt_centroids, L)
-        self.mask_onehot = []
-        for i in range(shape.n_list):
-            off = slots.take(1)[0]
-            m = np.zeros(shape.slots)
-            m[i * D] = 1.0
-            encode_plaintext(ctx, self.enc, m, mask_scale, off, self.lvl_sq)
-            self.mask_onehot.append(off)
         self._mask_scale = mask_scale
+        D, S = shape.D, shape.slots
+        # the client decrypts results from limb 0 alone: every decrypted
+        # coefficient (a distance times out_scale, plus noise) must stay well
+        # inside +-q_0 / 2; distances are at most (|q| + |x|)^2 <= 4 max |x|^2
+        bound = 4.0 * float(np.max((index.centroids.astype(np.float64) ** 2).sum(1))) * 4.0 + 64.0
+        assert bound * self.out_scale * 4 < self.p.q[0] / 2, "results would not decrypt from limb 0"
+        # ---- resident plaintexts ----
+        self.pt_centroid_cts = slots.take(shape.n_coarse)
+        self.pt_centroids = self.pt_centroid_cts[0]
+        vals = np.zeros((shape.n_coarse, S))
+        for c in range(index.n_list):
+            k, j = divmod(c, shape.per_ct)
+            vals[k, j * D:(j + 1) * D] = index.centroids[c]
+        encode_plaintexts(ctx, self.enc, vals, shape.scale, self.pt_centroid_cts, L)
+        self.mask_onehot = []
+        if shape.compaction == "reference":
+            m = np.zeros((shape.n_list, S))
+            m[np.arange(shape.n_list), np.arange(shape.n_list) * D] = 1.0
+            self.mask_onehot = slots.take(shape.n_list)
+            encode_plaintexts(ctx, self.enc, m, mask_scale, self.mask_onehot, self.lvl_sq)
+        else:
+            m = np.zeros((1, S))
+            m[0, np.arange(shape.per_ct) * D] = 1.0
+            self.mask_stride = slots.take(1)[0]
+            encode_plaintexts(ctx, self.enc, m, mask_scale, [self.mask_stride], self.lvl_sq)
         self.mask_prefix: dict[int, int] = {}
-        self.batches: list[list[tuple[int, int, list]]] = []
         B = shape.B
+        self.batches: list[list[tuple[int, int, list]]] = []
+        counts, vals, offs = set(), [], []
         for c in range(index.n_list):
             vl = index.lists[c]
             out = []
             for b0 in range(0, len(vl), B):
                 vids = vl[b0:b0 + B]
-                rec = index.reconstruct(vids)
-                packed = np.zeros(shape.slots)
-                for j in range(len(vids)):
-                    packed[np.arange(D) * B + j] = rec[j]
+                rec = index.reconstruct(vids)           # (cnt, D)
+                packed = np.zeros((D, B))
+                packed[:, :len(vids)] = rec.T             # slot d * B + j = x_j[d]
                 off = slots.take(1)[0]
-                encode_plaintext(ctx, self.enc, packed, shape.scale, off, L)
+                vals.append(packed.ravel())
+                offs.append(off)
                 out.append((off, len(vids), list(vids)))
-                self._prefix(len(vids))
+                counts.add(len(vids))
+                if len(vals) == 256:
+                    encode_plaintexts(ctx, self.enc, np.stack(vals), shape.scale, offs, L)
+                    vals, offs = [], []
             self.batches.append(out)
+        if vals:
+            encode_plaintexts(ctx, self.enc, np.stack(vals), shape.scale, offs, L)
+        for cnt in sorted(counts):
+            self._prefix(cnt)
+        # result ciphertexts per query: enough for the nprobe largest lists
+        most = sum(sorted((len(v) for v in index.lists), reverse=True)[:shape.nprobe])
+        self.n_res = max(1, -(-most // S))
         # ---- per-lane working ciphertexts ----
         self.work = []
         for _ in range(self.lanes):
             s = slots.take(8)
             self.work.append(dict(diff=(s[0], s[1]), sq=(s[2], s[3]), tmp=(s[4], s[5]), sel=(s[6], s[7])))
-        # stage 1b: the n_list - 1 masked ciphertexts of each lane's query,
-        # rotated side by side (lvl_out limbs each, packed)
-        w = self.lvl_out * n
-        per_lane = 2 * (shape.n_list - 1) * w
-        base = slots.take(self.compaction_slots(shape.n_list, L, n, slots.w, self.lanes))[0] if per_lane else 0
-        self.cmp = [[(base + k * per_lane + 2 * i * w, base + k * per_lane + (2 * i + 1) * w)
-                     for i in range(shape.n_list - 1)] for k in range(self.lanes)]
+        # stage 1b (reference compaction): the n_list - 1 masked ciphertexts of
+        # each lane's query, rotated side by side (lvl_out limbs each, packed)
+        self.cmp = []
+        if shape.compaction == "reference" and shape.n_list > 1:
+            w = self.lvl_out * n
+            per_lane = 2 * (shape.n_list - 1) * w
+            base = slots.take(self.compaction_slots(shape.n_list, L, n, slots.w, self.lanes))[0]
+            self.cmp = [[(base + k * per_lane + 2 * i * w, base + k * per_lane + (2 * i + 1) * w)
+                         for i in range(shape.n_list - 1)] for k in range(self.lanes)]
 
     @staticmethod
     def compaction_slots(n_list: int, L: int, n: int, slot_w: int, lanes: int) -> int:
-        """Slots of the stage-1b buffers: n_list - 1 ciphertexts at L - 2 limbs per lane."""
-        return -(-lanes * 2 * (n_list - 1) * (L - 2) * n // slot_w)
+        """Slots of the stage-1b buffers of the reference compaction: n_list - 1
+        ciphertexts at L - 2 limbs per lane."""
+        return -(-lanes * 2 * max(n_list - 1, 0) * (L - 2) * n // slot_w)
 
     def _prefix(self, count: int) -> int:
         if count not in self.mask_prefix:
@@ -152,8 +210,12 @@ class InteractiveQueryManager:
             steps.add(s)            # coarse tree sum
             steps.add(B * s)        # fine tree sum
             s <<= 1
-        for i in range(self.sh.n_list):
-            steps.update(pow2_steps(i * (D - 1)))
+        if self.sh.compaction == "reference":
+            for i in range(self.sh.n_list):
+                steps.update(pow2_steps(i * (D - 1)))
+        else:
+            for k in range(1, self.sh.n_coarse):
+                steps.update(-x for x in pow2_steps(k))
         top = max_candidates or self.sh.slots
         s = 1
         while s < top:
@@ -163,30 +225,62 @@ class InteractiveQueryManager:
 
     def new_query(self) -> QueryRecord:
         s = self.slots.take(8)
-        return QueryRecord((s[0], s[1]), (s[2], s[3]), (s[4], s[5]), (s[6], s[7]))
+        return QueryRecord((s[0], s[1]), (s[2], s[3]), (s[4], s[5]), (s[6], s[7]), results=[(s[6], s[7])])
 
     def alloc_queries(self, count: int) -> list[QueryRecord]:
-        """Records whose results (compacted coarse distances, candidate
-        distances; level lvl_out) are packed back to back in two outboxes, so
-        each reaches the host in one copy (read_outbox)."""
+        """Records whose results (compacted coarse distances; n_res candidate
+        ciphertexts; level lvl_out) are packed back to back in two outboxes, so
+        limb 0 of many reaches the host in one copy (read_results)."""
         w = self.lvl_out * self.p.n
-        k = -(-2 * count * w // self.slots.w)
-        comp = self.slots.take(k)[0]
-        dist = self.slots.take(k)[0]
+        comp = self.slots.take(-(-2 * count * w // self.slots.w))[0]
+        dist = self.slots.take(-(-2 * count * self.n_res * w // self.slots.w))[0]
         recs = []
         for i in range(count):
             s = self.slots.take(4)
+            res = [(dist + 2 * (i * self.n_res + k) * w, dist + (2 * (i * self.n_res + k) + 1) * w)
+                   for k in range(self.n_res)]
             recs.append(QueryRecord((s[0], s[1]), (s[2], s[3]),
-                                    (comp + 2 * i * w, comp + (2 * i + 1) * w),
-                                    (dist + 2 * i * w, dist + (2 * i + 1) * w)))
-        self._outbox = {"compact": comp, "dists": dist}
+                                    (comp + 2 * i * w, comp + (2 * i + 1) * w), res[0], results=res))
+        self._outbox = {"compact": (comp, 1), "dists": (dist, self.n_res)}
         return recs
 
-    def read_outbox(self, kind: str, count: int) -> np.ndarray:
-        """(count, 2, lvl_out * N) result ciphertexts of the first `count`
-        records from alloc_queries, in one device-to-host copy."""
-        w = self.lvl_out * self.p.n
-        return self.ctx.read_poly(self._outbox[kind], 2 * count * w).reshape(count, 2, w)
+    def record_index(self, kind: str, rec: QueryRecord) -> int:
+        base, per = self._outbox[kind]
+        first = rec.compact if kind == "compact" else rec.results[0]
+        return (first[0] - base) // (2 * per * self.lvl_out * self.p.n)
+
+    def read_results(self, kind: str, recs) -> np.ndarray:
+        """Limb 0 of both polynomials of the records' result ciphertexts:
+        (len(recs), per_record, 2, N); one strided copy per contiguous run of
+        records. Limb 0 is what the client decrypts (see __init__)."""
+        base, per = self._outbox[kind]
+        n, w = self.p.n, self.lvl_out * self.p.n
+        idx = [self.record_index(kind, r) for r in recs]
+        out = np.empty((len(recs), per, 2, n), dtype=np.uint64)
+        order = np.argsort(idx, kind="stable")
+        i = 0
+        while i < len(order):
+            j = i
+            while j + 1 < len(order) and idx[order[j + 1]] == idx[order[j]] + 1:
+                j += 1
+            rows = (j - i + 1) * per * 2
+            block = np.empty(rows * n, dtype=np.uint64)
+            L.check(self.lib.afhe_read_poly_rows(self.ctx.h, base + idx[order[i]] * per * 2 * w, w, rows, n,
+                                                 block.ctypes.data_as(L.P64)), "read_poly_rows")
+            block = block.reshape(j - i + 1, per, 2, n)
+            for k in range(i, j + 1):
+                out[order[k]] = block[k - i]
+            i = j + 1
+        return out
+
+    def coarse_from_slots(self, vals: np.ndarray) -> np.ndarray:
+        """(count, n_list) coarse distances from the decoded slots of the
+        compacted coarse ciphertexts."""
+        idx = [self.sh.coarse_slot(c) for c in range(self.sh.n_list)]
+        return vals[:, idx]
+
+    def coarse_slots_needed(self) -> int:
+        return max(self.sh.coarse_slot(c) for c in range(self.sh.n_list)) + 1
 
     # ---- batched C-ABI helpers ----
     @staticmethod
@@ -212,6 +306,10 @@ class InteractiveQueryManager:
         L.check(self.lib.afhe_eval_add_batch(self.ctx.h, self._refs(a), self._refs(b), self._refs(d), len(a), limbs),
                 "eval_add_batch")
 
+    def _copy(self, a, d, limbs):
+        L.check(self.lib.afhe_eval_copy_batch(self.ctx.h, self._refs(a), self._refs(d), len(a), limbs),
+                "eval_copy_batch")
+
     def _mult_plain(self, a, pts, d, limbs):
         L.check(self.lib.afhe_eval_mult_plain_rescale_batch(self.ctx.h, self._refs(a), self._offs(pts), self._refs(d),
                                                             len(a), limbs), "eval_mult_plain_rescale_batch")
@@ -224,17 +322,53 @@ class InteractiveQueryManager:
         L.check(self.lib.afhe_eval_sub_plain_batch(self.ctx.h, self._refs(a), self._offs(pts), self._refs(d), len(a),
                                                    limbs), "eval_sub_plain_batch")
 
+    def _rotate_grouped(self, items, limbs: int) -> None:
+        """Rotate each ciphertext of `items` ((ct, shift) pairs) in place by its
+        shift, as eval_rotate does it: |shift| in descending powers of two,
+        sign kept (fhe_host_driver.cpp:361-404). The steps run highest power
+        first, each as one batched launch over every item whose shift has
+        that bit, so every item sees exactly its own eval_rotate steps in
+        eval_rotate's order."""
+        items = [(ct, s) for ct, s in items if s]
+        if not items:
+            return
+        top = max(abs(s) for _, s in items).bit_length()
+        for b in range(top - 1, -1, -1):
+            for sign in (1, -1):
+                sub = [ct for ct, s in items if (s > 0) == (sign > 0) and (abs(s) >> b) & 1]
+                if sub:
+                    self._rotate(sub, sign * (1 << b), limbs)
+
+    def _accumulate(self, items, limbs: int) -> None:
+        """items: (target, first, src). Per target, its sources of this call
+        are summed pairwise, then copied into the target when one of them
+        starts the target's sum (`first`), else added to it. Modular
+        additions are exact, so any grouping gives the reference's running
+        sum word for word."""
+        by: dict = {}
+        for tgt, first, src in items:
+            e = by.setdefault(tgt, [False, []])
+            e[0] = e[0] or first
+            e[1].append(src)
+        self._sum_groups([g for _, g in by.values()], limbs)
+        copies = [(t, g[0]) for t, (f, g) in by.items() if f]
+        adds = [(t, g[0]) for t, (f, g) in by.items() if not f]
+        if copies:
+            self._copy([s_ for _, s_ in copies], [t for t, _ in copies], limbs)
+        if adds:
+            self._add([t for t, _ in adds], [s_ for _, s_ in adds], [t for t, _ in adds], limbs)
+
     # ---- stages ----
     def stage1_coarse(self, queries: list[QueryRecord]) -> None:
         """Stages 1 and 1b for every query (lanes at a time)."""
+        if self.sh.compaction == "packed":
+            return self._stage1_packed(queries)
         D, Ll = self.sh.D, self.L
         for c0 in range(0, len(queries), self.lanes):
             qs = queries[c0:c0 + self.lanes]
             w = self.work[:len(qs)]
             diff = [x["diff"] for x in w]
             sq = [x["sq"] for x in w]
-            tmp = [x["tmp"] for x in w]
-            sel = [x["sel"] for x in w]
             self._sub_plain([q.ct_query for q in qs], [self.pt_centroids] * len(qs), diff, Ll)
             self._square(diff, sq, Ll)
             s = 1
@@ -243,9 +377,31 @@ class InteractiveQueryManager:
                 s <<= 1
             self._compact(qs, sq)
 
+    def _stage1_packed(self, queries: list[QueryRecord]) -> None:
+        """Stage 1 and the packed compaction: items (query, coarse ciphertext k),
+        lanes at a time, query-major."""
+        D, Ll, nc = self.sh.D, self.L, self.sh.n_coarse
+        items = [(qi, k) for qi in range(len(queries)) for k in range(nc)]
+        for c0 in range(0, len(items), self.lanes):
+            it = items[c0:c0 + self.lanes]
+            w = self.work[:len(it)]
+            diff = [x["diff"] for x in w]
+            sq = [x["sq"] for x in w]
+            sel = [x["sel"] for x in w]
+            self._sub_plain([queries[qi].ct_query for qi, _ in it], [self.pt_centroid_cts[k] for _, k in it], diff,
+                            Ll)
+            self._square(diff, sq, Ll)
+            s = 1
+            while s < D:                     # sq += rot(sq, s)
+                self._rot_acc(sq, sq, s, self.lvl_sq)
+                s <<= 1
+            self._mult_plain(sq, [self.mask_stride] * len(it), sel, self.lvl_sq)
+            self._rotate_grouped([(sel[j], -k) for j, (_, k) in enumerate(it)], self.lvl_out)
+            self._accumulate([(queries[qi].compact, k == 0, sel[j]) for j, (qi, k) in enumerate(it)], self.lvl_out)
+
     def _compact(self, qs: list[QueryRecord], sq) -> None:
-        """Stage 1b for a chunk of queries: compact = sum over i of
-        rot(rescale(sq * mask_i), i * (D - 1)).
+        """Stage 1b (reference compaction) for a chunk of queries: compact =
+        sum over i of rot(rescale(sq * mask_i), i * (D - 1)).
 
         The reference runs the lists one after another, each rotation as
         eval_rotate's descending power-of-two steps, accumulating as it goes.
@@ -269,15 +425,10 @@ class InteractiveQueryManager:
         self._mult_plain(src, pts, dst, self.lvl_sq)
         if nl == 1:
             return
-        terms = [(self.cmp[k][i - 1], i * (D - 1)) for k in range(len(qs)) for i in range(1, nl)]
-        top = max(s for _, s in terms).bit_length()
-        for b in range(top - 1, -1, -1):
-            sub = [ct for ct, s in terms if (s >> b) & 1]
-            if sub:
-                self._rotate(sub, 1 << b, self.lvl_out)
+        self._rotate_grouped([(self.cmp[k][i - 1], i * (D - 1)) for k in range(len(qs)) for i in range(1, nl)],
+                             self.lvl_out)
         # per query: comp += sum of its n_list - 1 rotated terms
-        groups = [[comp[k]] + self.cmp[k] for k in range(len(qs))]
-        self._sum_groups(groups, self.lvl_out)
+        self._sum_groups([[comp[k]] + self.cmp[k] for k in range(len(qs))], self.lvl_out)
 
     def _sum_groups(self, groups, limbs: int) -> None:
         """groups[g][0] += groups[g][1] + ... , all groups side by side, by
@@ -295,7 +446,7 @@ class InteractiveQueryManager:
     def stage3_fine(self, queries: list[QueryRecord]) -> None:
         """Stage 3 for every (query, probed list, batch) item, lanes at a time.
         Each query's `probes` must be set (stage 2)."""
-        D, B, Ll = self.sh.D, self.sh.B, self.L
+        D, B, Ll, S = self.sh.D, self.sh.B, self.L, self.sh.slots
         items = []
         for qi, q in enumerate(queries):
             off = 0
@@ -305,12 +456,13 @@ class InteractiveQueryManager:
                     items.append((qi, pt, cnt, off))
                     q.vids.extend(vids)
                     off += cnt
+            if off > self.n_res * S:
+                raise ValueError("more candidates than the result ciphertexts hold")
         for c0 in range(0, len(items), self.lanes):
             it = items[c0:c0 + self.lanes]
             w = self.work[:len(it)]
             diff = [x["diff"] for x in w]
             sq = [x["sq"] for x in w]
-            tmp = [x["tmp"] for x in w]
             sel = [x["sel"] for x in w]
             self._sub_plain([queries[x[0]].ct_dim for x in it], [x[1] for x in it], diff, Ll)
             self._square(diff, sq, Ll)
@@ -319,31 +471,12 @@ class InteractiveQueryManager:
                 self._rot_acc(sq, sq, s, self.lvl_sq)
                 s <<= 1
             self._mult_plain(sq, [self._prefix(x[2]) for x in it], sel, self.lvl_sq)
-            # rotate each item by -offset: the same descending power-of-two steps
-            # as eval_rotate, grouped across items step by step
-            top = max((x[3] for x in it), default=0).bit_length()
-            for b in range(top - 1, -1, -1):
-                sub = [sel[k] for k, x in enumerate(it) if (x[3] >> b) & 1]
-                if sub:
-                    self._rotate(sub, -(1 << b), self.lvl_out)
-            # accumulate: each query's items of this chunk are summed pairwise
-            # (exact modular additions, so the order does not change a word);
-            # the chunk holding the query's offset-0 item starts its sum.
-            byq: dict[int, list[int]] = {}
-            for k, x in enumerate(it):
-                byq.setdefault(x[0], []).append(k)
-            self._sum_groups([[sel[k] for k in ks] for ks in byq.values()], self.lvl_out)
-            w_ = self.lvl_out * self.p.n
-            adds = []
-            for qi, ks in byq.items():
-                dst, head = queries[qi].dists, sel[ks[0]]
-                if any(it[k][3] == 0 for k in ks):
-                    L.check(self.lib.afhe_copy_poly(self.ctx.h, dst[0], head[0], w_), "copy_poly")
-                    L.check(self.lib.afhe_copy_poly(self.ctx.h, dst[1], head[1], w_), "copy_poly")
-                else:
-                    adds.append((dst, head))
-            if adds:
-                self._add([d for d, _ in adds], [h for _, h in adds], [d for d, _ in adds], self.lvl_out)
+            # rotate each item by -(offset mod slots): eval_rotate's steps,
+            # grouped across items step by step
+            self._rotate_grouped([(sel[k], -(x[3] % S)) for k, x in enumerate(it)], self.lvl_out)
+            # accumulate into result offset // slots; the item at slot 0 starts it
+            self._accumulate([(queries[x[0]].results[x[3] // S], x[3] % S == 0, sel[k]) for k, x in enumerate(it)],
+                             self.lvl_out)
 
     # ---- result transfer ----
     def read_ct(self, ct: tuple[int, int]) -> tuple[np.ndarray, np.ndarray]:

@@ -58,7 +58,7 @@ class Completion:
     done: float
     probes: list = field(default_factory=list)
     topk: list = field(default_factory=list)
-    result: np.ndarray | None = None    # (2, lvl_out * N) candidate-distance ciphertext, if kept
+    result: np.ndarray | None = None    # limb 0 of the candidate-distance ciphertexts, if kept
 
     @property
     def latency(self) -> float:
@@ -126,10 +126,10 @@ class WorkloadBackend:
             for r in recs:
                 self.pool.append([wl.ctx.read_poly(o, Lw) for o in (*r.ct_query, *r.ct_dim)])
         w = self.iqm.lvl_out * self.n
-        self.rec_words = 2 * w
         # device bytes one in-flight query holds: two encrypted queries at L
-        # limbs and two result ciphertexts at lvl_out limbs
-        self.bytes_per_query = (4 * Lw + 2 * self.rec_words) * 8
+        # limbs, the compacted coarse result and n_res candidate results at
+        # lvl_out limbs
+        self.bytes_per_query = (4 * Lw + 2 * w * (1 + self.iqm.n_res)) * 8
 
     def with_lanes(self, lanes: int) -> "WorkloadBackend":
         """The same server and encrypted-query pool, `lanes` ciphertexts per launch."""
@@ -160,30 +160,24 @@ class WorkloadBackend:
             self.iqm.lanes = lanes
 
     def fetch(self, kind: str, recs) -> np.ndarray:
-        """(len(recs), 2, lvl_out * N) result ciphertexts, copied to the host."""
-        base = self.iqm._outbox[kind]
-        idx = [(getattr(r, "compact" if kind == "compact" else "dists")[0] - base) // self.rec_words for r in recs]
-        out = np.empty((len(recs), 2, self.rec_words // 2), dtype=np.uint64)
-        order = np.argsort(idx)
-        i = 0
-        while i < len(order):                # one copy per contiguous run of records
-            j = i
-            while j + 1 < len(order) and idx[order[j + 1]] == idx[order[j]] + 1:
-                j += 1
-            first = idx[order[i]]
-            block = self.wl.ctx.read_poly(base + first * self.rec_words, (j - i + 1) * self.rec_words)
-            block = block.reshape(j - i + 1, 2, -1)
-            for k in range(i, j + 1):
-                out[order[k]] = block[k - i]
-            i = j + 1
-        return out
+        """Limb 0 of the records' result ciphertexts, copied to the host:
+        (len(recs), per_record, 2, N)."""
+        return self.iqm.read_results(kind, recs)
 
     def receive(self, kind: str, recs) -> dict:
-        """Results of `recs` to the client: the result ciphertexts to the host
-        ("box", (count, 2, lvl_out * N)), then the device part of the
-        client's decryption ("coef", (count, N) coefficients). Synchronous."""
+        """Results of `recs` to the client: limb 0 of the result ciphertexts
+        to the host ("box", (count, ciphertexts, 2, N)), then the device part
+        of the client's decryption ("coef", one row of N coefficients per
+        ciphertext). Synchronous."""
         box = self.fetch(kind, recs)
-        got = {"box": box, "coef": self.wl.client.decrypt_host_batch_coef(box, self.iqm.lvl_out)}
+        if kind == "dists":
+            # only the result ciphertexts that hold candidates
+            need = max(1, -(-max(len(r.vids) for r in recs) // self.iqm.sh.slots))
+            box = box[:, :need]
+        else:
+            box = box[:, :1]
+        coef = self.wl.client.decrypt_host_batch_coef(box.reshape(-1, 2, self.n), 1)
+        got = {"box": box, "coef": coef.reshape(len(recs), -1)}
         if kind == "dists":     # the record may be reused before the top-k is decoded
             got["vids"] = [list(r.vids) for r in recs]
         return got
@@ -191,16 +185,17 @@ class WorkloadBackend:
     def select(self, recs, got: dict) -> None:
         """Stage 2 on the host: decode the coarse distances, keep the nprobe nearest lists."""
         wl = self.wl
-        coarse = wl.client.enc.decode_batch(got["coef"], self.iqm.out_scale, wl.spec.n_list).real
-        for r, c in zip(recs, coarse):
+        vals = wl.client.enc.decode_batch(got["coef"], self.iqm.out_scale, self.iqm.coarse_slots_needed()).real
+        for r, c in zip(recs, self.iqm.coarse_from_slots(vals)):
             r.probes = list(np.argsort(c, kind="stable")[:wl.spec.nprobe])
 
     def topk(self, recs, got: dict) -> list[list[int]]:
         """Stage 4 on the host: decode the candidate distances, rank them."""
         wl = self.wl
         vids = got["vids"]
-        m = max(len(v) for v in vids)
-        d = wl.client.enc.decode_batch(got["coef"], self.iqm.out_scale, m).real
+        count = len(vids)
+        coef = got["coef"].reshape(-1, self.n)               # one row per result ciphertext
+        d = wl.client.enc.decode_batch(coef, self.iqm.out_scale).real.reshape(count, -1)
         out = []
         for v, row in zip(vids, d):
             order = np.argsort(row[:len(v)], kind="stable")[:wl.spec.top_k]

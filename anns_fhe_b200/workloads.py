@@ -42,11 +42,43 @@ class WorkloadSpec:
     alpha: int
     log_scale: int
     seed: int = 2024
+    compaction: str = "reference"
+    # index training (the reference's k-means by default)
+    kmeans_iters: int = 25
+    train_sample: int | None = None
+    pq_sample: int | None = None
+    init: str = "random"
 
 
 SMALL = WorkloadSpec("ivfpq_4096x64_nlist32_N8192_L3", n_vectors=4096, d=64, components=32, sigma=0.1, n_list=32,
                      M=8, K=256, nprobe=4, top_k=8, log_n=13, num_q=3, q_bits=50, num_p=1, p_bits=60, alpha=1,
                      log_scale=40)
+
+# Batched encrypted IVF-PQ ADC over a larger database: 1,000,000 x 128 from a
+# 1,024-component mixture (sigma 0.15), n_list 1024, PQ 16 x 256, nprobe 16;
+# CKKS N = 2^15, scale 2^40, 12 x 50-bit Q + 4 x 60-bit P, alpha 4 (dnum 3).
+# The centroids span 8 ciphertexts, so the coarse distances use the packed
+# compaction. The index trains on seeded samples (131,072 vectors for IVF,
+# 32,768 for PQ) with farthest-point seeding, then assigns every vector.
+LARGE = WorkloadSpec("ivfpq_1Mx128_nlist1024_N32768_L12", n_vectors=1_000_000, d=128, components=1024, sigma=0.15,
+                     n_list=1024, M=16, K=256, nprobe=16, top_k=8, log_n=15, num_q=12, q_bits=50, num_p=4,
+                     p_bits=60, alpha=4, log_scale=40, compaction="packed", kmeans_iters=8, train_sample=131072,
+                     pq_sample=32768, init="farthest")
+
+
+def query_layout(q: np.ndarray, sh: QueryShape) -> np.ndarray:
+    """Slots of ct_query: q replicated once per centroid of a coarse
+    ciphertext (slot c * D + d = q[d]); the reference replicates it n_list
+    times, one per centroid (generate_interactive_test_vectors.cpp:383-398)."""
+    reps = sh.n_list if sh.compaction == "reference" else sh.per_ct
+    out = np.zeros(sh.slots)
+    out[:reps * sh.D] = np.tile(np.asarray(q, dtype=np.float64), reps)
+    return out
+
+
+def dimpack_layout(q: np.ndarray, sh: QueryShape) -> np.ndarray:
+    """Slots of ct_query_dimpack: slot d * B + j = q[d] for every candidate j."""
+    return np.repeat(np.asarray(q, dtype=np.float64), sh.B)
 
 
 class Workload:
@@ -55,20 +87,27 @@ class Workload:
         self.spec = spec
         t0 = time.time()
         self.X = gaussian_mixture(spec.n_vectors, spec.d, spec.components, spec.sigma, spec.seed)
-        self.index = index or IvfPqIndex.train(self.X, spec.n_list, spec.M, spec.K, spec.seed)
+        self.index = index or IvfPqIndex.train(self.X, spec.n_list, spec.M, spec.K, spec.seed, iters=spec.kmeans_iters,
+                                               train_sample=spec.train_sample, pq_sample=spec.pq_sample,
+                                               init=spec.init)
         self.params = CkksParams.generate(spec.log_n, spec.num_q, spec.q_bits, spec.num_p, spec.p_bits, spec.alpha)
         n = self.params.n
         slots = n // 2
         shape = QueryShape(D=spec.d, n_list=spec.n_list, slots=slots, nprobe=spec.nprobe, top_k=spec.top_k,
-                           scale=float(2 ** spec.log_scale))
+                           scale=float(2 ** spec.log_scale), compaction=spec.compaction)
         slot_w = (self.params.L + self.params.K) * n
         B = slots // spec.d
         n_batches = sum(-(-len(v) // B) for v in self.index.lists)
+        n_res = -(-sum(sorted((len(v) for v in self.index.lists), reverse=True)[:spec.nprobe]) // slots)
         w_out = (self.params.L - 2) * n
-        most = max(max_queries, lanes)
-        dec_slots = -(-most * 2 * w_out // slot_w) + -(-most * w_out // slot_w)
-        n_slots = (16 + 1 + spec.n_list + 2 * n_batches + 8 * lanes + 8 * max_queries + 64 + max_queries
-                   + InteractiveQueryManager.compaction_slots(spec.n_list, self.params.L, n, slot_w, lanes)
+        most = max(max_queries, lanes) * max(n_res, 1)
+        # client staging: results arrive as limb 0 (N words per polynomial)
+        dec_slots = -(-most * 2 * n // slot_w) + -(-most * n // slot_w)
+        outbox_slots = -(-2 * max_queries * w_out // slot_w) + -(-2 * max_queries * n_res * w_out // slot_w)
+        masks = spec.n_list if spec.compaction == "reference" else 1
+        n_slots = (16 + shape.n_coarse + masks + n_batches + B + 8 * lanes + 4 * max_queries + outbox_slots + 64
+                   + InteractiveQueryManager.compaction_slots(spec.n_list if spec.compaction == "reference" else 1,
+                                                              self.params.L, n, slot_w, lanes)
                    + dec_slots)
         self.ctx = FheContext(self.params, poly_words=n_slots * slot_w,
                               key_words=(2 + 2 * (spec.log_n + 1)) * self.params.key_words() + 4096, device=device,
@@ -80,8 +119,8 @@ class Workload:
         self.client.install_keys(self.steps)
         self.records = self.iqm.alloc_queries(max_queries)
         # the client's decryption staging, sized once for the largest batch
-        self.client._region("dec_in", most * 2 * w_out)
-        self.client._region("dec_out", most * w_out)
+        self.client._region("dec_in", most * 2 * n)
+        self.client._region("dec_out", most * n)
         self.ctx.sync()
         self.setup_s = time.time() - t0
 
@@ -93,26 +132,35 @@ class Workload:
 
     # ---- client side ----
     def encrypt_queries(self, Q: np.ndarray, recs: list[QueryRecord]) -> None:
-        sh, D = self.iqm.sh, self.spec.d
-        B = sh.B
+        sh = self.iqm.sh
         for q, r in zip(Q, recs):
-            packed = np.zeros(sh.slots)
-            for c in range(sh.n_list):
-                packed[c * D:(c + 1) * D] = q
-            self.client.encrypt(packed, sh.scale, r.ct_query[0], r.ct_query[1])
-            dim = np.repeat(q.astype(np.float64), B)        # slot d*B + j = q[d]
-            self.client.encrypt(dim, sh.scale, r.ct_dim[0], r.ct_dim[1])
+            self.client.encrypt(query_layout(q, sh), sh.scale, r.ct_query[0], r.ct_query[1])
+            self.client.encrypt(dimpack_layout(q, sh), sh.scale, r.ct_dim[0], r.ct_dim[1])
 
-    def decrypt_slots(self, ct) -> np.ndarray:
-        return self.client.decrypt(ct[0], ct[1], self.iqm.lvl_out, self.iqm.out_scale).real
+    def decrypt_many(self, cts, slots: int | None = None) -> np.ndarray:
+        """Decrypt result ciphertexts resident on the device from limb 0 (the
+        messages are far below q_0 / 2; the query manager checks the bound)."""
+        return self.client.decrypt_batch(cts, 1, self.iqm.out_scale, slots).real
 
-    def decrypt_many(self, cts) -> np.ndarray:
-        return self.client.decrypt_batch(cts, self.iqm.lvl_out, self.iqm.out_scale).real
+    def coarse(self, recs) -> np.ndarray:
+        """(count, n_list) decrypted coarse distances."""
+        vals = self.decrypt_many([r.compact for r in recs], self.iqm.coarse_slots_needed())
+        return self.iqm.coarse_from_slots(vals)
+
+    def candidates(self, recs) -> list[np.ndarray]:
+        """Each query's decrypted candidate distances, in stage-3 order."""
+        S = self.iqm.sh.slots
+        need = [max(1, -(-len(r.vids) // S)) for r in recs]
+        vals = self.decrypt_many([ct for r, k in zip(recs, need) for ct in r.results[:k]])
+        out, i = [], 0
+        for r, k in zip(recs, need):
+            out.append(vals[i:i + k].ravel()[:len(r.vids)])
+            i += k
+        return out
 
     def select(self, recs) -> None:
         """Stage 2 (client): decrypt the compacted coarse distances, keep nprobe lists."""
-        coarse = self.decrypt_many([r.compact for r in recs])[:, :self.spec.n_list]
-        for r, c in zip(recs, coarse):
+        for r, c in zip(recs, self.coarse(recs)):
             r.probes = list(np.argsort(c, kind="stable")[:self.spec.nprobe])
 
     # ---- protocol ----
@@ -121,15 +169,12 @@ class Workload:
         recs = recs or self.records[:len(Q)]
         self.encrypt_queries(Q, recs)
         self.iqm.stage1_coarse(recs)
-        coarse = self.decrypt_many([r.compact for r in recs])[:, :self.spec.n_list]
         out = []
-        for r, c in zip(recs, coarse):
+        for r, c in zip(recs, self.coarse(recs)):
             r.probes = list(np.argsort(c, kind="stable")[:self.spec.nprobe])
             out.append({"coarse": c, "probes": r.probes})
         self.iqm.stage3_fine(recs)
-        dists = self.decrypt_many([r.dists for r in recs])
-        for r, o, d in zip(recs, out, dists):
-            d = d[:len(r.vids)]
+        for r, o, d in zip(recs, out, self.candidates(recs)):
             order = np.argsort(d, kind="stable")[:self.spec.top_k]
             o.update(dists=d, vids=list(r.vids), topk=[r.vids[i] for i in order])
         return out

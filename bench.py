@@ -65,19 +65,21 @@ def run_ours(args, rank: int, world: int):
 
     from anns_fhe_b200._lib import P64
     from anns_fhe_b200.replicas import aggregate, query_seed
-    from anns_fhe_b200.workloads import Workload
+    from anns_fhe_b200.workloads import LARGE, SMALL, Workload
 
     dev = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(dev)
+    spec = LARGE if args.workload == "large" else SMALL
     if args.batch <= 0:
-        # the key switch runs one CTA per ciphertext and one CTA per SM at a
-        # time: two full waves per launch
-        args.batch = 2 * torch.cuda.get_device_properties(dev).multi_processor_count
+        # small: the one-kernel key switch runs one CTA per ciphertext and one
+        # CTA per SM at a time, so two full waves per launch; large: 256
+        # queries per launch
+        args.batch = 256 if spec is LARGE else 2 * torch.cuda.get_device_properties(dev).multi_processor_count
     if args.lanes <= 0:
         args.lanes = args.batch
     # twice the records of a step: the serving leg keeps one tick's queries
     # in flight while admitting the next
-    wl = Workload(max_queries=2 * args.batch, lanes=args.lanes, device=dev)
+    wl = Workload(spec, max_queries=2 * args.batch, lanes=args.lanes, device=dev)
     stream = torch.cuda.ExternalStream(wl.ctx.lib.afhe_stream(wl.ctx.h), device=dev)
     iqm = wl.iqm
     recs = wl.records[:args.batch]
@@ -116,17 +118,19 @@ def run_ours(args, rank: int, world: int):
                 lib.afhe_write_poly_async(wl.ctx.h, off, C.cast(t.data_ptr(), P64), t.numel())
                 h2d += t.numel() * 8
         iqm.stage1_coarse(recs)
-        # client receives the compacted coarse distances, decrypts, selects
-        box = iqm.read_outbox("compact", len(recs))
+        # client receives limb 0 of the compacted coarse distances, decrypts, selects
+        box = iqm.read_results("compact", recs)[:, 0]
         d2h = box.nbytes
-        coarse = wl.client.decrypt_host_batch(box, iqm.lvl_out, iqm.out_scale, wl.spec.n_list).real
+        coarse = iqm.coarse_from_slots(
+            wl.client.decrypt_host_batch(box, 1, iqm.out_scale, iqm.coarse_slots_needed()).real)
         for r, c in zip(recs, coarse):
             r.probes = list(np.argsort(c, kind="stable")[:wl.spec.nprobe])
         iqm.stage3_fine(recs)
-        # client receives the candidate distances, decrypts, ranks
-        box = iqm.read_outbox("dists", len(recs))
+        # client receives limb 0 of the candidate distances, decrypts, ranks
+        box = iqm.read_results("dists", recs)
         d2h += box.nbytes
-        dists = wl.client.decrypt_host_batch(box, iqm.lvl_out, iqm.out_scale, max(len(r.vids) for r in recs)).real
+        S = iqm.sh.slots
+        dists = wl.client.decrypt_host_batch(box.reshape(-1, 2, n), 1, iqm.out_scale).real.reshape(len(recs), -1)
         for r, d in zip(recs, dists):
             np.argsort(d[:len(r.vids)], kind="stable")[:wl.spec.top_k]
         eb.record(stream)
@@ -181,10 +185,14 @@ def run_ours(args, rank: int, world: int):
         "clocks": summarize_clocks(samples),
         "gpu_launches": int(launches),
     }
-    line["serving"] = serve_leg(args, wl, [[t.numpy() for t in cts] for cts in pinned], rank)
-    line["roofline"] = ks_roofline(wl.params, args.lanes)
+    if not args.skip_serving:
+        line["serving"] = serve_leg(args, wl, [[t.numpy() for t in cts] for cts in pinned], rank)
+    if spec is SMALL:
+        line["roofline"] = ks_roofline(wl.params, args.lanes)
+    else:
+        line["config"]["setup_s"] = wl.setup_s
     wl.close()
-    if world == 1 and rank == 0 and not args.skip_cpu:
+    if world == 1 and rank == 0 and not args.skip_cpu and spec is SMALL:
         from oracle.chain import cpu_reference_rate
         ref = cpu_reference_rate(steps=1)
         line["cpu_baseline"] = ref["cpu_baseline"]
@@ -485,6 +493,9 @@ def main():
     ap.add_argument("--batch", type=int, default=0, help="queries per step (default: 2 x the SM count)")
     ap.add_argument("--lanes", type=int, default=0, help="ciphertexts per launch (default: the batch)")
     ap.add_argument("--skip-cpu", action="store_true", help="omit the cpu_baseline leg")
+    ap.add_argument("--skip-serving", action="store_true", help="omit the serving leg")
+    ap.add_argument("--workload", default="small", choices=["small", "large"],
+                    help="small: 4,096 x 64, N=2^13 (default); large: 1M x 128, n_list 1024, N=2^15")
     ap.add_argument("--plain-queries", type=int, default=16, help="queries timed on the plain path")
     ap.add_argument("--serve-rate", type=float, default=0.0, help="served trace rate (default: 10x plain)")
     ap.add_argument("--serve-seconds", type=float, default=5.0, help="served trace length")

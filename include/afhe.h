@@ -168,6 +168,14 @@ int afhe_read_key(afhe_ctx* ctx, uint64_t word_offset, uint64_t* dst, uint64_t c
 int afhe_write_poly_async(afhe_ctx* ctx, uint64_t word_offset, const uint64_t* src, uint64_t count);
 int afhe_read_poly_async(afhe_ctx* ctx, uint64_t word_offset, uint64_t* dst, uint64_t count);
 int afhe_copy_poly(afhe_ctx* ctx, uint64_t dst_offset, uint64_t src_offset, uint64_t count);
+/* Gather `rows` rows of `row_words` words, row r at word_offset + r * stride,
+ * into dst (rows * row_words words, packed), in one copy; synchronous. Reads
+ * one limb of many result ciphertexts, e.g. limb 0 of each, which is all a
+ * client needs to decrypt a message smaller than q_0 / 2. Replaces the
+ * reference host's word-by-word read-back of results from poly_gmem
+ * (SimMemoryBus, sim_memory_bus.h:10-34). */
+int afhe_read_poly_rows(afhe_ctx* ctx, uint64_t word_offset, uint64_t stride, uint64_t rows,
+                        uint64_t row_words, uint64_t* dst);
 
 /* Writes the context tables for level `level` (twiddles for all Q and P primes,
  * CRT tables for that level) into key_gmem in the reference's arrangement and
@@ -265,6 +273,11 @@ int afhe_eval_rotate_accumulate_batch(afhe_ctx* ctx, const afhe_ct_ref* in, cons
                                       uint32_t count, int32_t total_rot, uint32_t limbs);
 int afhe_eval_add_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const afhe_ct_ref* b, const afhe_ct_ref* dst,
                         uint32_t count, uint32_t limbs);
+/* dst[i] = a[i] (both polynomials, `limbs` limbs): the slot-to-slot copies the
+ * reference's host makes between operators (eval_sub_plain's c1 copy,
+ * fhe_host_driver.cpp:259-270), for many ciphertexts in one launch. */
+int afhe_eval_copy_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const afhe_ct_ref* dst, uint32_t count,
+                         uint32_t limbs);
 /* pt[i] is the plaintext polynomial offset for ciphertext i */
 int afhe_eval_sub_plain_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const uint64_t* pt, const afhe_ct_ref* dst,
                               uint32_t count, uint32_t limbs);

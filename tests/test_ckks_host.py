@@ -57,3 +57,24 @@ def test_pow2_steps():
     assert pow2_steps(63 * 5) == [256, 32, 16, 8, 2, 1]
     assert pow2_steps(-6) == [4, 2]
     assert sum(pow2_steps(12345)) == 12345
+
+
+def test_query_layouts():
+    """Client-side slot layouts: ct_query replicates q per centroid of a
+    coarse ciphertext, ct_dimpack puts q[d] at every candidate slot d * B + j."""
+    import numpy as np
+
+    from anns_fhe_b200.query import QueryShape
+    from anns_fhe_b200.workloads import dimpack_layout, query_layout
+    q = np.arange(8, dtype=np.float32) + 1
+    ref = QueryShape(D=8, n_list=4, slots=64, nprobe=1, top_k=1, scale=1.0)
+    a = query_layout(q, ref)
+    assert np.array_equal(a[:32], np.tile(q, 4)) and not a[32:].any()
+    packed = QueryShape(D=8, n_list=20, slots=64, nprobe=1, top_k=1, scale=1.0, compaction="packed")
+    assert packed.per_ct == 8 and packed.n_coarse == 3
+    assert np.array_equal(query_layout(q, packed), np.tile(q, 8))
+    d = dimpack_layout(q, packed)
+    assert d.size == 64 and all(d[i * 8 + j] == q[i] for i in range(8) for j in range(8))
+    # coarse slot map: list k * per_ct + c at slot c * D + k
+    assert packed.coarse_slot(8 * 2 + 5) == 5 * 8 + 2
+    assert sorted(packed.coarse_slot(c) for c in range(20)) == sorted({packed.coarse_slot(c) for c in range(20)})

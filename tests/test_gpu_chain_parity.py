@@ -8,6 +8,12 @@ generate_interactive_test_vectors.cpp:383-541. For each list, mask, rescale,
 eval_rotate by i (D - 1) and eval_add into a running sum; for each candidate
 batch, the same with -offset.
 
+For indexes whose centroids span several ciphertexts the chain compacts
+them the "packed" way (mask every centroid slot, rotate coarse ciphertext k
+right by k, sum), and candidates past the slot count continue in a second
+result ciphertext. That chain is replayed the same way, one ciphertext at a
+time, on the oracle.
+
 This test replays that sequential chain on the CPU oracle (the C restatement
 of the reference's HLS kernels) with the very keys, plaintexts and
 encrypted queries the GPU used, read back from the device. It then requires
@@ -44,35 +50,46 @@ def reference_chain(wl, ora, ct, ct_dim, probes):
 
     def pt(off, limbs):
         return wl.ctx.read_poly(off, limbs * n)
+
+    def tree(c, stride):
+        s = stride
+        while s < D * stride:
+            c = ora.eval_add(c, ora.eval_rotate(c, s, rot, L - 1), L - 1)
+            s <<= 1
+        return c
     # stage 1 / 1b
-    diff = ora.eval_sub_plain(ct, pt(iqm.pt_centroids, L), L)
-    sq = ora.eval_mult_relin_rescale(diff, diff, relin, L)
-    s = 1
-    while s < D:
-        sq = ora.eval_add(sq, ora.eval_rotate(sq, s, rot, L - 1), L - 1)
-        s <<= 1
     comp = None
-    for i in range(nl):
-        sel = ora.eval_mult_plain_rescale(sq, pt(iqm.mask_onehot[i], L - 1), L - 1)
-        if i:
-            sel = ora.eval_rotate(sel, i * (D - 1), rot, L - 2)
-        comp = sel if comp is None else ora.eval_add(comp, sel, L - 2)
-    # stage 3
-    off, acc = 0, None
+    if iqm.sh.compaction == "reference":
+        diff = ora.eval_sub_plain(ct, pt(iqm.pt_centroids, L), L)
+        sq = tree(ora.eval_mult_relin_rescale(diff, diff, relin, L), 1)
+        for i in range(nl):
+            sel = ora.eval_mult_plain_rescale(sq, pt(iqm.mask_onehot[i], L - 1), L - 1)
+            if i:
+                sel = ora.eval_rotate(sel, i * (D - 1), rot, L - 2)
+            comp = sel if comp is None else ora.eval_add(comp, sel, L - 2)
+    else:
+        # packed: coarse ciphertext k masked at every centroid slot, rotated right by k
+        for k, pk in enumerate(iqm.pt_centroid_cts):
+            diff = ora.eval_sub_plain(ct, pt(pk, L), L)
+            sq = tree(ora.eval_mult_relin_rescale(diff, diff, relin, L), 1)
+            sel = ora.eval_mult_plain_rescale(sq, pt(iqm.mask_stride, L - 1), L - 1)
+            if k:
+                sel = ora.eval_rotate(sel, -k, rot, L - 2)
+            comp = sel if comp is None else ora.eval_add(comp, sel, L - 2)
+    # stage 3: candidate p lands in result p // slots at slot p mod slots
+    S = iqm.sh.slots
+    off, acc = 0, {}
     for c in probes:
         for pt_off, cnt, _ in iqm.batches[c]:
             diff = ora.eval_sub_plain(ct_dim, pt(pt_off, L), L)
-            sq = ora.eval_mult_relin_rescale(diff, diff, relin, L)
-            s = B
-            while s < D * B:
-                sq = ora.eval_add(sq, ora.eval_rotate(sq, s, rot, L - 1), L - 1)
-                s <<= 1
+            sq = tree(ora.eval_mult_relin_rescale(diff, diff, relin, L), B)
             sel = ora.eval_mult_plain_rescale(sq, pt(iqm.mask_prefix[cnt], L - 1), L - 1)
-            if off:
-                sel = ora.eval_rotate(sel, -off, rot, L - 2)
-            acc = sel if acc is None else ora.eval_add(acc, sel, L - 2)
+            if off % S:
+                sel = ora.eval_rotate(sel, -(off % S), rot, L - 2)
+            r = off // S
+            acc[r] = sel if r not in acc else ora.eval_add(acc[r], sel, L - 2)
             off += cnt
-    return comp, acc
+    return comp, [acc[r] for r in sorted(acc)]
 
 
 def run_and_compare(spec, nq, lanes, orc):
@@ -88,17 +105,37 @@ def run_and_compare(spec, nq, lanes, orc):
         wl.select(recs)
         wl.iqm.stage3_fine(recs)
         ora = OracleCKKS(p.log_n, p.q, p.p, p.alpha, orc)
+        results_used = set()
         for r, (ct, ct_dim) in zip(recs, ins):
-            comp, acc = reference_chain(wl, ora, ct, ct_dim, r.probes)
-            got_c, got_d = wl.iqm.read_ct(r.compact), wl.iqm.read_ct(r.dists)
+            comp, accs = reference_chain(wl, ora, ct, ct_dim, r.probes)
+            got_c = wl.iqm.read_ct(r.compact)
             assert np.array_equal(got_c[0], comp[0]) and np.array_equal(got_c[1], comp[1]), "stage 1b differs"
-            assert np.array_equal(got_d[0], acc[0]) and np.array_equal(got_d[1], acc[1]), "stage 3 differs"
+            results_used.add(len(accs))
+            for k, acc in enumerate(accs):
+                got_d = wl.iqm.read_ct(r.results[k])
+                assert np.array_equal(got_d[0], acc[0]) and np.array_equal(got_d[1], acc[1]), \
+                    f"stage 3 result {k} differs"
+        return wl.iqm, results_used
     finally:
         wl.close()
 
 
+# the packed compaction and results spanning two ciphertexts: 128 lists of 8
+# dimensions over 2 coarse ciphertexts (64 centroids each at N = 2^10), 40
+# probes of about 16 vectors (> 512 candidates per query)
+TINY_PACKED = WorkloadSpec("ivfpq_2048x8_nlist128_N1024_L4_packed", n_vectors=2048, d=8, components=128,
+                           sigma=0.1, n_list=128, M=2, K=16, nprobe=40, top_k=4, log_n=10, num_q=4, q_bits=50,
+                           num_p=2, p_bits=60, alpha=2, log_scale=40, compaction="packed", init="farthest")
+
+
 def test_chain_matches_reference_small_ring(orc):
     run_and_compare(TINY, nq=3, lanes=4, orc=orc)
+
+
+def test_packed_chain_matches_oracle_replay(orc):
+    iqm, used = run_and_compare(TINY_PACKED, nq=2, lanes=16, orc=orc)
+    assert iqm.sh.n_coarse == 2 and iqm.n_res >= 2
+    assert max(used) >= 2, "no query spilled into a second result ciphertext"
 
 
 def test_chain_matches_reference_bench_configuration(orc):

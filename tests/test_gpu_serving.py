@@ -1,13 +1,14 @@
 """Serving loop on the GPU (small configuration: N = 2^13, 4,096 x 64
 database, n_list 32, nprobe 4).
 
-* Each query's result is the same alone and in the mix: the candidate-distance
-  ciphertext a query gets back from the continuous-batching server (several
-  queries admitted per tick, stage 1 of new queries beside stage 3 of earlier
-  ones, 8 ciphertexts per launch) is bit-identical to the one it gets when it
-  is served alone on the plain path (one ciphertext per launch, one query in
-  flight). Decrypted, the two are therefore equal, far inside the CKKS
-  tolerance of 1e-2 used for the plaintext comparison.
+* Each query's result is the same alone and in the mix: what the client
+  receives for a query's candidate distances (limb 0 of the result
+  ciphertexts, all it needs to decrypt) from the continuous-batching server
+  (several queries admitted per tick, stage 1 of new queries beside stage 3
+  of earlier ones, 8 ciphertexts per launch) is bit-identical to what it
+  receives when the query is served alone on the plain path (one ciphertext
+  per launch, one query in flight). Decrypted, the two are therefore equal,
+  far inside the CKKS tolerance of 1e-2 used for the plaintext comparison.
 * Probes and top-k equal the plaintext IVF-PQ search.
 * A short real-time Poisson trace completes every request.
 """
