@@ -202,7 +202,7 @@ cudaError_t launch_rescale(int log_n, const OpTabs& t, const LimbJob* jobs_q, ui
 // ---------------------------------------------------------------------------
 // Scratch layout per polynomial (S = slots_q + K limb slots, Q limb i at slot
 // i, special limb k at slot slots_q + k):
-//   coef   : slots_q * N   INTT of the input's Q limbs
+//   coef   : slots_q * N   INTT of the input's Q limbs, times qHatInv (ModUp's first factor)
 //   modup  : parts * S * N digit j's complementary limbs, evaluation form
 //   ext0   : S * N         sum_j digit_j * evk_b   (then ModDown input)
 //   ext1   : S * N         sum_j digit_j * evk_a
@@ -224,8 +224,36 @@ struct LoadGather {
     }
 };
 
+// Epilogue of the input's INTT: stores y_i = [x_i * qHatInv_i]_{q_i}, the
+// first factor of ModUp's base conversion (key_switch.cpp:7-60), once per
+// input limb instead of once per complementary output limb. job.aux = Q limb i.
+struct StoreQhatInv {
+    u64* scratch;
+    OpTabs t;
+    __device__ __forceinline__ void operator()(const LimbJob& j, const ZBases& zb, uint32_t z, uint32_t x, u64 v,
+                                               const PrimeConst& pc) const {
+        const uint32_t part = j.aux / t.alpha, idx = j.aux - part * t.alpha;
+        scratch[zb.out.at(z) + j.out + x] =
+            mul_shoup(v, __ldg(t.qhat_inv[part] + idx), __ldg(t.qhat_inv_sh[part] + idx), pc.q);
+    }
+};
+
+// Epilogue of the special limbs' INTT before ModDown: stores
+// [x_k * PHatInv_k]_{p_k}, the first factor of the P -> Q base conversion
+// (key_switch.cpp:62-163), once per special limb. job.aux = special limb k.
+struct StorePhatInv {
+    u64* scratch;
+    OpTabs t;
+    __device__ __forceinline__ void operator()(const LimbJob& j, const ZBases& zb, uint32_t z, uint32_t x, u64 v,
+                                               const PrimeConst& pc) const {
+        scratch[zb.out.at(z) + j.out + x] =
+            mul_shoup(v, __ldg(t.phat_inv_modp + j.aux), __ldg(t.phat_inv_modp_sh + j.aux), pc.q);
+    }
+};
+
 // ModUp base conversion as the NTT prologue: job.aux = digit << 16 | k, where
-// k is the output's position among the digit's complementary primes.
+// k is the output's position among the digit's complementary primes. Reads
+// y_i = [x_i * qHatInv_i]_{q_i} (StoreQhatInv) and sums y_i * [qHat_i]_p.
 struct ModUpLoad {
     const u64* scratch;   // coef region at zb.aux[z]
     OpTabs t;
@@ -238,16 +266,12 @@ struct ModUpLoad {
         const uint32_t size = (part == t.parts - 1) ? t.sizeQl - start : t.alpha;
         const uint32_t row = t.sizeQl - size + K;   // complementary primes of this digit
         const u64 p = pc.q, p2 = p << 1;
-        const u64* qi = t.qhat_inv[part];
-        const u64* qish = t.qhat_inv_sh[part];
         const u64* qm = t.qhat_modp[part];
         const u64* qmsh = t.qhat_modp_sh[part];
         u64 s = 0;
         for (uint32_t i = 0; i < size; ++i) {
             const uint32_t limb = start + i;
-            const u64 qq = t.pt.pc[limb].q;
-            u64 xv = scratch[zb.aux.at(z) + (u64)limb * n + x];
-            u64 y = mul_shoup(xv, __ldg(qi + i), __ldg(qish + i), qq);           // [x * qHatInv]_{q_i}
+            const u64 y = scratch[zb.aux.at(z) + (u64)limb * n + x];            // [x * qHatInv]_{q_i}
             u64 w = mul_shoup_lazy(y, __ldg(qm + i * row + k), __ldg(qmsh + i * row + k), p);
             s += w;
             s = s >= p2 ? s - p2 : s;
@@ -306,7 +330,8 @@ __global__ void __launch_bounds__(256) ks_mac_kernel(OpTabs t, uint32_t n, uint3
     }
 }
 
-// ModDown base conversion P -> Q as the NTT prologue (job = Q limb i).
+// ModDown base conversion P -> Q as the NTT prologue (job = Q limb i). Reads
+// [x_k * PHatInv_k]_{p_k} (StorePhatInv) and sums it times [PHat_k]_{q_i}.
 struct ModDownLoad {
     const u64* scratch;  // ext region at zb.aux[z]
     OpTabs t;
@@ -317,9 +342,7 @@ struct ModDownLoad {
         const uint32_t i = j.aux;
         u64 s = 0;
         for (uint32_t k = 0; k < K; ++k) {
-            const PrimeConst& pk = t.pt.pc[t.p_base + k];
-            u64 xv = scratch[zb.aux.at(z) + (u64)(slots_q + k) * n + x];
-            u64 y = mul_shoup(xv, __ldg(t.phat_inv_modp + k), __ldg(t.phat_inv_modp_sh + k), pk.q);
+            const u64 y = scratch[zb.aux.at(z) + (u64)(slots_q + k) * n + x];
             u64 w = mul_shoup_lazy(y, __ldg(t.phat_modq + k * t.sizeQl + i), __ldg(t.phat_modq_sh + k * t.sizeQl + i), q);
             s += w;
             s = s >= q2 ? s - q2 : s;
@@ -379,9 +402,10 @@ cudaError_t launch_key_switch(int log_n, const OpTabs& t, const LimbJob* jobs_qp
         a.out = a.mid;
         if (f.map)
             e = launch_ntt<true>(log_n, t.pt, jobs_qp, sizeQl, nz, scratch, a, LoadGather{arena, f.map},
-                                 StorePlain{scratch}, st);
+                                 StoreQhatInv{scratch, t}, st);
         else
-            e = launch_ntt<true>(log_n, t.pt, jobs_qp, sizeQl, nz, scratch, a, LoadPlain{arena}, StorePlain{scratch}, st);
+            e = launch_ntt<true>(log_n, t.pt, jobs_qp, sizeQl, nz, scratch, a, LoadPlain{arena},
+                                 StoreQhatInv{scratch, t}, st);
         if (e != cudaSuccess) return e;
     }
     // 2. ModUp: base conversion + NTT for every (digit, complementary limb)
@@ -410,9 +434,9 @@ cudaError_t launch_key_switch(int log_n, const OpTabs& t, const LimbJob* jobs_qp
         a.aux = a.src;
         a.mid = a.src;
         a.out = a.src;
-        // 4a. INTT of the special limbs, in place
+        // 4a. INTT of the special limbs, in place, times PHatInv
         e = launch_ntt<true>(log_n, t.pt, jobs_qp + slots_q, K, 2 * nz, scratch, a, LoadPlain{scratch},
-                             StorePlain{scratch}, st);
+                             StorePhatInv{scratch, t}, st);
         if (e != cudaSuccess) return e;
         // 4b. NTT over Q limbs with base-conversion prologue and ModDown epilogue
         ZBases b = a;

@@ -6,7 +6,7 @@
 // CTA carries one ciphertext polynomial through every step with the limb
 // being transformed held in shared memory:
 //
-//   phase 0  coef[i] = INTT(in[i]) for the input's Q limbs -> lane scratch
+//   phase 0  coef[i] = INTT(in[i]) * qHatInv_i for the input's Q limbs -> lane scratch
 //   phase 1  for every special slot k: the MAC over digits (each digit's value
 //            for the slot is the input itself when the slot is one of the
 //            digit's own limbs, else BConv(coef) + NTT); INTT of both
@@ -116,16 +116,14 @@ __device__ void mac_slot(const KsFusedArgs& a, uint32_t s, u64* W, u64* A0, u64*
             for (uint32_t k = 0; k < kPer; ++k) acc[k] = 0;
             for (uint32_t i = 0; i < size; ++i) {
                 const uint32_t limb = start + i;
-                const u64 qq = t.pt.pc[limb].q;
-                const u64 w0 = __ldg(t.qhat_inv[j] + i), w0s = __ldg(t.qhat_inv_sh[j] + i);
                 const u64 w1 = __ldg(t.qhat_modp[j] + i * row + kpos), w1s = __ldg(t.qhat_modp_sh[j] + i * row + kpos);
-                const u64* src = coef + ((u64)limb << LOGN);
+                const u64* src = coef + ((u64)limb << LOGN);     // [x * qHatInv]_{q_i} (phase 0)
                 u64 v[kPer];
 #pragma unroll
                 for (uint32_t k = 0; k < kPer; ++k) v[k] = src[pos<LOGN>(k)];
 #pragma unroll
                 for (uint32_t k = 0; k < kPer; ++k) {
-                    acc[k] += mul_shoup_lazy(mul_shoup(v[k], w0, w0s, qq), w1, w1s, q);
+                    acc[k] += mul_shoup_lazy(v[k], w1, w1s, q);
                     acc[k] = acc[k] >= p2 ? acc[k] - p2 : acc[k];
                 }
             }
@@ -411,8 +409,15 @@ __global__ void __launch_bounds__((1u << LOGN) / 8, 1) ks_fused_kernel(const KsF
         }
         __syncthreads();
         inv_ntt<LOGN>(W, t.pt, i, pc);
+        // stored times qHatInv: the first factor of ModUp's base conversion,
+        // once per limb instead of once per output slot
+        {
+            const uint32_t part = i / t.alpha, idx = i - part * t.alpha;
+            const u64 w0 = __ldg(t.qhat_inv[part] + idx), w0s = __ldg(t.qhat_inv_sh[part] + idx);
 #pragma unroll
-        for (uint32_t k = 0; k < kPer; ++k) coef[((u64)i << LOGN) + pos<LOGN>(k)] = W[padix(pos<LOGN>(k))];
+            for (uint32_t k = 0; k < kPer; ++k)
+                coef[((u64)i << LOGN) + pos<LOGN>(k)] = mul_shoup(W[padix(pos<LOGN>(k))], w0, w0s, pc.q);
+        }
         __syncthreads();
     }
     // phase 1: special slots -> INTT of both accumulators
@@ -423,11 +428,13 @@ __global__ void __launch_bounds__((1u << LOGN) / 8, 1) ks_fused_kernel(const KsF
         ntt2<true, LOGN>(A0, A1, t.pt, prime, pc);
         u64* d0 = pcoef + ((u64)(2 * k) << LOGN);
         u64* d1 = pcoef + ((u64)(2 * k + 1) << LOGN);
+        // stored times PHatInv_k: the first factor of ModDown's base conversion
+        const u64 w0 = __ldg(t.phat_inv_modp + k), w0s = __ldg(t.phat_inv_modp_sh + k);
 #pragma unroll
         for (uint32_t e = 0; e < kPer; ++e) {
             const uint32_t x = pos<LOGN>(e);
-            d0[x] = A0[padix(x)];
-            d1[x] = A1[padix(x)];
+            d0[x] = mul_shoup(A0[padix(x)], w0, w0s, pc.q);
+            d1[x] = mul_shoup(A1[padix(x)], w0, w0s, pc.q);
         }
         __syncthreads();
     }
@@ -448,16 +455,14 @@ __global__ void __launch_bounds__((1u << LOGN) / 8, 1) ks_fused_kernel(const KsF
 #pragma unroll
                 for (uint32_t e = 0; e < kPer; ++e) acc[e] = 0;
                 for (uint32_t k = 0; k < K; ++k) {
-                    const u64 pq = t.pt.pc[t.p_base + k].q;
-                    const u64 w0 = __ldg(t.phat_inv_modp + k), w0s = __ldg(t.phat_inv_modp_sh + k);
                     const u64 w1 = __ldg(t.phat_modq + k * l + i), w1s = __ldg(t.phat_modq_sh + k * l + i);
-                    const u64* src = pcoef + ((u64)(2 * k + h) << LOGN);
+                    const u64* src = pcoef + ((u64)(2 * k + h) << LOGN);   // [x * PHatInv]_{p_k} (phase 1)
                     u64 v[kPer];
 #pragma unroll
                     for (uint32_t e = 0; e < kPer; ++e) v[e] = src[pos<LOGN>(e)];
 #pragma unroll
                     for (uint32_t e = 0; e < kPer; ++e) {
-                        acc[e] += mul_shoup_lazy(mul_shoup(v[e], w0, w0s, pq), w1, w1s, q);
+                        acc[e] += mul_shoup_lazy(v[e], w1, w1s, q);
                         acc[e] = acc[e] >= q2 ? acc[e] - q2 : acc[e];
                     }
                 }

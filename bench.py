@@ -357,13 +357,13 @@ def profile_ks(lanes: int, level: int = 0):
     print(json.dumps(ks_roofline(p, lanes, level=level)))
 
 
-def profile_step(nq: int):
+def profile_step(nq: int, workload: str = "small", lanes: int = 0):
     """Profiling driver: one warm step, then one measured step of `nq` queries.
     Prints the kernel-launch counts an ncu launch list needs (-s / -c)."""
     import numpy as np  # noqa: F401
 
-    from anns_fhe_b200.workloads import Workload
-    wl = Workload(max_queries=nq, lanes=nq)
+    from anns_fhe_b200.workloads import LARGE, SMALL, Workload
+    wl = Workload(LARGE if workload == "large" else SMALL, max_queries=nq, lanes=lanes or nq)
     lib = wl.ctx.lib
     recs = wl.records[:nq]
     wl.encrypt_queries(wl.queries(nq, seed=7), recs)
@@ -515,7 +515,7 @@ def main():
     if args.serve_sweep:
         return serve_sweep([float(x) for x in args.serve_sweep.split(",")], args.serve_seconds, args.batch or 296)
     if args.profile_step:
-        return profile_step(args.profile_step)
+        return profile_step(args.profile_step, args.workload, args.lanes)
     if args.profile_ntt:
         return profile_ntt(args.profile_ntt, args.log_n)
     if args.profile_ks:
