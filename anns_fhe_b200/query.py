@@ -28,7 +28,9 @@ Two compactions:
     c * D + k). That takes n_coarse key switches per query instead of the
     reference's sum over lists of popcount(i * (D - 1)).
 Candidate distances past `slots` continue in further result ciphertexts
-(candidate p at slot p mod slots of result p // slots).
+(position p at slot p mod slots of result p // slots). A candidate batch
+never straddles two results: one that would not fit starts the next result,
+so every batch lands whole in one ciphertext.
 
 Phase-3 candidate plaintexts depend only on the index, so they are encoded
 once and stay resident in HBM (poly_gmem), as do the masks.
@@ -84,8 +86,24 @@ class QueryRecord:
     compact: tuple[int, int]
     dists: tuple[int, int]                          # the first result ciphertext
     probes: list = field(default_factory=list)
-    vids: list = field(default_factory=list)       # candidate position -> vector id (stage 3 order)
+    vids: list = field(default_factory=list)       # candidate vector ids (stage 3 order)
+    pos: list = field(default_factory=list)        # slot position of each candidate across the results
     results: list = field(default_factory=list)    # every result ciphertext (dists first)
+    level: int = 0          # limbs of the encrypted query (0: the top level L)
+    nprobe: int = 0         # lists the client selects (0: the shape's nprobe)
+
+
+def batch_offsets(counts, slots: int) -> list[int]:
+    """Slot offsets of consecutive candidate batches across the result
+    ciphertexts: back to back, except that a batch that would cross a
+    result's end starts the next result (offset a multiple of `slots`)."""
+    out, off = [], 0
+    for cnt in counts:
+        if off % slots + cnt > slots:
+            off = (off // slots + 1) * slots
+        out.append(off)
+        off += cnt
+    return out
 
 
 def pow2_steps(x: int) -> list[int]:
@@ -99,7 +117,16 @@ def pow2_steps(x: int) -> list[int]:
 
 
 class InteractiveQueryManager:
-    def __init__(self, ctx: FheContext, index: IvfPqIndex, shape: QueryShape, slots: Slots, lanes: int = MAX_LANES):
+    """The server chain over many queries. A query encrypted at level l runs
+    the chain at l: results at l - 2 limbs with scale Delta^2 / q_{l-1}. The
+    index's plaintexts are encoded once at the top level L. A plaintext at L
+    restricted to its first l limbs is the same plaintext at level l. Masks
+    are encoded per level, at scale q_{l-2}, the prime the mask rescale drops.
+    `levels` lists the query levels to prepare masks for (default: L only).
+    `max_nprobe` sizes the result ciphertexts (default: the shape's nprobe)."""
+
+    def __init__(self, ctx: FheContext, index: IvfPqIndex, shape: QueryShape, slots: Slots, lanes: int = MAX_LANES,
+                 levels=None, max_nprobe: int | None = None):
         self.ctx, self.index, self.sh = ctx, index, shape
         self.drv = FHEHostDriver(ctx)
         self.lib = ctx.lib
@@ -133,17 +160,26 @@ class InteractiveQueryManager:
             k, j = divmod(c, shape.per_ct)
             vals[k, j * D:(j + 1) * D] = index.centroids[c]
         encode_plaintexts(ctx, self.enc, vals, shape.scale, self.pt_centroid_cts, L)
-        self.mask_onehot = []
-        if shape.compaction == "reference":
-            m = np.zeros((shape.n_list, S))
-            m[np.arange(shape.n_list), np.arange(shape.n_list) * D] = 1.0
-            self.mask_onehot = slots.take(shape.n_list)
-            encode_plaintexts(ctx, self.enc, m, mask_scale, self.mask_onehot, self.lvl_sq)
-        else:
-            m = np.zeros((1, S))
-            m[0, np.arange(shape.per_ct) * D] = 1.0
-            self.mask_stride = slots.take(1)[0]
-            encode_plaintexts(ctx, self.enc, m, mask_scale, [self.mask_stride], self.lvl_sq)
+        self.levels = sorted(set(levels or [L]) | {L})
+        assert all(3 <= lv <= L for lv in self.levels), "query levels must be in [3, L]"
+        self._onehot: dict[int, list[int]] = {}      # level -> one-hot masks (reference compaction)
+        self._stride: dict[int, int] = {}             # level -> centroid-slot mask (packed compaction)
+        self._prefix_lv: dict[tuple[int, int], int] = {}
+        for lv in self.levels:
+            ms = float(self.p.q[lv - 2])
+            if shape.compaction == "reference":
+                m = np.zeros((shape.n_list, S))
+                m[np.arange(shape.n_list), np.arange(shape.n_list) * D] = 1.0
+                self._onehot[lv] = slots.take(shape.n_list)
+                encode_plaintexts(ctx, self.enc, m, ms, self._onehot[lv], lv - 1)
+            else:
+                m = np.zeros((1, S))
+                m[0, np.arange(shape.per_ct) * D] = 1.0
+                self._stride[lv] = slots.take(1)[0]
+                encode_plaintexts(ctx, self.enc, m, ms, [self._stride[lv]], lv - 1)
+        self.mask_onehot = self._onehot.get(L, [])
+        if shape.compaction == "packed":
+            self.mask_stride = self._stride[L]
         self.mask_prefix: dict[int, int] = {}
         B = shape.B
         self.batches: list[list[tuple[int, int, list]]] = []
@@ -167,11 +203,20 @@ class InteractiveQueryManager:
             self.batches.append(out)
         if vals:
             encode_plaintexts(ctx, self.enc, np.stack(vals), shape.scale, offs, L)
-        for cnt in sorted(counts):
-            self._prefix(cnt)
-        # result ciphertexts per query: enough for the nprobe largest lists
-        most = sum(sorted((len(v) for v in index.lists), reverse=True)[:shape.nprobe])
-        self.n_res = max(1, -(-most // S))
+        for lv in self.levels:
+            cs = sorted(counts)
+            m = np.zeros((len(cs), S))
+            for r, cnt in enumerate(cs):
+                m[r, :cnt] = 1.0
+            offs = slots.take(len(cs))
+            encode_plaintexts(ctx, self.enc, m, float(self.p.q[lv - 2]), offs, lv - 1)
+            for cnt, off in zip(cs, offs):
+                self._prefix_lv[(cnt, lv)] = off
+        self.mask_prefix = {cnt: self._prefix_lv[(cnt, L)] for cnt in counts}
+        # result ciphertexts per query: enough for the largest lists a query may probe
+        self.max_nprobe = max(max_nprobe or shape.nprobe, shape.nprobe)
+        most = sum(sorted((len(v) for v in index.lists), reverse=True)[:self.max_nprobe])
+        self.n_res = self.results_needed(most, S, B)
         # ---- per-lane working ciphertexts ----
         self.work = []
         for _ in range(self.lanes):
@@ -193,14 +238,44 @@ class InteractiveQueryManager:
         ciphertexts at L - 2 limbs per lane."""
         return -(-lanes * 2 * max(n_list - 1, 0) * (L - 2) * n // slot_w)
 
-    def _prefix(self, count: int) -> int:
-        if count not in self.mask_prefix:
+    @staticmethod
+    def results_needed(candidates: int, slots: int, B: int) -> int:
+        """Result ciphertexts for `candidates`: a result may end up to B - 1
+        slots short, because batches do not straddle results."""
+        return max(1, -(-candidates // (slots - B + 1)))
+
+    @staticmethod
+    def mask_slots(shape: QueryShape, levels: int, n_list_masks: bool) -> int:
+        """Slots the per-level masks take: one-hot masks (reference compaction)
+        or one stride mask, plus up to B prefix masks, per level."""
+        return levels * ((shape.n_list if n_list_masks else 1) + shape.B)
+
+    def level_of(self, rec: QueryRecord) -> int:
+        return rec.level or self.L
+
+    def out_scale_at(self, lv: int) -> float:
+        """Scale of the results of a query encrypted at level lv."""
+        return self.sh.scale * self.sh.scale / self.p.q[lv - 1]
+
+    def _prefix(self, count: int, lv: int | None = None) -> int:
+        """Mask of the first `count` slots for a query at level lv (prepared
+        for every candidate-batch size at construction)."""
+        lv = lv or self.L
+        key = (count, lv)
+        if key not in self._prefix_lv:
             off = self.slots.take(1)[0]
             m = np.zeros(self.sh.slots)
             m[:count] = 1.0
-            encode_plaintext(self.ctx, self.enc, m, self._mask_scale, off, self.lvl_sq)
-            self.mask_prefix[count] = off
-        return self.mask_prefix[count]
+            encode_plaintext(self.ctx, self.enc, m, float(self.p.q[lv - 2]), off, lv - 1)
+            self._prefix_lv[key] = off
+        return self._prefix_lv[key]
+
+    @staticmethod
+    def _by_level(recs, level_of):
+        groups: dict[int, list[int]] = {}
+        for i, r in enumerate(recs):
+            groups.setdefault(level_of(r), []).append(i)
+        return sorted(groups.items(), reverse=True)
 
     def rotation_steps(self, max_candidates: int | None = None) -> set[int]:
         D, B = self.sh.D, self.sh.B
@@ -360,10 +435,16 @@ class InteractiveQueryManager:
 
     # ---- stages ----
     def stage1_coarse(self, queries: list[QueryRecord]) -> None:
-        """Stages 1 and 1b for every query (lanes at a time)."""
-        if self.sh.compaction == "packed":
-            return self._stage1_packed(queries)
-        D, Ll = self.sh.D, self.L
+        """Stages 1 and 1b for every query (lanes at a time, one level at a time)."""
+        for lv, idx in self._by_level(queries, self.level_of):
+            qs = [queries[i] for i in idx]
+            if self.sh.compaction == "packed":
+                self._stage1_packed(qs, lv)
+            else:
+                self._stage1_reference(qs, lv)
+
+    def _stage1_reference(self, queries: list[QueryRecord], Ll: int) -> None:
+        D = self.sh.D
         for c0 in range(0, len(queries), self.lanes):
             qs = queries[c0:c0 + self.lanes]
             w = self.work[:len(qs)]
@@ -373,14 +454,14 @@ class InteractiveQueryManager:
             self._square(diff, sq, Ll)
             s = 1
             while s < D:                     # sq += rot(sq, s)
-                self._rot_acc(sq, sq, s, self.lvl_sq)
+                self._rot_acc(sq, sq, s, Ll - 1)
                 s <<= 1
-            self._compact(qs, sq)
+            self._compact(qs, sq, Ll)
 
-    def _stage1_packed(self, queries: list[QueryRecord]) -> None:
+    def _stage1_packed(self, queries: list[QueryRecord], Ll: int) -> None:
         """Stage 1 and the packed compaction: items (query, coarse ciphertext k),
         lanes at a time, query-major."""
-        D, Ll, nc = self.sh.D, self.L, self.sh.n_coarse
+        D, nc = self.sh.D, self.sh.n_coarse
         items = [(qi, k) for qi in range(len(queries)) for k in range(nc)]
         for c0 in range(0, len(items), self.lanes):
             it = items[c0:c0 + self.lanes]
@@ -393,13 +474,13 @@ class InteractiveQueryManager:
             self._square(diff, sq, Ll)
             s = 1
             while s < D:                     # sq += rot(sq, s)
-                self._rot_acc(sq, sq, s, self.lvl_sq)
+                self._rot_acc(sq, sq, s, Ll - 1)
                 s <<= 1
-            self._mult_plain(sq, [self.mask_stride] * len(it), sel, self.lvl_sq)
-            self._rotate_grouped([(sel[j], -k) for j, (_, k) in enumerate(it)], self.lvl_out)
-            self._accumulate([(queries[qi].compact, k == 0, sel[j]) for j, (qi, k) in enumerate(it)], self.lvl_out)
+            self._mult_plain(sq, [self._stride[Ll]] * len(it), sel, Ll - 1)
+            self._rotate_grouped([(sel[j], -k) for j, (_, k) in enumerate(it)], Ll - 2)
+            self._accumulate([(queries[qi].compact, k == 0, sel[j]) for j, (qi, k) in enumerate(it)], Ll - 2)
 
-    def _compact(self, qs: list[QueryRecord], sq) -> None:
+    def _compact(self, qs: list[QueryRecord], sq, Ll: int) -> None:
         """Stage 1b (reference compaction) for a chunk of queries: compact =
         sum over i of rot(rescale(sq * mask_i), i * (D - 1)).
 
@@ -415,20 +496,21 @@ class InteractiveQueryManager:
         depth is log2(max shift) rotations plus log2(n_list) additions,
         instead of one eval_rotate after another."""
         D, nl = self.sh.D, self.sh.n_list
+        onehot = self._onehot[Ll]
         comp = [q.compact for q in qs]
         src, pts, dst = [], [], []
         for k in range(len(qs)):
             for i in range(nl):
                 src.append(sq[k])
-                pts.append(self.mask_onehot[i])
+                pts.append(onehot[i])
                 dst.append(comp[k] if i == 0 else self.cmp[k][i - 1])
-        self._mult_plain(src, pts, dst, self.lvl_sq)
+        self._mult_plain(src, pts, dst, Ll - 1)
         if nl == 1:
             return
         self._rotate_grouped([(self.cmp[k][i - 1], i * (D - 1)) for k in range(len(qs)) for i in range(1, nl)],
-                             self.lvl_out)
+                             Ll - 2)
         # per query: comp += sum of its n_list - 1 rotated terms
-        self._sum_groups([[comp[k]] + self.cmp[k] for k in range(len(qs))], self.lvl_out)
+        self._sum_groups([[comp[k]] + self.cmp[k] for k in range(len(qs))], Ll - 2)
 
     def _sum_groups(self, groups, limbs: int) -> None:
         """groups[g][0] += groups[g][1] + ... , all groups side by side, by
@@ -446,18 +528,23 @@ class InteractiveQueryManager:
     def stage3_fine(self, queries: list[QueryRecord]) -> None:
         """Stage 3 for every (query, probed list, batch) item, lanes at a time.
         Each query's `probes` must be set (stage 2)."""
-        D, B, Ll, S = self.sh.D, self.sh.B, self.L, self.sh.slots
-        items = []
+        S = self.sh.slots
+        items: dict[int, list] = {}
         for qi, q in enumerate(queries):
-            off = 0
-            q.vids = []
-            for c in q.probes:
-                for pt, cnt, vids in self.batches[c]:
-                    items.append((qi, pt, cnt, off))
-                    q.vids.extend(vids)
-                    off += cnt
-            if off > self.n_res * S:
+            q.vids, q.pos = [], []
+            lst = items.setdefault(self.level_of(q), [])
+            bs = [b for c in q.probes for b in self.batches[c]]
+            for (pt, cnt, vids), off in zip(bs, batch_offsets([b[1] for b in bs], S)):
+                lst.append((qi, pt, cnt, off))
+                q.vids.extend(vids)
+                q.pos.extend(range(off, off + cnt))
+            if q.pos and q.pos[-1] >= self.n_res * S:
                 raise ValueError("more candidates than the result ciphertexts hold")
+        for lv in sorted(items, reverse=True):
+            self._stage3_items(queries, items[lv], lv)
+
+    def _stage3_items(self, queries: list[QueryRecord], items, Ll: int) -> None:
+        D, B, S = self.sh.D, self.sh.B, self.sh.slots
         for c0 in range(0, len(items), self.lanes):
             it = items[c0:c0 + self.lanes]
             w = self.work[:len(it)]
@@ -468,15 +555,15 @@ class InteractiveQueryManager:
             self._square(diff, sq, Ll)
             s = B
             while s < D * B:                 # sq += rot(sq, s)
-                self._rot_acc(sq, sq, s, self.lvl_sq)
+                self._rot_acc(sq, sq, s, Ll - 1)
                 s <<= 1
-            self._mult_plain(sq, [self._prefix(x[2]) for x in it], sel, self.lvl_sq)
+            self._mult_plain(sq, [self._prefix(x[2], Ll) for x in it], sel, Ll - 1)
             # rotate each item by -(offset mod slots): eval_rotate's steps,
             # grouped across items step by step
-            self._rotate_grouped([(sel[k], -(x[3] % S)) for k, x in enumerate(it)], self.lvl_out)
+            self._rotate_grouped([(sel[k], -(x[3] % S)) for k, x in enumerate(it)], Ll - 2)
             # accumulate into result offset // slots; the item at slot 0 starts it
             self._accumulate([(queries[x[0]].results[x[3] // S], x[3] % S == 0, sel[k]) for k, x in enumerate(it)],
-                             self.lvl_out)
+                             Ll - 2)
 
     # ---- result transfer ----
     def read_ct(self, ct: tuple[int, int]) -> tuple[np.ndarray, np.ndarray]:

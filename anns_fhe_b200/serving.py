@@ -48,6 +48,7 @@ class Request:
     qid: int
     arrival: float          # seconds from the start of the trace
     payload: int            # index into the backend's encrypted-query pool
+    nprobe: int = 0         # lists the client will probe (0: the workload's nprobe)
 
 
 @dataclass
@@ -80,9 +81,16 @@ def poisson_arrivals(rate: float, duration: float, seed: int) -> np.ndarray:
     return t[t < duration]
 
 
-def make_trace(arrivals: np.ndarray, pool: int, seed: int = 0) -> list[Request]:
+def make_trace(arrivals: np.ndarray, pool: int, seed: int = 0, nprobes=None) -> list[Request]:
+    """Requests at the given arrival times, each drawing a pooled encrypted
+    query (and, with `nprobes`, a probe count) uniformly from a seed."""
     rng = np.random.default_rng(seed)
-    return [Request(i, float(t), int(rng.integers(0, pool))) for i, t in enumerate(arrivals)]
+    out = []
+    for i, t in enumerate(arrivals):
+        payload = int(rng.integers(0, pool))
+        nprobe = int(nprobes[rng.integers(0, len(nprobes))]) if nprobes is not None else 0
+        out.append(Request(i, float(t), payload, nprobe))
+    return out
 
 
 def percentile(xs, p: float) -> float:
@@ -105,10 +113,11 @@ class WorkloadBackend:
     """
 
     def __init__(self, wl, Q: np.ndarray | None = None, lanes: int | None = None,
-                 pool: list[list[np.ndarray]] | None = None):
-        """Q: query vectors the client encrypts into the pool; or `pool`:
-        ciphertexts already encrypted, four host arrays (ct_query c0, c1,
-        ct_dim c0, c1) per query."""
+                 pool: list[list[np.ndarray]] | None = None, levels=None, pool_levels=None):
+        """Q: query vectors the client encrypts into the pool (query i at
+        levels[i] limbs, default the top level); or `pool`: ciphertexts
+        already encrypted, four host arrays (ct_query c0, c1, ct_dim c0, c1)
+        per query, at pool_levels[i] limbs (default the top level)."""
         self.wl = wl
         self.iqm = wl.iqm
         self.lib = wl.ctx.lib
@@ -118,13 +127,16 @@ class WorkloadBackend:
         self.n = wl.params.n
         Lw = wl.params.L * self.n
         self.pool: list[list[np.ndarray]] = list(pool or [])
+        self.pool_level = list(pool_levels) if pool_levels is not None else [wl.params.L] * len(self.pool)
         chunk = len(wl.records)
         for c0 in range(0, 0 if Q is None else len(Q), chunk):
             part = Q[c0:c0 + chunk]
             recs = wl.records[:len(part)]
-            wl.encrypt_queries(part, recs)
+            lv = None if levels is None else list(levels[c0:c0 + chunk])
+            wl.encrypt_queries(part, recs, lv)
             for r in recs:
-                self.pool.append([wl.ctx.read_poly(o, Lw) for o in (*r.ct_query, *r.ct_dim)])
+                self.pool.append([wl.ctx.read_poly(o, r.level * self.n) for o in (*r.ct_query, *r.ct_dim)])
+                self.pool_level.append(r.level)
         w = self.iqm.lvl_out * self.n
         # device bytes one in-flight query holds: two encrypted queries at L
         # limbs, the compacted coarse result and n_res candidate results at
@@ -138,9 +150,11 @@ class WorkloadBackend:
         other.lanes = lanes
         return other
 
-    def upload(self, rec, payload: int) -> None:
+    def upload(self, rec, req) -> None:
         from . import _lib as L
-        for off, a in zip((*rec.ct_query, *rec.ct_dim), self.pool[payload]):
+        rec.level = self.pool_level[req.payload]
+        rec.nprobe = req.nprobe
+        for off, a in zip((*rec.ct_query, *rec.ct_dim), self.pool[req.payload]):
             L.check(self.lib.afhe_write_poly_async(self.h, off, a.ctypes.data_as(L.P64), a.size), "write_poly_async")
 
     def coarse(self, recs) -> None:
@@ -172,22 +186,25 @@ class WorkloadBackend:
         box = self.fetch(kind, recs)
         if kind == "dists":
             # only the result ciphertexts that hold candidates
-            need = max(1, -(-max(len(r.vids) for r in recs) // self.iqm.sh.slots))
+            need = max(1, -(-max((max(r.pos) + 1 if r.pos else 1) for r in recs) // self.iqm.sh.slots))
             box = box[:, :need]
         else:
             box = box[:, :1]
         coef = self.wl.client.decrypt_host_batch_coef(box.reshape(-1, 2, self.n), 1)
-        got = {"box": box, "coef": coef.reshape(len(recs), -1)}
+        got = {"box": box, "coef": coef.reshape(len(recs), -1),
+               "scale": np.array([self.iqm.out_scale_at(self.iqm.level_of(r)) for r in recs])}
         if kind == "dists":     # the record may be reused before the top-k is decoded
             got["vids"] = [list(r.vids) for r in recs]
+            got["pos"] = [np.asarray(r.pos, dtype=np.int64) for r in recs]
         return got
 
     def select(self, recs, got: dict) -> None:
         """Stage 2 on the host: decode the coarse distances, keep the nprobe nearest lists."""
         wl = self.wl
-        vals = wl.client.enc.decode_batch(got["coef"], self.iqm.out_scale, self.iqm.coarse_slots_needed()).real
+        vals = wl.client.enc.decode_batch(got["coef"], 1.0, self.iqm.coarse_slots_needed())
+        vals = (vals / got["scale"][:, None]).real
         for r, c in zip(recs, self.iqm.coarse_from_slots(vals)):
-            r.probes = list(np.argsort(c, kind="stable")[:wl.spec.nprobe])
+            r.probes = list(np.argsort(c, kind="stable")[:r.nprobe or wl.spec.nprobe])
 
     def topk(self, recs, got: dict) -> list[list[int]]:
         """Stage 4 on the host: decode the candidate distances, rank them."""
@@ -195,10 +212,11 @@ class WorkloadBackend:
         vids = got["vids"]
         count = len(vids)
         coef = got["coef"].reshape(-1, self.n)               # one row per result ciphertext
-        d = wl.client.enc.decode_batch(coef, self.iqm.out_scale).real.reshape(count, -1)
+        per = coef.shape[0] // count
+        d = (wl.client.enc.decode_batch(coef, 1.0) / np.repeat(got["scale"], per)[:, None]).real.reshape(count, -1)
         out = []
-        for v, row in zip(vids, d):
-            order = np.argsort(row[:len(v)], kind="stable")[:wl.spec.top_k]
+        for v, p, row in zip(vids, got["pos"], d):
+            order = np.argsort(row[p], kind="stable")[:wl.spec.top_k]
             out.append([v[i] for i in order])
         return out
 
@@ -207,7 +225,7 @@ class ServingLoop:
     """Continuous batching over a backend (see the module docstring).
 
     backend: an object with `records`, `bytes_per_query`, `upload(rec,
-    payload)`, `coarse(recs)`, `fine(recs)`, `receive(kind, recs)`,
+    request)`, `coarse(recs)`, `fine(recs)`, `receive(kind, recs)`,
     `select(recs, got)` and `topk(recs, got)`; `WorkloadBackend` drives the
     GPU.
     budget_bytes: HBM the in-flight queries may hold (None: every record).
@@ -267,7 +285,7 @@ class ServingLoop:
                 continue
             arecs = [rec for _, rec, _ in admit]
             for req, rec, _ in admit:
-                self.b.upload(rec, req.payload)
+                self.b.upload(rec, req)
             if arecs:
                 self.b.coarse(arecs)
             # host work of the previous tick, overlapping the stage 1 just launched

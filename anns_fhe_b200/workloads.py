@@ -83,7 +83,9 @@ def dimpack_layout(q: np.ndarray, sh: QueryShape) -> np.ndarray:
 
 class Workload:
     def __init__(self, spec: WorkloadSpec = SMALL, max_queries: int = 64, lanes: int = 64, device: int = 0,
-                 index: IvfPqIndex | None = None):
+                 index: IvfPqIndex | None = None, levels=None, max_nprobe: int | None = None):
+        """levels: query levels to serve besides the top one (mixed-level
+        traffic); max_nprobe: the most lists one query may probe."""
         self.spec = spec
         t0 = time.time()
         self.X = gaussian_mixture(spec.n_vectors, spec.d, spec.components, spec.sigma, spec.seed)
@@ -98,14 +100,17 @@ class Workload:
         slot_w = (self.params.L + self.params.K) * n
         B = slots // spec.d
         n_batches = sum(-(-len(v) // B) for v in self.index.lists)
-        n_res = -(-sum(sorted((len(v) for v in self.index.lists), reverse=True)[:spec.nprobe]) // slots)
+        most_probes = max(max_nprobe or spec.nprobe, spec.nprobe)
+        n_res = InteractiveQueryManager.results_needed(
+            sum(sorted((len(v) for v in self.index.lists), reverse=True)[:most_probes]), slots, B)
+        lvls = sorted(set(levels or []) | {self.params.L})
         w_out = (self.params.L - 2) * n
         most = max(max_queries, lanes) * max(n_res, 1)
         # client staging: results arrive as limb 0 (N words per polynomial)
         dec_slots = -(-most * 2 * n // slot_w) + -(-most * n // slot_w)
         outbox_slots = -(-2 * max_queries * w_out // slot_w) + -(-2 * max_queries * n_res * w_out // slot_w)
-        masks = spec.n_list if spec.compaction == "reference" else 1
-        n_slots = (16 + shape.n_coarse + masks + n_batches + B + 8 * lanes + 4 * max_queries + outbox_slots + 64
+        masks = InteractiveQueryManager.mask_slots(shape, len(lvls), spec.compaction == "reference")
+        n_slots = (16 + shape.n_coarse + masks + n_batches + 8 * lanes + 4 * max_queries + outbox_slots + 64
                    + InteractiveQueryManager.compaction_slots(spec.n_list if spec.compaction == "reference" else 1,
                                                               self.params.L, n, slot_w, lanes)
                    + dec_slots)
@@ -114,7 +119,8 @@ class Workload:
                               max_batch=lanes)
         self.slots = Slots(self.params, 0, n_slots * slot_w)
         self.client = CkksClient(self.ctx, self.slots, seed=spec.seed + 7)
-        self.iqm = InteractiveQueryManager(self.ctx, self.index, shape, self.slots, lanes=lanes)
+        self.iqm = InteractiveQueryManager(self.ctx, self.index, shape, self.slots, lanes=lanes, levels=lvls,
+                                           max_nprobe=most_probes)
         self.steps = self.iqm.rotation_steps()
         self.client.install_keys(self.steps)
         self.records = self.iqm.alloc_queries(max_queries)
@@ -131,47 +137,60 @@ class Workload:
         return (self.X[idx] + rng.normal(0, self.spec.sigma / 2, (count, self.spec.d))).astype(np.float32)
 
     # ---- client side ----
-    def encrypt_queries(self, Q: np.ndarray, recs: list[QueryRecord]) -> None:
+    def encrypt_queries(self, Q: np.ndarray, recs: list[QueryRecord], levels=None) -> None:
+        """Encrypt each query (both layouts) into its record, at levels[i]
+        limbs (default: the top level)."""
         sh = self.iqm.sh
-        for q, r in zip(Q, recs):
-            self.client.encrypt(query_layout(q, sh), sh.scale, r.ct_query[0], r.ct_query[1])
-            self.client.encrypt(dimpack_layout(q, sh), sh.scale, r.ct_dim[0], r.ct_dim[1])
+        for i, (q, r) in enumerate(zip(Q, recs)):
+            lv = levels[i] if levels is not None else self.params.L
+            r.level = lv
+            self.client.encrypt(query_layout(q, sh), sh.scale, r.ct_query[0], r.ct_query[1], level=lv)
+            self.client.encrypt(dimpack_layout(q, sh), sh.scale, r.ct_dim[0], r.ct_dim[1], level=lv)
 
-    def decrypt_many(self, cts, slots: int | None = None) -> np.ndarray:
+    def decrypt_many(self, cts, scales, slots: int | None = None) -> np.ndarray:
         """Decrypt result ciphertexts resident on the device from limb 0 (the
-        messages are far below q_0 / 2; the query manager checks the bound)."""
-        return self.client.decrypt_batch(cts, 1, self.iqm.out_scale, slots).real
+        messages are far below q_0 / 2; the query manager checks the bound);
+        row i is decoded at scales[i]."""
+        coef = self.client.decrypt_batch_coef(cts, 1)
+        return (self.client.enc.decode_batch(coef, 1.0, slots) / np.asarray(scales, dtype=np.float64)[:, None]).real
 
     def coarse(self, recs) -> np.ndarray:
         """(count, n_list) decrypted coarse distances."""
-        vals = self.decrypt_many([r.compact for r in recs], self.iqm.coarse_slots_needed())
+        scales = [self.iqm.out_scale_at(self.iqm.level_of(r)) for r in recs]
+        vals = self.decrypt_many([r.compact for r in recs], scales, self.iqm.coarse_slots_needed())
         return self.iqm.coarse_from_slots(vals)
 
     def candidates(self, recs) -> list[np.ndarray]:
         """Each query's decrypted candidate distances, in stage-3 order."""
         S = self.iqm.sh.slots
-        need = [max(1, -(-len(r.vids) // S)) for r in recs]
-        vals = self.decrypt_many([ct for r, k in zip(recs, need) for ct in r.results[:k]])
+        need = [max(1, -(-(max(r.pos) + 1) // S)) if r.pos else 1 for r in recs]
+        scales = [self.iqm.out_scale_at(self.iqm.level_of(r)) for r, k in zip(recs, need) for _ in range(k)]
+        vals = self.decrypt_many([ct for r, k in zip(recs, need) for ct in r.results[:k]], scales)
         out, i = [], 0
         for r, k in zip(recs, need):
-            out.append(vals[i:i + k].ravel()[:len(r.vids)])
+            out.append(vals[i:i + k].ravel()[np.asarray(r.pos, dtype=np.int64)])
             i += k
         return out
 
     def select(self, recs) -> None:
-        """Stage 2 (client): decrypt the compacted coarse distances, keep nprobe lists."""
+        """Stage 2 (client): decrypt the compacted coarse distances, keep each
+        query's nprobe nearest lists."""
         for r, c in zip(recs, self.coarse(recs)):
-            r.probes = list(np.argsort(c, kind="stable")[:self.spec.nprobe])
+            r.probes = list(np.argsort(c, kind="stable")[:r.nprobe or self.spec.nprobe])
 
     # ---- protocol ----
-    def run(self, Q: np.ndarray, recs: list[QueryRecord] | None = None):
-        """Full protocol for a batch of queries; returns per-query dicts."""
+    def run(self, Q: np.ndarray, recs: list[QueryRecord] | None = None, levels=None, nprobes=None):
+        """Full protocol for a batch of queries; returns per-query dicts.
+        levels / nprobes: per-query encryption level and probe count
+        (default: the top level and the spec's nprobe)."""
         recs = recs or self.records[:len(Q)]
-        self.encrypt_queries(Q, recs)
+        for i, r in enumerate(recs):
+            r.nprobe = nprobes[i] if nprobes is not None else 0
+        self.encrypt_queries(Q, recs, levels)
         self.iqm.stage1_coarse(recs)
         out = []
         for r, c in zip(recs, self.coarse(recs)):
-            r.probes = list(np.argsort(c, kind="stable")[:self.spec.nprobe])
+            r.probes = list(np.argsort(c, kind="stable")[:r.nprobe or self.spec.nprobe])
             out.append({"coarse": c, "probes": r.probes})
         self.iqm.stage3_fine(recs)
         for r, o, d in zip(recs, out, self.candidates(recs)):
@@ -179,9 +198,9 @@ class Workload:
             o.update(dists=d, vids=list(r.vids), topk=[r.vids[i] for i in order])
         return out
 
-    def plaintext(self, q: np.ndarray):
+    def plaintext(self, q: np.ndarray, nprobe: int | None = None):
         coarse = plaintext_coarse(self.index, q)
-        probes, cand, dist, top = plaintext_search(self.index, q, self.spec.nprobe, self.spec.top_k)
+        probes, cand, dist, top = plaintext_search(self.index, q, nprobe or self.spec.nprobe, self.spec.top_k)
         return coarse, probes, cand, dist, top
 
     def close(self) -> None:

@@ -132,7 +132,7 @@ def run_ours(args, rank: int, world: int):
         S = iqm.sh.slots
         dists = wl.client.decrypt_host_batch(box.reshape(-1, 2, n), 1, iqm.out_scale).real.reshape(len(recs), -1)
         for r, d in zip(recs, dists):
-            np.argsort(d[:len(r.vids)], kind="stable")[:wl.spec.top_k]
+            np.argsort(d[np.asarray(r.pos)], kind="stable")[:wl.spec.top_k]
         eb.record(stream)
         eb.synchronize()
         return ea.elapsed_time(eb), h2d, d2h
@@ -232,29 +232,44 @@ def serve_leg(args, wl, host_cts, rank: int):
                                 f"unless --serve-rate is given)"}}
 
 
-def serve_sweep(rates, seconds: float, batch: int):
+def serve_sweep(rates, seconds: float, batch: int, workload: str = "small", mixed: bool = False,
+                plain_queries: int = 32):
     """Serving driver: the plain path's latency and rate, then the served loop
     at each offered rate for `seconds` (seeded Poisson arrivals); one JSON
-    line per rate."""
+    line per rate. `mixed` is the serving trace's query mix: levels drawn
+    from 6..12 and nprobe from {4, 8, 16, 32}, on the large configuration,
+    with a 120 GB admission budget."""
+    import numpy as np
+    import torch
+
     from anns_fhe_b200.serving import (Request, ServingLoop, WorkloadBackend, make_trace, percentile,
                                        poisson_arrivals, summarize)
-    from anns_fhe_b200.workloads import Workload
-    import torch
-    wl = Workload(max_queries=2 * batch, lanes=batch)
-    pool = WorkloadBackend(wl, wl.queries(batch, seed=77)).pool
-    be = WorkloadBackend(wl, pool=[[torch.from_numpy(a).pin_memory().numpy() for a in cts] for cts in pool])
+    from anns_fhe_b200.workloads import LARGE, SMALL, Workload
+    spec = LARGE if workload == "large" else SMALL
+    levels = list(range(6, spec.num_q + 1)) if mixed else None
+    nprobes = [4, 8, 16, 32] if mixed else None
+    wl = Workload(spec, max_queries=2 * batch, lanes=batch, levels=levels, max_nprobe=32 if mixed else None)
+    pool_levels = (np.random.default_rng(5).integers(6, spec.num_q + 1, batch).tolist() if mixed else None)
+    enc = WorkloadBackend(wl, wl.queries(batch, seed=77), levels=pool_levels)
+    be = WorkloadBackend(wl, pool=[[torch.from_numpy(a).pin_memory().numpy() for a in cts] for cts in enc.pool],
+                         pool_levels=enc.pool_level)
+    budget = 120e9 if mixed else None
     plain = be.with_lanes(1)
-    ServingLoop(plain, max_inflight=1).run([Request(0, 0.0, 0)], realtime=False)
-    svc = [ServingLoop(plain, max_inflight=1).run([Request(i, 0.0, i)], realtime=False)[0].service * 1e3
-           for i in range(32)]
-    print(json.dumps({"path": "plain", "queries_per_s": 1e3 * len(svc) / sum(svc),
-                      "p50_ms": percentile(svc, 50), "p99_ms": percentile(svc, 99)}), flush=True)
-    ServingLoop(be).run(make_trace(poisson_arrivals(200.0, 0.5, seed=1), pool=batch, seed=1))
+    ptrace = make_trace(np.zeros(plain_queries + 1), pool=batch, seed=9, nprobes=nprobes)
+    ServingLoop(plain, max_inflight=1).run([ptrace[0]], realtime=False)
+    svc = [ServingLoop(plain, max_inflight=1).run([r], realtime=False)[0].service * 1e3 for r in ptrace[1:]]
+    print(json.dumps({"path": "plain", "workload": spec.name, "mixed": mixed,
+                      "queries_per_s": 1e3 * len(svc) / sum(svc), "p50_ms": percentile(svc, 50),
+                      "p99_ms": percentile(svc, 99), "queries": len(svc)}), flush=True)
+    ServingLoop(be, budget_bytes=budget).run(make_trace(poisson_arrivals(max(rates[0], 1.0), 2.0, seed=1),
+                                                        pool=batch, seed=1, nprobes=nprobes))
     for r in rates:
-        trace = make_trace(poisson_arrivals(r, seconds, seed=int(r)), pool=batch, seed=int(r) + 1)
-        loop = ServingLoop(be)
+        trace = make_trace(poisson_arrivals(r, seconds, seed=int(r * 10)), pool=batch, seed=int(r * 10) + 1,
+                           nprobes=nprobes)
+        loop = ServingLoop(be, budget_bytes=budget)
         s = summarize(loop.run(trace))
-        s.update(path="served", offered_qps=r, offered=len(trace), ticks=loop.ticks, seconds=seconds)
+        s.update(path="served", offered_qps=r, offered=len(trace), ticks=loop.ticks, seconds=seconds,
+                 max_inflight=loop.capacity)
         print(json.dumps(s), flush=True)
     wl.close()
 
@@ -500,6 +515,7 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=0.0, help="served trace rate (default: 10x plain)")
     ap.add_argument("--serve-seconds", type=float, default=5.0, help="served trace length")
     ap.add_argument("--serve-sweep", default="", help="serving driver: comma-separated offered rates (queries/s)")
+    ap.add_argument("--mixed", action="store_true", help="serving driver: mixed query levels 6-12 and nprobe")
     ap.add_argument("--ntt-config", action="store_true", help="NTT microbenchmark driver (64 ct x 2 x 24 limbs, N=2^16)")
     ap.add_argument("--ks-config", action="store_true", help="batched key-switch driver (32 ct, N=2^16, dnum 3)")
     ap.add_argument("--profile-step", type=int, default=0, help="profiling driver: queries per step")
@@ -513,7 +529,9 @@ def main():
     if args.ks_config:
         return ks_config()
     if args.serve_sweep:
-        return serve_sweep([float(x) for x in args.serve_sweep.split(",")], args.serve_seconds, args.batch or 296)
+        return serve_sweep([float(x) for x in args.serve_sweep.split(",")], args.serve_seconds,
+                           args.batch or (256 if args.workload == "large" else 296), args.workload, args.mixed,
+                           args.plain_queries)
     if args.profile_step:
         return profile_step(args.profile_step, args.workload, args.lanes)
     if args.profile_ntt:

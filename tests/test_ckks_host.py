@@ -78,3 +78,22 @@ def test_query_layouts():
     # coarse slot map: list k * per_ct + c at slot c * D + k
     assert packed.coarse_slot(8 * 2 + 5) == 5 * 8 + 2
     assert sorted(packed.coarse_slot(c) for c in range(20)) == sorted({packed.coarse_slot(c) for c in range(20)})
+
+
+def test_batch_offsets_never_straddle():
+    """Candidate batches land whole in one result ciphertext, back to back
+    otherwise, and fit the number of results `results_needed` reserves."""
+    import numpy as np
+
+    from anns_fhe_b200.query import InteractiveQueryManager, batch_offsets
+    rng = np.random.default_rng(0)
+    for S, B in ((512, 64), (16384, 128), (4096, 64)):
+        counts = [int(x) for x in rng.integers(1, B + 1, 400)]
+        offs = batch_offsets(counts, S)
+        end = 0
+        for off, cnt in zip(offs, counts):
+            assert off // S == (off + cnt - 1) // S, "batch crosses a result boundary"
+            assert off == end or (off % S == 0 and off > end), "gap other than a result start"
+            end = off + cnt
+        assert end <= InteractiveQueryManager.results_needed(sum(counts), S, B) * S
+    assert batch_offsets([3, 3, 3], 8) == [0, 3, 8]

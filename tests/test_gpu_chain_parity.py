@@ -34,10 +34,11 @@ TINY = WorkloadSpec("ivfpq_512x8_nlist8_N1024_L3", n_vectors=512, d=8, component
                     nprobe=2, top_k=4, log_n=10, num_q=3, q_bits=50, num_p=1, p_bits=60, alpha=1, log_scale=40)
 
 
-def reference_chain(wl, ora, ct, ct_dim, probes):
-    """One query through the reference's sequential chain on the oracle."""
+def reference_chain(wl, ora, ct, ct_dim, probes, level=None):
+    """One query through the reference's sequential chain on the oracle, at
+    the query's level (default: the top level)."""
     iqm, p = wl.iqm, wl.params
-    n, L = p.n, p.L
+    n, L = p.n, level or p.L
     D, B, nl = iqm.sh.D, iqm.sh.B, iqm.sh.n_list
     kw = p.key_words()
     half = kw // 2
@@ -63,7 +64,7 @@ def reference_chain(wl, ora, ct, ct_dim, probes):
         diff = ora.eval_sub_plain(ct, pt(iqm.pt_centroids, L), L)
         sq = tree(ora.eval_mult_relin_rescale(diff, diff, relin, L), 1)
         for i in range(nl):
-            sel = ora.eval_mult_plain_rescale(sq, pt(iqm.mask_onehot[i], L - 1), L - 1)
+            sel = ora.eval_mult_plain_rescale(sq, pt(iqm._onehot[L][i], L - 1), L - 1)
             if i:
                 sel = ora.eval_rotate(sel, i * (D - 1), rot, L - 2)
             comp = sel if comp is None else ora.eval_add(comp, sel, L - 2)
@@ -72,7 +73,7 @@ def reference_chain(wl, ora, ct, ct_dim, probes):
         for k, pk in enumerate(iqm.pt_centroid_cts):
             diff = ora.eval_sub_plain(ct, pt(pk, L), L)
             sq = tree(ora.eval_mult_relin_rescale(diff, diff, relin, L), 1)
-            sel = ora.eval_mult_plain_rescale(sq, pt(iqm.mask_stride, L - 1), L - 1)
+            sel = ora.eval_mult_plain_rescale(sq, pt(iqm._stride[L], L - 1), L - 1)
             if k:
                 sel = ora.eval_rotate(sel, -k, rot, L - 2)
             comp = sel if comp is None else ora.eval_add(comp, sel, L - 2)
@@ -81,9 +82,11 @@ def reference_chain(wl, ora, ct, ct_dim, probes):
     off, acc = 0, {}
     for c in probes:
         for pt_off, cnt, _ in iqm.batches[c]:
+            if off % S + cnt > S:       # a batch that does not fit starts the next result
+                off = (off // S + 1) * S
             diff = ora.eval_sub_plain(ct_dim, pt(pt_off, L), L)
             sq = tree(ora.eval_mult_relin_rescale(diff, diff, relin, L), B)
-            sel = ora.eval_mult_plain_rescale(sq, pt(iqm.mask_prefix[cnt], L - 1), L - 1)
+            sel = ora.eval_mult_plain_rescale(sq, pt(iqm._prefix_lv[(cnt, L)], L - 1), L - 1)
             if off % S:
                 sel = ora.eval_rotate(sel, -(off % S), rot, L - 2)
             r = off // S
@@ -92,27 +95,29 @@ def reference_chain(wl, ora, ct, ct_dim, probes):
     return comp, [acc[r] for r in sorted(acc)]
 
 
-def run_and_compare(spec, nq, lanes, orc):
-    wl = Workload(spec, max_queries=nq, lanes=lanes)
+def run_and_compare(spec, nq, lanes, orc, levels=None):
+    """levels: per-query encryption levels (mixed in the same batches)."""
+    wl = Workload(spec, max_queries=nq, lanes=lanes, levels=sorted(set(levels)) if levels else None)
     try:
         p = wl.params
-        n, L = p.n, p.L
+        n = p.n
         recs = wl.records[:nq]
-        wl.encrypt_queries(wl.queries(nq, seed=21), recs)
-        ins = [((wl.ctx.read_poly(r.ct_query[0], L * n), wl.ctx.read_poly(r.ct_query[1], L * n)),
-                (wl.ctx.read_poly(r.ct_dim[0], L * n), wl.ctx.read_poly(r.ct_dim[1], L * n))) for r in recs]
+        wl.encrypt_queries(wl.queries(nq, seed=21), recs, levels)
+        ins = [((wl.ctx.read_poly(r.ct_query[0], r.level * n), wl.ctx.read_poly(r.ct_query[1], r.level * n)),
+                (wl.ctx.read_poly(r.ct_dim[0], r.level * n), wl.ctx.read_poly(r.ct_dim[1], r.level * n)))
+               for r in recs]
         wl.iqm.stage1_coarse(recs)
         wl.select(recs)
         wl.iqm.stage3_fine(recs)
         ora = OracleCKKS(p.log_n, p.q, p.p, p.alpha, orc)
         results_used = set()
         for r, (ct, ct_dim) in zip(recs, ins):
-            comp, accs = reference_chain(wl, ora, ct, ct_dim, r.probes)
-            got_c = wl.iqm.read_ct(r.compact)
+            comp, accs = reference_chain(wl, ora, ct, ct_dim, r.probes, r.level)
+            got_c = [a[:(r.level - 2) * n] for a in wl.iqm.read_ct(r.compact)]
             assert np.array_equal(got_c[0], comp[0]) and np.array_equal(got_c[1], comp[1]), "stage 1b differs"
             results_used.add(len(accs))
             for k, acc in enumerate(accs):
-                got_d = wl.iqm.read_ct(r.results[k])
+                got_d = [a[:(r.level - 2) * n] for a in wl.iqm.read_ct(r.results[k])]
                 assert np.array_equal(got_d[0], acc[0]) and np.array_equal(got_d[1], acc[1]), \
                     f"stage 3 result {k} differs"
         return wl.iqm, results_used
@@ -136,6 +141,13 @@ def test_packed_chain_matches_oracle_replay(orc):
     iqm, used = run_and_compare(TINY_PACKED, nq=2, lanes=16, orc=orc)
     assert iqm.sh.n_coarse == 2 and iqm.n_res >= 2
     assert max(used) >= 2, "no query spilled into a second result ciphertext"
+
+
+def test_mixed_levels_match_oracle_replay(orc):
+    """Queries at levels 4 and 3 in the same batches: each one's chain runs
+    at its own level (masks per level) and equals the oracle replay there."""
+    iqm, _ = run_and_compare(TINY_PACKED, nq=3, lanes=16, orc=orc, levels=[4, 3, 3])
+    assert iqm.levels == [3, 4]
 
 
 def test_chain_matches_reference_bench_configuration(orc):

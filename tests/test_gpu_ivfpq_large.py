@@ -36,7 +36,8 @@ TOL = 0.25
 
 @pytest.fixture(scope="module")
 def big():
-    wl = Workload(LARGE, max_queries=4, lanes=64)
+    # ready for the serving trace's mixed traffic: query levels 6-12, up to 32 probes
+    wl = Workload(LARGE, max_queries=4, lanes=64, levels=list(range(6, 13)), max_nprobe=32)
     yield wl
     wl.close()
 
@@ -53,18 +54,23 @@ def _same_up_to_ties(got, want_order, dist, margin):
     return ok, ties
 
 
-def test_large_end_to_end_matches_plaintext(big):
-    Q = big.queries(3, seed=8)
-    res = big.run(Q)
+@pytest.mark.parametrize("mixed", [False, True], ids=["top_level", "mixed_levels_and_probes"])
+def test_large_end_to_end_matches_plaintext(big, mixed):
+    """mixed: the serving trace's shapes, queries at levels 6, 9, 12 with 4,
+    32 and 16 probes in one batch."""
+    Q = big.queries(3, seed=8 + mixed)
+    levels, nprobes = ([6, 9, 12], [4, 32, 16]) if mixed else (None, None)
+    res = big.run(Q, levels=levels, nprobes=nprobes)
     errs = []
-    for q, r in zip(Q, res):
-        coarse, probes, cand, dist, top = big.plaintext(q)
+    for i, (q, r) in enumerate(zip(Q, res)):
+        npb = nprobes[i] if mixed else big.spec.nprobe
+        coarse, probes, cand, dist, top = big.plaintext(q, npb)
         ec = float(np.max(np.abs(r["coarse"] - coarse)))
         assert ec < TOL_COARSE, f"coarse error {ec}"
         assert len(r["coarse"]) == 1024
         order = np.argsort(coarse, kind="stable")
         ok, ties = _same_up_to_ties(r["probes"], order, np.sort(coarse), 2 * ec)
-        assert ok, f"probes differ beyond near-ties: {r['probes']} vs {list(order[:16])}"
+        assert ok, f"probes differ beyond near-ties: {r['probes']} vs {list(order[:npb])}"
         if ties:
             print(f"near-tie at the probe boundary: lists {[int(order[i]) for i in ties]}")
         if list(r["probes"]) != list(probes):

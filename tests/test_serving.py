@@ -28,10 +28,10 @@ class FakeBackend:
         self.payload = {}
         self.busy = set()      # records whose query's results are not yet on the host
 
-    def upload(self, rec, payload):
+    def upload(self, rec, req):
         assert rec.i not in self.busy, "record reused while its query is in flight"
         self.busy.add(rec.i)
-        self.payload[rec.i] = payload
+        self.payload[rec.i] = req.payload
 
     def coarse(self, recs):
         self.log.append(("coarse", [r.i for r in recs]))
@@ -119,6 +119,14 @@ def test_realtime_latency_and_order():
         assert c.done >= c.arrival and c.admitted >= c.arrival - 1e-9
     s = summarize(done)
     assert s["completed"] == 5 and s["p99_ms"] >= s["p50_ms"] >= 0
+
+
+def test_trace_mixed_probes():
+    tr = make_trace(np.arange(200) * 0.01, pool=5, seed=3, nprobes=[4, 8, 16, 32])
+    assert {r.nprobe for r in tr} == {4, 8, 16, 32}
+    assert all(0 <= r.payload < 5 for r in tr)
+    assert [r.nprobe for r in tr] == [r.nprobe for r in make_trace(np.arange(200) * 0.01, pool=5, seed=3,
+                                                                   nprobes=[4, 8, 16, 32])]
 
 
 def test_poisson_rate_and_percentile():
