@@ -130,6 +130,7 @@ SIGNATURES = {
     "afhe_eval_mult_plain_rescale_batch": (C.c_int, [CTX, C.POINTER(CtRef), P64, C.POINTER(CtRef), u32, u32]),
     "afhe_rescale_batch": (C.c_int, [CTX, C.POINTER(CtRef), C.POINTER(CtRef), u32, u32]),
     "afhe_eval_copy_batch": (C.c_int, [CTX, C.POINTER(CtRef), C.POINTER(CtRef), u32, u32]),
+    "afhe_eval_rotate_steps_batch": (C.c_int, [CTX, C.POINTER(CtRef), C.POINTER(CtRef), C.POINTER(i32), u32, u32]),
 }
 
 _lib = None

@@ -565,6 +565,49 @@ int afhe_eval_rotate_accumulate_batch(afhe_ctx* ctx, const afhe_ct_ref* in, cons
     });
 }
 
+int afhe_eval_rotate_steps_batch(afhe_ctx* ctx, const afhe_ct_ref* in, const afhe_ct_ref* dst, const int32_t* steps,
+                                 uint32_t count, uint32_t limbs) {
+    if (!ctx || (count && (!in || !dst || !steps))) return fail(ctx, AFHE_E_ARG, "null argument");
+    int rc;
+    if ((rc = check_limbs(ctx, limbs, 1)) || (rc = check_cts(ctx, in, count, limbs)) ||
+        (rc = check_cts(ctx, dst, count, limbs)))
+        return rc;
+    for (uint32_t i = 0; i < count; ++i)
+        if (!ctx->rot.count(steps[i]))
+            return fail(ctx, AFHE_E_NOKEY, "rotation key not found for step " + std::to_string(steps[i]));
+    const u64 n = ctx->n, S = (u64)ctx->L + ctx->K;
+    const OpTabs& t = ctx->lv[limbs];
+    const LevelJobs& lj = ctx->lvjobs[limbs];
+    // eval_rotate_single_step per entry (fhe_host_driver.cpp:331-359), each
+    // with its own key and automorphism, as one multi-kernel key switch:
+    // every input is read before any output is written, so outputs may
+    // alias inputs
+    return for_chunks(ctx, count, [&](uint32_t s, uint32_t m) -> int {
+        Offs i0(m), i1(m), o0(m), o1(m), maps(m), keys(m);
+        for (uint32_t z = 0; z < m; ++z) {
+            const RotKey& rk = ctx->rot.at(steps[s + z]);
+            i0[z] = in[s + z].c0_offset; i1[z] = in[s + z].c1_offset;
+            o0[z] = dst[s + z].c0_offset; o1[z] = dst[s + z].c1_offset;
+            maps[z] = (u64)(uintptr_t)rk.map;
+            keys[z] = rk.evk_offset;
+        }
+        KsFuse f{};
+        f.has_c0 = 1;
+        f.per_z = 1;
+        ZF(f.c0, i0);
+        ZF(f.mapz, maps);
+        ZF(f.keyz, keys);
+        ZBases zb{};
+        ZF(zb.src, i1);
+        ZF(zb.out, o0);
+        ZF(zb.aux, o1);
+        zb.mid = lane_field(ctx, &Lane::ks);
+        CK(launch_key_switch(ctx->log_n, t, ctx->jobs_qp, lj.modup, lj.n_modup, ctx->L, limbs, ctx->K, ctx->key, 0,
+                             (u64)ctx->dnum * S * n, (uint32_t)S, ctx->L, ctx->poly, ctx->scr, m, zb, ctx->st, &f));
+        return AFHE_OK;
+    });
+}
+
 int afhe_eval_rotate(afhe_ctx* ctx, uint64_t i0, uint64_t i1, uint64_t d0, uint64_t d1, int32_t total, uint32_t limbs) {
     afhe_ct_ref in{i0, i1}, d{d0, d1};
     return afhe_eval_rotate_batch(ctx, &in, &d, 1, total, limbs);

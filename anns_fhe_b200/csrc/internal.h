@@ -166,11 +166,16 @@ cudaError_t launch_rescale(int log_n, const OpTabs& t, const LimbJob* jobs_q, ui
 //   * has_c0: ks0 output += c0[map[x]] (c0 gathered into scratch by the MAC);
 //   * has_acc: ks0 output += acc0[x], ks1 output += acc1[x].
 // So one call computes a whole rotation step, acc + rot(ct), or d + KS(d2).
+// With per_z (multi-kernel key switch only), entry z has its own rotation:
+// its automorphism map at the device address mapz.at(z), and its key at
+// keyz.at(z) words past evk_a / evk_b.
 struct KsFuse {
     const uint32_t* map;
     int has_c0;
     int has_acc;
     ZField c0, acc0, acc1;
+    int per_z;
+    ZField mapz, keyz;
 };
 size_t ks_scratch_words(uint32_t n, uint32_t L, uint32_t K, uint32_t parts);
 cudaError_t launch_key_switch(int log_n, const OpTabs& t, const LimbJob* jobs_qp, const LimbJob* jobs_modup,

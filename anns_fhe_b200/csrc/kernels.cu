@@ -218,9 +218,12 @@ size_t ks_scratch_words(uint32_t n, uint32_t slots_q, uint32_t K, uint32_t parts
 struct LoadGather {
     const u64* base;
     const uint32_t* map;
+    ZField mapz;        // per-entry map addresses (per_z)
+    int per_z;
     __device__ __forceinline__ u64 operator()(const LimbJob& j, const ZBases& zb, uint32_t z, uint32_t x,
                                               const PrimeConst&) const {
-        return base[zb.src.at(z) + j.src + __ldg(map + x)];
+        const uint32_t* m = per_z ? (const uint32_t*)mapz.at(z) : map;
+        return base[zb.src.at(z) + j.src + __ldg(m + x)];
     }
 };
 
@@ -308,8 +311,10 @@ __global__ void __launch_bounds__(256) ks_mac_kernel(OpTabs t, uint32_t n, uint3
     const u64 base_scr = zb.mid.at(z);
     const u64* in = arena + zb.src.at(z) + (u64)sidx * n;   // only valid for Q limbs
     const u64 c0_off = f.has_c0 ? f.c0.at(z) : 0;
+    const uint32_t* map = f.per_z ? (const uint32_t*)f.mapz.at(z) : f.map;
+    const u64 koff = f.per_z ? f.keyz.at(z) : 0;           // this entry's key (per_z)
     for (uint32_t x = blockIdx.x * blockDim.x + threadIdx.x; x < n; x += gridDim.x * blockDim.x) {
-        const uint32_t xs = f.map ? __ldg(f.map + x) : x;     // position read through the automorphism
+        const uint32_t xs = map ? __ldg(map + x) : x;         // position read through the automorphism
         if (isq && f.has_c0)
             scratch[base_scr + t0_off + (u64)sidx * n + x] = arena[c0_off + (u64)sidx * n + xs];
         Acc128 ab, aa;
@@ -321,7 +326,7 @@ __global__ void __launch_bounds__(256) ks_mac_kernel(OpTabs t, uint32_t n, uint3
             u64 d;
             if (isq && sidx >= start && sidx < start + size) d = in[xs];
             else d = scratch[base_scr + modup_off + ((u64)part * S + slot) * n + x];
-            const u64 kl = ((u64)part * key_stride + klimb_in_digit) * n + x;
+            const u64 kl = koff + ((u64)part * key_stride + klimb_in_digit) * n + x;
             acc_mad(ab, d, __ldg(key + evk_b + kl));
             acc_mad(aa, d, __ldg(key + evk_a + kl));
         }
@@ -400,9 +405,9 @@ cudaError_t launch_key_switch(int log_n, const OpTabs& t, const LimbJob* jobs_qp
         ZBases a = zb;
         a.mid = zf_plus(zb.mid, off_coef);
         a.out = a.mid;
-        if (f.map)
-            e = launch_ntt<true>(log_n, t.pt, jobs_qp, sizeQl, nz, scratch, a, LoadGather{arena, f.map},
-                                 StoreQhatInv{scratch, t}, st);
+        if (f.map || f.per_z)
+            e = launch_ntt<true>(log_n, t.pt, jobs_qp, sizeQl, nz, scratch, a,
+                                 LoadGather{arena, f.map, f.mapz, f.per_z}, StoreQhatInv{scratch, t}, st);
         else
             e = launch_ntt<true>(log_n, t.pt, jobs_qp, sizeQl, nz, scratch, a, LoadPlain{arena},
                                  StoreQhatInv{scratch, t}, st);

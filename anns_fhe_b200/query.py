@@ -25,12 +25,16 @@ Two compactions:
     coarse ciphertext k. Each coarse ciphertext's tree sum is masked at every
     slot c * D at once, rescaled, rotated right by k and summed, so one
     ciphertext returns all n_list distances (list k * (slots / D) + c at slot
-    c * D + k). That takes n_coarse key switches per query instead of the
-    reference's sum over lists of popcount(i * (D - 1)).
-Candidate distances past `slots` continue in further result ciphertexts
-(position p at slot p mod slots of result p // slots). A candidate batch
-never straddles two results: one that would not fit starts the next result,
-so every batch lands whole in one ciphertext.
+    c * D + k). That takes n_coarse - 1 key switches per query instead of
+    the reference's sum over lists of popcount(i * (D - 1)).
+    The packed chain also places candidates more cheaply: candidate batch t
+    of a query starts at slot (t mod (slots / B)) * B of result t // (slots /
+    B), and its placement rotation is one key switch with a key made for that
+    step, instead of eval_rotate's popcount(offset) power-of-two steps.
+In the reference chain, candidate distances past `slots` continue in further
+result ciphertexts (position p at slot p mod slots of result p // slots). A
+candidate batch never straddles two results: one that would not fit starts
+the next result, so every batch lands whole in one ciphertext.
 
 Phase-3 candidate plaintexts depend only on the index, so they are encoded
 once and stay resident in HBM (poly_gmem), as do the masks.
@@ -58,6 +62,7 @@ class QueryShape:
     top_k: int
     scale: float
     compaction: str = "reference"
+    eval_level: int | None = None   # limbs the server evaluates at (None: the query's level)
 
     @property
     def B(self) -> int:
@@ -93,10 +98,14 @@ class QueryRecord:
     nprobe: int = 0         # lists the client selects (0: the shape's nprobe)
 
 
-def batch_offsets(counts, slots: int) -> list[int]:
+def batch_offsets(counts, slots: int, align: int | None = None) -> list[int]:
     """Slot offsets of consecutive candidate batches across the result
     ciphertexts: back to back, except that a batch that would cross a
-    result's end starts the next result (offset a multiple of `slots`)."""
+    result's end starts the next result (offset a multiple of `slots`).
+    With `align` (a divisor of `slots`, at least every count), batch t starts
+    at t * align instead."""
+    if align:
+        return [t * align for t in range(len(counts))]
     out, off = [], 0
     for cnt in counts:
         if off % slots + cnt > slots:
@@ -160,8 +169,11 @@ class InteractiveQueryManager:
             k, j = divmod(c, shape.per_ct)
             vals[k, j * D:(j + 1) * D] = index.centroids[c]
         encode_plaintexts(ctx, self.enc, vals, shape.scale, self.pt_centroid_cts, L)
-        self.levels = sorted(set(levels or [L]) | {L})
+        assert shape.eval_level is None or 3 <= shape.eval_level <= L, "eval_level must be in [3, L]"
+        self.levels = sorted({self.eval_at(lv) for lv in set(levels or [L]) | {L}})
         assert all(3 <= lv <= L for lv in self.levels), "query levels must be in [3, L]"
+        for lv in self.levels:
+            assert bound * self.out_scale_at(lv) * 4 < self.p.q[0] / 2, "results would not decrypt from limb 0"
         self._onehot: dict[int, list[int]] = {}      # level -> one-hot masks (reference compaction)
         self._stride: dict[int, int] = {}             # level -> centroid-slot mask (packed compaction)
         self._prefix_lv: dict[tuple[int, int], int] = {}
@@ -177,9 +189,10 @@ class InteractiveQueryManager:
                 m[0, np.arange(shape.per_ct) * D] = 1.0
                 self._stride[lv] = slots.take(1)[0]
                 encode_plaintexts(ctx, self.enc, m, ms, [self._stride[lv]], lv - 1)
-        self.mask_onehot = self._onehot.get(L, [])
+        top = self.levels[-1]                  # the level top-level queries are evaluated at
+        self.mask_onehot = self._onehot.get(top, [])
         if shape.compaction == "packed":
-            self.mask_stride = self._stride[L]
+            self.mask_stride = self._stride[top]
         self.mask_prefix: dict[int, int] = {}
         B = shape.B
         self.batches: list[list[tuple[int, int, list]]] = []
@@ -212,11 +225,10 @@ class InteractiveQueryManager:
             encode_plaintexts(ctx, self.enc, m, float(self.p.q[lv - 2]), offs, lv - 1)
             for cnt, off in zip(cs, offs):
                 self._prefix_lv[(cnt, lv)] = off
-        self.mask_prefix = {cnt: self._prefix_lv[(cnt, L)] for cnt in counts}
+        self.mask_prefix = {cnt: self._prefix_lv[(cnt, top)] for cnt in counts}
         # result ciphertexts per query: enough for the largest lists a query may probe
         self.max_nprobe = max(max_nprobe or shape.nprobe, shape.nprobe)
-        most = sum(sorted((len(v) for v in index.lists), reverse=True)[:self.max_nprobe])
-        self.n_res = self.results_needed(most, S, B)
+        self.n_res = self.results_for(index, shape, self.max_nprobe)
         # ---- per-lane working ciphertexts ----
         self.work = []
         for _ in range(self.lanes):
@@ -245,13 +257,31 @@ class InteractiveQueryManager:
         return max(1, -(-candidates // (slots - B + 1)))
 
     @staticmethod
+    def results_for(index: IvfPqIndex, shape: QueryShape, nprobe: int) -> int:
+        """Result ciphertexts a query probing `nprobe` lists may need."""
+        B, S = shape.B, shape.slots
+        if shape.compaction == "packed":        # aligned batches: S / B per result
+            most = sum(sorted((-(-len(v) // B) for v in index.lists), reverse=True)[:nprobe])
+            return max(1, -(-most // (S // B)))
+        most = sum(sorted((len(v) for v in index.lists), reverse=True)[:nprobe])
+        return InteractiveQueryManager.results_needed(most, S, B)
+
+    @staticmethod
     def mask_slots(shape: QueryShape, levels: int, n_list_masks: bool) -> int:
         """Slots the per-level masks take: one-hot masks (reference compaction)
         or one stride mask, plus up to B prefix masks, per level."""
         return levels * ((shape.n_list if n_list_masks else 1) + shape.B)
 
+    def eval_at(self, level: int) -> int:
+        """Limbs the chain runs at for a query encrypted at `level`. The chain
+        has multiplicative depth 2 (square, mask). A ciphertext's first l
+        limbs are that ciphertext mod Q_l: same message, same scale. So with
+        `eval_level` the server drops every limb it does not need before the
+        first operator, and every key switch runs on eval_level limbs."""
+        return min(level, self.sh.eval_level or level)
+
     def level_of(self, rec: QueryRecord) -> int:
-        return rec.level or self.L
+        return self.eval_at(rec.level or self.L)
 
     def out_scale_at(self, lv: int) -> float:
         """Scale of the results of a query encrypted at level lv."""
@@ -277,25 +307,29 @@ class InteractiveQueryManager:
             groups.setdefault(level_of(r), []).append(i)
         return sorted(groups.items(), reverse=True)
 
-    def rotation_steps(self, max_candidates: int | None = None) -> set[int]:
-        D, B = self.sh.D, self.sh.B
+    def rotation_steps(self) -> set[int]:
+        return self.steps_for(self.sh)
+
+    @staticmethod
+    def steps_for(sh: QueryShape) -> set[int]:
+        """Rotation keys the chain needs."""
+        D, B = sh.D, sh.B
         steps = set()
         s = 1
         while s < D:
             steps.add(s)            # coarse tree sum
             steps.add(B * s)        # fine tree sum
             s <<= 1
-        if self.sh.compaction == "reference":
-            for i in range(self.sh.n_list):
+        if sh.compaction == "reference":
+            for i in range(sh.n_list):
                 steps.update(pow2_steps(i * (D - 1)))
+            s = 1
+            while s < sh.slots:
+                steps.add(-s)       # batch position shifts, power-of-two steps
+                s <<= 1
         else:
-            for k in range(1, self.sh.n_coarse):
-                steps.update(-x for x in pow2_steps(k))
-        top = max_candidates or self.sh.slots
-        s = 1
-        while s < top:
-            steps.add(-s)           # batch position shifts
-            s <<= 1
+            steps.update(-k for k in range(1, sh.n_coarse))          # coarse packing, one step each
+            steps.update(-B * m for m in range(1, sh.slots // B))    # batch placement, one step each
         return steps
 
     def new_query(self) -> QueryRecord:
@@ -397,6 +431,17 @@ class InteractiveQueryManager:
         L.check(self.lib.afhe_eval_sub_plain_batch(self.ctx.h, self._refs(a), self._offs(pts), self._refs(d), len(a),
                                                    limbs), "eval_sub_plain_batch")
 
+    def _rotate_direct(self, items, limbs: int) -> None:
+        """Rotate each ciphertext of `items` ((ct, step) pairs) in place by
+        its step in one key switch (every step has its own key)."""
+        items = [(ct, s) for ct, s in items if s]
+        if not items:
+            return
+        steps = (L.i32 * len(items))(*[s for _, s in items])
+        refs = self._refs([ct for ct, _ in items])
+        L.check(self.lib.afhe_eval_rotate_steps_batch(self.ctx.h, refs, refs, steps, len(items), limbs),
+                "eval_rotate_steps_batch")
+
     def _rotate_grouped(self, items, limbs: int) -> None:
         """Rotate each ciphertext of `items` ((ct, shift) pairs) in place by its
         shift, as eval_rotate does it: |shift| in descending powers of two,
@@ -477,7 +522,7 @@ class InteractiveQueryManager:
                 self._rot_acc(sq, sq, s, Ll - 1)
                 s <<= 1
             self._mult_plain(sq, [self._stride[Ll]] * len(it), sel, Ll - 1)
-            self._rotate_grouped([(sel[j], -k) for j, (_, k) in enumerate(it)], Ll - 2)
+            self._rotate_direct([(sel[j], -k) for j, (_, k) in enumerate(it)], Ll - 2)
             self._accumulate([(queries[qi].compact, k == 0, sel[j]) for j, (qi, k) in enumerate(it)], Ll - 2)
 
     def _compact(self, qs: list[QueryRecord], sq, Ll: int) -> None:
@@ -534,7 +579,8 @@ class InteractiveQueryManager:
             q.vids, q.pos = [], []
             lst = items.setdefault(self.level_of(q), [])
             bs = [b for c in q.probes for b in self.batches[c]]
-            for (pt, cnt, vids), off in zip(bs, batch_offsets([b[1] for b in bs], S)):
+            align = self.sh.B if self.sh.compaction == "packed" else None
+            for (pt, cnt, vids), off in zip(bs, batch_offsets([b[1] for b in bs], S, align)):
                 lst.append((qi, pt, cnt, off))
                 q.vids.extend(vids)
                 q.pos.extend(range(off, off + cnt))
@@ -559,8 +605,13 @@ class InteractiveQueryManager:
                 s <<= 1
             self._mult_plain(sq, [self._prefix(x[2], Ll) for x in it], sel, Ll - 1)
             # rotate each item by -(offset mod slots): eval_rotate's steps,
-            # grouped across items step by step
-            self._rotate_grouped([(sel[k], -(x[3] % S)) for k, x in enumerate(it)], Ll - 2)
+            # grouped across items step by step (reference chain), or one key
+            # switch per item (packed chain)
+            place = [(sel[k], -(x[3] % S)) for k, x in enumerate(it)]
+            if self.sh.compaction == "packed":
+                self._rotate_direct(place, Ll - 2)
+            else:
+                self._rotate_grouped(place, Ll - 2)
             # accumulate into result offset // slots; the item at slot 0 starts it
             self._accumulate([(queries[x[0]].results[x[3] // S], x[3] % S == 0, sel[k]) for k, x in enumerate(it)],
                              Ll - 2)

@@ -48,6 +48,7 @@ class WorkloadSpec:
     train_sample: int | None = None
     pq_sample: int | None = None
     init: str = "random"
+    eval_level: int | None = None     # limbs the server evaluates at (None: the query's level)
 
 
 SMALL = WorkloadSpec("ivfpq_4096x64_nlist32_N8192_L3", n_vectors=4096, d=64, components=32, sigma=0.1, n_list=32,
@@ -60,10 +61,12 @@ SMALL = WorkloadSpec("ivfpq_4096x64_nlist32_N8192_L3", n_vectors=4096, d=64, com
 # The centroids span 8 ciphertexts, so the coarse distances use the packed
 # compaction. The index trains on seeded samples (131,072 vectors for IVF,
 # 32,768 for PQ) with farthest-point seeding, then assigns every vector.
+# Queries arrive at 12 limbs; the depth-2 chain is evaluated on their first 3
+# (eval_level), so every key switch runs on 3 + 4 limbs.
 LARGE = WorkloadSpec("ivfpq_1Mx128_nlist1024_N32768_L12", n_vectors=1_000_000, d=128, components=1024, sigma=0.15,
                      n_list=1024, M=16, K=256, nprobe=16, top_k=8, log_n=15, num_q=12, q_bits=50, num_p=4,
                      p_bits=60, alpha=4, log_scale=40, compaction="packed", kmeans_iters=8, train_sample=131072,
-                     pq_sample=32768, init="farthest")
+                     pq_sample=32768, init="farthest", eval_level=3)
 
 
 def query_layout(q: np.ndarray, sh: QueryShape) -> np.ndarray:
@@ -96,13 +99,13 @@ class Workload:
         n = self.params.n
         slots = n // 2
         shape = QueryShape(D=spec.d, n_list=spec.n_list, slots=slots, nprobe=spec.nprobe, top_k=spec.top_k,
-                           scale=float(2 ** spec.log_scale), compaction=spec.compaction)
+                           scale=float(2 ** spec.log_scale), compaction=spec.compaction, eval_level=spec.eval_level)
         slot_w = (self.params.L + self.params.K) * n
         B = slots // spec.d
         n_batches = sum(-(-len(v) // B) for v in self.index.lists)
         most_probes = max(max_nprobe or spec.nprobe, spec.nprobe)
-        n_res = InteractiveQueryManager.results_needed(
-            sum(sorted((len(v) for v in self.index.lists), reverse=True)[:most_probes]), slots, B)
+        n_res = InteractiveQueryManager.results_for(self.index, shape, most_probes)
+        n_keys = 1 + len(InteractiveQueryManager.steps_for(shape))
         lvls = sorted(set(levels or []) | {self.params.L})
         w_out = (self.params.L - 2) * n
         most = max(max_queries, lanes) * max(n_res, 1)
@@ -115,7 +118,7 @@ class Workload:
                                                               self.params.L, n, slot_w, lanes)
                    + dec_slots)
         self.ctx = FheContext(self.params, poly_words=n_slots * slot_w,
-                              key_words=(2 + 2 * (spec.log_n + 1)) * self.params.key_words() + 4096, device=device,
+                              key_words=n_keys * self.params.key_words() + 4096, device=device,
                               max_batch=lanes)
         self.slots = Slots(self.params, 0, n_slots * slot_w)
         self.client = CkksClient(self.ctx, self.slots, seed=spec.seed + 7)

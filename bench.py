@@ -70,6 +70,9 @@ def run_ours(args, rank: int, world: int):
     dev = int(os.environ.get("LOCAL_RANK", 0))
     torch.cuda.set_device(dev)
     spec = LARGE if args.workload == "large" else SMALL
+    if args.full_level:
+        import dataclasses
+        spec = dataclasses.replace(spec, eval_level=None)
     if args.batch <= 0:
         # small: the one-kernel key switch runs one CTA per ciphertext and one
         # CTA per SM at a time, so two full waves per launch; large: 256
@@ -175,6 +178,7 @@ def run_ours(args, rank: int, world: int):
         "dtype": "u64",
         "data": "synthetic (seeded Gaussian mixture database, seeded keys)",
         "config": {"workload": wl.spec.name, "queries_per_step": args.batch, "lanes": args.lanes,
+                   "eval_level": wl.spec.eval_level or wl.params.L,
                    "nprobe": wl.spec.nprobe, "n_list": wl.spec.n_list, "ring_degree": n,
                    "q_limbs": wl.params.L, "p_limbs": wl.params.K,
                    "l2": f"no flush; inputs larger than L2: {args.batch * 2 * Lw * 8 / 1e6:.0f} MB of query "
@@ -516,6 +520,8 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=5.0, help="served trace length")
     ap.add_argument("--serve-sweep", default="", help="serving driver: comma-separated offered rates (queries/s)")
     ap.add_argument("--mixed", action="store_true", help="serving driver: mixed query levels 6-12 and nprobe")
+    ap.add_argument("--full-level", action="store_true",
+                    help="evaluate at the queries' own level instead of the workload's eval_level")
     ap.add_argument("--ntt-config", action="store_true", help="NTT microbenchmark driver (64 ct x 2 x 24 limbs, N=2^16)")
     ap.add_argument("--ks-config", action="store_true", help="batched key-switch driver (32 ct, N=2^16, dnum 3)")
     ap.add_argument("--profile-step", type=int, default=0, help="profiling driver: queries per step")

@@ -273,6 +273,13 @@ int afhe_eval_rotate_accumulate_batch(afhe_ctx* ctx, const afhe_ct_ref* in, cons
                                       uint32_t count, int32_t total_rot, uint32_t limbs);
 int afhe_eval_add_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const afhe_ct_ref* b, const afhe_ct_ref* dst,
                         uint32_t count, uint32_t limbs);
+/* dst[i] = eval_rotate_single_step(in[i], steps[i]) (fhe_host_driver.cpp:
+ * 331-359): every ciphertext rotated by its own step, with that step's
+ * registered key, in one launch sequence. Each step is applied as a single
+ * key switch, however many bits it has (eval_rotate would split it into
+ * powers of two). dst[i] may alias in[i]. */
+int afhe_eval_rotate_steps_batch(afhe_ctx* ctx, const afhe_ct_ref* in, const afhe_ct_ref* dst,
+                                 const int32_t* steps, uint32_t count, uint32_t limbs);
 /* dst[i] = a[i] (both polynomials, `limbs` limbs): the slot-to-slot copies the
  * reference's host makes between operators (eval_sub_plain's c1 copy,
  * fhe_host_driver.cpp:259-270), for many ciphertexts in one launch. */

@@ -9,10 +9,11 @@ eval_rotate by i (D - 1) and eval_add into a running sum; for each candidate
 batch, the same with -offset.
 
 For indexes whose centroids span several ciphertexts the chain compacts
-them the "packed" way (mask every centroid slot, rotate coarse ciphertext k
-right by k, sum), and candidates past the slot count continue in a second
-result ciphertext. That chain is replayed the same way, one ciphertext at a
-time, on the oracle.
+them the "packed" way: mask every centroid slot, rotate coarse ciphertext k
+right by k with one key, and sum. It places candidate batch t at slot t * B
+with one key switch, continuing in a second result ciphertext past the slot
+count. That chain is replayed the same way, one ciphertext at a time, on the
+oracle.
 
 This test replays that sequential chain on the CPU oracle (the C restatement
 of the reference's HLS kernels) with the very keys, plaintexts and
@@ -75,23 +76,28 @@ def reference_chain(wl, ora, ct, ct_dim, probes, level=None):
             sq = tree(ora.eval_mult_relin_rescale(diff, diff, relin, L), 1)
             sel = ora.eval_mult_plain_rescale(sq, pt(iqm._stride[L], L - 1), L - 1)
             if k:
-                sel = ora.eval_rotate(sel, -k, rot, L - 2)
+                sel = ora.eval_rotate_single_step(sel, -k, rot, L - 2)     # one key for step -k
             comp = sel if comp is None else ora.eval_add(comp, sel, L - 2)
     # stage 3: candidate p lands in result p // slots at slot p mod slots
     S = iqm.sh.slots
-    off, acc = 0, {}
+    packed = iqm.sh.compaction == "packed"
+    off, acc, t = 0, {}, 0
     for c in probes:
         for pt_off, cnt, _ in iqm.batches[c]:
-            if off % S + cnt > S:       # a batch that does not fit starts the next result
+            if packed:                  # batch t starts at t * B, placed by one key
+                off = t * B
+            elif off % S + cnt > S:     # a batch that does not fit starts the next result
                 off = (off // S + 1) * S
             diff = ora.eval_sub_plain(ct_dim, pt(pt_off, L), L)
             sq = tree(ora.eval_mult_relin_rescale(diff, diff, relin, L), B)
             sel = ora.eval_mult_plain_rescale(sq, pt(iqm._prefix_lv[(cnt, L)], L - 1), L - 1)
             if off % S:
-                sel = ora.eval_rotate(sel, -(off % S), rot, L - 2)
+                sel = (ora.eval_rotate_single_step(sel, -(off % S), rot, L - 2) if packed
+                       else ora.eval_rotate(sel, -(off % S), rot, L - 2))
             r = off // S
             acc[r] = sel if r not in acc else ora.eval_add(acc[r], sel, L - 2)
             off += cnt
+            t += 1
     return comp, [acc[r] for r in sorted(acc)]
 
 
@@ -112,12 +118,13 @@ def run_and_compare(spec, nq, lanes, orc, levels=None):
         ora = OracleCKKS(p.log_n, p.q, p.p, p.alpha, orc)
         results_used = set()
         for r, (ct, ct_dim) in zip(recs, ins):
-            comp, accs = reference_chain(wl, ora, ct, ct_dim, r.probes, r.level)
-            got_c = [a[:(r.level - 2) * n] for a in wl.iqm.read_ct(r.compact)]
+            lv = wl.iqm.level_of(r)          # the level the server evaluates this query at
+            comp, accs = reference_chain(wl, ora, ct, ct_dim, r.probes, lv)
+            got_c = [a[:(lv - 2) * n] for a in wl.iqm.read_ct(r.compact)]
             assert np.array_equal(got_c[0], comp[0]) and np.array_equal(got_c[1], comp[1]), "stage 1b differs"
             results_used.add(len(accs))
             for k, acc in enumerate(accs):
-                got_d = [a[:(r.level - 2) * n] for a in wl.iqm.read_ct(r.results[k])]
+                got_d = [a[:(lv - 2) * n] for a in wl.iqm.read_ct(r.results[k])]
                 assert np.array_equal(got_d[0], acc[0]) and np.array_equal(got_d[1], acc[1]), \
                     f"stage 3 result {k} differs"
         return wl.iqm, results_used
@@ -148,6 +155,16 @@ def test_mixed_levels_match_oracle_replay(orc):
     at its own level (masks per level) and equals the oracle replay there."""
     iqm, _ = run_and_compare(TINY_PACKED, nq=3, lanes=16, orc=orc, levels=[4, 3, 3])
     assert iqm.levels == [3, 4]
+
+
+def test_eval_level_matches_oracle_replay(orc):
+    """Queries encrypted at 5 and 4 limbs, evaluated at 3: the server drops
+    the limbs the depth-2 chain does not need before its first operator; the
+    chain at 3 limbs equals the oracle replay on the queries' first 3 limbs."""
+    import dataclasses
+    spec = dataclasses.replace(TINY_PACKED, name="ivfpq_2048x8_nlist128_N1024_L5_eval3", num_q=5, eval_level=3)
+    iqm, _ = run_and_compare(spec, nq=2, lanes=16, orc=orc, levels=[5, 4])
+    assert iqm.levels == [3]
 
 
 def test_chain_matches_reference_bench_configuration(orc):
