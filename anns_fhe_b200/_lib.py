@@ -31,6 +31,7 @@ class Params(C.Structure):
         ("log_n", u32), ("num_q", u32), ("num_p", u32), ("alpha", u32),
         ("q", u64 * MAX_Q), ("p", u64 * MAX_P),
         ("poly_words", u64), ("key_words", u64), ("device", i32), ("max_batch", u32),
+        ("psi_q", u64 * MAX_Q), ("psi_p", u64 * MAX_P),
     ]
 
 

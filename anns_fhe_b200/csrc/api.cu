@@ -30,6 +30,14 @@ int cuda_fail(afhe_ctx* ctx, cudaError_t e, const char* where) {
 
 u64 host_shoup(u64 w, u64 q) { return (u64)(((unsigned __int128)w << 64) / q); }
 
+// The primitive 2N-th root behind prime i's twiddles (Q primes first, then
+// P): the one the parameters name, else the smallest.
+u64 root_of(const afhe_ctx* ctx, uint32_t i) {
+    const u64 psi = i < ctx->L ? ctx->prm.psi_q[i] : ctx->prm.psi_p[i - ctx->L];
+    const u64 q = i < ctx->L ? ctx->prm.q[i] : ctx->prm.p[i - ctx->L];
+    return psi ? psi : min_primitive_root(ctx->log_n, q);
+}
+
 int zf_from(afhe_ctx* ctx, const u64* vals, uint32_t n, ZField* out) {
     if (n == 0) { *out = zf_const(0); return AFHE_OK; }
     const u64 stride = n > 1 ? vals[1] - vals[0] : 0;
@@ -177,7 +185,7 @@ int build_native_tables(afhe_ctx* ctx) {
     std::vector<PrimeConst> pc(np);
     for (uint32_t i = 0; i < np; ++i) {
         u64 q = primes[i];
-        u64 psi = min_primitive_root(ctx->log_n, q);
+        u64 psi = root_of(ctx, i);
         gen_twiddles(ctx->log_n, q, psi, tw.data(), itw.data());
         for (uint32_t j = 0; j < n; ++j) {
             tw2[(size_t)i * n + j] = make_ulonglong2(tw[j], host_shoup(tw[j], q));
@@ -342,6 +350,9 @@ int afhe_ctx_create(const afhe_params* prm, afhe_ctx** out) {
             return fail(nullptr, AFHE_E_ARG, "every prime must be < 2^61, prime and == 1 mod 2N");
         for (size_t j = 0; j < i; ++j)
             if (all[j] == q) return fail(nullptr, AFHE_E_ARG, "primes must be distinct");
+        const u64 psi = i < prm->num_q ? prm->psi_q[i] : prm->psi_p[i - prm->num_q];
+        if (psi != 0 && (psi >= q || pow_mod(psi, 1ull << prm->log_n, q) != q - 1))
+            return fail(nullptr, AFHE_E_ARG, "psi must be a primitive 2N-th root of unity mod its prime");
     }
     afhe_ctx* ctx = new afhe_ctx();
     ctx->prm = *prm;
@@ -490,7 +501,7 @@ int afhe_ctx_write_context_tables(afhe_ctx* ctx, uint32_t level, afhe_context_la
     std::vector<u64> tw((size_t)(L + K) * n), itw((size_t)(L + K) * n);
     for (uint32_t i = 0; i < L + K; ++i) {
         u64 qq = i < L ? q[i] : p[i - L];
-        gen_twiddles(ctx->log_n, qq, min_primitive_root(ctx->log_n, qq), &tw[(size_t)i * n], &itw[(size_t)i * n]);
+        gen_twiddles(ctx->log_n, qq, root_of(ctx, i), &tw[(size_t)i * n], &itw[(size_t)i * n]);
     }
     // fhe_host_driver.cpp:63-86: twiddles (Q then P), inverse twiddles, CRT slots
     lay.twiddles_q_offset = cur;

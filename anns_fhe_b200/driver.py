@@ -113,6 +113,7 @@ class CkksParams:
     q: list[int]
     p: list[int]
     alpha: int
+    psi: tuple = ()     # primitive 2N-th roots behind the twiddles, Q then P (empty: the smallest)
 
     @property
     def n(self) -> int:
@@ -163,6 +164,11 @@ class FheContext:
             pr.q[i] = x
         for i, x in enumerate(params.p):
             pr.p[i] = x
+        for i, x in enumerate(params.psi):
+            if i < params.L:
+                pr.psi_q[i] = x
+            else:
+                pr.psi_p[i - params.L] = x
         pr.poly_words, pr.key_words, pr.device = poly_words, key_words, device
         pr.max_batch = max_batch
         self.max_batch = max_batch or 64

@@ -68,6 +68,11 @@ typedef struct afhe_params {
     int32_t device;            /* CUDA device ordinal */
     uint32_t max_batch;        /* ciphertexts per batched launch (context scratch lanes);
                                   0 selects 64 */
+    /* Primitive 2N-th root per prime behind the twiddles (tw[j] = psi^bitrev(j));
+     * 0 selects the smallest root. A package's own roots (its tw[N/2]) make
+     * every NTT match the package's evaluation-form data. */
+    uint64_t psi_q[AFHE_MAX_Q];
+    uint64_t psi_p[AFHE_MAX_P];
 } afhe_params;
 
 /* Scalar and array registers of fhe_accel_top (fhe_accel_top.h:8-55), with
