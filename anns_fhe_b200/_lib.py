@@ -100,6 +100,8 @@ SIGNATURES = {
     "afhe_read_poly_async": (C.c_int, [CTX, u64, P64, u64]),
     "afhe_copy_poly": (C.c_int, [CTX, u64, u64, u64]),
     "afhe_read_poly_rows": (C.c_int, [CTX, u64, u64, u64, u64, P64]),
+    "afhe_host_alloc": (C.c_int, [u64, C.POINTER(C.c_void_p)]),
+    "afhe_host_free": (C.c_int, [C.c_void_p]),
     "afhe_ctx_write_context_tables": (C.c_int, [CTX, u32, C.POINTER(ContextLayout)]),
     "afhe_dispatch": (C.c_int, [CTX, C.POINTER(AccelArgs)]),
     "afhe_set_relin_key": (C.c_int, [CTX, u64]),

@@ -292,7 +292,8 @@ class CkksClient:
         for i, (a, b) in enumerate(cts):
             arr[i].c0_offset, arr[i].c1_offset = a, b
         L.check(self.ctx.lib.afhe_decrypt_batch(self.ctx.h, arr, count, self.s_slot, out, level), "decrypt_batch")
-        limbs = self.ctx.read_poly(out, count * level * n).reshape(count, level * n)
+        limbs = self.ctx.read_poly(out, count * level * n,
+                                   self.ctx.staging.get("dec_coef", count * level * n)).reshape(count, level * n)
         if level == 1 and self.p.q[0] < 2**53:
             # residues below 2^53 convert to float64 exactly; centre in place
             q = float(self.p.q[0])

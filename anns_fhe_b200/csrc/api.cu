@@ -475,9 +475,28 @@ int afhe_read_poly_rows(afhe_ctx* ctx, uint64_t off, uint64_t stride, uint64_t r
     if (rows > 1 && stride > (~0ull - row_words) / (rows - 1)) return fail(ctx, AFHE_E_RANGE, "rows out of range");
     const u64 span = (rows - 1) * stride + row_words;
     if (!range_ok(off, span, ctx->prm.poly_words)) return fail(ctx, AFHE_E_RANGE, "rows out of poly_gmem");
-    CK(cudaMemcpy2DAsync(dst, row_words * 8, ctx->poly + off, stride * 8, row_words * 8, rows,
-                         cudaMemcpyDeviceToHost, ctx->st));
+    if (stride == row_words)   // contiguous rows: one plain copy
+        CK(cudaMemcpyAsync(dst, ctx->poly + off, span * 8, cudaMemcpyDeviceToHost, ctx->st));
+    else
+        CK(cudaMemcpy2DAsync(dst, row_words * 8, ctx->poly + off, stride * 8, row_words * 8, rows,
+                             cudaMemcpyDeviceToHost, ctx->st));
     CK(cudaStreamSynchronize(ctx->st));
+    return AFHE_OK;
+}
+
+int afhe_host_alloc(uint64_t bytes, void** out) {
+    if (!out) return fail(nullptr, AFHE_E_ARG, "null argument");
+    *out = nullptr;
+    if (bytes == 0) return AFHE_OK;
+    cudaError_t e = cudaHostAlloc(out, bytes, cudaHostAllocDefault);
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaHostAlloc");
+    return AFHE_OK;
+}
+
+int afhe_host_free(void* p) {
+    if (!p) return AFHE_OK;
+    cudaError_t e = cudaFreeHost(p);
+    if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaFreeHost");
     return AFHE_OK;
 }
 

@@ -152,6 +152,40 @@ class CkksParams:
         return 2 * self.dnum * (self.L + self.K) * self.n
 
 
+class PinnedStaging:
+    """Reusable page-locked host buffers by name (afhe_host_alloc), grown on
+    demand; `get` returns a uint64 view valid until the next `get` of the
+    same name."""
+
+    def __init__(self):
+        self.lib = L.load()
+        self.bufs: dict[str, tuple[int, int]] = {}
+
+    def get(self, name: str, words: int) -> np.ndarray:
+        ptr, cap = self.bufs.get(name, (0, 0))
+        if cap < words:
+            if ptr:
+                self.lib.afhe_host_free(C.c_void_p(ptr))
+            cap = max(words, 2 * cap)
+            p = C.c_void_p()
+            check(self.lib.afhe_host_alloc(cap * 8, C.byref(p)), "afhe_host_alloc")
+            ptr = p.value
+            self.bufs[name] = (ptr, cap)
+        return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(C.c_uint64)), shape=(cap,))[:words]
+
+    def close(self) -> None:
+        for ptr, _ in self.bufs.values():
+            if ptr:
+                self.lib.afhe_host_free(C.c_void_p(ptr))
+        self.bufs = {}
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class FheContext:
     """Device context: arenas, tables, key directory (one CUDA stream)."""
 
@@ -182,6 +216,9 @@ class FheContext:
         if getattr(self, "h", None):
             self.lib.afhe_ctx_destroy(self.h)
             self.h = None
+        if getattr(self, "_staging", None) is not None:
+            self._staging.close()
+            self._staging = None
 
     def __del__(self):
         try:
@@ -200,10 +237,17 @@ class FheContext:
         a = _u64(data).ravel()
         check(self.lib.afhe_write_poly(self.h, off, _p64(a), a.size), "write_poly")
 
-    def read_poly(self, off: int, count: int) -> np.ndarray:
-        a = np.empty(count, dtype=np.uint64)
+    def read_poly(self, off: int, count: int, out: np.ndarray | None = None) -> np.ndarray:
+        """`count` words at `off`; into `out` (e.g. a pinned staging view) if given."""
+        a = np.empty(count, dtype=np.uint64) if out is None else out[:count]
         check(self.lib.afhe_read_poly(self.h, off, _p64(a), count), "read_poly")
         return a
+
+    @property
+    def staging(self) -> "PinnedStaging":
+        if getattr(self, "_staging", None) is None:
+            self._staging = PinnedStaging()
+        return self._staging
 
     def write_key(self, off: int, data) -> None:
         a = _u64(data).ravel()

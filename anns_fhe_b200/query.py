@@ -358,14 +358,24 @@ class InteractiveQueryManager:
         first = rec.compact if kind == "compact" else rec.results[0]
         return (first[0] - base) // (2 * per * self.lvl_out * self.p.n)
 
-    def read_results(self, kind: str, recs) -> np.ndarray:
+    def read_results(self, kind: str, recs, staged: bool = False) -> np.ndarray:
         """Limb 0 of both polynomials of the records' result ciphertexts:
-        (len(recs), per_record, 2, N); one strided copy per contiguous run of
-        records. Limb 0 is what the client decrypts (see __init__)."""
+        (len(recs), per_record, 2, N); one copy per contiguous run of records.
+        Limb 0 is what the client decrypts (see __init__). With `staged`, the
+        array is a view of the context's page-locked staging, valid until the
+        next staged read of the same kind."""
         base, per = self._outbox[kind]
         n, w = self.p.n, self.lvl_out * self.p.n
         idx = [self.record_index(kind, r) for r in recs]
-        out = np.empty((len(recs), per, 2, n), dtype=np.uint64)
+        size = len(recs) * per * 2 * n
+        if staged:
+            out = self.ctx.staging.get("res_" + kind, size).reshape(len(recs), per, 2, n)
+        else:
+            out = np.empty((len(recs), per, 2, n), dtype=np.uint64)
+        if idx and idx == list(range(idx[0], idx[0] + len(idx))):     # one run, in order: read in place
+            L.check(self.lib.afhe_read_poly_rows(self.ctx.h, base + idx[0] * per * 2 * w, w, len(idx) * per * 2, n,
+                                                 out.ctypes.data_as(L.P64)), "read_poly_rows")
+            return out
         order = np.argsort(idx, kind="stable")
         i = 0
         while i < len(order):
@@ -580,11 +590,13 @@ class InteractiveQueryManager:
             lst = items.setdefault(self.level_of(q), [])
             bs = [b for c in q.probes for b in self.batches[c]]
             align = self.sh.B if self.sh.compaction == "packed" else None
-            for (pt, cnt, vids), off in zip(bs, batch_offsets([b[1] for b in bs], S, align)):
+            offs = batch_offsets([b[1] for b in bs], S, align)
+            for (pt, cnt, vids), off in zip(bs, offs):
                 lst.append((qi, pt, cnt, off))
                 q.vids.extend(vids)
-                q.pos.extend(range(off, off + cnt))
-            if q.pos and q.pos[-1] >= self.n_res * S:
+            q.pos = (np.concatenate([np.arange(off, off + b[1]) for b, off in zip(bs, offs)]) if bs
+                     else np.zeros(0, dtype=np.int64))
+            if len(q.pos) and q.pos[-1] >= self.n_res * S:
                 raise ValueError("more candidates than the result ciphertexts hold")
         for lv in sorted(items, reverse=True):
             self._stage3_items(queries, items[lv], lv)

@@ -175,8 +175,10 @@ class WorkloadBackend:
 
     def fetch(self, kind: str, recs) -> np.ndarray:
         """Limb 0 of the records' result ciphertexts, copied to the host:
-        (len(recs), per_record, 2, N)."""
-        return self.iqm.read_results(kind, recs)
+        (len(recs), per_record, 2, N), in page-locked staging. The loop
+        decodes (and copies what it keeps of) a tick's results before the
+        next tick reads the same kind again."""
+        return self.iqm.read_results(kind, recs, staged=True)
 
     def receive(self, kind: str, recs) -> dict:
         """Results of `recs` to the client: limb 0 of the result ciphertexts
@@ -186,7 +188,7 @@ class WorkloadBackend:
         box = self.fetch(kind, recs)
         if kind == "dists":
             # only the result ciphertexts that hold candidates
-            need = max(1, -(-max((max(r.pos) + 1 if r.pos else 1) for r in recs) // self.iqm.sh.slots))
+            need = max(1, -(-max((int(r.pos[-1]) + 1 if len(r.pos) else 1) for r in recs) // self.iqm.sh.slots))
             box = box[:, :need]
         else:
             box = box[:, :1]

@@ -166,7 +166,7 @@ class Workload:
     def candidates(self, recs) -> list[np.ndarray]:
         """Each query's decrypted candidate distances, in stage-3 order."""
         S = self.iqm.sh.slots
-        need = [max(1, -(-(max(r.pos) + 1) // S)) if r.pos else 1 for r in recs]
+        need = [max(1, -(-(int(r.pos[-1]) + 1) // S)) if len(r.pos) else 1 for r in recs]
         scales = [self.iqm.out_scale_at(self.iqm.level_of(r)) for r, k in zip(recs, need) for _ in range(k)]
         vals = self.decrypt_many([ct for r, k in zip(recs, need) for ct in r.results[:k]], scales)
         out, i = [], 0

@@ -122,7 +122,7 @@ def run_ours(args, rank: int, world: int):
                 h2d += t.numel() * 8
         iqm.stage1_coarse(recs)
         # client receives limb 0 of the compacted coarse distances, decrypts, selects
-        box = iqm.read_results("compact", recs)[:, 0]
+        box = iqm.read_results("compact", recs, staged=True)[:, 0]
         d2h = box.nbytes
         coarse = iqm.coarse_from_slots(
             wl.client.decrypt_host_batch(box, 1, iqm.out_scale, iqm.coarse_slots_needed()).real)
@@ -130,7 +130,7 @@ def run_ours(args, rank: int, world: int):
             r.probes = list(np.argsort(c, kind="stable")[:wl.spec.nprobe])
         iqm.stage3_fine(recs)
         # client receives limb 0 of the candidate distances, decrypts, ranks
-        box = iqm.read_results("dists", recs)
+        box = iqm.read_results("dists", recs, staged=True)
         d2h += box.nbytes
         S = iqm.sh.slots
         dists = wl.client.decrypt_host_batch(box.reshape(-1, 2, n), 1, iqm.out_scale).real.reshape(len(recs), -1)

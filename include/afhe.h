@@ -173,6 +173,12 @@ int afhe_read_key(afhe_ctx* ctx, uint64_t word_offset, uint64_t* dst, uint64_t c
 int afhe_write_poly_async(afhe_ctx* ctx, uint64_t word_offset, const uint64_t* src, uint64_t count);
 int afhe_read_poly_async(afhe_ctx* ctx, uint64_t word_offset, uint64_t* dst, uint64_t count);
 int afhe_copy_poly(afhe_ctx* ctx, uint64_t dst_offset, uint64_t src_offset, uint64_t count);
+/* Page-locked host memory for the transfers above (the reference's host
+ * buffers are std::vectors; pinned ones let copies run at full PCIe speed).
+ * afhe_host_free releases what afhe_host_alloc returned. No counterpart in
+ * the reference. */
+int afhe_host_alloc(uint64_t bytes, void** out);
+int afhe_host_free(void* p);
 /* Gather `rows` rows of `row_words` words, row r at word_offset + r * stride,
  * into dst (rows * row_words words, packed), in one copy; synchronous. Reads
  * one limb of many result ciphertexts, e.g. limb 0 of each, which is all a
