@@ -20,6 +20,7 @@ OK, E_ARG, E_RANGE, E_NOKEY, E_LEVEL, E_BUDGET, E_TIMEOUT, E_CUDA, E_STATE = ran
 
 OP_NTT, OP_INTT, OP_POLY_ADD, OP_POLY_SUB, OP_POLY_MUL_NTT = 1, 2, 3, 4, 5
 OP_AUTOMORPHISM, OP_KEY_SWITCH, OP_RESCALE, OP_LOAD_CONTEXT = 6, 7, 8, 99
+OPT_KS_FUSED, OPT_CHUNK = 1, 2
 
 u32, u64, i32 = C.c_uint32, C.c_uint64, C.c_int32
 P64 = C.POINTER(C.c_uint64)
@@ -101,6 +102,8 @@ SIGNATURES = {
     "afhe_copy_poly": (C.c_int, [CTX, u64, u64, u64]),
     "afhe_read_poly_rows": (C.c_int, [CTX, u64, u64, u64, u64, P64]),
     "afhe_host_alloc": (C.c_int, [u64, C.POINTER(C.c_void_p)]),
+    "afhe_ctx_set_option": (C.c_int, [CTX, u32, C.c_int64]),
+    "afhe_ctx_get_option": (C.c_int, [CTX, u32, C.POINTER(C.c_int64)]),
     "afhe_host_free": (C.c_int, [C.c_void_p]),
     "afhe_ctx_write_context_tables": (C.c_int, [CTX, u32, C.POINTER(ContextLayout)]),
     "afhe_dispatch": (C.c_int, [CTX, C.POINTER(AccelArgs)]),

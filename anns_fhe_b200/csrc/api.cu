@@ -484,6 +484,32 @@ int afhe_read_poly_rows(afhe_ctx* ctx, uint64_t off, uint64_t stride, uint64_t r
     return AFHE_OK;
 }
 
+int afhe_ctx_set_option(afhe_ctx* ctx, uint32_t option, int64_t value) {
+    if (!ctx) return fail(nullptr, AFHE_E_ARG, "null context");
+    switch (option) {
+    case AFHE_OPT_KS_FUSED:
+        if (value && !key_switch_fused_supported(ctx->log_n))
+            return fail(ctx, AFHE_E_ARG, "the one-kernel key switch needs N <= 2^13");
+        ctx->ks_fused = value != 0;
+        return AFHE_OK;
+    case AFHE_OPT_CHUNK:
+        if (value < 0 || value > (int64_t)ctx->lanes) return fail(ctx, AFHE_E_ARG, "chunk must be in [0, lanes]");
+        ctx->chunk = (uint32_t)value;
+        return AFHE_OK;
+    default:
+        return fail(ctx, AFHE_E_ARG, "unknown option");
+    }
+}
+
+int afhe_ctx_get_option(afhe_ctx* ctx, uint32_t option, int64_t* value) {
+    if (!ctx || !value) return fail(ctx, AFHE_E_ARG, "null argument");
+    switch (option) {
+    case AFHE_OPT_KS_FUSED: *value = ctx->ks_fused ? 1 : 0; return AFHE_OK;
+    case AFHE_OPT_CHUNK: *value = ctx->chunk ? ctx->chunk : ctx->lanes; return AFHE_OK;
+    default: return fail(ctx, AFHE_E_ARG, "unknown option");
+    }
+}
+
 int afhe_host_alloc(uint64_t bytes, void** out) {
     if (!out) return fail(nullptr, AFHE_E_ARG, "null argument");
     *out = nullptr;

@@ -274,7 +274,7 @@ int prep_key(afhe_ctx* ctx, u64 evk, ulonglong2** prep) {
 
 template <class F>
 int for_chunks(afhe_ctx* ctx, uint32_t count, F f) {
-    const uint32_t w = ctx->lanes;
+    const uint32_t w = ctx->chunk ? ctx->chunk : ctx->lanes;
     for (uint32_t s = 0; s < count; s += w) {
         uint32_t m = count - s < w ? count - s : w;
         int rc = f(s, m);

@@ -113,6 +113,7 @@ struct afhe_ctx {
     uint32_t lanes = 64;
     afhe::DescRing ring;
     bool ks_fused = true;   // one-kernel key switch where supported (AFHE_KS_FUSED=0 turns it off)
+    uint32_t chunk = 0;     // ciphertexts per launch of a batched call (0: all lanes)
 
     // key directory
     bool has_relin = false;

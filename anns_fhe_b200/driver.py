@@ -258,6 +258,14 @@ class FheContext:
         check(self.lib.afhe_read_key(self.h, off, _p64(a), count), "read_key")
         return a
 
+    def set_option(self, option: int, value: int) -> None:
+        check(self.lib.afhe_ctx_set_option(self.h, option, int(value)), "afhe_ctx_set_option")
+
+    def get_option(self, option: int) -> int:
+        v = C.c_int64()
+        check(self.lib.afhe_ctx_get_option(self.h, option, C.byref(v)), "afhe_ctx_get_option")
+        return int(v.value)
+
     def scratch_bytes(self) -> int:
         """Bytes of context-private device scratch (all lanes)."""
         return int(self.lib.afhe_scratch_words(self.h)) * 8

@@ -401,6 +401,25 @@ class InteractiveQueryManager:
     def coarse_slots_needed(self) -> int:
         return max(self.sh.coarse_slot(c) for c in range(self.sh.n_list)) + 1
 
+    # ---- tuning ----
+    def use_tuning(self, choices: dict | None) -> None:
+        """Per-level key-switch choices from the autotuner ({level: KsChoice});
+        None restores the context's defaults."""
+        self._tuning = choices or {}
+        self._opt_now = None
+
+    def _at(self, level: int) -> None:
+        """Apply the tuned options of the level an operator runs at."""
+        ch = getattr(self, "_tuning", {}).get(level)
+        if ch is None:
+            return
+        want = (int(ch.fused), int(ch.chunk))
+        if want != getattr(self, "_opt_now", None):
+            if self.p.log_n <= 13:
+                self.ctx.set_option(L.OPT_KS_FUSED, want[0])
+            self.ctx.set_option(L.OPT_CHUNK, min(want[1], self.ctx.max_batch))
+            self._opt_now = want
+
     # ---- batched C-ABI helpers ----
     @staticmethod
     def _refs(cts):
@@ -414,10 +433,12 @@ class InteractiveQueryManager:
         return (L.u64 * max(len(v), 1))(*v)
 
     def _rotate(self, cts, r, limbs):
+        self._at(limbs)
         L.check(self.lib.afhe_eval_rotate_batch(self.ctx.h, self._refs(cts), self._refs(cts), len(cts), r, limbs),
                 "eval_rotate_batch")
 
     def _rot_acc(self, src, acc, r, limbs):
+        self._at(limbs)
         L.check(self.lib.afhe_eval_rotate_accumulate_batch(self.ctx.h, self._refs(src), self._refs(acc), len(src), r,
                                                            limbs), "eval_rotate_accumulate_batch")
 
@@ -434,6 +455,7 @@ class InteractiveQueryManager:
                                                             len(a), limbs), "eval_mult_plain_rescale_batch")
 
     def _square(self, a, d, limbs):
+        self._at(limbs)
         L.check(self.lib.afhe_eval_mult_relin_rescale_batch(self.ctx.h, self._refs(a), self._refs(a), self._refs(d),
                                                             len(a), limbs), "eval_mult_relin_rescale_batch")
 
@@ -447,6 +469,7 @@ class InteractiveQueryManager:
         items = [(ct, s) for ct, s in items if s]
         if not items:
             return
+        self._at(limbs)
         steps = (L.i32 * len(items))(*[s for _, s in items])
         refs = self._refs([ct for ct, _ in items])
         L.check(self.lib.afhe_eval_rotate_steps_batch(self.ctx.h, refs, refs, steps, len(items), limbs),

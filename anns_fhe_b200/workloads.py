@@ -86,9 +86,12 @@ def dimpack_layout(q: np.ndarray, sh: QueryShape) -> np.ndarray:
 
 class Workload:
     def __init__(self, spec: WorkloadSpec = SMALL, max_queries: int = 64, lanes: int = 64, device: int = 0,
-                 index: IvfPqIndex | None = None, levels=None, max_nprobe: int | None = None):
+                 index: IvfPqIndex | None = None, levels=None, max_nprobe: int | None = None,
+                 tune: bool = False):
         """levels: query levels to serve besides the top one (mixed-level
-        traffic); max_nprobe: the most lists one query may probe."""
+        traffic); max_nprobe: the most lists one query may probe; tune: apply
+        the autotuner's key-switch choices (cached per GPU and parameter
+        set, measured when absent)."""
         self.spec = spec
         t0 = time.time()
         self.X = gaussian_mixture(spec.n_vectors, spec.d, spec.components, spec.sigma, spec.seed)
@@ -124,6 +127,12 @@ class Workload:
         self.client = CkksClient(self.ctx, self.slots, seed=spec.seed + 7)
         self.iqm = InteractiveQueryManager(self.ctx, self.index, shape, self.slots, lanes=lanes, levels=lvls,
                                            max_nprobe=most_probes)
+        self.tuning = None
+        if tune:
+            from .autotune import load_or_tune
+            lv = sorted({x for ev in self.iqm.levels for x in (ev, ev - 1, ev - 2) if x >= 1})
+            self.tuning = load_or_tune(self.params, lv, lanes, device)
+            self.iqm.use_tuning(self.tuning)
         self.steps = self.iqm.rotation_steps()
         self.client.install_keys(self.steps)
         self.records = self.iqm.alloc_queries(max_queries)

@@ -82,7 +82,7 @@ def run_ours(args, rank: int, world: int):
         args.lanes = args.batch
     # twice the records of a step: the serving leg keeps one tick's queries
     # in flight while admitting the next
-    wl = Workload(spec, max_queries=2 * args.batch, lanes=args.lanes, device=dev)
+    wl = Workload(spec, max_queries=2 * args.batch, lanes=args.lanes, device=dev, tune=not args.no_tune)
     stream = torch.cuda.ExternalStream(wl.ctx.lib.afhe_stream(wl.ctx.h), device=dev)
     iqm = wl.iqm
     recs = wl.records[:args.batch]
@@ -179,6 +179,8 @@ def run_ours(args, rank: int, world: int):
         "data": "synthetic (seeded Gaussian mixture database, seeded keys)",
         "config": {"workload": wl.spec.name, "queries_per_step": args.batch, "lanes": args.lanes,
                    "eval_level": wl.spec.eval_level or wl.params.L,
+                   "tuning": ({str(k): [int(v.fused), v.chunk] for k, v in wl.tuning.items()} if wl.tuning
+                              else None),
                    "nprobe": wl.spec.nprobe, "n_list": wl.spec.n_list, "ring_degree": n,
                    "q_limbs": wl.params.L, "p_limbs": wl.params.K,
                    "l2": f"no flush; inputs larger than L2: {args.batch * 2 * Lw * 8 / 1e6:.0f} MB of query "
@@ -513,6 +515,7 @@ def main():
     ap.add_argument("--lanes", type=int, default=0, help="ciphertexts per launch (default: the batch)")
     ap.add_argument("--skip-cpu", action="store_true", help="omit the cpu_baseline leg")
     ap.add_argument("--skip-serving", action="store_true", help="omit the serving leg")
+    ap.add_argument("--no-tune", action="store_true", help="skip the autotuner's key-switch choices")
     ap.add_argument("--workload", default="small", choices=["small", "large"],
                     help="small: 4,096 x 64, N=2^13 (default); large: 1M x 128, n_list 1024, N=2^15")
     ap.add_argument("--plain-queries", type=int, default=16, help="queries timed on the plain path")

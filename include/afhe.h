@@ -173,6 +173,16 @@ int afhe_read_key(afhe_ctx* ctx, uint64_t word_offset, uint64_t* dst, uint64_t c
 int afhe_write_poly_async(afhe_ctx* ctx, uint64_t word_offset, const uint64_t* src, uint64_t count);
 int afhe_read_poly_async(afhe_ctx* ctx, uint64_t word_offset, uint64_t* dst, uint64_t count);
 int afhe_copy_poly(afhe_ctx* ctx, uint64_t dst_offset, uint64_t src_offset, uint64_t count);
+/* Run-time options of a context (no counterpart in the reference; the
+ * autotuner, anns_fhe_b200/autotune.py, picks them per GPU and parameter set):
+ *   AFHE_OPT_KS_FUSED  1: the one-kernel key switch (N <= 2^13), 0: the
+ *                      multi-kernel pipeline. Same residues either way.
+ *   AFHE_OPT_CHUNK     ciphertexts per launch of a batched call, 1..lanes
+ *                      (0: all lanes). Same residues for any value. */
+#define AFHE_OPT_KS_FUSED 1u
+#define AFHE_OPT_CHUNK 2u
+int afhe_ctx_set_option(afhe_ctx* ctx, uint32_t option, int64_t value);
+int afhe_ctx_get_option(afhe_ctx* ctx, uint32_t option, int64_t* value);
 /* Page-locked host memory for the transfers above (the reference's host
  * buffers are std::vectors; pinned ones let copies run at full PCIe speed).
  * afhe_host_free releases what afhe_host_alloc returned. No counterpart in
