@@ -286,8 +286,8 @@ def query_seed_base(rank: int) -> int:
 
 # ncu --set full of ks_fused_kernel, 148 ciphertexts of N = 8192, 3 + 1 limbs
 # per launch (summary under profiles/)
-KS_TRAFFIC_148 = 107.2e6 + 70.4e6
-KS_FMAHEAVY_FRAC_148 = 0.588
+KS_TRAFFIC_148 = 106.9e6 + 68.4e6
+KS_FMAHEAVY_FRAC_148 = 0.580
 
 
 def load_peaks():
@@ -358,7 +358,7 @@ def ks_roofline(params, lanes: int, reps: int = 20, level: int = 0):
     traffic = None
     if (n, L, K) == (8192, 3, 1):
         # DRAM read + write of one 148-ciphertext launch from the ncu capture
-        # of this shape under profiles/: 177.6 MB, of which the key (read
+        # of this shape under profiles/: 175.3 MB, of which the key (read
         # once) is key_bytes; the rest grows with the ciphertexts.
         traffic = (KS_TRAFFIC_148 - key_bytes) * lanes / 148 + key_bytes
     return {"bound": "hbm", "kernel": f"ks_fused_kernel (rotation key switch, N={n}, {L} limbs, {lanes} ciphertexts/launch)",
