@@ -73,6 +73,35 @@ class Encoder:
         M = self.n * np.fft.ifft(y)
         return M[self.t] / scale
 
+    def decode_real_batch(self, coeffs: np.ndarray, scale, slots: int | None = None) -> np.ndarray:
+        """Real parts of decode_batch: slot j of row r is Re m_r(zeta^(5^j)) /
+        scale (scale: a number or one per row). One zero-padded real FFT of
+        length 2N evaluates m at every 2N-th root of unity. Root zeta^e and
+        its conjugate zeta^(2N-e) have equal real parts, so slot j reads bin
+        min(e_j, 2N - e_j). There is no complex twist, and only the needed
+        columns are gathered."""
+        if not hasattr(self, "_rbin"):
+            e = np.array([pow(5, j, 2 * self.n) for j in range(self.slots)], dtype=np.int64)
+            self._rbin = np.minimum(e, 2 * self.n - e)
+        c = np.asarray(coeffs, dtype=np.float64)
+        if slots is not None and slots <= 64:
+            # few slots: Re m(zeta^e) = sum_k c_k cos(pi k e / N), one matrix product
+            out = c @ self._cos_matrix(slots)
+        else:
+            R = _sfft.rfft(c, n=2 * self.n, axis=1, workers=-1)
+            idx = self._rbin if slots is None else self._rbin[:slots]
+            out = np.take(R.real, idx, axis=1)
+        sc = np.asarray(scale, dtype=np.float64)
+        return out / (sc[:, None] if sc.ndim else sc)
+
+    def _cos_matrix(self, slots: int) -> np.ndarray:
+        """(N, slots): cos(pi k e_j / N), the exponent reduced exactly mod 2N."""
+        if getattr(self, "_cos", None) is None or self._cos.shape[1] < slots:
+            k = np.arange(self.n, dtype=np.int64)[:, None]
+            m = (k * self._rbin[None, :slots]) % (2 * self.n)
+            self._cos = np.cos(np.pi * m / self.n)
+        return self._cos[:, :slots]
+
     def decode_batch(self, coeffs: np.ndarray, scale: float, slots: int | None = None) -> np.ndarray:
         """decode() for each row of a (count, N) coefficient array, the first
         `slots` slots (all by default); the transforms run on every host core."""

@@ -203,8 +203,7 @@ class WorkloadBackend:
     def select(self, recs, got: dict) -> None:
         """Stage 2 on the host: decode the coarse distances, keep the nprobe nearest lists."""
         wl = self.wl
-        vals = wl.client.enc.decode_batch(got["coef"], 1.0, self.iqm.coarse_slots_needed())
-        vals = (vals / got["scale"][:, None]).real
+        vals = wl.client.enc.decode_real_batch(got["coef"], got["scale"], self.iqm.coarse_slots_needed())
         for r, c in zip(recs, self.iqm.coarse_from_slots(vals)):
             r.probes = list(np.argsort(c, kind="stable")[:r.nprobe or wl.spec.nprobe])
 
@@ -215,7 +214,10 @@ class WorkloadBackend:
         count = len(vids)
         coef = got["coef"].reshape(-1, self.n)               # one row per result ciphertext
         per = coef.shape[0] // count
-        d = (wl.client.enc.decode_batch(coef, 1.0) / np.repeat(got["scale"], per)[:, None]).real.reshape(count, -1)
+        # one result each: decode only up to the last candidate slot
+        slots = (min(self.iqm.sh.slots, max((int(p[-1]) + 1 if len(p) else 1) for p in got["pos"]))
+                 if per == 1 else None)
+        d = wl.client.enc.decode_real_batch(coef, np.repeat(got["scale"], per), slots).reshape(count, -1)
         out = []
         for v, p, row in zip(vids, got["pos"], d):
             order = np.argsort(row[p], kind="stable")[:wl.spec.top_k]

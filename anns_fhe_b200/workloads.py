@@ -164,7 +164,7 @@ class Workload:
         messages are far below q_0 / 2; the query manager checks the bound);
         row i is decoded at scales[i]."""
         coef = self.client.decrypt_batch_coef(cts, 1)
-        return (self.client.enc.decode_batch(coef, 1.0, slots) / np.asarray(scales, dtype=np.float64)[:, None]).real
+        return self.client.enc.decode_real_batch(coef, np.asarray(scales, dtype=np.float64), slots)
 
     def coarse(self, recs) -> np.ndarray:
         """(count, n_list) decrypted coarse distances."""

@@ -124,8 +124,8 @@ def run_ours(args, rank: int, world: int):
         # client receives limb 0 of the compacted coarse distances, decrypts, selects
         box = iqm.read_results("compact", recs, staged=True)[:, 0]
         d2h = box.nbytes
-        coarse = iqm.coarse_from_slots(
-            wl.client.decrypt_host_batch(box, 1, iqm.out_scale, iqm.coarse_slots_needed()).real)
+        coarse = iqm.coarse_from_slots(wl.client.enc.decode_real_batch(
+            wl.client.decrypt_host_batch_coef(box, 1), iqm.out_scale, iqm.coarse_slots_needed()))
         for r, c in zip(recs, coarse):
             r.probes = list(np.argsort(c, kind="stable")[:wl.spec.nprobe])
         iqm.stage3_fine(recs)
@@ -133,7 +133,10 @@ def run_ours(args, rank: int, world: int):
         box = iqm.read_results("dists", recs, staged=True)
         d2h += box.nbytes
         S = iqm.sh.slots
-        dists = wl.client.decrypt_host_batch(box.reshape(-1, 2, n), 1, iqm.out_scale).real.reshape(len(recs), -1)
+        last = max((int(r.pos[-1]) + 1 if len(r.pos) else 1) for r in recs)
+        dists = wl.client.enc.decode_real_batch(wl.client.decrypt_host_batch_coef(box.reshape(-1, 2, n), 1),
+                                                iqm.out_scale, min(S, last) if box.shape[1] == 1 else None)
+        dists = dists.reshape(len(recs), -1)
         for r, d in zip(recs, dists):
             np.argsort(d[np.asarray(r.pos)], kind="stable")[:wl.spec.top_k]
         eb.record(stream)

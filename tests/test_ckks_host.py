@@ -97,3 +97,23 @@ def test_batch_offsets_never_straddle():
             end = off + cnt
         assert end <= InteractiveQueryManager.results_needed(sum(counts), S, B) * S
     assert batch_offsets([3, 3, 3], 8) == [0, 3, 8]
+
+
+def test_decode_real_matches_decode():
+    """The client's real decode (a zero-padded real FFT of length 2N, or a
+    cosine-matrix product for a few slots) gives the real parts of the
+    canonical-embedding decode, to float64 rounding, with per-row scales."""
+    import numpy as np
+
+    from anns_fhe_b200.ckks import Encoder
+    e = Encoder(10)
+    rng = np.random.default_rng(3)
+    coef = np.rint(rng.normal(0, 1e9, (5, 1024)))
+    want = np.stack([e.decode(c, 2.0**30).real for c in coef])
+    for slots in (None, 100, 8):
+        got = e.decode_real_batch(coef, 2.0**30, slots)
+        assert got.shape == (5, slots or 512)
+        assert np.max(np.abs(got - want[:, :got.shape[1]])) < 1e-12 * np.max(np.abs(want))
+    sc = np.array([1.0, 2.0, 4.0, 8.0, 16.0]) * 2.0**30
+    got = e.decode_real_batch(coef, sc, 8)
+    assert np.allclose(got * sc[:, None] / 2.0**30, e.decode_real_batch(coef, 2.0**30, 8), rtol=0, atol=1e-9)
