@@ -448,6 +448,7 @@ static int arena_copy(afhe_ctx* ctx, bool poly, bool to_dev, u64 off, void* host
     u64 size = poly ? ctx->prm.poly_words : ctx->prm.key_words;
     if (!range_ok(off, count, size)) return fail(ctx, AFHE_E_RANGE, "arena access out of range");
     if (count == 0) return AFHE_OK;
+    if (!host) return fail(ctx, AFHE_E_ARG, "null host buffer");
     u64* base = (poly ? ctx->poly : ctx->key) + off;
     cudaError_t e = to_dev ? cudaMemcpyAsync(base, host, count * 8, cudaMemcpyHostToDevice, ctx->st)
                            : cudaMemcpyAsync(host, base, count * 8, cudaMemcpyDeviceToHost, ctx->st);

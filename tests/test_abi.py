@@ -59,6 +59,42 @@ def test_ctx_create_rejects_bad_params(lib):
     assert lib.afhe_ctx_create(C.byref(p), C.byref(h)) == _lib.E_ARG
 
 
+def test_ctx_create_rejects_bad_primes_and_roots(lib):
+    """Parameter checks run before any device call, so they need no GPU."""
+    from anns_fhe_b200.driver import find_ntt_primes
+    q = find_ntt_primes(10, 40, 3)
+    p = find_ntt_primes(10, 45, 1)
+
+    def params(qs, ps, alpha=1, psi_q=()):
+        pr = _lib.Params()
+        pr.log_n, pr.num_q, pr.num_p, pr.alpha = 10, len(qs), len(ps), alpha
+        for i, x in enumerate(qs):
+            pr.q[i] = x
+        for i, x in enumerate(ps):
+            pr.p[i] = x
+        for i, x in enumerate(psi_q):
+            pr.psi_q[i] = x
+        pr.poly_words, pr.key_words = 1 << 14, 1 << 14
+        return pr
+
+    h = _lib.CTX()
+
+    def create(pr):
+        return lib.afhe_ctx_create(C.byref(pr), C.byref(h))
+
+    assert create(params([], p)) == _lib.E_ARG                      # no Q primes
+    assert create(params(q, [])) == _lib.E_ARG                      # no P primes
+    assert create(params(q, [q[0]])) == _lib.E_ARG                  # a prime twice
+    assert create(params(q, p, alpha=0)) == _lib.E_ARG
+    assert create(params(q[:2] + [10007], p)) == _lib.E_ARG          # prime, but not 1 mod 2N
+    # psi must be a primitive 2N-th root: psi^N = -1 mod q
+    assert create(params(q, p, psi_q=[1])) == _lib.E_ARG
+    assert create(params(q, p, psi_q=[q[0]])) == _lib.E_ARG          # not reduced
+    psi = lib.afhe_min_primitive_root(10, q[0])
+    assert pow(psi, 1 << 10, q[0]) == q[0] - 1
+    assert not h.value
+
+
 def test_null_context_is_an_error(lib):
     assert lib.afhe_sync(None) == _lib.E_ARG
     a = _lib.AccelArgs()
