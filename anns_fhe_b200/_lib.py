@@ -101,6 +101,9 @@ SIGNATURES = {
     "afhe_read_poly_async": (C.c_int, [CTX, u64, P64, u64]),
     "afhe_copy_poly": (C.c_int, [CTX, u64, u64, u64]),
     "afhe_read_poly_rows": (C.c_int, [CTX, u64, u64, u64, u64, P64]),
+    "afhe_read_poly_rows_async": (C.c_int, [CTX, u64, u64, u64, u64, P64]),
+    "afhe_fence": (C.c_int, [CTX, C.POINTER(C.c_uint64)]),
+    "afhe_fence_wait": (C.c_int, [CTX, u64]),
     "afhe_host_alloc": (C.c_int, [u64, C.POINTER(C.c_void_p)]),
     "afhe_ctx_set_option": (C.c_int, [CTX, u32, C.c_int64]),
     "afhe_ctx_get_option": (C.c_int, [CTX, u32, C.POINTER(C.c_int64)]),

@@ -323,14 +323,11 @@ class CkksClient:
         L.check(self.ctx.lib.afhe_decrypt_batch(self.ctx.h, arr, count, self.s_slot, out, level), "decrypt_batch")
         limbs = self.ctx.read_poly(out, count * level * n,
                                    self.ctx.staging.get("dec_coef", count * level * n)).reshape(count, level * n)
-        if level == 1 and self.p.q[0] < 2**53:
-            # residues below 2^53 convert to float64 exactly; centre in place
-            q = float(self.p.q[0])
-            coef = limbs.astype(np.float64)
-            coef -= q * (coef > q // 2)
-        else:
-            coef = np.stack([crt_centered(row, self.p.q[:level]).astype(np.float64) for row in limbs])
-        return coef
+        return centred_coefficients(limbs, self.p.q, level)
+
+    def decryptor(self, max_count: int, max_level: int = 1) -> "CkksDecryptor":
+        """This client's decryption on a device context of its own (see CkksDecryptor)."""
+        return CkksDecryptor(self, max_count, max_level)
 
     def decrypt_host_batch(self, cts: np.ndarray, level: int, scale: float, slots: int | None = None) -> np.ndarray:
         """Decrypt ciphertexts received as a host array (count, 2, level * N)."""
@@ -347,6 +344,61 @@ class CkksClient:
     def plaintext(self, values, scale: float, off: int, level: int) -> None:
         """Encode `values` into an evaluation-form plaintext at `off` (level limbs)."""
         self._put_ntt(off, self.enc.encode(values, scale), level)
+
+
+def centred_coefficients(limbs: np.ndarray, q, level: int) -> np.ndarray:
+    """(count, level * N) residues of decrypted polynomials -> (count, N)
+    float64 coefficients, centred in (-Q/2, Q/2] for Q = q_0 ... q_(level-1)."""
+    if level == 1 and q[0] < 2**53:
+        # residues below 2^53 convert to float64 exactly; centre in place
+        qf = float(q[0])
+        coef = limbs.astype(np.float64)
+        coef -= qf * (coef > q[0] // 2)
+        return coef
+    return np.stack([crt_centered(row, q[:level]).astype(np.float64) for row in limbs])
+
+
+class CkksDecryptor:
+    """The client's decryption on a device context of its own: its own stream
+    and arenas, holding only the first limbs of the secret key's evaluation
+    form. Its device work does not queue behind the server's work on the
+    server's context, so the client can decrypt the results of one group of
+    queries while the server computes the next group. Same arithmetic and
+    results as CkksClient.decrypt_host_batch_coef."""
+
+    def __init__(self, client: CkksClient, max_count: int, max_level: int = 1):
+        p = client.p
+        n = p.n
+        self.p, self.enc = p, client.enc
+        self.max_count, self.max_level = max_count, max_level
+        self.s_off = 0
+        self.in_off = max_level * n
+        self.out_off = self.in_off + 2 * max_count * max_level * n
+        self.ctx = FheContext(p, poly_words=self.out_off + max_count * max_level * n, key_words=n,
+                              device=client.ctx.device, max_batch=1)
+        self.ctx.write_poly(self.s_off, client.ctx.read_poly(client.s_slot, max_level * n))
+
+    def decrypt_host_batch_coef(self, cts: np.ndarray, level: int) -> np.ndarray:
+        """Ciphertexts received as a host array (count, 2, level * N) -> (count,
+        N) float64 coefficients: m = c0 + c1 s and the INTT on the device,
+        centring on the host."""
+        from . import _lib as L
+        n, count = self.p.n, cts.shape[0]
+        if count > self.max_count or not 1 <= level <= self.max_level:
+            raise ValueError(f"{count} ciphertexts at level {level}: the decryptor holds "
+                             f"{self.max_count} at levels up to {self.max_level}")
+        w = level * n
+        self.ctx.write_poly(self.in_off, np.ascontiguousarray(cts).reshape(-1))
+        arr = (L.CtRef * max(count, 1))()
+        for i in range(count):
+            arr[i].c0_offset, arr[i].c1_offset = self.in_off + 2 * i * w, self.in_off + (2 * i + 1) * w
+        L.check(self.ctx.lib.afhe_decrypt_batch(self.ctx.h, arr, count, self.s_off, self.out_off, level),
+                "decrypt_batch")
+        limbs = self.ctx.read_poly(self.out_off, count * w, self.ctx.staging.get("dec_coef", count * w))
+        return centred_coefficients(limbs.reshape(count, w), self.p.q, level)
+
+    def close(self) -> None:
+        self.ctx.close()
 
 
 def encode_plaintexts(ctx: FheContext, enc: Encoder, values: np.ndarray, scale: float, offs, level: int,

@@ -427,6 +427,7 @@ int afhe_ctx_destroy(afhe_ctx* ctx) {
     fr(ctx->ring.dev);
     if (ctx->ring.host) cudaFreeHost(ctx->ring.host);
     for (auto& ev : ctx->ring.ev) if (ev) cudaEventDestroy(ev);
+    for (auto& ev : ctx->fences) if (ev) cudaEventDestroy(ev);
     if (ctx->st) cudaStreamDestroy(ctx->st);
     delete ctx;
     return AFHE_OK;
@@ -468,8 +469,7 @@ int afhe_read_key(afhe_ctx* c, uint64_t o, uint64_t* d, uint64_t n) { return are
 int afhe_write_poly_async(afhe_ctx* c, uint64_t o, const uint64_t* s, uint64_t n) { return arena_copy(c, true, true, o, (void*)s, n, true); }
 int afhe_read_poly_async(afhe_ctx* c, uint64_t o, uint64_t* d, uint64_t n) { return arena_copy(c, true, false, o, d, n, true); }
 
-int afhe_read_poly_rows(afhe_ctx* ctx, uint64_t off, uint64_t stride, uint64_t rows, uint64_t row_words,
-                        uint64_t* dst) {
+static int read_rows(afhe_ctx* ctx, u64 off, u64 stride, u64 rows, u64 row_words, u64* dst, bool async) {
     if (!ctx || (rows && !dst)) return fail(ctx, AFHE_E_ARG, "null argument");
     if (rows == 0 || row_words == 0) return AFHE_OK;
     if (stride < row_words) return fail(ctx, AFHE_E_ARG, "row stride shorter than a row");
@@ -481,7 +481,38 @@ int afhe_read_poly_rows(afhe_ctx* ctx, uint64_t off, uint64_t stride, uint64_t r
     else
         CK(cudaMemcpy2DAsync(dst, row_words * 8, ctx->poly + off, stride * 8, row_words * 8, rows,
                              cudaMemcpyDeviceToHost, ctx->st));
-    CK(cudaStreamSynchronize(ctx->st));
+    if (!async) CK(cudaStreamSynchronize(ctx->st));
+    return AFHE_OK;
+}
+
+int afhe_read_poly_rows(afhe_ctx* ctx, uint64_t off, uint64_t stride, uint64_t rows, uint64_t row_words,
+                        uint64_t* dst) {
+    return read_rows(ctx, off, stride, rows, row_words, dst, false);
+}
+
+int afhe_read_poly_rows_async(afhe_ctx* ctx, uint64_t off, uint64_t stride, uint64_t rows, uint64_t row_words,
+                              uint64_t* dst) {
+    return read_rows(ctx, off, stride, rows, row_words, dst, true);
+}
+
+static constexpr size_t kFences = 64;
+
+int afhe_fence(afhe_ctx* ctx, uint64_t* fence) {
+    if (!ctx || !fence) return fail(ctx, AFHE_E_ARG, "null argument");
+    if (ctx->fences.empty()) ctx->fences.assign(kFences, nullptr);
+    cudaEvent_t& ev = ctx->fences[ctx->fence_next % kFences];
+    if (!ev) CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    CK(cudaEventRecord(ev, ctx->st));
+    *fence = ctx->fence_next++;
+    return AFHE_OK;
+}
+
+int afhe_fence_wait(afhe_ctx* ctx, uint64_t fence) {
+    if (!ctx) return fail(nullptr, AFHE_E_ARG, "null context");
+    if (fence >= ctx->fence_next) return fail(ctx, AFHE_E_ARG, "fence not issued by this context");
+    // a fence whose event was recorded again by a later fence waits for that
+    // later point of the same stream, which is after the work it marks
+    CK(cudaEventSynchronize(ctx->fences[fence % kFences]));
     return AFHE_OK;
 }
 

@@ -114,6 +114,9 @@ struct afhe_ctx {
     afhe::DescRing ring;
     bool ks_fused = true;   // one-kernel key switch where supported (AFHE_KS_FUSED=0 turns it off)
     uint32_t chunk = 0;     // ciphertexts per launch of a batched call (0: all lanes)
+    // afhe_fence: fence f is event fences[f % size], recorded on st
+    std::vector<cudaEvent_t> fences;
+    uint64_t fence_next = 0;
 
     // key directory
     bool has_relin = false;

@@ -206,6 +206,7 @@ class FheContext:
         pr.poly_words, pr.key_words, pr.device = poly_words, key_words, device
         pr.max_batch = max_batch
         self.max_batch = max_batch or 64
+        self.device = device
         h = L.CTX()
         check(self.lib.afhe_ctx_create(C.byref(pr), C.byref(h)), "afhe_ctx_create")
         self.h = h
@@ -272,6 +273,16 @@ class FheContext:
 
     def sync(self) -> None:
         check(self.lib.afhe_sync(self.h), "sync")
+
+    def fence(self) -> int:
+        """A fence after the work enqueued so far on the context's stream."""
+        f = C.c_uint64()
+        check(self.lib.afhe_fence(self.h, C.byref(f)), "fence")
+        return int(f.value)
+
+    def fence_wait(self, fence: int) -> None:
+        """Block until the work before `fence` has finished."""
+        check(self.lib.afhe_fence_wait(self.h, fence), "fence_wait")
 
     def write_context_tables(self, level: int) -> L.ContextLayout:
         lay = L.ContextLayout()

@@ -358,24 +358,30 @@ class InteractiveQueryManager:
         first = rec.compact if kind == "compact" else rec.results[0]
         return (first[0] - base) // (2 * per * self.lvl_out * self.p.n)
 
-    def read_results(self, kind: str, recs, staged: bool = False) -> np.ndarray:
+    def read_results(self, kind: str, recs, staged: bool = False, tag: str = "", wait: bool = True):
         """Limb 0 of both polynomials of the records' result ciphertexts:
         (len(recs), per_record, 2, N); one copy per contiguous run of records.
         Limb 0 is what the client decrypts (see __init__). With `staged`, the
         array is a view of the context's page-locked staging, valid until the
-        next staged read of the same kind."""
+        next staged read of the same kind and `tag`. With wait=False (staged
+        only) the copy of a contiguous run is only enqueued, and the call
+        returns (array, fence): the array holds the results once
+        ctx.fence_wait(fence) has returned."""
         base, per = self._outbox[kind]
         n, w = self.p.n, self.lvl_out * self.p.n
         idx = [self.record_index(kind, r) for r in recs]
         size = len(recs) * per * 2 * n
         if staged:
-            out = self.ctx.staging.get("res_" + kind, size).reshape(len(recs), per, 2, n)
+            out = self.ctx.staging.get("res_" + kind + tag, size).reshape(len(recs), per, 2, n)
         else:
+            if not wait:
+                raise ValueError("an asynchronous read needs page-locked staging")
             out = np.empty((len(recs), per, 2, n), dtype=np.uint64)
         if idx and idx == list(range(idx[0], idx[0] + len(idx))):     # one run, in order: read in place
-            L.check(self.lib.afhe_read_poly_rows(self.ctx.h, base + idx[0] * per * 2 * w, w, len(idx) * per * 2, n,
-                                                 out.ctypes.data_as(L.P64)), "read_poly_rows")
-            return out
+            fn = self.lib.afhe_read_poly_rows if wait else self.lib.afhe_read_poly_rows_async
+            L.check(fn(self.ctx.h, base + idx[0] * per * 2 * w, w, len(idx) * per * 2, n, out.ctypes.data_as(L.P64)),
+                    "read_poly_rows")
+            return out if wait else (out, self.ctx.fence())
         order = np.argsort(idx, kind="stable")
         i = 0
         while i < len(order):
@@ -390,7 +396,7 @@ class InteractiveQueryManager:
             for k in range(i, j + 1):
                 out[order[k]] = block[k - i]
             i = j + 1
-        return out
+        return out if wait else (out, self.ctx.fence())
 
     def coarse_from_slots(self, vals: np.ndarray) -> np.ndarray:
         """(count, n_list) coarse distances from the decoded slots of the

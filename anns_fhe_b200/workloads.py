@@ -84,6 +84,29 @@ def dimpack_layout(q: np.ndarray, sh: QueryShape) -> np.ndarray:
     return np.repeat(np.asarray(q, dtype=np.float64), sh.B)
 
 
+def ranked_prefix(vals: np.ndarray, pos, k: int) -> list[np.ndarray]:
+    """For each row r: the first k entries of argsort(vals[r, pos[r]],
+    kind="stable"), i.e. the k smallest values in order, ties by position.
+    The k-th smallest value of each row comes from one partition of a padded
+    matrix; only the entries up to it are then sorted, all rows together."""
+    rows = len(pos)
+    lens = np.array([len(p) for p in pos], dtype=np.int64)
+    width = int(lens.max()) if rows else 0
+    if width == 0 or k <= 0:
+        return [np.zeros(0, dtype=np.int64) for _ in range(rows)]
+    M = np.full((rows, width), np.inf)
+    r_idx = np.repeat(np.arange(rows), lens)
+    c_idx = np.arange(int(lens.sum())) - np.repeat(np.cumsum(lens) - lens, lens)
+    M[r_idx, c_idx] = vals[r_idx, np.concatenate([np.asarray(p, dtype=np.int64) for p in pos])]
+    kk = min(k, width)
+    kth = np.partition(M, kk - 1, axis=1)[:, kk - 1]
+    rr, cc = np.nonzero(M <= kth[:, None])
+    order = np.lexsort((cc, M[rr, cc], rr))          # by row, then value, then position
+    rr, cc = rr[order], cc[order]
+    starts = np.searchsorted(rr, np.arange(rows))
+    return [cc[starts[i]:starts[i] + min(kk, int(lens[i]))] for i in range(rows)]
+
+
 class Workload:
     def __init__(self, spec: WorkloadSpec = SMALL, max_queries: int = 64, lanes: int = 64, device: int = 0,
                  index: IvfPqIndex | None = None, levels=None, max_nprobe: int | None = None,
@@ -209,6 +232,64 @@ class Workload:
             order = np.argsort(d, kind="stable")[:self.spec.top_k]
             o.update(dists=d, vids=list(r.vids), topk=[r.vids[i] for i in order])
         return out
+
+    def run_host_pipelined(self, recs: list[QueryRecord], host_cts, dec, groups: int = 2):
+        """The interactive protocol for `recs` through the C ABI from host
+        buffers, with the records split into `groups` runs of consecutive
+        records whose client and server work overlap.
+
+        Per group: host->device copy of the encrypted queries (host_cts[i]:
+        record i's c0, c1 of both layouts, page-locked), stage 1/1b, and an
+        asynchronous copy of limb 0 of the compacted coarse distances to the
+        host. Then, group by group, the client waits for its group's copy,
+        decrypts (on its own context, `dec`: a CkksDecryptor), keeps the
+        nprobe nearest lists, and the server runs stage 3 with an
+        asynchronous copy back. Last, group by group, the client decrypts
+        and ranks the candidates. While the client works on one group the
+        server computes the next one's stage. Each query's result is the one
+        `run` gives. Returns (top-k id lists, host->device bytes,
+        device->host bytes)."""
+        from . import _lib as L
+        lib, h = self.ctx.lib, self.ctx.h
+        iqm, n, S = self.iqm, self.params.n, self.iqm.sh.slots
+        size = -(-len(recs) // max(1, groups))
+        parts = [(recs[i:i + size], host_cts[i:i + size]) for i in range(0, len(recs), size)]
+        h2d = d2h = 0
+        coarse = []
+        for g, (part, hp) in enumerate(parts):
+            for r, cts in zip(part, hp):
+                for off, a in zip((*r.ct_query, *r.ct_dim), cts):
+                    L.check(lib.afhe_write_poly_async(h, off, a.ctypes.data_as(L.P64), a.size), "write_poly_async")
+                    h2d += a.nbytes
+            iqm.stage1_coarse(part)
+            coarse.append(iqm.read_results("compact", part, staged=True, tag=str(g), wait=False))
+        fine = []
+        for g, (part, _) in enumerate(parts):
+            box, fence = coarse[g]
+            self.ctx.fence_wait(fence)
+            d2h += box.nbytes
+            scales = np.array([iqm.out_scale_at(iqm.level_of(r)) for r in part])
+            vals = dec.enc.decode_real_batch(dec.decrypt_host_batch_coef(box[:, 0], 1), scales,
+                                             iqm.coarse_slots_needed())
+            for r, c in zip(part, iqm.coarse_from_slots(vals)):
+                r.probes = list(np.argsort(c, kind="stable")[:r.nprobe or self.spec.nprobe])
+            iqm.stage3_fine(part)
+            fine.append(iqm.read_results("dists", part, staged=True, tag=str(g), wait=False))
+        out = []
+        for g, (part, _) in enumerate(parts):
+            box, fence = fine[g]
+            self.ctx.fence_wait(fence)
+            d2h += box.nbytes
+            pos = [np.asarray(r.pos, dtype=np.int64) for r in part]
+            last = max((int(p[-1]) + 1 if len(p) else 1) for p in pos)
+            need = -(-last // S)                      # result ciphertexts that hold candidates
+            scales = np.repeat([iqm.out_scale_at(iqm.level_of(r)) for r in part], need)
+            coef = dec.decrypt_host_batch_coef(box[:, :need].reshape(-1, 2, n), 1)
+            vals = dec.enc.decode_real_batch(coef, scales, min(S, last) if need == 1 else None)
+            vals = vals.reshape(len(part), -1)
+            for r, top in zip(part, ranked_prefix(vals, pos, self.spec.top_k)):
+                out.append([r.vids[i] for i in top])
+        return out, h2d, d2h
 
     def plaintext(self, q: np.ndarray, nprobe: int | None = None):
         coarse = plaintext_coarse(self.index, q)

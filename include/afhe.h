@@ -197,6 +197,17 @@ int afhe_host_free(void* p);
  * (SimMemoryBus, sim_memory_bus.h:10-34). */
 int afhe_read_poly_rows(afhe_ctx* ctx, uint64_t word_offset, uint64_t stride, uint64_t rows,
                         uint64_t row_words, uint64_t* dst);
+/* afhe_read_poly_rows enqueued on the context's stream without waiting: dst
+ * (page-locked, e.g. from afhe_host_alloc, for the copy to overlap) holds the
+ * rows once a fence issued after this call has been waited on. Lets a client
+ * take the results of one group of queries while the server works on the
+ * next; the reference host reads results synchronously (sim_memory_bus.h:10-34). */
+int afhe_read_poly_rows_async(afhe_ctx* ctx, uint64_t word_offset, uint64_t stride, uint64_t rows,
+                              uint64_t row_words, uint64_t* dst);
+/* Fences on the context's stream: afhe_fence marks all work enqueued so far;
+ * afhe_fence_wait blocks the host until that work has finished. */
+int afhe_fence(afhe_ctx* ctx, uint64_t* fence);
+int afhe_fence_wait(afhe_ctx* ctx, uint64_t fence);
 
 /* Writes the context tables for level `level` (twiddles for all Q and P primes,
  * CRT tables for that level) into key_gmem in the reference's arrangement and

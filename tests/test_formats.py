@@ -90,3 +90,26 @@ def test_check_catches_a_bad_constant(tmp_path):
     F.write_words(os.path.join(d, "n_inv.bin"), ninv)
     with pytest.raises(ValueError, match="n_inv"):
         F.check_package(F.load_package(d, prm.log_n, prm.alpha))
+
+
+def test_ranked_prefix_is_the_stable_argsort_prefix():
+    """The client's vectorised top-k equals np.argsort(kind="stable")[:k] row
+    by row: ragged rows, rows shorter than k, empty rows, and ties (including
+    ties at the k-th value)."""
+    from anns_fhe_b200.workloads import ranked_prefix
+    rng = np.random.default_rng(12)
+    for trial in range(40):
+        rows = int(rng.integers(1, 12))
+        width = int(rng.integers(1, 300))
+        vals = rng.integers(0, 6 if trial % 2 else 10**6, (rows, width)).astype(np.float64)
+        pos = []
+        for _ in range(rows):
+            m = int(rng.integers(0, width + 1))
+            sel = rng.choice(width, m, replace=False)      # any order: ties go by index in pos
+            pos.append(np.sort(sel) if trial % 3 else sel)
+        k = int(rng.integers(1, 12))
+        got = ranked_prefix(vals, pos, k)
+        for r in range(rows):
+            want = np.argsort(vals[r, pos[r]], kind="stable")[:k]
+            assert list(got[r]) == list(want), (trial, r)
+    assert ranked_prefix(np.zeros((2, 4)), [np.zeros(0, np.int64)] * 2, 3)[1].size == 0

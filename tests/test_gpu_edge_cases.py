@@ -269,3 +269,22 @@ def test_options_and_limits(ed):
     assert ei.value.status == L.E_ARG
     with FheContext(small, poly_words=1 << 12, key_words=1 << 12, max_batch=4096) as top:
         assert top.get_option(L.OPT_CHUNK) == 4096
+
+
+def test_fences_and_asynchronous_rows(ed):
+    lib, h, n = ed.lib, ed.h, ed.n
+    c = ed.ct(NQ)
+    ed.put_ct(0, c)
+    buf = ed.ctx.staging.get("edge_rows", 2 * n)
+    L.check(lib.afhe_read_poly_rows_async(h, ed.slot(0) + n, 2 * n, 2, n, buf.ctypes.data_as(L.P64)), "rows_async")
+    f = ed.ctx.fence()
+    ed.ctx.fence_wait(f)
+    assert np.array_equal(buf[:n], c[0][n:2 * n]) and np.array_equal(buf[n:], c[0][3 * n:4 * n])
+    # fence ids increase; a fence whose event was reused still waits and returns
+    later = [ed.ctx.fence() for _ in range(70)]
+    assert later == list(range(f + 1, f + 71))
+    ed.ctx.fence_wait(f)
+    ed.ctx.fence_wait(later[-1])
+    assert lib.afhe_fence_wait(h, later[-1] + 1) == L.E_ARG
+    assert lib.afhe_fence(h, C.POINTER(C.c_uint64)()) == L.E_ARG
+    assert lib.afhe_read_poly_rows_async(h, SLOTS * ed.PW - n, n, 2, n, buf.ctypes.data_as(L.P64)) == L.E_RANGE

@@ -58,3 +58,35 @@ def test_batched_equals_plain(wl):
         c2, d2 = wl.iqm.read_ct(r.compact), wl.iqm.read_ct(r.dists)
         assert all(np.array_equal(x, y) for x, y in zip(c, c2))
         assert all(np.array_equal(x, y) for x, y in zip(d, d2))
+
+
+def test_pipelined_host_protocol(wl):
+    """The host-buffer protocol with the queries split into groups whose
+    client and server work overlap (asynchronous result reads, fences, the
+    client decrypting on a context of its own) gives the same probes and
+    top-k for 1, 2 and 4 groups, and the plaintext search's top-k. The
+    decryptor's coefficients equal the client's own decryption."""
+    Q = wl.queries(6, seed=11)
+    recs = wl.records[:6]
+    for r in recs:
+        r.nprobe = 0
+    wl.encrypt_queries(Q, recs)
+    w = wl.params.L * wl.params.n
+    host = [[wl.ctx.read_poly(o, w) for o in (*r.ct_query, *r.ct_dim)] for r in recs]
+    dec = wl.client.decryptor(6 * max(1, wl.iqm.n_res))
+    try:
+        outs = []
+        for groups in (1, 2, 4):
+            top, h2d, d2h = wl.run_host_pipelined(recs, host, dec, groups)
+            assert h2d == 6 * 4 * w * 8 and d2h > 0
+            outs.append((top, [list(r.probes) for r in recs]))
+        assert outs[0] == outs[1] == outs[2]
+        for q, t, pr in zip(Q, *outs[1]):
+            coarse, probes, cand, dist, want = wl.plaintext(q)
+            assert pr == list(probes) and t == list(want)
+        box = wl.iqm.read_results("compact", recs)[:, 0]
+        assert np.array_equal(dec.decrypt_host_batch_coef(box, 1), wl.client.decrypt_host_batch_coef(box, 1))
+        with pytest.raises(ValueError):
+            dec.decrypt_host_batch_coef(np.zeros((6 * max(1, wl.iqm.n_res) + 1, 2, wl.params.n), np.uint64), 1)
+    finally:
+        dec.close()
