@@ -16,13 +16,15 @@ protocol is the one in docs/interactive_search_protocol.md:13-55.
   - stage 1/1b for the requests admitted since the last tick;
   - stage 3 for the queries whose lists the client selected from the
     previous tick's results.
-  The client's host work for the previous tick (decoding, list selection,
-  top-k) runs while this tick's stage 1 is on the GPU. Then both kinds of
-  results are copied to the host, and the device part of the client's
-  decryption runs. A query's record is freed once its candidate distances
-  are on the host. A request that arrives while a tick is on the GPU is
-  admitted at the next tick. Its stage 1 then shares the GPU with other
-  queries' stage 3.
+  Both kinds of results are copied to the host behind the tick's launches,
+  without waiting. At the next tick, once its stage 1 is launched, the
+  client waits for those copies and does its work on them: decryption (on
+  a device context of its own, so it does not queue behind the server),
+  decoding, list selection, top-k. So the GPU has the next stage 1 while
+  the client works. A query's record is freed once the copy of its
+  candidate distances is enqueued. A request that arrives while a tick is
+  on the GPU is admitted at the next tick. Its stage 1 then shares the GPU
+  with other queries' stage 3.
 * Results are independent of the mix. Each ciphertext's residues are those
   of the one-ciphertext-at-a-time chain, whatever else shares its launches,
   so a query's result ciphertexts are bit-identical alone and in any mix.
@@ -142,6 +144,7 @@ class WorkloadBackend:
         # limbs, the compacted coarse result and n_res candidate results at
         # lvl_out limbs
         self.bytes_per_query = (4 * Lw + 2 * w * (1 + self.iqm.n_res)) * 8
+        self._dec = {"dec": None}
 
     def with_lanes(self, lanes: int) -> "WorkloadBackend":
         """The same server and encrypted-query pool, `lanes` ciphertexts per launch."""
@@ -180,24 +183,38 @@ class WorkloadBackend:
         next tick reads the same kind again."""
         return self.iqm.read_results(kind, recs, staged=True)
 
-    def receive(self, kind: str, recs) -> dict:
-        """Results of `recs` to the client: limb 0 of the result ciphertexts
-        to the host ("box", (count, ciphertexts, 2, N)), then the device part
-        of the client's decryption ("coef", one row of N coefficients per
-        ciphertext). Synchronous."""
-        box = self.fetch(kind, recs)
-        if kind == "dists":
-            # only the result ciphertexts that hold candidates
-            need = max(1, -(-max((int(r.pos[-1]) + 1 if len(r.pos) else 1) for r in recs) // self.iqm.sh.slots))
-            box = box[:, :need]
-        else:
-            box = box[:, :1]
-        coef = self.wl.client.decrypt_host_batch_coef(box.reshape(-1, 2, self.n), 1)
-        got = {"box": box, "coef": coef.reshape(len(recs), -1),
-               "scale": np.array([self.iqm.out_scale_at(self.iqm.level_of(r)) for r in recs])}
-        if kind == "dists":     # the record may be reused before the top-k is decoded
-            got["vids"] = [list(r.vids) for r in recs]
-            got["pos"] = [np.asarray(r.pos, dtype=np.int64) for r in recs]
+    def request(self, kind: str, recs) -> dict:
+        """Enqueue the copy of the records' results (limb 0) to the host
+        behind the work already on the context stream, without waiting; the
+        handle carries what `receive` needs. The records may be reused as
+        soon as this returns: later work on them is ordered after the copy."""
+        box, fence = self.iqm.read_results(kind, recs, staged=True, wait=False)
+        h = {"kind": kind, "box": box, "fence": fence, "count": len(recs),
+             "scale": np.array([self.iqm.out_scale_at(self.iqm.level_of(r)) for r in recs])}
+        if kind == "dists":     # only the result ciphertexts that hold candidates
+            h["need"] = max(1, -(-max((int(r.pos[-1]) + 1 if len(r.pos) else 1) for r in recs) // self.iqm.sh.slots))
+            h["vids"] = [list(r.vids) for r in recs]
+            h["pos"] = [np.asarray(r.pos, dtype=np.int64) for r in recs]
+        return h
+
+    def _decryptor(self, count: int):
+        """The client's decryption context (shared by with_lanes copies),
+        grown to hold `count` ciphertexts."""
+        d = self._dec.get("dec")
+        if d is None or d.max_count < count:
+            cap = max(count, 2 * d.max_count if d else 0, self.lanes * max(1, self.iqm.n_res))
+            self._dec["dec"] = d = self.wl.client.decryptor(cap)
+        return d
+
+    def receive(self, h: dict) -> dict:
+        """A request's results to the client: wait for its copy, then the
+        device part of the client's decryption ("coef", one row of N
+        coefficients per ciphertext), on the client's own context, so it does
+        not wait for the server's work enqueued since the request."""
+        self.wl.ctx.fence_wait(h["fence"])
+        box = h["box"][:, :h.get("need", 1)]
+        coef = self._decryptor(box.shape[0] * box.shape[1]).decrypt_host_batch_coef(box.reshape(-1, 2, self.n), 1)
+        got = dict(h, box=box, coef=coef.reshape(h["count"], -1))
         return got
 
     def select(self, recs, got: dict) -> None:
@@ -229,7 +246,8 @@ class ServingLoop:
     """Continuous batching over a backend (see the module docstring).
 
     backend: an object with `records`, `bytes_per_query`, `upload(rec,
-    request)`, `coarse(recs)`, `fine(recs)`, `receive(kind, recs)`,
+    request)`, `coarse(recs)`, `fine(recs)`, `request(kind, recs)` (enqueue
+    the copy of results to the host, return a handle), `receive(handle)`,
     `select(recs, got)` and `topk(recs, got)`; `WorkloadBackend` drives the
     GPU.
     budget_bytes: HBM the in-flight queries may hold (None: every record).
@@ -237,17 +255,27 @@ class ServingLoop:
     max_admit: queries admitted per tick (None: the backend's lanes).
     keep_results: keep each query's candidate-distance ciphertext.
 
-    A tick, in order: admit arrived requests and launch their stage 1; decode,
-    on the host, the results the previous tick received, while that stage 1
-    runs on the GPU (selections, and the top-k of finished queries); launch
-    stage 3 for the queries just selected; receive this tick's results
-    (device to host, client decryption on the device). A record is freed as
-    soon as its query's candidate distances are on the host.
+    A tick, in order: admit arrived requests and launch their stage 1; take
+    the results the previous tick requested and do the client's work on
+    them while that stage 1 runs on the GPU (decryption on the client's own
+    context, selections, and the top-k of finished queries); launch stage 3
+    for the queries just selected; request this tick's results (copies to
+    the host enqueued behind its launches). A record is freed as soon as the
+    copy of its query's candidate distances is enqueued: later work on the
+    record is ordered after it on the stream.
     """
 
     def __init__(self, backend, budget_bytes: int | None = None, max_inflight: int | None = None,
-                 max_admit: int | None = None, keep_results: bool = False):
+                 max_admit: int | None = None, keep_results: bool = False, defer_from: int | None = 64):
+        """defer_from: the client takes a tick's results during the next tick
+        (behind that tick's stage 1) when the tick ran at least this many
+        queries (stage 1 plus stage 3), and at the end of the tick otherwise.
+        Deferring keeps the GPU busy while the client works, which pays
+        when ticks are large; taking them at once puts no stage-1 launch
+        ahead of them, which keeps latency down when ticks are small.
+        0: always defer; None: never."""
         self.b = backend
+        self.defer_from = defer_from
         cap = len(backend.records)
         if budget_bytes is not None:
             cap = min(cap, int(budget_bytes // backend.bytes_per_query))
@@ -260,16 +288,18 @@ class ServingLoop:
         self.keep = keep_results
         self.ticks = 0
         self.tick_log: list[tuple[int, int]] = []      # (stage-1 queries, stage-3 queries) per tick
+        self.deferred: list[bool] = []                 # per tick: results taken during the next tick
 
     def run(self, trace: list[Request], realtime: bool = True, clock=time.perf_counter) -> list[Completion]:
         """Serve `trace` (sorted by arrival). With realtime=False every request
         counts as arrived at once (the order and mixing of a saturated
         server, used by tests); latencies are then measured from the start."""
         free = deque(self.b.records[:self.capacity])
+        place = {id(r): i for i, r in enumerate(self.b.records)}
         pending = deque(sorted(trace, key=lambda r: r.arrival))
         waiting: deque = deque()
-        coarse_got = None      # (entries, received) of the last tick's stage 1
-        fine_got = None        # (entries, received) of the last tick's stage 3
+        coarse_got = None      # (entries, request handle) of the last tick's stage 1
+        fine_got = None        # (entries, request handle) of the last tick's stage 3
         done: list[Completion] = []
         t0 = clock()
         now = lambda: clock() - t0  # noqa: E731
@@ -281,6 +311,9 @@ class ServingLoop:
             while waiting and free and len(admit) < self.max_admit:
                 req = waiting.popleft()
                 admit.append((req, free.popleft(), now()))
+            # records in allocation order, so results come back as runs of
+            # consecutive records, copied in place without waiting
+            admit.sort(key=lambda e: place[id(e[1])])
             if not admit and not coarse_got and not fine_got:
                 if pending:                      # idle: wait for the next arrival
                     dt = pending[0].arrival - now()
@@ -292,14 +325,17 @@ class ServingLoop:
                 self.b.upload(rec, req)
             if arecs:
                 self.b.coarse(arecs)
-            # host work of the previous tick, overlapping the stage 1 just launched
+            # the previous tick's results, and the client's work on them,
+            # overlapping the stage 1 just launched
             selected = []
             if coarse_got:
-                entries, got = coarse_got
+                entries, got, taken = coarse_got
+                got = got if taken else self.b.receive(got)
                 self.b.select([rec for _, rec, _ in entries], got)
                 selected = [(req, rec, adm, list(rec.probes)) for req, rec, adm in entries]
             if fine_got:
-                entries, got = fine_got
+                entries, got, taken = fine_got
+                got = got if taken else self.b.receive(got)
                 tops = self.b.topk([rec for _, rec, _, _ in entries], got)
                 t_done = now()
                 for k, ((req, rec, adm, probes), top) in enumerate(zip(entries, tops)):
@@ -311,9 +347,17 @@ class ServingLoop:
             if arecs or srecs:
                 self.ticks += 1
                 self.tick_log.append((len(arecs), len(srecs)))
-            coarse_got = (admit, self.b.receive("compact", arecs)) if arecs else None
-            fine_got = (selected, self.b.receive("dists", srecs)) if srecs else None
-            for rec in srecs:                    # results are on the host: the record is free
+            # copies of this tick's results to the host, behind its launches;
+            # the client takes them next tick
+            now_ = self.defer_from is None or len(arecs) + len(srecs) < self.defer_from
+            coarse_got = (admit, self.b.request("compact", arecs), False) if arecs else None
+            fine_got = (selected, self.b.request("dists", srecs), False) if srecs else None
+            if arecs or srecs:
+                self.deferred.append(not now_)
+            if now_:
+                coarse_got = coarse_got and (admit, self.b.receive(coarse_got[1]), True)
+                fine_got = fine_got and (selected, self.b.receive(fine_got[1]), True)
+            for rec in srecs:                    # the copy is enqueued before any reuse: the record is free
                 free.append(rec)
         return done
 

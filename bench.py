@@ -204,18 +204,20 @@ def serve_leg(args, wl, host_cts, rank: int):
     be = WorkloadBackend(wl, pool=host_cts)
     plain = be.with_lanes(1)
     nplain = max(1, args.plain_queries)
-    ServingLoop(plain, max_inflight=1).run([Request(0, 0.0, 0)], realtime=False)     # warm-up
+    ServingLoop(plain, max_inflight=1, defer_from=None).run([Request(0, 0.0, 0)], realtime=False)     # warm-up
     svc = []
     for i in range(nplain):
-        c = ServingLoop(plain, max_inflight=1).run([Request(i, 0.0, i % len(host_cts))], realtime=False)[0]
+        c = ServingLoop(plain, max_inflight=1, defer_from=None).run([Request(i, 0.0, i % len(host_cts))],
+                                                                     realtime=False)[0]
         svc.append(c.service * 1e3)
     plain_qps = 1e3 * nplain / sum(svc)
     rate = args.serve_rate or 10.0 * plain_qps
     warm = make_trace(poisson_arrivals(rate, 0.3, seed=query_seed_base(rank) + 1), pool=len(host_cts), seed=1)
-    ServingLoop(be).run(warm)
+    defer = defer_arg(args.defer_from)
+    ServingLoop(be, defer_from=defer).run(warm)
     trace = make_trace(poisson_arrivals(rate, args.serve_seconds, seed=query_seed_base(rank) + 2),
                        pool=len(host_cts), seed=2)
-    loop = ServingLoop(be)
+    loop = ServingLoop(be, defer_from=defer)
     done = loop.run(trace)
     s = summarize(done)
     return {"plain": {"queries_per_s": plain_qps, "p50_ms": percentile(svc, 50), "p99_ms": percentile(svc, 99),
@@ -223,12 +225,13 @@ def serve_leg(args, wl, host_cts, rank: int):
             "served": {"offered_qps": rate, "queries_per_s": s["qps"], "p50_ms": s["p50_ms"], "p99_ms": s["p99_ms"],
                        "completed": s["completed"], "offered": len(trace), "seconds": args.serve_seconds,
                        "ticks": loop.ticks, "lanes": be.lanes, "max_inflight": loop.capacity,
+                       "defer_from": defer, "deferred_ticks": sum(loop.deferred),
                        "trace": f"seeded Poisson arrivals at {rate:.0f} queries/s (10x the plain path's rate "
                                 f"unless --serve-rate is given)"}}
 
 
 def serve_sweep(rates, seconds: float, batch: int, workload: str = "small", mixed: bool = False,
-                plain_queries: int = 32):
+                plain_queries: int = 32, defer_from: int | None = 64):
     """Serving driver: the plain path's latency and rate, then the served loop
     at each offered rate for `seconds` (seeded Poisson arrivals); one JSON
     line per rate. `mixed` is the serving trace's query mix: levels drawn
@@ -251,22 +254,30 @@ def serve_sweep(rates, seconds: float, batch: int, workload: str = "small", mixe
     budget = 120e9 if mixed else None
     plain = be.with_lanes(1)
     ptrace = make_trace(np.zeros(plain_queries + 1), pool=batch, seed=9, nprobes=nprobes)
-    ServingLoop(plain, max_inflight=1).run([ptrace[0]], realtime=False)
-    svc = [ServingLoop(plain, max_inflight=1).run([r], realtime=False)[0].service * 1e3 for r in ptrace[1:]]
+    ServingLoop(plain, max_inflight=1, defer_from=None).run([ptrace[0]], realtime=False)
+    svc = [ServingLoop(plain, max_inflight=1, defer_from=None).run([r], realtime=False)[0].service * 1e3
+           for r in ptrace[1:]]
     print(json.dumps({"path": "plain", "workload": spec.name, "mixed": mixed,
                       "queries_per_s": 1e3 * len(svc) / sum(svc), "p50_ms": percentile(svc, 50),
                       "p99_ms": percentile(svc, 99), "queries": len(svc)}), flush=True)
-    ServingLoop(be, budget_bytes=budget).run(make_trace(poisson_arrivals(max(rates[0], 1.0), 2.0, seed=1),
-                                                        pool=batch, seed=1, nprobes=nprobes))
+    ServingLoop(be, budget_bytes=budget, defer_from=defer_from).run(
+        make_trace(poisson_arrivals(max(rates[0], 1.0), 2.0, seed=1), pool=batch, seed=1, nprobes=nprobes))
     for r in rates:
         trace = make_trace(poisson_arrivals(r, seconds, seed=int(r * 10)), pool=batch, seed=int(r * 10) + 1,
                            nprobes=nprobes)
-        loop = ServingLoop(be, budget_bytes=budget)
+        loop = ServingLoop(be, budget_bytes=budget, defer_from=defer_from)
         s = summarize(loop.run(trace))
         s.update(path="served", offered_qps=r, offered=len(trace), ticks=loop.ticks, seconds=seconds,
-                 max_inflight=loop.capacity)
+                 max_inflight=loop.capacity, defer_from=defer_from,
+                 deferred_ticks=sum(loop.deferred))
         print(json.dumps(s), flush=True)
     wl.close()
+
+
+def defer_arg(v: int) -> int | None:
+    """--defer-from: a tick's results are taken during the next tick when it
+    ran at least this many queries (-1: never)."""
+    return None if v < 0 else v
 
 
 def query_seed_base(rank: int) -> int:
@@ -514,6 +525,9 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=5.0, help="served trace length")
     ap.add_argument("--serve-sweep", default="", help="serving driver: comma-separated offered rates (queries/s)")
     ap.add_argument("--mixed", action="store_true", help="serving driver: mixed query levels 6-12 and nprobe")
+    ap.add_argument("--defer-from", type=int, default=64,
+                    help="serving: ticks of at least this many queries hand their results to the client "
+                         "during the next tick (-1: never)")
     ap.add_argument("--full-level", action="store_true",
                     help="evaluate at the queries' own level instead of the workload's eval_level")
     ap.add_argument("--ntt-config", action="store_true", help="NTT microbenchmark driver (64 ct x 2 x 24 limbs, N=2^16)")
@@ -531,7 +545,7 @@ def main():
     if args.serve_sweep:
         return serve_sweep([float(x) for x in args.serve_sweep.split(",")], args.serve_seconds,
                            args.batch or (256 if args.workload == "large" else 296), args.workload, args.mixed,
-                           args.plain_queries)
+                           args.plain_queries, defer_arg(args.defer_from))
     if args.profile_step:
         return profile_step(args.profile_step, args.workload, args.lanes)
     if args.profile_ntt:

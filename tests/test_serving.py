@@ -44,7 +44,7 @@ class FakeBackend:
         """The log grouped by tick: a tick runs stage 1 (if any) then stage 3 (if any)."""
         out = []
         for kind, ids in self.log:
-            if kind.startswith("receive"):
+            if kind.startswith("receive") or kind.startswith("request"):
                 continue
             if kind == "fine" and out and "coarse" in out[-1] and "fine" not in out[-1]:
                 out[-1]["fine"] = ids
@@ -52,12 +52,19 @@ class FakeBackend:
                 out.append({kind: ids})
         return out
 
-    def receive(self, kind, recs):
-        self.log.append(("receive-" + kind, [r.i for r in recs]))
+    def request(self, kind, recs):
+        # the copy is enqueued: the records may be reused from here on
+        self.log.append(("request-" + kind, [r.i for r in recs]))
         if kind == "dists":
             self.busy -= {r.i for r in recs}
-        return {"box": np.zeros((len(recs), 2, 4), dtype=np.uint64), "ids": [r.i for r in recs],
-                "payload": [self.payload[r.i] for r in recs]}
+        return {"kind": kind, "ids": [r.i for r in recs], "payload": [self.payload[r.i] for r in recs],
+                "taken": False}
+
+    def receive(self, h):
+        assert not h["taken"], "a handle received twice"
+        h["taken"] = True
+        self.log.append(("receive-" + h["kind"], h["ids"]))
+        return {"box": np.zeros((len(h["ids"]), 2, 4), dtype=np.uint64), "ids": h["ids"], "payload": h["payload"]}
 
     def select(self, recs, got):
         assert got["ids"] == [r.i for r in recs]
@@ -135,3 +142,57 @@ def test_poisson_rate_and_percentile():
     assert abs(len(t) / 20.0 - 200.0) < 15.0
     assert np.array_equal(t, poisson_arrivals(200.0, 20.0, seed=4))
     assert percentile([1, 2, 3, 4], 50) == 2 and percentile([1, 2, 3, 4], 99) == 4
+
+
+def test_results_taken_next_tick_behind_its_stage1():
+    """A tick's results are requested (copies enqueued) at its end and taken
+    by the client in the next tick, after that tick's stage 1 is launched.
+    Each kind's handle is taken before the next request of the same kind, so
+    one staging buffer per kind suffices."""
+    be = FakeBackend(records=8, lanes=2)
+    loop = ServingLoop(be, defer_from=0)
+    done = loop.run([Request(i, 0.0, i) for i in range(7)], realtime=False)
+    assert len(done) == 7
+    open_req = {}
+    for kind, ids in be.log:
+        if kind.startswith("request-"):
+            k = kind[len("request-"):]
+            assert k not in open_req, f"a second {k} request before the first was taken"
+            open_req[k] = ids
+        elif kind.startswith("receive-"):
+            assert open_req.pop(kind[len("receive-"):]) == ids
+    assert not open_req
+    # a tick is [stage 1] [take the previous results] [stage 3] [requests]:
+    # the stage 1 of a tick is launched before the client takes anything
+    kinds = [k.split("-")[0] for k, _ in be.log]
+    for a, b in zip(kinds, kinds[1:]):
+        if b == "coarse":
+            assert a == "request"
+        if b == "receive":
+            assert a in ("coarse", "request", "receive")
+
+
+@pytest.mark.parametrize("defer_from", [None, 5])
+def test_small_ticks_take_results_at_once(defer_from):
+    """With defer_from=None every tick's results are taken at its end; with a
+    threshold, ticks that ran fewer queries take them at once and larger ones
+    during the next tick, after its stage 1 is launched. Every request still
+    completes once."""
+    be = FakeBackend(records=8, lanes=3)
+    loop = ServingLoop(be, defer_from=defer_from)
+    done = loop.run([Request(i, 0.0, i) for i in range(9)], realtime=False)
+    assert sorted(c.qid for c in done) == list(range(9))
+    assert len(loop.deferred) == len(loop.tick_log)
+    for deferred, (a, f) in zip(loop.deferred, loop.tick_log):
+        assert deferred == (defer_from is not None and a + f >= defer_from)
+    if defer_from is not None:
+        assert any(loop.deferred) and not all(loop.deferred)
+    # a tick whose results were taken at once: its requests are followed by
+    # their receives directly
+    kinds = [k for k, _ in be.log]
+    reqs = [i for i, k in enumerate(kinds) if k.startswith("request") and
+            (i + 1 == len(kinds) or not kinds[i + 1].startswith("request"))]
+    assert len(reqs) == len(loop.tick_log)
+    for i, deferred in zip(reqs, loop.deferred):
+        if not deferred:
+            assert kinds[i + 1].startswith("receive")
