@@ -326,8 +326,16 @@ class CkksClient:
         return centred_coefficients(limbs, self.p.q, level)
 
     def decryptor(self, max_count: int, max_level: int = 1) -> "CkksDecryptor":
-        """This client's decryption on a device context of its own (see CkksDecryptor)."""
-        return CkksDecryptor(self, max_count, max_level)
+        """This client's decryption on a device context of its own (see
+        CkksDecryptor); closed with close_decryptors()."""
+        d = CkksDecryptor(self, max_count, max_level)
+        self._decryptors = getattr(self, "_decryptors", []) + [d]
+        return d
+
+    def close_decryptors(self) -> None:
+        for d in getattr(self, "_decryptors", []):
+            d.close()
+        self._decryptors = []
 
     def decrypt_host_batch(self, cts: np.ndarray, level: int, scale: float, slots: int | None = None) -> np.ndarray:
         """Decrypt ciphertexts received as a host array (count, 2, level * N)."""
@@ -351,9 +359,8 @@ def centred_coefficients(limbs: np.ndarray, q, level: int) -> np.ndarray:
     float64 coefficients, centred in (-Q/2, Q/2] for Q = q_0 ... q_(level-1)."""
     if level == 1 and q[0] < 2**53:
         # residues below 2^53 convert to float64 exactly; centre in place
-        qf = float(q[0])
         coef = limbs.astype(np.float64)
-        coef -= qf * (coef > q[0] // 2)
+        coef -= float(q[0]) * (coef > float(q[0] // 2))
         return coef
     return np.stack([crt_centered(row, q[:level]).astype(np.float64) for row in limbs])
 

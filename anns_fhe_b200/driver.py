@@ -159,10 +159,10 @@ class PinnedStaging:
 
     def __init__(self):
         self.lib = L.load()
-        self.bufs: dict[str, tuple[int, int]] = {}
+        self.bufs: dict[str, tuple[int, int, np.ndarray]] = {}     # name: (pointer, words, view)
 
     def get(self, name: str, words: int) -> np.ndarray:
-        ptr, cap = self.bufs.get(name, (0, 0))
+        ptr, cap, view = self.bufs.get(name, (0, 0, None))
         if cap < words:
             if ptr:
                 self.lib.afhe_host_free(C.c_void_p(ptr))
@@ -170,11 +170,12 @@ class PinnedStaging:
             p = C.c_void_p()
             check(self.lib.afhe_host_alloc(cap * 8, C.byref(p)), "afhe_host_alloc")
             ptr = p.value
-            self.bufs[name] = (ptr, cap)
-        return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(C.c_uint64)), shape=(cap,))[:words]
+            view = np.frombuffer((C.c_uint64 * cap).from_address(ptr), dtype=np.uint64)
+            self.bufs[name] = (ptr, cap, view)
+        return view[:words]
 
     def close(self) -> None:
-        for ptr, _ in self.bufs.values():
+        for ptr, _, _ in self.bufs.values():
             if ptr:
                 self.lib.afhe_host_free(C.c_void_p(ptr))
         self.bufs = {}

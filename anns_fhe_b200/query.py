@@ -41,6 +41,8 @@ once and stay resident in HBM (poly_gmem), as do the masks.
 """
 from __future__ import annotations
 
+import ctypes as C
+import itertools
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -360,13 +362,14 @@ class InteractiveQueryManager:
 
     def read_results(self, kind: str, recs, staged: bool = False, tag: str = "", wait: bool = True):
         """Limb 0 of both polynomials of the records' result ciphertexts:
-        (len(recs), per_record, 2, N); one copy per contiguous run of records.
+        (len(recs), per_record, 2, N); one copy per run of consecutive records.
         Limb 0 is what the client decrypts (see __init__). With `staged`, the
         array is a view of the context's page-locked staging, valid until the
         next staged read of the same kind and `tag`. With wait=False (staged
-        only) the copy of a contiguous run is only enqueued, and the call
-        returns (array, fence): the array holds the results once
-        ctx.fence_wait(fence) has returned."""
+        only) the call returns (array, fence): the array holds the results
+        once ctx.fence_wait(fence) has returned. The copies are only enqueued
+        when the records are in ascending order of their outbox places (as
+        allocated); otherwise they are made at once."""
         base, per = self._outbox[kind]
         n, w = self.p.n, self.lvl_out * self.p.n
         idx = [self.record_index(kind, r) for r in recs]
@@ -377,10 +380,16 @@ class InteractiveQueryManager:
             if not wait:
                 raise ValueError("an asynchronous read needs page-locked staging")
             out = np.empty((len(recs), per, 2, n), dtype=np.uint64)
-        if idx and idx == list(range(idx[0], idx[0] + len(idx))):     # one run, in order: read in place
+        if all(a < b for a, b in zip(idx, idx[1:])):     # ascending: each run of records straight into place
             fn = self.lib.afhe_read_poly_rows if wait else self.lib.afhe_read_poly_rows_async
-            L.check(fn(self.ctx.h, base + idx[0] * per * 2 * w, w, len(idx) * per * 2, n, out.ctypes.data_as(L.P64)),
-                    "read_poly_rows")
+            i = 0
+            while i < len(idx):
+                j = i
+                while j + 1 < len(idx) and idx[j + 1] == idx[j] + 1:
+                    j += 1
+                L.check(fn(self.ctx.h, base + idx[i] * per * 2 * w, w, (j - i + 1) * per * 2, n,
+                           out[i:j + 1].ctypes.data_as(L.P64)), "read_poly_rows")
+                i = j + 1
             return out if wait else (out, self.ctx.fence())
         order = np.argsort(idx, kind="stable")
         i = 0
@@ -429,19 +438,29 @@ class InteractiveQueryManager:
     # ---- batched C-ABI helpers ----
     @staticmethod
     def _refs(cts):
-        arr = (L.CtRef * max(len(cts), 1))()
-        for i, (a, b) in enumerate(cts):
-            arr[i].c0_offset, arr[i].c1_offset = a, b
-        return arr
+        """An afhe_ct_ref array for the C ABI from (c0, c1) pairs: a list of
+        pairs or an (m, 2) array. The pointer keeps its array alive."""
+        if isinstance(cts, np.ndarray):
+            a = np.ascontiguousarray(cts, dtype=np.uint64).reshape(-1)
+        else:
+            a = np.fromiter(itertools.chain.from_iterable(cts), dtype=np.uint64, count=2 * len(cts))
+        if a.size == 0:
+            a = np.zeros(2, dtype=np.uint64)
+        return a.ctypes.data_as(C.POINTER(L.CtRef))
 
     @staticmethod
     def _offs(v):
-        return (L.u64 * max(len(v), 1))(*v)
+        """A uint64 array for the C ABI from offsets (a list or an array)."""
+        a = np.ascontiguousarray(v, dtype=np.uint64) if isinstance(v, np.ndarray) else \
+            np.fromiter(v, dtype=np.uint64, count=len(v))
+        if a.size == 0:
+            a = np.zeros(1, dtype=np.uint64)
+        return a.ctypes.data_as(L.P64)
 
     def _rotate(self, cts, r, limbs):
         self._at(limbs)
-        L.check(self.lib.afhe_eval_rotate_batch(self.ctx.h, self._refs(cts), self._refs(cts), len(cts), r, limbs),
-                "eval_rotate_batch")
+        refs = self._refs(cts)
+        L.check(self.lib.afhe_eval_rotate_batch(self.ctx.h, refs, refs, len(cts), r, limbs), "eval_rotate_batch")
 
     def _rot_acc(self, src, acc, r, limbs):
         self._at(limbs)
@@ -491,12 +510,17 @@ class InteractiveQueryManager:
         items = [(ct, s) for ct, s in items if s]
         if not items:
             return
-        top = max(abs(s) for _, s in items).bit_length()
-        for b in range(top - 1, -1, -1):
-            for sign in (1, -1):
-                sub = [ct for ct, s in items if (s > 0) == (sign > 0) and (abs(s) >> b) & 1]
-                if sub:
-                    self._rotate(sub, sign * (1 << b), limbs)
+        m = len(items)
+        cts = np.fromiter(itertools.chain.from_iterable(ct for ct, _ in items), dtype=np.uint64,
+                          count=2 * m).reshape(m, 2)
+        shift = np.fromiter((s for _, s in items), dtype=np.int64, count=m)
+        mag, up = np.abs(shift), shift > 0
+        for b in range(int(mag.max()).bit_length() - 1, -1, -1):
+            has = ((mag >> b) & 1).astype(bool)
+            for sign, side in ((1, up), (-1, ~up)):
+                sel = has & side
+                if sel.any():
+                    self._rotate(cts[sel], sign * (1 << b), limbs)
 
     def _accumulate(self, items, limbs: int) -> None:
         """items: (target, first, src). Per target, its sources of this call

@@ -145,6 +145,7 @@ class WorkloadBackend:
         # lvl_out limbs
         self.bytes_per_query = (4 * Lw + 2 * w * (1 + self.iqm.n_res)) * 8
         self._dec = {"dec": None}
+        self._pool_ptrs: dict = {}
 
     def with_lanes(self, lanes: int) -> "WorkloadBackend":
         """The same server and encrypted-query pool, `lanes` ciphertexts per launch."""
@@ -157,8 +158,11 @@ class WorkloadBackend:
         from . import _lib as L
         rec.level = self.pool_level[req.payload]
         rec.nprobe = req.nprobe
-        for off, a in zip((*rec.ct_query, *rec.ct_dim), self.pool[req.payload]):
-            L.check(self.lib.afhe_write_poly_async(self.h, off, a.ctypes.data_as(L.P64), a.size), "write_poly_async")
+        ptrs = self._pool_ptrs.get(req.payload)
+        if ptrs is None:          # pointers made once per pool entry (each keeps its array alive)
+            ptrs = self._pool_ptrs[req.payload] = [(a.ctypes.data_as(L.P64), a.size) for a in self.pool[req.payload]]
+        for off, (p, size) in zip((*rec.ct_query, *rec.ct_dim), ptrs):
+            L.check(self.lib.afhe_write_poly_async(self.h, off, p, size), "write_poly_async")
 
     def coarse(self, recs) -> None:
         lanes = self.iqm.lanes
@@ -235,11 +239,8 @@ class WorkloadBackend:
         slots = (min(self.iqm.sh.slots, max((int(p[-1]) + 1 if len(p) else 1) for p in got["pos"]))
                  if per == 1 else None)
         d = wl.client.enc.decode_real_batch(coef, np.repeat(got["scale"], per), slots).reshape(count, -1)
-        out = []
-        for v, p, row in zip(vids, got["pos"], d):
-            order = np.argsort(row[p], kind="stable")[:wl.spec.top_k]
-            out.append([v[i] for i in order])
-        return out
+        from .workloads import ranked_prefix
+        return [[v[i] for i in top] for v, top in zip(vids, ranked_prefix(d, got["pos"], wl.spec.top_k))]
 
 
 class ServingLoop:

@@ -297,4 +297,5 @@ class Workload:
         return coarse, probes, cand, dist, top
 
     def close(self) -> None:
+        self.client.close_decryptors()
         self.ctx.close()
