@@ -147,6 +147,16 @@ class WorkloadBackend:
         self._dec = {"dec": None}
         self._pool_ptrs: dict = {}
 
+    def prepare(self) -> None:
+        """Make, before serving, what the loop would otherwise allocate while
+        requests wait: the client's decryption context at its full size and
+        the page-locked staging of both kinds of results for every record."""
+        n_res = max(1, self.iqm.n_res)
+        dec = self._decryptor(len(self.records) * n_res)
+        dec.ctx.staging.get("dec_coef", len(self.records) * n_res * self.n)
+        for kind, per in (("compact", 1), ("dists", n_res)):
+            self.wl.ctx.staging.get("res_" + kind, len(self.records) * per * 2 * self.n)
+
     def with_lanes(self, lanes: int) -> "WorkloadBackend":
         """The same server and encrypted-query pool, `lanes` ciphertexts per launch."""
         other = object.__new__(WorkloadBackend)

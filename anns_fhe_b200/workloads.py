@@ -233,6 +233,55 @@ class Workload:
             o.update(dists=d, vids=list(r.vids), topk=[r.vids[i] for i in order])
         return out
 
+    # ---- protocol from host buffers, in groups of queries ----
+    def _group_stage1(self, part, hp, tag: str):
+        """Host->device copy of a group's encrypted queries (four page-locked
+        arrays per query), stage 1/1b, and an asynchronous copy of limb 0 of
+        the compacted coarse distances to the host. Returns (box, fence,
+        bytes copied to the device)."""
+        from . import _lib as L
+        lib, h = self.ctx.lib, self.ctx.h
+        h2d = 0
+        for r, cts in zip(part, hp):
+            for off, a in zip((*r.ct_query, *r.ct_dim), cts):
+                L.check(lib.afhe_write_poly_async(h, off, a.ctypes.data_as(L.P64), a.size), "write_poly_async")
+                h2d += a.nbytes
+        self.iqm.stage1_coarse(part)
+        box, fence = self.iqm.read_results("compact", part, staged=True, tag=tag, wait=False)
+        return box, fence, h2d
+
+    def _group_stage3(self, part, coarse, dec, tag: str):
+        """The client takes a group's coarse distances (waits for their copy,
+        decrypts on `dec`, keeps the nprobe nearest lists); the server runs
+        stage 3 with an asynchronous copy back. Returns (box, fence, bytes
+        copied to the host for the coarse distances)."""
+        box, fence, _ = coarse
+        iqm = self.iqm
+        self.ctx.fence_wait(fence)
+        scales = np.array([iqm.out_scale_at(iqm.level_of(r)) for r in part])
+        vals = dec.enc.decode_real_batch(dec.decrypt_host_batch_coef(box[:, 0], 1), scales,
+                                         iqm.coarse_slots_needed())
+        for r, c in zip(part, iqm.coarse_from_slots(vals)):
+            r.probes = list(np.argsort(c, kind="stable")[:r.nprobe or self.spec.nprobe])
+        iqm.stage3_fine(part)
+        fbox, ffence = iqm.read_results("dists", part, staged=True, tag=tag, wait=False)
+        return fbox, ffence, box.nbytes
+
+    def _group_topk(self, part, fine, dec):
+        """The client takes a group's candidate distances: waits for their
+        copy, decrypts the result ciphertexts that hold candidates, decodes,
+        ranks. Returns (top-k id lists, bytes copied to the host)."""
+        box, fence, _ = fine
+        iqm, n, S = self.iqm, self.params.n, self.iqm.sh.slots
+        self.ctx.fence_wait(fence)
+        pos = [np.asarray(r.pos, dtype=np.int64) for r in part]
+        last = max((int(p[-1]) + 1 if len(p) else 1) for p in pos)
+        need = -(-last // S)                      # result ciphertexts that hold candidates
+        scales = np.repeat([iqm.out_scale_at(iqm.level_of(r)) for r in part], need)
+        coef = dec.decrypt_host_batch_coef(box[:, :need].reshape(-1, 2, n), 1)
+        vals = dec.enc.decode_real_batch(coef, scales, min(S, last) if need == 1 else None).reshape(len(part), -1)
+        return [[r.vids[i] for i in top] for r, top in zip(part, ranked_prefix(vals, pos, self.spec.top_k))], box.nbytes
+
     def run_host_pipelined(self, recs: list[QueryRecord], host_cts, dec, groups: int = 2):
         """The interactive protocol for `recs` through the C ABI from host
         buffers, with the records split into `groups` runs of consecutive
@@ -249,47 +298,57 @@ class Workload:
         server computes the next one's stage. Each query's result is the one
         `run` gives. Returns (top-k id lists, host->device bytes,
         device->host bytes)."""
-        from . import _lib as L
-        lib, h = self.ctx.lib, self.ctx.h
-        iqm, n, S = self.iqm, self.params.n, self.iqm.sh.slots
         size = -(-len(recs) // max(1, groups))
         parts = [(recs[i:i + size], host_cts[i:i + size]) for i in range(0, len(recs), size)]
-        h2d = d2h = 0
-        coarse = []
-        for g, (part, hp) in enumerate(parts):
-            for r, cts in zip(part, hp):
-                for off, a in zip((*r.ct_query, *r.ct_dim), cts):
-                    L.check(lib.afhe_write_poly_async(h, off, a.ctypes.data_as(L.P64), a.size), "write_poly_async")
-                    h2d += a.nbytes
-            iqm.stage1_coarse(part)
-            coarse.append(iqm.read_results("compact", part, staged=True, tag=str(g), wait=False))
-        fine = []
-        for g, (part, _) in enumerate(parts):
-            box, fence = coarse[g]
-            self.ctx.fence_wait(fence)
-            d2h += box.nbytes
-            scales = np.array([iqm.out_scale_at(iqm.level_of(r)) for r in part])
-            vals = dec.enc.decode_real_batch(dec.decrypt_host_batch_coef(box[:, 0], 1), scales,
-                                             iqm.coarse_slots_needed())
-            for r, c in zip(part, iqm.coarse_from_slots(vals)):
-                r.probes = list(np.argsort(c, kind="stable")[:r.nprobe or self.spec.nprobe])
-            iqm.stage3_fine(part)
-            fine.append(iqm.read_results("dists", part, staged=True, tag=str(g), wait=False))
+        coarse = [self._group_stage1(part, hp, str(g)) for g, (part, hp) in enumerate(parts)]
+        h2d = sum(c[2] for c in coarse)
+        fine = [self._group_stage3(part, coarse[g], dec, str(g)) for g, (part, _) in enumerate(parts)]
+        d2h = sum(f[2] for f in fine)
         out = []
         for g, (part, _) in enumerate(parts):
-            box, fence = fine[g]
-            self.ctx.fence_wait(fence)
-            d2h += box.nbytes
-            pos = [np.asarray(r.pos, dtype=np.int64) for r in part]
-            last = max((int(p[-1]) + 1 if len(p) else 1) for p in pos)
-            need = -(-last // S)                      # result ciphertexts that hold candidates
-            scales = np.repeat([iqm.out_scale_at(iqm.level_of(r)) for r in part], need)
-            coef = dec.decrypt_host_batch_coef(box[:, :need].reshape(-1, 2, n), 1)
-            vals = dec.enc.decode_real_batch(coef, scales, min(S, last) if need == 1 else None)
-            vals = vals.reshape(len(part), -1)
-            for r, top in zip(part, ranked_prefix(vals, pos, self.spec.top_k)):
-                out.append([r.vids[i] for i in top])
+            top, nb = self._group_topk(part, fine[g], dec)
+            out += top
+            d2h += nb
         return out, h2d, d2h
+
+    def run_host_stream(self, recs: list[QueryRecord], host_cts, dec, total: int, group: int):
+        """`total` queries streamed through the protocol from host buffers:
+        query i is host_cts[i % len(host_cts)], in groups of `group`
+        consecutive queries. Group g runs on records slice g mod k of `recs`
+        (k = len(recs) // group slices of `group` records, k >= 3).
+
+        A software pipeline over the groups: while the server computes
+        group g's stage 1, the client selects group g - 1's lists (and its
+        stage 3 is enqueued) and ranks group g - 2's candidates. So the
+        client's work and the copies overlap the GPU everywhere but at the
+        two ends of the stream. Returns (top-k id lists, host->device bytes,
+        device->host bytes)."""
+        k = len(recs) // group
+        if k < 3:
+            raise ValueError("a stream keeps three groups in flight: len(recs) >= 3 * group")
+        G = -(-total // group)
+
+        def part_of(g):
+            size = min(group, total - g * group)
+            base = (g % k) * group
+            return recs[base:base + size], [host_cts[(g * group + i) % len(host_cts)] for i in range(size)]
+
+        coarse, fine, tops = {}, {}, [None] * G
+        h2d = d2h = 0
+        for it in range(G + 2):
+            if it < G:
+                part, hp = part_of(it)
+                coarse[it] = self._group_stage1(part, hp, "s%d" % (it % k))
+                h2d += coarse[it][2]
+            g = it - 1
+            if 0 <= g < G:
+                fine[g] = self._group_stage3(part_of(g)[0], coarse.pop(g), dec, "s%d" % (g % k))
+                d2h += fine[g][2]
+            g = it - 2
+            if 0 <= g < G:
+                tops[g], nb = self._group_topk(part_of(g)[0], fine.pop(g), dec)
+                d2h += nb
+        return [t for grp in tops for t in grp], h2d, d2h
 
     def plaintext(self, q: np.ndarray, nprobe: int | None = None):
         coarse = plaintext_coarse(self.index, q)

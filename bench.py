@@ -13,9 +13,11 @@ A step is one batch of `--batch` queries through the server's operator chain
   copy of the encrypted queries, stage 1/1b, device->host of the compacted
   coarse distances, client decrypt + selection, stage 3, device->host of the
   candidate distances, client decrypt + top-k, timed on the context stream.
-  The batch runs as two groups of queries (--e2e-groups) whose client and
-  server work overlap (Workload.run_host_pipelined); the client decrypts on
-  a device context of its own.
+  The K steps stream as groups of half a batch (--e2e-groups) whose client
+  and server work overlap (Workload.run_host_stream): while the server runs
+  one group's stage 1, the client selects for the group before it and ranks
+  the one before that. The client decrypts on a device context of its own.
+  Every step's queries are copied in and its results out.
 * --impl reference: the oracle restatement of the same chain on the host's
   cores (one query per process), see oracle/chain.py.
 
@@ -117,16 +119,26 @@ def run_ours(args, rank: int, world: int):
     # the client decrypts on a context of its own, so that its device work
     # does not queue behind the server's next group
     groups = max(1, args.e2e_groups)
-    dec = wl.client.decryptor(-(-args.batch // groups) * max(1, iqm.n_res))
+    group = -(-args.batch // groups)
+    dec = wl.client.decryptor(group * max(1, iqm.n_res))
     host_np = [[t.numpy() for t in cts] for cts in pinned]
 
-    def e2e_step():
+    def e2e_stream(steps):
+        """`steps` batches of queries streamed in groups (Workload.run_host_stream)
+        over all records; one timed region. With one group per batch, batch
+        after batch without overlap (Workload.run_host_pipelined)."""
         ea, eb = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ea.record(stream)
-        _, h2d, d2h = wl.run_host_pipelined(recs, host_np, dec, groups)
+        if groups > 1:
+            _, h2d, d2h = wl.run_host_stream(wl.records, host_np, dec, steps * args.batch, group)
+        else:
+            h2d = d2h = 0
+            for _ in range(steps):
+                _, a, b = wl.run_host_pipelined(recs, host_np, dec, 1)
+                h2d, d2h = h2d + a, d2h + b
         eb.record(stream)
         eb.synchronize()
-        return ea.elapsed_time(eb), h2d, d2h
+        return ea.elapsed_time(eb), h2d // steps, d2h // steps
 
     for _ in range(args.warmup):
         device_step()
@@ -145,10 +157,9 @@ def run_ours(args, rank: int, world: int):
     stop.set()
     th.join()
     total_ms = sum(ms)
-    for _ in range(max(1, args.warmup // 2)):
-        e2e_step()
-    e2e = [e2e_step() for _ in range(args.steps)]
-    e2e_ms = sum(x[0] for x in e2e)
+    e2e_stream(max(1, args.warmup // 2) + 1)
+    e2e = [e2e_stream(args.steps)]
+    e2e_ms = e2e[0][0]
     # replicas: all ranks' queries over the slowest rank's time
     total_ms, queries = aggregate(total_ms, args.batch * args.steps)
     e2e_ms, _ = aggregate(e2e_ms, args.batch * args.steps)
@@ -201,7 +212,9 @@ def serve_leg(args, wl, host_cts, rank: int):
     host buffers in and out, client decryption included."""
     from anns_fhe_b200.serving import (Request, ServingLoop, WorkloadBackend, make_trace, percentile,
                                        poisson_arrivals, summarize)
+    import gc
     be = WorkloadBackend(wl, pool=host_cts)
+    be.prepare()
     plain = be.with_lanes(1)
     nplain = max(1, args.plain_queries)
     ServingLoop(plain, max_inflight=1, defer_from=None).run([Request(0, 0.0, 0)], realtime=False)     # warm-up
@@ -217,6 +230,7 @@ def serve_leg(args, wl, host_cts, rank: int):
     ServingLoop(be, defer_from=defer).run(warm)
     trace = make_trace(poisson_arrivals(rate, args.serve_seconds, seed=query_seed_base(rank) + 2),
                        pool=len(host_cts), seed=2)
+    gc.collect()
     loop = ServingLoop(be, defer_from=defer)
     done = loop.run(trace)
     s = summarize(done)
@@ -251,6 +265,7 @@ def serve_sweep(rates, seconds: float, batch: int, workload: str = "small", mixe
     enc = WorkloadBackend(wl, wl.queries(batch, seed=77), levels=pool_levels)
     be = WorkloadBackend(wl, pool=[[torch.from_numpy(a).pin_memory().numpy() for a in cts] for cts in enc.pool],
                          pool_levels=enc.pool_level)
+    be.prepare()
     budget = 120e9 if mixed else None
     plain = be.with_lanes(1)
     ptrace = make_trace(np.zeros(plain_queries + 1), pool=batch, seed=9, nprobes=nprobes)
@@ -265,6 +280,7 @@ def serve_sweep(rates, seconds: float, batch: int, workload: str = "small", mixe
     for r in rates:
         trace = make_trace(poisson_arrivals(r, seconds, seed=int(r * 10)), pool=batch, seed=int(r * 10) + 1,
                            nprobes=nprobes)
+        __import__("gc").collect()
         loop = ServingLoop(be, budget_bytes=budget, defer_from=defer_from)
         s = summarize(loop.run(trace))
         s.update(path="served", offered_qps=r, offered=len(trace), ticks=loop.ticks, seconds=seconds,

@@ -84,6 +84,12 @@ def test_pipelined_host_protocol(wl):
         for q, t, pr in zip(Q, *outs[1]):
             coarse, probes, cand, dist, want = wl.plaintext(q)
             assert pr == list(probes) and t == list(want)
+        # streamed: 14 queries (the 6 in turn) in groups of 2 over 4 slices of the 8 records
+        top, h2d, d2h = wl.run_host_stream(wl.records[:8], host, dec, total=14, group=2)
+        assert top == [outs[0][0][i % 6] for i in range(14)]
+        assert h2d == 14 * 4 * w * 8
+        with pytest.raises(ValueError):
+            wl.run_host_stream(wl.records[:5], host, dec, total=4, group=2)
         box = wl.iqm.read_results("compact", recs)[:, 0]
         assert np.array_equal(dec.decrypt_host_batch_coef(box, 1), wl.client.decrypt_host_batch_coef(box, 1))
         with pytest.raises(ValueError):
