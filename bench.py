@@ -418,6 +418,85 @@ def profile_step(nq: int, workload: str = "small", lanes: int = 0):
     wl.close()
 
 
+def profile_host(batch: int = 296, steps: int = 5):
+    """Profiling driver for the end-to-end path on the host: (1) one batch
+    through the protocol one phase at a time, each phase followed by a
+    synchronisation, its wall time averaged over `steps` steps; (2) the
+    streamed end-to-end run (Workload.run_host_stream) under cProfile, the
+    host functions with the most own time. One JSON line each."""
+    import cProfile
+    import pstats
+
+    import numpy as np
+    import torch
+
+    from anns_fhe_b200._lib import P64, check
+    from anns_fhe_b200.workloads import SMALL, Workload
+    wl = Workload(SMALL, max_queries=2 * batch, lanes=batch)
+    iqm, n = wl.iqm, wl.params.n
+    recs = wl.records[:batch]
+    wl.encrypt_queries(wl.queries(batch, seed=1000), recs)
+    Lw = wl.params.L * n
+    host = [[torch.from_numpy(wl.ctx.read_poly(o, Lw)).pin_memory().numpy() for o in (*r.ct_query, *r.ct_dim)]
+            for r in recs]
+    dec = wl.client.decryptor(batch * max(1, iqm.n_res))
+    phases: dict = {}
+
+    def mark(name, t0):
+        wl.ctx.sync()
+        t = time.perf_counter()
+        phases[name] = phases.get(name, 0.0) + (t - t0) * 1e3
+        return t
+
+    def phased_step():
+        t = time.perf_counter()
+        for r, cts in zip(recs, host):
+            for off, a in zip((*r.ct_query, *r.ct_dim), cts):
+                check(wl.ctx.lib.afhe_write_poly_async(wl.ctx.h, off, a.ctypes.data_as(P64), a.size), "write")
+        t = mark("h2d", t)
+        iqm.stage1_coarse(recs)
+        t = mark("stage1", t)
+        box = iqm.read_results("compact", recs, staged=True)[:, 0]
+        t = mark("d2h_coarse", t)
+        coef = dec.decrypt_host_batch_coef(box, 1)
+        t = mark("client_decrypt_coarse", t)
+        vals = dec.enc.decode_real_batch(coef, iqm.out_scale, iqm.coarse_slots_needed())
+        for r, c in zip(recs, iqm.coarse_from_slots(vals)):
+            r.probes = list(np.argsort(c, kind="stable")[:wl.spec.nprobe])
+        t = mark("client_decode_select", t)
+        iqm.stage3_fine(recs)
+        t = mark("stage3", t)
+        fbox = iqm.read_results("dists", recs, staged=True)
+        t = mark("d2h_dists", t)
+        wl._group_topk(recs, (fbox, wl.ctx.fence(), 0), dec)
+        mark("client_decrypt_decode_topk", t)
+
+    for _ in range(2):
+        phased_step()
+    phases.clear()
+    for _ in range(steps):
+        phased_step()
+    total = sum(phases.values()) / steps
+    print(json.dumps({"profile": "phases", "queries_per_step": batch, "ms": {k: round(v / steps, 2) for k, v in
+                      phases.items()}, "total_ms": round(total, 2), "queries_per_s": round(batch / total * 1e3, 1)}),
+          flush=True)
+    wl.run_host_stream(wl.records, host, dec, 2 * batch, batch // 2)
+    pr = cProfile.Profile()
+    t = time.perf_counter()
+    pr.enable()
+    wl.run_host_stream(wl.records, host, dec, steps * batch, batch // 2)
+    pr.disable()
+    wall = time.perf_counter() - t
+    st = pstats.Stats(pr)
+    rows = sorted(st.stats.items(), key=lambda kv: -kv[1][2])[:15]
+    print(json.dumps({"profile": "stream_cprofile", "queries": steps * batch, "wall_s": round(wall, 3),
+                      "queries_per_s_under_profiler": round(steps * batch / wall, 1),
+                      "top_own_time": [{"fn": f"{os.path.basename(k[0])}:{k[1]}({k[2]})", "calls": v[1],
+                                        "own_ms": round(v[2] * 1e3, 1), "cum_ms": round(v[3] * 1e3, 1)}
+                                       for k, v in rows]}), flush=True)
+    wl.close()
+
+
 def profile_ntt(polys: int, log_n: int = 13, reps: int = 10):
     """Profiling driver: batched in-place NTT / INTT over `polys` polynomials of
     4 limbs (the key switch's shape), forward then inverse, `reps` each."""
@@ -549,6 +628,8 @@ def main():
     ap.add_argument("--ntt-config", action="store_true", help="NTT microbenchmark driver (64 ct x 2 x 24 limbs, N=2^16)")
     ap.add_argument("--ks-config", action="store_true", help="batched key-switch driver (32 ct, N=2^16, dnum 3)")
     ap.add_argument("--profile-step", type=int, default=0, help="profiling driver: queries per step")
+    ap.add_argument("--profile-host", action="store_true",
+                    help="profiling driver: end-to-end phases and the streamed run's host hotspots")
     ap.add_argument("--profile-ntt", type=int, default=0, help="profiling driver: polynomials per NTT launch")
     ap.add_argument("--profile-ks", type=int, default=0, help="profiling driver: ciphertexts per key-switch launch")
     ap.add_argument("--level", type=int, default=0, help="limbs for --profile-ks (default: all)")
@@ -564,6 +645,8 @@ def main():
                            args.plain_queries, defer_arg(args.defer_from))
     if args.profile_step:
         return profile_step(args.profile_step, args.workload, args.lanes)
+    if args.profile_host:
+        return profile_host()
     if args.profile_ntt:
         return profile_ntt(args.profile_ntt, args.log_n)
     if args.profile_ks:
