@@ -1,6 +1,7 @@
 """Host-side helpers of the query chain, on the CPU: the ctypes arrays the
 batched entry points take, the grouping of rotations into power-of-two
-steps, and the centring of decrypted residues."""
+steps, the centring of decrypted residues, and the schedules of the
+end-to-end protocol in groups (pipelined and streamed)."""
 import ctypes as C
 
 import numpy as np
@@ -74,3 +75,79 @@ def test_centred_coefficients(level):
     got = centred_coefficients(limbs, q, level)
     want = np.stack([crt_centered(row, q[:level]).astype(np.float64) for row in limbs])
     assert np.array_equal(got, want)
+
+
+class _FakeStreamWorkload:
+    """Stands in for Workload in run_host_stream / run_host_pipelined: the
+    group steps are recorded, and each record slice's use is checked."""
+
+    def __init__(self):
+        self.log = []
+        self.in_use = set()
+
+    def _group_stage1(self, part, hp, tag):
+        ids = tuple(id(r) for r in part)
+        assert not (set(ids) & self.in_use), "a record reused while its group is in flight"
+        self.in_use |= set(ids)
+        self.log.append(("stage1", [r.qid for r in part], tag))
+        for r, h in zip(part, hp):
+            r.payload = h
+        return ("box", "fence", 10 * len(part))
+
+    def _group_stage3(self, part, coarse, dec, tag):
+        assert coarse[2] == 10 * len(part)
+        self.log.append(("stage3", [r.qid for r in part], tag))
+        return ("fbox", "ffence", 1)
+
+    def _group_topk(self, part, fine, dec):
+        self.log.append(("topk", [r.qid for r in part]))
+        self.in_use -= {id(r) for r in part}
+        return [[r.payload] for r in part], 2
+
+
+class _Rec:
+    def __init__(self, qid):
+        self.qid = qid
+
+
+@pytest.mark.parametrize("total,group,slices", [(14, 2, 4), (9, 4, 3), (1, 3, 3), (12, 3, 5)])
+def test_stream_schedule(total, group, slices):
+    """run_host_stream: group g's stage 1 is enqueued before the client
+    selects for g - 1 and ranks g - 2; three groups at most are in flight,
+    each on its own slice of the records; results come back in query order,
+    query i being host entry i mod len(host)."""
+    from anns_fhe_b200.workloads import Workload
+    fake = _FakeStreamWorkload()
+    recs = [_Rec(i) for i in range(slices * group)]
+    host = [f"q{i}" for i in range(5)]
+    tops, h2d, d2h = Workload.run_host_stream(fake, recs, host, None, total, group)
+    G = -(-total // group)
+    assert tops == [[host[i % len(host)]] for i in range(total)]
+    assert h2d == 10 * total and d2h == G * (1 + 2)
+    kinds = [e[0] for e in fake.log]
+    assert kinds.count("stage1") == kinds.count("stage3") == kinds.count("topk") == G
+    # the order of the software pipeline
+    want = []
+    for it in range(G + 2):
+        if it < G:
+            want.append("stage1")
+        if 0 <= it - 1 < G:
+            want.append("stage3")
+        if 0 <= it - 2 < G:
+            want.append("topk")
+    assert kinds == want
+    assert not fake.in_use
+    with pytest.raises(ValueError):
+        Workload.run_host_stream(fake, recs[:2 * group], host, None, total, group)
+
+
+def test_pipelined_groups_schedule():
+    """run_host_pipelined: every group's stage 1 first, then each group's
+    selection and stage 3, then each group's ranking."""
+    from anns_fhe_b200.workloads import Workload
+    fake = _FakeStreamWorkload()
+    recs = [_Rec(i) for i in range(7)]
+    tops, h2d, d2h = Workload.run_host_pipelined(fake, recs, [f"q{i}" for i in range(7)], None, 3)
+    assert tops == [[f"q{i}"] for i in range(7)]
+    assert [e[0] for e in fake.log] == ["stage1"] * 3 + ["stage3"] * 3 + ["topk"] * 3
+    assert [e[1] for e in fake.log[:3]] == [[0, 1, 2], [3, 4, 5], [6]]
