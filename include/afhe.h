@@ -205,7 +205,9 @@ int afhe_read_poly_rows(afhe_ctx* ctx, uint64_t word_offset, uint64_t stride, ui
 int afhe_read_poly_rows_async(afhe_ctx* ctx, uint64_t word_offset, uint64_t stride, uint64_t rows,
                               uint64_t row_words, uint64_t* dst);
 /* Fences on the context's stream: afhe_fence marks all work enqueued so far;
- * afhe_fence_wait blocks the host until that work has finished. */
+ * afhe_fence_wait blocks the host until that work has finished. No reference
+ * counterpart: the reference's accelerator call returns when the operation is
+ * done (fhe_host_driver.cpp:177-204 calls fhe_accel_top synchronously). */
 int afhe_fence(afhe_ctx* ctx, uint64_t* fence);
 int afhe_fence_wait(afhe_ctx* ctx, uint64_t fence);
 
