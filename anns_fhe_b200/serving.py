@@ -110,8 +110,9 @@ class WorkloadBackend:
     The encrypted-query pool is held on the host. The client encrypts each
     distinct query once, and a request's admission copies its four ciphertexts
     into the record on the context stream. Results come back to the host with
-    one copy per contiguous run of records. The client decrypts them with its
-    secret key, as in the bench's end-to-end step.
+    one asynchronous copy per run of consecutive records (`request`), into
+    page-locked staging. The client decrypts them with its secret key on a
+    device context of its own (`receive`), as in the bench's end-to-end step.
     """
 
     def __init__(self, wl, Q: np.ndarray | None = None, lanes: int | None = None,
@@ -189,13 +190,6 @@ class WorkloadBackend:
             self.iqm.stage3_fine(recs)
         finally:
             self.iqm.lanes = lanes
-
-    def fetch(self, kind: str, recs) -> np.ndarray:
-        """Limb 0 of the records' result ciphertexts, copied to the host:
-        (len(recs), per_record, 2, N), in page-locked staging. The loop
-        decodes (and copies what it keeps of) a tick's results before the
-        next tick reads the same kind again."""
-        return self.iqm.read_results(kind, recs, staged=True)
 
     def request(self, kind: str, recs) -> dict:
         """Enqueue the copy of the records' results (limb 0) to the host
