@@ -196,3 +196,36 @@ def test_accel_top_abi_vs_reference(ref, orc, refimg):
             assert np.array_equal(poly, rp), f"op {op}"
     finally:
         orc.free_ctx(ctx)
+
+
+@pytest.mark.parametrize("level", [2, 6])
+def test_rescale_vs_reference_lower_levels(ref, orc, level):
+    """Rescale from `level` limbs (tables for that level), as the reference
+    does it below the top."""
+    q, p = primes_for(14, 11, 45, 4, 60, first_bits=60)
+    img = AccelImage(14, q, p, alpha=4, table_level=level)
+    rng = np.random.default_rng(60 + level)
+    a = uniform_residues(rng, q[:level], REF_N)
+    itl = img.itw_q[(level - 1) * REF_N:level * REF_N]
+    r = ref.rescale(a, q, itl, img.tw_q, img.qlql, img.qlinv)
+    o = orc.rescale(a, q[:level], itl, img.tw_q, img.qlql, img.qlinv, REF_N)
+    assert np.array_equal(r, o)
+
+
+@pytest.mark.parametrize("sq", [9, 11])
+def test_key_switch_vs_reference_partial_digits(ref, orc, sq):
+    """The reference kernel takes three digits of alpha = 4 limbs; at 9 and 11
+    limbs its last digit holds 1 and 3 limbs."""
+    q, p = primes_for(14, 11, 45, 4, 60, first_bits=60)
+    img = AccelImage(14, q, p, alpha=4, table_level=sq, numPartQ=3, key_level=sq, seed=sq)
+    n, K = REF_N, 4
+    rng = np.random.default_rng(80 + sq)
+    c = uniform_residues(rng, q[:sq], n)
+    key = img.key[img.off["evk"]:img.off["evk"] + 2 * 3 * (sq + K) * n]
+    r0, r1 = ref.key_switch(c, key, 0, 3 * (sq + K) * n, sq, K, 3, 4, img.q, img.p, img.tw_q, img.itw_q,
+                            img.tw_p, img.itw_p, img.qhat_inv, img.qhat_modp, img.pinv, img.phinv, img.phq)
+    o0, o1 = orc.key_switch(c, np.concatenate(img.evk_a), np.concatenate(img.evk_b), sq + K, sq, sq, K, 3, 4,
+                            img.q, img.p, img.tw_q, img.itw_q, img.tw_p, img.itw_p, img.qhat_inv, img.qhat_modp,
+                            img.pinv, img.phinv, img.phq, n)
+    assert np.array_equal(r0, o0)
+    assert np.array_equal(r1, o1)
