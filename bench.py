@@ -187,7 +187,8 @@ def run_ours(args, rank: int, world: int):
                          f"ciphertexts and {wl.ctx.scratch_bytes() / 1e9:.1f} GB of lane scratch per step "
                          f"(L2 126 MB)"},
         "e2e": {"value": queries / (e2e_ms / 1e3), "unit": "queries/s",
-                "h2d_bytes_per_step": e2e[0][1], "d2h_bytes_per_step": e2e[0][2], "groups": groups},
+                "h2d_bytes_per_step": e2e[0][1], "d2h_bytes_per_step": e2e[0][2], "groups": groups,
+                "streamed": groups > 1, "queries_per_group": group},
         "clocks": summarize_clocks(samples),
         "gpu_launches": int(launches),
     }
