@@ -1,7 +1,7 @@
 """The encrypted IVF-PQ server chain on the CPU oracle (timed CPU baseline).
 
-TEST / BASELINE INFRASTRUCTURE ONLY: bench.py's reference arm and its
-cpu_baseline leg time this; the product never runs it.
+TEST INFRASTRUCTURE ONLY: bench.py's reference arm and its cpu_baseline
+leg time this; the product never runs it.
 
 Runs exactly the operator sequence of anns_fhe_b200/query.py (the reference's
 InteractiveQueryManager chain, interactive_query_manager.cpp:85-303 with the
