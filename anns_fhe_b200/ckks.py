@@ -358,10 +358,9 @@ def centred_coefficients(limbs: np.ndarray, q, level: int) -> np.ndarray:
     """(count, level * N) residues of decrypted polynomials -> (count, N)
     float64 coefficients, centred in (-Q/2, Q/2] for Q = q_0 ... q_(level-1)."""
     if level == 1 and q[0] < 2**53:
-        # residues below 2^53 convert to float64 exactly; centre in place
-        coef = limbs.astype(np.float64)
-        coef -= float(q[0]) * (coef > float(q[0] // 2))
-        return coef
+        # centre in 64-bit integers, then convert: values below 2^53 are exact
+        s = limbs.view(np.int64)
+        return (s - (s > q[0] // 2) * np.int64(q[0])).astype(np.float64)
     return np.stack([crt_centered(row, q[:level]).astype(np.float64) for row in limbs])
 
 

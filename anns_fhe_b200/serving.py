@@ -229,8 +229,10 @@ class WorkloadBackend:
         """Stage 2 on the host: decode the coarse distances, keep the nprobe nearest lists."""
         wl = self.wl
         vals = wl.client.enc.decode_real_batch(got["coef"], got["scale"], self.iqm.coarse_slots_needed())
-        for r, c in zip(recs, self.iqm.coarse_from_slots(vals)):
-            r.probes = list(np.argsort(c, kind="stable")[:r.nprobe or wl.spec.nprobe])
+        from .workloads import nearest_lists
+        for r, pr in zip(recs, nearest_lists(self.iqm.coarse_from_slots(vals),
+                                             [r.nprobe or wl.spec.nprobe for r in recs])):
+            r.probes = pr
 
     def topk(self, recs, got: dict) -> list[list[int]]:
         """Stage 4 on the host: decode the candidate distances, rank them."""

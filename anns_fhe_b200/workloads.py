@@ -84,6 +84,16 @@ def dimpack_layout(q: np.ndarray, sh: QueryShape) -> np.ndarray:
     return np.repeat(np.asarray(q, dtype=np.float64), sh.B)
 
 
+def nearest_lists(coarse: np.ndarray, nprobes) -> list[list[int]]:
+    """Row r's first nprobes[r] entries of argsort(coarse[r], kind="stable"):
+    the lists a client probes, ties to the lower list. One stable sort of all
+    rows together."""
+    if len(coarse) == 0:
+        return []
+    order = np.argsort(coarse, axis=1, kind="stable")[:, :max(nprobes)]
+    return [row[:k].tolist() for row, k in zip(order, nprobes)]
+
+
 def ranked_prefix(vals: np.ndarray, pos, k: int) -> list[np.ndarray]:
     """For each row r: the first k entries of argsort(vals[r, pos[r]],
     kind="stable"), i.e. the k smallest values in order, ties by position.
@@ -261,8 +271,9 @@ class Workload:
         scales = np.array([iqm.out_scale_at(iqm.level_of(r)) for r in part])
         vals = dec.enc.decode_real_batch(dec.decrypt_host_batch_coef(box[:, 0], 1), scales,
                                          iqm.coarse_slots_needed())
-        for r, c in zip(part, iqm.coarse_from_slots(vals)):
-            r.probes = list(np.argsort(c, kind="stable")[:r.nprobe or self.spec.nprobe])
+        for r, pr in zip(part, nearest_lists(iqm.coarse_from_slots(vals),
+                                             [r.nprobe or self.spec.nprobe for r in part])):
+            r.probes = pr
         iqm.stage3_fine(part)
         fbox, ffence = iqm.read_results("dists", part, staged=True, tag=tag, wait=False)
         return fbox, ffence, box.nbytes

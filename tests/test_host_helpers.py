@@ -151,3 +151,16 @@ def test_pipelined_groups_schedule():
     assert tops == [[f"q{i}"] for i in range(7)]
     assert [e[0] for e in fake.log] == ["stage1"] * 3 + ["stage3"] * 3 + ["topk"] * 3
     assert [e[1] for e in fake.log[:3]] == [[0, 1, 2], [3, 4, 5], [6]]
+
+
+def test_nearest_lists_is_the_stable_argsort_prefix():
+    from anns_fhe_b200.workloads import nearest_lists
+    rng = np.random.default_rng(3)
+    for trial in range(20):
+        rows, lists = int(rng.integers(1, 40)), int(rng.integers(1, 64))
+        coarse = rng.integers(0, 5 if trial % 2 else 10**6, (rows, lists)).astype(np.float64)   # ties when small
+        nprobes = [int(rng.integers(1, lists + 1)) for _ in range(rows)]
+        got = nearest_lists(coarse, nprobes)
+        for r in range(rows):
+            assert got[r] == list(np.argsort(coarse[r], kind="stable")[:nprobes[r]])
+    assert nearest_lists(np.zeros((0, 4)), []) == []
