@@ -498,6 +498,68 @@ def profile_host(batch: int = 296, steps: int = 5):
     wl.close()
 
 
+def ref_shape(seconds: float = 10.0, cts: int = 128, reps: int = 10):
+    """Reference-shape driver: key switches per second at the reference's own
+    shape (N = 16384, 11 Q primes of which 10 in use, 4 P primes, alpha 4:
+    three digits). CPU: the reference's HLS key switch compiled from its
+    sources (oracle/_ref), one process per host core, timed first so the
+    spawned pool never sits beside a CUDA context. GPU: this repository's
+    batched key switch on the same primes, `cts` ciphertexts per launch, as
+    afhe_eval_rotate_batch by one step (the automorphism is folded into the
+    key switch's loads; c0's automorphism and add are the only extra work),
+    CUDA events on the context stream. One JSON line."""
+    import ctypes as C
+
+    import numpy as np
+
+    from anns_fhe_b200._lib import CtRef, check
+    from anns_fhe_b200.driver import CkksParams, FheContext, find_ntt_primes
+    q = find_ntt_primes(14, 60, 1)
+    q += find_ntt_primes(14, 45, 10, q)
+    p = find_ntt_primes(14, 60, 4, q)
+    from oracle.refshape import PARTS, SIZE_QL, reference_key_switch_rate
+    cpu = reference_key_switch_rate(q, p, seconds=seconds)
+
+    import torch
+    prm = CkksParams(14, q, p, 4)
+    n, sq = prm.n, SIZE_QL
+    assert prm.dnum == PARTS
+    w = sq * n
+    ctx = FheContext(prm, poly_words=4 * cts * w, key_words=prm.key_words(), max_batch=cts)
+    rng = np.random.default_rng(5)
+    allp = prm.q + prm.p
+    ctx.write_key(0, np.concatenate([rng.integers(0, x, n, dtype=np.uint64) for _ in range(2 * prm.dnum)
+                                     for x in allp]))
+    check(ctx.lib.afhe_add_rotation_key(ctx.h, 1, 0), "add_rotation_key")
+    for z in range(2 * cts):
+        ctx.write_poly(z * w, np.concatenate([rng.integers(0, x, n, dtype=np.uint64) for x in prm.q[:sq]]))
+    ins, outs = (CtRef * cts)(), (CtRef * cts)()
+    for z in range(cts):
+        ins[z].c0_offset, ins[z].c1_offset = 2 * z * w, (2 * z + 1) * w
+        outs[z].c0_offset, outs[z].c1_offset = (2 * cts + 2 * z) * w, (2 * cts + 2 * z + 1) * w
+    stream = torch.cuda.ExternalStream(ctx.lib.afhe_stream(ctx.h))
+
+    def launch():
+        check(ctx.lib.afhe_eval_rotate_batch(ctx.h, ins, outs, cts, 1, sq), "eval_rotate_batch")
+    for _ in range(3):
+        launch()
+    ctx.sync()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        launch()
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    ctx.close()
+    gpu = cts * reps / (ms / 1e3)
+    print(json.dumps({"driver": "reference shape", "unit": "key switches/s",
+                      "shape": f"N = 16384, {sq} of 11 Q limbs + 4 P limbs, {PARTS} digits of 4",
+                      "gpu": {"value": gpu, "ciphertexts_per_launch": cts, "launches": reps,
+                              "ms_per_launch": ms / reps},
+                      "cpu_reference": cpu, "gpu_over_cpu": gpu / cpu["value"]}), flush=True)
+
+
 def profile_ntt(polys: int, log_n: int = 13, reps: int = 10):
     """Profiling driver: batched in-place NTT / INTT over `polys` polynomials of
     4 limbs (the key switch's shape), forward then inverse, `reps` each."""
@@ -631,6 +693,10 @@ def main():
     ap.add_argument("--profile-step", type=int, default=0, help="profiling driver: queries per step")
     ap.add_argument("--profile-host", action="store_true",
                     help="profiling driver: end-to-end phases and the streamed run's host hotspots")
+    ap.add_argument("--ref-shape", action="store_true",
+                    help="key switches/s at the reference's own shape: its compiled HLS code on the host "
+                         "cores beside the batched GPU key switch")
+    ap.add_argument("--ref-seconds", type=float, default=10.0, help="--ref-shape: seconds per host process")
     ap.add_argument("--profile-ntt", type=int, default=0, help="profiling driver: polynomials per NTT launch")
     ap.add_argument("--profile-ks", type=int, default=0, help="profiling driver: ciphertexts per key-switch launch")
     ap.add_argument("--level", type=int, default=0, help="limbs for --profile-ks (default: all)")
@@ -648,6 +714,8 @@ def main():
         return profile_step(args.profile_step, args.workload, args.lanes)
     if args.profile_host:
         return profile_host()
+    if args.ref_shape:
+        return ref_shape(args.ref_seconds)
     if args.profile_ntt:
         return profile_ntt(args.profile_ntt, args.log_n)
     if args.profile_ks:
