@@ -31,13 +31,18 @@ def served():
     wl.close()
 
 
-def test_result_same_alone_and_in_mix(served):
+@pytest.mark.parametrize("defer_from", [None, 0], ids=["taken_at_once", "taken_next_tick"])
+def test_result_same_alone_and_in_mix(served, defer_from):
+    """defer_from=0: every tick's results reach the client during the next
+    tick, behind that tick's stage-1 launch, while their records are already
+    reused; the results are still the plain path's, word for word."""
     wl, Q, be = served
     trace = [Request(i, 0.0, i) for i in range(len(Q))]
-    loop = ServingLoop(be, max_admit=3, keep_results=True)
+    loop = ServingLoop(be, max_admit=3, keep_results=True, defer_from=defer_from)
     mix = {c.qid: c for c in loop.run(trace, realtime=False)}
     assert sorted(mix) == list(range(len(Q)))
     assert any(a and f for a, f in loop.tick_log), "no tick mixed stage 1 and stage 3"
+    assert all(loop.deferred) if defer_from == 0 else not any(loop.deferred)
     plain = be.with_lanes(1)
     for req in trace:
         alone = ServingLoop(plain, max_inflight=1, keep_results=True).run([req], realtime=False)
