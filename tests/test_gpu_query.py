@@ -96,3 +96,22 @@ def test_pipelined_host_protocol(wl):
             dec.decrypt_host_batch_coef(np.zeros((6 * max(1, wl.iqm.n_res) + 1, 2, wl.params.n), np.uint64), 1)
     finally:
         dec.close()
+
+
+def test_decryptor_at_every_level(wl):
+    """The client's own decryption context gives the client's coefficients
+    at level 1 (limb 0, the fast centring) and at the top level (CRT)."""
+    recs = wl.records[:2]
+    wl.encrypt_queries(wl.queries(2, seed=4), recs)
+    n, L = wl.params.n, wl.params.L
+    cts = np.stack([np.stack([wl.ctx.read_poly(r.ct_query[0], L * n), wl.ctx.read_poly(r.ct_query[1], L * n)])
+                    for r in recs])
+    dec = wl.client.decryptor(2, max_level=L)
+    try:
+        for lv in sorted({1, L}):
+            part = np.ascontiguousarray(cts[:, :, :lv * n])
+            assert np.array_equal(dec.decrypt_host_batch_coef(part, lv), wl.client.decrypt_host_batch_coef(part, lv))
+        with pytest.raises(ValueError):
+            dec.decrypt_host_batch_coef(cts[:, :, :n], L + 1)
+    finally:
+        dec.close()
