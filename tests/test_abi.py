@@ -101,3 +101,24 @@ def test_null_context_is_an_error(lib):
     assert lib.afhe_dispatch(None, C.byref(a)) == _lib.E_ARG
     buf = np.zeros(4, dtype=np.uint64)
     assert lib.afhe_write_poly(None, 0, buf.ctypes.data_as(_lib.P64), 4) == _lib.E_ARG
+
+
+def test_plain_c_caller_compiles_links_and_runs(lib):
+    """tests/c/abi_host_calls.c includes include/afhe.h, links libafhe.so
+    with gcc and makes the host-only calls and parameter checks from C."""
+    import os
+    import shutil
+    import subprocess
+    if shutil.which("gcc") is None:
+        pytest.skip("gcc absent")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    libdir = os.path.join(root, "anns_fhe_b200", "lib")
+    out_dir = os.path.join(root, "tests", "c", "_build")
+    os.makedirs(out_dir, exist_ok=True)
+    exe = os.path.join(out_dir, "abi_host_calls")
+    subprocess.run(["gcc", "-std=c11", "-Wall", "-Wextra", "-Werror", "-I", os.path.join(root, "include"),
+                    os.path.join(root, "tests", "c", "abi_host_calls.c"), "-L", libdir, "-lafhe",
+                    f"-Wl,-rpath,{libdir}", "-o", exe], check=True)
+    r = subprocess.run([exe], capture_output=True, text=True, timeout=60)
+    assert r.returncode == 0, (r.returncode, r.stdout, r.stderr)
+    assert r.stdout.splitlines() == ["primes ok", "root ok", "galois ok", "checks ok: bad argument"]
