@@ -11,6 +11,10 @@ if ROOT not in sys.path:
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
+    # temporary files stay inside the tree (git-ignored), not in the system's temp folder
+    if not config.option.basetemp:
+        os.makedirs(os.path.join(ROOT, "tests", "_build"), exist_ok=True)
+        config.option.basetemp = os.path.join(ROOT, "tests", "_build", "pytest-tmp")
 
 
 @pytest.fixture(scope="session")
