@@ -389,6 +389,15 @@ int afhe_ctx_create(const afhe_params* prm, afhe_ctx** out) {
         if (e != cudaSuccess) { rc = cuda_fail(ctx, e, "clear arenas"); break; }
         rc = build_native_tables(ctx);
         if (rc != AFHE_OK) break;
+        // afhe_key_switch_noalloc must allocate nothing when called; with
+        // CUDA's lazy module loading the first lookup of its static array
+        // loads (and so allocates) it, so the lookup happens here. A failure
+        // is reported by that entry point, not by context creation.
+        ctx->noalloc_err = noalloc_scratch_address(&ctx->noalloc_scr);
+        if (ctx->noalloc_err != cudaSuccess) {
+            ctx->noalloc_scr = nullptr;
+            cudaGetLastError();
+        }
         DescRing& r = ctx->ring;
         r.seg_words = 1u << 16;
         r.nseg = 32;

@@ -124,6 +124,12 @@ struct afhe_ctx {
     ulonglong2* relin_prep = nullptr;
     std::map<int32_t, afhe::RotKey> rot;
 
+    // device address of the static working array of afhe_key_switch_noalloc
+    // on this context's device, looked up when the context is created (null
+    // if the lookup failed; noalloc_err then holds the CUDA error)
+    afhe::u64* noalloc_scr = nullptr;
+    cudaError_t noalloc_err = cudaSuccess;
+
     std::string err;
 };
 

@@ -19,6 +19,10 @@ u64 host_shoup(u64 w, u64 q);
 // [off, off + count) after they were overwritten (driver.cu).
 int refresh_key_preps(afhe_ctx* ctx, u64 off, u64 count);
 void free_key_preps(afhe_ctx* ctx);
+// Device address of afhe_key_switch_noalloc's static working array on the
+// current device (noalloc.cu). Loads the array's module if lazy loading has
+// not yet done so, which is why contexts call it once at creation.
+cudaError_t noalloc_scratch_address(u64** out);
 
 #define CK(expr)                                                        \
     do {                                                                \

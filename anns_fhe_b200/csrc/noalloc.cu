@@ -6,18 +6,25 @@
 // that cannot afford the device-wide synchronisation cudaMalloc / cudaFree may
 // imply. afhe_key_switch_noalloc gives them the key switch with its working
 // memory in a fixed array compiled into this library instead of allocated
-// memory: the array below is static device memory, created when the library is
-// loaded on a device and held by every GPU that loads it until the process
-// exits, so its size is kept modest (16 MiB).
+// memory: the array below is static device memory, held by every GPU that
+// loads this library's module until the process exits, so its size is kept
+// modest (16 MiB).
+//
+// With CUDA's lazy module loading the array is created when its module is
+// first used on a device, and creating it allocates. So its address is looked
+// up when a context is created (afhe_ctx_create calls
+// noalloc_scratch_address with the context's device current), never on the
+// entry point's path: by the time a caller's pool takes the GPU's memory, a
+// context on that device already exists and the array is in place.
 //
 // The array is shared by every call on a device and keeps the previous call's
 // contents. The key switch writes every scratch word before reading it, so no
 // clearing is needed. Calls whose execution overlaps on the GPU (different
 // streams, or several contexts on one device) race on the array; the caller
-// must order them.
+// must order them. The entry point always runs the multi-kernel key switch
+// (INTT, ModUp NTT, inner product, ModDown), whatever the context's
+// AFHE_OPT_KS_FUSED setting; the residues are the same either way.
 #include <cuda_runtime.h>
-
-#include <mutex>
 
 #include "internal.h"
 #include "lanes.h"
@@ -27,30 +34,34 @@ using namespace afhe;
 namespace {
 
 constexpr size_t kNoallocScratchWords = size_t(1) << 21;   // 16 MiB of uint64_t
-constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) u64 g_noalloc_scratch[kNoallocScratchWords];
 
-// Host code must not use g_noalloc_scratch's name as an address (on the host
-// it names a shadow variable, not device memory): the device address is looked
-// up once per device with that device current, and cached.
-std::mutex g_mu;
-u64* g_dev_addr[kMaxDevices] = {};
-
-int scratch_address(afhe_ctx* ctx, u64** out) {
-    if (ctx->device < 0 || ctx->device >= kMaxDevices) return fail(ctx, AFHE_E_ARG, "device ordinal out of range");
-    std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_dev_addr[ctx->device]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGetSymbolAddress(noalloc scratch)");
-        g_dev_addr[ctx->device] = (u64*)p;
+// Restores the caller's current device when the entry point returns.
+struct DeviceGuard {
+    int prev = -1;
+    cudaError_t enter(int dev) {
+        cudaError_t e = cudaGetDevice(&prev);
+        if (e != cudaSuccess) { prev = -1; return e; }
+        return prev == dev ? cudaSuccess : cudaSetDevice(dev);
     }
-    *out = g_dev_addr[ctx->device];
-    return AFHE_OK;
-}
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
 
 }  // namespace
+
+// Host code must not use g_noalloc_scratch's name as an address (on the host
+// it names a shadow variable, not device memory): the device address comes
+// from cudaGetSymbolAddress with the device current.
+cudaError_t afhe::noalloc_scratch_address(u64** out) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    *out = e == cudaSuccess ? (u64*)p : nullptr;
+    return e;
+}
 
 extern "C" int afhe_key_switch_noalloc(afhe_ctx* ctx, uint64_t* io, uint64_t evk_offset, uint32_t limbs) {
     if (!ctx || !io) return fail(ctx, AFHE_E_ARG, "null argument");
@@ -62,11 +73,10 @@ extern "C" int afhe_key_switch_noalloc(afhe_ctx* ctx, uint64_t* io, uint64_t evk
         return fail(ctx, AFHE_E_BUDGET,
                     "afhe_key_switch_noalloc: this parameter set needs " + std::to_string(need) +
                         " scratch words, more than the fixed " + std::to_string(kNoallocScratchWords));
-    cudaError_t e = cudaSetDevice(ctx->device);
+    if (!ctx->noalloc_scr) return cuda_fail(ctx, ctx->noalloc_err, "cudaGetSymbolAddress(noalloc scratch) at context creation");
+    DeviceGuard dg;
+    cudaError_t e = dg.enter(ctx->device);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
-    u64* scratch = nullptr;
-    int rc = scratch_address(ctx, &scratch);
-    if (rc != AFHE_OK) return rc;
     const u64 w = (u64)limbs * ctx->n;
     ZBases zb{};
     zb.src = zf_const(0);        // input at io[0, w)
@@ -77,7 +87,7 @@ extern "C" int afhe_key_switch_noalloc(afhe_ctx* ctx, uint64_t* io, uint64_t evk
     const LevelJobs& lj = ctx->lvjobs[limbs];
     e = launch_key_switch(ctx->log_n, ctx->lv[limbs], ctx->jobs_qp, lj.modup, lj.n_modup, ctx->L, limbs, ctx->K,
                           ctx->key, evk_offset, evk_offset + (u64)ctx->dnum * S * ctx->n, (uint32_t)S, ctx->L, io,
-                          scratch, 1, zb, ctx->st);
+                          ctx->noalloc_scr, 1, zb, ctx->st);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "afhe_key_switch_noalloc launch");
     return AFHE_OK;
 }

@@ -154,18 +154,22 @@ class CkksParams:
 
 class PinnedStaging:
     """Reusable page-locked host buffers by name (afhe_host_alloc), grown on
-    demand; `get` returns a uint64 view valid until the next `get` of the
-    same name."""
+    demand; `get` returns a uint64 view whose contents the next `get` of the
+    same name may reuse. A buffer replaced by a larger one is not freed until
+    `close`: an asynchronous copy still in flight into it (a read enqueued
+    without waiting) keeps a valid destination, and so does a view taken
+    earlier."""
 
     def __init__(self):
         self.lib = L.load()
         self.bufs: dict[str, tuple[int, int, np.ndarray]] = {}     # name: (pointer, words, view)
+        self.retired: list[int] = []
 
     def get(self, name: str, words: int) -> np.ndarray:
         ptr, cap, view = self.bufs.get(name, (0, 0, None))
         if cap < words:
             if ptr:
-                self.lib.afhe_host_free(C.c_void_p(ptr))
+                self.retired.append(ptr)
             cap = max(words, 2 * cap)
             p = C.c_void_p()
             check(self.lib.afhe_host_alloc(cap * 8, C.byref(p)), "afhe_host_alloc")
@@ -175,10 +179,11 @@ class PinnedStaging:
         return view[:words]
 
     def close(self) -> None:
-        for ptr, _, _ in self.bufs.values():
+        for ptr in [b[0] for b in self.bufs.values()] + self.retired:
             if ptr:
                 self.lib.afhe_host_free(C.c_void_p(ptr))
         self.bufs = {}
+        self.retired = []
 
     def __del__(self):
         try:

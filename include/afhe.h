@@ -274,10 +274,14 @@ int afhe_eval_rotate(afhe_ctx* ctx, uint64_t in_c0, uint64_t in_c1, uint64_t dst
  *   evk_offset: the key in key_gmem (full-level layout, as afhe_key_switch).
  * Working memory is a fixed 16 MiB array of static device memory in this
  * library (held on every GPU that loads it until exit); parameter sets whose
- * key switch needs more return AFHE_E_BUDGET. The first call on a device looks
- * up that array's address (cudaGetSymbolAddress), so make it before any stream
- * capture. All calls on a device share the array: calls that overlap on the
- * GPU race and must be ordered by the caller. */
+ * key switch needs more return AFHE_E_BUDGET. afhe_ctx_create loads that array
+ * on the context's device and looks up its address (cudaGetSymbolAddress), so
+ * the entry point itself neither allocates nor loads anything: create the
+ * context before a pool allocator takes the GPU's memory. All calls on a
+ * device share the array: calls that overlap on the GPU race and must be
+ * ordered by the caller. It always runs the multi-kernel key switch (slower
+ * than afhe_key_switch's one-kernel path at N <= 2^13, same residues), and it
+ * leaves the caller's current device as it found it. */
 int afhe_key_switch_noalloc(afhe_ctx* ctx, uint64_t* io, uint64_t evk_offset, uint32_t limbs);
 
 /* ---- batched composite operators ------------------------------------------ */

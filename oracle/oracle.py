@@ -1,5 +1,7 @@
 """Python access to the oracle: the C restatement (liborc.so) and, where it was
-built, the reference's own HLS C-simulation (_ref/libref_hls.so).
+built, the reference's own HLS C-simulation (_ref/libref_hls.so at the
+reference's N = 16384, and _ref/libref_hls_n<N>.so for the other ring degrees
+the recipe builds from the same sources).
 
 TEST INFRASTRUCTURE ONLY. Imported by tests/, __graft_entry__.smoke() and the
 CPU-baseline legs of bench.py, as the checker; the product never imports it.
@@ -19,6 +21,12 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORC_LIB = os.path.join(HERE, "liborc.so")
 REF_LIB = os.path.join(HERE, "_ref", "libref_hls.so")
 REF_N = 16384
+
+
+def ref_lib_path(n: int = REF_N) -> str:
+    """The reference build for ring degree n: verbatim at 16384, else the
+    recipe's copy with the ring-degree literals rewritten."""
+    return REF_LIB if n == REF_N else os.path.join(HERE, "_ref", f"libref_hls_n{n}.so")
 
 P64 = C.POINTER(C.c_uint64)
 P32 = C.POINTER(C.c_uint32)
@@ -77,6 +85,49 @@ class tables_py:
         return (np.array([pw[b] for b in br], dtype=np.uint64), np.array([ipw[b] for b in br], dtype=np.uint64))
 
     @staticmethod
+    def is_prime(x: int) -> bool:
+        """Deterministic Miller-Rabin for x < 2^64."""
+        if x < 2:
+            return False
+        small = (2, 3, 5, 7, 11, 13, 17, 19, 23, 29, 31, 37)
+        for b in small:
+            if x % b == 0:
+                return x == b
+        d, r = x - 1, 0
+        while d % 2 == 0:
+            d //= 2
+            r += 1
+        for b in small:
+            y = pow(b, d, x)
+            if y in (1, x - 1):
+                continue
+            for _ in range(r - 1):
+                y = y * y % x
+                if y == x - 1:
+                    break
+            else:
+                return False
+        return True
+
+    @staticmethod
+    def ntt_primes(log_n: int, bits: int, count: int, exclude=()) -> list[int]:
+        """The `count` largest primes below 2^bits that are 1 mod 2N, skipping
+        `exclude`: the deterministic search the product's tables use
+        (largest candidate first, step 2N)."""
+        m = 2 << log_n
+        c = ((1 << bits) - 1) // m * m + 1
+        if c >= 1 << bits:
+            c -= m
+        out = []
+        while len(out) < count:
+            if c <= m:
+                raise ValueError("ran out of NTT-friendly primes")
+            if c not in exclude and tables_py.is_prime(c):
+                out.append(c)
+            c -= m
+        return out
+
+    @staticmethod
     def barrett(q: int):
         k = 2 * q.bit_length() + 3
         m = (1 << k) // q
@@ -128,11 +179,12 @@ class tables_py:
         """Evaluation-form permutation: slot i holds a(psi^(2 bitrev(i) + 1))."""
         n = 1 << log_n
         m = 2 * n
-        out = np.zeros(n, dtype=np.uint32)
-        for i in range(n):
-            e = k * (2 * tables_py.bitrev(i, log_n) + 1) % m
-            out[i] = tables_py.bitrev((e - 1) // 2, log_n)
-        return out
+        idx = np.arange(n, dtype=np.int64)
+        br = np.zeros(n, dtype=np.int64)
+        for b in range(log_n):
+            br |= ((idx >> b) & 1) << (log_n - 1 - b)
+        e = (int(k) * (2 * br + 1)) % m
+        return br[(e - 1) // 2].astype(np.uint32)
 
 
 # ---------------------------------------------------------------------------
@@ -273,12 +325,15 @@ class RefTopArgs(C.Structure):
 
 
 class Ref:
-    """_ref/libref_hls.so: the reference's HLS functions, N = 16384 only."""
+    """The reference's HLS functions at ring degree n (16384: the verbatim
+    build; 8192 / 32768: the recipe's builds of the same sources)."""
 
-    def __init__(self):
-        if not os.path.exists(REF_LIB):
-            raise FileNotFoundError(REF_LIB)
-        lib = C.CDLL(REF_LIB)
+    def __init__(self, n: int = REF_N):
+        path = ref_lib_path(n)
+        if not os.path.exists(path):
+            raise FileNotFoundError(path)
+        lib = C.CDLL(path)
+        self.n = n
         sig = {
             "ref_mod_mul": (u64, [u64, u64, u64, u64, u64, u32]),
             "ref_ntt_forward": (None, [P64, P64, u64, u64, u64, u32]),
@@ -292,15 +347,23 @@ class Ref:
                                       P32, P64, P64, P32, P64, P64, P64, P64, P64, P64, P64, P64, P64, P64, P64,
                                       P64, P64, P64, P64]),
             "ref_fhe_accel_top": (None, [P64, u64, P64, u64, C.POINTER(RefTopArgs)]),
+            "ref_ring_degree": (u32, []),
+            "ref_bus_new": (C.c_void_p, [u64, u64]),
+            "ref_bus_free": (None, [C.c_void_p]),
+            "ref_bus_write_poly": (None, [C.c_void_p, u64, P64, u64]),
+            "ref_bus_read_poly": (None, [C.c_void_p, u64, P64, u64]),
+            "ref_bus_write_key": (None, [C.c_void_p, u64, P64, u64]),
+            "ref_bus_accel_top": (None, [C.c_void_p, C.POINTER(RefTopArgs)]),
         }
         for k, (r, a) in sig.items():
             f = getattr(lib, k)
             f.restype, f.argtypes = r, a
         self.lib = lib
+        assert lib.ref_ring_degree() == n, "reference build has another ring degree"
 
     @staticmethod
-    def available() -> bool:
-        return os.path.exists(REF_LIB)
+    def available(n: int = REF_N) -> bool:
+        return os.path.exists(ref_lib_path(n))
 
     def mod_mul(self, a, b, q):
         lo, hi, k = tables_py.barrett(q)
@@ -315,7 +378,7 @@ class Ref:
     def intt(self, a, itw, q):
         x = _u(a).copy()
         lo, hi, k = tables_py.barrett(q)
-        self.lib.ref_intt_inverse(_p(x), _p(_u(itw)), pow(REF_N, -1, q), q, lo, hi, k)
+        self.lib.ref_intt_inverse(_p(x), _p(_u(itw)), pow(self.n, -1, q), q, lo, hi, k)
         return x
 
     def poly(self, op, a, b, q):
@@ -341,7 +404,7 @@ class Ref:
 
     def rescale(self, a, q, itw_last, tw, qlql, qlinv):
         a = _u(a)
-        n = REF_N
+        n = self.n
         L = a.size // n
         o = np.zeros((L - 1) * n, dtype=np.uint64)
         q = _u(q[:L])
@@ -352,7 +415,7 @@ class Ref:
 
     def key_switch(self, c_in, key_words, evk_a_off, evk_b_off, sizeQl, sizeP, parts, alpha, q, p, tw_q, itw_q,
                    tw_p, itw_p, qhat_inv, qhat_modp, pinv, phinv, phq):
-        n = REF_N
+        n = self.n
         assert parts == 3, "the reference kernel takes exactly three digit tables"
         o0 = np.zeros(sizeQl * n, dtype=np.uint64)
         o1 = np.zeros(sizeQl * n, dtype=np.uint64)
@@ -373,6 +436,10 @@ class Ref:
 
     def accel_top(self, poly: np.ndarray, key: np.ndarray, args) -> None:
         """One fhe_accel_top call; `args` is afhe_accel_args-shaped (offsets < 2^32)."""
+        self.lib.ref_fhe_accel_top(_p(poly), poly.size, _p(key), key.size, C.byref(self.top_args(args)))
+
+    @staticmethod
+    def top_args(args) -> RefTopArgs:
         r = RefTopArgs()
         for f in ("op_code", "src_a_offset", "src_b_offset", "dst_offset", "evk_offset", "active_limbs",
                   "prime_idx", "galois_elt", "sizeQl", "sizeP", "numPartQ", "alpha", "n_inv_mod_q_last"):
@@ -394,4 +461,35 @@ class Ref:
                 args.p_hat_mod_q_offset, args.qlql_offset, args.qlinv_offset]
         for i, v in enumerate(offs):
             r.table_offsets[i] = v
-        self.lib.ref_fhe_accel_top(_p(poly), poly.size, _p(key), key.size, C.byref(r))
+        return r
+
+
+class RefBus:
+    """The reference's SimMemoryBus (cpp_host_model/src/sim_memory_bus.h:10-34)
+    held across fhe_accel_top calls, as FHEHostDriver::dispatch drives it
+    (fhe_host_driver.cpp:177-204): arenas stay resident between operators."""
+
+    def __init__(self, ref: Ref, poly_words: int, key_words: int):
+        self.ref, self.lib = ref, ref.lib
+        self.h = self.lib.ref_bus_new(poly_words, key_words)
+
+    def write_poly(self, off: int, x) -> None:
+        x = _u(x)
+        self.lib.ref_bus_write_poly(self.h, off, _p(x), x.size)
+
+    def read_poly(self, off: int, count: int) -> np.ndarray:
+        o = np.empty(count, dtype=np.uint64)
+        self.lib.ref_bus_read_poly(self.h, off, _p(o), count)
+        return o
+
+    def write_key(self, off: int, x) -> None:
+        x = _u(x)
+        self.lib.ref_bus_write_key(self.h, off, _p(x), x.size)
+
+    def top(self, r: RefTopArgs) -> None:
+        self.lib.ref_bus_accel_top(self.h, C.byref(r))
+
+    def close(self) -> None:
+        if self.h:
+            self.lib.ref_bus_free(self.h)
+            self.h = None

@@ -17,6 +17,11 @@
 //   approx_mod_down         hardware_fpga_model/hls/src/key_switch.cpp:62
 //   key_switch              hardware_fpga_model/hls/src/key_switch.cpp:167
 //   fhe_accel_top           hardware_fpga_model/hls/src/fhe_accel_top.cpp:90
+//   SimMemoryBus            cpp_host_model/src/sim_memory_bus.h:10-34
+//
+// The same shim is built against the verbatim sources (N = 16384) and against
+// copies whose ring-degree literals the recipe rewrites (N = 8192, 32768); it
+// takes the ring degree from the sources' own hls_params.h.
 #include <cstdint>
 #include <cstring>
 #include <vector>
@@ -28,6 +33,7 @@
 #include "rescale.h"
 #include "key_switch.h"
 #include "fhe_accel_top.h"
+#include "sim_memory_bus.h"
 
 static inline ap_uint<128> mk128(uint64_t lo, uint64_t hi) {
     return (ap_uint<128>(hi) << 64) | ap_uint<128>(lo);
@@ -63,7 +69,7 @@ struct ref_top_args {
 
 extern "C" {
 
-uint32_t ref_ring_degree(void) { return 16384; }
+uint32_t ref_ring_degree(void) { return (uint32_t)N; }
 
 uint64_t ref_mod_add(uint64_t a, uint64_t b, uint64_t q) { return mod_add(a, b, q); }
 uint64_t ref_mod_sub(uint64_t a, uint64_t b, uint64_t q) { return mod_sub(a, b, q); }
@@ -106,7 +112,7 @@ void ref_fast_bases_conv(const uint64_t* in, uint64_t* out, uint32_t n_in, uint3
     std::vector<ap_uint<128>> mi(n_in), mo(n_out);
     for (uint32_t i = 0; i < n_in; ++i) mi[i] = mk128(m_in_lo[i], m_in_hi[i]);
     for (uint32_t i = 0; i < n_out; ++i) mo[i] = mk128(m_out_lo[i], m_out_hi[i]);
-    std::vector<uint64_t> buf((size_t)n_in * 16384);
+    std::vector<uint64_t> buf((size_t)n_in * N);
     fast_bases_conv(in, out, n_in, n_out, in_primes, out_primes, qhat_inv, qhat_modp,
                     mi.data(), k_in, mo.data(), k_out, buf.data());
 }
@@ -121,7 +127,7 @@ void ref_approx_mod_down(const uint64_t* in, uint64_t* out, uint32_t nq, uint32_
     std::vector<ap_uint<128>> mp(np), mq(nq);
     for (uint32_t i = 0; i < np; ++i) mp[i] = mk128(mp_lo[i], mp_hi[i]);
     for (uint32_t i = 0; i < nq; ++i) mq[i] = mk128(mq_lo[i], mq_hi[i]);
-    std::vector<uint64_t> buf_p((size_t)np * 16384), part((size_t)nq * 16384), xq((size_t)np * 16384);
+    std::vector<uint64_t> buf_p((size_t)np * N), part((size_t)nq * N), xq((size_t)np * N);
     approx_mod_down(in, out, nq, np, q, p, p_inv_mod_q, p_hat_inv_mod_p, p_hat_mod_q, inv_tw_p, tw_q,
                     mp.data(), kp, mq.data(), kq, n_inv_p, buf_p.data(), part.data(), xq.data());
 }
@@ -143,7 +149,7 @@ void ref_key_switch(const uint64_t* c_in, const uint64_t* key_words, uint64_t n_
     for (uint32_t i = 0; i < sizeP; ++i) mp[i] = mk128(mp_lo[i], mp_hi[i]);
     std::vector<ap_uint<512>> beats;
     pack_beats(key_words, n_key_words, beats);
-    const size_t W = (size_t)15 * 16384;
+    const size_t W = (size_t)MAX_LIMBS * N;
     std::vector<uint64_t> ext0(W), ext1(W), parts(W), compl_(W), digit(W);
     key_switch(c_in, beats.data(), evk_a_offset, evk_b_offset, out0, out1, sizeQl, sizeP, numPartQ, alpha,
                q, p, mq.data(), kq, mp.data(), kp, tw_q, itw_q, tw_p, itw_p, n_inv_q, n_inv_p,
@@ -151,13 +157,7 @@ void ref_key_switch(const uint64_t* c_in, const uint64_t* key_words, uint64_t n_
                ext0.data(), ext1.data(), parts.data(), compl_.data(), digit.data());
 }
 
-// One fhe_accel_top call over word arenas. The arenas are packed into 512-bit
-// beats, the kernel runs, and both arenas are unpacked back in place.
-void ref_fhe_accel_top(uint64_t* poly_words, uint64_t n_poly_words, uint64_t* key_words, uint64_t n_key_words,
-                       const ref_top_args* a) {
-    std::vector<ap_uint<512>> pg, kg;
-    pack_beats(poly_words, n_poly_words, pg);
-    pack_beats(key_words, n_key_words, kg);
+static void call_top(ap_uint<512>* pg, ap_uint<512>* kg, const ref_top_args* a) {
     uint64_t rns[15], pp[4], nq[15], np[4];
     ap_uint<128> mq[15], mp[4];
     uint32_t kq[15], kp[4];
@@ -170,11 +170,41 @@ void ref_fhe_accel_top(uint64_t* poly_words, uint64_t n_poly_words, uint64_t* ke
         mp[i] = mk128(a->barrett_m_p_lo[i], a->barrett_m_p_hi[i]);
     }
     const uint32_t* o = a->table_offsets;
-    fhe_accel_top(pg.data(), kg.data(), a->op_code, a->src_a_offset, a->src_b_offset, a->dst_offset,
+    fhe_accel_top(pg, kg, a->op_code, a->src_a_offset, a->src_b_offset, a->dst_offset,
                   a->evk_offset, a->active_limbs, a->prime_idx, a->galois_elt,
                   a->sizeQl, a->sizeP, a->numPartQ, a->alpha,
                   rns, pp, mq, kq, mp, kp, nq, np, a->n_inv_mod_q_last,
                   o[0], o[1], o[2], o[3], o[4], o[5], o[6], o[7], o[8], o[9], o[10], o[11], o[12], o[13], o[14]);
+}
+
+// The reference's own memory bus (cpp_host_model/src/sim_memory_bus.h:10-34)
+// held across calls, so that a sequence of fhe_accel_top calls runs on
+// resident arenas the way FHEHostDriver::dispatch (fhe_host_driver.cpp:177-204)
+// drives them.
+void* ref_bus_new(uint64_t poly_words, uint64_t key_words) { return new SimMemoryBus(poly_words, key_words); }
+void ref_bus_free(void* bus) { delete static_cast<SimMemoryBus*>(bus); }
+void ref_bus_write_poly(void* bus, uint64_t off, const uint64_t* src, uint64_t count) {
+    static_cast<SimMemoryBus*>(bus)->write_poly((uint32_t)off, src, count);
+}
+void ref_bus_read_poly(void* bus, uint64_t off, uint64_t* dst, uint64_t count) {
+    static_cast<SimMemoryBus*>(bus)->read_poly((uint32_t)off, dst, count);
+}
+void ref_bus_write_key(void* bus, uint64_t off, const uint64_t* src, uint64_t count) {
+    static_cast<SimMemoryBus*>(bus)->write_key(off, src, count);
+}
+void ref_bus_accel_top(void* bus, const ref_top_args* a) {
+    SimMemoryBus* b = static_cast<SimMemoryBus*>(bus);
+    call_top(b->poly_gmem_ptr(), b->key_gmem_ptr(), a);
+}
+
+// One fhe_accel_top call over word arenas. The arenas are packed into 512-bit
+// beats, the kernel runs, and both arenas are unpacked back in place.
+void ref_fhe_accel_top(uint64_t* poly_words, uint64_t n_poly_words, uint64_t* key_words, uint64_t n_key_words,
+                       const ref_top_args* a) {
+    std::vector<ap_uint<512>> pg, kg;
+    pack_beats(poly_words, n_poly_words, pg);
+    pack_beats(key_words, n_key_words, kg);
+    call_top(pg.data(), kg.data(), a);
     unpack_beats(pg, poly_words, n_poly_words);
     unpack_beats(kg, key_words, n_key_words);
 }

@@ -48,7 +48,15 @@ def reference_chain(wl, ora, ct, ct_dim, probes, level=None):
         k = wl.ctx.read_key(off, kw)
         return k[:half], k[half:]
     relin = key(0)
-    rot = {s: key(kw * (1 + i)) for i, s in enumerate(sorted(wl.steps))}
+    where = {s: kw * (1 + i) for i, s in enumerate(sorted(wl.steps))}
+
+    class Keys(dict):
+        """Rotation keys read back from the device when first used (a
+        configuration may hold more than a hundred keys of 25 MB)."""
+        def __missing__(self, step):
+            self[step] = key(where[step])
+            return self[step]
+    rot = Keys()
 
     def pt(off, limbs):
         return wl.ctx.read_poly(off, limbs * n)
@@ -169,3 +177,29 @@ def test_eval_level_matches_oracle_replay(orc):
 
 def test_chain_matches_reference_bench_configuration(orc):
     run_and_compare(SMALL, nq=1, lanes=8, orc=orc)
+
+
+# The large IVF-PQ configuration's CKKS parameters and query shape (N = 2^15,
+# 12 x 50-bit Q + 4 x 60-bit P, alpha 4, d = 128, so B = 128 and 128
+# centroids per coarse ciphertext; packed compaction; placement by one key
+# per step) over a database small enough for the oracle to replay one query:
+# 256 lists in 2 coarse ciphertexts, 2 probed lists.
+CFG4_PARAMS = WorkloadSpec("ivfpq_2048x128_nlist256_N32768_L12", n_vectors=2048, d=128, components=256, sigma=0.15,
+                           n_list=256, M=16, K=256, nprobe=2, top_k=8, log_n=15, num_q=12, q_bits=50, num_p=4,
+                           p_bits=60, alpha=4, log_scale=40, compaction="packed", init="farthest")
+
+
+def test_large_configuration_parameters_at_eval_level(orc):
+    """One query at 12 limbs, evaluated at 3 (what the large configuration's
+    bench runs): every key switch on 3 + 4 limbs, one digit."""
+    import dataclasses
+    spec = dataclasses.replace(CFG4_PARAMS, name=CFG4_PARAMS.name + "_eval3", eval_level=3)
+    iqm, _ = run_and_compare(spec, nq=1, lanes=4, orc=orc)
+    assert iqm.levels == [3] and iqm.sh.n_coarse == 2
+
+
+def test_large_configuration_parameters_at_full_level(orc):
+    """One query evaluated at its own 12 limbs: key switches at 12 and 11
+    limbs (3 digits of 4 limbs, the last one 4 or 3), rescales to 10."""
+    iqm, _ = run_and_compare(CFG4_PARAMS, nq=1, lanes=4, orc=orc)
+    assert iqm.levels == [12] and iqm.sh.n_coarse == 2

@@ -16,8 +16,14 @@ SHAPES = {
     "n16384_a2": (14, 6, 50, 2, 60, 2),
     "n65536_a3": (16, 5, 50, 3, 60, 3),
     "n1024_a4": (10, 7, 40, 2, 45, 4),
+    # the large IVF-PQ configuration's exact parameter set: N = 2^15,
+    # 12 x 50-bit Q + 4 x 60-bit P, alpha 4 (dnum 3)
+    "cfg4_n32768": (15, 12, 50, 4, 60, 4),
 }
 STEPS = (1, 2, 4, -1, -2)
+# levels at which every key-switching operator is checked: the top level, a
+# middle one and the lowest the depth-2 query chain runs at
+LEVELS = {"cfg4_n32768": (12, 6, 3)}
 
 
 class Setup:
@@ -65,6 +71,7 @@ class Setup:
 @pytest.fixture(scope="module", params=list(SHAPES))
 def su(request, orc):
     s = Setup(request.param, orc)
+    s.name = request.param
     yield s
     s.ctx.close()
 
@@ -201,3 +208,28 @@ def test_batched_equals_single(su):
         e0, e1 = su.ora.eval_rotate(c, 3, su.rot, lvl)
         assert np.array_equal(su.get(8 + 2 * i, lvl), e0)
         assert np.array_equal(su.get(9 + 2 * i, lvl), e1)
+
+
+def test_key_switching_operators_at_levels(su):
+    """Key switch, eval_mult_relin_rescale and eval_rotate (single steps and
+    multi-step totals) at a high, a middle and a low level, each against the
+    oracle (for the large configuration's parameters: levels 12, 6 and 3,
+    where the last digit holds 4, 2 and 3 limbs)."""
+    levels = LEVELS.get(su.name, tuple(sorted({su.L, max(2, su.L // 2), 2}, reverse=True)))
+    a, b = su.keys[0]
+    for lvl in levels:
+        x = su.ct(lvl)[0]
+        su.put(0, x)
+        su.drv.key_switch(su.slot(0), 0, su.slot(1), su.slot(2), lvl)
+        e0, e1 = su.ora.key_switch(x, a, b, lvl)
+        assert np.array_equal(su.get(1, lvl), e0) and np.array_equal(su.get(2, lvl), e1), ("ks", lvl)
+        A, B = su.ct(lvl), su.ct(lvl)
+        for i, v in enumerate(A + B):
+            su.put(i, v)
+        su.drv.eval_mult_relin_rescale(su.slot(0), su.slot(1), su.slot(2), su.slot(3), su.slot(4), su.slot(5), lvl)
+        e0, e1 = su.ora.eval_mult_relin_rescale(A, B, su.keys[0], lvl)
+        assert np.array_equal(su.get(4, lvl - 1), e0) and np.array_equal(su.get(5, lvl - 1), e1), ("relin", lvl)
+        for total in (1, -2, 7):
+            su.drv.eval_rotate(su.slot(0), su.slot(1), su.slot(6), su.slot(7), total, lvl)
+            e0, e1 = su.ora.eval_rotate(A, total, su.rot, lvl)
+            assert np.array_equal(su.get(6, lvl), e0) and np.array_equal(su.get(7, lvl), e1), ("rot", lvl, total)

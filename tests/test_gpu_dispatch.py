@@ -17,6 +17,9 @@ SHAPES = {
     "cfg1_n8192": (13, 3, 50, 1, 60, None, 1, 3),
     "n1024": (10, 4, 30, 2, 31, None, 2, 4),
     "n65536": (16, 5, 50, 2, 60, None, 2, 5),
+    # the large IVF-PQ configuration's parameter set: N = 2^15, 12 x 50-bit Q
+    # + 4 x 60-bit P, alpha 4, tables and key switch at all 12 limbs (dnum 3)
+    "cfg4_n32768": (15, 12, 50, 4, 60, None, 4, 12),
 }
 
 

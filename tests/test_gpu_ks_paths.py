@@ -21,8 +21,16 @@ SHAPES = {
     "n4096_a2": (12, 5, 45, 2, 50, 2),
     "n2048_a3": (11, 7, 40, 3, 45, 3),
     "n1024_a1k2": (10, 4, 40, 2, 45, 1),
+    # the large IVF-PQ configuration's parameter set (N = 2^15, 12 + 4 limbs,
+    # alpha 4), checked at levels 12, 6 and 3 only
+    "cfg4_n32768": (15, 12, 50, 4, 60, 4),
 }
 STEPS = (1, 2, -1, -2, 4)
+LEVELS = {"cfg4_n32768": (12, 6, 3)}
+
+
+def levels_of(pr):
+    return LEVELS.get(pr.name, tuple(range(pr.L, 0, -1)))
 
 
 def make_ctx(prm, fused, poly_words, key_words):
@@ -79,6 +87,7 @@ class Pair:
 @pytest.fixture(scope="module", params=list(SHAPES))
 def pr(request, orc):
     p = Pair(request.param, orc)
+    p.name = request.param
     yield p
     for ctx, _ in p.ctxs:
         ctx.close()
@@ -91,7 +100,7 @@ def both(pr, fn):
 
 def test_key_switch_every_level(pr):
     a, b = pr.keys[0]
-    for lvl in range(pr.L, 0, -1):
+    for lvl in levels_of(pr):
         x = pr.ct(lvl)[0]
         e0, e1 = pr.ora.key_switch(x, a, b, lvl)
 
@@ -120,7 +129,7 @@ def test_mult_relin_rescale(pr):
 
 @pytest.mark.parametrize("total", [1, -1, 3, 7, -3])
 def test_rotate_every_level(pr, total):
-    for lvl in range(pr.L, 0, -1):
+    for lvl in levels_of(pr):
         A = pr.ct(lvl)
         e0, e1 = pr.ora.eval_rotate(A, total, pr.rot, lvl)
 

@@ -229,3 +229,125 @@ def test_key_switch_vs_reference_partial_digits(ref, orc, sq):
                             img.pinv, img.phinv, img.phq, n)
     assert np.array_equal(r0, o0)
     assert np.array_equal(r1, o1)
+
+
+# ---------------------------------------------------------------------------
+# the reference's sources built at other ring degrees (oracle/Makefile rewrites
+# their N = 16384 literals): each build against the C restatement, which the
+# tests above pin to the verbatim build
+# ---------------------------------------------------------------------------
+@pytest.mark.parametrize("log_n,nq,qb,np_,pb,alpha", [(13, 3, 50, 1, 60, 1), (15, 9, 50, 4, 60, 4)],
+                         ids=["n8192_3q1p_a1", "n32768_9q4p_a4"])
+def test_reference_at_other_ring_degrees(orc, log_n, nq, qb, np_, pb, alpha):
+    """Every op code through the rebuilt reference's fhe_accel_top, once over
+    word arenas and once over its own SimMemoryBus held across the calls,
+    equals the restatement: the small configuration's shape (N = 8192, 3 + 1
+    limbs, alpha 1) and, at the large configuration's ring (N = 32768) and
+    primes' sizes, 9 + 4 limbs with alpha 4. The reference's OP 99 loads
+    tables for exactly three digits (fhe_accel_top.cpp:204-207 sizes the last
+    one as active_limbs - 2 alpha), so its table load needs 2 alpha <
+    active_limbs; 9 limbs give digits of 4, 4 and 1."""
+    from anns_fhe_b200 import _lib as L
+    from oracle.oracle import Ref, RefBus, build_oracle
+    n = 1 << log_n
+    if not Ref.available(n):
+        try:
+            build_oracle(ref=True)
+        except Exception:
+            pass
+    if not Ref.available(n):
+        pytest.skip(f"reference build for N = {n} absent (reference tree absent)")
+    ref = Ref(n)
+    q, p = primes_for(log_n, nq, qb, np_, pb)
+    img = AccelImage(log_n, q, p, alpha=alpha, table_level=nq)
+    PW = (nq + np_) * n
+    poly = np.zeros(6 * PW, dtype=np.uint64)
+    rng = np.random.default_rng(log_n)
+    poly[:nq * n] = uniform_residues(rng, q, n)
+    poly[PW:PW + nq * n] = uniform_residues(rng, q, n)
+    m = T.auto_map(log_n, T.galois(log_n, 3)).astype(np.uint64)
+    poly[5 * PW:5 * PW + n // 2] = m[0::2] | (m[1::2] << np.uint64(32))
+    key = img.key.copy()
+    rp, rk = poly.copy(), key.copy()
+    bus = RefBus(ref, poly.size, key.size)
+    bus.write_poly(0, poly)
+    bus.write_key(0, key)
+    ctx = orc.new_ctx(n)
+    try:
+        for op, limbs, kw in [
+            (L.OP_LOAD_CONTEXT, nq, {}),
+            (L.OP_NTT, nq, dict(src_a_offset=0, dst_offset=2 * PW)),
+            (L.OP_INTT, nq, dict(src_a_offset=2 * PW, dst_offset=3 * PW)),
+            (L.OP_POLY_ADD, nq, dict(src_a_offset=0, src_b_offset=PW, dst_offset=2 * PW)),
+            (L.OP_POLY_SUB, nq, dict(src_a_offset=0, src_b_offset=PW, dst_offset=2 * PW)),
+            (L.OP_POLY_MUL_NTT, nq, dict(src_a_offset=0, src_b_offset=PW, dst_offset=2 * PW)),
+            (L.OP_AUTOMORPHISM, nq, dict(src_a_offset=0, src_b_offset=5 * PW, dst_offset=3 * PW)),
+            (L.OP_RESCALE, nq, dict(src_a_offset=0, src_b_offset=PW, dst_offset=3 * PW)),
+            (L.OP_KEY_SWITCH, nq, dict(src_a_offset=PW, dst_offset=2 * PW)),
+        ]:
+            a = img.args(op, limbs, **kw)
+            assert orc.accel_top(ctx, poly, key, a) == 0
+            ref.accel_top(rp, rk, a)
+            bus.top(Ref.top_args(a))
+            assert np.array_equal(poly, rp), f"op {op}"
+            assert np.array_equal(bus.read_poly(0, poly.size), poly), f"op {op} (bus)"
+    finally:
+        orc.free_ctx(ctx)
+        bus.close()
+
+
+def test_reference_host_sequence_matches_composites(orc):
+    """The timed CPU baseline (oracle/refchain.py) drives the reference's
+    fhe_accel_top in FHEHostDriver's operator sequence. At the level its
+    tables are loaded for, eval_mult_relin_rescale, eval_rotate and
+    eval_sub_plain / eval_add there equal the oracle's composites, so the
+    sequence it times is the reference's chain (small configuration's shape:
+    N = 8192, 3 + 1 limbs, alpha 1)."""
+    from oracle.composite import OracleCKKS
+    from oracle.oracle import Ref, build_oracle
+    from oracle.refchain import HostDriver, RefBusBackend
+    log_n, n, L, alpha = 13, 8192, 3, 1
+    if not Ref.available(n):
+        try:
+            build_oracle(ref=True)
+        except Exception:
+            pass
+    if not Ref.available(n):
+        pytest.skip("reference build for N = 8192 absent (reference tree absent)")
+    q = T.ntt_primes(log_n, 50, L)
+    p = T.ntt_primes(log_n, 60, 1, q)
+    ora = OracleCKKS(log_n, q, p, alpha, orc)
+    t = ora.tables(L)
+    rng = np.random.default_rng(33)
+    allp = q + p
+    ka = np.concatenate([uniform_residues(rng, allp, n) for _ in range(ora.dnum)])
+    kb = np.concatenate([uniform_residues(rng, allp, n) for _ in range(ora.dnum)])
+    tables = dict(tw=np.concatenate(ora.tw), itw=np.concatenate(ora.itw), qhat_inv=t["qhat_inv"],
+                  qhat_modp=t["qhat_modp"], pinv=t["pinv"], phinv=t["phinv"], phq=t["phq"], qlql=t["qlql"],
+                  qlinv=t["qlinv"], key=np.concatenate([ka, kb]))
+    W = 8 * n
+    steps = [1, 2, 4]
+    bus = RefBusBackend(n, 20 * W, 2 * len(allp) * n + 2048 + 2 * ora.dnum * (L + 1) * n)
+    try:
+        drv = HostDriver(bus, log_n, q, p, alpha, L, 1, steps, W, 10 * W, 16 * W, 2 * len(allp) * n + 2048,
+                         tables=tables)
+        A = (uniform_residues(rng, q, n), uniform_residues(rng, q, n))
+        pt = uniform_residues(rng, q, n)
+        for i, v in enumerate(A + (pt,)):
+            bus.write_poly(i * W, v)
+        drv.eval_mult_relin_rescale(0, W, 0, W, 3 * W, 4 * W, L)
+        e0, e1 = ora.eval_mult_relin_rescale(A, A, (ka, kb), L)
+        assert np.array_equal(bus.read_poly(3 * W, (L - 1) * n), e0)
+        assert np.array_equal(bus.read_poly(4 * W, (L - 1) * n), e1)
+        rot = {s: (ka, kb) for s in steps}
+        drv.eval_rotate(0, W, 5 * W, 6 * W, 7, L)
+        e0, e1 = ora.eval_rotate(A, 7, rot, L)
+        assert np.array_equal(bus.read_poly(5 * W, L * n), e0)
+        assert np.array_equal(bus.read_poly(6 * W, L * n), e1)
+        drv.eval_sub_plain(0, W, 2 * W, 7 * W, 8 * W, L)
+        drv.eval_add(7 * W, 8 * W, 5 * W, 6 * W, 7 * W, 8 * W, L)
+        e0, e1 = ora.eval_add(ora.eval_sub_plain(A, pt, L), (e0, e1), L)
+        assert np.array_equal(bus.read_poly(7 * W, L * n), e0)
+        assert np.array_equal(bus.read_poly(8 * W, L * n), e1)
+    finally:
+        bus.close()
