@@ -63,6 +63,10 @@ def chunk_candidates(lanes: int, sms: int) -> list[int]:
 
 
 TIE = 0.10   # candidates within this fraction of the fastest count as ties
+# Version of the key-switch kernels a cache was tuned against: a cache from
+# other kernels (e.g. before the one-kernel path existed at this ring degree)
+# is tuned again.
+KERNELS = 2
 
 
 def pick(timings: dict) -> tuple:
@@ -111,7 +115,7 @@ def tune(params: CkksParams, levels, lanes: int, device: int = 0, verbose: bool 
         for i in range(2 * count):
             ctx.write_poly(i * w_max, np.concatenate([rng.integers(0, q, n, dtype=np.uint64)
                                                       for q in params.q[:max(levels)]]))
-        fused_ok = params.log_n <= 13
+        fused_ok = ctx.get_option(L.OPT_KS_FUSED) == 1    # the context enables it where the GPU can run it
         out = {}
         for lv in sorted(set(levels)):
             timings = {}
@@ -133,7 +137,7 @@ def save(path: str, params: CkksParams, choices: dict, lanes: int) -> None:
     os.makedirs(os.path.dirname(path), exist_ok=True)
     with open(path, "w") as f:
         json.dump({"gpu": gpu_name(), "log_n": params.log_n, "L": params.L, "K": params.K,
-                   "alpha": params.alpha, "lanes": lanes,
+                   "alpha": params.alpha, "lanes": lanes, "kernels": KERNELS,
                    "levels": {str(k): asdict(v) for k, v in sorted(choices.items())}}, f, indent=1)
 
 
@@ -143,7 +147,7 @@ def load(path: str, lanes: int) -> dict | None:
         return None
     with open(path) as f:
         d = json.load(f)
-    if d.get("lanes") != lanes:
+    if d.get("lanes") != lanes or d.get("kernels") != KERNELS:
         return None
     return {int(k): KsChoice(**v) for k, v in d["levels"].items()}
 

@@ -1,7 +1,10 @@
-"""Build the CUDA C-ABI library ``anns_fhe_b200/lib/libafhe.so`` for sm_100a.
+"""Build the CUDA C-ABI library ``anns_fhe_b200/lib/libafhe.so`` for sm_100a,
+and ``lib/libafhe_accel_top.so``, the reference's ``fhe_accel_top`` symbol over
+it (csrc/fhe_accel_top_shim.cpp), which a host built against the reference's
+kernel ABI links in place of the HLS kernel object.
 
 Plain ``nvcc -shared`` over the sources in ``csrc/``; no torch extension, no
-JIT cache: the library is built in-tree so it travels with the working tree.
+JIT cache: the libraries are built in-tree so they travel with the working tree.
 
     python -m anns_fhe_b200.build [--force] [--ptxas-verbose]
 """
@@ -17,6 +20,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libafhe.so")
+SHIM = os.path.join(LIBDIR, "libafhe_accel_top.so")
+SHIM_SRC = os.path.join(CSRC, "fhe_accel_top_shim.cpp")
 ROOT = os.path.dirname(HERE)
 INCLUDE = os.path.join(ROOT, "include")
 
@@ -41,9 +46,26 @@ def _stale() -> bool:
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
+def build_shim(force: bool = False) -> str:
+    """Compile libafhe_accel_top.so (host C++ only, linked to libafhe.so)."""
+    if not force and os.path.exists(SHIM) and os.path.getmtime(SHIM) >= max(
+            os.path.getmtime(SHIM_SRC), os.path.getmtime(LIB), os.path.getmtime(os.path.join(INCLUDE, "afhe.h"))):
+        return SHIM
+    cxx = shutil.which("g++") or "g++"
+    cmd = [cxx, "-O2", "-std=c++17", "-fPIC", "-shared", "-Wall", "-I", INCLUDE, "-o", SHIM + ".tmp", SHIM_SRC,
+           "-L", LIBDIR, "-lafhe", "-Wl,-rpath,$ORIGIN"]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError("g++ failed:\n" + res.stdout + res.stderr)
+    os.replace(SHIM + ".tmp", SHIM)
+    return SHIM
+
+
 def build(force: bool = False, ptxas_verbose: bool = False, quiet: bool = True) -> str:
-    """Compile libafhe.so if missing or older than its sources; return its path."""
+    """Compile libafhe.so (and the fhe_accel_top binding) if missing or older
+    than their sources; return the path of libafhe.so."""
     if not force and not _stale():
+        build_shim()
         return LIB
     os.makedirs(LIBDIR, exist_ok=True)
     tmp = LIB + ".tmp"
@@ -61,6 +83,7 @@ def build(force: bool = False, ptxas_verbose: bool = False, quiet: bool = True) 
     if not quiet or ptxas_verbose:
         sys.stdout.write(res.stdout + res.stderr)
     os.replace(tmp, LIB)
+    build_shim(force=True)
     return LIB
 
 

@@ -38,15 +38,10 @@ u64 root_of(const afhe_ctx* ctx, uint32_t i) {
     return psi ? psi : min_primitive_root(ctx->log_n, q);
 }
 
-int zf_from(afhe_ctx* ctx, const u64* vals, uint32_t n, ZField* out) {
-    if (n == 0) { *out = zf_const(0); return AFHE_OK; }
-    const u64 stride = n > 1 ? vals[1] - vals[0] : 0;
-    bool prog = true;
-    for (uint32_t i = 1; i < n && prog; ++i) prog = (vals[i] - vals[i - 1]) == stride;
-    if (prog) { *out = zf_stride(vals[0], stride); return AFHE_OK; }
+int ring_put(afhe_ctx* ctx, const void* src, size_t words, u64** dev) {
     DescRing& r = ctx->ring;
-    if (n > r.seg_words) return fail(ctx, AFHE_E_ARG, "batch too large for the descriptor ring");
-    if (r.pos + n > r.seg_words) {
+    if (words > r.seg_words) return fail(ctx, AFHE_E_ARG, "descriptor too large for the descriptor ring");
+    if (r.pos + words > r.seg_words) {
         CK(cudaEventRecord(r.ev[r.cur], ctx->st));
         r.used[r.cur] = 1;
         r.cur = (r.cur + 1) % r.nseg;
@@ -54,12 +49,26 @@ int zf_from(afhe_ctx* ctx, const u64* vals, uint32_t n, ZField* out) {
         r.pos = 0;
     }
     const size_t at = r.cur * r.seg_words + r.pos;
-    std::memcpy(r.host + at, vals, n * sizeof(u64));
-    CK(cudaMemcpyAsync(r.dev + at, r.host + at, n * sizeof(u64), cudaMemcpyHostToDevice, ctx->st));
+    std::memcpy(r.host + at, src, words * sizeof(u64));
+    CK(cudaMemcpyAsync(r.dev + at, r.host + at, words * sizeof(u64), cudaMemcpyHostToDevice, ctx->st));
+    *dev = r.dev + at;
+    r.pos += (words + 31) & ~(size_t)31;
+    return AFHE_OK;
+}
+
+int zf_from(afhe_ctx* ctx, const u64* vals, uint32_t n, ZField* out) {
+    if (n == 0) { *out = zf_const(0); return AFHE_OK; }
+    const u64 stride = n > 1 ? vals[1] - vals[0] : 0;
+    bool prog = true;
+    for (uint32_t i = 1; i < n && prog; ++i) prog = (vals[i] - vals[i - 1]) == stride;
+    if (prog) { *out = zf_stride(vals[0], stride); return AFHE_OK; }
+    if (n > ctx->ring.seg_words) return fail(ctx, AFHE_E_ARG, "batch too large for the descriptor ring");
+    u64* dev = nullptr;
+    int rc = ring_put(ctx, vals, n, &dev);
+    if (rc != AFHE_OK) return rc;
     ZField f{};
-    f.arr = r.dev + at;
+    f.arr = dev;
     *out = f;
-    r.pos += (n + 31) & ~(size_t)31;
     return AFHE_OK;
 }
 }  // namespace afhe
@@ -430,7 +439,7 @@ int afhe_ctx_destroy(afhe_ctx* ctx) {
     fr(ctx->poly); fr(ctx->key); fr(ctx->lvbuf); fr(ctx->jobs_qp);
     for (auto& j : ctx->lvjobs) fr(j.modup);
     for (DevPrimeSet* s : {&ctx->nat, &ctx->ld}) { fr(s->pc); fr(s->tw); fr(s->itw); fr(s->tw2); fr(s->itw2); }
-    fr(ctx->ld_crt); fr(ctx->ld_crt_sh); fr(ctx->ld_mod); fr(ctx->ld_jobs);
+    fr(ctx->ld_crt); fr(ctx->ld_crt_sh); fr(ctx->ld_mod);
     for (auto& kv : ctx->rot) fr(kv.second.map);
     free_key_preps(ctx);
     fr(ctx->ring.dev);
@@ -748,6 +757,7 @@ int load_context(afhe_ctx* ctx, const afhe_accel_args* a) {
     ctx->ld_p.assign(a->p_primes, a->p_primes + K);
     ctx->ld_ninv_q.assign(a->n_inv_q, a->n_inv_q + L);
     ctx->ld_ninv_p.assign(a->n_inv_p, a->n_inv_p + K);
+    std::fill(ctx->ld_tabs_key, ctx->ld_tabs_key + 4, -1);    // tables prepared from the old load are stale
     ctx->loaded = true;
     return AFHE_OK;
 }
@@ -768,6 +778,11 @@ int check_call_primes(afhe_ctx* ctx, const afhe_accel_args* a, uint32_t nq, uint
 // Per-call working copy of the loaded CRT tables reduced by, and with
 // companions for, the moduli each entry multiplies under at level sizeQl.
 int prep_loaded_tables(afhe_ctx* ctx, uint32_t sizeQl, uint32_t parts, uint32_t alpha, bool ks, OpTabs* t) {
+    const int key[4] = {(int)sizeQl, (int)parts, (int)alpha, ks ? 1 : 0};
+    if (std::equal(key, key + 4, ctx->ld_tabs_key)) {   // prepared by an earlier call, in stream order
+        *t = ctx->ld_tabs;
+        return AFHE_OK;
+    }
     const uint32_t K = ctx->ld_np, Lld = ctx->ld_nq;
     const size_t W = ctx->ld_crt_words;
     std::vector<u64> mods(W, 0);
@@ -823,24 +838,26 @@ int prep_loaded_tables(afhe_ctx* ctx, uint32_t sizeQl, uint32_t parts, uint32_t 
     t->qlql_sh = ctx->ld_crt_sh + ctx->ld_off_qlql;
     t->qlinv = work + ctx->ld_off_qlinv;
     t->qlinv_sh = ctx->ld_crt_sh + ctx->ld_off_qlinv;
+    // the moduli go through the pinned descriptor ring: no host wait, and the
+    // working copy is rewritten in stream order after every earlier use
     cudaStream_t st = ctx->st;
+    u64* dmods = nullptr;
+    int rc = ring_put(ctx, mods.data(), W, &dmods);
+    if (rc != AFHE_OK) return rc;
     CK(cudaMemcpyAsync(work, ctx->ld_crt, W * 8, cudaMemcpyDeviceToDevice, st));
-    CK(cudaMemcpyAsync(ctx->ld_mod, mods.data(), W * 8, cudaMemcpyHostToDevice, st));
-    CK(launch_companions(work, ctx->ld_crt_sh, ctx->ld_mod, W, st));
-    CK(cudaStreamSynchronize(st));
+    CK(launch_companions(work, ctx->ld_crt_sh, dmods, W, st));
+    ctx->ld_tabs = *t;
+    std::copy(key, key + 4, ctx->ld_tabs_key);
     return AFHE_OK;
 }
 
-int upload_jobs(afhe_ctx* ctx, const std::vector<LimbJob>& jobs) {
-    if (ctx->ld_jobs_cap < jobs.size()) {
-        if (ctx->ld_jobs) cudaFree(ctx->ld_jobs);
-        ctx->ld_jobs = nullptr;
-        CK(dalloc(&ctx->ld_jobs, jobs.size()));
-        ctx->ld_jobs_cap = jobs.size();
-    }
-    CK(cudaMemcpyAsync(ctx->ld_jobs, jobs.data(), jobs.size() * sizeof(LimbJob), cudaMemcpyHostToDevice, ctx->st));
-    CK(cudaStreamSynchronize(ctx->st));
-    return AFHE_OK;
+// The call's job list, staged through the descriptor ring (no host wait).
+int upload_jobs(afhe_ctx* ctx, const std::vector<LimbJob>& jobs, const LimbJob** dev) {
+    static_assert(sizeof(LimbJob) % sizeof(u64) == 0, "LimbJob is staged as words");
+    u64* d = nullptr;
+    int rc = ring_put(ctx, jobs.data(), jobs.size() * sizeof(LimbJob) / sizeof(u64), &d);
+    *dev = (const LimbJob*)d;
+    return rc;
 }
 
 bool overlap(u64 a, u64 aw, u64 b, u64 bw) { return a < b + bw && b < a + aw; }
@@ -881,14 +898,15 @@ extern "C" int afhe_dispatch(afhe_ctx* ctx, const afhe_accel_args* a) {
             return fail(ctx, AFHE_E_RANGE, "NTT operands out of range");
         std::vector<LimbJob> jobs(L);
         for (uint32_t i = 0; i < L; ++i) { jobs[i].src = jobs[i].dst = jobs[i].out = (u64)i * n; jobs[i].prime = i; jobs[i].aux = i; }
-        if ((rc = upload_jobs(ctx, jobs)) != AFHE_OK) return rc;
+        const LimbJob* djobs = nullptr;
+        if ((rc = upload_jobs(ctx, jobs, &djobs)) != AFHE_OK) return rc;
         u64 src; bool in_scr;
         if ((rc = stage(ctx, a->src_a_offset, LN, a->dst_offset, LN, 0, &src, &in_scr)) != AFHE_OK) return rc;
         ZBases zb{};
         zb.src = zf_const(src);
         zb.mid = zf_const(a->dst_offset);
         zb.out = zf_const(a->dst_offset);
-        CK(launch_ntt_plain(a->op_code == AFHE_OP_INTT, ctx->log_n, ctx->ld.view(), ctx->ld_jobs, L,
+        CK(launch_ntt_plain(a->op_code == AFHE_OP_INTT, ctx->log_n, ctx->ld.view(), djobs, L,
                             in_scr ? ctx->scr : ctx->poly, ctx->poly, 1, zb, st));
         break;
     }
@@ -904,9 +922,10 @@ extern "C" int afhe_dispatch(afhe_ctx* ctx, const afhe_accel_args* a) {
             if (a->rns_primes[i] < 3 || a->rns_primes[i] >= (1ull << 61)) return fail(ctx, AFHE_E_ARG, "modulus out of range");
             pc[i] = host_prime_const(a->rns_primes[i], 1, 1);
         }
-        PrimeConst* dpc = nullptr;
-        CK(dalloc(&dpc, L));
-        CK(cudaMemcpyAsync(dpc, pc.data(), L * sizeof(PrimeConst), cudaMemcpyHostToDevice, st));
+        static_assert(sizeof(PrimeConst) % sizeof(u64) == 0, "PrimeConst is staged as words");
+        u64* dpc_words = nullptr;
+        if ((rc = ring_put(ctx, pc.data(), L * sizeof(PrimeConst) / sizeof(u64), &dpc_words)) != AFHE_OK) return rc;
+        const PrimeConst* dpc = (const PrimeConst*)dpc_words;
         // operands that partially overlap the output are staged (scratch words [0, 2LN))
         u64 sa, sb; bool ia, ib;
         if ((rc = stage(ctx, a->src_a_offset, LN, a->dst_offset, LN, 0, &sa, &ia)) != AFHE_OK) return rc;
@@ -925,8 +944,6 @@ extern "C" int afhe_dispatch(afhe_ctx* ctx, const afhe_accel_args* a) {
             zb.src = zf_const(sa); zb.aux = zf_const(sb); zb.out = zf_const(a->dst_offset);
             CK(launch_elementwise(op, dpc, 0, ctx->poly, n, L, 1, zb, st));
         }
-        CK(cudaStreamSynchronize(st));
-        cudaFree(dpc);
         break;
     }
     case AFHE_OP_AUTOMORPHISM: {
@@ -953,7 +970,8 @@ extern "C" int afhe_dispatch(afhe_ctx* ctx, const afhe_accel_args* a) {
         if ((rc = prep_loaded_tables(ctx, L, 1, 1, false, &t)) != AFHE_OK) return rc;
         std::vector<LimbJob> jobs(L);
         for (uint32_t i = 0; i < L; ++i) { jobs[i].src = jobs[i].dst = jobs[i].out = (u64)i * n; jobs[i].prime = i; jobs[i].aux = i; }
-        if ((rc = upload_jobs(ctx, jobs)) != AFHE_OK) return rc;
+        const LimbJob* djobs = nullptr;
+        if ((rc = upload_jobs(ctx, jobs, &djobs)) != AFHE_OK) return rc;
         // fhe_accel_top.cpp:283-297: both inputs are loaded before anything is stored
         const u64 s_in = 0, s_tmp = 2 * LN, s_out = 4 * LN;
         CK(cudaMemcpyAsync(ctx->scr + s_in, ctx->poly + a->src_a_offset, LN * 8, cudaMemcpyDeviceToDevice, st));
@@ -962,7 +980,7 @@ extern "C" int afhe_dispatch(afhe_ctx* ctx, const afhe_accel_args* a) {
         zb.src = zf_stride(s_in, LN);
         zb.out = zf_stride(s_out, out);
         zb.mid = zf_stride(s_tmp, LN);
-        CK(launch_rescale(ctx->log_n, t, ctx->ld_jobs, L, ctx->scr, ctx->scr, 2, zb, st));
+        CK(launch_rescale(ctx->log_n, t, djobs, L, ctx->scr, ctx->scr, 2, zb, st));
         CK(cudaMemcpyAsync(ctx->poly + a->dst_offset, ctx->scr + s_out, 2 * out * 8, cudaMemcpyDeviceToDevice, st));
         break;
     }
@@ -1002,7 +1020,8 @@ extern "C" int afhe_dispatch(afhe_ctx* ctx, const afhe_accel_args* a) {
                 ++n_modup;
             }
         }
-        if ((rc = upload_jobs(ctx, jobs)) != AFHE_OK) return rc;
+        const LimbJob* djobs = nullptr;
+        if ((rc = upload_jobs(ctx, jobs, &djobs)) != AFHE_OK) return rc;
         const u64 kw = ks_scratch_words(n, sq, K, parts);
         if (SQ + kw > ctx->scr_words) return fail(ctx, AFHE_E_ARG, "scratch too small for this key switch");
         // input staged into scratch (fhe_accel_top.cpp:299-300 loads it first)
@@ -1016,7 +1035,7 @@ extern "C" int afhe_dispatch(afhe_ctx* ctx, const afhe_accel_args* a) {
         zb.mid = zf_const(SQ);
         zb.out = zf_const(o_scr);        // ks0
         zb.aux = zf_const(o_scr + SQ);   // ks1
-        CK(launch_key_switch(ctx->log_n, t, ctx->ld_jobs, ctx->ld_jobs + sq + K, n_modup, sq, sq, K, ctx->key,
+        CK(launch_key_switch(ctx->log_n, t, djobs, djobs + sq + K, n_modup, sq, sq, K, ctx->key,
                              a->evk_offset, a->evk_offset + (u64)parts * (sq + K) * n, sq + K, sq, ctx->scr, ctx->scr,
                              1, zb, st));
         CK(cudaMemcpyAsync(ctx->poly + a->dst_offset, ctx->scr + o_scr, 2 * SQ * 8, cudaMemcpyDeviceToDevice, st));
@@ -1025,6 +1044,6 @@ extern "C" int afhe_dispatch(afhe_ctx* ctx, const afhe_accel_args* a) {
     default:
         return fail(ctx, AFHE_E_ARG, "unknown op code");
     }
-    CK(cudaStreamSynchronize(st));
+    // enqueued on the context stream; afhe_read_* and afhe_sync wait for it
     return AFHE_OK;
 }

@@ -579,17 +579,22 @@ int afhe_eval_rotate_steps_batch(afhe_ctx* ctx, const afhe_ct_ref* in, const afh
     const OpTabs& t = ctx->lv[limbs];
     const LevelJobs& lj = ctx->lvjobs[limbs];
     // eval_rotate_single_step per entry (fhe_host_driver.cpp:331-359), each
-    // with its own key and automorphism, as one multi-kernel key switch:
-    // every input is read before any output is written, so outputs may
-    // alias inputs
+    // with its own key and automorphism, in one key switch launch sequence.
+    // The multi-kernel key switch reads every input before it writes any
+    // output, so outputs may alias inputs anywhere; the one-kernel key switch
+    // runs its entries concurrently, so it takes a chunk whose outputs alias
+    // only their own entry's inputs.
     return for_chunks(ctx, count, [&](uint32_t s, uint32_t m) -> int {
-        Offs i0(m), i1(m), o0(m), o1(m), maps(m), keys(m);
+        Offs i0(m), i1(m), o0(m), o1(m), maps(m), keys(m), preps(m);
+        bool all_prep = true;
         for (uint32_t z = 0; z < m; ++z) {
             const RotKey& rk = ctx->rot.at(steps[s + z]);
             i0[z] = in[s + z].c0_offset; i1[z] = in[s + z].c1_offset;
             o0[z] = dst[s + z].c0_offset; o1[z] = dst[s + z].c1_offset;
             maps[z] = (u64)(uintptr_t)rk.map;
             keys[z] = rk.evk_offset;
+            preps[z] = (u64)(uintptr_t)rk.prep;
+            all_prep = all_prep && rk.prep;
         }
         KsFuse f{};
         f.has_c0 = 1;
@@ -602,6 +607,16 @@ int afhe_eval_rotate_steps_batch(afhe_ctx* ctx, const afhe_ct_ref* in, const afh
         ZF(zb.out, o0);
         ZF(zb.aux, o1);
         zb.mid = lane_field(ctx, &Lane::ks);
+        if (ctx->ks_fused && fused_rotation_safe(i0, i1, o0, o1, (u64)limbs * n)) {
+            const ulonglong2* prep = nullptr;
+            if (all_prep) {
+                ZF(f.prepz, preps);
+                prep = ctx->rot.at(steps[s]).prep;
+            }
+            CK(launch_key_switch_fused(ctx->log_n, t, limbs, ctx->K, ctx->key, 0, (u64)ctx->dnum * S * n, (uint32_t)S,
+                                       ctx->L, ctx->poly, ctx->scr, m, zb, ctx->st, &f, prep));
+            return AFHE_OK;
+        }
         CK(launch_key_switch(ctx->log_n, t, ctx->jobs_qp, lj.modup, lj.n_modup, ctx->L, limbs, ctx->K, ctx->key, 0,
                              (u64)ctx->dnum * S * n, (uint32_t)S, ctx->L, ctx->poly, ctx->scr, m, zb, ctx->st, &f));
         return AFHE_OK;

@@ -104,8 +104,10 @@ struct afhe_ctx {
     size_t ld_crt_words = 0;
     std::vector<size_t> ld_off_qhat_inv, ld_off_qhat_modp;
     size_t ld_off_pinv = 0, ld_off_phatinv = 0, ld_off_phatmodq = 0, ld_off_qlql = 0, ld_off_qlinv = 0;
-    afhe::LimbJob* ld_jobs = nullptr;  // per-call job list (device)
-    size_t ld_jobs_cap = 0;
+    // loaded tables prepared for the last (sizeQl, parts, alpha, key switch)
+    // a dispatched op used; reused while the next op has the same shape
+    int ld_tabs_key[4] = {-1, -1, -1, -1};
+    afhe::OpTabs ld_tabs{};
 
     // scratch for composite operators (context-private), `lanes` lanes
     afhe::u64* scr = nullptr;
@@ -176,16 +178,17 @@ cudaError_t launch_rescale(int log_n, const OpTabs& t, const LimbJob* jobs_q, ui
 //   * has_c0: ks0 output += c0[map[x]] (c0 gathered into scratch by the MAC);
 //   * has_acc: ks0 output += acc0[x], ks1 output += acc1[x].
 // So one call computes a whole rotation step, acc + rot(ct), or d + KS(d2).
-// With per_z (multi-kernel key switch only), entry z has its own rotation:
-// its automorphism map at the device address mapz.at(z), and its key at
-// keyz.at(z) words past evk_a / evk_b.
+// With per_z, entry z has its own rotation: its automorphism map at the
+// device address mapz.at(z), its key at keyz.at(z) words past evk_a / evk_b,
+// and (one-kernel key switch with prepared keys) that key's prepared copy at
+// the device address prepz.at(z).
 struct KsFuse {
     const uint32_t* map;
     int has_c0;
     int has_acc;
     ZField c0, acc0, acc1;
     int per_z;
-    ZField mapz, keyz;
+    ZField mapz, keyz, prepz;
 };
 size_t ks_scratch_words(uint32_t n, uint32_t L, uint32_t K, uint32_t parts);
 cudaError_t launch_key_switch(int log_n, const OpTabs& t, const LimbJob* jobs_qp, const LimbJob* jobs_modup,
@@ -194,8 +197,9 @@ cudaError_t launch_key_switch(int log_n, const OpTabs& t, const LimbJob* jobs_qp
                               u64* arena, u64* scratch, uint32_t nz, const ZBases& zb, cudaStream_t st,
                               const KsFuse* fuse = nullptr);
 
-// The same key switch as one kernel per polynomial (N <= 2^13): each CTA
-// keeps the limb being transformed and both accumulators in shared memory
+// The same key switch as one kernel per polynomial: for N <= 2^13 one CTA,
+// above that a cluster of N / 2^13 CTAs (distributed shared memory) keeps
+// the limb being transformed and both accumulators in shared memory
 // and needs ks_fused_scratch_words(...) words of scratch at zb.mid (the INTT
 // of the input's limbs and of the special accumulators). Entries of one
 // launch run concurrently, so an entry's outputs must not overlap another

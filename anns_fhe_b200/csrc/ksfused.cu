@@ -1,10 +1,11 @@
-// ksfused.cu -- the whole hybrid key switch in one kernel, for N <= 2^13.
+// ksfused.cu -- the whole hybrid key switch in one kernel, N = 2^10 .. 2^16.
 //
 // Same arithmetic as launch_key_switch (key_switch.cpp:167-439 restated:
 // INTT of the input's limbs, fast_bases_conv to each digit's complementary
 // primes, NTT, inner product with evk_a / evk_b, approx_mod_down), but one
-// CTA carries one ciphertext polynomial through every step with the limb
-// being transformed held in shared memory:
+// polynomial is carried through every step by one CTA (N <= 2^13) or by a
+// thread-block cluster of CL = N / 2^13 CTAs (N = 2^14, 2^15, 2^16: 2, 4 or
+// 8 CTAs), with the limb being transformed held in shared memory:
 //
 //   phase 0  coef[i] = INTT(in[i]) * qHatInv_i for the input's Q limbs -> lane scratch
 //   phase 1  for every special slot k: the MAC over digits (each digit's value
@@ -17,15 +18,29 @@
 //            the store of output limb i
 //
 // Shared memory: three padded limb buffers (W for transforms, A0 / A1 for the
-// two accumulators), 3 * (N + N/16) words = 204 KB at N = 8192. The key limbs
-// every CTA of a launch reads are the same, so they come from L2. A registered
-// key comes as a prepared copy of (k mod q, Shoup companion) pairs, so each
-// inner-product term is one Shoup multiplication.
+// two accumulators). A cluster splits each buffer: CTA r holds elements
+// [r QN, (r + 1) QN), QN = 2^13, so every CTA uses 3 * (QN + QN/16) words =
+// 204 KB whatever N is. The transforms' low 13 butterfly stages run inside a
+// CTA on its slice (the tile code of ntt.cuh, with the slice index as the
+// index bits above the tile); the top log2(CL) stages combine the CL slices
+// and run across the cluster through distributed shared memory, between two
+// cluster barriers: forward NTTs start with them, inverse NTTs end with them
+// (where the last one folds in N^-1). Element-wise work (base conversions,
+// inner products, ModDown combine) runs on each CTA's own slice.
+//
+// The key limbs every CTA of a launch reads are the same, so they come from
+// L2. A registered key comes as a prepared copy of (k mod q, Shoup
+// companion) pairs, so each inner-product term is one Shoup multiplication.
 //
 // In place is safe: input limb i is read only while slot i is processed, and
-// output limb i is written after every read of input limb i and of the
-// gathered c0 limb i (staged in shared memory behind a barrier).
+// output limb i is written after every read of input limb i (the cluster
+// barriers of the transforms in between) and of the gathered c0 limb i
+// (staged in shared memory behind a barrier across the whole cluster).
+#include <cooperative_groups.h>
+
 #include "internal.h"
+
+namespace cg = cooperative_groups;
 
 namespace afhe {
 
@@ -45,50 +60,217 @@ struct KsFusedArgs {
     u64 prep_b;               // offset of the evk_b digits in prep
 };
 
+constexpr int kLogQ = 13;    // log2 of the slice a CTA holds at N >= 2^13
+
+// One polynomial per CTA (LOGCL = 0) or per cluster of 2^LOGCL CTAs; each CTA
+// holds 2^LOGQ elements of every buffer. Local positions e < 2^LOGQ, global
+// positions x = rank * 2^LOGQ + e.
+template <int LOGQ, int LOGCL>
+struct Geo {
+    static constexpr int LOGN = LOGQ + LOGCL;
+    static constexpr uint32_t QN = 1u << LOGQ;
+    static constexpr uint32_t CL = 1u << LOGCL;
+    static constexpr uint32_t THREADS = QN / 8;
+    __device__ __forceinline__ static uint32_t rank() {
+        if constexpr (LOGCL == 0) return 0;
+        else return cg::this_cluster().block_rank();
+    }
+    // every element of every CTA's slices is visible to every CTA after this
+    __device__ __forceinline__ static void sync_all() {
+        if constexpr (LOGCL == 0) __syncthreads();
+        else cg::this_cluster().sync();
+    }
+    __device__ __forceinline__ static uint32_t z() { return blockIdx.x >> LOGCL; }
+};
+
 // digit j of a level-l key switch: limbs [start, start + size)
 __device__ __forceinline__ void digit_range(const OpTabs& t, uint32_t j, uint32_t& start, uint32_t& size) {
     start = j * t.alpha;
     size = (j == t.parts - 1) ? t.sizeQl - start : t.alpha;
 }
 
-// Not inlined: each transform gets its own register allocation instead of
-// competing with the caller's live state (1024 threads leave 64 registers).
-template <int LOGN>
-__device__ __noinline__ void fwd_ntt(u64* buf, const PrimeTables pt, uint32_t prime, const PrimeConst pc) {
-    ntt_rounds<false, LOGN, 0, false, 0>(buf, pt.tw2 + ((u64)prime << LOGN), pc, 0u, LOGN, 0, true);
+// The top LOGCL butterfly stages of a forward NTT, across the cluster: the
+// CL elements x = k QN + j (k < CL) form a column of CL values, transformed
+// by the stages of bits LOGN - 1 .. LOGQ (block b of stage s uses tw[2^s + b]).
+// CTA r takes the columns j in [r QN / CL, (r + 1) QN / CL).
+template <int LOGQ, int LOGCL, int NB>
+__device__ __forceinline__ void cross_fwd(u64* const (&bufs)[NB], const ulonglong2* __restrict__ tw,
+                                          const PrimeConst& pc) {
+    using G = Geo<LOGQ, LOGCL>;
+    constexpr uint32_t CL = G::CL, PER = G::QN / CL;
+    cg::cluster_group cl = cg::this_cluster();
+    const uint32_t r = cl.block_rank();
+    const u64 q = pc.q, q2 = q << 1;
+    ulonglong2 w[CL - 1];
+#pragma unroll
+    for (uint32_t i = 1; i < CL; ++i) w[i - 1] = __ldg(tw + i);
+    u64* rb[NB][CL];
+#pragma unroll
+    for (int b = 0; b < NB; ++b)
+#pragma unroll
+        for (uint32_t k = 0; k < CL; ++k) rb[b][k] = cl.map_shared_rank(bufs[b], k);
+    for (uint32_t jj = threadIdx.x; jj < PER; jj += G::THREADS) {
+        const uint32_t e = padix(r * PER + jj);
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            u64 v[CL];
+#pragma unroll
+            for (uint32_t k = 0; k < CL; ++k) v[k] = rb[b][k][e];
+#pragma unroll
+            for (int s = 0; s < LOGCL; ++s) {
+                const uint32_t m = 1u << s, t = CL >> (s + 1);
+#pragma unroll
+                for (uint32_t blk = 0; blk < m; ++blk)
+#pragma unroll
+                    for (uint32_t i = 0; i < t; ++i)
+                        ct_bfly(v[blk * 2 * t + i], v[blk * 2 * t + i + t], w[m + blk - 1], q, q2);
+            }
+#pragma unroll
+            for (uint32_t k = 0; k < CL; ++k) rb[b][k][e] = v[k];
+        }
+    }
 }
 
-template <int LOGN>
+// The top LOGCL stages of an inverse NTT (Gentleman-Sande, bits LOGQ ..
+// LOGN - 1), the last one with N^-1 folded in; outputs canonical.
+template <int LOGQ, int LOGCL, int NB>
+__device__ __forceinline__ void cross_inv(u64* const (&bufs)[NB], const ulonglong2* __restrict__ itw,
+                                          const PrimeConst& pc) {
+    using G = Geo<LOGQ, LOGCL>;
+    constexpr uint32_t CL = G::CL, PER = G::QN / CL;
+    cg::cluster_group cl = cg::this_cluster();
+    const uint32_t r = cl.block_rank();
+    const u64 q = pc.q, q2 = q << 1;
+    ulonglong2 w[CL > 2 ? CL - 1 : 1];
+#pragma unroll
+    for (uint32_t i = 2; i < CL; ++i) w[i - 1] = __ldg(itw + i);   // itw[1] enters through pc.w1ninv
+    u64* rb[NB][CL];
+#pragma unroll
+    for (int b = 0; b < NB; ++b)
+#pragma unroll
+        for (uint32_t k = 0; k < CL; ++k) rb[b][k] = cl.map_shared_rank(bufs[b], k);
+    for (uint32_t jj = threadIdx.x; jj < PER; jj += G::THREADS) {
+        const uint32_t e = padix(r * PER + jj);
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            u64 v[CL];
+#pragma unroll
+            for (uint32_t k = 0; k < CL; ++k) v[k] = rb[b][k][e];
+#pragma unroll
+            for (int s = LOGCL - 1; s >= 0; --s) {
+                const uint32_t m = 1u << s, t = CL >> (s + 1);
+                if (s == 0) {
+#pragma unroll
+                    for (uint32_t i = 0; i < t; ++i) gs_bfly_last(v[i], v[i + t], pc, q2);
+                } else {
+#pragma unroll
+                    for (uint32_t blk = 0; blk < m; ++blk)
+#pragma unroll
+                        for (uint32_t i = 0; i < t; ++i)
+                            gs_bfly(v[blk * 2 * t + i], v[blk * 2 * t + i + t], w[m + blk - 1], q, q2);
+                }
+            }
+#pragma unroll
+            for (uint32_t k = 0; k < CL; ++k) rb[b][k][e] = v[k];
+        }
+    }
+}
+
+// Forward NTT of one buffer. On entry this CTA's slice is written (and
+// visible after a CTA barrier); on return the slice holds lazy residues in
+// [0, 4q). Not inlined: each transform gets its own register allocation
+// instead of competing with the caller's live state (1024 threads leave 64
+// registers).
+template <int LOGQ, int LOGCL>
+__device__ __noinline__ void fwd_ntt(u64* buf, const PrimeTables pt, uint32_t prime, const PrimeConst pc) {
+    using G = Geo<LOGQ, LOGCL>;
+    const ulonglong2* tw = pt.tw2 + ((u64)prime << G::LOGN);
+    if constexpr (LOGCL > 0) {
+        u64* const one[1] = {buf};
+        G::sync_all();
+        cross_fwd<LOGQ, LOGCL, 1>(one, tw, pc);
+        G::sync_all();
+    }
+    ntt_rounds<false, LOGQ, 0, false, 0>(buf, tw, pc, G::rank(), G::LOGN, 0, true);
+}
+
+// Inverse NTT of one buffer; on return the slice holds canonical residues.
+template <int LOGQ, int LOGCL>
 __device__ __noinline__ void inv_ntt(u64* buf, const PrimeTables pt, uint32_t prime, const PrimeConst pc) {
-    ntt_rounds<true, LOGN, 0, false, 0>(buf, pt.itw2 + ((u64)prime << LOGN), pc, 0u, LOGN, 0, true);
+    using G = Geo<LOGQ, LOGCL>;
+    const ulonglong2* itw = pt.itw2 + ((u64)prime << G::LOGN);
+    ntt_rounds<true, LOGQ, 0, false, 0>(buf, itw, pc, G::rank(), G::LOGN, 0, LOGCL == 0);
+    if constexpr (LOGCL > 0) {
+        u64* const one[1] = {buf};
+        G::sync_all();
+        cross_inv<LOGQ, LOGCL, 1>(one, itw, pc);
+        G::sync_all();
+    }
 }
 
 // Two limbs of the same prime transformed together (shared twiddles).
-template <bool INV, int LOGN>
+template <bool INV, int LOGQ, int LOGCL>
 __device__ __noinline__ void ntt2(u64* b0, u64* b1, const PrimeTables pt, uint32_t prime, const PrimeConst pc) {
+    using G = Geo<LOGQ, LOGCL>;
     u64* const bufs[2] = {b0, b1};
-    ntt_rounds_n<INV, LOGN, 0, false, 0, 8, 2>(bufs, (INV ? pt.itw2 : pt.tw2) + ((u64)prime << LOGN), pc, 0u, LOGN,
-                                                0, true);
+    const ulonglong2* tw = (INV ? pt.itw2 : pt.tw2) + ((u64)prime << G::LOGN);
+    if constexpr (!INV && LOGCL > 0) {
+        G::sync_all();
+        cross_fwd<LOGQ, LOGCL, 2>(bufs, tw, pc);
+        G::sync_all();
+    }
+    ntt_rounds_n<INV, LOGQ, 0, false, 0, 8, 2>(bufs, tw, pc, G::rank(), G::LOGN, 0, !INV || LOGCL == 0);
+    if constexpr (INV && LOGCL > 0) {
+        G::sync_all();
+        cross_inv<LOGQ, LOGCL, 2>(bufs, tw, pc);
+        G::sync_all();
+    }
 }
 
-// Every element-wise pass below gives each thread the positions
-// x_k = threadIdx.x + k * N/8, k < 8, and issues a chunk's global loads before
-// its arithmetic, so several L2 round trips are in flight per thread.
+// Every element-wise pass below gives each thread the local positions
+// e_k = threadIdx.x + k * QN/8, k < 8 (global x_k = rank * QN + e_k), and
+// issues a chunk's global loads before its arithmetic, so several L2 round
+// trips are in flight per thread.
 constexpr uint32_t kPer = 8;     // positions per thread
 constexpr uint32_t kChunk = 4;   // positions whose loads are issued together
 
-template <int LOGN>
-__device__ __forceinline__ uint32_t pos(uint32_t k) { return threadIdx.x + k * ((1u << LOGN) / 8); }
+template <int LOGQ>
+__device__ __forceinline__ uint32_t lpos(uint32_t k) { return threadIdx.x + k * ((1u << LOGQ) / 8); }
 
 // gathered position of x: the automorphism's source index, or x itself
 __device__ __forceinline__ uint32_t gpos(const uint32_t* map, uint32_t x) { return map ? __ldg(map + x) : x; }
 
-// Inner product for one slot (Q limb `s` < l, or special limb s - l) into A0 / A1:
-// A0 = sum_j d_j * evk_b[j], A1 = sum_j d_j * evk_a[j] (mod the slot's prime).
-template <int LOGN, bool PREP>
-__device__ void mac_slot(const KsFusedArgs& a, uint32_t s, u64* W, u64* A0, u64* A1, const u64* __restrict__ in,
-                         const u64* __restrict__ coef) {
+// This entry's rotation (automorphism map, key offset, prepared key).
+struct EntryKey {
+    const uint32_t* map;
+    u64 koff;
+    const ulonglong2* prep;
+};
+
+__device__ __forceinline__ EntryKey entry_key(const KsFusedArgs& a, uint32_t z) {
+    EntryKey k;
+    if (a.f.per_z) {
+        k.map = (const uint32_t*)a.f.mapz.at(z);
+        k.koff = a.f.keyz.at(z);
+        k.prep = a.prep ? (const ulonglong2*)a.f.prepz.at(z) : nullptr;
+    } else {
+        k.map = a.f.map;
+        k.koff = 0;
+        k.prep = a.prep;
+    }
+    return k;
+}
+
+// Inner product for one slot (Q limb `s` < l, or special limb s - l) into
+// this CTA's slices of A0 / A1: A0 = sum_j d_j * evk_b[j], A1 = sum_j d_j *
+// evk_a[j] (mod the slot's prime).
+template <int LOGQ, int LOGCL, bool PREP>
+__device__ void mac_slot(const KsFusedArgs& a, const EntryKey& ek, uint32_t s, u64* W, u64* A0, u64* A1,
+                         const u64* __restrict__ in, const u64* __restrict__ coef) {
+    using G = Geo<LOGQ, LOGCL>;
+    constexpr int LOGN = G::LOGN;
     constexpr uint32_t N = 1u << LOGN;
+    const uint32_t x0 = G::rank() * G::QN;
     const OpTabs& t = a.t;
     const uint32_t l = a.sizeQl;
     const bool isq = s < l;
@@ -97,16 +279,16 @@ __device__ void mac_slot(const KsFusedArgs& a, uint32_t s, u64* W, u64* A0, u64*
     const PrimeConst pc = t.pt.pc[prime];
     const ModConst mc = modconst_of(pc);
     const u64 q = pc.q, p2 = q << 1;
-    const uint32_t* map = a.f.map;
+    const uint32_t* map = ek.map;
     for (uint32_t j = 0; j < t.parts; ++j) {
         uint32_t start, size;
         digit_range(t, j, start, size);
         const bool own = isq && s >= start && s < start + size;
         const u64 kofs = ((u64)j * a.key_stride + klimb) * N;
-        const u64* kb = a.key + a.evk_b + kofs;
-        const u64* ka = a.key + a.evk_a + kofs;
-        const ulonglong2* pb2 = PREP ? a.prep + a.prep_b + kofs : nullptr;
-        const ulonglong2* pa2 = PREP ? a.prep + kofs : nullptr;
+        const u64* kb = a.key + a.evk_b + ek.koff + kofs;
+        const u64* ka = a.key + a.evk_a + ek.koff + kofs;
+        const ulonglong2* pb2 = PREP ? ek.prep + a.prep_b + kofs : nullptr;
+        const ulonglong2* pa2 = PREP ? ek.prep + kofs : nullptr;
         if (!own) {
             // W = BConv_j(coef) at this slot's prime, then NTT
             const uint32_t row = l - size + a.K;
@@ -117,10 +299,10 @@ __device__ void mac_slot(const KsFusedArgs& a, uint32_t s, u64* W, u64* A0, u64*
             for (uint32_t i = 0; i < size; ++i) {
                 const uint32_t limb = start + i;
                 const u64 w1 = __ldg(t.qhat_modp[j] + i * row + kpos), w1s = __ldg(t.qhat_modp_sh[j] + i * row + kpos);
-                const u64* src = coef + ((u64)limb << LOGN);     // [x * qHatInv]_{q_i} (phase 0)
+                const u64* src = coef + ((u64)limb << LOGN) + x0;     // [x * qHatInv]_{q_i} (phase 0)
                 u64 v[kPer];
 #pragma unroll
-                for (uint32_t k = 0; k < kPer; ++k) v[k] = src[pos<LOGN>(k)];
+                for (uint32_t k = 0; k < kPer; ++k) v[k] = src[lpos<LOGQ>(k)];
 #pragma unroll
                 for (uint32_t k = 0; k < kPer; ++k) {
                     acc[k] += mul_shoup_lazy(v[k], w1, w1s, q);
@@ -128,9 +310,9 @@ __device__ void mac_slot(const KsFusedArgs& a, uint32_t s, u64* W, u64* A0, u64*
                 }
             }
 #pragma unroll
-            for (uint32_t k = 0; k < kPer; ++k) W[padix(pos<LOGN>(k))] = csub(acc[k], q);
+            for (uint32_t k = 0; k < kPer; ++k) W[padix(lpos<LOGQ>(k))] = csub(acc[k], q);
             __syncthreads();
-            fwd_ntt<LOGN>(W, t.pt, prime, pc);
+            fwd_ntt<LOGQ, LOGCL>(W, t.pt, prime, pc);
         }
         const u64* src = in + ((u64)s << LOGN);
         if (PREP) {
@@ -142,14 +324,14 @@ __device__ void mac_slot(const KsFusedArgs& a, uint32_t s, u64* W, u64* A0, u64*
                 ulonglong2 vb[kChunk], va[kChunk];
 #pragma unroll
                 for (uint32_t k = 0; k < kChunk; ++k) {
-                    const uint32_t x = pos<LOGN>(c + k);
+                    const uint32_t x = x0 + lpos<LOGQ>(c + k);
                     vb[k] = __ldg(pb2 + x);
                     va[k] = __ldg(pa2 + x);
-                    d[k] = own ? src[gpos(map, x)] : W[padix(x)];   // any d < 2^64 is valid for Shoup
+                    d[k] = own ? src[gpos(map, x)] : W[padix(lpos<LOGQ>(c + k))];   // any d < 2^64 is valid for Shoup
                 }
 #pragma unroll
                 for (uint32_t k = 0; k < kChunk; ++k) {
-                    const uint32_t e = padix(pos<LOGN>(c + k));
+                    const uint32_t e = padix(lpos<LOGQ>(c + k));
                     u64 pb = mul_shoup_lazy(d[k], vb[k].x, vb[k].y, q);
                     u64 pa = mul_shoup_lazy(d[k], va[k].x, va[k].y, q);
                     if (j > 0) {
@@ -168,14 +350,14 @@ __device__ void mac_slot(const KsFusedArgs& a, uint32_t s, u64* W, u64* A0, u64*
                 u64 d[kChunk], vb[kChunk], va[kChunk];
 #pragma unroll
                 for (uint32_t k = 0; k < kChunk; ++k) {
-                    const uint32_t x = pos<LOGN>(c + k);
+                    const uint32_t x = x0 + lpos<LOGQ>(c + k);
                     vb[k] = __ldg(kb + x);
                     va[k] = __ldg(ka + x);
-                    d[k] = own ? src[gpos(map, x)] : canon4(W[padix(x)], q);
+                    d[k] = own ? src[gpos(map, x)] : canon4(W[padix(lpos<LOGQ>(c + k))], q);
                 }
 #pragma unroll
                 for (uint32_t k = 0; k < kChunk; ++k) {
-                    const uint32_t e = padix(pos<LOGN>(c + k));
+                    const uint32_t e = padix(lpos<LOGQ>(c + k));
                     u64 pb = mul_mod(d[k], vb[k], mc);
                     u64 pa = mul_mod(d[k], va[k], mc);
                     if (j > 0) {
@@ -191,46 +373,48 @@ __device__ void mac_slot(const KsFusedArgs& a, uint32_t s, u64* W, u64* A0, u64*
     }
 }
 
-// The key switch at one Q limb with one special prime (a single digit):
-// nothing leaves shared memory between the input load and the output store.
+// The key switch at one Q limb with one special prime (a single digit), N <=
+// 2^13: nothing leaves shared memory between the input load and the output
+// store.
 //   W = INTT_q0(in), W = BConv(W) to P, W = NTT_P(W); A_h = W * key_h[P];
 //   (A0, A1) = INTT_P; BConv to q0 in place; (A0, A1) = NTT_q0;
 //   out_h = (in * key_h[q0] - A_h) * P^-1 (+ extras), the own digit's product
 //   computed in the same pass. Same residues as the general path.
 template <int LOGN, bool PREP>
-__device__ __forceinline__ void ks_one_limb(const KsFusedArgs& a, u64* W, u64* A0, u64* A1) {
+__device__ __forceinline__ void ks_one_limb(const KsFusedArgs& a, const EntryKey& ek, u64* W, u64* A0, u64* A1) {
     constexpr uint32_t N = 1u << LOGN;
     const uint32_t z = blockIdx.x;
     const OpTabs& t = a.t;
-    const uint32_t* map = a.f.map;
+    const uint32_t* map = ek.map;
     const u64* in = a.arena + a.in.at(z);
     const PrimeConst pq = t.pt.pc[0], pp = t.pt.pc[t.p_base];
     const u64 q = pq.q, p = pp.q;
+    const u64* key = a.key + ek.koff;
     // W = INTT_q0(input through the automorphism)
     {
         uint32_t g[kPer];
         u64 v[kPer];
 #pragma unroll
-        for (uint32_t k = 0; k < kPer; ++k) g[k] = gpos(map, pos<LOGN>(k));
+        for (uint32_t k = 0; k < kPer; ++k) g[k] = gpos(map, lpos<LOGN>(k));
 #pragma unroll
         for (uint32_t k = 0; k < kPer; ++k) v[k] = in[g[k]];
 #pragma unroll
-        for (uint32_t k = 0; k < kPer; ++k) W[padix(pos<LOGN>(k))] = v[k];
+        for (uint32_t k = 0; k < kPer; ++k) W[padix(lpos<LOGN>(k))] = v[k];
     }
     __syncthreads();
-    inv_ntt<LOGN>(W, t.pt, 0, pq);
+    inv_ntt<LOGN, 0>(W, t.pt, 0, pq);
     // BConv q0 -> P in place (digit 0's only limb), then NTT_P
     {
         const u64 w0 = __ldg(t.qhat_inv[0]), w0s = __ldg(t.qhat_inv_sh[0]);
         const u64 w1 = __ldg(t.qhat_modp[0]), w1s = __ldg(t.qhat_modp_sh[0]);
 #pragma unroll
         for (uint32_t k = 0; k < kPer; ++k) {
-            const uint32_t e = padix(pos<LOGN>(k));
+            const uint32_t e = padix(lpos<LOGN>(k));
             W[e] = csub(mul_shoup_lazy(mul_shoup(W[e], w0, w0s, q), w1, w1s, p), p);
         }
     }
     __syncthreads();
-    fwd_ntt<LOGN>(W, t.pt, t.p_base, pp);
+    fwd_ntt<LOGN, 0>(W, t.pt, t.p_base, pp);
     // inner product at P
     {
         const u64 kofs = (u64)a.key_pbase * N;
@@ -239,14 +423,14 @@ __device__ __forceinline__ void ks_one_limb(const KsFusedArgs& a, u64* W, u64* A
         for (uint32_t c = 0; c < kPer; c += kChunk) {
             u64 d[kChunk], rb[kChunk], ra[kChunk];
 #pragma unroll
-            for (uint32_t k = 0; k < kChunk; ++k) d[k] = W[padix(pos<LOGN>(c + k))];
+            for (uint32_t k = 0; k < kChunk; ++k) d[k] = W[padix(lpos<LOGN>(c + k))];
             if (PREP) {
                 ulonglong2 vb[kChunk], va[kChunk];
 #pragma unroll
                 for (uint32_t k = 0; k < kChunk; ++k) {
-                    const uint32_t x = pos<LOGN>(c + k);
-                    vb[k] = __ldg(a.prep + a.prep_b + kofs + x);
-                    va[k] = __ldg(a.prep + kofs + x);
+                    const uint32_t x = lpos<LOGN>(c + k);
+                    vb[k] = __ldg(ek.prep + a.prep_b + kofs + x);
+                    va[k] = __ldg(ek.prep + kofs + x);
                 }
 #pragma unroll
                 for (uint32_t k = 0; k < kChunk; ++k) {
@@ -257,9 +441,9 @@ __device__ __forceinline__ void ks_one_limb(const KsFusedArgs& a, u64* W, u64* A
                 u64 vb[kChunk], va[kChunk];
 #pragma unroll
                 for (uint32_t k = 0; k < kChunk; ++k) {
-                    const uint32_t x = pos<LOGN>(c + k);
-                    vb[k] = __ldg(a.key + a.evk_b + kofs + x);
-                    va[k] = __ldg(a.key + a.evk_a + kofs + x);
+                    const uint32_t x = lpos<LOGN>(c + k);
+                    vb[k] = __ldg(key + a.evk_b + kofs + x);
+                    va[k] = __ldg(key + a.evk_a + kofs + x);
                 }
 #pragma unroll
                 for (uint32_t k = 0; k < kChunk; ++k) {
@@ -269,27 +453,27 @@ __device__ __forceinline__ void ks_one_limb(const KsFusedArgs& a, u64* W, u64* A
             }
 #pragma unroll
             for (uint32_t k = 0; k < kChunk; ++k) {
-                const uint32_t e = padix(pos<LOGN>(c + k));
+                const uint32_t e = padix(lpos<LOGN>(c + k));
                 A0[e] = rb[k];
                 A1[e] = ra[k];
             }
         }
     }
     __syncthreads();
-    ntt2<true, LOGN>(A0, A1, t.pt, t.p_base, pp);
+    ntt2<true, LOGN, 0>(A0, A1, t.pt, t.p_base, pp);
     // BConv P -> q0 in place on both, then NTT_q0 of both
     {
         const u64 w0 = __ldg(t.phat_inv_modp), w0s = __ldg(t.phat_inv_modp_sh);
         const u64 w1 = __ldg(t.phat_modq), w1s = __ldg(t.phat_modq_sh);
 #pragma unroll
         for (uint32_t k = 0; k < kPer; ++k) {
-            const uint32_t e = padix(pos<LOGN>(k));
+            const uint32_t e = padix(lpos<LOGN>(k));
             A0[e] = csub(mul_shoup_lazy(mul_shoup(A0[e], w0, w0s, p), w1, w1s, q), q);
             A1[e] = csub(mul_shoup_lazy(mul_shoup(A1[e], w0, w0s, p), w1, w1s, q), q);
         }
     }
     __syncthreads();
-    ntt2<false, LOGN>(A0, A1, t.pt, 0, pq);
+    ntt2<false, LOGN, 0>(A0, A1, t.pt, 0, pq);
     // out_h = (in * key_h[q0] - A_h) * P^-1, staged in A_h: the input and the
     // gathered c0 may alias the outputs
     {
@@ -301,7 +485,7 @@ __device__ __forceinline__ void ks_one_limb(const KsFusedArgs& a, u64* W, u64* A
             u64 d[kChunk], cv[kChunk], rb[kChunk], ra[kChunk];
 #pragma unroll
             for (uint32_t k = 0; k < kChunk; ++k) {
-                const uint32_t g = gpos(map, pos<LOGN>(c + k));
+                const uint32_t g = gpos(map, lpos<LOGN>(c + k));
                 d[k] = in[g];
                 cv[k] = a.f.has_c0 ? cb[g] : 0;
             }
@@ -309,9 +493,9 @@ __device__ __forceinline__ void ks_one_limb(const KsFusedArgs& a, u64* W, u64* A
                 ulonglong2 vb[kChunk], va[kChunk];
 #pragma unroll
                 for (uint32_t k = 0; k < kChunk; ++k) {
-                    const uint32_t x = pos<LOGN>(c + k);
-                    vb[k] = __ldg(a.prep + a.prep_b + x);
-                    va[k] = __ldg(a.prep + x);
+                    const uint32_t x = lpos<LOGN>(c + k);
+                    vb[k] = __ldg(ek.prep + a.prep_b + x);
+                    va[k] = __ldg(ek.prep + x);
                 }
 #pragma unroll
                 for (uint32_t k = 0; k < kChunk; ++k) {
@@ -322,9 +506,9 @@ __device__ __forceinline__ void ks_one_limb(const KsFusedArgs& a, u64* W, u64* A
                 u64 vb[kChunk], va[kChunk];
 #pragma unroll
                 for (uint32_t k = 0; k < kChunk; ++k) {
-                    const uint32_t x = pos<LOGN>(c + k);
-                    vb[k] = __ldg(a.key + a.evk_b + x);
-                    va[k] = __ldg(a.key + a.evk_a + x);
+                    const uint32_t x = lpos<LOGN>(c + k);
+                    vb[k] = __ldg(key + a.evk_b + x);
+                    va[k] = __ldg(key + a.evk_a + x);
                 }
 #pragma unroll
                 for (uint32_t k = 0; k < kChunk; ++k) {
@@ -334,7 +518,7 @@ __device__ __forceinline__ void ks_one_limb(const KsFusedArgs& a, u64* W, u64* A
             }
 #pragma unroll
             for (uint32_t k = 0; k < kChunk; ++k) {
-                const uint32_t e = padix(pos<LOGN>(c + k));
+                const uint32_t e = padix(lpos<LOGN>(c + k));
                 u64 r0 = mul_shoup(sub_mod(rb[k], canon4(A0[e], q), q), pinv, pinv_sh, q);
                 const u64 r1 = mul_shoup(sub_mod(ra[k], canon4(A1[e], q), q), pinv, pinv_sh, q);
                 if (a.f.has_c0) r0 = add_mod(r0, cv[k], q);
@@ -354,13 +538,13 @@ __device__ __forceinline__ void ks_one_limb(const KsFusedArgs& a, u64* W, u64* A
             u64 e0[kChunk], e1[kChunk];
 #pragma unroll
             for (uint32_t k = 0; k < kChunk; ++k) {
-                const uint32_t x = pos<LOGN>(c + k);
+                const uint32_t x = lpos<LOGN>(c + k);
                 e0[k] = a.f.has_acc ? x0[x] : 0;
                 e1[k] = a.f.has_acc ? x1[x] : 0;
             }
 #pragma unroll
             for (uint32_t k = 0; k < kChunk; ++k) {
-                const uint32_t x = pos<LOGN>(c + k);
+                const uint32_t x = lpos<LOGN>(c + k);
                 u64 r0 = A0[padix(x)], r1 = A1[padix(x)];
                 if (a.f.has_acc) {
                     r0 = add_mod(r0, e0[k], q);
@@ -373,21 +557,26 @@ __device__ __forceinline__ void ks_one_limb(const KsFusedArgs& a, u64* W, u64* A
     }
 }
 
-template <int LOGN, bool PREP>
-__global__ void __launch_bounds__((1u << LOGN) / 8, 1) ks_fused_kernel(const KsFusedArgs a) {
-    constexpr uint32_t N = 1u << LOGN;
-    constexpr uint32_t PADN = N + N / 16;
+template <int LOGQ, int LOGCL, bool PREP>
+__global__ void __launch_bounds__((1u << LOGQ) / 8, 1) ks_fused_kernel(const KsFusedArgs a) {
+    using G = Geo<LOGQ, LOGCL>;
+    constexpr int LOGN = G::LOGN;
+    constexpr uint32_t PADQ = G::QN + G::QN / 16;
     extern __shared__ u64 smem[];
     u64* W = smem;
-    u64* A0 = smem + PADN;
-    u64* A1 = smem + 2 * PADN;
-    const uint32_t z = blockIdx.x;
+    u64* A0 = smem + PADQ;
+    u64* A1 = smem + 2 * PADQ;
+    const uint32_t z = G::z();
+    const uint32_t x0 = G::rank() * G::QN;
     const OpTabs& t = a.t;
     const uint32_t l = a.sizeQl, K = a.K;
-    const uint32_t* map = a.f.map;
-    if (l == 1 && K == 1) {
-        ks_one_limb<LOGN, PREP>(a, W, A0, A1);
-        return;
+    const EntryKey ek = entry_key(a, z);
+    const uint32_t* map = ek.map;
+    if constexpr (LOGCL == 0) {
+        if (l == 1 && K == 1) {
+            ks_one_limb<LOGN, PREP>(a, ek, W, A0, A1);
+            return;
+        }
     }
     const u64* in = a.arena + a.in.at(z);
     u64* coef = a.scratch + a.mid.at(z);          // l limbs
@@ -401,14 +590,14 @@ __global__ void __launch_bounds__((1u << LOGN) / 8, 1) ks_fused_kernel(const KsF
             uint32_t g[kPer];
             u64 v[kPer];
 #pragma unroll
-            for (uint32_t k = 0; k < kPer; ++k) g[k] = gpos(map, pos<LOGN>(k));
+            for (uint32_t k = 0; k < kPer; ++k) g[k] = gpos(map, x0 + lpos<LOGQ>(k));
 #pragma unroll
             for (uint32_t k = 0; k < kPer; ++k) v[k] = src[g[k]];
 #pragma unroll
-            for (uint32_t k = 0; k < kPer; ++k) W[padix(pos<LOGN>(k))] = v[k];
+            for (uint32_t k = 0; k < kPer; ++k) W[padix(lpos<LOGQ>(k))] = v[k];
         }
         __syncthreads();
-        inv_ntt<LOGN>(W, t.pt, i, pc);
+        inv_ntt<LOGQ, LOGCL>(W, t.pt, i, pc);
         // stored times qHatInv: the first factor of ModUp's base conversion,
         // once per limb instead of once per output slot
         {
@@ -416,23 +605,23 @@ __global__ void __launch_bounds__((1u << LOGN) / 8, 1) ks_fused_kernel(const KsF
             const u64 w0 = __ldg(t.qhat_inv[part] + idx), w0s = __ldg(t.qhat_inv_sh[part] + idx);
 #pragma unroll
             for (uint32_t k = 0; k < kPer; ++k)
-                coef[((u64)i << LOGN) + pos<LOGN>(k)] = mul_shoup(W[padix(pos<LOGN>(k))], w0, w0s, pc.q);
+                coef[((u64)i << LOGN) + x0 + lpos<LOGQ>(k)] = mul_shoup(W[padix(lpos<LOGQ>(k))], w0, w0s, pc.q);
         }
         __syncthreads();
     }
     // phase 1: special slots -> INTT of both accumulators
     for (uint32_t k = 0; k < K; ++k) {
-        mac_slot<LOGN, PREP>(a, l + k, W, A0, A1, in, coef);
+        mac_slot<LOGQ, LOGCL, PREP>(a, ek, l + k, W, A0, A1, in, coef);
         const uint32_t prime = t.p_base + k;
         const PrimeConst pc = t.pt.pc[prime];
-        ntt2<true, LOGN>(A0, A1, t.pt, prime, pc);
-        u64* d0 = pcoef + ((u64)(2 * k) << LOGN);
-        u64* d1 = pcoef + ((u64)(2 * k + 1) << LOGN);
+        ntt2<true, LOGQ, LOGCL>(A0, A1, t.pt, prime, pc);
+        u64* d0 = pcoef + ((u64)(2 * k) << LOGN) + x0;
+        u64* d1 = pcoef + ((u64)(2 * k + 1) << LOGN) + x0;
         // stored times PHatInv_k: the first factor of ModDown's base conversion
         const u64 w0 = __ldg(t.phat_inv_modp + k), w0s = __ldg(t.phat_inv_modp_sh + k);
 #pragma unroll
         for (uint32_t e = 0; e < kPer; ++e) {
-            const uint32_t x = pos<LOGN>(e);
+            const uint32_t x = lpos<LOGQ>(e);
             d0[x] = mul_shoup(A0[padix(x)], w0, w0s, pc.q);
             d1[x] = mul_shoup(A1[padix(x)], w0, w0s, pc.q);
         }
@@ -443,7 +632,7 @@ __global__ void __launch_bounds__((1u << LOGN) / 8, 1) ks_fused_kernel(const KsF
     const u64 c0 = a.f.has_c0 ? a.f.c0.at(z) : 0;
     const u64 ac0 = a.f.has_acc ? a.f.acc0.at(z) : 0, ac1 = a.f.has_acc ? a.f.acc1.at(z) : 0;
     for (uint32_t i = 0; i < l; ++i) {
-        mac_slot<LOGN, PREP>(a, i, W, A0, A1, in, coef);
+        mac_slot<LOGQ, LOGCL, PREP>(a, ek, i, W, A0, A1, in, coef);
         const PrimeConst pc = t.pt.pc[i];
         const u64 q = pc.q, q2 = q << 1;
         const u64 pinv = __ldg(t.p_inv_mod_q + i), pinv_sh = __ldg(t.p_inv_mod_q_sh + i);
@@ -456,10 +645,10 @@ __global__ void __launch_bounds__((1u << LOGN) / 8, 1) ks_fused_kernel(const KsF
                 for (uint32_t e = 0; e < kPer; ++e) acc[e] = 0;
                 for (uint32_t k = 0; k < K; ++k) {
                     const u64 w1 = __ldg(t.phat_modq + k * l + i), w1s = __ldg(t.phat_modq_sh + k * l + i);
-                    const u64* src = pcoef + ((u64)(2 * k + h) << LOGN);   // [x * PHatInv]_{p_k} (phase 1)
+                    const u64* src = pcoef + ((u64)(2 * k + h) << LOGN) + x0;   // [x * PHatInv]_{p_k} (phase 1)
                     u64 v[kPer];
 #pragma unroll
-                    for (uint32_t e = 0; e < kPer; ++e) v[e] = src[pos<LOGN>(e)];
+                    for (uint32_t e = 0; e < kPer; ++e) v[e] = src[lpos<LOGQ>(e)];
 #pragma unroll
                     for (uint32_t e = 0; e < kPer; ++e) {
                         acc[e] += mul_shoup_lazy(v[e], w1, w1s, q);
@@ -467,29 +656,30 @@ __global__ void __launch_bounds__((1u << LOGN) / 8, 1) ks_fused_kernel(const KsF
                     }
                 }
 #pragma unroll
-                for (uint32_t e = 0; e < kPer; ++e) W[padix(pos<LOGN>(e))] = csub(acc[e], q);
+                for (uint32_t e = 0; e < kPer; ++e) W[padix(lpos<LOGQ>(e))] = csub(acc[e], q);
             }
             __syncthreads();
-            fwd_ntt<LOGN>(W, t.pt, i, pc);
+            fwd_ntt<LOGQ, LOGCL>(W, t.pt, i, pc);
             // (x_Q - y) * P^-1 plus the fused extras. The gathered c0 limb i
-            // is staged in A and stored after a barrier (c0 may alias out0);
+            // is staged in A and stored after a barrier over every CTA of the
+            // polynomial (c0 may alias out0, and the gather reads any slice);
             // every other output goes straight out (each element is read and
             // written by the same thread).
             const bool stage = h == 0 && a.f.has_c0;
-            const u64 ob = (h ? o1 : o0) + ((u64)i << LOGN);
-            const u64 ab = (h ? ac1 : ac0) + ((u64)i << LOGN);
+            const u64 ob = (h ? o1 : o0) + ((u64)i << LOGN) + x0;
+            const u64 ab = (h ? ac1 : ac0) + ((u64)i << LOGN) + x0;
             const u64* cb = a.arena + c0 + ((u64)i << LOGN);
 #pragma unroll
             for (uint32_t c = 0; c < kPer; c += kChunk) {
                 u64 ex[kChunk];
 #pragma unroll
                 for (uint32_t e = 0; e < kChunk; ++e) {
-                    const uint32_t x = pos<LOGN>(c + e);
-                    ex[e] = stage ? cb[gpos(map, x)] : (a.f.has_acc ? a.arena[ab + x] : 0);
+                    const uint32_t x = lpos<LOGQ>(c + e);
+                    ex[e] = stage ? cb[gpos(map, x0 + x)] : (a.f.has_acc ? a.arena[ab + x] : 0);
                 }
 #pragma unroll
                 for (uint32_t e = 0; e < kChunk; ++e) {
-                    const uint32_t x = pos<LOGN>(c + e);
+                    const uint32_t x = lpos<LOGQ>(c + e);
                     // A may be lazy in [0, 2q): the difference is then in
                     // [0, 2q) and mul_shoup returns it canonical
                     u64 r = mul_shoup(sub_mod(A[padix(x)], canon4(W[padix(x)], q), q), pinv, pinv_sh, q);
@@ -499,15 +689,15 @@ __global__ void __launch_bounds__((1u << LOGN) / 8, 1) ks_fused_kernel(const KsF
                 }
             }
             if (stage) {
-                __syncthreads();
+                G::sync_all();
 #pragma unroll
                 for (uint32_t c = 0; c < kPer; c += kChunk) {
                     u64 ex[kChunk];
 #pragma unroll
-                    for (uint32_t e = 0; e < kChunk; ++e) ex[e] = a.f.has_acc ? a.arena[ab + pos<LOGN>(c + e)] : 0;
+                    for (uint32_t e = 0; e < kChunk; ++e) ex[e] = a.f.has_acc ? a.arena[ab + lpos<LOGQ>(c + e)] : 0;
 #pragma unroll
                     for (uint32_t e = 0; e < kChunk; ++e) {
-                        const uint32_t x = pos<LOGN>(c + e);
+                        const uint32_t x = lpos<LOGQ>(c + e);
                         u64 r = A[padix(x)];
                         if (a.f.has_acc) r = add_mod(r, ex[e], q);
                         a.arena[ob + x] = r;
@@ -519,21 +709,68 @@ __global__ void __launch_bounds__((1u << LOGN) / 8, 1) ks_fused_kernel(const KsF
     }
 }
 
-template <int LOGN, bool PREP>
+template <int LOGQ, int LOGCL, bool PREP>
 cudaError_t launch_fused_v(const KsFusedArgs& a, uint32_t nz, cudaStream_t st) {
-    constexpr uint32_t N = 1u << LOGN;
-    const size_t smem = 3ull * (N + N / 16) * sizeof(u64);
-    auto kern = ks_fused_kernel<LOGN, PREP>;
+    constexpr uint32_t QN = 1u << LOGQ;
+    const size_t smem = 3ull * (QN + QN / 16) * sizeof(u64);
+    auto kern = ks_fused_kernel<LOGQ, LOGCL, PREP>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    kern<<<nz, N / 8, smem, st>>>(a);
+    if constexpr (LOGCL == 0) {
+        kern<<<nz, QN / 8, smem, st>>>(a);
+    } else {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(nz << LOGCL, 1, 1);
+        cfg.blockDim = dim3(QN / 8, 1, 1);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = 1u << LOGCL;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        e = cudaLaunchKernelEx(&cfg, kern, a);
+        if (e != cudaSuccess) return e;
+    }
     count_launches(1);
     return cudaGetLastError();
 }
 
-template <int LOGN>
+template <int LOGQ, int LOGCL>
 cudaError_t launch_fused(const KsFusedArgs& a, uint32_t nz, cudaStream_t st) {
-    return a.prep ? launch_fused_v<LOGN, true>(a, nz, st) : launch_fused_v<LOGN, false>(a, nz, st);
+    return a.prep ? launch_fused_v<LOGQ, LOGCL, true>(a, nz, st) : launch_fused_v<LOGQ, LOGCL, false>(a, nz, st);
+}
+
+// Clusters the GPU can hold at once for the kernel at N = 2^(13 + logcl)
+// (0 when it cannot place even one: the multi-kernel path is used then).
+template <int LOGCL>
+int cluster_capacity() {
+    constexpr uint32_t QN = 1u << kLogQ;
+    const size_t smem = 3ull * (QN + QN / 16) * sizeof(u64);
+    auto kern = ks_fused_kernel<kLogQ, LOGCL, true>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(1u << LOGCL, 1, 1);
+    cfg.blockDim = dim3(QN / 8, 1, 1);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 1u << LOGCL;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int n = 0;
+    if (cudaOccupancyMaxActiveClusters(&n, kern, &cfg) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
 }
 
 __global__ void key_prep_kernel(const u64* __restrict__ key, ulonglong2* __restrict__ prep,
@@ -547,7 +784,15 @@ __global__ void key_prep_kernel(const u64* __restrict__ key, ulonglong2* __restr
 
 }  // namespace
 
-bool key_switch_fused_supported(int log_n) { return log_n >= 10 && log_n <= 13; }
+bool key_switch_fused_supported(int log_n) {
+    if (log_n >= 10 && log_n <= 13) return true;
+    switch (log_n) {
+    case 14: return cluster_capacity<1>() > 0;
+    case 15: return cluster_capacity<2>() > 0;
+    case 16: return cluster_capacity<3>() > 0;
+    default: return false;
+    }
+}
 
 size_t ks_fused_scratch_words(uint32_t n, uint32_t sizeQl, uint32_t K) { return (size_t)n * (sizeQl + 2 * K); }
 
@@ -585,10 +830,13 @@ cudaError_t launch_key_switch_fused(int log_n, const OpTabs& t, uint32_t sizeQl,
     a.prep = prep;
     a.prep_b = evk_b - evk_a;
     switch (log_n) {
-    case 10: return launch_fused<10>(a, nz, st);
-    case 11: return launch_fused<11>(a, nz, st);
-    case 12: return launch_fused<12>(a, nz, st);
-    case 13: return launch_fused<13>(a, nz, st);
+    case 10: return launch_fused<10, 0>(a, nz, st);
+    case 11: return launch_fused<11, 0>(a, nz, st);
+    case 12: return launch_fused<12, 0>(a, nz, st);
+    case 13: return launch_fused<13, 0>(a, nz, st);
+    case 14: return launch_fused<kLogQ, 1>(a, nz, st);
+    case 15: return launch_fused<kLogQ, 2>(a, nz, st);
+    case 16: return launch_fused<kLogQ, 3>(a, nz, st);
     default: return cudaErrorInvalidValue;
     }
 }

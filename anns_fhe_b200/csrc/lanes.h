@@ -68,5 +68,10 @@ inline ZField lane_field(const afhe_ctx* c, u64 Lane::*member) {
 // Field for per-ciphertext offsets vals[0..n): strided when they form an
 // arithmetic progression, else staged through the context's descriptor ring.
 int zf_from(afhe_ctx* ctx, const u64* vals, uint32_t n, ZField* out);
+// Copy `words` words through the context's pinned descriptor ring to device
+// memory, enqueued on the context stream; *dev stays valid for the work
+// enqueued after it (the ring reuses a segment only once the stream has
+// passed it).
+int ring_put(afhe_ctx* ctx, const void* src, size_t words, u64** dev);
 
 }  // namespace afhe

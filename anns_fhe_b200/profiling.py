@@ -1,0 +1,287 @@
+"""Measurement helpers and profiling drivers (the commands `profiles/` quotes).
+
+* `ks_roofline`: the dominant operation of a query step, a rotation key
+  switch over a batch of ciphertexts at the chain's evaluation shape, timed
+  alone with CUDA events on the context stream; its algorithmic bytes and
+  the achieved fraction of the HBM peak.
+* drivers for ncu captures, each a plain program whose launches are easy to
+  count: `python -m anns_fhe_b200.profiling ks|ntt|step|host ...`.
+
+Algorithmic bytes of one rotation key switch per ciphertext: c0 and c1 read,
+both outputs written (4 x l limbs of N words); the rotation key (2 x dnum x
+(l + K) limbs, the digits this level reads) once per launch.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import time
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+# DRAM traffic and integer-pipe use of the key switch from ncu captures of the
+# current kernels (`--set full`, clocks not locked), per (N, l, K): the
+# traffic of one launch sequence per ciphertext (its scratch and I/O grow with
+# the ciphertexts), the key's bytes read once, the kernel, and the busiest
+# integer pipe's utilisation. The captures are summarised under profiles/.
+KS_CAPTURES: dict = {
+    (8192, 3, 1): {"kernel": "ks_fused_kernel<13, 1>", "ciphertexts": 148, "dram_bytes": 175.3e6,
+                   "fmaheavy": 0.580},
+}
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        d = json.load(open(path))
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ks_roofline(params, lanes: int, reps: int = 20, level: int = 0, nbuf: int = 5):
+    """One rotation step (a key switch with the automorphism folded into its
+    loads) of `lanes` ciphertexts at `level` limbs per call, `nbuf` input
+    batches cycled so the inputs stream from HBM; `reps` calls timed with
+    CUDA events on the context stream after `nbuf` warm-up calls."""
+    import numpy as np
+    import torch
+
+    from ._lib import CtRef
+    from .driver import FheContext
+    p = params
+    n, K = p.n, p.K
+    L = level or p.L
+    w = L * n
+    kw = p.key_words()
+    ctx = FheContext(p, poly_words=(nbuf + 1) * lanes * 2 * w, key_words=kw, max_batch=lanes,
+                     device=torch.cuda.current_device())
+    try:
+        rng = np.random.default_rng(3)
+        allp = p.q + p.p
+        ctx.write_key(0, np.concatenate([rng.integers(0, q, n, dtype=np.uint64) for _ in range(2 * p.dnum)
+                                         for q in allp]))
+        ctx.lib.afhe_add_rotation_key(ctx.h, 1, 0)
+        limb = np.concatenate([rng.integers(0, q, n, dtype=np.uint64) for q in p.q[:L]])
+        for i in range((nbuf + 1) * lanes * 2):
+            ctx.write_poly(i * w, limb)
+
+        def refs(first):
+            arr = (CtRef * lanes)()
+            for i in range(lanes):
+                arr[i].c0_offset, arr[i].c1_offset = (first + 2 * i) * w, (first + 2 * i + 1) * w
+            return arr
+        ins = [refs(b * lanes * 2) for b in range(nbuf)]
+        out = refs(nbuf * lanes * 2)
+        st = torch.cuda.ExternalStream(ctx.lib.afhe_stream(ctx.h), device=torch.cuda.current_device())
+        for b in range(nbuf):
+            ctx.lib.afhe_eval_rotate_batch(ctx.h, ins[b], out, lanes, 1, L)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = ctx.lib.afhe_kernel_launches()
+        e0.record(st)
+        for r in range(reps):
+            ctx.lib.afhe_eval_rotate_batch(ctx.h, ins[r % nbuf], out, lanes, 1, L)
+        e1.record(st)
+        e1.synchronize()
+        launches = (ctx.lib.afhe_kernel_launches() - l0) / reps
+        ms = e0.elapsed_time(e1) / reps
+        fused = int(ctx.get_option(1))
+    finally:
+        ctx.close()
+    parts = -(-L // p.alpha)
+    key_bytes = 2 * parts * (L + K) * n * 8
+    bytes_per_call = lanes * 4 * w * 8 + key_bytes
+    achieved = bytes_per_call / (ms * 1e-3) / 1e9
+    peak, src = load_peaks()
+    cap = KS_CAPTURES.get((n, L, K))
+    traffic = int_pipe = None
+    if cap and launches == 1 and fused:
+        # the capture's per-ciphertext traffic scaled to this launch, the key once
+        traffic = (cap["dram_bytes"] - key_bytes) * lanes / cap["ciphertexts"] + key_bytes
+        int_pipe = {"pipe": "fmaheavy (IMAD)", "frac": cap["fmaheavy"], "kernel": cap["kernel"]}
+    kind = "one-kernel" if fused and launches == 1 else f"{launches:g}-launch"
+    return {"bound": "hbm", "kernel": f"rotation key switch, {kind} (N={n}, {L} + {K} limbs, "
+                                      f"{lanes} ciphertexts per call)",
+            "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "peak_source": src, "traffic": traffic, "ms_per_call": ms, "launches_per_call": launches,
+            "algorithmic_bytes_per_call": bytes_per_call, "int_pipe": int_pipe}
+
+
+# ---------------------------------------------------------------------------
+# profiling drivers
+# ---------------------------------------------------------------------------
+def profile_ks(lanes: int, workload: str = "small", level: int = 0):
+    """The roofline measurement of the key switch alone (five warm-up calls,
+    then 20 measured) at `level` limbs (default: the workload's evaluation
+    level)."""
+    from .driver import CkksParams
+    from .workloads import LARGE, SMALL
+    spec = LARGE if workload == "large" else SMALL
+    p = CkksParams.generate(spec.log_n, spec.num_q, spec.q_bits, spec.num_p, spec.p_bits, spec.alpha)
+    print(json.dumps(ks_roofline(p, lanes, level=level or spec.eval_level or spec.num_q)))
+
+
+def profile_step(nq: int, workload: str = "small", lanes: int = 0):
+    """One warm step, then one measured step of `nq` queries. Prints the
+    kernel-launch counts an ncu launch list needs (-s / -c)."""
+    from .workloads import LARGE, SMALL, Workload
+    wl = Workload(LARGE if workload == "large" else SMALL, max_queries=nq, lanes=lanes or nq)
+    lib = wl.ctx.lib
+    recs = wl.records[:nq]
+    wl.encrypt_queries(wl.queries(nq, seed=7), recs)
+
+    def step():
+        wl.iqm.stage1_coarse(recs)
+        wl.select(recs)
+        wl.iqm.stage3_fine(recs)
+        wl.ctx.sync()
+    step()
+    a = lib.afhe_kernel_launches()
+    t = time.time()
+    step()
+    print(f"WARM_LAUNCHES={a} STEP_LAUNCHES={lib.afhe_kernel_launches() - a} step_s={time.time() - t:.3f}")
+    wl.close()
+
+
+def profile_ntt(polys: int, log_n: int = 13, reps: int = 10):
+    """Batched in-place NTT / INTT over `polys` polynomials of 4 limbs (the
+    key switch's shape), forward then inverse, `reps` each."""
+    import ctypes as C
+
+    import numpy as np
+    import torch
+
+    from ._lib import P64
+    from .driver import CkksParams, FheContext
+    prm = CkksParams.generate(log_n, 3, 50, 1, 60, 1)
+    n, limbs = prm.n, 4
+    ctx = FheContext(prm, poly_words=polys * limbs * n, key_words=1024)
+    rng = np.random.default_rng(1)
+    limb_data = np.concatenate([rng.integers(0, q, n, dtype=np.uint64) for q in prm.q + prm.p])
+    for b in range(polys):
+        ctx.write_poly(b * limbs * n, limb_data)
+    offs = (C.c_uint64 * polys)(*[b * limbs * n for b in range(polys)])
+    lib = ctx.lib
+    st = torch.cuda.ExternalStream(lib.afhe_stream(ctx.h))
+    for inv in (0, 1):
+        lib.afhe_ntt_batch(ctx.h, C.cast(offs, P64), polys, limbs, inv)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(reps):
+            lib.afhe_ntt_batch(ctx.h, C.cast(offs, P64), polys, limbs, inv)
+        e1.record(st)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        gb = 2 * polys * limbs * n * 8 / 1e9
+        print(f"log_n={log_n} inverse={inv} {polys}x{limbs} limbs: {ms * 1e3:.1f} us per launch, "
+              f"{gb / (ms * 1e-3):.0f} GB/s")
+    ctx.close()
+
+
+def profile_host(batch: int = 296, steps: int = 5):
+    """The end-to-end path on the host: (1) one batch through the protocol one
+    phase at a time, each phase followed by a synchronisation, its wall time
+    averaged over `steps` steps; (2) the streamed end-to-end run under
+    cProfile, the host functions with the most own time. One JSON line each."""
+    import cProfile
+    import pstats
+
+    import numpy as np
+    import torch
+
+    from ._lib import P64, check
+    from .workloads import SMALL, Workload
+    wl = Workload(SMALL, max_queries=2 * batch, lanes=batch)
+    iqm = wl.iqm
+    recs = wl.records[:batch]
+    wl.encrypt_queries(wl.queries(batch, seed=1000), recs)
+    Lw = wl.params.L * wl.params.n
+    host = [[torch.from_numpy(wl.ctx.read_poly(o, Lw)).pin_memory().numpy() for o in (*r.ct_query, *r.ct_dim)]
+            for r in recs]
+    dec = wl.client.decryptor(batch * max(1, iqm.n_res))
+    phases: dict = {}
+
+    def mark(name, t0):
+        wl.ctx.sync()
+        t = time.perf_counter()
+        phases[name] = phases.get(name, 0.0) + (t - t0) * 1e3
+        return t
+
+    def phased_step():
+        t = time.perf_counter()
+        for r, cts in zip(recs, host):
+            for off, a in zip((*r.ct_query, *r.ct_dim), cts):
+                check(wl.ctx.lib.afhe_write_poly_async(wl.ctx.h, off, a.ctypes.data_as(P64), a.size), "write")
+        t = mark("h2d", t)
+        iqm.stage1_coarse(recs)
+        t = mark("stage1", t)
+        box = iqm.read_results("compact", recs, staged=True)[:, 0]
+        t = mark("d2h_coarse", t)
+        coef = dec.decrypt_host_batch_coef(box, 1)
+        t = mark("client_decrypt_coarse", t)
+        vals = dec.enc.decode_real_batch(coef, iqm.out_scale, iqm.coarse_slots_needed())
+        for r, c in zip(recs, iqm.coarse_from_slots(vals)):
+            r.probes = list(np.argsort(c, kind="stable")[:wl.spec.nprobe])
+        t = mark("client_decode_select", t)
+        iqm.stage3_fine(recs)
+        t = mark("stage3", t)
+        fbox = iqm.read_results("dists", recs, staged=True)
+        t = mark("d2h_dists", t)
+        wl._group_topk(recs, (fbox, wl.ctx.fence(), 0), dec)
+        mark("client_decrypt_decode_topk", t)
+
+    for _ in range(2):
+        phased_step()
+    phases.clear()
+    for _ in range(steps):
+        phased_step()
+    total = sum(phases.values()) / steps
+    print(json.dumps({"profile": "phases", "queries_per_step": batch,
+                      "ms": {k: round(v / steps, 2) for k, v in phases.items()}, "total_ms": round(total, 2),
+                      "queries_per_s": round(batch / total * 1e3, 1)}), flush=True)
+    wl.run_host_stream(wl.records, host, dec, 2 * batch, batch // 2)
+    pr = cProfile.Profile()
+    t = time.perf_counter()
+    pr.enable()
+    wl.run_host_stream(wl.records, host, dec, steps * batch, batch // 2)
+    pr.disable()
+    wall = time.perf_counter() - t
+    st = pstats.Stats(pr)
+    rows = sorted(st.stats.items(), key=lambda kv: -kv[1][2])[:15]
+    print(json.dumps({"profile": "stream_cprofile", "queries": steps * batch, "wall_s": round(wall, 3),
+                      "queries_per_s_under_profiler": round(steps * batch / wall, 1),
+                      "top_own_time": [{"fn": f"{os.path.basename(k[0])}:{k[1]}({k[2]})", "calls": v[1],
+                                        "own_ms": round(v[2] * 1e3, 1), "cum_ms": round(v[3] * 1e3, 1)}
+                                       for k, v in rows]}), flush=True)
+    wl.close()
+
+
+def main() -> None:
+    ap = argparse.ArgumentParser(prog="python -m anns_fhe_b200.profiling")
+    sub = ap.add_subparsers(dest="what", required=True)
+    a = sub.add_parser("ks", help="rotation key switch alone: ciphertexts per call")
+    a.add_argument("lanes", type=int)
+    a.add_argument("--workload", default="small", choices=["small", "large"])
+    a.add_argument("--level", type=int, default=0)
+    a = sub.add_parser("ntt", help="batched NTT / INTT: polynomials per launch")
+    a.add_argument("polys", type=int)
+    a.add_argument("--log-n", type=int, default=13)
+    a = sub.add_parser("step", help="one query step: queries per step")
+    a.add_argument("queries", type=int)
+    a.add_argument("--workload", default="small", choices=["small", "large"])
+    a.add_argument("--lanes", type=int, default=0)
+    sub.add_parser("host", help="end-to-end phases and the streamed run's host hotspots")
+    args = ap.parse_args()
+    if args.what == "ks":
+        profile_ks(args.lanes, args.workload, args.level)
+    elif args.what == "ntt":
+        profile_ntt(args.polys, args.log_n)
+    elif args.what == "step":
+        profile_step(args.queries, args.workload, args.lanes)
+    else:
+        profile_host()
+
+
+if __name__ == "__main__":
+    main()

@@ -172,25 +172,16 @@ class InteractiveQueryManager:
             vals[k, j * D:(j + 1) * D] = index.centroids[c]
         encode_plaintexts(ctx, self.enc, vals, shape.scale, self.pt_centroid_cts, L)
         assert shape.eval_level is None or 3 <= shape.eval_level <= L, "eval_level must be in [3, L]"
-        self.levels = sorted({self.eval_at(lv) for lv in set(levels or [L]) | {L}})
+        self._query_levels = set(levels or [L]) | {L}
+        self._bound = bound
+        self.levels = sorted({self.eval_at(lv) for lv in self._query_levels})
         assert all(3 <= lv <= L for lv in self.levels), "query levels must be in [3, L]"
-        for lv in self.levels:
-            assert bound * self.out_scale_at(lv) * 4 < self.p.q[0] / 2, "results would not decrypt from limb 0"
         self._onehot: dict[int, list[int]] = {}      # level -> one-hot masks (reference compaction)
         self._stride: dict[int, int] = {}             # level -> centroid-slot mask (packed compaction)
         self._prefix_lv: dict[tuple[int, int], int] = {}
+        self._counts: list[int] = []
         for lv in self.levels:
-            ms = float(self.p.q[lv - 2])
-            if shape.compaction == "reference":
-                m = np.zeros((shape.n_list, S))
-                m[np.arange(shape.n_list), np.arange(shape.n_list) * D] = 1.0
-                self._onehot[lv] = slots.take(shape.n_list)
-                encode_plaintexts(ctx, self.enc, m, ms, self._onehot[lv], lv - 1)
-            else:
-                m = np.zeros((1, S))
-                m[0, np.arange(shape.per_ct) * D] = 1.0
-                self._stride[lv] = slots.take(1)[0]
-                encode_plaintexts(ctx, self.enc, m, ms, [self._stride[lv]], lv - 1)
+            self._level_masks(lv)
         top = self.levels[-1]                  # the level top-level queries are evaluated at
         self.mask_onehot = self._onehot.get(top, [])
         if shape.compaction == "packed":
@@ -218,15 +209,9 @@ class InteractiveQueryManager:
             self.batches.append(out)
         if vals:
             encode_plaintexts(ctx, self.enc, np.stack(vals), shape.scale, offs, L)
+        self._counts = sorted(counts)
         for lv in self.levels:
-            cs = sorted(counts)
-            m = np.zeros((len(cs), S))
-            for r, cnt in enumerate(cs):
-                m[r, :cnt] = 1.0
-            offs = slots.take(len(cs))
-            encode_plaintexts(ctx, self.enc, m, float(self.p.q[lv - 2]), offs, lv - 1)
-            for cnt, off in zip(cs, offs):
-                self._prefix_lv[(cnt, lv)] = off
+            self._prefix_masks(lv)
         self.mask_prefix = {cnt: self._prefix_lv[(cnt, top)] for cnt in counts}
         # result ciphertexts per query: enough for the largest lists a query may probe
         self.max_nprobe = max(max_nprobe or shape.nprobe, shape.nprobe)
@@ -245,6 +230,47 @@ class InteractiveQueryManager:
             base = slots.take(self.compaction_slots(shape.n_list, L, n, slots.w, self.lanes))[0]
             self.cmp = [[(base + k * per_lane + 2 * i * w, base + k * per_lane + (2 * i + 1) * w)
                          for i in range(shape.n_list - 1)] for k in range(self.lanes)]
+
+    def _level_masks(self, lv: int) -> None:
+        """The compaction masks of level lv, at scale q_{lv-2} (the prime the
+        mask rescale drops)."""
+        sh, S, D = self.sh, self.sh.slots, self.sh.D
+        assert self._bound * self.out_scale_at(lv) * 4 < self.p.q[0] / 2, "results would not decrypt from limb 0"
+        ms = float(self.p.q[lv - 2])
+        if sh.compaction == "reference":
+            m = np.zeros((sh.n_list, S))
+            m[np.arange(sh.n_list), np.arange(sh.n_list) * D] = 1.0
+            self._onehot[lv] = self.slots.take(sh.n_list)
+            encode_plaintexts(self.ctx, self.enc, m, ms, self._onehot[lv], lv - 1)
+        else:
+            m = np.zeros((1, S))
+            m[0, np.arange(sh.per_ct) * D] = 1.0
+            self._stride[lv] = self.slots.take(1)[0]
+            encode_plaintexts(self.ctx, self.enc, m, ms, [self._stride[lv]], lv - 1)
+
+    def _prefix_masks(self, lv: int) -> None:
+        """Masks of the first `count` slots, for every candidate-batch size."""
+        cs = self._counts
+        m = np.zeros((len(cs), self.sh.slots))
+        for r, cnt in enumerate(cs):
+            m[r, :cnt] = 1.0
+        offs = self.slots.take(len(cs))
+        encode_plaintexts(self.ctx, self.enc, m, float(self.p.q[lv - 2]), offs, lv - 1)
+        for cnt, off in zip(cs, offs):
+            self._prefix_lv[(cnt, lv)] = off
+
+    def set_eval_level(self, level: int | None) -> None:
+        """Change the limbs the server evaluates queries at (None: each query's
+        own level). Masks for levels not prepared yet are encoded now (the
+        Workload reserves their slots). Call it between steps, with no query
+        in flight."""
+        assert level is None or 3 <= level <= self.L, "eval_level must be in [3, L]"
+        self.sh.eval_level = level
+        for lv in sorted({self.eval_at(x) for x in self._query_levels}):
+            if lv not in self.levels:
+                self._level_masks(lv)
+                self._prefix_masks(lv)
+                self.levels = sorted(self.levels + [lv])
 
     @staticmethod
     def compaction_slots(n_list: int, L: int, n: int, slot_w: int, lanes: int) -> int:
@@ -422,6 +448,8 @@ class InteractiveQueryManager:
         None restores the context's defaults."""
         self._tuning = choices or {}
         self._opt_now = None
+        if not hasattr(self, "_fused_ok"):
+            self._fused_ok = self.ctx.get_option(L.OPT_KS_FUSED) == 1
 
     def _at(self, level: int) -> None:
         """Apply the tuned options of the level an operator runs at."""
@@ -430,7 +458,7 @@ class InteractiveQueryManager:
             return
         want = (int(ch.fused), int(ch.chunk))
         if want != getattr(self, "_opt_now", None):
-            if self.p.log_n <= 13:
+            if want[0] == 0 or self._fused_ok:
                 self.ctx.set_option(L.OPT_KS_FUSED, want[0])
             self.ctx.set_option(L.OPT_CHUNK, min(want[1], self.ctx.max_batch))
             self._opt_now = want

@@ -120,11 +120,12 @@ def ranked_prefix(vals: np.ndarray, pos, k: int) -> list[np.ndarray]:
 class Workload:
     def __init__(self, spec: WorkloadSpec = SMALL, max_queries: int = 64, lanes: int = 64, device: int = 0,
                  index: IvfPqIndex | None = None, levels=None, max_nprobe: int | None = None,
-                 tune: bool = False):
+                 tune: bool = False, spare_levels: int = 0):
         """levels: query levels to serve besides the top one (mixed-level
         traffic); max_nprobe: the most lists one query may probe; tune: apply
         the autotuner's key-switch choices (cached per GPU and parameter
-        set, measured when absent)."""
+        set, measured when absent); spare_levels: room for the masks of that
+        many more evaluation levels (InteractiveQueryManager.set_eval_level)."""
         self.spec = spec
         t0 = time.time()
         self.X = gaussian_mixture(spec.n_vectors, spec.d, spec.components, spec.sigma, spec.seed)
@@ -148,7 +149,7 @@ class Workload:
         # client staging: results arrive as limb 0 (N words per polynomial)
         dec_slots = -(-most * 2 * n // slot_w) + -(-most * n // slot_w)
         outbox_slots = -(-2 * max_queries * w_out // slot_w) + -(-2 * max_queries * n_res * w_out // slot_w)
-        masks = InteractiveQueryManager.mask_slots(shape, len(lvls), spec.compaction == "reference")
+        masks = InteractiveQueryManager.mask_slots(shape, len(lvls) + spare_levels, spec.compaction == "reference")
         n_slots = (16 + shape.n_coarse + masks + n_batches + 8 * lanes + 4 * max_queries + outbox_slots + 64
                    + InteractiveQueryManager.compaction_slots(spec.n_list if spec.compaction == "reference" else 1,
                                                               self.params.L, n, slot_w, lanes)

@@ -220,7 +220,13 @@ int afhe_ctx_write_context_tables(afhe_ctx* ctx, uint32_t level, afhe_context_la
 /* ---- kernel ABI ------------------------------------------------------------ */
 /* fhe_accel_top (fhe_accel_top.cpp:90-328): one op over the arenas. OP 99 copies
  * the tables named by the offsets from key_gmem into the context (the reference
- * keeps them in static on-chip arrays); ops 1-8 use those loaded tables. */
+ * keeps them in static on-chip arrays); ops 1-8 use those loaded tables.
+ * Ops 1-8 allocate nothing and do not wait: they are enqueued on the context's
+ * stream in call order (their small per-call descriptors go through pinned
+ * staging) and return; afhe_read_poly / afhe_read_key / afhe_sync wait for
+ * them. The reference's fhe_accel_top returns when the op is done; a caller
+ * that reads the device arenas by other means calls afhe_sync first. OP 99,
+ * a one-time set-up, waits for its copies. */
 int afhe_dispatch(afhe_ctx* ctx, const afhe_accel_args* args);
 
 /* ---- key directory (FHEHostDriver m_cfg.relin_key_offset / m_rot_keys) ---- */

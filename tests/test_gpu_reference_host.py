@@ -1,0 +1,135 @@
+"""The reference's own host program drives the GPU through afhe_dispatch.
+
+The reference's SimMemoryBus, FHEHostDriver and InteractiveQueryManager
+(cpp_host_model/src/*.cpp) are compiled verbatim twice (oracle/Makefile):
+once with the reference's HLS fhe_accel_top, the CPU C-simulation, and once
+with anns_fhe_b200/lib/libafhe_accel_top.so, this repository's fhe_accel_top
+symbol over afhe_dispatch (csrc/fhe_accel_top_shim.cpp). Both load the same
+context directory through FHEHostDriver::initialize_context_from_directory
+(fhe_host_driver.cpp:18-175; written by anns_fhe_b200.formats.save_package,
+with the CRT tables beside it where the driver looks for them), get the same
+encrypted query, centroid plaintext and masks in their poly_gmem slots
+(interactive_query_manager.h:17-36), and run the query manager's stage 1
+(interactive_query_manager.cpp:85-119) and stage 1b's loop (:121-178) at the
+reference's own shape: N = 16384, 11 Q limbs (60-bit first, then 45-bit) + 4 P
+limbs, alpha 4. Every word of poly_gmem must then be identical.
+
+The reference's memory map has two collisions, both worked around here
+without touching its code:
+* eval_mult_relin_rescale (fhe_host_driver.cpp:296-305) writes the rescaled
+  c0 and c1, 2 x 10 limbs, from SCRATCH_TMP (0x540000), past
+  SCRATCH_AUTO_MAP (0x580000) where initialize_context_from_directory put the
+  automorphism maps of the first rotation keys it read
+  (fhe_host_driver.cpp:124-137); the next rotation with those keys then
+  gathers through residues instead of indices and reads outside its buffer
+  (the reference's CPU build stops with a segmentation fault). The context
+  directory here lists four rotation keys the chain never uses first, so
+  their maps take the overwritten words;
+* stage 1b's masks 4-7 (SLOT_PT_MASK + (i % 8) x 15N) overlap SCRATCH_D0 ..
+  SCRATCH_D2, so scratch results replace them before they are read; the
+  harness runs stage 1b's loop through the same FHEHostDriver calls with
+  those four masks placed after the maps (oracle/ref_iqm_harness.cpp).
+Nothing else of the reference's host code is changed: the driver's level
+handling (tables loaded once for 11 limbs, rotation keys stored 14 limbs per
+digit, numPartQ fixed at 3) is the reference's, and the GPU path reproduces
+its results word for word, as a drop-in for the accelerator must.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+import pytest
+
+from anns_fhe_b200 import formats as F
+from anns_fhe_b200.driver import CkksParams
+from oracle.oracle import tables_py as T
+from tests.helpers import primes_for, uniform_residues
+
+pytestmark = pytest.mark.gpu
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF = os.path.join(os.path.dirname(HERE), "oracle", "_ref")
+P64 = C.POINTER(C.c_uint64)
+POLY_WORDS, KEY_WORDS = 8388608, 67108864          # SimMemoryBus's defaults (sim_memory_bus.h:13)
+N = 16384
+SLOT_CT_QUERY_C0, SLOT_CT_QUERY_C1, SLOT_PT_CENTROIDS = 0x0, 0x40000, 0x80000
+SLOT_PT_MASK = 0x300000
+MASK_HI = 0x600000                                   # masks 4-7, after the rotation maps
+UNUSED_STEPS = [3, 5, 6, 7]                          # their maps take the words rescale overwrites
+
+
+def load(name):
+    path = os.path.join(REF, name)
+    if not os.path.exists(path):
+        pytest.skip(f"{name} not built (the reference tree was absent when the oracle was built)")
+    lib = C.CDLL(path)
+    lib.rh_new.restype, lib.rh_new.argtypes = C.c_void_p, [C.c_char_p, C.c_uint64, C.c_uint64]
+    lib.rh_free.argtypes = [C.c_void_p]
+    lib.rh_write_poly.argtypes = [C.c_void_p, C.c_uint64, P64, C.c_uint64]
+    lib.rh_read_poly.argtypes = [C.c_void_p, C.c_uint64, P64, C.c_uint64]
+    lib.rh_stage1.argtypes = [C.c_void_p]
+    lib.rh_stage1b.argtypes = [C.c_void_p, C.c_uint32]
+    return lib
+
+
+def write_package(root, prm, rng):
+    """The context directory (vectors/) and, one folder up, the CRT tables
+    for the 11-limb level under the names the driver reads
+    (fhe_host_driver.cpp:89-103)."""
+    n, L, K = prm.n, prm.L, prm.K
+    allp = prm.q + prm.p
+
+    def key():
+        return np.concatenate([uniform_residues(rng, allp, n) for _ in range(2 * prm.dnum)])
+    steps = [1 << s for s in range(12)]           # tree sum 1..64 and the stage-1b shifts i * 127, i < 32
+    vec = os.path.join(root, "vectors")
+    F.save_package(vec, prm, relin=key(), rot={s: key() for s in UNUSED_STEPS + steps})
+    # the directory lists the unused keys first: the driver places maps in listing order
+    meta = dict(F.read_rotation_meta(os.path.join(vec, "rotation_keys_meta.txt")))
+    F.write_rotation_meta(os.path.join(vec, "rotation_keys_meta.txt"),
+                          [(s, meta[s]) for s in UNUSED_STEPS + steps])
+    for j in range(3):
+        a, b = T.part_qhat(prm.q, L, prm.alpha, j, prm.p)
+        F.write_words(os.path.join(root, f"tv_keyswitch_PartQlHatInvModq_{j}.bin"), a)
+        F.write_words(os.path.join(root, f"tv_keyswitch_PartQlHatModp_{j}.bin"), b)
+    pinv, phinv, phq = T.moddown(prm.q, L, prm.p)
+    F.write_words(os.path.join(root, "tv_keyswitch_PInvModq.bin"), pinv)
+    F.write_words(os.path.join(root, "tv_keyswitch_PHatInvModp.bin"), phinv)
+    F.write_words(os.path.join(root, "tv_keyswitch_PHatModq.bin"), phq)
+    qlql, qlinv = T.rescale(prm.q, L)
+    F.write_words(os.path.join(root, "QlQlInvModqlDivqlModq.bin"), qlql)
+    F.write_words(os.path.join(root, "qlInvModq.bin"), qlinv)
+    return vec
+
+
+def test_reference_query_manager_on_gpu_equals_reference_on_cpu(tmp_path):
+    cpu, gpu = load("libref_iqm_cpu.so"), load("libref_iqm_gpu.so")
+    q, p = primes_for(14, 11, 45, 4, 60, first_bits=60)
+    prm = CkksParams(14, q, p, 4)
+    rng = np.random.default_rng(2024)
+    vec = write_package(str(tmp_path), prm, rng)
+    inputs = [(SLOT_CT_QUERY_C0, uniform_residues(rng, q, N)), (SLOT_CT_QUERY_C1, uniform_residues(rng, q, N)),
+              (SLOT_PT_CENTROIDS, uniform_residues(rng, q, N))]
+    inputs += [(SLOT_PT_MASK + i * 15 * N if i < 4 else MASK_HI + (i - 4) * 15 * N, uniform_residues(rng, q[:10], N))
+               for i in range(8)]
+    arenas = []
+    for lib in (cpu, gpu):
+        h = lib.rh_new(vec.encode(), POLY_WORDS, KEY_WORDS)
+        assert h
+        try:
+            for off, x in inputs:
+                lib.rh_write_poly(h, off, x.ctypes.data_as(P64), x.size)
+            lib.rh_stage1(h)
+            lib.rh_stage1b(h, MASK_HI)
+            out = np.empty(POLY_WORDS, dtype=np.uint64)
+            lib.rh_read_poly(h, 0, out.ctypes.data_as(P64), POLY_WORDS)
+            arenas.append(out)
+        finally:
+            lib.rh_free(h)
+    shim = C.CDLL(os.path.join(os.path.dirname(HERE), "anns_fhe_b200", "lib", "libafhe_accel_top.so"))
+    assert shim.afhe_accel_top_last_status() == 0
+    shim.afhe_accel_top_release()
+    compact = 0x1C0000
+    assert np.any(arenas[0][compact:compact + 9 * N] != 0), "stage 1b wrote nothing"
+    diff = np.nonzero(arenas[0] != arenas[1])[0]
+    assert diff.size == 0, f"{diff.size} words of poly_gmem differ, first at {diff[0]:#x}"
