@@ -5,7 +5,7 @@
   alone with CUDA events on the context stream; its algorithmic bytes and
   the achieved fraction of the HBM peak.
 * drivers for ncu captures, each a plain program whose launches are easy to
-  count: `python -m anns_fhe_b200.profiling ks|ntt|step|host ...`.
+  count: `python -m anns_fhe_b200.profiling ks|ntt|step|host|dispatch ...`.
 
 Algorithmic bytes of one rotation key switch per ciphertext: c0 and c1 read,
 both outputs written (4 x l limbs of N words); the rotation key (2 x dnum x
@@ -257,6 +257,53 @@ def profile_host(batch: int = 296, steps: int = 5):
     wl.close()
 
 
+def profile_dispatch(calls: int = 200, log_n: int = 13):
+    """Host-to-completion cost of afhe_dispatch per op code, one polynomial
+    per call, as a host driving the reference's kernel ABI issues them: the
+    small configuration's shape (3 + 1 limbs, alpha 1). `calls` calls of each
+    op back to back, then one wait: microseconds per call (wall clock, so the
+    host's share and the device's are both in it)."""
+    import numpy as np
+
+    from . import _lib as L
+    from .driver import CkksParams, FheContext
+    prm = CkksParams.generate(log_n, 3, 50, 1, 60, 1)
+    n, Lq = prm.n, prm.L
+    pw = 16 * (Lq + prm.K) * n
+    ctx = FheContext(prm, poly_words=pw, key_words=4 * prm.key_words() + 8 * (Lq + prm.K) * n)
+    try:
+        lay = ctx.write_context_tables(Lq)
+        rng = np.random.default_rng(4)
+        ctx.write_key(lay.first_free_offset, np.concatenate([rng.integers(0, q, n, dtype=np.uint64)
+                                                             for _ in range(2 * prm.dnum) for q in prm.q + prm.p]))
+        W = (Lq + prm.K) * n
+        for i in range(4):
+            ctx.write_poly(i * W, np.concatenate([rng.integers(0, q, n, dtype=np.uint64) for q in prm.q]))
+        L.check(ctx.dispatch(ctx.accel_args(L.OP_LOAD_CONTEXT, Lq, lay)), "OP 99")
+        ops = {"ntt": (L.OP_NTT, dict(src_a_offset=0, dst_offset=4 * W)),
+               "intt": (L.OP_INTT, dict(src_a_offset=0, dst_offset=4 * W)),
+               "poly_add": (L.OP_POLY_ADD, dict(src_a_offset=0, src_b_offset=W, dst_offset=4 * W)),
+               "poly_mul_ntt": (L.OP_POLY_MUL_NTT, dict(src_a_offset=0, src_b_offset=W, dst_offset=4 * W)),
+               "rescale": (L.OP_RESCALE, dict(src_a_offset=0, src_b_offset=W, dst_offset=4 * W)),
+               "key_switch": (L.OP_KEY_SWITCH, dict(src_a_offset=0, dst_offset=4 * W,
+                                                    evk_offset=lay.first_free_offset))}
+        out = {}
+        for name, (op, kw) in ops.items():
+            a = ctx.accel_args(op, Lq, lay, **kw)
+            for _ in range(5):
+                L.check(ctx.dispatch(a), name)
+            ctx.sync()
+            t = time.perf_counter()
+            for _ in range(calls):
+                ctx.dispatch(a)
+            ctx.sync()
+            out[name] = round((time.perf_counter() - t) / calls * 1e6, 1)
+    finally:
+        ctx.close()
+    print(json.dumps({"profile": "afhe_dispatch", "ring_degree": n, "limbs": f"{Lq} + {prm.K}",
+                      "us_per_call": out, "calls": calls}))
+
+
 def main() -> None:
     ap = argparse.ArgumentParser(prog="python -m anns_fhe_b200.profiling")
     sub = ap.add_subparsers(dest="what", required=True)
@@ -272,6 +319,8 @@ def main() -> None:
     a.add_argument("--workload", default="small", choices=["small", "large"])
     a.add_argument("--lanes", type=int, default=0)
     sub.add_parser("host", help="end-to-end phases and the streamed run's host hotspots")
+    a = sub.add_parser("dispatch", help="afhe_dispatch cost per call and op code")
+    a.add_argument("--calls", type=int, default=200)
     args = ap.parse_args()
     if args.what == "ks":
         profile_ks(args.lanes, args.workload, args.level)
@@ -279,6 +328,8 @@ def main() -> None:
         profile_ntt(args.polys, args.log_n)
     elif args.what == "step":
         profile_step(args.queries, args.workload, args.lanes)
+    elif args.what == "dispatch":
+        profile_dispatch(args.calls)
     else:
         profile_host()
 
