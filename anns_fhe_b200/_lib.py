@@ -20,7 +20,7 @@ OK, E_ARG, E_RANGE, E_NOKEY, E_LEVEL, E_BUDGET, E_TIMEOUT, E_CUDA, E_STATE = ran
 
 OP_NTT, OP_INTT, OP_POLY_ADD, OP_POLY_SUB, OP_POLY_MUL_NTT = 1, 2, 3, 4, 5
 OP_AUTOMORPHISM, OP_KEY_SWITCH, OP_RESCALE, OP_LOAD_CONTEXT = 6, 7, 8, 99
-OPT_KS_FUSED, OPT_CHUNK = 1, 2
+OPT_KS_FUSED, OPT_CHUNK, OPT_FUSED_MIN = 1, 2, 3
 
 u32, u64, i32 = C.c_uint32, C.c_uint64, C.c_int32
 P64 = C.POINTER(C.c_uint64)
@@ -134,6 +134,7 @@ SIGNATURES = {
     "afhe_decrypt_batch": (C.c_int, [CTX, C.POINTER(CtRef), u32, u64, u64, u32]),
     "afhe_key_switch_noalloc": (C.c_int, [CTX, C.c_void_p, u64, u32]),
     "afhe_eval_rotate_accumulate_batch": (C.c_int, [CTX, C.POINTER(CtRef), C.POINTER(CtRef), u32, i32, u32]),
+    "afhe_eval_rotate_accumulate_levels_batch": (C.c_int, [CTX, C.POINTER(CtRef), C.POINTER(CtRef), P32, u32, i32]),
     "afhe_eval_add_batch": (C.c_int, [CTX, C.POINTER(CtRef), C.POINTER(CtRef), C.POINTER(CtRef), u32, u32]),
     "afhe_eval_sub_plain_batch": (C.c_int, [CTX, C.POINTER(CtRef), P64, C.POINTER(CtRef), u32, u32]),
     "afhe_eval_mult_plain_rescale_batch": (C.c_int, [CTX, C.POINTER(CtRef), P64, C.POINTER(CtRef), u32, u32]),

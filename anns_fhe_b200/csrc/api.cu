@@ -296,6 +296,10 @@ int build_native_tables(afhe_ctx* ctx) {
         t.qlinv = b + R.qlinv.v;
         t.qlinv_sh = b + R.qlinv.sh;
     }
+    // the same tables as one device array, for launches whose entries run at
+    // different levels
+    CK(dalloc(&ctx->lv_dev, L + 1));
+    CK(cudaMemcpy(ctx->lv_dev, ctx->lv.data(), (L + 1) * sizeof(OpTabs), cudaMemcpyHostToDevice));
 
     // job templates
     std::vector<LimbJob> jq(np);
@@ -385,6 +389,16 @@ int afhe_ctx_create(const afhe_params* prm, afhe_ctx** out) {
         {
             const char* v = std::getenv("AFHE_KS_FUSED");
             ctx->ks_fused = key_switch_fused_supported(ctx->log_n) && !(v && v[0] == '0');
+            // the one-kernel path carries a ciphertext per CTA (per cluster of
+            // N / 2^13 CTAs above N = 2^13): below half a wave of SMs a launch
+            // leaves most of the GPU idle, and the limb-parallel multi-kernel
+            // path is faster
+            int sms = 148;
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, ctx->device);
+            const int cl = ctx->log_n > 13 ? 1 << (ctx->log_n - 13) : 1;
+            ctx->fused_min = (uint32_t)std::max(1, sms / (2 * cl));
+            const char* m = std::getenv("AFHE_FUSED_MIN");
+            if (m && std::atoi(m) >= 1) ctx->fused_min = (uint32_t)std::atoi(m);
         }
         if (ctx->lanes > 4096) { rc = fail(ctx, AFHE_E_ARG, "max_batch must be <= 4096"); break; }
         ctx->scr_words = (size_t)ctx->lanes * lane_words(ctx);
@@ -436,7 +450,7 @@ int afhe_ctx_destroy(afhe_ctx* ctx) {
     cudaSetDevice(ctx->device);
     if (ctx->st) cudaStreamSynchronize(ctx->st);
     auto fr = [](void* p) { if (p) cudaFree(p); };
-    fr(ctx->poly); fr(ctx->key); fr(ctx->lvbuf); fr(ctx->jobs_qp);
+    fr(ctx->poly); fr(ctx->key); fr(ctx->lvbuf); fr(ctx->lv_dev); fr(ctx->jobs_qp);
     for (auto& j : ctx->lvjobs) fr(j.modup);
     for (DevPrimeSet* s : {&ctx->nat, &ctx->ld}) { fr(s->pc); fr(s->tw); fr(s->itw); fr(s->tw2); fr(s->itw2); }
     fr(ctx->ld_crt); fr(ctx->ld_crt_sh); fr(ctx->ld_mod);
@@ -539,12 +553,16 @@ int afhe_ctx_set_option(afhe_ctx* ctx, uint32_t option, int64_t value) {
     switch (option) {
     case AFHE_OPT_KS_FUSED:
         if (value && !key_switch_fused_supported(ctx->log_n))
-            return fail(ctx, AFHE_E_ARG, "the one-kernel key switch needs N <= 2^13");
+            return fail(ctx, AFHE_E_ARG, "the one-kernel key switch cannot run on this GPU at this ring degree");
         ctx->ks_fused = value != 0;
         return AFHE_OK;
     case AFHE_OPT_CHUNK:
         if (value < 0 || value > (int64_t)ctx->lanes) return fail(ctx, AFHE_E_ARG, "chunk must be in [0, lanes]");
         ctx->chunk = (uint32_t)value;
+        return AFHE_OK;
+    case AFHE_OPT_FUSED_MIN:
+        if (value < 1 || value > 4096) return fail(ctx, AFHE_E_ARG, "fused minimum must be in [1, 4096]");
+        ctx->fused_min = (uint32_t)value;
         return AFHE_OK;
     default:
         return fail(ctx, AFHE_E_ARG, "unknown option");
@@ -556,6 +574,7 @@ int afhe_ctx_get_option(afhe_ctx* ctx, uint32_t option, int64_t* value) {
     switch (option) {
     case AFHE_OPT_KS_FUSED: *value = ctx->ks_fused ? 1 : 0; return AFHE_OK;
     case AFHE_OPT_CHUNK: *value = ctx->chunk ? ctx->chunk : ctx->lanes; return AFHE_OK;
+    case AFHE_OPT_FUSED_MIN: *value = ctx->fused_min; return AFHE_OK;
     default: return fail(ctx, AFHE_E_ARG, "unknown option");
     }
 }

@@ -16,6 +16,7 @@
 
 #include <algorithm>
 #include <cstdlib>
+#include <map>
 #include <vector>
 
 #include "internal.h"
@@ -68,8 +69,11 @@ int check_cts(afhe_ctx* ctx, const afhe_ct_ref* v, uint32_t count, uint32_t limb
 // optional fusion (automorphism gather, c0 add, accumulate; see KsFuse).
 // `fused_ok` is false when an entry's outputs may overlap another entry's
 // inputs, which the one-kernel key switch cannot order.
+// With lvz (mixed levels, one-kernel key switch only), entry z runs at level
+// lvz.at(z) and `limbs` is the largest of them.
 int ks_batch(afhe_ctx* ctx, const ZField& in, const ZField& out0, const ZField& out1, uint32_t nz, u64 evk,
-             uint32_t limbs, const KsFuse* fuse = nullptr, bool fused_ok = true, const ulonglong2* prep = nullptr) {
+             uint32_t limbs, const KsFuse* fuse = nullptr, bool fused_ok = true, const ulonglong2* prep = nullptr,
+             const ZField* lvz = nullptr) {
     const u64 n = ctx->n, S = (u64)ctx->L + ctx->K;
     const OpTabs& t = ctx->lv[limbs];
     const LevelJobs& lj = ctx->lvjobs[limbs];
@@ -78,9 +82,11 @@ int ks_batch(afhe_ctx* ctx, const ZField& in, const ZField& out0, const ZField& 
     zb.out = out0;
     zb.aux = out1;
     zb.mid = lane_field(ctx, &Lane::ks);
-    if (ctx->ks_fused && fused_ok) {
+    if (lvz && !(ctx->ks_fused && fused_ok)) return fail(ctx, AFHE_E_STATE, "mixed levels need the one-kernel key switch");
+    if (ctx->ks_fused && fused_ok && (lvz || nz >= ctx->fused_min)) {
         CK(launch_key_switch_fused(ctx->log_n, t, limbs, ctx->K, ctx->key, evk, evk + (u64)ctx->dnum * S * n,
-                                   (uint32_t)S, ctx->L, ctx->poly, ctx->scr, nz, zb, ctx->st, fuse, prep));
+                                   (uint32_t)S, ctx->L, ctx->poly, ctx->scr, nz, zb, ctx->st, fuse, prep,
+                                   lvz ? ctx->lv_dev : nullptr, lvz));
         return AFHE_OK;
     }
     CK(launch_key_switch(ctx->log_n, t, ctx->jobs_qp, lj.modup, lj.n_modup, ctx->L, limbs, ctx->K, ctx->key, evk,
@@ -165,7 +171,7 @@ int mult_relin_rescale_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const afhe_ct_
 // Inputs may alias outputs; acc may alias dst.
 int rotate_step_batch(afhe_ctx* ctx, const ZField& in0, const ZField& in1, const ZField& d0, const ZField& d1,
                       uint32_t nz, int32_t step, uint32_t limbs, const ZField* acc0 = nullptr,
-                      const ZField* acc1 = nullptr, bool fused_ok = true) {
+                      const ZField* acc1 = nullptr, bool fused_ok = true, const ZField* lvz = nullptr) {
     auto it = ctx->rot.find(step);
     if (it == ctx->rot.end()) return fail(ctx, AFHE_E_NOKEY, "rotation key not found for step " + std::to_string(step));
     const RotKey& rk = it->second;
@@ -175,7 +181,7 @@ int rotate_step_batch(afhe_ctx* ctx, const ZField& in0, const ZField& in1, const
     f.c0 = in0;
     f.has_acc = acc0 != nullptr;
     if (acc0) { f.acc0 = *acc0; f.acc1 = *acc1; }
-    return ks_batch(ctx, in1, d0, d1, nz, rk.evk_offset, limbs, &f, fused_ok, rk.prep);
+    return ks_batch(ctx, in1, d0, d1, nz, rk.evk_offset, limbs, &f, fused_ok, rk.prep, lvz);
 }
 
 // Whether the one-kernel key switch may run a rotation batch: its entries run
@@ -565,6 +571,66 @@ int afhe_eval_rotate_accumulate_batch(afhe_ctx* ctx, const afhe_ct_ref* in, cons
     });
 }
 
+int afhe_eval_rotate_accumulate_levels_batch(afhe_ctx* ctx, const afhe_ct_ref* in, const afhe_ct_ref* acc,
+                                             const uint32_t* levels, uint32_t count, int32_t total) {
+    if (!ctx || (count && (!in || !acc || !levels))) return fail(ctx, AFHE_E_ARG, "null argument");
+    int rc;
+    uint32_t top = 1;
+    for (uint32_t i = 0; i < count; ++i) {
+        if ((rc = check_limbs(ctx, levels[i], 1)) || (rc = check_cts(ctx, in + i, 1, levels[i])) ||
+            (rc = check_cts(ctx, acc + i, 1, levels[i])))
+            return rc;
+        top = std::max(top, levels[i]);
+    }
+    long long rem = std::llabs((long long)total);
+    std::vector<int32_t> steps;
+    while (rem > 0) {
+        long long st = 1;
+        while ((st << 1) <= rem) st <<= 1;
+        steps.push_back((int32_t)(total > 0 ? st : -st));
+        rem -= st;
+    }
+    for (int32_t st : steps)
+        if (!ctx->rot.count(st)) return fail(ctx, AFHE_E_NOKEY, "rotation key not found for step " + std::to_string(st));
+    return for_chunks(ctx, count, [&](uint32_t s, uint32_t m) -> int {
+        Offs i0(m), i1(m), o0(m), o1(m), lv(m);
+        uint32_t mx = 1;
+        for (uint32_t z = 0; z < m; ++z) {
+            i0[z] = in[s + z].c0_offset; i1[z] = in[s + z].c1_offset;
+            o0[z] = acc[s + z].c0_offset; o1[z] = acc[s + z].c1_offset;
+            lv[z] = levels[s + z];
+            mx = std::max(mx, levels[s + z]);
+        }
+        if (total == 0 || !ctx->ks_fused || !fused_rotation_safe(i0, i1, o0, o1, (u64)top * ctx->n)) {
+            // one launch sequence per level, entries of a level together
+            std::map<uint32_t, std::vector<uint32_t>> by;
+            for (uint32_t z = 0; z < m; ++z) by[levels[s + z]].push_back(z);
+            for (auto& kv : by) {
+                std::vector<afhe_ct_ref> a, b;
+                for (uint32_t z : kv.second) { a.push_back(in[s + z]); b.push_back(acc[s + z]); }
+                int r = afhe_eval_rotate_accumulate_batch(ctx, a.data(), b.data(), (uint32_t)a.size(), total, kv.first);
+                if (r != AFHE_OK) return r;
+            }
+            return AFHE_OK;
+        }
+        ZField fi0, fi1, fo0, fo1, flv;
+        ZF(fi0, i0); ZF(fi1, i1); ZF(fo0, o0); ZF(fo1, o1); ZF(flv, lv);
+        const ZField x0 = lane_temp_field(ctx, 2), x1 = lane_temp_field(ctx, 5);
+        ZField c0 = fi0, c1 = fi1;
+        for (size_t k = 0; k < steps.size(); ++k) {
+            const bool last = k + 1 == steps.size();
+            const ZField& n0 = last ? fo0 : x0;
+            const ZField& n1 = last ? fo1 : x1;
+            int r = rotate_step_batch(ctx, c0, c1, n0, n1, m, steps[k], mx, last ? &fo0 : nullptr,
+                                      last ? &fo1 : nullptr, true, &flv);
+            if (r != AFHE_OK) return r;
+            c0 = n0;
+            c1 = n1;
+        }
+        return AFHE_OK;
+    });
+}
+
 int afhe_eval_rotate_steps_batch(afhe_ctx* ctx, const afhe_ct_ref* in, const afhe_ct_ref* dst, const int32_t* steps,
                                  uint32_t count, uint32_t limbs) {
     if (!ctx || (count && (!in || !dst || !steps))) return fail(ctx, AFHE_E_ARG, "null argument");
@@ -607,7 +673,7 @@ int afhe_eval_rotate_steps_batch(afhe_ctx* ctx, const afhe_ct_ref* in, const afh
         ZF(zb.out, o0);
         ZF(zb.aux, o1);
         zb.mid = lane_field(ctx, &Lane::ks);
-        if (ctx->ks_fused && fused_rotation_safe(i0, i1, o0, o1, (u64)limbs * n)) {
+        if (ctx->ks_fused && m >= ctx->fused_min && fused_rotation_safe(i0, i1, o0, o1, (u64)limbs * n)) {
             const ulonglong2* prep = nullptr;
             if (all_prep) {
                 ZF(f.prepz, preps);

@@ -90,6 +90,7 @@ struct afhe_ctx {
     afhe::DevPrimeSet nat;
     afhe::u64* lvbuf = nullptr;                 // per-level CRT tables
     std::vector<afhe::OpTabs> lv;                // index = level (1..L)
+    afhe::OpTabs* lv_dev = nullptr;              // the same, in device memory (mixed-level launches)
     afhe::LimbJob* jobs_qp = nullptr;            // slot i -> prime i, offsets i*N, for i < L + K
     std::vector<afhe::LevelJobs> lvjobs;         // index = level
 
@@ -116,6 +117,7 @@ struct afhe_ctx {
     afhe::DescRing ring;
     bool ks_fused = true;   // one-kernel key switch where supported (AFHE_KS_FUSED=0 turns it off)
     uint32_t chunk = 0;     // ciphertexts per launch of a batched call (0: all lanes)
+    uint32_t fused_min = 1; // launches of fewer ciphertexts take the multi-kernel key switch
     // afhe_fence: fence f is event fences[f % size], recorded on st
     std::vector<cudaEvent_t> fences;
     uint64_t fence_next = 0;
@@ -212,7 +214,11 @@ size_t ks_fused_scratch_words(uint32_t n, uint32_t sizeQl, uint32_t K);
 cudaError_t launch_key_switch_fused(int log_n, const OpTabs& t, uint32_t sizeQl, uint32_t K, const u64* key, u64 evk_a,
                                     u64 evk_b, uint32_t key_stride, uint32_t key_pbase, u64* arena, u64* scratch,
                                     uint32_t nz, const ZBases& zb, cudaStream_t st, const KsFuse* fuse = nullptr,
-                                    const ulonglong2* prep = nullptr);
+                                    const ulonglong2* prep = nullptr, const OpTabs* lvtabs = nullptr,
+                                    const ZField* lvz = nullptr);
+// With lvtabs and lvz (mixed levels), entry z runs at level lvz->at(z) with
+// the tables lvtabs[level] (a device copy of the context's per-level tables;
+// sizeQl is then the largest level), each reading and writing that many limbs.
 // prep[w] = (k mod q, companion) for k = key[w], w < words, where word w
 // belongs to key limb slot (w / n) mod S and slot i uses prime pc[i].
 cudaError_t launch_key_prep(const u64* key, ulonglong2* prep, const PrimeConst* pc, uint32_t n, uint32_t S, u64 words,

@@ -58,6 +58,11 @@ struct KsFusedArgs {
     KsFuse f;
     const ulonglong2* prep;   // prepared key (evk_a digits, then evk_b digits), or null
     u64 prep_b;               // offset of the evk_b digits in prep
+    // mixed levels: entry z runs at level lvz.at(z) with the tables
+    // lvtabs[level] (device copy of the context's per-level tables); null:
+    // every entry at sizeQl with t
+    const OpTabs* lvtabs;
+    ZField lvz;
 };
 
 constexpr int kLogQ = 13;    // log2 of the slice a CTA holds at N >= 2^13
@@ -265,14 +270,13 @@ __device__ __forceinline__ EntryKey entry_key(const KsFusedArgs& a, uint32_t z) 
 // this CTA's slices of A0 / A1: A0 = sum_j d_j * evk_b[j], A1 = sum_j d_j *
 // evk_a[j] (mod the slot's prime).
 template <int LOGQ, int LOGCL, bool PREP>
-__device__ void mac_slot(const KsFusedArgs& a, const EntryKey& ek, uint32_t s, u64* W, u64* A0, u64* A1,
+__device__ void mac_slot(const KsFusedArgs& a, const OpTabs& t, uint32_t l, const EntryKey& ek, uint32_t s, u64* W,
+                         u64* A0, u64* A1,
                          const u64* __restrict__ in, const u64* __restrict__ coef) {
     using G = Geo<LOGQ, LOGCL>;
     constexpr int LOGN = G::LOGN;
     constexpr uint32_t N = 1u << LOGN;
     const uint32_t x0 = G::rank() * G::QN;
-    const OpTabs& t = a.t;
-    const uint32_t l = a.sizeQl;
     const bool isq = s < l;
     const uint32_t prime = isq ? s : t.p_base + (s - l);
     const uint32_t klimb = isq ? s : a.key_pbase + (s - l);
@@ -381,10 +385,10 @@ __device__ void mac_slot(const KsFusedArgs& a, const EntryKey& ek, uint32_t s, u
 //   out_h = (in * key_h[q0] - A_h) * P^-1 (+ extras), the own digit's product
 //   computed in the same pass. Same residues as the general path.
 template <int LOGN, bool PREP>
-__device__ __forceinline__ void ks_one_limb(const KsFusedArgs& a, const EntryKey& ek, u64* W, u64* A0, u64* A1) {
+__device__ __forceinline__ void ks_one_limb(const KsFusedArgs& a, const OpTabs& t, const EntryKey& ek, u64* W, u64* A0,
+                                            u64* A1) {
     constexpr uint32_t N = 1u << LOGN;
     const uint32_t z = blockIdx.x;
-    const OpTabs& t = a.t;
     const uint32_t* map = ek.map;
     const u64* in = a.arena + a.in.at(z);
     const PrimeConst pq = t.pt.pc[0], pp = t.pt.pc[t.p_base];
@@ -568,13 +572,14 @@ __global__ void __launch_bounds__((1u << LOGQ) / 8, 1) ks_fused_kernel(const KsF
     u64* A1 = smem + 2 * PADQ;
     const uint32_t z = G::z();
     const uint32_t x0 = G::rank() * G::QN;
-    const OpTabs& t = a.t;
-    const uint32_t l = a.sizeQl, K = a.K;
+    const uint32_t l = a.lvtabs ? (uint32_t)a.lvz.at(z) : a.sizeQl;
+    const OpTabs& t = a.lvtabs ? a.lvtabs[l] : a.t;
+    const uint32_t K = a.K;
     const EntryKey ek = entry_key(a, z);
     const uint32_t* map = ek.map;
     if constexpr (LOGCL == 0) {
         if (l == 1 && K == 1) {
-            ks_one_limb<LOGN, PREP>(a, ek, W, A0, A1);
+            ks_one_limb<LOGN, PREP>(a, t, ek, W, A0, A1);
             return;
         }
     }
@@ -611,7 +616,7 @@ __global__ void __launch_bounds__((1u << LOGQ) / 8, 1) ks_fused_kernel(const KsF
     }
     // phase 1: special slots -> INTT of both accumulators
     for (uint32_t k = 0; k < K; ++k) {
-        mac_slot<LOGQ, LOGCL, PREP>(a, ek, l + k, W, A0, A1, in, coef);
+        mac_slot<LOGQ, LOGCL, PREP>(a, t, l, ek, l + k, W, A0, A1, in, coef);
         const uint32_t prime = t.p_base + k;
         const PrimeConst pc = t.pt.pc[prime];
         ntt2<true, LOGQ, LOGCL>(A0, A1, t.pt, prime, pc);
@@ -632,7 +637,7 @@ __global__ void __launch_bounds__((1u << LOGQ) / 8, 1) ks_fused_kernel(const KsF
     const u64 c0 = a.f.has_c0 ? a.f.c0.at(z) : 0;
     const u64 ac0 = a.f.has_acc ? a.f.acc0.at(z) : 0, ac1 = a.f.has_acc ? a.f.acc1.at(z) : 0;
     for (uint32_t i = 0; i < l; ++i) {
-        mac_slot<LOGQ, LOGCL, PREP>(a, ek, i, W, A0, A1, in, coef);
+        mac_slot<LOGQ, LOGCL, PREP>(a, t, l, ek, i, W, A0, A1, in, coef);
         const PrimeConst pc = t.pt.pc[i];
         const u64 q = pc.q, q2 = q << 1;
         const u64 pinv = __ldg(t.p_inv_mod_q + i), pinv_sh = __ldg(t.p_inv_mod_q_sh + i);
@@ -809,7 +814,7 @@ cudaError_t launch_key_prep(const u64* key, ulonglong2* prep, const PrimeConst* 
 cudaError_t launch_key_switch_fused(int log_n, const OpTabs& t, uint32_t sizeQl, uint32_t K, const u64* key, u64 evk_a,
                                     u64 evk_b, uint32_t key_stride, uint32_t key_pbase, u64* arena, u64* scratch,
                                     uint32_t nz, const ZBases& zb, cudaStream_t st, const KsFuse* fuse,
-                                    const ulonglong2* prep) {
+                                    const ulonglong2* prep, const OpTabs* lvtabs, const ZField* lvz) {
     if (nz == 0) return cudaSuccess;
     KsFusedArgs a{};
     a.t = t;
@@ -829,6 +834,10 @@ cudaError_t launch_key_switch_fused(int log_n, const OpTabs& t, uint32_t sizeQl,
     if (fuse) a.f = *fuse;
     a.prep = prep;
     a.prep_b = evk_b - evk_a;
+    if (lvtabs && lvz) {
+        a.lvtabs = lvtabs;
+        a.lvz = *lvz;
+    }
     switch (log_n) {
     case 10: return launch_fused<10, 0>(a, nz, st);
     case 11: return launch_fused<11, 0>(a, nz, st);

@@ -21,6 +21,8 @@ limb), so tests can regenerate any part of the inputs without keeping them.
 """
 from __future__ import annotations
 
+import ctypes as C
+
 import numpy as np
 
 from . import _lib as L
@@ -147,8 +149,18 @@ class KeySwitchBatch:
             arr[i].c0_offset, arr[i].c1_offset = a, b
         return arr
 
-    def rotate_step(self, step: int, which=None) -> int:
-        """x += rot(x, step) for the ciphertexts `which` (default all); returns calls made."""
+    def rotate_step(self, step: int, which=None, by_level: bool = False) -> int:
+        """x += rot(x, step) for the ciphertexts `which` (default all), every
+        level in one call (afhe_eval_rotate_accumulate_levels_batch), or with
+        by_level one call per level group; returns calls made."""
+        zs_all = list(range(self.cts) if which is None else which)
+        if not by_level:
+            refs = self._refs([self.ct(z) for z in zs_all])
+            lv = (C.c_uint32 * len(zs_all))(*[self.levels[z] for z in zs_all])
+            L.check(self.ctx.lib.afhe_eval_rotate_accumulate_levels_batch(self.ctx.h, refs, refs, lv, len(zs_all),
+                                                                          step),
+                    "eval_rotate_accumulate_levels_batch")
+            return 1
         calls = 0
         for lv, zs in sorted(self.groups(which).items()):
             refs = self._refs([self.ct(z) for z in zs])
@@ -166,9 +178,9 @@ class KeySwitchBatch:
             calls += 1
         return calls
 
-    def run(self, which=None) -> None:
+    def run(self, which=None, by_level: bool = False) -> None:
         for s in self.steps:
-            self.rotate_step(s, which)
+            self.rotate_step(s, which, by_level)
         self.rescale(which)
 
     def read_ct(self, z: int, out: bool = False) -> tuple[np.ndarray, np.ndarray]:

@@ -181,6 +181,12 @@ int afhe_copy_poly(afhe_ctx* ctx, uint64_t dst_offset, uint64_t src_offset, uint
  *                      (0: all lanes). Same residues for any value. */
 #define AFHE_OPT_KS_FUSED 1u
 #define AFHE_OPT_CHUNK 2u
+/*   AFHE_OPT_FUSED_MIN launches of fewer ciphertexts than this take the
+ *                      multi-kernel key switch even where the one-kernel path
+ *                      is on (it carries one ciphertext per CTA, or per
+ *                      cluster above N = 2^13, so a small launch leaves most
+ *                      SMs idle). Default: half a wave of SMs. Same residues. */
+#define AFHE_OPT_FUSED_MIN 3u
 int afhe_ctx_set_option(afhe_ctx* ctx, uint32_t option, int64_t value);
 int afhe_ctx_get_option(afhe_ctx* ctx, uint32_t option, int64_t* value);
 /* Page-locked host memory for the transfers above (the reference's host
@@ -315,6 +321,15 @@ uint64_t afhe_kernel_launches(void);
  * into acc in its epilogue. */
 int afhe_eval_rotate_accumulate_batch(afhe_ctx* ctx, const afhe_ct_ref* in, const afhe_ct_ref* acc,
                                       uint32_t count, int32_t total_rot, uint32_t limbs);
+/* afhe_eval_rotate_accumulate_batch for ciphertexts at different levels:
+ * acc[i] = acc[i] + rotate(in[i], total_rot), each at levels[i] limbs, in one
+ * launch per rotation step (the one-kernel key switch reads each entry's
+ * level's tables; without it, or when entries' outputs overlap other
+ * entries' inputs, one launch sequence per level). Each result equals the
+ * single-level call's. The reference runs one ciphertext at a time
+ * (fhe_host_driver.cpp:361-404, then eval_add :248-257). */
+int afhe_eval_rotate_accumulate_levels_batch(afhe_ctx* ctx, const afhe_ct_ref* in, const afhe_ct_ref* acc,
+                                             const uint32_t* levels, uint32_t count, int32_t total_rot);
 int afhe_eval_add_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const afhe_ct_ref* b, const afhe_ct_ref* dst,
                         uint32_t count, uint32_t limbs);
 /* dst[i] = eval_rotate_single_step(in[i], steps[i]) (fhe_host_driver.cpp:

@@ -5,6 +5,13 @@ import sys
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+# Contexts made by the tests take the one-kernel key switch for launches of
+# any size (the library's default sends launches smaller than half a wave of
+# SMs to the multi-kernel path), so single-ciphertext checks exercise it; the
+# multi-kernel path has its own contexts (AFHE_KS_FUSED=0) in the tests that
+# compare the two.
+os.environ.setdefault("AFHE_FUSED_MIN", "1")
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 

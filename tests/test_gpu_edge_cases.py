@@ -257,11 +257,17 @@ def test_options_and_limits(ed):
     assert lib.afhe_ctx_set_option(h, L.OPT_CHUNK, 0) == L.OK
     # a null host buffer with a non-zero count
     assert lib.afhe_read_poly(h, 0, C.POINTER(C.c_uint64)(), 8) == L.E_ARG
-    # the one-kernel key switch is for N <= 2^13
+    # above N = 2^13 the one-kernel key switch runs on thread-block clusters:
+    # on by default where the GPU can place them, and it can be switched
     q, p = primes_for(14, 2, 40, 1, 45)
     with FheContext(CkksParams(14, q, p, 1), poly_words=1 << 16, key_words=1 << 16, max_batch=1) as big:
-        assert big.lib.afhe_ctx_set_option(big.h, L.OPT_KS_FUSED, 1) == L.E_ARG
+        assert big.get_option(L.OPT_KS_FUSED) == 1
         assert big.lib.afhe_ctx_set_option(big.h, L.OPT_KS_FUSED, 0) == L.OK
+        assert big.lib.afhe_ctx_set_option(big.h, L.OPT_KS_FUSED, 1) == L.OK
+        # smallest launch the one-kernel path takes
+        assert big.lib.afhe_ctx_set_option(big.h, L.OPT_FUSED_MIN, 0) == L.E_ARG
+        assert big.lib.afhe_ctx_set_option(big.h, L.OPT_FUSED_MIN, 5) == L.OK
+        assert big.get_option(L.OPT_FUSED_MIN) == 5
     # max_batch: 4096 is the largest
     small = CkksParams(10, ed.prm.q[:2], ed.prm.p[:1], 1)
     with pytest.raises(L.AfheError) as ei:

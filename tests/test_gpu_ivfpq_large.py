@@ -14,9 +14,10 @@ other slots stay near 1e-3. Coarse distances (64 key switches) stay near
 
 How the checks use it:
 * calibration: one query (its own seed) per chain shape measures the error
-  of every candidate slot and of every coarse list; a slot's bound is
-  3 x (its calibrated error + the median calibrated error), at least 5e-3
-  (coarse: 2e-2 where the calibration saw less);
+  of every slot of its result ciphertexts (slots without a candidate decode
+  to 0 plus the bias) and of every coarse list; a slot's bound is 3 x (its
+  calibrated error + the median calibrated error), at least 5e-3 (coarse:
+  2e-2 where the calibration saw less);
 * selection: test queries are picked from the plaintext side alone, scanning
   seeds for ones whose rank gaps exceed the bounds on both sides: every pair
   of consecutive coarse distances up to rank nprobe + 1, every pair of
@@ -86,12 +87,19 @@ def calibrate(big, nprobe, level):
         cand = np.array([v for c in probes for v in big.index.lists[c]])
         rec = big.index.reconstruct(cand)
         dist = ((q[0][None, :].astype(np.float64) - rec) ** 2).sum(1)
-    pos = positions(big, probes) % S
-    ed = np.abs(r["dists"] - dist)
-    med = float(np.median(ed))
-    bound = np.full(S, 5e-3)
-    np.maximum.at(bound, pos, 3 * (ed + med))
-    return cbound, bound, float(ec.max()), float(ed.max())
+    # every slot of the result ciphertexts that hold candidates: the
+    # candidate's distance where one sits, 0 (masked) elsewhere
+    pos = positions(big, probes)
+    rec = big.records[0]
+    need = int(pos[-1]) // S + 1
+    scale = big.iqm.out_scale_at(big.iqm.level_of(rec))
+    vals = big.decrypt_many(rec.results[:need], [scale] * need).ravel()
+    want = np.zeros(need * S)
+    want[pos] = dist
+    err = np.abs(vals - want).reshape(need, S).max(axis=0)
+    med = float(np.median(err))
+    bound = np.maximum(5e-3, 3 * (err + med))
+    return cbound, bound, float(ec.max()), float(err.max())
 
 
 def qualifies(big, q, nprobe, cbound, bound):

@@ -80,12 +80,19 @@ def test_rotate_step_and_rescale_vs_oracle(ksb, orc):
 
 
 def test_chain_batched_equals_alone(ksb):
+    """The chain over all 32 ciphertexts, every level in one launch per step,
+    equals each ciphertext's chain run alone and the chain run one level
+    group at a time."""
     wl = ksb
     wl.reset()
     wl.run()
-    zs = _three_levels(wl)
-    batched = {z: (wl.read_ct(z, out=True)) for z in zs}
-    for z in zs:
+    batched = {z: (wl.read_ct(z, out=True)) for z in range(wl.cts)}
+    wl.reset()
+    wl.run(by_level=True)
+    for z in range(wl.cts):
+        g = wl.read_ct(z, out=True)
+        assert np.array_equal(g[0], batched[z][0]) and np.array_equal(g[1], batched[z][1]), f"level groups, {z}"
+    for z in _three_levels(wl):
         wl.reset([z])
         wl.run([z])
         alone = wl.read_ct(z, out=True)

@@ -12,7 +12,8 @@ encrypted query, centroid plaintext and masks in their poly_gmem slots
 (interactive_query_manager.h:17-36), and run the query manager's stage 1
 (interactive_query_manager.cpp:85-119) and stage 1b's loop (:121-178) at the
 reference's own shape: N = 16384, 11 Q limbs (60-bit first, then 45-bit) + 4 P
-limbs, alpha 4. Every word of poly_gmem must then be identical.
+limbs, alpha 4, all primes 60-bit (below). Every word of poly_gmem must
+then be identical.
 
 The reference's memory map has two collisions, both worked around here
 without touching its code:
@@ -33,6 +34,16 @@ Nothing else of the reference's host code is changed: the driver's level
 handling (tables loaded once for 11 limbs, rotation keys stored 14 limbs per
 digit, numPartQ fixed at 3) is the reference's, and the GPU path reproduces
 its results word for word, as a drop-in for the accelerator must.
+
+Below the loaded level that handling makes the reference's key switch and
+rescale read tables laid out for 11 limbs (fhe_accel_top.cpp:194-214 loads
+one level): a base-conversion entry reduced modulo one prime is multiplied
+under another. Its Barrett multiplication (mod_arith.cpp:15-25) is exact
+only while the product stays below 2^(2 bits(q)), which a 60-bit entry
+times a 45-bit residue does not; the GPU path multiplies exactly. With every
+prime 60 bits wide each such product stays in the exact range, so both
+paths compute the same (level-mismatched but well-defined) residues, and
+the comparison covers every operator the stages issue.
 """
 import ctypes as C
 import os
@@ -104,7 +115,7 @@ def write_package(root, prm, rng):
 
 def test_reference_query_manager_on_gpu_equals_reference_on_cpu(tmp_path):
     cpu, gpu = load("libref_iqm_cpu.so"), load("libref_iqm_gpu.so")
-    q, p = primes_for(14, 11, 45, 4, 60, first_bits=60)
+    q, p = primes_for(14, 11, 60, 4, 60)
     prm = CkksParams(14, q, p, 4)
     rng = np.random.default_rng(2024)
     vec = write_package(str(tmp_path), prm, rng)
