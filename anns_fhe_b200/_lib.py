@@ -70,6 +70,15 @@ class CtRef(C.Structure):
     _fields_ = [("c0_offset", u64), ("c1_offset", u64)]
 
 
+class IvfpqShape(C.Structure):
+    _fields_ = [("D", u32), ("n_list", u32), ("slots", u32), ("lanes", u32), ("packed", u32), ("eval_level", u32)]
+
+
+class IvfpqQuery(C.Structure):
+    _fields_ = [("ct_query", CtRef), ("ct_dim", CtRef), ("compact", CtRef), ("results", C.POINTER(CtRef)),
+                ("n_results", u32), ("level", u32), ("probes", C.POINTER(u32)), ("nprobe", u32)]
+
+
 CTX = C.c_void_p
 
 # name -> (restype, argtypes)
@@ -141,6 +150,16 @@ SIGNATURES = {
     "afhe_rescale_batch": (C.c_int, [CTX, C.POINTER(CtRef), C.POINTER(CtRef), u32, u32]),
     "afhe_eval_copy_batch": (C.c_int, [CTX, C.POINTER(CtRef), C.POINTER(CtRef), u32, u32]),
     "afhe_eval_rotate_steps_batch": (C.c_int, [CTX, C.POINTER(CtRef), C.POINTER(CtRef), C.POINTER(i32), u32, u32]),
+    "afhe_ivfpq_create": (C.c_int, [CTX, C.POINTER(IvfpqShape), C.POINTER(C.c_void_p)]),
+    "afhe_ivfpq_destroy": (C.c_int, [C.c_void_p]),
+    "afhe_ivfpq_set_centroids": (C.c_int, [C.c_void_p, P64, u32]),
+    "afhe_ivfpq_set_level_masks": (C.c_int, [C.c_void_p, u32, P64, u32]),
+    "afhe_ivfpq_set_prefix_mask": (C.c_int, [C.c_void_p, u32, u32, u64]),
+    "afhe_ivfpq_set_list": (C.c_int, [C.c_void_p, u32, P64, P32, u32]),
+    "afhe_ivfpq_set_lanes": (C.c_int, [C.c_void_p, C.POINTER(CtRef), u32, C.POINTER(CtRef)]),
+    "afhe_ivfpq_set_tuning": (C.c_int, [C.c_void_p, u32, i32, u32]),
+    "afhe_ivfpq_stage1": (C.c_int, [C.c_void_p, C.POINTER(IvfpqQuery), u32]),
+    "afhe_ivfpq_stage3": (C.c_int, [C.c_void_p, C.POINTER(IvfpqQuery), u32]),
 }
 
 _lib = None

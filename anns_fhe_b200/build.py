@@ -25,7 +25,7 @@ SHIM_SRC = os.path.join(CSRC, "fhe_accel_top_shim.cpp")
 ROOT = os.path.dirname(HERE)
 INCLUDE = os.path.join(ROOT, "include")
 
-SOURCES = ["api.cu", "driver.cu", "kernels.cu", "ksfused.cu", "noalloc.cu", "tables.cpp"]
+SOURCES = ["api.cu", "driver.cu", "ivfpq.cu", "kernels.cu", "ksfused.cu", "noalloc.cu", "tables.cpp"]
 HEADERS = ["internal.h", "lanes.h", "modarith.cuh", "ntt.cuh", "tables.h"]
 
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]

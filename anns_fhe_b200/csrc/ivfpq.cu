@@ -1,0 +1,446 @@
+// ivfpq.cu -- the encrypted IVF-PQ query chain's server stages in C++.
+//
+// The reference's InteractiveQueryManager (cpp_host_model/src/
+// interactive_query_manager.cpp:85-303, semantics fixed by integration_tools/
+// generate_interactive_test_vectors.cpp:383-541) runs one query's stages one
+// ciphertext at a time through FHEHostDriver. This driver runs the same
+// stages for many queries at once: every operator is one batched call over
+// up to `lanes` ciphertexts (queries in stage 1, (query, list, batch) items in
+// stage 3), and every ciphertext's residues are the ones the one-at-a-time
+// chain produces:
+//
+//   stage 1   ct_diff = ct_query - pt_centroids; ct_sq = rescale(ct_diff^2);
+//             tree sum with rotations 1, 2, .., D/2
+//   stage 1b  reference compaction: for list i, mask slot i D, rescale,
+//             rotate by i (D - 1) (eval_rotate's power-of-two steps), sum;
+//             packed compaction (centroids over several ciphertexts): mask
+//             every centroid slot of coarse ciphertext k, rescale, rotate by
+//             -k in one key switch, sum
+//   stage 3   per candidate batch: ct_dim - pt_batch, square, rescale, tree
+//             sum with rotations B, 2B, .., B D/2, mask the batch's slots,
+//             rescale, place it at its slot offset (eval_rotate's steps, or
+//             one key switch per batch when packed), accumulate into the
+//             query's result ciphertext
+//
+// Plaintexts, masks and working ciphertexts stay resident in poly_gmem at the
+// offsets the caller registers (anns_fhe_b200/query.py encodes them). Modular
+// additions are exact, so summing a query's terms pairwise gives the
+// reference's running sum word for word.
+#include <algorithm>
+#include <cstdlib>
+#include <map>
+#include <vector>
+
+#include "internal.h"
+#include "lanes.h"
+
+using namespace afhe;
+
+struct afhe_ivfpq {
+    afhe_ctx* ctx = nullptr;
+    afhe_ivfpq_shape sh{};
+    std::vector<u64> centroid_cts;                      // [n_coarse]
+    std::map<uint32_t, std::vector<u64>> masks;         // level -> one-hot [n_list] or stride [1]
+    std::map<std::pair<uint32_t, uint32_t>, u64> prefix;   // (level, count) -> mask of the first count slots
+    std::vector<std::vector<std::pair<u64, uint32_t>>> lists;   // list -> (plaintext, candidates) per batch
+    std::vector<afhe_ct_ref> work;                      // diff, sq, sel per lane
+    std::vector<afhe_ct_ref> cmp;                       // (n_list - 1) per lane: reference compaction terms
+    std::map<uint32_t, std::pair<int32_t, uint32_t>> tuning;   // level -> (one-kernel, chunk)
+    bool fused_ok = false;                              // the one-kernel key switch was on at creation
+};
+
+namespace {
+
+typedef std::vector<afhe_ct_ref> Cts;
+
+int fail_h(afhe_ivfpq* h, int code, const char* msg) { return fail(h ? h->ctx : nullptr, code, msg); }
+
+uint32_t n_coarse(const afhe_ivfpq_shape& s) {
+    const uint32_t per = s.slots / s.D;
+    return (s.n_list + per - 1) / per;
+}
+
+uint32_t eval_at(const afhe_ivfpq* h, uint32_t level) {
+    const uint32_t lv = level ? level : h->ctx->L;
+    return h->sh.eval_level ? std::min(lv, h->sh.eval_level) : lv;
+}
+
+// The tuned options of the level an operator runs at (query.py _at).
+void at(afhe_ivfpq* h, uint32_t limbs) {
+    auto it = h->tuning.find(limbs);
+    if (it == h->tuning.end()) return;
+    const int32_t fused = it->second.first;
+    if (fused == 0 || (fused > 0 && h->fused_ok)) afhe_ctx_set_option(h->ctx, AFHE_OPT_KS_FUSED, fused);
+    afhe_ctx_set_option(h->ctx, AFHE_OPT_CHUNK, std::min<uint32_t>(it->second.second, h->ctx->lanes));
+}
+
+#define RC(expr)                              \
+    do {                                      \
+        int _rc = (expr);                     \
+        if (_rc != AFHE_OK) return _rc;       \
+    } while (0)
+
+int add(afhe_ivfpq* h, const Cts& a, const Cts& b, const Cts& d, uint32_t limbs) {
+    return a.empty() ? AFHE_OK : afhe_eval_add_batch(h->ctx, a.data(), b.data(), d.data(), (uint32_t)a.size(), limbs);
+}
+
+int copy(afhe_ivfpq* h, const Cts& a, const Cts& d, uint32_t limbs) {
+    return a.empty() ? AFHE_OK : afhe_eval_copy_batch(h->ctx, a.data(), d.data(), (uint32_t)a.size(), limbs);
+}
+
+int rot_acc(afhe_ivfpq* h, const Cts& src, const Cts& acc, int32_t r, uint32_t limbs) {
+    at(h, limbs);
+    return afhe_eval_rotate_accumulate_batch(h->ctx, src.data(), acc.data(), (uint32_t)src.size(), r, limbs);
+}
+
+int square(afhe_ivfpq* h, const Cts& a, const Cts& d, uint32_t limbs) {
+    at(h, limbs);
+    return afhe_eval_mult_relin_rescale_batch(h->ctx, a.data(), a.data(), d.data(), (uint32_t)a.size(), limbs);
+}
+
+// dst = rescale(a * pt) per entry
+int mult_plain(afhe_ivfpq* h, const Cts& a, const std::vector<u64>& pts, const Cts& d, uint32_t limbs) {
+    return afhe_eval_mult_plain_rescale_batch(h->ctx, a.data(), pts.data(), d.data(), (uint32_t)a.size(), limbs);
+}
+
+// Each (ct, step) rotated in place by its step in one key switch.
+int rotate_direct(afhe_ivfpq* h, const std::vector<std::pair<afhe_ct_ref, int32_t>>& items, uint32_t limbs) {
+    Cts cts;
+    std::vector<int32_t> steps;
+    for (auto& it : items)
+        if (it.second) {
+            cts.push_back(it.first);
+            steps.push_back(it.second);
+        }
+    if (cts.empty()) return AFHE_OK;
+    at(h, limbs);
+    return afhe_eval_rotate_steps_batch(h->ctx, cts.data(), cts.data(), steps.data(), (uint32_t)cts.size(), limbs);
+}
+
+// Each (ct, shift) rotated in place as eval_rotate does it (fhe_host_driver.cpp:
+// 361-404): |shift| in descending powers of two, sign kept; one batched call
+// per (power, sign) over the items whose shift has that bit.
+int rotate_grouped(afhe_ivfpq* h, const std::vector<std::pair<afhe_ct_ref, int32_t>>& items, uint32_t limbs) {
+    uint32_t top = 0;
+    for (auto& it : items) top = std::max<uint32_t>(top, (uint32_t)std::abs(it.second));
+    if (!top) return AFHE_OK;
+    int b = 31;
+    while (!((top >> b) & 1u)) --b;
+    for (; b >= 0; --b)
+        for (int sign : {1, -1}) {
+            Cts sel;
+            for (auto& it : items) {
+                const int32_t s = it.second;
+                if (s && ((s > 0) == (sign > 0)) && ((((uint32_t)std::abs(s)) >> b) & 1u)) sel.push_back(it.first);
+            }
+            if (sel.empty()) continue;
+            at(h, limbs);
+            RC(afhe_eval_rotate_batch(h->ctx, sel.data(), sel.data(), (uint32_t)sel.size(), sign * (1 << b), limbs));
+        }
+    return AFHE_OK;
+}
+
+// groups[g][0] += groups[g][1] + ... by pairwise batched additions.
+int sum_groups(afhe_ivfpq* h, std::vector<Cts> live, uint32_t limbs) {
+    for (;;) {
+        Cts a, b;
+        for (auto& g : live)
+            for (size_t j = 0; j + 1 < g.size(); j += 2) {
+                a.push_back(g[j]);
+                b.push_back(g[j + 1]);
+            }
+        if (a.empty()) return AFHE_OK;
+        RC(add(h, a, b, a, limbs));
+        for (auto& g : live) {
+            Cts k;
+            for (size_t j = 0; j < g.size(); j += 2) k.push_back(g[j]);
+            g.swap(k);
+        }
+    }
+}
+
+bool same(const afhe_ct_ref& a, const afhe_ct_ref& b) { return a.c0_offset == b.c0_offset && a.c1_offset == b.c1_offset; }
+
+// items (target, first, src): per target its sources summed pairwise, then
+// copied into the target when one of them starts the target's sum, else added.
+int accumulate(afhe_ivfpq* h, const std::vector<std::pair<std::pair<afhe_ct_ref, bool>, afhe_ct_ref>>& items,
+               uint32_t limbs) {
+    std::vector<afhe_ct_ref> targets;
+    std::vector<bool> first;
+    std::vector<Cts> groups;
+    for (auto& it : items) {
+        size_t g = 0;
+        while (g < targets.size() && !same(targets[g], it.first.first)) ++g;
+        if (g == targets.size()) {
+            targets.push_back(it.first.first);
+            first.push_back(false);
+            groups.emplace_back();
+        }
+        first[g] = first[g] || it.first.second;
+        groups[g].push_back(it.second);
+    }
+    RC(sum_groups(h, groups, limbs));
+    Cts cs, ct, as, at_;
+    for (size_t g = 0; g < targets.size(); ++g) {
+        if (first[g]) { cs.push_back(groups[g][0]); ct.push_back(targets[g]); }
+        else { as.push_back(groups[g][0]); at_.push_back(targets[g]); }
+    }
+    RC(copy(h, cs, ct, limbs));
+    return add(h, at_, as, at_, limbs);
+}
+
+int sub_plain(afhe_ivfpq* h, const Cts& a, const std::vector<u64>& pts, const Cts& d, uint32_t limbs) {
+    return afhe_eval_sub_plain_batch(h->ctx, a.data(), pts.data(), d.data(), (uint32_t)a.size(), limbs);
+}
+
+// queries by the level they run at, highest first (query.py _by_level)
+std::vector<std::pair<uint32_t, std::vector<uint32_t>>> by_level(afhe_ivfpq* h, const afhe_ivfpq_query* q,
+                                                                  uint32_t count) {
+    std::map<uint32_t, std::vector<uint32_t>> g;
+    for (uint32_t i = 0; i < count; ++i) g[eval_at(h, q[i].level)].push_back(i);
+    return std::vector<std::pair<uint32_t, std::vector<uint32_t>>>(g.rbegin(), g.rend());
+}
+
+int stage1_packed(afhe_ivfpq* h, const afhe_ivfpq_query* q, const std::vector<uint32_t>& idx, uint32_t Ll) {
+    const uint32_t D = h->sh.D, nc = n_coarse(h->sh), lanes = h->sh.lanes;
+    std::vector<std::pair<uint32_t, uint32_t>> items;
+    for (uint32_t qi : idx)
+        for (uint32_t k = 0; k < nc; ++k) items.push_back({qi, k});
+    for (size_t c0 = 0; c0 < items.size(); c0 += lanes) {
+        const size_t m = std::min<size_t>(lanes, items.size() - c0);
+        Cts diff(m), sq(m), sel(m), in(m);
+        std::vector<u64> pts(m), stride(m, h->masks[Ll][0]);
+        for (size_t j = 0; j < m; ++j) {
+            diff[j] = h->work[3 * j];
+            sq[j] = h->work[3 * j + 1];
+            sel[j] = h->work[3 * j + 2];
+            in[j] = q[items[c0 + j].first].ct_query;
+            pts[j] = h->centroid_cts[items[c0 + j].second];
+        }
+        RC(sub_plain(h, in, pts, diff, Ll));
+        RC(square(h, diff, sq, Ll));
+        for (uint32_t s = 1; s < D; s <<= 1) RC(rot_acc(h, sq, sq, (int32_t)s, Ll - 1));
+        RC(mult_plain(h, sq, stride, sel, Ll - 1));
+        std::vector<std::pair<afhe_ct_ref, int32_t>> rot;
+        std::vector<std::pair<std::pair<afhe_ct_ref, bool>, afhe_ct_ref>> acc;
+        for (size_t j = 0; j < m; ++j) {
+            const uint32_t k = items[c0 + j].second;
+            rot.push_back({sel[j], -(int32_t)k});
+            acc.push_back({{q[items[c0 + j].first].compact, k == 0}, sel[j]});
+        }
+        RC(rotate_direct(h, rot, Ll - 2));
+        RC(accumulate(h, acc, Ll - 2));
+    }
+    return AFHE_OK;
+}
+
+int stage1_reference(afhe_ivfpq* h, const afhe_ivfpq_query* q, const std::vector<uint32_t>& idx, uint32_t Ll) {
+    const uint32_t D = h->sh.D, nl = h->sh.n_list, lanes = h->sh.lanes;
+    const std::vector<u64>& onehot = h->masks[Ll];
+    for (size_t c0 = 0; c0 < idx.size(); c0 += lanes) {
+        const size_t m = std::min<size_t>(lanes, idx.size() - c0);
+        Cts diff(m), sq(m), in(m);
+        std::vector<u64> pts(m, h->centroid_cts[0]);
+        for (size_t j = 0; j < m; ++j) {
+            diff[j] = h->work[3 * j];
+            sq[j] = h->work[3 * j + 1];
+            in[j] = q[idx[c0 + j]].ct_query;
+        }
+        RC(sub_plain(h, in, pts, diff, Ll));
+        RC(square(h, diff, sq, Ll));
+        for (uint32_t s = 1; s < D; s <<= 1) RC(rot_acc(h, sq, sq, (int32_t)s, Ll - 1));
+        // stage 1b: every (query, list) term masked in one batched operator,
+        // rotated step by step across the terms, summed pairwise
+        Cts src, dst;
+        std::vector<u64> masks;
+        for (size_t k = 0; k < m; ++k)
+            for (uint32_t i = 0; i < nl; ++i) {
+                src.push_back(sq[k]);
+                masks.push_back(onehot[i]);
+                dst.push_back(i == 0 ? q[idx[c0 + k]].compact : h->cmp[k * (nl - 1) + i - 1]);
+            }
+        RC(mult_plain(h, src, masks, dst, Ll - 1));
+        if (nl == 1) continue;
+        std::vector<std::pair<afhe_ct_ref, int32_t>> rot;
+        std::vector<Cts> groups;
+        for (size_t k = 0; k < m; ++k) {
+            Cts g{q[idx[c0 + k]].compact};
+            for (uint32_t i = 1; i < nl; ++i) {
+                rot.push_back({h->cmp[k * (nl - 1) + i - 1], (int32_t)(i * (D - 1))});
+                g.push_back(h->cmp[k * (nl - 1) + i - 1]);
+            }
+            groups.push_back(g);
+        }
+        RC(rotate_grouped(h, rot, Ll - 2));
+        RC(sum_groups(h, groups, Ll - 2));
+    }
+    return AFHE_OK;
+}
+
+struct Item {
+    uint32_t qi;
+    u64 pt;
+    uint32_t cnt;
+    u64 off;
+};
+
+int stage3_items(afhe_ivfpq* h, const afhe_ivfpq_query* q, const std::vector<Item>& items, uint32_t Ll) {
+    const uint32_t D = h->sh.D, S = h->sh.slots, B = S / D, lanes = h->sh.lanes;
+    for (size_t c0 = 0; c0 < items.size(); c0 += lanes) {
+        const size_t m = std::min<size_t>(lanes, items.size() - c0);
+        Cts diff(m), sq(m), sel(m), in(m);
+        std::vector<u64> pts(m), prefix(m);
+        for (size_t j = 0; j < m; ++j) {
+            const Item& it = items[c0 + j];
+            diff[j] = h->work[3 * j];
+            sq[j] = h->work[3 * j + 1];
+            sel[j] = h->work[3 * j + 2];
+            in[j] = q[it.qi].ct_dim;
+            pts[j] = it.pt;
+            auto pm = h->prefix.find({Ll, it.cnt});
+            if (pm == h->prefix.end()) return fail_h(h, AFHE_E_STATE, "no prefix mask for a candidate count at this level");
+            prefix[j] = pm->second;
+        }
+        RC(sub_plain(h, in, pts, diff, Ll));
+        RC(square(h, diff, sq, Ll));
+        for (uint32_t s = B; s < D * B; s <<= 1) RC(rot_acc(h, sq, sq, (int32_t)s, Ll - 1));
+        RC(mult_plain(h, sq, prefix, sel, Ll - 1));
+        std::vector<std::pair<afhe_ct_ref, int32_t>> place;
+        std::vector<std::pair<std::pair<afhe_ct_ref, bool>, afhe_ct_ref>> acc;
+        for (size_t j = 0; j < m; ++j) {
+            const Item& it = items[c0 + j];
+            place.push_back({sel[j], -(int32_t)(it.off % S)});
+            acc.push_back({{q[it.qi].results[it.off / S], it.off % S == 0}, sel[j]});
+        }
+        RC(h->sh.packed ? rotate_direct(h, place, Ll - 2) : rotate_grouped(h, place, Ll - 2));
+        RC(accumulate(h, acc, Ll - 2));
+    }
+    return AFHE_OK;
+}
+
+int check_query(afhe_ivfpq* h, const afhe_ivfpq_query& q) {
+    if (q.level > h->ctx->L || (q.level && q.level < 3)) return fail_h(h, AFHE_E_LEVEL, "query level outside [3, L]");
+    if (!h->masks.count(eval_at(h, q.level))) return fail_h(h, AFHE_E_STATE, "no masks for the query's level");
+    return AFHE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int afhe_ivfpq_create(afhe_ctx* ctx, const afhe_ivfpq_shape* shape, afhe_ivfpq** out) {
+    if (!ctx || !shape || !out) return fail(ctx, AFHE_E_ARG, "null argument");
+    const afhe_ivfpq_shape& s = *shape;
+    if (s.D < 2 || (s.D & (s.D - 1)) || s.slots != ctx->n / 2 || s.D > s.slots || s.n_list < 1 || s.lanes < 1 ||
+        s.lanes > ctx->lanes)
+        return fail(ctx, AFHE_E_ARG, "ivfpq shape: D a power of two <= N/2, slots = N/2, lanes in [1, context lanes]");
+    if (!s.packed && s.n_list * s.D > s.slots) return fail(ctx, AFHE_E_ARG, "centroids do not fit one ciphertext");
+    if (s.packed && n_coarse(s) > s.D) return fail(ctx, AFHE_E_ARG, "packed compaction needs n_coarse <= D");
+    if (s.eval_level && (s.eval_level < 3 || s.eval_level > ctx->L)) return fail(ctx, AFHE_E_LEVEL, "eval_level in [3, L]");
+    afhe_ivfpq* h = new afhe_ivfpq();
+    h->ctx = ctx;
+    h->sh = s;
+    h->lists.resize(s.n_list);
+    int64_t v = 0;
+    h->fused_ok = afhe_ctx_get_option(ctx, AFHE_OPT_KS_FUSED, &v) == AFHE_OK && v == 1;
+    *out = h;
+    return AFHE_OK;
+}
+
+int afhe_ivfpq_destroy(afhe_ivfpq* h) {
+    delete h;
+    return AFHE_OK;
+}
+
+int afhe_ivfpq_set_centroids(afhe_ivfpq* h, const uint64_t* pts, uint32_t count) {
+    if (!h || !pts) return fail_h(h, AFHE_E_ARG, "null argument");
+    if (count != n_coarse(h->sh)) return fail_h(h, AFHE_E_ARG, "one centroid plaintext per coarse ciphertext");
+    h->centroid_cts.assign(pts, pts + count);
+    return AFHE_OK;
+}
+
+int afhe_ivfpq_set_level_masks(afhe_ivfpq* h, uint32_t level, const uint64_t* masks, uint32_t count) {
+    if (!h || !masks) return fail_h(h, AFHE_E_ARG, "null argument");
+    if (count != (h->sh.packed ? 1u : h->sh.n_list)) return fail_h(h, AFHE_E_ARG, "n_list one-hot masks, or one stride mask");
+    h->masks[level].assign(masks, masks + count);
+    return AFHE_OK;
+}
+
+int afhe_ivfpq_set_prefix_mask(afhe_ivfpq* h, uint32_t level, uint32_t count, uint64_t pt) {
+    if (!h) return fail_h(h, AFHE_E_ARG, "null argument");
+    h->prefix[{level, count}] = pt;
+    return AFHE_OK;
+}
+
+int afhe_ivfpq_set_list(afhe_ivfpq* h, uint32_t list, const uint64_t* pts, const uint32_t* counts, uint32_t batches) {
+    if (!h || (batches && (!pts || !counts))) return fail_h(h, AFHE_E_ARG, "null argument");
+    if (list >= h->sh.n_list) return fail_h(h, AFHE_E_RANGE, "list out of range");
+    auto& v = h->lists[list];
+    v.clear();
+    for (uint32_t b = 0; b < batches; ++b) {
+        if (counts[b] < 1 || counts[b] > h->sh.slots / h->sh.D) return fail_h(h, AFHE_E_ARG, "batch count outside [1, B]");
+        v.push_back({pts[b], counts[b]});
+    }
+    return AFHE_OK;
+}
+
+int afhe_ivfpq_set_lanes(afhe_ivfpq* h, const afhe_ct_ref* work, uint32_t lanes, const afhe_ct_ref* cmp) {
+    if (!h || !work) return fail_h(h, AFHE_E_ARG, "null argument");
+    if (lanes < h->sh.lanes) return fail_h(h, AFHE_E_ARG, "a diff / sq / sel ciphertext triple for every lane");
+    h->work.assign(work, work + 3 * (size_t)lanes);
+    if (!h->sh.packed && h->sh.n_list > 1) {
+        if (!cmp) return fail_h(h, AFHE_E_ARG, "the reference compaction needs n_list - 1 term ciphertexts per lane");
+        h->cmp.assign(cmp, cmp + (size_t)lanes * (h->sh.n_list - 1));
+    }
+    return AFHE_OK;
+}
+
+int afhe_ivfpq_set_tuning(afhe_ivfpq* h, uint32_t level, int32_t fused, uint32_t chunk) {
+    if (!h) return fail_h(h, AFHE_E_ARG, "null argument");
+    h->tuning[level] = {fused, chunk};
+    return AFHE_OK;
+}
+
+int afhe_ivfpq_stage1(afhe_ivfpq* h, const afhe_ivfpq_query* q, uint32_t count) {
+    if (!h || (count && !q)) return fail_h(h, AFHE_E_ARG, "null argument");
+    if (h->work.empty() || h->centroid_cts.empty()) return fail_h(h, AFHE_E_STATE, "lanes and centroids not set");
+    for (uint32_t i = 0; i < count; ++i) RC(check_query(h, q[i]));
+    for (auto& g : by_level(h, q, count))
+        RC(h->sh.packed ? stage1_packed(h, q, g.second, g.first) : stage1_reference(h, q, g.second, g.first));
+    return AFHE_OK;
+}
+
+int afhe_ivfpq_stage3(afhe_ivfpq* h, const afhe_ivfpq_query* q, uint32_t count) {
+    if (!h || (count && !q)) return fail_h(h, AFHE_E_ARG, "null argument");
+    if (h->work.empty()) return fail_h(h, AFHE_E_STATE, "lanes not set");
+    const uint32_t S = h->sh.slots, B = S / h->sh.D;
+    std::map<uint32_t, std::vector<Item>> items;
+    for (uint32_t qi = 0; qi < count; ++qi) {
+        RC(check_query(h, q[qi]));
+        if (q[qi].nprobe && !q[qi].probes) return fail_h(h, AFHE_E_ARG, "null probes");
+        auto& lst = items[eval_at(h, q[qi].level)];
+        u64 off = 0;
+        uint32_t t = 0;
+        for (uint32_t p = 0; p < q[qi].nprobe; ++p) {
+            const uint32_t c = q[qi].probes[p];
+            if (c >= h->sh.n_list) return fail_h(h, AFHE_E_RANGE, "probed list out of range");
+            for (auto& b : h->lists[c]) {
+                u64 at_;
+                if (h->sh.packed) {
+                    at_ = (u64)t * B;            // batch t at slot t B
+                } else {
+                    if (off % S + b.second > S) off = (off / S + 1) * S;   // no batch straddles two results
+                    at_ = off;
+                    off += b.second;
+                }
+                if (at_ / S >= q[qi].n_results) return fail_h(h, AFHE_E_RANGE, "more candidates than the result ciphertexts hold");
+                lst.push_back({qi, b.first, b.second, at_});
+                ++t;
+            }
+        }
+    }
+    for (auto it = items.rbegin(); it != items.rend(); ++it) RC(stage3_items(h, q, it->second, it->first));
+    return AFHE_OK;
+}
+
+}  // extern "C"

@@ -38,6 +38,12 @@ the next result, so every batch lands whole in one ciphertext.
 
 Phase-3 candidate plaintexts depend only on the index, so they are encoded
 once and stay resident in HBM (poly_gmem), as do the masks.
+
+By default the stages run in C++ (afhe_ivfpq_stage1 / afhe_ivfpq_stage3 in
+libafhe.so, csrc/ivfpq.cu): this class encodes the plaintexts, registers their
+offsets with the native driver and keeps the host bookkeeping (candidate ids,
+slot positions). `native=False` runs the same stages from Python over the
+batched C ABI; both issue the same operators and give identical residues.
 """
 from __future__ import annotations
 
@@ -137,8 +143,10 @@ class InteractiveQueryManager:
     `max_nprobe` sizes the result ciphertexts (default: the shape's nprobe)."""
 
     def __init__(self, ctx: FheContext, index: IvfPqIndex, shape: QueryShape, slots: Slots, lanes: int = MAX_LANES,
-                 levels=None, max_nprobe: int | None = None):
+                 levels=None, max_nprobe: int | None = None, native: bool = True):
         self.ctx, self.index, self.sh = ctx, index, shape
+        self.native = native
+        self._nh, self._nh_key, self._nh_ver = None, None, 0
         self.drv = FHEHostDriver(ctx)
         self.lib = ctx.lib
         self.p = ctx.params
@@ -271,6 +279,7 @@ class InteractiveQueryManager:
                 self._level_masks(lv)
                 self._prefix_masks(lv)
                 self.levels = sorted(self.levels + [lv])
+        self._nh_ver += 1
 
     @staticmethod
     def compaction_slots(n_list: int, L: int, n: int, slot_w: int, lanes: int) -> int:
@@ -326,6 +335,7 @@ class InteractiveQueryManager:
             m[:count] = 1.0
             encode_plaintext(self.ctx, self.enc, m, float(self.p.q[lv - 2]), off, lv - 1)
             self._prefix_lv[key] = off
+            self._nh_ver += 1
         return self._prefix_lv[key]
 
     @staticmethod
@@ -448,6 +458,7 @@ class InteractiveQueryManager:
         None restores the context's defaults."""
         self._tuning = choices or {}
         self._opt_now = None
+        self._nh_ver += 1
         if not hasattr(self, "_fused_ok"):
             self._fused_ok = self.ctx.get_option(L.OPT_KS_FUSED) == 1
 
@@ -462,6 +473,62 @@ class InteractiveQueryManager:
                 self.ctx.set_option(L.OPT_KS_FUSED, want[0])
             self.ctx.set_option(L.OPT_CHUNK, min(want[1], self.ctx.max_batch))
             self._opt_now = want
+
+    # ---- the native stage driver ----
+    def _native_handle(self) -> C.c_void_p:
+        """The afhe_ivfpq handle for the current lanes, eval_level, masks and
+        tuning (re-registered when one of them changed)."""
+        key = (self.lanes, self.sh.eval_level, self._nh_ver)
+        if self._nh is not None and self._nh_key == key:
+            return self._nh
+        self.close_native()
+        sh = self.sh
+        shape = L.IvfpqShape(sh.D, sh.n_list, sh.slots, self.lanes, int(sh.compaction == "packed"),
+                             sh.eval_level or 0)
+        h = C.c_void_p()
+        L.check(self.lib.afhe_ivfpq_create(self.ctx.h, C.byref(shape), C.byref(h)), "ivfpq_create")
+        self._nh = h
+        lib = self.lib
+        L.check(lib.afhe_ivfpq_set_centroids(h, self._offs(self.pt_centroid_cts), len(self.pt_centroid_cts)),
+                "ivfpq_set_centroids")
+        for lv in self.levels:
+            m = self._onehot[lv] if sh.compaction == "reference" else [self._stride[lv]]
+            L.check(lib.afhe_ivfpq_set_level_masks(h, lv, self._offs(m), len(m)), "ivfpq_set_level_masks")
+        for (cnt, lv), off in self._prefix_lv.items():
+            L.check(lib.afhe_ivfpq_set_prefix_mask(h, lv, cnt, off), "ivfpq_set_prefix_mask")
+        for c, bs in enumerate(self.batches):
+            cnts = np.array([b[1] for b in bs] or [0], dtype=np.uint32)
+            L.check(lib.afhe_ivfpq_set_list(h, c, self._offs([b[0] for b in bs]), cnts.ctypes.data_as(L.P32),
+                                            len(bs)), "ivfpq_set_list")
+        work = self._refs([w[k] for w in self.work[:self.lanes] for k in ("diff", "sq", "sel")])
+        cmp = self._refs([c for row in self.cmp[:self.lanes] for c in row]) if self.cmp else None
+        L.check(lib.afhe_ivfpq_set_lanes(h, work, self.lanes, cmp), "ivfpq_set_lanes")
+        for lv, ch in getattr(self, "_tuning", {}).items():
+            L.check(lib.afhe_ivfpq_set_tuning(h, lv, int(ch.fused), int(ch.chunk)), "ivfpq_set_tuning")
+        self._nh_key = key
+        return h
+
+    def close_native(self) -> None:
+        if self._nh is not None:
+            self.lib.afhe_ivfpq_destroy(self._nh)
+            self._nh, self._nh_key = None, None
+
+    @staticmethod
+    def _native_queries(queries, probes: bool):
+        """An afhe_ivfpq_query array for the records; the arrays it points to
+        are kept alive by the returned list."""
+        arr = (L.IvfpqQuery * max(1, len(queries)))()
+        keep = [arr]
+        for q, r in zip(arr, queries):
+            q.ct_query, q.ct_dim, q.compact = L.CtRef(*r.ct_query), L.CtRef(*r.ct_dim), L.CtRef(*r.compact)
+            res = (L.CtRef * len(r.results))(*[L.CtRef(*c) for c in r.results])
+            q.results, q.n_results, q.level = res, len(r.results), r.level
+            keep.append(res)
+            if probes:
+                pr = (C.c_uint32 * max(1, len(r.probes)))(*[int(c) for c in r.probes])
+                q.probes, q.nprobe = pr, len(r.probes)
+                keep.append(pr)
+        return arr, keep
 
     # ---- batched C-ABI helpers ----
     @staticmethod
@@ -572,6 +639,11 @@ class InteractiveQueryManager:
     # ---- stages ----
     def stage1_coarse(self, queries: list[QueryRecord]) -> None:
         """Stages 1 and 1b for every query (lanes at a time, one level at a time)."""
+        if self.native:
+            arr, keep = self._native_queries(queries, probes=False)
+            L.check(self.lib.afhe_ivfpq_stage1(self._native_handle(), arr, len(queries)), "ivfpq_stage1")
+            self._opt_now = None
+            return
         for lv, idx in self._by_level(queries, self.level_of):
             qs = [queries[i] for i in idx]
             if self.sh.compaction == "packed":
@@ -679,6 +751,14 @@ class InteractiveQueryManager:
                      else np.zeros(0, dtype=np.int64))
             if len(q.pos) and q.pos[-1] >= self.n_res * S:
                 raise ValueError("more candidates than the result ciphertexts hold")
+        if self.native:
+            for lv, it in items.items():
+                for x in it:
+                    self._prefix(x[2], lv)          # every batch size's mask at this level exists
+            arr, keep = self._native_queries(queries, probes=True)
+            L.check(self.lib.afhe_ivfpq_stage3(self._native_handle(), arr, len(queries)), "ivfpq_stage3")
+            self._opt_now = None
+            return
         for lv in sorted(items, reverse=True):
             self._stage3_items(queries, items[lv], lv)
 

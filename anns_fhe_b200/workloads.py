@@ -368,5 +368,6 @@ class Workload:
         return coarse, probes, cand, dist, top
 
     def close(self) -> None:
+        self.iqm.close_native()
         self.client.close_decryptors()
         self.ctx.close()

@@ -355,6 +355,57 @@ int afhe_eval_mult_plain_rescale_batch(afhe_ctx* ctx, const afhe_ct_ref* a, cons
 int afhe_rescale_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const afhe_ct_ref* dst, uint32_t count,
                        uint32_t in_limbs);
 
+/* ---- encrypted IVF-PQ server stages ---------------------------------------- */
+/* InteractiveQueryManager's server stages (cpp_host_model/src/
+ * interactive_query_manager.cpp:85-303) for many queries at once: stage 1 +
+ * 1b (coarse distances, compacted) and stage 3 (candidate distances, placed
+ * in the query's result ciphertexts), each operator one batched call over up
+ * to `lanes` ciphertexts. Every result ciphertext is word for word the one
+ * the one-query-at-a-time chain writes. The plaintexts (centroids, index
+ * batches, masks) are encoded by the caller into poly_gmem and registered by
+ * offset; the handle holds offsets only. */
+typedef struct afhe_ivfpq afhe_ivfpq;
+typedef struct afhe_ivfpq_shape {
+    uint32_t D;           /* vector dimension, a power of two */
+    uint32_t n_list;      /* coarse lists */
+    uint32_t slots;       /* N / 2 */
+    uint32_t lanes;       /* ciphertexts per batched call, <= the context's lanes */
+    uint32_t packed;      /* 0: the reference's compaction (one-hot masks, eval_rotate's
+                             power-of-two steps); 1: centroids over ceil(n_list / (slots / D))
+                             ciphertexts, one stride mask, one key switch per placement */
+    uint32_t eval_level;  /* limbs the chain runs at (0: each query's own level) */
+} afhe_ivfpq_shape;
+typedef struct afhe_ivfpq_query {
+    afhe_ct_ref ct_query;        /* the query, repeated every D slots (stage 1 input) */
+    afhe_ct_ref ct_dim;          /* the query, dimension d in slots d B .. d B + B - 1 (stage 3 input) */
+    afhe_ct_ref compact;         /* stage 1b output: the compacted coarse distances */
+    const afhe_ct_ref* results;  /* stage 3 outputs, n_results ciphertexts */
+    uint32_t n_results;
+    uint32_t level;              /* limbs of the encrypted query (0: the top level) */
+    const uint32_t* probes;      /* stage 3: the lists the client selected, in order */
+    uint32_t nprobe;
+} afhe_ivfpq_query;
+int afhe_ivfpq_create(afhe_ctx* ctx, const afhe_ivfpq_shape* shape, afhe_ivfpq** out);
+int afhe_ivfpq_destroy(afhe_ivfpq* h);
+/* One centroid plaintext per coarse ciphertext (1, or ceil(n_list D / slots) packed). */
+int afhe_ivfpq_set_centroids(afhe_ivfpq* h, const uint64_t* pts, uint32_t count);
+/* The compaction masks of queries evaluated at `level` limbs: n_list one-hot
+ * masks (slot i D), or the one stride mask (packed). */
+int afhe_ivfpq_set_level_masks(afhe_ivfpq* h, uint32_t level, const uint64_t* masks, uint32_t count);
+/* The mask of the first `count` slots for queries evaluated at `level`. */
+int afhe_ivfpq_set_prefix_mask(afhe_ivfpq* h, uint32_t level, uint32_t count, uint64_t pt);
+/* List `list`'s candidate batches: plaintext offsets and candidates per batch. */
+int afhe_ivfpq_set_list(afhe_ivfpq* h, uint32_t list, const uint64_t* pts, const uint32_t* counts,
+                        uint32_t batches);
+/* Working ciphertexts: work[3 j .. 3 j + 2] = lane j's diff, sq, sel;
+ * cmp[j (n_list - 1) + i - 1] = lane j's stage-1b term i (reference compaction). */
+int afhe_ivfpq_set_lanes(afhe_ivfpq* h, const afhe_ct_ref* work, uint32_t lanes, const afhe_ct_ref* cmp);
+/* Key-switch options for operators at `level` limbs: fused (-1 leave, 0 off,
+ * 1 on) and chunk, as afhe_ctx_set_option's AFHE_OPT_KS_FUSED / AFHE_OPT_CHUNK. */
+int afhe_ivfpq_set_tuning(afhe_ivfpq* h, uint32_t level, int32_t fused, uint32_t chunk);
+int afhe_ivfpq_stage1(afhe_ivfpq* h, const afhe_ivfpq_query* queries, uint32_t count);
+int afhe_ivfpq_stage3(afhe_ivfpq* h, const afhe_ivfpq_query* queries, uint32_t count);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,122 @@
+// Test helper: the batched C-ABI operators and options that the native stage
+// driver (anns_fhe_b200/csrc/ivfpq.cu) calls, as host stubs that record each
+// call instead of running it. Linked with ivfpq.cu into a test library, it
+// lets the CPU tests compare the native driver's operator sequence with the
+// Python stage driver's (anns_fhe_b200/query.py, native=False), call by call.
+#include <string>
+#include <vector>
+
+#include "internal.h"
+
+namespace {
+std::vector<std::string> g_log;
+int64_t g_fused = 1, g_chunk = 0;
+
+void refs(std::string& s, const afhe_ct_ref* r, uint32_t n) {
+    for (uint32_t i = 0; i < n; ++i)
+        s += " " + std::to_string(r[i].c0_offset) + ":" + std::to_string(r[i].c1_offset);
+    s += " |";
+}
+void words(std::string& s, const uint64_t* p, uint32_t n) {
+    for (uint32_t i = 0; i < n; ++i) s += " " + std::to_string(p[i]);
+    s += " |";
+}
+std::string head(const char* name, uint32_t limbs, bool ks) {
+    std::string s = std::string(name) + " " + std::to_string(limbs);
+    if (ks) s += " fused=" + std::to_string(g_fused) + " chunk=" + std::to_string(g_chunk);
+    return s + " |";
+}
+}  // namespace
+
+namespace afhe {
+int fail(afhe_ctx* ctx, int code, const std::string& msg) {
+    if (ctx) ctx->err = msg;
+    g_log.push_back("error " + std::to_string(code) + " " + msg);
+    return code;
+}
+}  // namespace afhe
+
+extern "C" {
+
+afhe_ctx* trace_ctx_new(uint32_t L, uint32_t n, uint32_t lanes) {
+    afhe_ctx* c = new afhe_ctx();
+    c->L = L;
+    c->n = n;
+    c->lanes = lanes;
+    g_log.clear();
+    g_fused = 1;
+    g_chunk = 0;
+    return c;
+}
+void trace_ctx_free(afhe_ctx* c) { delete c; }
+uint32_t trace_count() { return (uint32_t)g_log.size(); }
+const char* trace_line(uint32_t i) { return i < g_log.size() ? g_log[i].c_str() : ""; }
+
+int afhe_ctx_set_option(afhe_ctx*, uint32_t option, int64_t value) {
+    if (option == AFHE_OPT_KS_FUSED) g_fused = value;
+    if (option == AFHE_OPT_CHUNK) g_chunk = value;
+    return AFHE_OK;
+}
+int afhe_ctx_get_option(afhe_ctx*, uint32_t option, int64_t* value) {
+    *value = option == AFHE_OPT_KS_FUSED ? g_fused : g_chunk;
+    return AFHE_OK;
+}
+int afhe_eval_add_batch(afhe_ctx*, const afhe_ct_ref* a, const afhe_ct_ref* b, const afhe_ct_ref* d, uint32_t n,
+                        uint32_t limbs) {
+    std::string s = head("add", limbs, false);
+    refs(s, a, n), refs(s, b, n), refs(s, d, n);
+    g_log.push_back(s);
+    return AFHE_OK;
+}
+int afhe_eval_copy_batch(afhe_ctx*, const afhe_ct_ref* a, const afhe_ct_ref* d, uint32_t n, uint32_t limbs) {
+    std::string s = head("copy", limbs, false);
+    refs(s, a, n), refs(s, d, n);
+    g_log.push_back(s);
+    return AFHE_OK;
+}
+int afhe_eval_sub_plain_batch(afhe_ctx*, const afhe_ct_ref* a, const uint64_t* pt, const afhe_ct_ref* d, uint32_t n,
+                              uint32_t limbs) {
+    std::string s = head("sub_plain", limbs, false);
+    refs(s, a, n), words(s, pt, n), refs(s, d, n);
+    g_log.push_back(s);
+    return AFHE_OK;
+}
+int afhe_eval_mult_plain_rescale_batch(afhe_ctx*, const afhe_ct_ref* a, const uint64_t* pt, const afhe_ct_ref* d,
+                                       uint32_t n, uint32_t limbs) {
+    std::string s = head("mult_plain", limbs, false);
+    refs(s, a, n), words(s, pt, n), refs(s, d, n);
+    g_log.push_back(s);
+    return AFHE_OK;
+}
+int afhe_eval_mult_relin_rescale_batch(afhe_ctx*, const afhe_ct_ref* a, const afhe_ct_ref* b, const afhe_ct_ref* d,
+                                       uint32_t n, uint32_t limbs) {
+    std::string s = head("square", limbs, true);
+    refs(s, a, n), refs(s, b, n), refs(s, d, n);
+    g_log.push_back(s);
+    return AFHE_OK;
+}
+int afhe_eval_rotate_batch(afhe_ctx*, const afhe_ct_ref* in, const afhe_ct_ref* d, uint32_t n, int32_t rot,
+                           uint32_t limbs) {
+    std::string s = head("rotate", limbs, true) + " " + std::to_string(rot) + " |";
+    refs(s, in, n), refs(s, d, n);
+    g_log.push_back(s);
+    return AFHE_OK;
+}
+int afhe_eval_rotate_accumulate_batch(afhe_ctx*, const afhe_ct_ref* in, const afhe_ct_ref* acc, uint32_t n,
+                                      int32_t rot, uint32_t limbs) {
+    std::string s = head("rot_acc", limbs, true) + " " + std::to_string(rot) + " |";
+    refs(s, in, n), refs(s, acc, n);
+    g_log.push_back(s);
+    return AFHE_OK;
+}
+int afhe_eval_rotate_steps_batch(afhe_ctx*, const afhe_ct_ref* in, const afhe_ct_ref* d, const int32_t* steps,
+                                 uint32_t n, uint32_t limbs) {
+    std::string s = head("rotate_steps", limbs, true);
+    for (uint32_t i = 0; i < n; ++i) s += " " + std::to_string(steps[i]);
+    s += " |";
+    refs(s, in, n), refs(s, d, n);
+    g_log.push_back(s);
+    return AFHE_OK;
+}
+
+}  // extern "C"
