@@ -20,7 +20,7 @@ OK, E_ARG, E_RANGE, E_NOKEY, E_LEVEL, E_BUDGET, E_TIMEOUT, E_CUDA, E_STATE = ran
 
 OP_NTT, OP_INTT, OP_POLY_ADD, OP_POLY_SUB, OP_POLY_MUL_NTT = 1, 2, 3, 4, 5
 OP_AUTOMORPHISM, OP_KEY_SWITCH, OP_RESCALE, OP_LOAD_CONTEXT = 6, 7, 8, 99
-OPT_KS_FUSED, OPT_CHUNK, OPT_FUSED_MIN = 1, 2, 3
+OPT_KS_FUSED, OPT_CHUNK, OPT_FUSED_MIN, OPT_KS_CAPACITY = 1, 2, 3, 4
 
 u32, u64, i32 = C.c_uint32, C.c_uint64, C.c_int32
 P64 = C.POINTER(C.c_uint64)
@@ -150,6 +150,10 @@ SIGNATURES = {
     "afhe_rescale_batch": (C.c_int, [CTX, C.POINTER(CtRef), C.POINTER(CtRef), u32, u32]),
     "afhe_eval_copy_batch": (C.c_int, [CTX, C.POINTER(CtRef), C.POINTER(CtRef), u32, u32]),
     "afhe_eval_rotate_steps_batch": (C.c_int, [CTX, C.POINTER(CtRef), C.POINTER(CtRef), C.POINTER(i32), u32, u32]),
+    "afhe_ntt_plan_count": (C.c_int, [u32, P32]),
+    "afhe_ntt_plan_describe": (C.c_int, [u32, u32, C.c_char_p, u32]),
+    "afhe_ntt_set_plan": (C.c_int, [u32, u32]),
+    "afhe_ntt_get_plan": (C.c_int, [u32, P32]),
     "afhe_ivfpq_create": (C.c_int, [CTX, C.POINTER(IvfpqShape), C.POINTER(C.c_void_p)]),
     "afhe_ivfpq_destroy": (C.c_int, [C.c_void_p]),
     "afhe_ivfpq_set_centroids": (C.c_int, [C.c_void_p, P64, u32]),

@@ -1,19 +1,23 @@
-"""Autotuner for the batched key switch.
+"""Autotuner for the batched key switch and the NTT's tile shapes.
 
 For a parameter set on a given GPU it picks, per level, the key-switch
-implementation (the one-kernel key switch for N <= 2^13, or the multi-kernel
-ModUp / inner product / ModDown pipeline) and the number of ciphertexts per
-launch (a tile of the batch: fewer per launch shortens the tail of the last
-wave, more amortises launches and the key's L2 footprint). It times rotation
-batches on the device. The residues are the same for every choice, so the
-tuner only trades speed. Results are cached per (GPU, N, L, K, alpha) as JSON
-under anns_fhe_b200/tuning/.
+implementation (the one-kernel key switch, or the multi-kernel ModUp / inner
+product / ModDown pipeline) and the number of ciphertexts per launch (a tile
+of the batch: fewer per launch shortens the tail of the last wave, more
+amortises launches and the key's L2 footprint). It times rotation batches on
+the device. It also times every NTT plan of the ring degree (afhe_ntt_set_plan:
+values per thread for one-pass transforms; columns per CTA and chunk-tile size
+for two-pass ones) on batched forward and inverse transforms, and keeps the
+fastest. The residues are the same for every choice, so the tuner only trades
+speed. Results are cached per (GPU, N, L, K, alpha) as JSON under
+anns_fhe_b200/tuning/, with every candidate's time.
 
     python -m anns_fhe_b200.autotune --workload small     # tune and write the cache
 """
 from __future__ import annotations
 
 import argparse
+import ctypes as C
 import json
 import os
 import time
@@ -55,10 +59,13 @@ def cache_path(params: CkksParams, name: str | None = None) -> str:
     return os.path.join(CACHE_DIR, f"{gpu}_N{params.n}_L{params.L}_K{params.K}_a{params.alpha}.json")
 
 
-def chunk_candidates(lanes: int, sms: int) -> list[int]:
+def chunk_candidates(lanes: int, sms: int, capacity: int = 0) -> list[int]:
     """Ciphertexts per launch to try: fractions and multiples of one wave of
-    SMs, up to the context's lanes."""
+    SMs, multiples of the one-kernel key switch's capacity (ciphertexts it
+    runs at once; full waves), up to the context's lanes."""
     c = {max(1, sms // 4), max(1, sms // 2), sms, 2 * sms, 3 * sms, 4 * sms, lanes}
+    if capacity > 0:
+        c |= {k * capacity for k in range(1, 9)}
     return sorted(x for x in c if 1 <= x <= lanes)
 
 
@@ -66,7 +73,58 @@ TIE = 0.10   # candidates within this fraction of the fastest count as ties
 # Version of the key-switch kernels a cache was tuned against: a cache from
 # other kernels (e.g. before the one-kernel path existed at this ring degree)
 # is tuned again.
-KERNELS = 2
+KERNELS = 3
+
+
+def ntt_plan_count(log_n: int) -> int:
+    n = C.c_uint32()
+    L.check(L.load().afhe_ntt_plan_count(log_n, C.byref(n)), "ntt_plan_count")
+    return n.value
+
+
+def ntt_plan_describe(log_n: int, plan: int) -> str:
+    buf = C.create_string_buffer(160)
+    L.check(L.load().afhe_ntt_plan_describe(log_n, plan, buf, len(buf)), "ntt_plan_describe")
+    return buf.value.decode()
+
+
+def set_ntt_plan(log_n: int, plan: int) -> None:
+    """Tile shapes of every NTT at ring degree 2^log_n, process-wide."""
+    L.check(L.load().afhe_ntt_set_plan(log_n, plan), "ntt_set_plan")
+
+
+def get_ntt_plan(log_n: int) -> int:
+    p = C.c_uint32()
+    L.check(L.load().afhe_ntt_get_plan(log_n, C.byref(p)), "ntt_get_plan")
+    return p.value
+
+
+def time_ntt_plans(ctx: FheContext, polys: int, limbs: int, reps: int = 3) -> dict:
+    """{plan: microseconds per limb of a forward plus an inverse transform}
+    over `polys` polynomials of `limbs` limbs at offsets 0, limbs N, ...
+    (best of `reps` after a warm-up call each). Restores the plan in force."""
+    n, log_n = ctx.params.n, ctx.params.log_n
+    offs = (L.u64 * polys)(*[z * limbs * n for z in range(polys)])
+    ptr = C.cast(offs, L.P64)
+    lib = ctx.lib
+    keep = get_ntt_plan(log_n)
+    out = {}
+    try:
+        for plan in range(ntt_plan_count(log_n)):
+            set_ntt_plan(log_n, plan)
+            best = float("inf")
+            for r in range(reps + 1):
+                ctx.sync()
+                t0 = time.perf_counter()
+                L.check(lib.afhe_ntt_batch(ctx.h, ptr, polys, limbs, 0), "ntt_batch")
+                L.check(lib.afhe_ntt_batch(ctx.h, ptr, polys, limbs, 1), "ntt_batch")
+                ctx.sync()
+                if r:
+                    best = min(best, time.perf_counter() - t0)
+            out[plan] = best / (polys * limbs) * 1e6
+    finally:
+        set_ntt_plan(log_n, keep)
+    return out
 
 
 def pick(timings: dict) -> tuple:
@@ -116,12 +174,13 @@ def tune(params: CkksParams, levels, lanes: int, device: int = 0, verbose: bool 
             ctx.write_poly(i * w_max, np.concatenate([rng.integers(0, q, n, dtype=np.uint64)
                                                       for q in params.q[:max(levels)]]))
         fused_ok = ctx.get_option(L.OPT_KS_FUSED) == 1    # the context enables it where the GPU can run it
+        cap = ctx.get_option(L.OPT_KS_CAPACITY) if fused_ok else 0
         out = {}
         for lv in sorted(set(levels)):
             timings = {}
             for fused in ([True, False] if fused_ok else [False]):
                 ctx.set_option(L.OPT_KS_FUSED, int(fused))
-                for c in chunk_candidates(lanes, sm_count(device)):
+                for c in chunk_candidates(lanes, sm_count(device), cap if fused else 0):
                     ctx.set_option(L.OPT_CHUNK, c)
                     timings[(fused, c)] = time_rotations(ctx, lv, count)
                     if verbose:
@@ -133,32 +192,68 @@ def tune(params: CkksParams, levels, lanes: int, device: int = 0, verbose: bool 
         ctx.close()
 
 
-def save(path: str, params: CkksParams, choices: dict, lanes: int) -> None:
+def tune_ntt(params: CkksParams, lanes: int, device: int = 0, verbose: bool = False) -> dict:
+    """{"plan": fastest, "us_per_limb": {plan: time}, "describe": {plan: text}}
+    for batched transforms of `lanes` ciphertexts (2 lanes polynomials) at
+    the top level, capped at 2 GB of device memory."""
+    n, log_n, limbs = params.n, params.log_n, params.L
+    polys = max(1, min(2 * lanes, (2 << 30) // (limbs * n * 8)))
+    ctx = FheContext(params, poly_words=polys * limbs * n, key_words=1024, device=device, max_batch=1)
+    try:
+        rng = np.random.default_rng(11)
+        for z in range(polys):
+            ctx.write_poly(z * limbs * n, np.concatenate([rng.integers(0, q, n, dtype=np.uint64)
+                                                          for q in params.q[:limbs]]))
+        t = time_ntt_plans(ctx, polys, limbs)
+    finally:
+        ctx.close()
+    best = min(t, key=lambda p: (t[p] > min(t.values()) * (1 + TIE / 2), p))   # plan 0 unless another is clearly faster
+    if verbose:
+        for p, us in t.items():
+            print(f"NTT plan {p} ({ntt_plan_describe(log_n, p)}): {us:.3f} us/limb")
+    return {"plan": best, "us_per_limb": {str(p): v for p, v in t.items()},
+            "describe": {str(p): ntt_plan_describe(log_n, p) for p in t}}
+
+
+def save(path: str, params: CkksParams, choices: dict, lanes: int, ntt: dict | None = None) -> None:
     os.makedirs(os.path.dirname(path), exist_ok=True)
     with open(path, "w") as f:
         json.dump({"gpu": gpu_name(), "log_n": params.log_n, "L": params.L, "K": params.K,
                    "alpha": params.alpha, "lanes": lanes, "kernels": KERNELS,
-                   "levels": {str(k): asdict(v) for k, v in sorted(choices.items())}}, f, indent=1)
+                   "levels": {str(k): asdict(v) for k, v in sorted(choices.items())},
+                   "ntt": ntt}, f, indent=1)
 
 
-def load(path: str, lanes: int) -> dict | None:
-    """Cached choices, if the cache exists and was tuned for the same lanes."""
+def load_full(path: str, lanes: int) -> tuple[dict, dict | None] | None:
+    """(key-switch choices, NTT record) of a cache tuned for the same lanes
+    and kernels, else None."""
     if not os.path.exists(path):
         return None
     with open(path) as f:
         d = json.load(f)
     if d.get("lanes") != lanes or d.get("kernels") != KERNELS:
         return None
-    return {int(k): KsChoice(**v) for k, v in d["levels"].items()}
+    return {int(k): KsChoice(**v) for k, v in d["levels"].items()}, d.get("ntt")
+
+
+def load(path: str, lanes: int) -> dict | None:
+    """Cached key-switch choices, if the cache exists and was tuned for the same lanes."""
+    got = load_full(path, lanes)
+    return got[0] if got else None
 
 
 def load_or_tune(params: CkksParams, levels, lanes: int, device: int = 0) -> dict:
+    """Key-switch choices per level (cached or measured now); the NTT plan of
+    the cache (measured now when absent) is put in force."""
     path = cache_path(params)
-    got = load(path, lanes)
-    if got is not None and set(levels) <= set(got):
-        return got
-    choices = tune(params, levels, lanes, device)
-    save(path, params, choices, lanes)
+    got = load_full(path, lanes)
+    if got is not None and set(levels) <= set(got[0]) and got[1]:
+        choices, ntt = got
+    else:
+        choices = tune(params, levels, lanes, device)
+        ntt = tune_ntt(params, lanes, device)
+        save(path, params, choices, lanes, ntt)
+    set_ntt_plan(params.log_n, int(ntt["plan"]))
     return choices
 
 
@@ -174,9 +269,10 @@ def main() -> None:
     top = spec.eval_level or spec.num_q
     levels = [lv for lv in (top, top - 1, top - 2) if lv >= 1]
     choices = tune(params, levels, lanes, verbose=True)
+    ntt = tune_ntt(params, lanes, verbose=True)
     path = cache_path(params)
-    save(path, params, choices, lanes)
-    print(json.dumps({str(k): asdict(v) for k, v in choices.items()}), "->", path)
+    save(path, params, choices, lanes, ntt)
+    print(json.dumps({"levels": {str(k): asdict(v) for k, v in choices.items()}, "ntt_plan": ntt["plan"]}), "->", path)
 
 
 if __name__ == "__main__":

@@ -3,7 +3,7 @@ and ``lib/libafhe_accel_top.so``, the reference's ``fhe_accel_top`` symbol over
 it (csrc/fhe_accel_top_shim.cpp), which a host built against the reference's
 kernel ABI links in place of the HLS kernel object.
 
-Plain ``nvcc -shared`` over the sources in ``csrc/``; no torch extension, no
+One ``nvcc -c`` per source in ``csrc/`` (in parallel), linked by ``nvcc -shared``; no torch extension, no
 JIT cache: the libraries are built in-tree so they travel with the working tree.
 
     python -m anns_fhe_b200.build [--force] [--ptxas-verbose]
@@ -11,6 +11,7 @@ JIT cache: the libraries are built in-tree so they travel with the working tree.
 from __future__ import annotations
 
 import argparse
+import concurrent.futures
 import os
 import shutil
 import subprocess
@@ -22,6 +23,7 @@ LIBDIR = os.path.join(HERE, "lib")
 LIB = os.path.join(LIBDIR, "libafhe.so")
 SHIM = os.path.join(LIBDIR, "libafhe_accel_top.so")
 SHIM_SRC = os.path.join(CSRC, "fhe_accel_top_shim.cpp")
+OBJDIR = os.path.join(os.path.dirname(HERE), "_build", "afhe")
 ROOT = os.path.dirname(HERE)
 INCLUDE = os.path.join(ROOT, "include")
 
@@ -68,20 +70,32 @@ def build(force: bool = False, ptxas_verbose: bool = False, quiet: bool = True) 
         build_shim()
         return LIB
     os.makedirs(LIBDIR, exist_ok=True)
+    os.makedirs(OBJDIR, exist_ok=True)
+    nvcc = nvcc_path()
+
+    def compile_one(src: str):
+        obj = os.path.join(OBJDIR, src + ".o")
+        cmd = [nvcc, "-O3", "-std=c++17", *ARCH_FLAGS, "-lineinfo", "-Xcompiler", "-fPIC,-O3",
+               "--expt-relaxed-constexpr", "-I", INCLUDE, "-I", CSRC, "-c", os.path.join(CSRC, src), "-o", obj]
+        if ptxas_verbose:
+            cmd.insert(1, "-Xptxas=-v")
+        return obj, subprocess.run(cmd, capture_output=True, text=True)
+
+    # one nvcc per source, side by side (the NTT and key-switch instances dominate)
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, min(len(SOURCES), os.cpu_count() or 1))) as ex:
+        results = list(ex.map(compile_one, SOURCES))
+    log = ""
+    for src, (obj, res) in zip(SOURCES, results):
+        if res.returncode != 0:
+            raise RuntimeError(f"nvcc failed on {src}:\n" + res.stdout + res.stderr)
+        log += res.stdout + res.stderr
     tmp = LIB + ".tmp"
-    cmd = [
-        nvcc_path(), "-O3", "-std=c++17", *ARCH_FLAGS, "-lineinfo",
-        "-Xcompiler", "-fPIC,-O3", "-shared", "--expt-relaxed-constexpr",
-        "-I", INCLUDE, "-I", CSRC,
-        "-o", tmp, *[os.path.join(CSRC, f) for f in SOURCES],
-    ]
-    if ptxas_verbose:
-        cmd.insert(1, "-Xptxas=-v")
-    res = subprocess.run(cmd, capture_output=True, text=True)
+    res = subprocess.run([nvcc, *ARCH_FLAGS, "-shared", "-o", tmp, *[obj for obj, _ in results]],
+                         capture_output=True, text=True)
     if res.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + res.stdout + res.stderr)
+        raise RuntimeError("nvcc link failed:\n" + res.stdout + res.stderr)
     if not quiet or ptxas_verbose:
-        sys.stdout.write(res.stdout + res.stderr)
+        sys.stdout.write(log + res.stdout + res.stderr)
     os.replace(tmp, LIB)
     build_shim(force=True)
     return LIB

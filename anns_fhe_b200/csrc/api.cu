@@ -575,6 +575,10 @@ int afhe_ctx_get_option(afhe_ctx* ctx, uint32_t option, int64_t* value) {
     case AFHE_OPT_KS_FUSED: *value = ctx->ks_fused ? 1 : 0; return AFHE_OK;
     case AFHE_OPT_CHUNK: *value = ctx->chunk ? ctx->chunk : ctx->lanes; return AFHE_OK;
     case AFHE_OPT_FUSED_MIN: *value = ctx->fused_min; return AFHE_OK;
+    case AFHE_OPT_KS_CAPACITY:
+        if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, AFHE_E_CUDA, "cudaSetDevice");
+        *value = key_switch_fused_capacity(ctx->log_n);
+        return AFHE_OK;
     default: return fail(ctx, AFHE_E_ARG, "unknown option");
     }
 }
@@ -592,6 +596,37 @@ int afhe_host_free(void* p) {
     if (!p) return AFHE_OK;
     cudaError_t e = cudaFreeHost(p);
     if (e != cudaSuccess) return cuda_fail(nullptr, e, "cudaFreeHost");
+    return AFHE_OK;
+}
+
+int afhe_ntt_plan_count(uint32_t log_n, uint32_t* count) {
+    if (!count) return fail(nullptr, AFHE_E_ARG, "null argument");
+    *count = (uint32_t)ntt_plan_count((int)log_n);
+    return *count ? AFHE_OK : fail(nullptr, AFHE_E_ARG, "log_n outside [10, 16]");
+}
+
+int afhe_ntt_plan_describe(uint32_t log_n, uint32_t plan, char* buf, uint32_t len) {
+    if (!buf || !len) return fail(nullptr, AFHE_E_ARG, "null argument");
+    if (plan >= (uint32_t)ntt_plan_count((int)log_n)) return fail(nullptr, AFHE_E_ARG, "no such plan");
+    const NttPlan fwd = make_plan((int)log_n, false, (int)plan);
+    if (fwd.npass == 1)
+        snprintf(buf, len, "one pass, %d values per thread", fwd.ept[0]);
+    else
+        snprintf(buf, len, "columns %d per CTA (%d values per thread), chunk tiles %d words (%d values per thread)",
+                 1 << fwd.g[0].log_c, fwd.ept[0], 1 << (fwd.g[1].P + fwd.g[1].log_c), fwd.ept[1]);
+    return AFHE_OK;
+}
+
+int afhe_ntt_set_plan(uint32_t log_n, uint32_t plan) {
+    if (plan >= (uint32_t)ntt_plan_count((int)log_n)) return fail(nullptr, AFHE_E_ARG, "no such plan");
+    set_ntt_plan((int)log_n, (int)plan);
+    return AFHE_OK;
+}
+
+int afhe_ntt_get_plan(uint32_t log_n, uint32_t* plan) {
+    if (!plan) return fail(nullptr, AFHE_E_ARG, "null argument");
+    if (!ntt_plan_count((int)log_n)) return fail(nullptr, AFHE_E_ARG, "log_n outside [10, 16]");
+    *plan = (uint32_t)ntt_plan((int)log_n);
     return AFHE_OK;
 }
 

@@ -210,6 +210,9 @@ cudaError_t launch_key_switch(int log_n, const OpTabs& t, const LimbJob* jobs_qp
 // region's word order) as (k mod q, Shoup companion) pairs; the inner product
 // then multiplies with Shoup's method instead of a full 128-bit reduction.
 bool key_switch_fused_supported(int log_n);
+// ciphertexts the one-kernel key switch holds at once on the current device
+// (resident CTAs at N <= 2^13, resident clusters above; 0: cannot run)
+int key_switch_fused_capacity(int log_n);
 size_t ks_fused_scratch_words(uint32_t n, uint32_t sizeQl, uint32_t K);
 cudaError_t launch_key_switch_fused(int log_n, const OpTabs& t, uint32_t sizeQl, uint32_t K, const u64* key, u64 evk_a,
                                     u64 evk_b, uint32_t key_stride, uint32_t key_pbase, u64* arena, u64* scratch,

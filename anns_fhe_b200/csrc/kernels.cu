@@ -20,6 +20,10 @@ static std::atomic<uint64_t> g_launches{0};
 void count_launches(uint64_t k) { g_launches.fetch_add(k, std::memory_order_relaxed); }
 uint64_t launches_so_far() { return g_launches.load(std::memory_order_relaxed); }
 
+static std::atomic<int> g_ntt_plan[17];
+int ntt_plan(int log_n) { return log_n >= 0 && log_n <= 16 ? g_ntt_plan[log_n].load(std::memory_order_relaxed) : 0; }
+void set_ntt_plan(int log_n, int plan) { g_ntt_plan[log_n].store(plan, std::memory_order_relaxed); }
+
 // ---------------------------------------------------------------------------
 // elementwise
 // ---------------------------------------------------------------------------

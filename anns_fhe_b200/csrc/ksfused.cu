@@ -778,6 +778,13 @@ int cluster_capacity() {
     return n;
 }
 
+template <class Kern>
+cudaError_t occupancy_of(Kern kern, uint32_t threads, size_t smem, int* per_sm) {
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    return cudaOccupancyMaxActiveBlocksPerMultiprocessor(per_sm, kern, (int)threads, smem);
+}
+
 __global__ void key_prep_kernel(const u64* __restrict__ key, ulonglong2* __restrict__ prep,
                                 const PrimeConst* __restrict__ pc, uint32_t n, uint32_t S, u64 words) {
     for (u64 w = blockIdx.x * (u64)blockDim.x + threadIdx.x; w < words; w += (u64)gridDim.x * blockDim.x) {
@@ -788,6 +795,32 @@ __global__ void key_prep_kernel(const u64* __restrict__ key, ulonglong2* __restr
 }
 
 }  // namespace
+
+int key_switch_fused_capacity(int log_n) {
+    if (log_n >= 14 && log_n <= 16)
+        return log_n == 14 ? cluster_capacity<1>() : log_n == 15 ? cluster_capacity<2>() : cluster_capacity<3>();
+    if (log_n < 10 || log_n > 13) return 0;
+    int dev = 0, sms = 0, per = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    const uint32_t qn = 1u << log_n;
+    const size_t smem = 3ull * (qn + qn / 16) * sizeof(u64);
+    cudaError_t e = cudaSuccess;
+    switch (log_n) {
+    case 10: e = occupancy_of(ks_fused_kernel<10, 0, true>, qn / 8, smem, &per); break;
+    case 11: e = occupancy_of(ks_fused_kernel<11, 0, true>, qn / 8, smem, &per); break;
+    case 12: e = occupancy_of(ks_fused_kernel<12, 0, true>, qn / 8, smem, &per); break;
+    default: e = occupancy_of(ks_fused_kernel<13, 0, true>, qn / 8, smem, &per); break;
+    }
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return per * sms;
+}
 
 bool key_switch_fused_supported(int log_n) {
     if (log_n >= 10 && log_n <= 13) return true;

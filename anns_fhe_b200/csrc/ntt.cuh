@@ -269,19 +269,19 @@ __device__ __forceinline__ void ntt_rounds(u64* sm, const ulonglong2* tw, const 
 
 // One pass over 2^(P + LOGC)-word tiles: stage the tile in shared memory
 // (through the prologue on the first pass), run the rounds, write it back
-// (through the epilogue on the last pass, canonical residues).
-// Values per thread: 16 for 8192-word tiles (512 threads, two CTAs per SM
-// whose barriers interleave), else 8.
-constexpr int ntt_ept(int P, int LOGC) { return P + LOGC >= 13 ? 16 : 8; }
+// (through the epilogue on the last pass, canonical residues). EPT values per
+// thread (8 or 16); CTAs of 1024 threads are launched one per SM's register
+// budget, smaller ones two.
+constexpr uint32_t ntt_threads(int P, int LOGC, int EPT) { return (1u << (P + LOGC)) / EPT; }
+constexpr int ntt_min_ctas(int P, int LOGC, int EPT) { return ntt_threads(P, LOGC, EPT) >= 1024 ? 1 : 2; }
 
-template <bool INV, int P, int LOGC, bool COL, class Pro, class Epi>
-__global__ void __launch_bounds__((1u << (P + LOGC)) / ntt_ept(P, LOGC), 2)
+template <bool INV, int P, int LOGC, bool COL, int EPT, class Pro, class Epi>
+__global__ void __launch_bounds__(ntt_threads(P, LOGC, EPT), ntt_min_ctas(P, LOGC, EPT))
 ntt_kernel(NttGeom g, PrimeTables pt, const LimbJob* __restrict__ jobs, u64* __restrict__ mid,
            const ZBases zb, Pro pro, Epi epi) {
     extern __shared__ u64 sm[];
     constexpr uint32_t C = 1u << LOGC;
     constexpr uint32_t TILE = 1u << (P + LOGC);
-    constexpr int EPT = ntt_ept(P, LOGC);
     constexpr uint32_t T = TILE / EPT;
     const LimbJob job = jobs[blockIdx.y];
     const uint32_t z = blockIdx.z;
@@ -317,49 +317,97 @@ ntt_kernel(NttGeom g, PrimeTables pt, const LimbJob* __restrict__ jobs, u64* __r
     }
 }
 
-// Pass plan for a transform of size 2^log_n.
+// Tile shapes of a transform ("plans"), chosen per ring degree at run time
+// (afhe_ntt_set_plan; the autotuner times them). Every plan computes the
+// same butterflies on the same values, so the residues do not depend on it.
+//   N <= 2^13, one pass over the whole limb: plan 0 the default values per
+//     thread (16 for 8192-word limbs, else 8), plan 1 the other choice;
+//   N >= 2^14, two passes (high bits in columns, then low bits in chunks):
+//     plan = 3 * t + c: columns per CTA 2^{4, 3, 5}[c] in the column pass,
+//     chunk-pass tiles of 2^{12, 13}[t] words. Plan 0 is 16 columns and
+//     4096-word tiles.
+// Values per thread in a two-pass transform: 16 for 8192-word tiles, else 8.
+constexpr int kNttPlansOnePass = 2;
+constexpr int kNttPlansTwoPass = 6;
+inline int ntt_plan_count(int log_n) {
+    return log_n < 10 || log_n > 16 ? 0 : (log_n <= 13 ? kNttPlansOnePass : kNttPlansTwoPass);
+}
+// the plan in force per log_n, process-wide (kernels.cu)
+int ntt_plan(int log_n);
+void set_ntt_plan(int log_n, int plan);
+
 struct NttPlan {
     int npass;
+    int ept[2];
     NttGeom g[2];
 };
 
-inline NttPlan make_plan(int log_n, bool inverse) {
+inline NttPlan make_plan(int log_n, bool inverse, int plan) {
     NttPlan pl;
-    if (log_n <= 13) {   // whole limb in shared memory (<= 68 KB), N / 8 threads
+    if (log_n <= 13) {   // whole limb in shared memory (<= 68 KB)
         pl.npass = 1;
         NttGeom a{};
         a.log_n = log_n; a.lo_bit = 0; a.P = log_n; a.log_c = 0; a.first = 1; a.last = 1;
         pl.g[0] = a;
+        const int def = log_n >= 13 ? 16 : 8;
+        pl.ept[0] = plan == 1 ? 24 - def : def;
         return pl;
     }
+    static const int col_c[3] = {4, 3, 5};
+    const int c = col_c[plan % 3], tl = 12 + plan / 3;
     int pa = (log_n + 1) / 2;     // high (column) pass bits
     int pb = log_n - pa;          // low (chunk) pass bits
     NttGeom col{}, chk{};
-    col.log_n = log_n; col.lo_bit = pb; col.P = pa; col.log_c = 4;
-    chk.log_n = log_n; chk.lo_bit = 0; chk.P = pb; chk.log_c = 12 - pb;
+    col.log_n = log_n; col.lo_bit = pb; col.P = pa; col.log_c = c;
+    chk.log_n = log_n; chk.lo_bit = 0; chk.P = pb; chk.log_c = tl - pb;
+    const int ept_col = pa + c >= 13 ? 16 : 8, ept_chk = tl >= 13 ? 16 : 8;
     pl.npass = 2;
-    if (!inverse) { pl.g[0] = col; pl.g[1] = chk; }
-    else { pl.g[0] = chk; pl.g[1] = col; }
+    if (!inverse) { pl.g[0] = col; pl.g[1] = chk; pl.ept[0] = ept_col; pl.ept[1] = ept_chk; }
+    else { pl.g[0] = chk; pl.g[1] = col; pl.ept[0] = ept_chk; pl.ept[1] = ept_col; }
     pl.g[0].first = 1; pl.g[0].last = 0;
     pl.g[1].first = 0; pl.g[1].last = 1;
     return pl;
 }
 
-template <bool INV, int P, int LOGC, bool COL, class Pro, class Epi>
+template <bool INV, int P, int LOGC, bool COL, int EPT, class Pro, class Epi>
 inline cudaError_t launch_pass(const NttGeom& g, const PrimeTables& pt, const LimbJob* jobs, uint32_t njobs,
                                uint32_t nz, u64* mid, const ZBases& zb, const Pro& pro, const Epi& epi,
                                cudaStream_t st) {
     constexpr uint32_t TILE = 1u << (P + LOGC);
     const uint32_t ctas = 1u << (g.log_n - P - LOGC);
     const size_t smem = (size_t)(TILE + TILE / 16) * sizeof(u64);
-    auto kern = ntt_kernel<INV, P, LOGC, COL, Pro, Epi>;
+    auto kern = ntt_kernel<INV, P, LOGC, COL, EPT, Pro, Epi>;
     if (smem > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
-    kern<<<dim3(ctas, njobs, nz), TILE / ntt_ept(P, LOGC), smem, st>>>(g, pt, jobs, mid, zb, pro, epi);
+    kern<<<dim3(ctas, njobs, nz), ntt_threads(P, LOGC, EPT), smem, st>>>(g, pt, jobs, mid, zb, pro, epi);
     count_launches(1);
     return cudaSuccess;
+}
+
+// The pass with geometry g and EPT values per thread, dispatched to its
+// compile-time instance (every shape some plan uses).
+template <bool INV, class Pro, class Epi>
+inline cudaError_t launch_shape(const NttGeom& g, int ept, const PrimeTables& pt, const LimbJob* jobs,
+                                uint32_t njobs, uint32_t nz, u64* mid, const ZBases& zb, const Pro& pro,
+                                const Epi& epi, cudaStream_t st) {
+#define AFHE_NTT_SHAPE(P_, C_, COL_, EPT_)                                                                  \
+    if (g.P == P_ && g.log_c == C_ && (g.lo_bit > 0) == COL_ && ept == EPT_)                                \
+        return launch_pass<INV, P_, C_, COL_, EPT_>(g, pt, jobs, njobs, nz, mid, zb, pro, epi, st);
+    // one pass
+    AFHE_NTT_SHAPE(10, 0, false, 8) AFHE_NTT_SHAPE(10, 0, false, 16)
+    AFHE_NTT_SHAPE(11, 0, false, 8) AFHE_NTT_SHAPE(11, 0, false, 16)
+    AFHE_NTT_SHAPE(12, 0, false, 8) AFHE_NTT_SHAPE(12, 0, false, 16)
+    AFHE_NTT_SHAPE(13, 0, false, 8) AFHE_NTT_SHAPE(13, 0, false, 16)
+    // column passes: 2^7 (N = 2^14) or 2^8 (2^15, 2^16) bits, 8 / 16 / 32 columns
+    AFHE_NTT_SHAPE(7, 3, true, 8) AFHE_NTT_SHAPE(7, 4, true, 8) AFHE_NTT_SHAPE(7, 5, true, 8)
+    AFHE_NTT_SHAPE(8, 3, true, 8) AFHE_NTT_SHAPE(8, 4, true, 8) AFHE_NTT_SHAPE(8, 5, true, 16)
+    // chunk passes: 4096- or 8192-word tiles
+    AFHE_NTT_SHAPE(7, 5, false, 8) AFHE_NTT_SHAPE(7, 6, false, 16)
+    AFHE_NTT_SHAPE(8, 4, false, 8) AFHE_NTT_SHAPE(8, 5, false, 16)
+#undef AFHE_NTT_SHAPE
+    return cudaErrorInvalidValue;
 }
 
 // Launch a full transform over `njobs` limbs x `nz` polynomials. Between
@@ -368,26 +416,9 @@ template <bool INV, class Pro, class Epi>
 inline cudaError_t launch_ntt(int log_n, const PrimeTables& pt, const LimbJob* jobs, uint32_t njobs, uint32_t nz,
                               u64* mid, const ZBases& zb, Pro pro, Epi epi, cudaStream_t st) {
     if (njobs == 0 || nz == 0) return cudaSuccess;
-    NttPlan pl = make_plan(log_n, INV);
+    NttPlan pl = make_plan(log_n, INV, ntt_plan(log_n));
     for (int i = 0; i < pl.npass; ++i) {
-        const NttGeom& g = pl.g[i];
-        const bool col = g.lo_bit > 0;
-        cudaError_t e = cudaErrorInvalidValue;
-        if (!col && g.log_c == 0) {
-            switch (g.P) {
-            case 10: e = launch_pass<INV, 10, 0, false>(g, pt, jobs, njobs, nz, mid, zb, pro, epi, st); break;
-            case 11: e = launch_pass<INV, 11, 0, false>(g, pt, jobs, njobs, nz, mid, zb, pro, epi, st); break;
-            case 12: e = launch_pass<INV, 12, 0, false>(g, pt, jobs, njobs, nz, mid, zb, pro, epi, st); break;
-            case 13: e = launch_pass<INV, 13, 0, false>(g, pt, jobs, njobs, nz, mid, zb, pro, epi, st); break;
-            default: break;
-            }
-        } else if (col && g.log_c == 4) {
-            if (g.P == 7) e = launch_pass<INV, 7, 4, true>(g, pt, jobs, njobs, nz, mid, zb, pro, epi, st);
-            else if (g.P == 8) e = launch_pass<INV, 8, 4, true>(g, pt, jobs, njobs, nz, mid, zb, pro, epi, st);
-        } else if (!col) {
-            if (g.P == 7 && g.log_c == 5) e = launch_pass<INV, 7, 5, false>(g, pt, jobs, njobs, nz, mid, zb, pro, epi, st);
-            else if (g.P == 8 && g.log_c == 4) e = launch_pass<INV, 8, 4, false>(g, pt, jobs, njobs, nz, mid, zb, pro, epi, st);
-        }
+        cudaError_t e = launch_shape<INV>(pl.g[i], pl.ept[i], pt, jobs, njobs, nz, mid, zb, pro, epi, st);
         if (e != cudaSuccess) return e;
     }
     return cudaGetLastError();

@@ -127,6 +127,8 @@ def measure(args, spec, rank: int, world: int, steps: int, warmup: int, batch: i
     legs) the full-level sample, serving and roofline. Returns the line."""
     import torch
 
+    from anns_fhe_b200 import _lib as L
+    from anns_fhe_b200.autotune import get_ntt_plan
     from anns_fhe_b200.replicas import aggregate, query_seed
     from anns_fhe_b200.workloads import Workload
 
@@ -196,7 +198,9 @@ def measure(args, spec, rank: int, world: int, steps: int, warmup: int, batch: i
             "run": {"lanes": lanes, "setup_s": round(wl.setup_s, 1),
                     "tuning": ({str(k): [int(v.fused), v.chunk] for k, v in wl.tuning.items()} if wl.tuning
                                else None),
-                    "lane_scratch_gb": round(wl.ctx.scratch_bytes() / 1e9, 1)},
+                    "lane_scratch_gb": round(wl.ctx.scratch_bytes() / 1e9, 1),
+                    "ks_capacity": wl.ctx.get_option(L.OPT_KS_CAPACITY),
+                    "ntt_plan": get_ntt_plan(spec.log_n), "stage_driver": "native" if wl.iqm.native else "python"},
         }
         if legs and large and not args.skip_full_level:
             line["full_level"] = full_level_leg(wl, stream, rank)
@@ -370,11 +374,19 @@ def ntt_config(reps: int = 5):
 
     from anns_fhe_b200.primitives import NttBatch
     from anns_fhe_b200.profiling import load_peaks
+    from anns_fhe_b200.autotune import ntt_plan_describe, set_ntt_plan, time_ntt_plans
     wl = NttBatch()
     st = torch.cuda.ExternalStream(wl.ctx.lib.afhe_stream(wl.ctx.h))
     peak, src = load_peaks()
+    # every tile plan timed (autotuner), the fastest used below
+    plans = time_ntt_plans(wl.ctx, wl.polys, wl.limbs)
+    best = min(plans, key=plans.get)
+    set_ntt_plan(wl.params.log_n, best)
+    for z in range(wl.polys):
+        wl.ctx.write_poly(z * wl.w, wl.input_poly(z))
     out = {"workload": "ntt_64ct_x2_x24limbs_N65536", "algorithmic_bytes_per_call": wl.algorithmic_bytes(),
-           "butterflies_per_call": wl.butterflies()}
+           "butterflies_per_call": wl.butterflies(), "plan": best, "plan_shape": ntt_plan_describe(16, best),
+           "plans_us_per_limb_fwd_plus_inv": {str(k): round(v, 3) for k, v in plans.items()}}
     for inv in (False, True):
         for _ in range(2):
             wl.transform(inv)

@@ -175,7 +175,8 @@ int afhe_read_poly_async(afhe_ctx* ctx, uint64_t word_offset, uint64_t* dst, uin
 int afhe_copy_poly(afhe_ctx* ctx, uint64_t dst_offset, uint64_t src_offset, uint64_t count);
 /* Run-time options of a context (no counterpart in the reference; the
  * autotuner, anns_fhe_b200/autotune.py, picks them per GPU and parameter set):
- *   AFHE_OPT_KS_FUSED  1: the one-kernel key switch (N <= 2^13), 0: the
+ *   AFHE_OPT_KS_FUSED  1: the one-kernel key switch (one CTA per ciphertext
+ *                      at N <= 2^13, a cluster of N / 2^13 CTAs above), 0: the
  *                      multi-kernel pipeline. Same residues either way.
  *   AFHE_OPT_CHUNK     ciphertexts per launch of a batched call, 1..lanes
  *                      (0: all lanes). Same residues for any value. */
@@ -187,6 +188,11 @@ int afhe_copy_poly(afhe_ctx* ctx, uint64_t dst_offset, uint64_t src_offset, uint
  *                      cluster above N = 2^13, so a small launch leaves most
  *                      SMs idle). Default: half a wave of SMs. Same residues. */
 #define AFHE_OPT_FUSED_MIN 3u
+/*   AFHE_OPT_KS_CAPACITY (read only) ciphertexts the one-kernel key switch
+ *                      runs at once on this GPU (CTAs, or clusters above
+ *                      N = 2^13, resident together): a launch of a multiple
+ *                      of it fills its waves; 0 where it cannot run. */
+#define AFHE_OPT_KS_CAPACITY 4u
 int afhe_ctx_set_option(afhe_ctx* ctx, uint32_t option, int64_t value);
 int afhe_ctx_get_option(afhe_ctx* ctx, uint32_t option, int64_t* value);
 /* Page-locked host memory for the transfers above (the reference's host
@@ -313,6 +319,18 @@ int afhe_ntt_batch(afhe_ctx* ctx, const uint64_t* polys, uint32_t count, uint32_
  * (generate_interactive_test_vectors.cpp:443-447); decoding is the caller's. */
 int afhe_decrypt_batch(afhe_ctx* ctx, const afhe_ct_ref* cts, uint32_t count, uint64_t s_offset,
                        uint64_t out_offset, uint32_t limbs);
+/* NTT tile shapes ("plans"), per ring degree 2^log_n, process-wide (every
+ * context of that degree, from the next launch). Plans change only launch
+ * shapes; every plan gives the same residues. N <= 2^13 (one pass over the
+ * limb): 2 plans, values per thread 8 or 16. N >= 2^14 (two passes): 6 plans,
+ * columns per CTA of the column pass (16, 8, 32) x words per tile of the
+ * chunk pass (4096, 8192). Plan 0 is the default. The autotuner
+ * (anns_fhe_b200/autotune.py) times them. The one-kernel key switch has its
+ * own transform and ignores the plan. */
+int afhe_ntt_plan_count(uint32_t log_n, uint32_t* count);
+int afhe_ntt_plan_describe(uint32_t log_n, uint32_t plan, char* buf, uint32_t len);
+int afhe_ntt_set_plan(uint32_t log_n, uint32_t plan);
+int afhe_ntt_get_plan(uint32_t log_n, uint32_t* plan);
 /* Kernels launched by this library so far (host-side count, all contexts). */
 uint64_t afhe_kernel_launches(void);
 /* acc[i] = acc[i] + rotate(in[i], total_rot), bit-identical to eval_rotate
