@@ -27,7 +27,10 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 # integer pipe's utilisation. The captures are summarised under profiles/.
 KS_CAPTURES: dict = {
     (8192, 3, 1): {"kernel": "ks_fused_kernel<13, 1>", "ciphertexts": 148, "dram_bytes": 175.3e6,
-                   "fmaheavy": 0.580},
+                   "pipe": "fmaheavy (IMAD)", "util": 0.580},
+    # clusters of 4 CTAs; 37 clusters ran as two waves (32 resident at once)
+    (32768, 3, 4): {"kernel": "ks_fused_kernel<13, 2, 1>", "ciphertexts": 37, "dram_bytes": 402.9e6,
+                    "pipe": "alu", "util": 0.387},
 }
 
 
@@ -99,7 +102,8 @@ def ks_roofline(params, lanes: int, reps: int = 20, level: int = 0, nbuf: int = 
     if cap and launches == 1 and fused:
         # the capture's per-ciphertext traffic scaled to this launch, the key once
         traffic = (cap["dram_bytes"] - key_bytes) * lanes / cap["ciphertexts"] + key_bytes
-        int_pipe = {"pipe": "fmaheavy (IMAD)", "frac": cap["fmaheavy"], "kernel": cap["kernel"]}
+        int_pipe = {"pipe": cap["pipe"], "frac": cap["util"], "kernel": cap["kernel"],
+                    "captured_ciphertexts": cap["ciphertexts"]}
     kind = "one-kernel" if fused and launches == 1 else f"{launches:g}-launch"
     return {"bound": "hbm", "kernel": f"rotation key switch, {kind} (N={n}, {L} + {K} limbs, "
                                       f"{lanes} ciphertexts per call)",

@@ -31,7 +31,9 @@ same scale. A step is 256 queries through the server's operator chain
   the continuous-batching server on a Poisson trace).
 
 --workload small makes the small configuration the headline. The config 2,
-3 and 5 drivers are --ntt-config, --ks-config and --serve-sweep.
+3 and 5 drivers are --ntt-config, --ks-config and --serve-sweep;
+--ref-shape times the key switch at the reference's own shape (N = 2^14,
+three digits) on the GPU beside the reference's HLS key switch on the host.
 
 Multi-GPU: replicas only (independent queries per rank, no collective).
 """
@@ -407,6 +409,68 @@ def ntt_config(reps: int = 5):
     print(json.dumps(out))
 
 
+def ref_shape(seconds: float = 10.0, cts: int = 128, reps: int = 10):
+    """Reference-shape driver: key switches per second at the reference's own
+    shape (N = 16384, 11 Q primes of which 10 in use, 4 P primes, alpha 4:
+    three digits). CPU: the reference's HLS key switch compiled from its
+    sources (oracle/_ref), one process per host core, timed first so the
+    spawned pool never sits beside a CUDA context. GPU: this repository's
+    batched key switch on the same primes, `cts` ciphertexts per launch, as
+    afhe_eval_rotate_batch by one step (the automorphism is folded into the
+    key switch's loads; c0's automorphism and add are the only extra work),
+    CUDA events on the context stream. One JSON line."""
+    import ctypes as C
+
+    import numpy as np
+
+    from anns_fhe_b200._lib import CtRef, check
+    from anns_fhe_b200.driver import CkksParams, FheContext, find_ntt_primes
+    q = find_ntt_primes(14, 60, 1)
+    q += find_ntt_primes(14, 45, 10, q)
+    p = find_ntt_primes(14, 60, 4, q)
+    from oracle.refshape import PARTS, SIZE_QL, reference_key_switch_rate
+    cpu = reference_key_switch_rate(q, p, seconds=seconds)
+
+    import torch
+    prm = CkksParams(14, q, p, 4)
+    n, sq = prm.n, SIZE_QL
+    assert prm.dnum == PARTS
+    w = sq * n
+    ctx = FheContext(prm, poly_words=4 * cts * w, key_words=prm.key_words(), max_batch=cts)
+    rng = np.random.default_rng(5)
+    allp = prm.q + prm.p
+    ctx.write_key(0, np.concatenate([rng.integers(0, x, n, dtype=np.uint64) for _ in range(2 * prm.dnum)
+                                     for x in allp]))
+    check(ctx.lib.afhe_add_rotation_key(ctx.h, 1, 0), "add_rotation_key")
+    for z in range(2 * cts):
+        ctx.write_poly(z * w, np.concatenate([rng.integers(0, x, n, dtype=np.uint64) for x in prm.q[:sq]]))
+    ins, outs = (CtRef * cts)(), (CtRef * cts)()
+    for z in range(cts):
+        ins[z].c0_offset, ins[z].c1_offset = 2 * z * w, (2 * z + 1) * w
+        outs[z].c0_offset, outs[z].c1_offset = (2 * cts + 2 * z) * w, (2 * cts + 2 * z + 1) * w
+    stream = torch.cuda.ExternalStream(ctx.lib.afhe_stream(ctx.h))
+
+    def launch():
+        check(ctx.lib.afhe_eval_rotate_batch(ctx.h, ins, outs, cts, 1, sq), "eval_rotate_batch")
+    for _ in range(3):
+        launch()
+    ctx.sync()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(reps):
+        launch()
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    ctx.close()
+    gpu = cts * reps / (ms / 1e3)
+    print(json.dumps({"driver": "reference shape", "unit": "key switches/s",
+                      "shape": f"N = 16384, {sq} of 11 Q limbs + 4 P limbs, {PARTS} digits of 4",
+                      "gpu": {"value": gpu, "ciphertexts_per_launch": cts, "launches": reps,
+                              "ms_per_launch": ms / reps},
+                      "cpu_reference": cpu, "gpu_over_cpu": gpu / cpu["value"]}), flush=True)
+
+
 def ks_config(reps: int = 3):
     """Config 3: batched hybrid key switching and rotation at N = 2^16 (24 + 8
     limbs, dnum 3): 32 ciphertexts at seeded levels 8-24, rotate-and-sum by
@@ -466,9 +530,14 @@ def main():
     ap.add_argument("--mixed", action="store_true", help="--serve-sweep: mixed query levels 6-12 and nprobe")
     ap.add_argument("--ntt-config", action="store_true", help="config 2 driver (64 ct x 2 x 24 limbs, N=2^16)")
     ap.add_argument("--ks-config", action="store_true", help="config 3 driver (32 ct, N=2^16, dnum 3)")
+    ap.add_argument("--ref-shape", action="store_true",
+                    help="key switches/s at the reference's own shape (N=2^14, 3 digits): its HLS key switch "
+                         "on the host cores beside this one on the GPU")
     args = ap.parse_args()
     if args.ntt_config:
         return ntt_config()
+    if args.ref_shape:
+        return ref_shape()
     if args.ks_config:
         return ks_config()
     if args.serve_sweep:
