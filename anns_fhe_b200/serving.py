@@ -273,16 +273,24 @@ class ServingLoop:
     """
 
     def __init__(self, backend, budget_bytes: int | None = None, max_inflight: int | None = None,
-                 max_admit: int | None = None, keep_results: bool = False, defer_from: int | None = 64):
+                 max_admit: int | None = None, keep_results: bool = False, defer_from: int | None = 64,
+                 shed_after: float | None = None):
         """defer_from: the client takes a tick's results during the next tick
         (behind that tick's stage 1) when the tick ran at least this many
         queries (stage 1 plus stage 3), and at the end of the tick otherwise.
         Deferring keeps the GPU busy while the client works, which pays
         when ticks are large; taking them at once puts no stage-1 launch
         ahead of them, which keeps latency down when ticks are small.
-        0: always defer; None: never."""
+        0: always defer; None: never.
+        shed_after: load shedding (real-time runs): a request still waiting
+        for admission this many seconds after its arrival is refused (kept
+        in `shed`) instead of served late. Above the server's capacity the
+        queue then stays bounded, and the completed requests' latency stays
+        near shed_after plus one query's service time. None: never shed."""
         self.b = backend
         self.defer_from = defer_from
+        self.shed_after = shed_after
+        self.shed: list[Request] = []
         cap = len(backend.records)
         if budget_bytes is not None:
             cap = min(cap, int(budget_bytes // backend.bytes_per_query))
@@ -314,6 +322,9 @@ class ServingLoop:
             t = now()
             while pending and (not realtime or pending[0].arrival <= t):
                 waiting.append(pending.popleft())
+            if realtime and self.shed_after is not None:
+                while waiting and t - waiting[0].arrival > self.shed_after:
+                    self.shed.append(waiting.popleft())
             admit = []
             while waiting and free and len(admit) < self.max_admit:
                 req = waiting.popleft()

@@ -323,11 +323,15 @@ def run_reference(args):
 # drivers for the other configurations
 # ---------------------------------------------------------------------------
 def serve_sweep(rates, seconds: float, batch: int, workload: str = "small", mixed: bool = False,
-                plain_queries: int = 32, defer_from: int | None = 64):
+                plain_queries: int = 32, defer_from: int | None = 64, shed_after: float | None = None,
+                max_admit: int | None = None):
     """Config 5: the plain path's latency and rate, then the served loop at
     each offered rate for `seconds` (seeded Poisson arrivals); one JSON line
     per rate. `mixed`: levels drawn from 6..12 and nprobe from {4, 8, 16, 32},
-    on the large configuration, with a 120 GB admission budget."""
+    on the large configuration, with a 120 GB admission budget. shed_after:
+    requests not admitted within this many seconds of arriving are refused
+    (counted as shed), which bounds the queue above capacity; max_admit:
+    queries admitted per tick (default: the lanes)."""
     import gc
 
     import numpy as np
@@ -360,10 +364,13 @@ def serve_sweep(rates, seconds: float, batch: int, workload: str = "small", mixe
         trace = make_trace(poisson_arrivals(r, seconds, seed=int(r * 10)), pool=batch, seed=int(r * 10) + 1,
                            nprobes=nprobes)
         gc.collect()
-        loop = ServingLoop(be, budget_bytes=budget, defer_from=defer_from)
+        loop = ServingLoop(be, budget_bytes=budget, defer_from=defer_from, shed_after=shed_after,
+                           max_admit=max_admit)
         s = summarize(loop.run(trace))
         s.update(path="served", offered_qps=r, offered=len(trace), ticks=loop.ticks, seconds=seconds,
-                 max_inflight=loop.capacity, defer_from=defer_from, deferred_ticks=sum(loop.deferred))
+                 max_inflight=loop.capacity, defer_from=defer_from, deferred_ticks=sum(loop.deferred),
+                 shed=len(loop.shed), shed_after_s=shed_after, max_admit=loop.max_admit,
+                 goodput_qps=s["completed"] / seconds if s.get("completed") else 0.0)
         print(json.dumps(s), flush=True)
     wl.close()
 
@@ -528,6 +535,9 @@ def main():
                          "during the next tick (-1: never)")
     ap.add_argument("--serve-sweep", default="", help="config 5 driver: comma-separated offered rates (queries/s)")
     ap.add_argument("--mixed", action="store_true", help="--serve-sweep: mixed query levels 6-12 and nprobe")
+    ap.add_argument("--shed-after", type=float, default=0.0,
+                    help="--serve-sweep: refuse requests not admitted within this many seconds (0: never)")
+    ap.add_argument("--serve-admit", type=int, default=0, help="--serve-sweep: queries admitted per tick")
     ap.add_argument("--ntt-config", action="store_true", help="config 2 driver (64 ct x 2 x 24 limbs, N=2^16)")
     ap.add_argument("--ks-config", action="store_true", help="config 3 driver (32 ct, N=2^16, dnum 3)")
     ap.add_argument("--ref-shape", action="store_true",
@@ -543,7 +553,8 @@ def main():
     if args.serve_sweep:
         return serve_sweep([float(x) for x in args.serve_sweep.split(",")], args.serve_seconds,
                            args.batch or default_batch(spec_of(args.workload)), args.workload, args.mixed,
-                           args.plain_queries, None if args.defer_from < 0 else args.defer_from)
+                           args.plain_queries, None if args.defer_from < 0 else args.defer_from,
+                           args.shed_after or None, args.serve_admit or None)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if args.impl == "reference":

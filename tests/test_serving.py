@@ -196,3 +196,25 @@ def test_small_ticks_take_results_at_once(defer_from):
     for i, deferred in zip(reqs, loop.deferred):
         if not deferred:
             assert kinds[i + 1].startswith("receive")
+
+
+def test_shedding_bounds_the_queue_under_overload():
+    """Requests waiting longer than shed_after are refused, the rest complete
+    once; without shedding every request completes."""
+    import time as _t
+
+    class SlowBackend(FakeBackend):
+        def coarse(self, recs):
+            _t.sleep(0.004)
+            super().coarse(recs)
+
+    arr = np.arange(120) * 0.0005            # 2,000 requests/s for 60 ms
+    be = SlowBackend(records=4, lanes=2)
+    loop = ServingLoop(be, shed_after=0.01)
+    done = loop.run(make_trace(arr, pool=3, seed=2), realtime=True)
+    ids = [c.qid for c in done] + [r.qid for r in loop.shed]
+    assert sorted(ids) == list(range(120)), "a request was lost or served twice"
+    assert loop.shed, "nothing shed at 2,000 requests/s on a server of about 250"
+    assert all(c.admitted - c.arrival <= 0.01 + 0.05 for c in done)     # the deadline plus about a tick
+    be2 = SlowBackend(records=4, lanes=2)
+    assert len(ServingLoop(be2).run(make_trace(arr[:20], pool=3, seed=2), realtime=True)) == 20
