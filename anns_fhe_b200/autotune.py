@@ -36,6 +36,7 @@ class KsChoice:
     fused: bool
     chunk: int
     us_per_ct: float
+    ept: int = 8          # values per thread of the one-kernel key switch (AFHE_OPT_KS_EPT)
 
 
 def gpu_name(device: int = 0) -> str:
@@ -73,7 +74,7 @@ TIE = 0.10   # candidates within this fraction of the fastest count as ties
 # Version of the key-switch kernels a cache was tuned against: a cache from
 # other kernels (e.g. before the one-kernel path existed at this ring degree)
 # is tuned again.
-KERNELS = 3
+KERNELS = 4
 
 
 def ntt_plan_count(log_n: int) -> int:
@@ -128,10 +129,11 @@ def time_ntt_plans(ctx: FheContext, polys: int, limbs: int, reps: int = 3) -> di
 
 
 def pick(timings: dict) -> tuple:
-    """The (fused, chunk) of {(fused, chunk): us_per_ct} to use: among the
+    """The key of {(fused, chunk[, ept]): us_per_ct} to use: among the
     candidates within TIE of the fastest, the largest chunk (fewest
     launches; a chain's batches are rarely a multiple of the tile, and every
-    extra launch costs its tail), then the one-kernel path."""
+    extra launch costs its tail), then the one-kernel path, then the
+    fastest."""
     best = min(timings.values())
     near = [k for k, v in timings.items() if v <= best * (1 + TIE)]
     return max(near, key=lambda k: (k[1], k[0], -timings[k]))
@@ -174,19 +176,22 @@ def tune(params: CkksParams, levels, lanes: int, device: int = 0, verbose: bool 
             ctx.write_poly(i * w_max, np.concatenate([rng.integers(0, q, n, dtype=np.uint64)
                                                       for q in params.q[:max(levels)]]))
         fused_ok = ctx.get_option(L.OPT_KS_FUSED) == 1    # the context enables it where the GPU can run it
-        cap = ctx.get_option(L.OPT_KS_CAPACITY) if fused_ok else 0
+        shapes = [(True, 8), (True, 16), (False, 8)] if fused_ok else [(False, 8)]
         out = {}
         for lv in sorted(set(levels)):
             timings = {}
-            for fused in ([True, False] if fused_ok else [False]):
+            for fused, ept in shapes:
                 ctx.set_option(L.OPT_KS_FUSED, int(fused))
-                for c in chunk_candidates(lanes, sm_count(device), cap if fused else 0):
+                ctx.set_option(L.OPT_KS_EPT, ept)
+                cap = ctx.get_option(L.OPT_KS_CAPACITY) if fused else 0
+                for c in chunk_candidates(lanes, sm_count(device), cap):
                     ctx.set_option(L.OPT_CHUNK, c)
-                    timings[(fused, c)] = time_rotations(ctx, lv, count)
+                    timings[(fused, c, ept)] = time_rotations(ctx, lv, count)
                     if verbose:
-                        print(f"level {lv} fused={fused} chunk={c}: {timings[(fused, c)]:.2f} us/ct")
-            f, c = pick(timings)
-            out[lv] = KsChoice(f, c, timings[(f, c)])
+                        print(f"level {lv} fused={fused} ept={ept} chunk={c}: {timings[(fused, c, ept)]:.2f} us/ct")
+            f, c, e = pick(timings)
+            out[lv] = KsChoice(f, c, timings[(f, c, e)], e)
+        ctx.set_option(L.OPT_KS_EPT, 8)
         return out
     finally:
         ctx.close()

@@ -564,6 +564,12 @@ int afhe_ctx_set_option(afhe_ctx* ctx, uint32_t option, int64_t value) {
         if (value < 1 || value > 4096) return fail(ctx, AFHE_E_ARG, "fused minimum must be in [1, 4096]");
         ctx->fused_min = (uint32_t)value;
         return AFHE_OK;
+    case AFHE_OPT_KS_EPT:
+        if (value != 8 && value != 16) return fail(ctx, AFHE_E_ARG, "values per thread must be 8 or 16");
+        ctx->ks_ept = (uint32_t)value;
+        return AFHE_OK;
+    case AFHE_OPT_KS_CAPACITY:
+        return fail(ctx, AFHE_E_ARG, "the key-switch capacity is read only");
     default:
         return fail(ctx, AFHE_E_ARG, "unknown option");
     }
@@ -575,9 +581,10 @@ int afhe_ctx_get_option(afhe_ctx* ctx, uint32_t option, int64_t* value) {
     case AFHE_OPT_KS_FUSED: *value = ctx->ks_fused ? 1 : 0; return AFHE_OK;
     case AFHE_OPT_CHUNK: *value = ctx->chunk ? ctx->chunk : ctx->lanes; return AFHE_OK;
     case AFHE_OPT_FUSED_MIN: *value = ctx->fused_min; return AFHE_OK;
+    case AFHE_OPT_KS_EPT: *value = ctx->ks_ept; return AFHE_OK;
     case AFHE_OPT_KS_CAPACITY:
         if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, AFHE_E_CUDA, "cudaSetDevice");
-        *value = key_switch_fused_capacity(ctx->log_n);
+        *value = key_switch_fused_capacity(ctx->log_n, (int)ctx->ks_ept);
         return AFHE_OK;
     default: return fail(ctx, AFHE_E_ARG, "unknown option");
     }

@@ -45,7 +45,11 @@ struct afhe_ivfpq {
     std::vector<std::vector<std::pair<u64, uint32_t>>> lists;   // list -> (plaintext, candidates) per batch
     std::vector<afhe_ct_ref> work;                      // diff, sq, sel per lane
     std::vector<afhe_ct_ref> cmp;                       // (n_list - 1) per lane: reference compaction terms
-    std::map<uint32_t, std::pair<int32_t, uint32_t>> tuning;   // level -> (one-kernel, chunk)
+    struct Tuning {
+        int32_t fused;
+        uint32_t chunk, ept;
+    };
+    std::map<uint32_t, Tuning> tuning;                 // level -> key-switch options
     bool fused_ok = false;                              // the one-kernel key switch was on at creation
 };
 
@@ -69,9 +73,10 @@ uint32_t eval_at(const afhe_ivfpq* h, uint32_t level) {
 void at(afhe_ivfpq* h, uint32_t limbs) {
     auto it = h->tuning.find(limbs);
     if (it == h->tuning.end()) return;
-    const int32_t fused = it->second.first;
-    if (fused == 0 || (fused > 0 && h->fused_ok)) afhe_ctx_set_option(h->ctx, AFHE_OPT_KS_FUSED, fused);
-    afhe_ctx_set_option(h->ctx, AFHE_OPT_CHUNK, std::min<uint32_t>(it->second.second, h->ctx->lanes));
+    const afhe_ivfpq::Tuning& o = it->second;
+    if (o.fused == 0 || (o.fused > 0 && h->fused_ok)) afhe_ctx_set_option(h->ctx, AFHE_OPT_KS_FUSED, o.fused);
+    afhe_ctx_set_option(h->ctx, AFHE_OPT_CHUNK, std::min<uint32_t>(o.chunk, h->ctx->lanes));
+    if (o.ept) afhe_ctx_set_option(h->ctx, AFHE_OPT_KS_EPT, o.ept);
 }
 
 #define RC(expr)                              \
@@ -395,9 +400,10 @@ int afhe_ivfpq_set_lanes(afhe_ivfpq* h, const afhe_ct_ref* work, uint32_t lanes,
     return AFHE_OK;
 }
 
-int afhe_ivfpq_set_tuning(afhe_ivfpq* h, uint32_t level, int32_t fused, uint32_t chunk) {
+int afhe_ivfpq_set_tuning(afhe_ivfpq* h, uint32_t level, int32_t fused, uint32_t chunk, uint32_t ept) {
     if (!h) return fail_h(h, AFHE_E_ARG, "null argument");
-    h->tuning[level] = {fused, chunk};
+    if (ept && ept != 8 && ept != 16) return fail_h(h, AFHE_E_ARG, "values per thread must be 8 or 16");
+    h->tuning[level] = {fused, chunk, ept};
     return AFHE_OK;
 }
 

@@ -70,12 +70,12 @@ constexpr int kLogQ = 13;    // log2 of the slice a CTA holds at N >= 2^13
 // One polynomial per CTA (LOGCL = 0) or per cluster of 2^LOGCL CTAs; each CTA
 // holds 2^LOGQ elements of every buffer. Local positions e < 2^LOGQ, global
 // positions x = rank * 2^LOGQ + e.
-template <int LOGQ, int LOGCL>
+template <int LOGQ, int LOGCL, int E = 8>
 struct Geo {
     static constexpr int LOGN = LOGQ + LOGCL;
     static constexpr uint32_t QN = 1u << LOGQ;
     static constexpr uint32_t CL = 1u << LOGCL;
-    static constexpr uint32_t THREADS = QN / 8;
+    static constexpr uint32_t THREADS = QN / E;
     __device__ __forceinline__ static uint32_t rank() {
         if constexpr (LOGCL == 0) return 0;
         else return cg::this_cluster().block_rank();
@@ -98,10 +98,10 @@ __device__ __forceinline__ void digit_range(const OpTabs& t, uint32_t j, uint32_
 // CL elements x = k QN + j (k < CL) form a column of CL values, transformed
 // by the stages of bits LOGN - 1 .. LOGQ (block b of stage s uses tw[2^s + b]).
 // CTA r takes the columns j in [r QN / CL, (r + 1) QN / CL).
-template <int LOGQ, int LOGCL, int NB>
+template <int LOGQ, int LOGCL, int NB, int E>
 __device__ __forceinline__ void cross_fwd(u64* const (&bufs)[NB], const ulonglong2* __restrict__ tw,
                                           const PrimeConst& pc) {
-    using G = Geo<LOGQ, LOGCL>;
+    using G = Geo<LOGQ, LOGCL, E>;
     constexpr uint32_t CL = G::CL, PER = G::QN / CL;
     cg::cluster_group cl = cg::this_cluster();
     const uint32_t r = cl.block_rank();
@@ -138,10 +138,10 @@ __device__ __forceinline__ void cross_fwd(u64* const (&bufs)[NB], const ulonglon
 
 // The top LOGCL stages of an inverse NTT (Gentleman-Sande, bits LOGQ ..
 // LOGN - 1), the last one with N^-1 folded in; outputs canonical.
-template <int LOGQ, int LOGCL, int NB>
+template <int LOGQ, int LOGCL, int NB, int E>
 __device__ __forceinline__ void cross_inv(u64* const (&bufs)[NB], const ulonglong2* __restrict__ itw,
                                           const PrimeConst& pc) {
-    using G = Geo<LOGQ, LOGCL>;
+    using G = Geo<LOGQ, LOGCL, E>;
     constexpr uint32_t CL = G::CL, PER = G::QN / CL;
     cg::cluster_group cl = cg::this_cluster();
     const uint32_t r = cl.block_rank();
@@ -186,61 +186,62 @@ __device__ __forceinline__ void cross_inv(u64* const (&bufs)[NB], const ulonglon
 // [0, 4q). Not inlined: each transform gets its own register allocation
 // instead of competing with the caller's live state (1024 threads leave 64
 // registers).
-template <int LOGQ, int LOGCL>
+template <int LOGQ, int LOGCL, int E>
 __device__ __noinline__ void fwd_ntt(u64* buf, const PrimeTables pt, uint32_t prime, const PrimeConst pc) {
-    using G = Geo<LOGQ, LOGCL>;
+    using G = Geo<LOGQ, LOGCL, E>;
     const ulonglong2* tw = pt.tw2 + ((u64)prime << G::LOGN);
     if constexpr (LOGCL > 0) {
         u64* const one[1] = {buf};
         G::sync_all();
-        cross_fwd<LOGQ, LOGCL, 1>(one, tw, pc);
+        cross_fwd<LOGQ, LOGCL, 1, E>(one, tw, pc);
         G::sync_all();
     }
-    ntt_rounds<false, LOGQ, 0, false, 0>(buf, tw, pc, G::rank(), G::LOGN, 0, true);
+    ntt_rounds<false, LOGQ, 0, false, 0, E>(buf, tw, pc, G::rank(), G::LOGN, 0, true);
 }
 
 // Inverse NTT of one buffer; on return the slice holds canonical residues.
-template <int LOGQ, int LOGCL>
+template <int LOGQ, int LOGCL, int E>
 __device__ __noinline__ void inv_ntt(u64* buf, const PrimeTables pt, uint32_t prime, const PrimeConst pc) {
-    using G = Geo<LOGQ, LOGCL>;
+    using G = Geo<LOGQ, LOGCL, E>;
     const ulonglong2* itw = pt.itw2 + ((u64)prime << G::LOGN);
-    ntt_rounds<true, LOGQ, 0, false, 0>(buf, itw, pc, G::rank(), G::LOGN, 0, LOGCL == 0);
+    ntt_rounds<true, LOGQ, 0, false, 0, E>(buf, itw, pc, G::rank(), G::LOGN, 0, LOGCL == 0);
     if constexpr (LOGCL > 0) {
         u64* const one[1] = {buf};
         G::sync_all();
-        cross_inv<LOGQ, LOGCL, 1>(one, itw, pc);
+        cross_inv<LOGQ, LOGCL, 1, E>(one, itw, pc);
         G::sync_all();
     }
 }
 
 // Two limbs of the same prime transformed together (shared twiddles).
-template <bool INV, int LOGQ, int LOGCL>
+template <bool INV, int LOGQ, int LOGCL, int E>
 __device__ __noinline__ void ntt2(u64* b0, u64* b1, const PrimeTables pt, uint32_t prime, const PrimeConst pc) {
-    using G = Geo<LOGQ, LOGCL>;
+    using G = Geo<LOGQ, LOGCL, E>;
     u64* const bufs[2] = {b0, b1};
     const ulonglong2* tw = (INV ? pt.itw2 : pt.tw2) + ((u64)prime << G::LOGN);
     if constexpr (!INV && LOGCL > 0) {
         G::sync_all();
-        cross_fwd<LOGQ, LOGCL, 2>(bufs, tw, pc);
+        cross_fwd<LOGQ, LOGCL, 2, E>(bufs, tw, pc);
         G::sync_all();
     }
-    ntt_rounds_n<INV, LOGQ, 0, false, 0, 8, 2>(bufs, tw, pc, G::rank(), G::LOGN, 0, !INV || LOGCL == 0);
+    ntt_rounds_n<INV, LOGQ, 0, false, 0, E, 2>(bufs, tw, pc, G::rank(), G::LOGN, 0, !INV || LOGCL == 0);
     if constexpr (INV && LOGCL > 0) {
         G::sync_all();
-        cross_inv<LOGQ, LOGCL, 2>(bufs, tw, pc);
+        cross_inv<LOGQ, LOGCL, 2, E>(bufs, tw, pc);
         G::sync_all();
     }
 }
 
-// Every element-wise pass below gives each thread the local positions
-// e_k = threadIdx.x + k * QN/8, k < 8 (global x_k = rank * QN + e_k), and
-// issues a chunk's global loads before its arithmetic, so several L2 round
-// trips are in flight per thread.
-constexpr uint32_t kPer = 8;     // positions per thread
+// Every element-wise pass below gives each of the QN / E threads the local
+// positions e_k = threadIdx.x + k * QN/E, k < E (global x_k = rank * QN +
+// e_k), and issues a chunk's global loads before its arithmetic, so several
+// L2 round trips are in flight per thread. E (values per thread: 8, or 16
+// with half the threads and twice the registers each) is the kernel's
+// template parameter, picked at run time (AFHE_OPT_KS_EPT).
 constexpr uint32_t kChunk = 4;   // positions whose loads are issued together
 
-template <int LOGQ>
-__device__ __forceinline__ uint32_t lpos(uint32_t k) { return threadIdx.x + k * ((1u << LOGQ) / 8); }
+template <int LOGQ, int E>
+__device__ __forceinline__ uint32_t lpos(uint32_t k) { return threadIdx.x + k * ((1u << LOGQ) / E); }
 
 // gathered position of x: the automorphism's source index, or x itself
 __device__ __forceinline__ uint32_t gpos(const uint32_t* map, uint32_t x) { return map ? __ldg(map + x) : x; }
@@ -269,11 +270,11 @@ __device__ __forceinline__ EntryKey entry_key(const KsFusedArgs& a, uint32_t z) 
 // Inner product for one slot (Q limb `s` < l, or special limb s - l) into
 // this CTA's slices of A0 / A1: A0 = sum_j d_j * evk_b[j], A1 = sum_j d_j *
 // evk_a[j] (mod the slot's prime).
-template <int LOGQ, int LOGCL, bool PREP>
+template <int LOGQ, int LOGCL, bool PREP, int E>
 __device__ void mac_slot(const KsFusedArgs& a, const OpTabs& t, uint32_t l, const EntryKey& ek, uint32_t s, u64* W,
                          u64* A0, u64* A1,
                          const u64* __restrict__ in, const u64* __restrict__ coef) {
-    using G = Geo<LOGQ, LOGCL>;
+    using G = Geo<LOGQ, LOGCL, E>;
     constexpr int LOGN = G::LOGN;
     constexpr uint32_t N = 1u << LOGN;
     const uint32_t x0 = G::rank() * G::QN;
@@ -297,45 +298,45 @@ __device__ void mac_slot(const KsFusedArgs& a, const OpTabs& t, uint32_t l, cons
             // W = BConv_j(coef) at this slot's prime, then NTT
             const uint32_t row = l - size + a.K;
             const uint32_t kpos = isq ? (s < start ? s : s - size) : (l - size) + (s - l);
-            u64 acc[kPer];
+            u64 acc[E];
 #pragma unroll
-            for (uint32_t k = 0; k < kPer; ++k) acc[k] = 0;
+            for (uint32_t k = 0; k < E; ++k) acc[k] = 0;
             for (uint32_t i = 0; i < size; ++i) {
                 const uint32_t limb = start + i;
                 const u64 w1 = __ldg(t.qhat_modp[j] + i * row + kpos), w1s = __ldg(t.qhat_modp_sh[j] + i * row + kpos);
                 const u64* src = coef + ((u64)limb << LOGN) + x0;     // [x * qHatInv]_{q_i} (phase 0)
-                u64 v[kPer];
+                u64 v[E];
 #pragma unroll
-                for (uint32_t k = 0; k < kPer; ++k) v[k] = src[lpos<LOGQ>(k)];
+                for (uint32_t k = 0; k < E; ++k) v[k] = src[lpos<LOGQ, E>(k)];
 #pragma unroll
-                for (uint32_t k = 0; k < kPer; ++k) {
+                for (uint32_t k = 0; k < E; ++k) {
                     acc[k] += mul_shoup_lazy(v[k], w1, w1s, q);
                     acc[k] = acc[k] >= p2 ? acc[k] - p2 : acc[k];
                 }
             }
 #pragma unroll
-            for (uint32_t k = 0; k < kPer; ++k) W[padix(lpos<LOGQ>(k))] = csub(acc[k], q);
+            for (uint32_t k = 0; k < E; ++k) W[padix(lpos<LOGQ, E>(k))] = csub(acc[k], q);
             __syncthreads();
-            fwd_ntt<LOGQ, LOGCL>(W, t.pt, prime, pc);
+            fwd_ntt<LOGQ, LOGCL, E>(W, t.pt, prime, pc);
         }
         const u64* src = in + ((u64)s << LOGN);
         if (PREP) {
             // Shoup products with the prepared key; the accumulators stay lazy
             // in [0, 2q) (both consumers accept that range)
 #pragma unroll
-            for (uint32_t c = 0; c < kPer; c += kChunk) {
+            for (uint32_t c = 0; c < E; c += kChunk) {
                 u64 d[kChunk];
                 ulonglong2 vb[kChunk], va[kChunk];
 #pragma unroll
                 for (uint32_t k = 0; k < kChunk; ++k) {
-                    const uint32_t x = x0 + lpos<LOGQ>(c + k);
+                    const uint32_t x = x0 + lpos<LOGQ, E>(c + k);
                     vb[k] = __ldg(pb2 + x);
                     va[k] = __ldg(pa2 + x);
-                    d[k] = own ? src[gpos(map, x)] : W[padix(lpos<LOGQ>(c + k))];   // any d < 2^64 is valid for Shoup
+                    d[k] = own ? src[gpos(map, x)] : W[padix(lpos<LOGQ, E>(c + k))];   // any d < 2^64 is valid for Shoup
                 }
 #pragma unroll
                 for (uint32_t k = 0; k < kChunk; ++k) {
-                    const uint32_t e = padix(lpos<LOGQ>(c + k));
+                    const uint32_t e = padix(lpos<LOGQ, E>(c + k));
                     u64 pb = mul_shoup_lazy(d[k], vb[k].x, vb[k].y, q);
                     u64 pa = mul_shoup_lazy(d[k], va[k].x, va[k].y, q);
                     if (j > 0) {
@@ -350,18 +351,18 @@ __device__ void mac_slot(const KsFusedArgs& a, const OpTabs& t, uint32_t l, cons
             }
         } else {
 #pragma unroll
-            for (uint32_t c = 0; c < kPer; c += kChunk) {
+            for (uint32_t c = 0; c < E; c += kChunk) {
                 u64 d[kChunk], vb[kChunk], va[kChunk];
 #pragma unroll
                 for (uint32_t k = 0; k < kChunk; ++k) {
-                    const uint32_t x = x0 + lpos<LOGQ>(c + k);
+                    const uint32_t x = x0 + lpos<LOGQ, E>(c + k);
                     vb[k] = __ldg(kb + x);
                     va[k] = __ldg(ka + x);
-                    d[k] = own ? src[gpos(map, x)] : canon4(W[padix(lpos<LOGQ>(c + k))], q);
+                    d[k] = own ? src[gpos(map, x)] : canon4(W[padix(lpos<LOGQ, E>(c + k))], q);
                 }
 #pragma unroll
                 for (uint32_t k = 0; k < kChunk; ++k) {
-                    const uint32_t e = padix(lpos<LOGQ>(c + k));
+                    const uint32_t e = padix(lpos<LOGQ, E>(c + k));
                     u64 pb = mul_mod(d[k], vb[k], mc);
                     u64 pa = mul_mod(d[k], va[k], mc);
                     if (j > 0) {
@@ -384,7 +385,7 @@ __device__ void mac_slot(const KsFusedArgs& a, const OpTabs& t, uint32_t l, cons
 //   (A0, A1) = INTT_P; BConv to q0 in place; (A0, A1) = NTT_q0;
 //   out_h = (in * key_h[q0] - A_h) * P^-1 (+ extras), the own digit's product
 //   computed in the same pass. Same residues as the general path.
-template <int LOGN, bool PREP>
+template <int LOGN, bool PREP, int E>
 __device__ __forceinline__ void ks_one_limb(const KsFusedArgs& a, const OpTabs& t, const EntryKey& ek, u64* W, u64* A0,
                                             u64* A1) {
     constexpr uint32_t N = 1u << LOGN;
@@ -396,43 +397,43 @@ __device__ __forceinline__ void ks_one_limb(const KsFusedArgs& a, const OpTabs& 
     const u64* key = a.key + ek.koff;
     // W = INTT_q0(input through the automorphism)
     {
-        uint32_t g[kPer];
-        u64 v[kPer];
+        uint32_t g[E];
+        u64 v[E];
 #pragma unroll
-        for (uint32_t k = 0; k < kPer; ++k) g[k] = gpos(map, lpos<LOGN>(k));
+        for (uint32_t k = 0; k < E; ++k) g[k] = gpos(map, lpos<LOGN, E>(k));
 #pragma unroll
-        for (uint32_t k = 0; k < kPer; ++k) v[k] = in[g[k]];
+        for (uint32_t k = 0; k < E; ++k) v[k] = in[g[k]];
 #pragma unroll
-        for (uint32_t k = 0; k < kPer; ++k) W[padix(lpos<LOGN>(k))] = v[k];
+        for (uint32_t k = 0; k < E; ++k) W[padix(lpos<LOGN, E>(k))] = v[k];
     }
     __syncthreads();
-    inv_ntt<LOGN, 0>(W, t.pt, 0, pq);
+    inv_ntt<LOGN, 0, E>(W, t.pt, 0, pq);
     // BConv q0 -> P in place (digit 0's only limb), then NTT_P
     {
         const u64 w0 = __ldg(t.qhat_inv[0]), w0s = __ldg(t.qhat_inv_sh[0]);
         const u64 w1 = __ldg(t.qhat_modp[0]), w1s = __ldg(t.qhat_modp_sh[0]);
 #pragma unroll
-        for (uint32_t k = 0; k < kPer; ++k) {
-            const uint32_t e = padix(lpos<LOGN>(k));
+        for (uint32_t k = 0; k < E; ++k) {
+            const uint32_t e = padix(lpos<LOGN, E>(k));
             W[e] = csub(mul_shoup_lazy(mul_shoup(W[e], w0, w0s, q), w1, w1s, p), p);
         }
     }
     __syncthreads();
-    fwd_ntt<LOGN, 0>(W, t.pt, t.p_base, pp);
+    fwd_ntt<LOGN, 0, E>(W, t.pt, t.p_base, pp);
     // inner product at P
     {
         const u64 kofs = (u64)a.key_pbase * N;
         const ModConst mc = modconst_of(pp);
 #pragma unroll 1
-        for (uint32_t c = 0; c < kPer; c += kChunk) {
+        for (uint32_t c = 0; c < E; c += kChunk) {
             u64 d[kChunk], rb[kChunk], ra[kChunk];
 #pragma unroll
-            for (uint32_t k = 0; k < kChunk; ++k) d[k] = W[padix(lpos<LOGN>(c + k))];
+            for (uint32_t k = 0; k < kChunk; ++k) d[k] = W[padix(lpos<LOGN, E>(c + k))];
             if (PREP) {
                 ulonglong2 vb[kChunk], va[kChunk];
 #pragma unroll
                 for (uint32_t k = 0; k < kChunk; ++k) {
-                    const uint32_t x = lpos<LOGN>(c + k);
+                    const uint32_t x = lpos<LOGN, E>(c + k);
                     vb[k] = __ldg(ek.prep + a.prep_b + kofs + x);
                     va[k] = __ldg(ek.prep + kofs + x);
                 }
@@ -445,7 +446,7 @@ __device__ __forceinline__ void ks_one_limb(const KsFusedArgs& a, const OpTabs& 
                 u64 vb[kChunk], va[kChunk];
 #pragma unroll
                 for (uint32_t k = 0; k < kChunk; ++k) {
-                    const uint32_t x = lpos<LOGN>(c + k);
+                    const uint32_t x = lpos<LOGN, E>(c + k);
                     vb[k] = __ldg(key + a.evk_b + kofs + x);
                     va[k] = __ldg(key + a.evk_a + kofs + x);
                 }
@@ -457,27 +458,27 @@ __device__ __forceinline__ void ks_one_limb(const KsFusedArgs& a, const OpTabs& 
             }
 #pragma unroll
             for (uint32_t k = 0; k < kChunk; ++k) {
-                const uint32_t e = padix(lpos<LOGN>(c + k));
+                const uint32_t e = padix(lpos<LOGN, E>(c + k));
                 A0[e] = rb[k];
                 A1[e] = ra[k];
             }
         }
     }
     __syncthreads();
-    ntt2<true, LOGN, 0>(A0, A1, t.pt, t.p_base, pp);
+    ntt2<true, LOGN, 0, E>(A0, A1, t.pt, t.p_base, pp);
     // BConv P -> q0 in place on both, then NTT_q0 of both
     {
         const u64 w0 = __ldg(t.phat_inv_modp), w0s = __ldg(t.phat_inv_modp_sh);
         const u64 w1 = __ldg(t.phat_modq), w1s = __ldg(t.phat_modq_sh);
 #pragma unroll
-        for (uint32_t k = 0; k < kPer; ++k) {
-            const uint32_t e = padix(lpos<LOGN>(k));
+        for (uint32_t k = 0; k < E; ++k) {
+            const uint32_t e = padix(lpos<LOGN, E>(k));
             A0[e] = csub(mul_shoup_lazy(mul_shoup(A0[e], w0, w0s, p), w1, w1s, q), q);
             A1[e] = csub(mul_shoup_lazy(mul_shoup(A1[e], w0, w0s, p), w1, w1s, q), q);
         }
     }
     __syncthreads();
-    ntt2<false, LOGN, 0>(A0, A1, t.pt, 0, pq);
+    ntt2<false, LOGN, 0, E>(A0, A1, t.pt, 0, pq);
     // out_h = (in * key_h[q0] - A_h) * P^-1, staged in A_h: the input and the
     // gathered c0 may alias the outputs
     {
@@ -485,11 +486,11 @@ __device__ __forceinline__ void ks_one_limb(const KsFusedArgs& a, const OpTabs& 
         const u64 pinv = __ldg(t.p_inv_mod_q), pinv_sh = __ldg(t.p_inv_mod_q_sh);
         const u64* cb = a.arena + (a.f.has_c0 ? a.f.c0.at(z) : 0);
 #pragma unroll 1
-        for (uint32_t c = 0; c < kPer; c += kChunk) {
+        for (uint32_t c = 0; c < E; c += kChunk) {
             u64 d[kChunk], cv[kChunk], rb[kChunk], ra[kChunk];
 #pragma unroll
             for (uint32_t k = 0; k < kChunk; ++k) {
-                const uint32_t g = gpos(map, lpos<LOGN>(c + k));
+                const uint32_t g = gpos(map, lpos<LOGN, E>(c + k));
                 d[k] = in[g];
                 cv[k] = a.f.has_c0 ? cb[g] : 0;
             }
@@ -497,7 +498,7 @@ __device__ __forceinline__ void ks_one_limb(const KsFusedArgs& a, const OpTabs& 
                 ulonglong2 vb[kChunk], va[kChunk];
 #pragma unroll
                 for (uint32_t k = 0; k < kChunk; ++k) {
-                    const uint32_t x = lpos<LOGN>(c + k);
+                    const uint32_t x = lpos<LOGN, E>(c + k);
                     vb[k] = __ldg(ek.prep + a.prep_b + x);
                     va[k] = __ldg(ek.prep + x);
                 }
@@ -510,7 +511,7 @@ __device__ __forceinline__ void ks_one_limb(const KsFusedArgs& a, const OpTabs& 
                 u64 vb[kChunk], va[kChunk];
 #pragma unroll
                 for (uint32_t k = 0; k < kChunk; ++k) {
-                    const uint32_t x = lpos<LOGN>(c + k);
+                    const uint32_t x = lpos<LOGN, E>(c + k);
                     vb[k] = __ldg(key + a.evk_b + x);
                     va[k] = __ldg(key + a.evk_a + x);
                 }
@@ -522,7 +523,7 @@ __device__ __forceinline__ void ks_one_limb(const KsFusedArgs& a, const OpTabs& 
             }
 #pragma unroll
             for (uint32_t k = 0; k < kChunk; ++k) {
-                const uint32_t e = padix(lpos<LOGN>(c + k));
+                const uint32_t e = padix(lpos<LOGN, E>(c + k));
                 u64 r0 = mul_shoup(sub_mod(rb[k], canon4(A0[e], q), q), pinv, pinv_sh, q);
                 const u64 r1 = mul_shoup(sub_mod(ra[k], canon4(A1[e], q), q), pinv, pinv_sh, q);
                 if (a.f.has_c0) r0 = add_mod(r0, cv[k], q);
@@ -538,17 +539,17 @@ __device__ __forceinline__ void ks_one_limb(const KsFusedArgs& a, const OpTabs& 
         const u64* x0 = a.arena + (a.f.has_acc ? a.f.acc0.at(z) : 0);
         const u64* x1 = a.arena + (a.f.has_acc ? a.f.acc1.at(z) : 0);
 #pragma unroll 1
-        for (uint32_t c = 0; c < kPer; c += kChunk) {
+        for (uint32_t c = 0; c < E; c += kChunk) {
             u64 e0[kChunk], e1[kChunk];
 #pragma unroll
             for (uint32_t k = 0; k < kChunk; ++k) {
-                const uint32_t x = lpos<LOGN>(c + k);
+                const uint32_t x = lpos<LOGN, E>(c + k);
                 e0[k] = a.f.has_acc ? x0[x] : 0;
                 e1[k] = a.f.has_acc ? x1[x] : 0;
             }
 #pragma unroll
             for (uint32_t k = 0; k < kChunk; ++k) {
-                const uint32_t x = lpos<LOGN>(c + k);
+                const uint32_t x = lpos<LOGN, E>(c + k);
                 u64 r0 = A0[padix(x)], r1 = A1[padix(x)];
                 if (a.f.has_acc) {
                     r0 = add_mod(r0, e0[k], q);
@@ -561,9 +562,9 @@ __device__ __forceinline__ void ks_one_limb(const KsFusedArgs& a, const OpTabs& 
     }
 }
 
-template <int LOGQ, int LOGCL, bool PREP>
-__global__ void __launch_bounds__((1u << LOGQ) / 8, 1) ks_fused_kernel(const KsFusedArgs a) {
-    using G = Geo<LOGQ, LOGCL>;
+template <int LOGQ, int LOGCL, bool PREP, int E>
+__global__ void __launch_bounds__((1u << LOGQ) / E, 1) ks_fused_kernel(const KsFusedArgs a) {
+    using G = Geo<LOGQ, LOGCL, E>;
     constexpr int LOGN = G::LOGN;
     constexpr uint32_t PADQ = G::QN + G::QN / 16;
     extern __shared__ u64 smem[];
@@ -579,7 +580,7 @@ __global__ void __launch_bounds__((1u << LOGQ) / 8, 1) ks_fused_kernel(const KsF
     const uint32_t* map = ek.map;
     if constexpr (LOGCL == 0) {
         if (l == 1 && K == 1) {
-            ks_one_limb<LOGN, PREP>(a, t, ek, W, A0, A1);
+            ks_one_limb<LOGN, PREP, E>(a, t, ek, W, A0, A1);
             return;
         }
     }
@@ -592,41 +593,41 @@ __global__ void __launch_bounds__((1u << LOGQ) / 8, 1) ks_fused_kernel(const KsF
         const PrimeConst pc = t.pt.pc[i];
         const u64* src = in + ((u64)i << LOGN);
         {
-            uint32_t g[kPer];
-            u64 v[kPer];
+            uint32_t g[E];
+            u64 v[E];
 #pragma unroll
-            for (uint32_t k = 0; k < kPer; ++k) g[k] = gpos(map, x0 + lpos<LOGQ>(k));
+            for (uint32_t k = 0; k < E; ++k) g[k] = gpos(map, x0 + lpos<LOGQ, E>(k));
 #pragma unroll
-            for (uint32_t k = 0; k < kPer; ++k) v[k] = src[g[k]];
+            for (uint32_t k = 0; k < E; ++k) v[k] = src[g[k]];
 #pragma unroll
-            for (uint32_t k = 0; k < kPer; ++k) W[padix(lpos<LOGQ>(k))] = v[k];
+            for (uint32_t k = 0; k < E; ++k) W[padix(lpos<LOGQ, E>(k))] = v[k];
         }
         __syncthreads();
-        inv_ntt<LOGQ, LOGCL>(W, t.pt, i, pc);
+        inv_ntt<LOGQ, LOGCL, E>(W, t.pt, i, pc);
         // stored times qHatInv: the first factor of ModUp's base conversion,
         // once per limb instead of once per output slot
         {
             const uint32_t part = i / t.alpha, idx = i - part * t.alpha;
             const u64 w0 = __ldg(t.qhat_inv[part] + idx), w0s = __ldg(t.qhat_inv_sh[part] + idx);
 #pragma unroll
-            for (uint32_t k = 0; k < kPer; ++k)
-                coef[((u64)i << LOGN) + x0 + lpos<LOGQ>(k)] = mul_shoup(W[padix(lpos<LOGQ>(k))], w0, w0s, pc.q);
+            for (uint32_t k = 0; k < E; ++k)
+                coef[((u64)i << LOGN) + x0 + lpos<LOGQ, E>(k)] = mul_shoup(W[padix(lpos<LOGQ, E>(k))], w0, w0s, pc.q);
         }
         __syncthreads();
     }
     // phase 1: special slots -> INTT of both accumulators
     for (uint32_t k = 0; k < K; ++k) {
-        mac_slot<LOGQ, LOGCL, PREP>(a, t, l, ek, l + k, W, A0, A1, in, coef);
+        mac_slot<LOGQ, LOGCL, PREP, E>(a, t, l, ek, l + k, W, A0, A1, in, coef);
         const uint32_t prime = t.p_base + k;
         const PrimeConst pc = t.pt.pc[prime];
-        ntt2<true, LOGQ, LOGCL>(A0, A1, t.pt, prime, pc);
+        ntt2<true, LOGQ, LOGCL, E>(A0, A1, t.pt, prime, pc);
         u64* d0 = pcoef + ((u64)(2 * k) << LOGN) + x0;
         u64* d1 = pcoef + ((u64)(2 * k + 1) << LOGN) + x0;
         // stored times PHatInv_k: the first factor of ModDown's base conversion
         const u64 w0 = __ldg(t.phat_inv_modp + k), w0s = __ldg(t.phat_inv_modp_sh + k);
 #pragma unroll
-        for (uint32_t e = 0; e < kPer; ++e) {
-            const uint32_t x = lpos<LOGQ>(e);
+        for (uint32_t e = 0; e < E; ++e) {
+            const uint32_t x = lpos<LOGQ, E>(e);
             d0[x] = mul_shoup(A0[padix(x)], w0, w0s, pc.q);
             d1[x] = mul_shoup(A1[padix(x)], w0, w0s, pc.q);
         }
@@ -637,7 +638,7 @@ __global__ void __launch_bounds__((1u << LOGQ) / 8, 1) ks_fused_kernel(const KsF
     const u64 c0 = a.f.has_c0 ? a.f.c0.at(z) : 0;
     const u64 ac0 = a.f.has_acc ? a.f.acc0.at(z) : 0, ac1 = a.f.has_acc ? a.f.acc1.at(z) : 0;
     for (uint32_t i = 0; i < l; ++i) {
-        mac_slot<LOGQ, LOGCL, PREP>(a, t, l, ek, i, W, A0, A1, in, coef);
+        mac_slot<LOGQ, LOGCL, PREP, E>(a, t, l, ek, i, W, A0, A1, in, coef);
         const PrimeConst pc = t.pt.pc[i];
         const u64 q = pc.q, q2 = q << 1;
         const u64 pinv = __ldg(t.p_inv_mod_q + i), pinv_sh = __ldg(t.p_inv_mod_q_sh + i);
@@ -645,26 +646,26 @@ __global__ void __launch_bounds__((1u << LOGQ) / 8, 1) ks_fused_kernel(const KsF
             u64* A = h ? A1 : A0;
             // W = BConv of the special limbs to q_i (approx_mod_down's fast_bases_conv), then NTT
             {
-                u64 acc[kPer];
+                u64 acc[E];
 #pragma unroll
-                for (uint32_t e = 0; e < kPer; ++e) acc[e] = 0;
+                for (uint32_t e = 0; e < E; ++e) acc[e] = 0;
                 for (uint32_t k = 0; k < K; ++k) {
                     const u64 w1 = __ldg(t.phat_modq + k * l + i), w1s = __ldg(t.phat_modq_sh + k * l + i);
                     const u64* src = pcoef + ((u64)(2 * k + h) << LOGN) + x0;   // [x * PHatInv]_{p_k} (phase 1)
-                    u64 v[kPer];
+                    u64 v[E];
 #pragma unroll
-                    for (uint32_t e = 0; e < kPer; ++e) v[e] = src[lpos<LOGQ>(e)];
+                    for (uint32_t e = 0; e < E; ++e) v[e] = src[lpos<LOGQ, E>(e)];
 #pragma unroll
-                    for (uint32_t e = 0; e < kPer; ++e) {
+                    for (uint32_t e = 0; e < E; ++e) {
                         acc[e] += mul_shoup_lazy(v[e], w1, w1s, q);
                         acc[e] = acc[e] >= q2 ? acc[e] - q2 : acc[e];
                     }
                 }
 #pragma unroll
-                for (uint32_t e = 0; e < kPer; ++e) W[padix(lpos<LOGQ>(e))] = csub(acc[e], q);
+                for (uint32_t e = 0; e < E; ++e) W[padix(lpos<LOGQ, E>(e))] = csub(acc[e], q);
             }
             __syncthreads();
-            fwd_ntt<LOGQ, LOGCL>(W, t.pt, i, pc);
+            fwd_ntt<LOGQ, LOGCL, E>(W, t.pt, i, pc);
             // (x_Q - y) * P^-1 plus the fused extras. The gathered c0 limb i
             // is staged in A and stored after a barrier over every CTA of the
             // polynomial (c0 may alias out0, and the gather reads any slice);
@@ -675,16 +676,16 @@ __global__ void __launch_bounds__((1u << LOGQ) / 8, 1) ks_fused_kernel(const KsF
             const u64 ab = (h ? ac1 : ac0) + ((u64)i << LOGN) + x0;
             const u64* cb = a.arena + c0 + ((u64)i << LOGN);
 #pragma unroll
-            for (uint32_t c = 0; c < kPer; c += kChunk) {
+            for (uint32_t c = 0; c < E; c += kChunk) {
                 u64 ex[kChunk];
 #pragma unroll
                 for (uint32_t e = 0; e < kChunk; ++e) {
-                    const uint32_t x = lpos<LOGQ>(c + e);
+                    const uint32_t x = lpos<LOGQ, E>(c + e);
                     ex[e] = stage ? cb[gpos(map, x0 + x)] : (a.f.has_acc ? a.arena[ab + x] : 0);
                 }
 #pragma unroll
                 for (uint32_t e = 0; e < kChunk; ++e) {
-                    const uint32_t x = lpos<LOGQ>(c + e);
+                    const uint32_t x = lpos<LOGQ, E>(c + e);
                     // A may be lazy in [0, 2q): the difference is then in
                     // [0, 2q) and mul_shoup returns it canonical
                     u64 r = mul_shoup(sub_mod(A[padix(x)], canon4(W[padix(x)], q), q), pinv, pinv_sh, q);
@@ -696,13 +697,13 @@ __global__ void __launch_bounds__((1u << LOGQ) / 8, 1) ks_fused_kernel(const KsF
             if (stage) {
                 G::sync_all();
 #pragma unroll
-                for (uint32_t c = 0; c < kPer; c += kChunk) {
+                for (uint32_t c = 0; c < E; c += kChunk) {
                     u64 ex[kChunk];
 #pragma unroll
-                    for (uint32_t e = 0; e < kChunk; ++e) ex[e] = a.f.has_acc ? a.arena[ab + lpos<LOGQ>(c + e)] : 0;
+                    for (uint32_t e = 0; e < kChunk; ++e) ex[e] = a.f.has_acc ? a.arena[ab + lpos<LOGQ, E>(c + e)] : 0;
 #pragma unroll
                     for (uint32_t e = 0; e < kChunk; ++e) {
-                        const uint32_t x = lpos<LOGQ>(c + e);
+                        const uint32_t x = lpos<LOGQ, E>(c + e);
                         u64 r = A[padix(x)];
                         if (a.f.has_acc) r = add_mod(r, ex[e], q);
                         a.arena[ob + x] = r;
@@ -714,19 +715,19 @@ __global__ void __launch_bounds__((1u << LOGQ) / 8, 1) ks_fused_kernel(const KsF
     }
 }
 
-template <int LOGQ, int LOGCL, bool PREP>
+template <int LOGQ, int LOGCL, bool PREP, int E>
 cudaError_t launch_fused_v(const KsFusedArgs& a, uint32_t nz, cudaStream_t st) {
     constexpr uint32_t QN = 1u << LOGQ;
     const size_t smem = 3ull * (QN + QN / 16) * sizeof(u64);
-    auto kern = ks_fused_kernel<LOGQ, LOGCL, PREP>;
+    auto kern = ks_fused_kernel<LOGQ, LOGCL, PREP, E>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     if constexpr (LOGCL == 0) {
-        kern<<<nz, QN / 8, smem, st>>>(a);
+        kern<<<nz, QN / E, smem, st>>>(a);
     } else {
         cudaLaunchConfig_t cfg = {};
         cfg.gridDim = dim3(nz << LOGCL, 1, 1);
-        cfg.blockDim = dim3(QN / 8, 1, 1);
+        cfg.blockDim = dim3(QN / E, 1, 1);
         cfg.dynamicSmemBytes = smem;
         cfg.stream = st;
         cudaLaunchAttribute attr[1];
@@ -744,24 +745,26 @@ cudaError_t launch_fused_v(const KsFusedArgs& a, uint32_t nz, cudaStream_t st) {
 }
 
 template <int LOGQ, int LOGCL>
-cudaError_t launch_fused(const KsFusedArgs& a, uint32_t nz, cudaStream_t st) {
-    return a.prep ? launch_fused_v<LOGQ, LOGCL, true>(a, nz, st) : launch_fused_v<LOGQ, LOGCL, false>(a, nz, st);
+cudaError_t launch_fused(const KsFusedArgs& a, uint32_t nz, cudaStream_t st, int ept) {
+    if (ept == 16)
+        return a.prep ? launch_fused_v<LOGQ, LOGCL, true, 16>(a, nz, st) : launch_fused_v<LOGQ, LOGCL, false, 16>(a, nz, st);
+    return a.prep ? launch_fused_v<LOGQ, LOGCL, true, 8>(a, nz, st) : launch_fused_v<LOGQ, LOGCL, false, 8>(a, nz, st);
 }
 
 // Clusters the GPU can hold at once for the kernel at N = 2^(13 + logcl)
 // (0 when it cannot place even one: the multi-kernel path is used then).
-template <int LOGCL>
+template <int LOGCL, int E = 8>
 int cluster_capacity() {
     constexpr uint32_t QN = 1u << kLogQ;
     const size_t smem = 3ull * (QN + QN / 16) * sizeof(u64);
-    auto kern = ks_fused_kernel<kLogQ, LOGCL, true>;
+    auto kern = ks_fused_kernel<kLogQ, LOGCL, true, E>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
         cudaGetLastError();
         return 0;
     }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(1u << LOGCL, 1, 1);
-    cfg.blockDim = dim3(QN / 8, 1, 1);
+    cfg.blockDim = dim3(QN / E, 1, 1);
     cfg.dynamicSmemBytes = smem;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
@@ -796,9 +799,13 @@ __global__ void key_prep_kernel(const u64* __restrict__ key, ulonglong2* __restr
 
 }  // namespace
 
-int key_switch_fused_capacity(int log_n) {
-    if (log_n >= 14 && log_n <= 16)
+int key_switch_fused_capacity(int log_n, int ept) {
+    if (log_n >= 14 && log_n <= 16) {
+        if (ept == 16)
+            return log_n == 14 ? cluster_capacity<1, 16>() : log_n == 15 ? cluster_capacity<2, 16>()
+                                                                          : cluster_capacity<3, 16>();
         return log_n == 14 ? cluster_capacity<1>() : log_n == 15 ? cluster_capacity<2>() : cluster_capacity<3>();
+    }
     if (log_n < 10 || log_n > 13) return 0;
     int dev = 0, sms = 0, per = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
@@ -809,11 +816,20 @@ int key_switch_fused_capacity(int log_n) {
     const uint32_t qn = 1u << log_n;
     const size_t smem = 3ull * (qn + qn / 16) * sizeof(u64);
     cudaError_t e = cudaSuccess;
-    switch (log_n) {
-    case 10: e = occupancy_of(ks_fused_kernel<10, 0, true>, qn / 8, smem, &per); break;
-    case 11: e = occupancy_of(ks_fused_kernel<11, 0, true>, qn / 8, smem, &per); break;
-    case 12: e = occupancy_of(ks_fused_kernel<12, 0, true>, qn / 8, smem, &per); break;
-    default: e = occupancy_of(ks_fused_kernel<13, 0, true>, qn / 8, smem, &per); break;
+    if (ept == 16) {
+        switch (log_n) {
+        case 10: e = occupancy_of(ks_fused_kernel<10, 0, true, 16>, qn / 16, smem, &per); break;
+        case 11: e = occupancy_of(ks_fused_kernel<11, 0, true, 16>, qn / 16, smem, &per); break;
+        case 12: e = occupancy_of(ks_fused_kernel<12, 0, true, 16>, qn / 16, smem, &per); break;
+        default: e = occupancy_of(ks_fused_kernel<13, 0, true, 16>, qn / 16, smem, &per); break;
+        }
+    } else {
+        switch (log_n) {
+        case 10: e = occupancy_of(ks_fused_kernel<10, 0, true, 8>, qn / 8, smem, &per); break;
+        case 11: e = occupancy_of(ks_fused_kernel<11, 0, true, 8>, qn / 8, smem, &per); break;
+        case 12: e = occupancy_of(ks_fused_kernel<12, 0, true, 8>, qn / 8, smem, &per); break;
+        default: e = occupancy_of(ks_fused_kernel<13, 0, true, 8>, qn / 8, smem, &per); break;
+        }
     }
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -847,7 +863,7 @@ cudaError_t launch_key_prep(const u64* key, ulonglong2* prep, const PrimeConst* 
 cudaError_t launch_key_switch_fused(int log_n, const OpTabs& t, uint32_t sizeQl, uint32_t K, const u64* key, u64 evk_a,
                                     u64 evk_b, uint32_t key_stride, uint32_t key_pbase, u64* arena, u64* scratch,
                                     uint32_t nz, const ZBases& zb, cudaStream_t st, const KsFuse* fuse,
-                                    const ulonglong2* prep, const OpTabs* lvtabs, const ZField* lvz) {
+                                    const ulonglong2* prep, const OpTabs* lvtabs, const ZField* lvz, int ept) {
     if (nz == 0) return cudaSuccess;
     KsFusedArgs a{};
     a.t = t;
@@ -872,13 +888,13 @@ cudaError_t launch_key_switch_fused(int log_n, const OpTabs& t, uint32_t sizeQl,
         a.lvz = *lvz;
     }
     switch (log_n) {
-    case 10: return launch_fused<10, 0>(a, nz, st);
-    case 11: return launch_fused<11, 0>(a, nz, st);
-    case 12: return launch_fused<12, 0>(a, nz, st);
-    case 13: return launch_fused<13, 0>(a, nz, st);
-    case 14: return launch_fused<kLogQ, 1>(a, nz, st);
-    case 15: return launch_fused<kLogQ, 2>(a, nz, st);
-    case 16: return launch_fused<kLogQ, 3>(a, nz, st);
+    case 10: return launch_fused<10, 0>(a, nz, st, ept);
+    case 11: return launch_fused<11, 0>(a, nz, st, ept);
+    case 12: return launch_fused<12, 0>(a, nz, st, ept);
+    case 13: return launch_fused<13, 0>(a, nz, st, ept);
+    case 14: return launch_fused<kLogQ, 1>(a, nz, st, ept);
+    case 15: return launch_fused<kLogQ, 2>(a, nz, st, ept);
+    case 16: return launch_fused<kLogQ, 3>(a, nz, st, ept);
     default: return cudaErrorInvalidValue;
     }
 }

@@ -193,6 +193,10 @@ int afhe_copy_poly(afhe_ctx* ctx, uint64_t dst_offset, uint64_t src_offset, uint
  *                      N = 2^13, resident together): a launch of a multiple
  *                      of it fills its waves; 0 where it cannot run. */
 #define AFHE_OPT_KS_CAPACITY 4u
+/*   AFHE_OPT_KS_EPT    values per thread of the one-kernel key switch: 8
+ *                      (N / 8 threads per CTA slice, the default) or 16 (half
+ *                      the threads, twice the registers each). Same residues. */
+#define AFHE_OPT_KS_EPT 5u
 int afhe_ctx_set_option(afhe_ctx* ctx, uint32_t option, int64_t value);
 int afhe_ctx_get_option(afhe_ctx* ctx, uint32_t option, int64_t* value);
 /* Page-locked host memory for the transfers above (the reference's host
@@ -419,8 +423,9 @@ int afhe_ivfpq_set_list(afhe_ivfpq* h, uint32_t list, const uint64_t* pts, const
  * cmp[j (n_list - 1) + i - 1] = lane j's stage-1b term i (reference compaction). */
 int afhe_ivfpq_set_lanes(afhe_ivfpq* h, const afhe_ct_ref* work, uint32_t lanes, const afhe_ct_ref* cmp);
 /* Key-switch options for operators at `level` limbs: fused (-1 leave, 0 off,
- * 1 on) and chunk, as afhe_ctx_set_option's AFHE_OPT_KS_FUSED / AFHE_OPT_CHUNK. */
-int afhe_ivfpq_set_tuning(afhe_ivfpq* h, uint32_t level, int32_t fused, uint32_t chunk);
+ * 1 on), chunk and values per thread (0: leave), as afhe_ctx_set_option's
+ * AFHE_OPT_KS_FUSED / AFHE_OPT_CHUNK / AFHE_OPT_KS_EPT. */
+int afhe_ivfpq_set_tuning(afhe_ivfpq* h, uint32_t level, int32_t fused, uint32_t chunk, uint32_t ept);
 int afhe_ivfpq_stage1(afhe_ivfpq* h, const afhe_ivfpq_query* queries, uint32_t count);
 int afhe_ivfpq_stage3(afhe_ivfpq* h, const afhe_ivfpq_query* queries, uint32_t count);
 

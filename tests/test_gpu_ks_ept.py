@@ -1,0 +1,50 @@
+"""The one-kernel key switch gives the same residues at 8 and at 16 values
+per thread (AFHE_OPT_KS_EPT), at every ring degree it runs at: one CTA per
+ciphertext (N = 2^10, 2^13) and clusters of 2, 4 and 8 CTAs (N = 2^14, 2^15,
+2^16). The workload is a rotate-and-sum chain over ciphertexts at mixed
+levels in one launch per step (afhe_eval_rotate_accumulate_levels_batch),
+then a rescale; the 8-value kernel is checked against the oracle by
+test_gpu_ks_paths.py and test_gpu_primitives_n65536.py."""
+import numpy as np
+import pytest
+
+from anns_fhe_b200 import _lib as L
+from anns_fhe_b200.primitives import KeySwitchBatch
+
+pytestmark = pytest.mark.gpu
+
+# log_n, num_q, num_p, alpha, level range, ciphertexts
+SHAPES = {
+    "n1024": (10, 4, 2, 1, (1, 4), 6),
+    "n8192": (13, 3, 1, 1, (1, 3), 6),
+    "n16384_cl2": (14, 6, 2, 3, (2, 6), 5),
+    "n32768_cl4": (15, 12, 4, 4, (3, 12), 4),
+    "n65536_cl8": (16, 8, 4, 4, (3, 8), 3),
+}
+
+
+@pytest.mark.parametrize("shape", list(SHAPES))
+def test_values_per_thread_same_residues(shape):
+    log_n, nq, np_, alpha, lv, cts = SHAPES[shape]
+    ksb = KeySwitchBatch(cts=cts, log_n=log_n, num_q=nq, num_p=np_, alpha=alpha, level_range=lv, steps=[1, 2, 8],
+                         lanes=cts)
+    try:
+        if ksb.ctx.get_option(L.OPT_KS_FUSED) != 1:
+            pytest.skip("the one-kernel key switch does not run on this GPU at this ring degree")
+        ksb.ctx.set_option(L.OPT_FUSED_MIN, 1)
+        out = {}
+        for ept in (8, 16):
+            ksb.ctx.set_option(L.OPT_KS_EPT, ept)
+            assert ksb.ctx.get_option(L.OPT_KS_EPT) == ept
+            assert ksb.ctx.get_option(L.OPT_KS_CAPACITY) > 0
+            ksb.reset()
+            ksb.run()
+            ksb.ctx.sync()
+            out[ept] = [x for z in range(cts) for o in (False, True) for x in ksb.read_ct(z, o)]
+        for i, (a, b) in enumerate(zip(out[8], out[16])):
+            assert np.array_equal(a, b), f"{shape}: polynomial {i} differs between 8 and 16 values per thread"
+        assert any(np.any(a) for a in out[8])
+        with pytest.raises(L.AfheError):
+            ksb.ctx.set_option(L.OPT_KS_EPT, 12)
+    finally:
+        ksb.close()

@@ -69,7 +69,8 @@ class FakeLib:
     def _head(self, name, limbs, ks):
         s = f"{name} {limbs}"
         if ks:
-            s += f" fused={self.ctx.opts[L.OPT_KS_FUSED]} chunk={self.ctx.opts[L.OPT_CHUNK]}"
+            s += (f" fused={self.ctx.opts[L.OPT_KS_FUSED]} chunk={self.ctx.opts[L.OPT_CHUNK]}"
+                  f" ept={self.ctx.opts[L.OPT_KS_EPT]}")
         return s + " |"
 
     def afhe_eval_add_batch(self, h, a, b, d, n, limbs):
@@ -111,7 +112,7 @@ class FakeCtx:
     def __init__(self, lanes):
         self.h = None
         self.max_batch = lanes
-        self.opts = {L.OPT_KS_FUSED: 1, L.OPT_CHUNK: 0}
+        self.opts = {L.OPT_KS_FUSED: 1, L.OPT_CHUNK: 0, L.OPT_KS_EPT: 8}
 
     def set_option(self, option, value):
         self.opts[option] = value
@@ -121,8 +122,8 @@ class FakeCtx:
 
 
 class Choice:
-    def __init__(self, fused, chunk):
-        self.fused, self.chunk = fused, chunk
+    def __init__(self, fused, chunk, ept=8):
+        self.fused, self.chunk, self.ept = fused, chunk, ept
 
 
 def build_manager(rng, *, D, n_list, slots, L_top, lanes, compaction, eval_level, levels, tuning, ctx_lanes):
@@ -194,8 +195,8 @@ def run_native(trace, m, recs, L_top, n, ctx_lanes, stage):
 
 CASES = {
     "reference_mixed_levels": dict(D=8, n_list=4, slots=64, L_top=6, lanes=3, compaction="reference",
-                                   eval_level=None, levels=[6, 5, 4], tuning={6: (1, 2), 5: (0, 3), 4: (1, 1),
-                                                                             3: (0, 2), 2: (1, 3)}),
+                                   eval_level=None, levels=[6, 5, 4], tuning={6: (1, 2, 16), 5: (0, 3), 4: (1, 1),
+                                                                             3: (0, 2), 2: (1, 3, 16)}),
     "reference_one_lane": dict(D=8, n_list=5, slots=64, L_top=5, lanes=1, compaction="reference", eval_level=None,
                                levels=[5], tuning={}),
     "packed_eval_level": dict(D=8, n_list=20, slots=64, L_top=7, lanes=4, compaction="packed", eval_level=4,
@@ -219,7 +220,7 @@ def test_native_driver_issues_the_python_drivers_operators(trace, case, stage):
         m.stage3_fine(recs)
     want = py.log
     assert want, "the Python driver issued nothing"
-    m.ctx.opts = {L.OPT_KS_FUSED: 1, L.OPT_CHUNK: 0}
+    m.ctx.opts = {L.OPT_KS_FUSED: 1, L.OPT_CHUNK: 0, L.OPT_KS_EPT: 8}
     got = run_native(trace, m, recs, kw["L_top"], 2 * kw["slots"], ctx_lanes, stage)
     for i, (a, b) in enumerate(zip(got, want)):
         assert a == b, f"call {i} differs:\n native {a[:300]}\n python {b[:300]}"
