@@ -43,11 +43,13 @@ def load_peaks():
         return 6650.0, "fallback"
 
 
-def ks_roofline(params, lanes: int, reps: int = 20, level: int = 0, nbuf: int = 5):
+def ks_roofline(params, lanes: int, reps: int = 20, level: int = 0, nbuf: int = 5, choice=None):
     """One rotation step (a key switch with the automorphism folded into its
     loads) of `lanes` ciphertexts at `level` limbs per call, `nbuf` input
     batches cycled so the inputs stream from HBM; `reps` calls timed with
-    CUDA events on the context stream after `nbuf` warm-up calls."""
+    CUDA events on the context stream after `nbuf` warm-up calls. `choice`:
+    the autotuner's key-switch options for this level (KsChoice), else the
+    context's defaults."""
     import numpy as np
     import torch
 
@@ -66,6 +68,12 @@ def ks_roofline(params, lanes: int, reps: int = 20, level: int = 0, nbuf: int = 
         ctx.write_key(0, np.concatenate([rng.integers(0, q, n, dtype=np.uint64) for _ in range(2 * p.dnum)
                                          for q in allp]))
         ctx.lib.afhe_add_rotation_key(ctx.h, 1, 0)
+        if choice is not None:
+            if not choice.fused or ctx.get_option(1) == 1:
+                ctx.set_option(1, int(choice.fused))
+            ctx.set_option(2, min(int(choice.chunk), lanes))
+            ctx.set_option(5, int(getattr(choice, "ept", 8)))
+        ept = ctx.get_option(5)
         limb = np.concatenate([rng.integers(0, q, n, dtype=np.uint64) for q in p.q[:L]])
         for i in range((nbuf + 1) * lanes * 2):
             ctx.write_poly(i * w, limb)
@@ -99,12 +107,12 @@ def ks_roofline(params, lanes: int, reps: int = 20, level: int = 0, nbuf: int = 
     peak, src = load_peaks()
     cap = KS_CAPTURES.get((n, L, K))
     traffic = int_pipe = None
-    if cap and launches == 1 and fused:
+    if cap and launches == 1 and fused and ept == cap.get("ept", 8):
         # the capture's per-ciphertext traffic scaled to this launch, the key once
         traffic = (cap["dram_bytes"] - key_bytes) * lanes / cap["ciphertexts"] + key_bytes
         int_pipe = {"pipe": cap["pipe"], "frac": cap["util"], "kernel": cap["kernel"],
                     "captured_ciphertexts": cap["ciphertexts"]}
-    kind = "one-kernel" if fused and launches == 1 else f"{launches:g}-launch"
+    kind = f"one-kernel, {ept} values per thread" if fused and launches == 1 else f"{launches:g}-launch"
     return {"bound": "hbm", "kernel": f"rotation key switch, {kind} (N={n}, {L} + {K} limbs, "
                                       f"{lanes} ciphertexts per call)",
             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -115,15 +123,17 @@ def ks_roofline(params, lanes: int, reps: int = 20, level: int = 0, nbuf: int = 
 # ---------------------------------------------------------------------------
 # profiling drivers
 # ---------------------------------------------------------------------------
-def profile_ks(lanes: int, workload: str = "small", level: int = 0):
+def profile_ks(lanes: int, workload: str = "small", level: int = 0, ept: int = 8):
     """The roofline measurement of the key switch alone (five warm-up calls,
     then 20 measured) at `level` limbs (default: the workload's evaluation
-    level)."""
+    level), the one-kernel key switch at `ept` values per thread."""
+    from .autotune import KsChoice
     from .driver import CkksParams
     from .workloads import LARGE, SMALL
     spec = LARGE if workload == "large" else SMALL
     p = CkksParams.generate(spec.log_n, spec.num_q, spec.q_bits, spec.num_p, spec.p_bits, spec.alpha)
-    print(json.dumps(ks_roofline(p, lanes, level=level or spec.eval_level or spec.num_q)))
+    print(json.dumps(ks_roofline(p, lanes, level=level or spec.eval_level or spec.num_q,
+                                 choice=KsChoice(True, lanes, 0.0, ept))))
 
 
 def profile_step(nq: int, workload: str = "small", lanes: int = 0):
@@ -315,6 +325,7 @@ def main() -> None:
     a.add_argument("lanes", type=int)
     a.add_argument("--workload", default="small", choices=["small", "large"])
     a.add_argument("--level", type=int, default=0)
+    a.add_argument("--ept", type=int, default=8, choices=[8, 16], help="values per thread (one-kernel path)")
     a = sub.add_parser("ntt", help="batched NTT / INTT: polynomials per launch")
     a.add_argument("polys", type=int)
     a.add_argument("--log-n", type=int, default=13)
@@ -327,7 +338,7 @@ def main() -> None:
     a.add_argument("--calls", type=int, default=200)
     args = ap.parse_args()
     if args.what == "ks":
-        profile_ks(args.lanes, args.workload, args.level)
+        profile_ks(args.lanes, args.workload, args.level, args.ept)
     elif args.what == "ntt":
         profile_ntt(args.polys, args.log_n)
     elif args.what == "step":

@@ -212,7 +212,8 @@ def measure(args, spec, rank: int, world: int, steps: int, warmup: int, batch: i
         wl.close()
     if legs:
         from anns_fhe_b200.profiling import ks_roofline
-        line["roofline"] = ks_roofline(wl.params, lanes, level=spec.eval_level or spec.num_q)
+        ev = spec.eval_level or spec.num_q
+        line["roofline"] = ks_roofline(wl.params, lanes, level=ev, choice=(wl.tuning or {}).get(ev))
     return line
 
 
