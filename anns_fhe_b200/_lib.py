@@ -70,6 +70,12 @@ class CtRef(C.Structure):
     _fields_ = [("c0_offset", u64), ("c1_offset", u64)]
 
 
+class PqIndex(C.Structure):
+    _fields_ = [("n_list", u32), ("d", u32), ("M", u32), ("K", u32), ("n", u64),
+                ("centroids", C.POINTER(C.c_float)), ("codebooks", C.POINTER(C.c_float)),
+                ("codes", C.POINTER(C.c_uint8)), ("assignments", C.POINTER(u32))]
+
+
 class IvfpqShape(C.Structure):
     _fields_ = [("D", u32), ("n_list", u32), ("slots", u32), ("lanes", u32), ("packed", u32), ("eval_level", u32)]
 
@@ -154,6 +160,10 @@ SIGNATURES = {
     "afhe_ntt_plan_describe": (C.c_int, [u32, u32, C.c_char_p, u32]),
     "afhe_ntt_set_plan": (C.c_int, [u32, u32]),
     "afhe_ntt_get_plan": (C.c_int, [u32, P32]),
+    "afhe_encode_batch": (C.c_int, [CTX, C.POINTER(C.c_double), u32, u32, C.c_double, u32, P64]),
+    "afhe_pq_create": (C.c_int, [CTX, C.POINTER(PqIndex), C.POINTER(C.c_void_p)]),
+    "afhe_pq_destroy": (C.c_int, [C.c_void_p]),
+    "afhe_pq_encode_batches": (C.c_int, [C.c_void_p, P32, P32, P32, u32, C.c_double, u32, P64]),
     "afhe_ivfpq_create": (C.c_int, [CTX, C.POINTER(IvfpqShape), C.POINTER(C.c_void_p)]),
     "afhe_ivfpq_destroy": (C.c_int, [C.c_void_p]),
     "afhe_ivfpq_set_centroids": (C.c_int, [C.c_void_p, P64, u32]),

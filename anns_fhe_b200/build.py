@@ -27,7 +27,7 @@ OBJDIR = os.path.join(os.path.dirname(HERE), "_build", "afhe")
 ROOT = os.path.dirname(HERE)
 INCLUDE = os.path.join(ROOT, "include")
 
-SOURCES = ["api.cu", "driver.cu", "ivfpq.cu", "kernels.cu", "ksfused.cu", "noalloc.cu", "tables.cpp"]
+SOURCES = ["api.cu", "driver.cu", "encode.cu", "ivfpq.cu", "kernels.cu", "ksfused.cu", "noalloc.cu", "tables.cpp"]
 HEADERS = ["internal.h", "lanes.h", "modarith.cuh", "ntt.cuh", "tables.h"]
 
 ARCH_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a"]

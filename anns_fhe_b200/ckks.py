@@ -22,6 +22,8 @@ automorphisms); the host samples randomness, encodes and decodes.
 """
 from __future__ import annotations
 
+import ctypes as C
+
 import numpy as np
 import scipy.fft as _sfft
 
@@ -407,11 +409,54 @@ class CkksDecryptor:
         self.ctx.close()
 
 
-def encode_plaintexts(ctx: FheContext, enc: Encoder, values: np.ndarray, scale: float, offs, level: int,
-                      chunk: int = 256) -> None:
-    """Server-side encoding of many plaintexts: row i of `values` into the
-    evaluation-form polynomial at offs[i] (level limbs); host FFTs in chunks,
-    one batched NTT per chunk on the device."""
+def encode_plaintexts(ctx: FheContext, enc: Encoder, values: np.ndarray, scale: float, offs, level: int) -> None:
+    """Server-side encoding of many real plaintexts on the device
+    (afhe_encode_batch: special FFT, rounding, RNS, NTT): row i of `values`
+    into the evaluation-form polynomial at offs[i] (level limbs). `enc` is the
+    encoder whose slot order the device follows (the same canonical
+    embedding)."""
+    from . import _lib as L
+    v = np.ascontiguousarray(values, dtype=np.float64)
+    if v.ndim == 1:
+        v = v[None, :]
+    o = np.ascontiguousarray(offs, dtype=np.uint64)
+    assert v.shape[0] == o.size and v.shape[1] <= enc.slots
+    L.check(ctx.lib.afhe_encode_batch(ctx.h, v.ctypes.data_as(C.POINTER(C.c_double)), v.shape[0], v.shape[1],
+                                      float(scale), level, o.ctypes.data_as(L.P64)), "encode_batch")
+
+
+def encode_index_batches(ctx: FheContext, index, vids, first, counts, offs, scale: float, level: int) -> None:
+    """The stage-3 candidate plaintexts built and encoded on the device
+    (afhe_pq_*): batch b holds candidates vids[first[b] .. first[b] +
+    counts[b]); slot d B + j = component d of candidate j's reconstruction
+    (centroid of its list + its PQ codewords)."""
+    from . import _lib as L
+    cent = np.ascontiguousarray(index.centroids, dtype=np.float32)
+    books = np.ascontiguousarray(index.codebooks, dtype=np.float32)
+    codes = np.ascontiguousarray(index.codes, dtype=np.uint8)
+    assign = np.ascontiguousarray(index.assignments, dtype=np.uint32)
+    M, K, sd = books.shape
+    ix = L.PqIndex(cent.shape[0], cent.shape[1], M, K, codes.shape[0], cent.ctypes.data_as(C.POINTER(C.c_float)),
+                   books.ctypes.data_as(C.POINTER(C.c_float)), codes.ctypes.data_as(C.POINTER(C.c_uint8)),
+                   assign.ctypes.data_as(L.P32))
+    h = C.c_void_p()
+    L.check(ctx.lib.afhe_pq_create(ctx.h, C.byref(ix), C.byref(h)), "pq_create")
+    try:
+        v = np.ascontiguousarray(vids, dtype=np.uint32)
+        f = np.ascontiguousarray(first, dtype=np.uint32)
+        c = np.ascontiguousarray(counts, dtype=np.uint32)
+        o = np.ascontiguousarray(offs, dtype=np.uint64)
+        L.check(ctx.lib.afhe_pq_encode_batches(h, v.ctypes.data_as(L.P32), f.ctypes.data_as(L.P32),
+                                               c.ctypes.data_as(L.P32), o.size, float(scale), level,
+                                               o.ctypes.data_as(L.P64)), "pq_encode_batches")
+    finally:
+        ctx.lib.afhe_pq_destroy(h)
+
+
+def encode_plaintexts_host(ctx: FheContext, enc: Encoder, values: np.ndarray, scale: float, offs, level: int,
+                           chunk: int = 256) -> None:
+    """encode_plaintexts with the host encoder (numpy FFT) and a device NTT:
+    the exactly rounded coefficients, for comparison."""
     from . import _lib as L
     primes = [np.int64(q) for q in ctx.params.q[:level]]
     for c0 in range(0, len(offs), chunk):

@@ -54,7 +54,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _lib as L
-from .ckks import Encoder, Slots, encode_plaintext, encode_plaintexts
+from .ckks import Encoder, Slots, encode_index_batches, encode_plaintext, encode_plaintexts
 from .driver import FheContext, FHEHostDriver
 from .ivfpq import IvfPqIndex
 
@@ -197,26 +197,24 @@ class InteractiveQueryManager:
         self.mask_prefix: dict[int, int] = {}
         B = shape.B
         self.batches: list[list[tuple[int, int, list]]] = []
-        counts, vals, offs = set(), [], []
+        counts, bvids, bfirst, bcnt, boffs = set(), [], [], [], []
         for c in range(index.n_list):
             vl = index.lists[c]
             out = []
             for b0 in range(0, len(vl), B):
                 vids = vl[b0:b0 + B]
-                rec = index.reconstruct(vids)           # (cnt, D)
-                packed = np.zeros((D, B))
-                packed[:, :len(vids)] = rec.T             # slot d * B + j = x_j[d]
                 off = slots.take(1)[0]
-                vals.append(packed.ravel())
-                offs.append(off)
+                bfirst.append(len(bvids))
+                bcnt.append(len(vids))
+                bvids.extend(vids)
+                boffs.append(off)
                 out.append((off, len(vids), list(vids)))
                 counts.add(len(vids))
-                if len(vals) == 256:
-                    encode_plaintexts(ctx, self.enc, np.stack(vals), shape.scale, offs, L)
-                    vals, offs = [], []
             self.batches.append(out)
-        if vals:
-            encode_plaintexts(ctx, self.enc, np.stack(vals), shape.scale, offs, L)
+        # built on the device from the index: slot d * B + j = x_j[d] (x_j the
+        # reconstruction of candidate j: centroid + PQ codewords)
+        if boffs:
+            encode_index_batches(ctx, index, bvids, bfirst, bcnt, boffs, shape.scale, L)
         self._counts = sorted(counts)
         for lv in self.levels:
             self._prefix_masks(lv)

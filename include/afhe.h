@@ -377,6 +377,40 @@ int afhe_eval_mult_plain_rescale_batch(afhe_ctx* ctx, const afhe_ct_ref* a, cons
 int afhe_rescale_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const afhe_ct_ref* dst, uint32_t count,
                        uint32_t in_limbs);
 
+/* ---- server-side plaintext encoding ---------------------------------------- */
+/* CKKS encoding of `count` real slot vectors on the device: row i of `values`
+ * (host, count x slots doubles, row-major; slots <= N/2, the rest zero) at
+ * `scale` into the evaluation-form polynomial at pt[i] (level limbs). The
+ * server's plaintexts of the reference are OpenFHE's MakeCKKSPackedPlaintext
+ * (fhe_core/fhe_searcher.cpp:334-368; centroids and masks in
+ * integration_tools/generate_interactive_test_vectors.cpp:461-521). Slot j is
+ * the value at the root exp(i pi 5^j / N); the inverse embedding is a
+ * double-precision special FFT, coefficients rounded to nearest (equal to the
+ * exactly rounded ones but where a value lies within the transform's
+ * rounding error of a half-integer). AFHE_E_ARG if a coefficient reaches
+ * 2^62. */
+int afhe_encode_batch(afhe_ctx* ctx, const double* values, uint32_t count, uint32_t slots, double scale,
+                      uint32_t level, const uint64_t* pt);
+/* An IVF-PQ index held in device memory, to build the dimension-major
+ * candidate plaintexts of stage 3 there (fhe_searcher.cpp:334-368): candidate
+ * = the centroid of its list + its PQ codewords (residual PQ). */
+typedef struct afhe_pq_index {
+    uint32_t n_list, d, M, K;     /* M sub-quantizers of d / M components, K codewords each (<= 256) */
+    uint64_t n;                   /* vectors */
+    const float* centroids;       /* n_list x d */
+    const float* codebooks;       /* M x K x (d / M) */
+    const uint8_t* codes;         /* n x M */
+    const uint32_t* assignments;  /* n: the list of each vector */
+} afhe_pq_index;
+typedef struct afhe_pq afhe_pq;
+int afhe_pq_create(afhe_ctx* ctx, const afhe_pq_index* index, afhe_pq** out);
+int afhe_pq_destroy(afhe_pq* pq);
+/* Batch b: candidates vids[first[b] .. first[b] + count[b]) (count <= N / 2d);
+ * slot d' B + j (B = N / 2d) = component d' of candidate j, 0 past the count;
+ * encoded as afhe_encode_batch does into pt[b]. */
+int afhe_pq_encode_batches(afhe_pq* pq, const uint32_t* vids, const uint32_t* first, const uint32_t* count,
+                           uint32_t batches, double scale, uint32_t level, const uint64_t* pt);
+
 /* ---- encrypted IVF-PQ server stages ---------------------------------------- */
 /* InteractiveQueryManager's server stages (cpp_host_model/src/
  * interactive_query_manager.cpp:85-303) for many queries at once: stage 1 +
