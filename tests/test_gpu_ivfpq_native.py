@@ -24,20 +24,25 @@ def results(wl, recs):
 
 
 def both_ways(wl, Q, levels=None, nprobes=None):
+    """The protocol once through the native driver (encryption, stage 1,
+    the client's selection, stage 3), then stages 1 and 3 again from Python
+    on the same encrypted queries and selections."""
     recs = wl.records[:len(Q)]
     out = {}
-    for native in (True, False):
-        wl.iqm.native = native
-        try:
-            for r in recs:
-                for ct in [r.compact] + r.results:       # nothing left from the other run
-                    z = np.zeros(wl.iqm.lvl_out * wl.params.n, dtype=np.uint64)
-                    wl.ctx.write_poly(ct[0], z)
-                    wl.ctx.write_poly(ct[1], z)
-            res = wl.run(Q, recs, levels=levels, nprobes=nprobes)
-            out[native] = (results(wl, recs), [list(x["probes"]) for x in res], [x["topk"] for x in res])
-        finally:
-            wl.iqm.native = True
+    wl.run(Q, recs, levels=levels, nprobes=nprobes)
+    out[True] = results(wl, recs)
+    z = np.zeros(wl.iqm.lvl_out * wl.params.n, dtype=np.uint64)
+    for r in recs:
+        for ct in [r.compact] + r.results:       # nothing left from the native run
+            wl.ctx.write_poly(ct[0], z)
+            wl.ctx.write_poly(ct[1], z)
+    wl.iqm.native = False
+    try:
+        wl.iqm.stage1_coarse(recs)
+        wl.iqm.stage3_fine(recs)
+        out[False] = results(wl, recs)
+    finally:
+        wl.iqm.native = True
     return out
 
 
@@ -56,8 +61,7 @@ def test_native_equals_python(spec, levels, nprobes, lanes):
     try:
         Q = wl.queries(n, seed=31)
         out = both_ways(wl, Q, levels, nprobes)
-        (rn, pn, tn), (rp, pp, tp) = out[True], out[False]
-        assert pn == pp and tn == tp
+        rn, rp = out[True], out[False]
         assert any(np.any(c0) for c0, _ in rn), "the native run wrote nothing"
         for i, ((a0, a1), (b0, b1)) in enumerate(zip(rn, rp)):
             assert np.array_equal(a0, b0) and np.array_equal(a1, b1), f"ciphertext {i} differs"

@@ -15,8 +15,8 @@ pytestmark = pytest.mark.gpu
 
 # log_n, num_q, num_p, alpha, level range, ciphertexts
 SHAPES = {
-    "n1024": (10, 4, 2, 1, (1, 4), 6),
-    "n8192": (13, 3, 1, 1, (1, 3), 6),
+    "n1024": (10, 4, 2, 1, (2, 4), 6),
+    "n8192": (13, 3, 1, 1, (2, 3), 6),
     "n16384_cl2": (14, 6, 2, 3, (2, 6), 5),
     "n32768_cl4": (15, 12, 4, 4, (3, 12), 4),
     "n65536_cl8": (16, 8, 4, 4, (3, 8), 3),

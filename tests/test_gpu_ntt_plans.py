@@ -44,8 +44,9 @@ def test_every_plan_same_residues(log_n, orc):
         for plan, o in outs.items():
             for z in range(wl.polys):
                 assert np.array_equal(o[z], outs[0][z]), f"plan {plan} ({ntt_plan_describe(log_n, plan)}) differs"
+        set_ntt_plan(log_n, 0)
         t = time_ntt_plans(wl.ctx, wl.polys, wl.limbs, reps=1)
-        assert set(t) == set(range(ntt_plan_count(log_n))) and get_ntt_plan(log_n) == keep
+        assert set(t) == set(range(ntt_plan_count(log_n))) and get_ntt_plan(log_n) == 0   # restored
     finally:
         set_ntt_plan(log_n, keep)
         wl.close()
