@@ -20,7 +20,7 @@ OK, E_ARG, E_RANGE, E_NOKEY, E_LEVEL, E_BUDGET, E_TIMEOUT, E_CUDA, E_STATE = ran
 
 OP_NTT, OP_INTT, OP_POLY_ADD, OP_POLY_SUB, OP_POLY_MUL_NTT = 1, 2, 3, 4, 5
 OP_AUTOMORPHISM, OP_KEY_SWITCH, OP_RESCALE, OP_LOAD_CONTEXT = 6, 7, 8, 99
-OPT_KS_FUSED, OPT_CHUNK, OPT_FUSED_MIN, OPT_KS_CAPACITY, OPT_KS_EPT = 1, 2, 3, 4, 5
+OPT_KS_FUSED, OPT_CHUNK, OPT_FUSED_MIN, OPT_KS_CAPACITY, OPT_KS_EPT, OPT_KS_SLICE = 1, 2, 3, 4, 5, 6
 
 u32, u64, i32 = C.c_uint32, C.c_uint64, C.c_int32
 P64 = C.POINTER(C.c_uint64)
@@ -171,7 +171,7 @@ SIGNATURES = {
     "afhe_ivfpq_set_prefix_mask": (C.c_int, [C.c_void_p, u32, u32, u64]),
     "afhe_ivfpq_set_list": (C.c_int, [C.c_void_p, u32, P64, P32, u32]),
     "afhe_ivfpq_set_lanes": (C.c_int, [C.c_void_p, C.POINTER(CtRef), u32, C.POINTER(CtRef)]),
-    "afhe_ivfpq_set_tuning": (C.c_int, [C.c_void_p, u32, i32, u32, u32]),
+    "afhe_ivfpq_set_tuning": (C.c_int, [C.c_void_p, u32, i32, u32, u32, u32]),
     "afhe_ivfpq_stage1": (C.c_int, [C.c_void_p, C.POINTER(IvfpqQuery), u32]),
     "afhe_ivfpq_stage3": (C.c_int, [C.c_void_p, C.POINTER(IvfpqQuery), u32]),
 }

@@ -37,6 +37,7 @@ class KsChoice:
     chunk: int
     us_per_ct: float
     ept: int = 8          # values per thread of the one-kernel key switch (AFHE_OPT_KS_EPT)
+    slice: int = 13       # log2 of a cluster CTA's slice (AFHE_OPT_KS_SLICE; 12 at N = 2^14, 2^15)
 
 
 def gpu_name(device: int = 0) -> str:
@@ -74,7 +75,7 @@ TIE = 0.10   # candidates within this fraction of the fastest count as ties
 # Version of the key-switch kernels a cache was tuned against: a cache from
 # other kernels (e.g. before the one-kernel path existed at this ring degree)
 # is tuned again.
-KERNELS = 4
+KERNELS = 5
 
 
 def ntt_plan_count(log_n: int) -> int:
@@ -129,7 +130,7 @@ def time_ntt_plans(ctx: FheContext, polys: int, limbs: int, reps: int = 3) -> di
 
 
 def pick(timings: dict) -> tuple:
-    """The key of {(fused, chunk[, ept]): us_per_ct} to use: among the
+    """The key of {(fused, chunk[, ept, slice]): us_per_ct} to use: among the
     candidates within TIE of the fastest, the largest chunk (fewest
     launches; a chain's batches are rarely a multiple of the tile, and every
     extra launch costs its tail), then the one-kernel path, then the
@@ -176,22 +177,32 @@ def tune(params: CkksParams, levels, lanes: int, device: int = 0, verbose: bool 
             ctx.write_poly(i * w_max, np.concatenate([rng.integers(0, q, n, dtype=np.uint64)
                                                       for q in params.q[:max(levels)]]))
         fused_ok = ctx.get_option(L.OPT_KS_FUSED) == 1    # the context enables it where the GPU can run it
-        shapes = [(True, 8), (True, 16), (False, 8)] if fused_ok else [(False, 8)]
+        shapes = [(True, 8, 13), (True, 16, 13), (False, 8, 13)] if fused_ok else [(False, 8, 13)]
+        if fused_ok and params.log_n in (14, 15):
+            try:
+                ctx.set_option(L.OPT_KS_SLICE, 12)
+                shapes.insert(2, (True, 8, 12))
+            except L.AfheError:
+                pass                     # two CTAs per SM cannot be placed in clusters here
+            ctx.set_option(L.OPT_KS_SLICE, 13)
         out = {}
         for lv in sorted(set(levels)):
             timings = {}
-            for fused, ept in shapes:
+            for fused, ept, sl in shapes:
                 ctx.set_option(L.OPT_KS_FUSED, int(fused))
                 ctx.set_option(L.OPT_KS_EPT, ept)
+                ctx.set_option(L.OPT_KS_SLICE, sl)
                 cap = ctx.get_option(L.OPT_KS_CAPACITY) if fused else 0
                 for c in chunk_candidates(lanes, sm_count(device), cap):
                     ctx.set_option(L.OPT_CHUNK, c)
-                    timings[(fused, c, ept)] = time_rotations(ctx, lv, count)
+                    timings[(fused, c, ept, sl)] = time_rotations(ctx, lv, count)
                     if verbose:
-                        print(f"level {lv} fused={fused} ept={ept} chunk={c}: {timings[(fused, c, ept)]:.2f} us/ct")
-            f, c, e = pick(timings)
-            out[lv] = KsChoice(f, c, timings[(f, c, e)], e)
+                        print(f"level {lv} fused={fused} ept={ept} slice=2^{sl} chunk={c}: "
+                              f"{timings[(fused, c, ept, sl)]:.2f} us/ct")
+            f, c, e, sl = pick(timings)
+            out[lv] = KsChoice(f, c, timings[(f, c, e, sl)], e, sl)
         ctx.set_option(L.OPT_KS_EPT, 8)
+        ctx.set_option(L.OPT_KS_SLICE, 13)
         return out
     finally:
         ctx.close()

@@ -568,6 +568,15 @@ int afhe_ctx_set_option(afhe_ctx* ctx, uint32_t option, int64_t value) {
         if (value != 8 && value != 16) return fail(ctx, AFHE_E_ARG, "values per thread must be 8 or 16");
         ctx->ks_ept = (uint32_t)value;
         return AFHE_OK;
+    case AFHE_OPT_KS_SLICE:
+        if (value != 12 && value != 13) return fail(ctx, AFHE_E_ARG, "the slice must be 2^12 or 2^13 values");
+        if (value == 12 && (ctx->log_n == 14 || ctx->log_n == 15)) {
+            if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, AFHE_E_CUDA, "cudaSetDevice");
+            if (key_switch_fused_capacity(ctx->log_n, 8, 12) <= 0)
+                return fail(ctx, AFHE_E_ARG, "clusters of 2^12-value slices cannot run on this GPU");
+        }
+        ctx->ks_slice = (uint32_t)value;
+        return AFHE_OK;
     case AFHE_OPT_KS_CAPACITY:
         return fail(ctx, AFHE_E_ARG, "the key-switch capacity is read only");
     default:
@@ -582,9 +591,10 @@ int afhe_ctx_get_option(afhe_ctx* ctx, uint32_t option, int64_t* value) {
     case AFHE_OPT_CHUNK: *value = ctx->chunk ? ctx->chunk : ctx->lanes; return AFHE_OK;
     case AFHE_OPT_FUSED_MIN: *value = ctx->fused_min; return AFHE_OK;
     case AFHE_OPT_KS_EPT: *value = ctx->ks_ept; return AFHE_OK;
+    case AFHE_OPT_KS_SLICE: *value = ctx->ks_slice; return AFHE_OK;
     case AFHE_OPT_KS_CAPACITY:
         if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, AFHE_E_CUDA, "cudaSetDevice");
-        *value = key_switch_fused_capacity(ctx->log_n, (int)ctx->ks_ept);
+        *value = key_switch_fused_capacity(ctx->log_n, (int)ctx->ks_ept, (int)ctx->ks_slice);
         return AFHE_OK;
     default: return fail(ctx, AFHE_E_ARG, "unknown option");
     }

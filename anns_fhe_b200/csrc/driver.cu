@@ -86,7 +86,7 @@ int ks_batch(afhe_ctx* ctx, const ZField& in, const ZField& out0, const ZField& 
     if (ctx->ks_fused && fused_ok && (lvz || nz >= ctx->fused_min)) {
         CK(launch_key_switch_fused(ctx->log_n, t, limbs, ctx->K, ctx->key, evk, evk + (u64)ctx->dnum * S * n,
                                    (uint32_t)S, ctx->L, ctx->poly, ctx->scr, nz, zb, ctx->st, fuse, prep,
-                                   lvz ? ctx->lv_dev : nullptr, lvz, (int)ctx->ks_ept));
+                                   lvz ? ctx->lv_dev : nullptr, lvz, (int)ctx->ks_ept, (int)ctx->ks_slice));
         return AFHE_OK;
     }
     CK(launch_key_switch(ctx->log_n, t, ctx->jobs_qp, lj.modup, lj.n_modup, ctx->L, limbs, ctx->K, ctx->key, evk,
@@ -681,7 +681,7 @@ int afhe_eval_rotate_steps_batch(afhe_ctx* ctx, const afhe_ct_ref* in, const afh
             }
             CK(launch_key_switch_fused(ctx->log_n, t, limbs, ctx->K, ctx->key, 0, (u64)ctx->dnum * S * n, (uint32_t)S,
                                        ctx->L, ctx->poly, ctx->scr, m, zb, ctx->st, &f, prep, nullptr, nullptr,
-                                       (int)ctx->ks_ept));
+                                       (int)ctx->ks_ept, (int)ctx->ks_slice));
             return AFHE_OK;
         }
         CK(launch_key_switch(ctx->log_n, t, ctx->jobs_qp, lj.modup, lj.n_modup, ctx->L, limbs, ctx->K, ctx->key, 0,

@@ -119,6 +119,7 @@ struct afhe_ctx {
     uint32_t chunk = 0;     // ciphertexts per launch of a batched call (0: all lanes)
     uint32_t fused_min = 1; // launches of fewer ciphertexts take the multi-kernel key switch
     uint32_t ks_ept = 8;    // values per thread of the one-kernel key switch (8 or 16)
+    uint32_t ks_slice = 13; // log2 of the slice a CTA of a cluster holds (12: N = 2^14, 2^15 only)
     // afhe_fence: fence f is event fences[f % size], recorded on st
     std::vector<cudaEvent_t> fences;
     uint64_t fence_next = 0;
@@ -213,13 +214,13 @@ cudaError_t launch_key_switch(int log_n, const OpTabs& t, const LimbJob* jobs_qp
 bool key_switch_fused_supported(int log_n);
 // ciphertexts the one-kernel key switch holds at once on the current device
 // (resident CTAs at N <= 2^13, resident clusters above; 0: cannot run)
-int key_switch_fused_capacity(int log_n, int ept = 8);
+int key_switch_fused_capacity(int log_n, int ept = 8, int slice = 13);
 size_t ks_fused_scratch_words(uint32_t n, uint32_t sizeQl, uint32_t K);
 cudaError_t launch_key_switch_fused(int log_n, const OpTabs& t, uint32_t sizeQl, uint32_t K, const u64* key, u64 evk_a,
                                     u64 evk_b, uint32_t key_stride, uint32_t key_pbase, u64* arena, u64* scratch,
                                     uint32_t nz, const ZBases& zb, cudaStream_t st, const KsFuse* fuse = nullptr,
                                     const ulonglong2* prep = nullptr, const OpTabs* lvtabs = nullptr,
-                                    const ZField* lvz = nullptr, int ept = 8);
+                                    const ZField* lvz = nullptr, int ept = 8, int slice = 13);
 // With lvtabs and lvz (mixed levels), entry z runs at level lvz->at(z) with
 // the tables lvtabs[level] (a device copy of the context's per-level tables;
 // sizeQl is then the largest level), each reading and writing that many limbs.

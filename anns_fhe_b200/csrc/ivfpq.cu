@@ -47,7 +47,7 @@ struct afhe_ivfpq {
     std::vector<afhe_ct_ref> cmp;                       // (n_list - 1) per lane: reference compaction terms
     struct Tuning {
         int32_t fused;
-        uint32_t chunk, ept;
+        uint32_t chunk, ept, slice;
     };
     std::map<uint32_t, Tuning> tuning;                 // level -> key-switch options
     bool fused_ok = false;                              // the one-kernel key switch was on at creation
@@ -77,6 +77,7 @@ void at(afhe_ivfpq* h, uint32_t limbs) {
     if (o.fused == 0 || (o.fused > 0 && h->fused_ok)) afhe_ctx_set_option(h->ctx, AFHE_OPT_KS_FUSED, o.fused);
     afhe_ctx_set_option(h->ctx, AFHE_OPT_CHUNK, std::min<uint32_t>(o.chunk, h->ctx->lanes));
     if (o.ept) afhe_ctx_set_option(h->ctx, AFHE_OPT_KS_EPT, o.ept);
+    if (o.slice) afhe_ctx_set_option(h->ctx, AFHE_OPT_KS_SLICE, o.slice);
 }
 
 #define RC(expr)                              \
@@ -400,10 +401,12 @@ int afhe_ivfpq_set_lanes(afhe_ivfpq* h, const afhe_ct_ref* work, uint32_t lanes,
     return AFHE_OK;
 }
 
-int afhe_ivfpq_set_tuning(afhe_ivfpq* h, uint32_t level, int32_t fused, uint32_t chunk, uint32_t ept) {
+int afhe_ivfpq_set_tuning(afhe_ivfpq* h, uint32_t level, int32_t fused, uint32_t chunk, uint32_t ept,
+                          uint32_t slice) {
     if (!h) return fail_h(h, AFHE_E_ARG, "null argument");
     if (ept && ept != 8 && ept != 16) return fail_h(h, AFHE_E_ARG, "values per thread must be 8 or 16");
-    h->tuning[level] = {fused, chunk, ept};
+    if (slice && slice != 12 && slice != 13) return fail_h(h, AFHE_E_ARG, "the slice must be 2^12 or 2^13 values");
+    h->tuning[level] = {fused, chunk, ept, slice};
     return AFHE_OK;
 }
 

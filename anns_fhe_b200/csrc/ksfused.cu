@@ -65,7 +65,7 @@ struct KsFusedArgs {
     ZField lvz;
 };
 
-constexpr int kLogQ = 13;    // log2 of the slice a CTA holds at N >= 2^13
+constexpr int kLogQ = 13;    // log2 of the slice a CTA holds at N >= 2^13 (12 on request at N = 2^14, 2^15)
 
 // One polynomial per CTA (LOGCL = 0) or per cluster of 2^LOGCL CTAs; each CTA
 // holds 2^LOGQ elements of every buffer. Local positions e < 2^LOGQ, global
@@ -562,8 +562,11 @@ __device__ __forceinline__ void ks_one_limb(const KsFusedArgs& a, const OpTabs& 
     }
 }
 
+// Slices of 2^12 in a cluster (N = 2^14, 2^15) take 104 KB of shared memory
+// and 512 threads: two CTAs per SM, whose barriers interleave.
 template <int LOGQ, int LOGCL, bool PREP, int E>
-__global__ void __launch_bounds__((1u << LOGQ) / E, 1) ks_fused_kernel(const KsFusedArgs a) {
+__global__ void __launch_bounds__((1u << LOGQ) / E, (LOGCL > 0 && LOGQ < 13) ? 2 : 1)
+    ks_fused_kernel(const KsFusedArgs a) {
     using G = Geo<LOGQ, LOGCL, E>;
     constexpr int LOGN = G::LOGN;
     constexpr uint32_t PADQ = G::QN + G::QN / 16;
@@ -751,13 +754,19 @@ cudaError_t launch_fused(const KsFusedArgs& a, uint32_t nz, cudaStream_t st, int
     return a.prep ? launch_fused_v<LOGQ, LOGCL, true, 8>(a, nz, st) : launch_fused_v<LOGQ, LOGCL, false, 8>(a, nz, st);
 }
 
-// Clusters the GPU can hold at once for the kernel at N = 2^(13 + logcl)
+// 2^12-value slices (clusters of 4 or 8 CTAs, two CTAs per SM), 8 values per thread
+template <int LOGCL>
+cudaError_t launch_slice12(const KsFusedArgs& a, uint32_t nz, cudaStream_t st) {
+    return a.prep ? launch_fused_v<12, LOGCL, true, 8>(a, nz, st) : launch_fused_v<12, LOGCL, false, 8>(a, nz, st);
+}
+
+// Clusters the GPU can hold at once for the kernel at N = 2^(LOGQ + LOGCL)
 // (0 when it cannot place even one: the multi-kernel path is used then).
-template <int LOGCL, int E = 8>
+template <int LOGCL, int E = 8, int LOGQ = kLogQ>
 int cluster_capacity() {
-    constexpr uint32_t QN = 1u << kLogQ;
+    constexpr uint32_t QN = 1u << LOGQ;
     const size_t smem = 3ull * (QN + QN / 16) * sizeof(u64);
-    auto kern = ks_fused_kernel<kLogQ, LOGCL, true, E>;
+    auto kern = ks_fused_kernel<LOGQ, LOGCL, true, E>;
     if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) {
         cudaGetLastError();
         return 0;
@@ -799,7 +808,9 @@ __global__ void key_prep_kernel(const u64* __restrict__ key, ulonglong2* __restr
 
 }  // namespace
 
-int key_switch_fused_capacity(int log_n, int ept) {
+int key_switch_fused_capacity(int log_n, int ept, int slice) {
+    if (slice == 12 && (log_n == 14 || log_n == 15))
+        return log_n == 14 ? cluster_capacity<2, 8, 12>() : cluster_capacity<3, 8, 12>();
     if (log_n >= 14 && log_n <= 16) {
         if (ept == 16)
             return log_n == 14 ? cluster_capacity<1, 16>() : log_n == 15 ? cluster_capacity<2, 16>()
@@ -863,7 +874,8 @@ cudaError_t launch_key_prep(const u64* key, ulonglong2* prep, const PrimeConst* 
 cudaError_t launch_key_switch_fused(int log_n, const OpTabs& t, uint32_t sizeQl, uint32_t K, const u64* key, u64 evk_a,
                                     u64 evk_b, uint32_t key_stride, uint32_t key_pbase, u64* arena, u64* scratch,
                                     uint32_t nz, const ZBases& zb, cudaStream_t st, const KsFuse* fuse,
-                                    const ulonglong2* prep, const OpTabs* lvtabs, const ZField* lvz, int ept) {
+                                    const ulonglong2* prep, const OpTabs* lvtabs, const ZField* lvz, int ept,
+                                    int slice) {
     if (nz == 0) return cudaSuccess;
     KsFusedArgs a{};
     a.t = t;
@@ -892,8 +904,8 @@ cudaError_t launch_key_switch_fused(int log_n, const OpTabs& t, uint32_t sizeQl,
     case 11: return launch_fused<11, 0>(a, nz, st, ept);
     case 12: return launch_fused<12, 0>(a, nz, st, ept);
     case 13: return launch_fused<13, 0>(a, nz, st, ept);
-    case 14: return launch_fused<kLogQ, 1>(a, nz, st, ept);
-    case 15: return launch_fused<kLogQ, 2>(a, nz, st, ept);
+    case 14: return slice == 12 ? launch_slice12<2>(a, nz, st) : launch_fused<kLogQ, 1>(a, nz, st, ept);
+    case 15: return slice == 12 ? launch_slice12<3>(a, nz, st) : launch_fused<kLogQ, 2>(a, nz, st, ept);
     case 16: return launch_fused<kLogQ, 3>(a, nz, st, ept);
     default: return cudaErrorInvalidValue;
     }

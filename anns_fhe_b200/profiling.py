@@ -73,7 +73,8 @@ def ks_roofline(params, lanes: int, reps: int = 20, level: int = 0, nbuf: int = 
                 ctx.set_option(1, int(choice.fused))
             ctx.set_option(2, min(int(choice.chunk), lanes))
             ctx.set_option(5, int(getattr(choice, "ept", 8)))
-        ept = ctx.get_option(5)
+            ctx.set_option(6, int(getattr(choice, "slice", 13)))
+        ept, slc = ctx.get_option(5), ctx.get_option(6)
         limb = np.concatenate([rng.integers(0, q, n, dtype=np.uint64) for q in p.q[:L]])
         for i in range((nbuf + 1) * lanes * 2):
             ctx.write_poly(i * w, limb)
@@ -107,12 +108,13 @@ def ks_roofline(params, lanes: int, reps: int = 20, level: int = 0, nbuf: int = 
     peak, src = load_peaks()
     cap = KS_CAPTURES.get((n, L, K))
     traffic = int_pipe = None
-    if cap and launches == 1 and fused and ept == cap.get("ept", 8):
+    if cap and launches == 1 and fused and ept == cap.get("ept", 8) and slc == cap.get("slice", 13):
         # the capture's per-ciphertext traffic scaled to this launch, the key once
         traffic = (cap["dram_bytes"] - key_bytes) * lanes / cap["ciphertexts"] + key_bytes
         int_pipe = {"pipe": cap["pipe"], "frac": cap["util"], "kernel": cap["kernel"],
                     "captured_ciphertexts": cap["ciphertexts"]}
-    kind = f"one-kernel, {ept} values per thread" if fused and launches == 1 else f"{launches:g}-launch"
+    shape = f", 2^{slc}-value slices" if n >= 1 << 14 else ""
+    kind = f"one-kernel, {ept} values per thread{shape}" if fused and launches == 1 else f"{launches:g}-launch"
     return {"bound": "hbm", "kernel": f"rotation key switch, {kind} (N={n}, {L} + {K} limbs, "
                                       f"{lanes} ciphertexts per call)",
             "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
@@ -123,7 +125,7 @@ def ks_roofline(params, lanes: int, reps: int = 20, level: int = 0, nbuf: int = 
 # ---------------------------------------------------------------------------
 # profiling drivers
 # ---------------------------------------------------------------------------
-def profile_ks(lanes: int, workload: str = "small", level: int = 0, ept: int = 8):
+def profile_ks(lanes: int, workload: str = "small", level: int = 0, ept: int = 8, slc: int = 13):
     """The roofline measurement of the key switch alone (five warm-up calls,
     then 20 measured) at `level` limbs (default: the workload's evaluation
     level), the one-kernel key switch at `ept` values per thread."""
@@ -133,7 +135,7 @@ def profile_ks(lanes: int, workload: str = "small", level: int = 0, ept: int = 8
     spec = LARGE if workload == "large" else SMALL
     p = CkksParams.generate(spec.log_n, spec.num_q, spec.q_bits, spec.num_p, spec.p_bits, spec.alpha)
     print(json.dumps(ks_roofline(p, lanes, level=level or spec.eval_level or spec.num_q,
-                                 choice=KsChoice(True, lanes, 0.0, ept))))
+                                 choice=KsChoice(True, lanes, 0.0, ept, slc))))
 
 
 def profile_step(nq: int, workload: str = "small", lanes: int = 0):
@@ -326,6 +328,7 @@ def main() -> None:
     a.add_argument("--workload", default="small", choices=["small", "large"])
     a.add_argument("--level", type=int, default=0)
     a.add_argument("--ept", type=int, default=8, choices=[8, 16], help="values per thread (one-kernel path)")
+    a.add_argument("--slice", type=int, default=13, choices=[12, 13], help="log2 of a cluster CTA's slice")
     a = sub.add_parser("ntt", help="batched NTT / INTT: polynomials per launch")
     a.add_argument("polys", type=int)
     a.add_argument("--log-n", type=int, default=13)
@@ -338,7 +341,7 @@ def main() -> None:
     a.add_argument("--calls", type=int, default=200)
     args = ap.parse_args()
     if args.what == "ks":
-        profile_ks(args.lanes, args.workload, args.level, args.ept)
+        profile_ks(args.lanes, args.workload, args.level, args.ept, args.slice)
     elif args.what == "ntt":
         profile_ntt(args.polys, args.log_n)
     elif args.what == "step":

@@ -465,12 +465,13 @@ class InteractiveQueryManager:
         ch = getattr(self, "_tuning", {}).get(level)
         if ch is None:
             return
-        want = (int(ch.fused), int(ch.chunk), int(getattr(ch, "ept", 8)))
+        want = (int(ch.fused), int(ch.chunk), int(getattr(ch, "ept", 8)), int(getattr(ch, "slice", 13)))
         if want != getattr(self, "_opt_now", None):
             if want[0] == 0 or self._fused_ok:
                 self.ctx.set_option(L.OPT_KS_FUSED, want[0])
             self.ctx.set_option(L.OPT_CHUNK, min(want[1], self.ctx.max_batch))
             self.ctx.set_option(L.OPT_KS_EPT, want[2])
+            self.ctx.set_option(L.OPT_KS_SLICE, want[3])
             self._opt_now = want
 
     # ---- the native stage driver ----
@@ -503,8 +504,8 @@ class InteractiveQueryManager:
         cmp = self._refs([c for row in self.cmp[:self.lanes] for c in row]) if self.cmp else None
         L.check(lib.afhe_ivfpq_set_lanes(h, work, self.lanes, cmp), "ivfpq_set_lanes")
         for lv, ch in getattr(self, "_tuning", {}).items():
-            L.check(lib.afhe_ivfpq_set_tuning(h, lv, int(ch.fused), int(ch.chunk), int(getattr(ch, "ept", 8))),
-                    "ivfpq_set_tuning")
+            L.check(lib.afhe_ivfpq_set_tuning(h, lv, int(ch.fused), int(ch.chunk), int(getattr(ch, "ept", 8)),
+                                              int(getattr(ch, "slice", 13))), "ivfpq_set_tuning")
         self._nh_key = key
         return h
 

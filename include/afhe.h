@@ -197,6 +197,13 @@ int afhe_copy_poly(afhe_ctx* ctx, uint64_t dst_offset, uint64_t src_offset, uint
  *                      (N / 8 threads per CTA slice, the default) or 16 (half
  *                      the threads, twice the registers each). Same residues. */
 #define AFHE_OPT_KS_EPT 5u
+/*   AFHE_OPT_KS_SLICE  log2 of the slice each CTA of a cluster holds in the
+ *                      one-kernel key switch at N = 2^14 and 2^15: 13 (the
+ *                      default: clusters of N / 2^13 CTAs of 1024 threads, one
+ *                      per SM) or 12 (clusters of N / 2^12 CTAs of 512 threads,
+ *                      two per SM; 8 values per thread). Ignored at other N.
+ *                      Same residues. */
+#define AFHE_OPT_KS_SLICE 6u
 int afhe_ctx_set_option(afhe_ctx* ctx, uint32_t option, int64_t value);
 int afhe_ctx_get_option(afhe_ctx* ctx, uint32_t option, int64_t* value);
 /* Page-locked host memory for the transfers above (the reference's host
@@ -457,9 +464,10 @@ int afhe_ivfpq_set_list(afhe_ivfpq* h, uint32_t list, const uint64_t* pts, const
  * cmp[j (n_list - 1) + i - 1] = lane j's stage-1b term i (reference compaction). */
 int afhe_ivfpq_set_lanes(afhe_ivfpq* h, const afhe_ct_ref* work, uint32_t lanes, const afhe_ct_ref* cmp);
 /* Key-switch options for operators at `level` limbs: fused (-1 leave, 0 off,
- * 1 on), chunk and values per thread (0: leave), as afhe_ctx_set_option's
- * AFHE_OPT_KS_FUSED / AFHE_OPT_CHUNK / AFHE_OPT_KS_EPT. */
-int afhe_ivfpq_set_tuning(afhe_ivfpq* h, uint32_t level, int32_t fused, uint32_t chunk, uint32_t ept);
+ * 1 on), chunk, values per thread and slice (0: leave), as
+ * afhe_ctx_set_option's AFHE_OPT_KS_FUSED / _CHUNK / _KS_EPT / _KS_SLICE. */
+int afhe_ivfpq_set_tuning(afhe_ivfpq* h, uint32_t level, int32_t fused, uint32_t chunk, uint32_t ept,
+                          uint32_t slice);
 int afhe_ivfpq_stage1(afhe_ivfpq* h, const afhe_ivfpq_query* queries, uint32_t count);
 int afhe_ivfpq_stage3(afhe_ivfpq* h, const afhe_ivfpq_query* queries, uint32_t count);
 

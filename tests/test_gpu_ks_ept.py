@@ -1,7 +1,8 @@
 """The one-kernel key switch gives the same residues at 8 and at 16 values
 per thread (AFHE_OPT_KS_EPT), at every ring degree it runs at: one CTA per
 ciphertext (N = 2^10, 2^13) and clusters of 2, 4 and 8 CTAs (N = 2^14, 2^15,
-2^16). The workload is a rotate-and-sum chain over ciphertexts at mixed
+2^16); and with 2^12-value slices, clusters of 4 and 8 CTAs two to an SM
+(AFHE_OPT_KS_SLICE 12, N = 2^14 and 2^15). The workload is a rotate-and-sum chain over ciphertexts at mixed
 levels in one launch per step (afhe_eval_rotate_accumulate_levels_batch),
 then a rescale; the 8-value kernel is checked against the oracle by
 test_gpu_ks_paths.py and test_gpu_primitives_n65536.py."""
@@ -33,18 +34,24 @@ def test_values_per_thread_same_residues(shape):
             pytest.skip("the one-kernel key switch does not run on this GPU at this ring degree")
         ksb.ctx.set_option(L.OPT_FUSED_MIN, 1)
         out = {}
-        for ept in (8, 16):
+        variants = [(8, 13), (16, 13)] + ([(8, 12)] if log_n in (14, 15) else [])
+        for ept, sl in variants:
             ksb.ctx.set_option(L.OPT_KS_EPT, ept)
-            assert ksb.ctx.get_option(L.OPT_KS_EPT) == ept
+            ksb.ctx.set_option(L.OPT_KS_SLICE, sl)
+            assert ksb.ctx.get_option(L.OPT_KS_EPT) == ept and ksb.ctx.get_option(L.OPT_KS_SLICE) == sl
             assert ksb.ctx.get_option(L.OPT_KS_CAPACITY) > 0
             ksb.reset()
             ksb.run()
             ksb.ctx.sync()
-            out[ept] = [x for z in range(cts) for o in (False, True) for x in ksb.read_ct(z, o)]
-        for i, (a, b) in enumerate(zip(out[8], out[16])):
-            assert np.array_equal(a, b), f"{shape}: polynomial {i} differs between 8 and 16 values per thread"
-        assert any(np.any(a) for a in out[8])
+            out[(ept, sl)] = [x for z in range(cts) for o in (False, True) for x in ksb.read_ct(z, o)]
+        for v in variants[1:]:
+            for i, (a, b) in enumerate(zip(out[(8, 13)], out[v])):
+                assert np.array_equal(a, b), f"{shape}: polynomial {i} differs under {v} (values per thread, slice)"
+        assert any(np.any(a) for a in out[(8, 13)])
+        ksb.ctx.set_option(L.OPT_KS_SLICE, 13)
         with pytest.raises(L.AfheError):
             ksb.ctx.set_option(L.OPT_KS_EPT, 12)
+        with pytest.raises(L.AfheError):
+            ksb.ctx.set_option(L.OPT_KS_SLICE, 11)
     finally:
         ksb.close()

@@ -70,7 +70,7 @@ class FakeLib:
         s = f"{name} {limbs}"
         if ks:
             s += (f" fused={self.ctx.opts[L.OPT_KS_FUSED]} chunk={self.ctx.opts[L.OPT_CHUNK]}"
-                  f" ept={self.ctx.opts[L.OPT_KS_EPT]}")
+                  f" ept={self.ctx.opts[L.OPT_KS_EPT]} slice={self.ctx.opts[L.OPT_KS_SLICE]}")
         return s + " |"
 
     def afhe_eval_add_batch(self, h, a, b, d, n, limbs):
@@ -112,7 +112,7 @@ class FakeCtx:
     def __init__(self, lanes):
         self.h = None
         self.max_batch = lanes
-        self.opts = {L.OPT_KS_FUSED: 1, L.OPT_CHUNK: 0, L.OPT_KS_EPT: 8}
+        self.opts = {L.OPT_KS_FUSED: 1, L.OPT_CHUNK: 0, L.OPT_KS_EPT: 8, L.OPT_KS_SLICE: 13}
 
     def set_option(self, option, value):
         self.opts[option] = value
@@ -122,8 +122,8 @@ class FakeCtx:
 
 
 class Choice:
-    def __init__(self, fused, chunk, ept=8):
-        self.fused, self.chunk, self.ept = fused, chunk, ept
+    def __init__(self, fused, chunk, ept=8, slice=13):
+        self.fused, self.chunk, self.ept, self.slice = fused, chunk, ept, slice
 
 
 def build_manager(rng, *, D, n_list, slots, L_top, lanes, compaction, eval_level, levels, tuning, ctx_lanes):
@@ -200,7 +200,7 @@ CASES = {
     "reference_one_lane": dict(D=8, n_list=5, slots=64, L_top=5, lanes=1, compaction="reference", eval_level=None,
                                levels=[5], tuning={}),
     "packed_eval_level": dict(D=8, n_list=20, slots=64, L_top=7, lanes=4, compaction="packed", eval_level=4,
-                              levels=[7, 6], tuning={4: (1, 4), 3: (0, 2), 2: (1, 4)}),
+                              levels=[7, 6], tuning={4: (1, 4, 8, 12), 3: (0, 2), 2: (1, 4)}),
     "packed_mixed_levels": dict(D=4, n_list=30, slots=32, L_top=6, lanes=5, compaction="packed", eval_level=None,
                                 levels=[6, 5, 3], tuning={5: (1, 5), 4: (1, 1)}),
 }
@@ -220,7 +220,7 @@ def test_native_driver_issues_the_python_drivers_operators(trace, case, stage):
         m.stage3_fine(recs)
     want = py.log
     assert want, "the Python driver issued nothing"
-    m.ctx.opts = {L.OPT_KS_FUSED: 1, L.OPT_CHUNK: 0, L.OPT_KS_EPT: 8}
+    m.ctx.opts = {L.OPT_KS_FUSED: 1, L.OPT_CHUNK: 0, L.OPT_KS_EPT: 8, L.OPT_KS_SLICE: 13}
     got = run_native(trace, m, recs, kw["L_top"], 2 * kw["slots"], ctx_lanes, stage)
     for i, (a, b) in enumerate(zip(got, want)):
         assert a == b, f"call {i} differs:\n native {a[:300]}\n python {b[:300]}"
