@@ -76,6 +76,10 @@ class PqIndex(C.Structure):
                 ("codes", C.POINTER(C.c_uint8)), ("assignments", C.POINTER(u32))]
 
 
+class KsOptions(C.Structure):
+    _fields_ = [("fused", i32), ("chunk", u32), ("ept", u32), ("slice", u32), ("fused_min", u32)]
+
+
 class IvfpqShape(C.Structure):
     _fields_ = [("D", u32), ("n_list", u32), ("slots", u32), ("lanes", u32), ("packed", u32), ("eval_level", u32)]
 
@@ -171,7 +175,7 @@ SIGNATURES = {
     "afhe_ivfpq_set_prefix_mask": (C.c_int, [C.c_void_p, u32, u32, u64]),
     "afhe_ivfpq_set_list": (C.c_int, [C.c_void_p, u32, P64, P32, u32]),
     "afhe_ivfpq_set_lanes": (C.c_int, [C.c_void_p, C.POINTER(CtRef), u32, C.POINTER(CtRef)]),
-    "afhe_ivfpq_set_tuning": (C.c_int, [C.c_void_p, u32, i32, u32, u32, u32]),
+    "afhe_ivfpq_set_tuning": (C.c_int, [C.c_void_p, u32, C.POINTER(KsOptions)]),
     "afhe_ivfpq_stage1": (C.c_int, [C.c_void_p, C.POINTER(IvfpqQuery), u32]),
     "afhe_ivfpq_stage3": (C.c_int, [C.c_void_p, C.POINTER(IvfpqQuery), u32]),
 }

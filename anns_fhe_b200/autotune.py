@@ -38,6 +38,7 @@ class KsChoice:
     us_per_ct: float
     ept: int = 8          # values per thread of the one-kernel key switch (AFHE_OPT_KS_EPT)
     slice: int = 13       # log2 of a cluster CTA's slice (AFHE_OPT_KS_SLICE; 12 at N = 2^14, 2^15)
+    fused_min: int = 0    # launches of fewer ciphertexts take the multi-kernel path (0: context default)
 
 
 def gpu_name(device: int = 0) -> str:
@@ -75,7 +76,7 @@ TIE = 0.10   # candidates within this fraction of the fastest count as ties
 # Version of the key-switch kernels a cache was tuned against: a cache from
 # other kernels (e.g. before the one-kernel path existed at this ring degree)
 # is tuned again.
-KERNELS = 5
+KERNELS = 6
 
 
 def ntt_plan_count(log_n: int) -> int:
@@ -160,6 +161,35 @@ def time_rotations(ctx: FheContext, level: int, count: int, reps: int = 3) -> fl
     return best / count * 1e6
 
 
+def fused_crossover(ctx: FheContext, level: int, lanes: int, verbose: bool = False) -> int:
+    """The fewest ciphertexts per launch from which the one-kernel key switch
+    (one CTA or cluster per ciphertext) beats the multi-kernel pipeline (which
+    spreads one ciphertext over many CTAs) at every larger count tried:
+    AFHE_OPT_FUSED_MIN for this level. The context's options are restored."""
+    keep = ctx.get_option(L.OPT_FUSED_MIN)
+    counts = [c for c in (1, 2, 4, 8, 16, 32, 64, 128) if c <= lanes]
+    wins = {}
+    try:
+        ctx.set_option(L.OPT_FUSED_MIN, 1)
+        for c in counts:
+            ctx.set_option(L.OPT_KS_FUSED, 1)
+            t1 = time_rotations(ctx, level, c)
+            ctx.set_option(L.OPT_KS_FUSED, 0)
+            t0 = time_rotations(ctx, level, c)
+            wins[c] = t1 <= t0
+            if verbose:
+                print(f"level {level}, {c} per launch: one-kernel {t1:.2f}, multi-kernel {t0:.2f} us/ct")
+    finally:
+        ctx.set_option(L.OPT_KS_FUSED, 1)
+        ctx.set_option(L.OPT_FUSED_MIN, keep)
+    fmin = min(4096, 2 * counts[-1]) if counts else 1
+    for c in reversed(counts):
+        if not wins[c]:
+            break
+        fmin = c
+    return fmin
+
+
 def tune(params: CkksParams, levels, lanes: int, device: int = 0, verbose: bool = False) -> dict:
     """{level: KsChoice} measured on `device`."""
     n = params.n
@@ -200,9 +230,15 @@ def tune(params: CkksParams, levels, lanes: int, device: int = 0, verbose: bool 
                         print(f"level {lv} fused={fused} ept={ept} slice=2^{sl} chunk={c}: "
                               f"{timings[(fused, c, ept, sl)]:.2f} us/ct")
             f, c, e, sl = pick(timings)
-            out[lv] = KsChoice(f, c, timings[(f, c, e, sl)], e, sl)
+            fmin = 0
+            if f:
+                ctx.set_option(L.OPT_KS_EPT, e)
+                ctx.set_option(L.OPT_KS_SLICE, sl)
+                fmin = fused_crossover(ctx, lv, lanes, verbose)
+            out[lv] = KsChoice(f, c, timings[(f, c, e, sl)], e, sl, fmin)
         ctx.set_option(L.OPT_KS_EPT, 8)
         ctx.set_option(L.OPT_KS_SLICE, 13)
+        ctx.set_option(L.OPT_KS_FUSED, 1 if fused_ok else 0)
         return out
     finally:
         ctx.close()

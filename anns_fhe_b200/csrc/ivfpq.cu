@@ -45,11 +45,7 @@ struct afhe_ivfpq {
     std::vector<std::vector<std::pair<u64, uint32_t>>> lists;   // list -> (plaintext, candidates) per batch
     std::vector<afhe_ct_ref> work;                      // diff, sq, sel per lane
     std::vector<afhe_ct_ref> cmp;                       // (n_list - 1) per lane: reference compaction terms
-    struct Tuning {
-        int32_t fused;
-        uint32_t chunk, ept, slice;
-    };
-    std::map<uint32_t, Tuning> tuning;                 // level -> key-switch options
+    std::map<uint32_t, afhe_ks_options> tuning;        // level -> key-switch options
     bool fused_ok = false;                              // the one-kernel key switch was on at creation
 };
 
@@ -73,11 +69,12 @@ uint32_t eval_at(const afhe_ivfpq* h, uint32_t level) {
 void at(afhe_ivfpq* h, uint32_t limbs) {
     auto it = h->tuning.find(limbs);
     if (it == h->tuning.end()) return;
-    const afhe_ivfpq::Tuning& o = it->second;
+    const afhe_ks_options& o = it->second;
     if (o.fused == 0 || (o.fused > 0 && h->fused_ok)) afhe_ctx_set_option(h->ctx, AFHE_OPT_KS_FUSED, o.fused);
-    afhe_ctx_set_option(h->ctx, AFHE_OPT_CHUNK, std::min<uint32_t>(o.chunk, h->ctx->lanes));
+    if (o.chunk) afhe_ctx_set_option(h->ctx, AFHE_OPT_CHUNK, std::min<uint32_t>(o.chunk, h->ctx->lanes));
     if (o.ept) afhe_ctx_set_option(h->ctx, AFHE_OPT_KS_EPT, o.ept);
     if (o.slice) afhe_ctx_set_option(h->ctx, AFHE_OPT_KS_SLICE, o.slice);
+    if (o.fused_min) afhe_ctx_set_option(h->ctx, AFHE_OPT_FUSED_MIN, o.fused_min);
 }
 
 #define RC(expr)                              \
@@ -401,12 +398,12 @@ int afhe_ivfpq_set_lanes(afhe_ivfpq* h, const afhe_ct_ref* work, uint32_t lanes,
     return AFHE_OK;
 }
 
-int afhe_ivfpq_set_tuning(afhe_ivfpq* h, uint32_t level, int32_t fused, uint32_t chunk, uint32_t ept,
-                          uint32_t slice) {
-    if (!h) return fail_h(h, AFHE_E_ARG, "null argument");
-    if (ept && ept != 8 && ept != 16) return fail_h(h, AFHE_E_ARG, "values per thread must be 8 or 16");
-    if (slice && slice != 12 && slice != 13) return fail_h(h, AFHE_E_ARG, "the slice must be 2^12 or 2^13 values");
-    h->tuning[level] = {fused, chunk, ept, slice};
+int afhe_ivfpq_set_tuning(afhe_ivfpq* h, uint32_t level, const afhe_ks_options* o) {
+    if (!h || !o) return fail_h(h, AFHE_E_ARG, "null argument");
+    if (o->ept && o->ept != 8 && o->ept != 16) return fail_h(h, AFHE_E_ARG, "values per thread must be 8 or 16");
+    if (o->slice && o->slice != 12 && o->slice != 13) return fail_h(h, AFHE_E_ARG, "the slice must be 2^12 or 2^13 values");
+    if (o->fused_min > 4096) return fail_h(h, AFHE_E_ARG, "fused minimum must be in [1, 4096]");
+    h->tuning[level] = *o;
     return AFHE_OK;
 }
 

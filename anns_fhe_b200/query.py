@@ -465,13 +465,17 @@ class InteractiveQueryManager:
         ch = getattr(self, "_tuning", {}).get(level)
         if ch is None:
             return
-        want = (int(ch.fused), int(ch.chunk), int(getattr(ch, "ept", 8)), int(getattr(ch, "slice", 13)))
+        want = (int(ch.fused), int(ch.chunk), int(getattr(ch, "ept", 8)), int(getattr(ch, "slice", 13)),
+                int(getattr(ch, "fused_min", 0)))
         if want != getattr(self, "_opt_now", None):
             if want[0] == 0 or self._fused_ok:
                 self.ctx.set_option(L.OPT_KS_FUSED, want[0])
-            self.ctx.set_option(L.OPT_CHUNK, min(want[1], self.ctx.max_batch))
+            if want[1]:
+                self.ctx.set_option(L.OPT_CHUNK, min(want[1], self.ctx.max_batch))
             self.ctx.set_option(L.OPT_KS_EPT, want[2])
             self.ctx.set_option(L.OPT_KS_SLICE, want[3])
+            if want[4]:
+                self.ctx.set_option(L.OPT_FUSED_MIN, want[4])
             self._opt_now = want
 
     # ---- the native stage driver ----
@@ -504,8 +508,9 @@ class InteractiveQueryManager:
         cmp = self._refs([c for row in self.cmp[:self.lanes] for c in row]) if self.cmp else None
         L.check(lib.afhe_ivfpq_set_lanes(h, work, self.lanes, cmp), "ivfpq_set_lanes")
         for lv, ch in getattr(self, "_tuning", {}).items():
-            L.check(lib.afhe_ivfpq_set_tuning(h, lv, int(ch.fused), int(ch.chunk), int(getattr(ch, "ept", 8)),
-                                              int(getattr(ch, "slice", 13))), "ivfpq_set_tuning")
+            o = L.KsOptions(int(ch.fused), int(ch.chunk), int(getattr(ch, "ept", 8)), int(getattr(ch, "slice", 13)),
+                            int(getattr(ch, "fused_min", 0)))
+            L.check(lib.afhe_ivfpq_set_tuning(h, lv, C.byref(o)), "ivfpq_set_tuning")
         self._nh_key = key
         return h
 

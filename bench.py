@@ -198,7 +198,7 @@ def measure(args, spec, rank: int, world: int, steps: int, warmup: int, batch: i
             "clocks": summarize_clocks(samples),
             "gpu_launches": int(launches),
             "run": {"lanes": lanes, "setup_s": round(wl.setup_s, 1),
-                    "tuning": ({str(k): [int(v.fused), v.chunk, v.ept, v.slice] for k, v in wl.tuning.items()} if wl.tuning
+                    "tuning": ({str(k): [int(v.fused), v.chunk, v.ept, v.slice, v.fused_min] for k, v in wl.tuning.items()} if wl.tuning
                                else None),
                     "lane_scratch_gb": round(wl.ctx.scratch_bytes() / 1e9, 1),
                     "ks_capacity": wl.ctx.get_option(L.OPT_KS_CAPACITY),

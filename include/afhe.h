@@ -463,11 +463,15 @@ int afhe_ivfpq_set_list(afhe_ivfpq* h, uint32_t list, const uint64_t* pts, const
 /* Working ciphertexts: work[3 j .. 3 j + 2] = lane j's diff, sq, sel;
  * cmp[j (n_list - 1) + i - 1] = lane j's stage-1b term i (reference compaction). */
 int afhe_ivfpq_set_lanes(afhe_ivfpq* h, const afhe_ct_ref* work, uint32_t lanes, const afhe_ct_ref* cmp);
-/* Key-switch options for operators at `level` limbs: fused (-1 leave, 0 off,
- * 1 on), chunk, values per thread and slice (0: leave), as
- * afhe_ctx_set_option's AFHE_OPT_KS_FUSED / _CHUNK / _KS_EPT / _KS_SLICE. */
-int afhe_ivfpq_set_tuning(afhe_ivfpq* h, uint32_t level, int32_t fused, uint32_t chunk, uint32_t ept,
-                          uint32_t slice);
+/* Key-switch options applied around every operator the stages issue at
+ * `level` limbs (afhe_ctx_set_option's AFHE_OPT_KS_FUSED, AFHE_OPT_CHUNK,
+ * AFHE_OPT_KS_EPT, AFHE_OPT_KS_SLICE, AFHE_OPT_FUSED_MIN): fused -1 leaves
+ * the context's setting, any other field 0 leaves it. */
+typedef struct afhe_ks_options {
+    int32_t fused;
+    uint32_t chunk, ept, slice, fused_min;
+} afhe_ks_options;
+int afhe_ivfpq_set_tuning(afhe_ivfpq* h, uint32_t level, const afhe_ks_options* opts);
 int afhe_ivfpq_stage1(afhe_ivfpq* h, const afhe_ivfpq_query* queries, uint32_t count);
 int afhe_ivfpq_stage3(afhe_ivfpq* h, const afhe_ivfpq_query* queries, uint32_t count);
 

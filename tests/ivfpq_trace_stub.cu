@@ -10,7 +10,7 @@
 
 namespace {
 std::vector<std::string> g_log;
-int64_t g_fused = 1, g_chunk = 0, g_ept = 8, g_slice = 13;
+int64_t g_fused = 1, g_chunk = 0, g_ept = 8, g_slice = 13, g_fmin = 18;
 
 void refs(std::string& s, const afhe_ct_ref* r, uint32_t n) {
     for (uint32_t i = 0; i < n; ++i)
@@ -25,7 +25,7 @@ std::string head(const char* name, uint32_t limbs, bool ks) {
     std::string s = std::string(name) + " " + std::to_string(limbs);
     if (ks)
         s += " fused=" + std::to_string(g_fused) + " chunk=" + std::to_string(g_chunk) + " ept=" + std::to_string(g_ept) +
-             " slice=" + std::to_string(g_slice);
+             " slice=" + std::to_string(g_slice) + " fmin=" + std::to_string(g_fmin);
     return s + " |";
 }
 }  // namespace
@@ -50,6 +50,7 @@ afhe_ctx* trace_ctx_new(uint32_t L, uint32_t n, uint32_t lanes) {
     g_chunk = 0;
     g_ept = 8;
     g_slice = 13;
+    g_fmin = 18;
     return c;
 }
 void trace_ctx_free(afhe_ctx* c) { delete c; }
@@ -61,13 +62,15 @@ int afhe_ctx_set_option(afhe_ctx*, uint32_t option, int64_t value) {
     if (option == AFHE_OPT_CHUNK) g_chunk = value;
     if (option == AFHE_OPT_KS_EPT) g_ept = value;
     if (option == AFHE_OPT_KS_SLICE) g_slice = value;
+    if (option == AFHE_OPT_FUSED_MIN) g_fmin = value;
     return AFHE_OK;
 }
 int afhe_ctx_get_option(afhe_ctx*, uint32_t option, int64_t* value) {
     *value = option == AFHE_OPT_KS_FUSED ? g_fused
              : option == AFHE_OPT_KS_EPT ? g_ept
              : option == AFHE_OPT_KS_SLICE ? g_slice
-                                           : g_chunk;
+             : option == AFHE_OPT_FUSED_MIN ? g_fmin
+                                            : g_chunk;
     return AFHE_OK;
 }
 int afhe_eval_add_batch(afhe_ctx*, const afhe_ct_ref* a, const afhe_ct_ref* b, const afhe_ct_ref* d, uint32_t n,

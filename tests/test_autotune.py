@@ -34,3 +34,38 @@ def test_cache_round_trip(tmp_path):
     assert A.load_full(path, 296) == (ch, ntt)
     assert A.load(path, 128) is None            # tuned for another batch size
     assert A.load(str(tmp_path / "absent.json"), 296) is None
+
+
+def test_fused_crossover_picks_the_count_from_which_the_one_kernel_path_wins(monkeypatch):
+    """fused_crossover: the smallest tried count from which the one-kernel key
+    switch is at least as fast as the multi-kernel pipeline at every larger
+    count; the context's options come back as they were."""
+    from anns_fhe_b200 import _lib as L
+
+    class Ctx:
+        def __init__(self):
+            self.o = {L.OPT_FUSED_MIN: 18, L.OPT_KS_FUSED: 1}
+
+        def get_option(self, k):
+            return self.o[k]
+
+        def set_option(self, k, v):
+            self.o[k] = v
+
+    def times(one, multi):
+        def t(ctx, level, count, reps=3):
+            return (one if ctx.o[L.OPT_KS_FUSED] else multi)[count]
+        return t
+    ctx = Ctx()
+    one = {1: 9.0, 2: 5.0, 4: 3.0, 8: 2.0, 16: 1.0, 32: 0.6, 64: 0.5, 128: 0.4}
+    multi = {1: 4.0, 2: 3.0, 4: 2.5, 8: 2.2, 16: 2.0, 32: 2.0, 64: 2.0, 128: 2.0}
+    monkeypatch.setattr(A, "time_rotations", times(one, multi))
+    assert A.fused_crossover(ctx, 3, 256) == 8
+    assert ctx.o == {L.OPT_FUSED_MIN: 18, L.OPT_KS_FUSED: 1}
+    # a count where the one-kernel path loses again above a win does not count
+    one[32] = 2.5
+    assert A.fused_crossover(ctx, 3, 256) == 64
+    # never faster within the lanes: beyond the largest count tried
+    monkeypatch.setattr(A, "time_rotations", times({c: 9.0 for c in one}, multi))
+    assert A.fused_crossover(ctx, 3, 16) == 32
+    assert A.fused_crossover(ctx, 3, 1) == 2

@@ -70,7 +70,8 @@ class FakeLib:
         s = f"{name} {limbs}"
         if ks:
             s += (f" fused={self.ctx.opts[L.OPT_KS_FUSED]} chunk={self.ctx.opts[L.OPT_CHUNK]}"
-                  f" ept={self.ctx.opts[L.OPT_KS_EPT]} slice={self.ctx.opts[L.OPT_KS_SLICE]}")
+                  f" ept={self.ctx.opts[L.OPT_KS_EPT]} slice={self.ctx.opts[L.OPT_KS_SLICE]}"
+                  f" fmin={self.ctx.opts[L.OPT_FUSED_MIN]}")
         return s + " |"
 
     def afhe_eval_add_batch(self, h, a, b, d, n, limbs):
@@ -112,7 +113,7 @@ class FakeCtx:
     def __init__(self, lanes):
         self.h = None
         self.max_batch = lanes
-        self.opts = {L.OPT_KS_FUSED: 1, L.OPT_CHUNK: 0, L.OPT_KS_EPT: 8, L.OPT_KS_SLICE: 13}
+        self.opts = {L.OPT_KS_FUSED: 1, L.OPT_CHUNK: 0, L.OPT_KS_EPT: 8, L.OPT_KS_SLICE: 13, L.OPT_FUSED_MIN: 18}
 
     def set_option(self, option, value):
         self.opts[option] = value
@@ -122,8 +123,8 @@ class FakeCtx:
 
 
 class Choice:
-    def __init__(self, fused, chunk, ept=8, slice=13):
-        self.fused, self.chunk, self.ept, self.slice = fused, chunk, ept, slice
+    def __init__(self, fused, chunk, ept=8, slice=13, fused_min=0):
+        self.fused, self.chunk, self.ept, self.slice, self.fused_min = fused, chunk, ept, slice, fused_min
 
 
 def build_manager(rng, *, D, n_list, slots, L_top, lanes, compaction, eval_level, levels, tuning, ctx_lanes):
@@ -195,7 +196,7 @@ def run_native(trace, m, recs, L_top, n, ctx_lanes, stage):
 
 CASES = {
     "reference_mixed_levels": dict(D=8, n_list=4, slots=64, L_top=6, lanes=3, compaction="reference",
-                                   eval_level=None, levels=[6, 5, 4], tuning={6: (1, 2, 16), 5: (0, 3), 4: (1, 1),
+                                   eval_level=None, levels=[6, 5, 4], tuning={6: (1, 2, 16, 13, 3), 5: (0, 3), 4: (1, 1),
                                                                              3: (0, 2), 2: (1, 3, 16)}),
     "reference_one_lane": dict(D=8, n_list=5, slots=64, L_top=5, lanes=1, compaction="reference", eval_level=None,
                                levels=[5], tuning={}),
@@ -220,7 +221,7 @@ def test_native_driver_issues_the_python_drivers_operators(trace, case, stage):
         m.stage3_fine(recs)
     want = py.log
     assert want, "the Python driver issued nothing"
-    m.ctx.opts = {L.OPT_KS_FUSED: 1, L.OPT_CHUNK: 0, L.OPT_KS_EPT: 8, L.OPT_KS_SLICE: 13}
+    m.ctx.opts = {L.OPT_KS_FUSED: 1, L.OPT_CHUNK: 0, L.OPT_KS_EPT: 8, L.OPT_KS_SLICE: 13, L.OPT_FUSED_MIN: 18}
     got = run_native(trace, m, recs, kw["L_top"], 2 * kw["slots"], ctx_lanes, stage)
     for i, (a, b) in enumerate(zip(got, want)):
         assert a == b, f"call {i} differs:\n native {a[:300]}\n python {b[:300]}"
