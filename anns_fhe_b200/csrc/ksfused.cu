@@ -94,26 +94,21 @@ __device__ __forceinline__ void digit_range(const OpTabs& t, uint32_t j, uint32_
     size = (j == t.parts - 1) ? t.sizeQl - start : t.alpha;
 }
 
-// The top LOGCL + X butterfly stages of a forward NTT, across the cluster.
-// The slice of CTA r is split into 2^X chunks of CH = QN / 2^X values; the
-// VC = CL 2^X elements x = k CH + j (k < VC: chunk k & (2^X - 1) of CTA
-// k >> X) form a column of VC values, transformed by the stages of bits
-// LOGN - 1 .. LOGQ - X (block b of stage s uses tw[2^s + b]). CTA r takes the
-// columns j in [r CH / CL, (r + 1) CH / CL). With X = 1 the slice's top bit
-// joins the cluster pass, and the CTA's own rounds cover the low LOGQ - 1
-// bits in whole radix-8 rounds.
-template <int LOGQ, int LOGCL, int NB, int E, int X = 0>
+// The top LOGCL butterfly stages of a forward NTT, across the cluster: the
+// CL elements x = k QN + j (k < CL) form a column of CL values, transformed
+// by the stages of bits LOGN - 1 .. LOGQ (block b of stage s uses tw[2^s + b]).
+// CTA r takes the columns j in [r QN / CL, (r + 1) QN / CL).
+template <int LOGQ, int LOGCL, int NB, int E>
 __device__ __forceinline__ void cross_fwd(u64* const (&bufs)[NB], const ulonglong2* __restrict__ tw,
                                           const PrimeConst& pc) {
     using G = Geo<LOGQ, LOGCL, E>;
-    constexpr uint32_t CL = G::CL, VC = CL << X, CH = G::QN >> X, PER = CH / CL;
-    constexpr int LV = LOGCL + X;
+    constexpr uint32_t CL = G::CL, PER = G::QN / CL;
     cg::cluster_group cl = cg::this_cluster();
     const uint32_t r = cl.block_rank();
     const u64 q = pc.q, q2 = q << 1;
-    ulonglong2 w[VC - 1];
+    ulonglong2 w[CL - 1];
 #pragma unroll
-    for (uint32_t i = 1; i < VC; ++i) w[i - 1] = __ldg(tw + i);
+    for (uint32_t i = 1; i < CL; ++i) w[i - 1] = __ldg(tw + i);
     u64* rb[NB][CL];
 #pragma unroll
     for (int b = 0; b < NB; ++b)
@@ -123,12 +118,12 @@ __device__ __forceinline__ void cross_fwd(u64* const (&bufs)[NB], const ulonglon
         const uint32_t e = padix(r * PER + jj);
 #pragma unroll
         for (int b = 0; b < NB; ++b) {
-            u64 v[VC];
+            u64 v[CL];
 #pragma unroll
-            for (uint32_t k = 0; k < VC; ++k) v[k] = rb[b][k >> X][e + padix((k & ((1u << X) - 1)) * CH)];
+            for (uint32_t k = 0; k < CL; ++k) v[k] = rb[b][k][e];
 #pragma unroll
-            for (int s = 0; s < LV; ++s) {
-                const uint32_t m = 1u << s, t = VC >> (s + 1);
+            for (int s = 0; s < LOGCL; ++s) {
+                const uint32_t m = 1u << s, t = CL >> (s + 1);
 #pragma unroll
                 for (uint32_t blk = 0; blk < m; ++blk)
 #pragma unroll
@@ -136,26 +131,24 @@ __device__ __forceinline__ void cross_fwd(u64* const (&bufs)[NB], const ulonglon
                         ct_bfly(v[blk * 2 * t + i], v[blk * 2 * t + i + t], w[m + blk - 1], q, q2);
             }
 #pragma unroll
-            for (uint32_t k = 0; k < VC; ++k) rb[b][k >> X][e + padix((k & ((1u << X) - 1)) * CH)] = v[k];
+            for (uint32_t k = 0; k < CL; ++k) rb[b][k][e] = v[k];
         }
     }
 }
 
-// The top LOGCL + X stages of an inverse NTT (Gentleman-Sande, bits
-// LOGQ - X .. LOGN - 1; columns as in cross_fwd), the last one with N^-1
-// folded in; outputs canonical.
-template <int LOGQ, int LOGCL, int NB, int E, int X = 0>
+// The top LOGCL stages of an inverse NTT (Gentleman-Sande, bits LOGQ ..
+// LOGN - 1), the last one with N^-1 folded in; outputs canonical.
+template <int LOGQ, int LOGCL, int NB, int E>
 __device__ __forceinline__ void cross_inv(u64* const (&bufs)[NB], const ulonglong2* __restrict__ itw,
                                           const PrimeConst& pc) {
     using G = Geo<LOGQ, LOGCL, E>;
-    constexpr uint32_t CL = G::CL, VC = CL << X, CH = G::QN >> X, PER = CH / CL;
-    constexpr int LV = LOGCL + X;
+    constexpr uint32_t CL = G::CL, PER = G::QN / CL;
     cg::cluster_group cl = cg::this_cluster();
     const uint32_t r = cl.block_rank();
     const u64 q = pc.q, q2 = q << 1;
-    ulonglong2 w[VC > 2 ? VC - 1 : 1];
+    ulonglong2 w[CL > 2 ? CL - 1 : 1];
 #pragma unroll
-    for (uint32_t i = 2; i < VC; ++i) w[i - 1] = __ldg(itw + i);   // itw[1] enters through pc.w1ninv
+    for (uint32_t i = 2; i < CL; ++i) w[i - 1] = __ldg(itw + i);   // itw[1] enters through pc.w1ninv
     u64* rb[NB][CL];
 #pragma unroll
     for (int b = 0; b < NB; ++b)
@@ -165,12 +158,12 @@ __device__ __forceinline__ void cross_inv(u64* const (&bufs)[NB], const ulonglon
         const uint32_t e = padix(r * PER + jj);
 #pragma unroll
         for (int b = 0; b < NB; ++b) {
-            u64 v[VC];
+            u64 v[CL];
 #pragma unroll
-            for (uint32_t k = 0; k < VC; ++k) v[k] = rb[b][k >> X][e + padix((k & ((1u << X) - 1)) * CH)];
+            for (uint32_t k = 0; k < CL; ++k) v[k] = rb[b][k][e];
 #pragma unroll
-            for (int s = LV - 1; s >= 0; --s) {
-                const uint32_t m = 1u << s, t = VC >> (s + 1);
+            for (int s = LOGCL - 1; s >= 0; --s) {
+                const uint32_t m = 1u << s, t = CL >> (s + 1);
                 if (s == 0) {
 #pragma unroll
                     for (uint32_t i = 0; i < t; ++i) gs_bfly_last(v[i], v[i + t], pc, q2);
@@ -183,16 +176,10 @@ __device__ __forceinline__ void cross_inv(u64* const (&bufs)[NB], const ulonglon
                 }
             }
 #pragma unroll
-            for (uint32_t k = 0; k < VC; ++k) rb[b][k >> X][e + padix((k & ((1u << X) - 1)) * CH)] = v[k];
+            for (uint32_t k = 0; k < CL; ++k) rb[b][k][e] = v[k];
         }
     }
 }
-
-// A cluster transform folds the slice's top bit into the cross-cluster pass
-// when the slice's bits would leave a lone radix-2 round (13 = 4 x 3 + 1):
-// the CTA's rounds then cover 2^X chunks of LOGQ - X bits each.
-template <int LOGQ, int LOGCL>
-constexpr int fold_bits() { return (LOGCL > 0 && LOGCL < 3 && LOGQ % 3 == 1) ? 1 : 0; }
 
 // Forward NTT of one buffer. On entry this CTA's slice is written (and
 // visible after a CTA barrier); on return the slice holds lazy residues in
@@ -202,28 +189,26 @@ constexpr int fold_bits() { return (LOGCL > 0 && LOGCL < 3 && LOGQ % 3 == 1) ? 1
 template <int LOGQ, int LOGCL, int E>
 __device__ __noinline__ void fwd_ntt(u64* buf, const PrimeTables pt, uint32_t prime, const PrimeConst pc) {
     using G = Geo<LOGQ, LOGCL, E>;
-    constexpr int X = fold_bits<LOGQ, LOGCL>();
     const ulonglong2* tw = pt.tw2 + ((u64)prime << G::LOGN);
     if constexpr (LOGCL > 0) {
         u64* const one[1] = {buf};
         G::sync_all();
-        cross_fwd<LOGQ, LOGCL, 1, E, X>(one, tw, pc);
+        cross_fwd<LOGQ, LOGCL, 1, E>(one, tw, pc);
         G::sync_all();
     }
-    ntt_rounds<false, LOGQ - X, X, false, 0, E>(buf, tw, pc, G::rank() << X, G::LOGN, 0, true);
+    ntt_rounds<false, LOGQ, 0, false, 0, E>(buf, tw, pc, G::rank(), G::LOGN, 0, true);
 }
 
 // Inverse NTT of one buffer; on return the slice holds canonical residues.
 template <int LOGQ, int LOGCL, int E>
 __device__ __noinline__ void inv_ntt(u64* buf, const PrimeTables pt, uint32_t prime, const PrimeConst pc) {
     using G = Geo<LOGQ, LOGCL, E>;
-    constexpr int X = fold_bits<LOGQ, LOGCL>();
     const ulonglong2* itw = pt.itw2 + ((u64)prime << G::LOGN);
-    ntt_rounds<true, LOGQ - X, X, false, 0, E>(buf, itw, pc, G::rank() << X, G::LOGN, 0, LOGCL == 0);
+    ntt_rounds<true, LOGQ, 0, false, 0, E>(buf, itw, pc, G::rank(), G::LOGN, 0, LOGCL == 0);
     if constexpr (LOGCL > 0) {
         u64* const one[1] = {buf};
         G::sync_all();
-        cross_inv<LOGQ, LOGCL, 1, E, X>(one, itw, pc);
+        cross_inv<LOGQ, LOGCL, 1, E>(one, itw, pc);
         G::sync_all();
     }
 }
@@ -232,18 +217,17 @@ __device__ __noinline__ void inv_ntt(u64* buf, const PrimeTables pt, uint32_t pr
 template <bool INV, int LOGQ, int LOGCL, int E>
 __device__ __noinline__ void ntt2(u64* b0, u64* b1, const PrimeTables pt, uint32_t prime, const PrimeConst pc) {
     using G = Geo<LOGQ, LOGCL, E>;
-    constexpr int X = fold_bits<LOGQ, LOGCL>();
     u64* const bufs[2] = {b0, b1};
     const ulonglong2* tw = (INV ? pt.itw2 : pt.tw2) + ((u64)prime << G::LOGN);
     if constexpr (!INV && LOGCL > 0) {
         G::sync_all();
-        cross_fwd<LOGQ, LOGCL, 2, E, X>(bufs, tw, pc);
+        cross_fwd<LOGQ, LOGCL, 2, E>(bufs, tw, pc);
         G::sync_all();
     }
-    ntt_rounds_n<INV, LOGQ - X, X, false, 0, E, 2>(bufs, tw, pc, G::rank() << X, G::LOGN, 0, !INV || LOGCL == 0);
+    ntt_rounds_n<INV, LOGQ, 0, false, 0, E, 2>(bufs, tw, pc, G::rank(), G::LOGN, 0, !INV || LOGCL == 0);
     if constexpr (INV && LOGCL > 0) {
         G::sync_all();
-        cross_inv<LOGQ, LOGCL, 2, E, X>(bufs, tw, pc);
+        cross_inv<LOGQ, LOGCL, 2, E>(bufs, tw, pc);
         G::sync_all();
     }
 }
