@@ -616,6 +616,25 @@ int afhe_host_free(void* p) {
     return AFHE_OK;
 }
 
+int afhe_automorphism_from_map(afhe_ctx* ctx, uint64_t src, uint64_t map_off, uint64_t dst, uint32_t limbs,
+                               uint32_t /*galois_elt*/) {
+    if (!ctx) return fail(nullptr, AFHE_E_ARG, "null context");
+    const u64 n = ctx->n, LN = (u64)limbs * n, pw = ctx->prm.poly_words;
+    if (limbs < 1 || limbs > ctx->L + ctx->K) return fail(ctx, AFHE_E_ARG, "limbs must be in [1, L + K]");
+    if (!range_ok(src, LN, pw) || !range_ok(map_off, n / 2, pw) || !range_ok(dst, LN, pw))
+        return fail(ctx, AFHE_E_RANGE, "automorphism operands out of range");
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, AFHE_E_CUDA, "cudaSetDevice");
+    cudaStream_t st = ctx->st;
+    // map and source staged in scratch first (a gather cannot run in place)
+    CK(cudaMemcpyAsync(ctx->scr, ctx->poly + map_off, (n / 2) * 8, cudaMemcpyDeviceToDevice, st));
+    CK(cudaMemcpyAsync(ctx->scr + n, ctx->poly + src, LN * 8, cudaMemcpyDeviceToDevice, st));
+    ZBases zb{};
+    zb.src = zf_const(ctx->prm.poly_words + n);
+    zb.out = zf_const(dst);
+    CK(launch_automorphism(nullptr, ctx->scr, ctx->poly, n, limbs, 1, zb, st));
+    return AFHE_OK;
+}
+
 int afhe_ntt_plan_count(uint32_t log_n, uint32_t* count) {
     if (!count) return fail(nullptr, AFHE_E_ARG, "null argument");
     *count = (uint32_t)ntt_plan_count((int)log_n);

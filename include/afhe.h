@@ -272,6 +272,13 @@ int afhe_poly_add(afhe_ctx* ctx, uint64_t a, uint64_t b, uint64_t dst, uint32_t 
 int afhe_poly_sub(afhe_ctx* ctx, uint64_t a, uint64_t b, uint64_t dst, uint32_t limbs);
 int afhe_poly_mul_ntt(afhe_ctx* ctx, uint64_t a, uint64_t b, uint64_t dst, uint32_t limbs);
 int afhe_automorphism(afhe_ctx* ctx, uint64_t src, uint32_t galois_elt, uint64_t dst, uint32_t limbs);
+/* FHEHostDriver::automorphism with its own arguments (fhe_host_driver.h:82):
+ * the permutation is read from poly_gmem at auto_map_offset (N 32-bit source
+ * indices, two per word, as initialize_context_from_directory stores them,
+ * fhe_host_driver.cpp:141-154); galois_elt is not used, as in the reference
+ * (OP 6, fhe_accel_top.cpp:272-281). In place is allowed. */
+int afhe_automorphism_from_map(afhe_ctx* ctx, uint64_t src, uint64_t auto_map_offset, uint64_t dst, uint32_t limbs,
+                               uint32_t galois_elt);
 /* rescale c0 and c1 from `limbs` to `limbs - 1` (fhe_host_driver.cpp:362-365) */
 int afhe_rescale(afhe_ctx* ctx, uint64_t c0_in, uint64_t c1_in, uint64_t c0_out, uint64_t c1_out,
                  uint32_t limbs);
