@@ -21,16 +21,20 @@ import time
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 # DRAM traffic and integer-pipe use of the key switch from ncu captures of the
-# current kernels (`--set full`, clocks not locked), per (N, l, K): the
+# current kernels (`--set full`, clocks not locked), per (N, l, K, slice): the
 # traffic of one launch sequence per ciphertext (its scratch and I/O grow with
 # the ciphertexts), the key's bytes read once, the kernel, and the busiest
 # integer pipe's utilisation. The captures are summarised under profiles/.
 KS_CAPTURES: dict = {
-    (8192, 3, 1): {"kernel": "ks_fused_kernel<13, 1>", "ciphertexts": 148, "dram_bytes": 175.3e6,
-                   "pipe": "fmaheavy (IMAD)", "util": 0.580},
-    # clusters of 4 CTAs; 37 clusters ran as two waves (32 resident at once)
-    (32768, 3, 4): {"kernel": "ks_fused_kernel<13, 2, 1>", "ciphertexts": 37, "dram_bytes": 402.9e6,
-                    "pipe": "alu", "util": 0.387},
+    (8192, 3, 1, 13): {"kernel": "ks_fused_kernel<13, 1>", "ciphertexts": 148, "dram_bytes": 175.3e6,
+                       "pipe": "fmaheavy (IMAD)", "util": 0.580},
+    # clusters of 4 CTAs of 2^13-value slices, one per SM; 37 clusters ran as
+    # two waves (33 resident at once)
+    (32768, 3, 4, 13): {"kernel": "ks_fused_kernel<13, 2, 1>", "ciphertexts": 37, "dram_bytes": 402.9e6,
+                        "pipe": "alu", "util": 0.387},
+    # clusters of 8 CTAs of 2^12-value slices, two per SM; 66 = two full waves
+    (32768, 3, 4, 12): {"kernel": "ks_fused_kernel<12, 3, 1, 8>", "ciphertexts": 66, "dram_bytes": 715.8e6,
+                        "pipe": "alu", "util": 0.370},
 }
 
 
@@ -106,9 +110,9 @@ def ks_roofline(params, lanes: int, reps: int = 20, level: int = 0, nbuf: int = 
     bytes_per_call = lanes * 4 * w * 8 + key_bytes
     achieved = bytes_per_call / (ms * 1e-3) / 1e9
     peak, src = load_peaks()
-    cap = KS_CAPTURES.get((n, L, K))
+    cap = KS_CAPTURES.get((n, L, K, slc if n >= 1 << 14 else 13))
     traffic = int_pipe = None
-    if cap and launches == 1 and fused and ept == cap.get("ept", 8) and slc == cap.get("slice", 13):
+    if cap and launches == 1 and fused and ept == cap.get("ept", 8):
         # the capture's per-ciphertext traffic scaled to this launch, the key once
         traffic = (cap["dram_bytes"] - key_bytes) * lanes / cap["ciphertexts"] + key_bytes
         int_pipe = {"pipe": cap["pipe"], "frac": cap["util"], "kernel": cap["kernel"],
