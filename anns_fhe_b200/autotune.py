@@ -76,7 +76,7 @@ TIE = 0.10   # candidates within this fraction of the fastest count as ties
 # Version of the key-switch kernels a cache was tuned against: a cache from
 # other kernels (e.g. before the one-kernel path existed at this ring degree)
 # is tuned again.
-KERNELS = 6
+KERNELS = 7
 
 
 def ntt_plan_count(log_n: int) -> int:
@@ -130,15 +130,21 @@ def time_ntt_plans(ctx: FheContext, polys: int, limbs: int, reps: int = 3) -> di
     return out
 
 
+SHAPE_TIE = 0.03   # 16 values per thread must beat 8 by more than this to be picked
+
+
 def pick(timings: dict) -> tuple:
     """The key of {(fused, chunk[, ept, slice]): us_per_ct} to use: among the
     candidates within TIE of the fastest, the largest chunk (fewest
     launches; a chain's batches are rarely a multiple of the tile, and every
     extra launch costs its tail), then the one-kernel path, then the
-    fastest."""
-    best = min(timings.values())
-    near = [k for k, v in timings.items() if v <= best * (1 + TIE)]
-    return max(near, key=lambda k: (k[1], k[0], -timings[k]))
+    fastest. 16 values per thread counts SHAPE_TIE slower than measured: an
+    isolated rotation batch favours it slightly more than the chain does."""
+    def eff(k):
+        return timings[k] * (1 + SHAPE_TIE) if len(k) > 2 and k[2] != 8 else timings[k]
+    best = min(eff(k) for k in timings)
+    near = [k for k in timings if eff(k) <= best * (1 + TIE)]
+    return max(near, key=lambda k: (k[1], k[0], -eff(k)))
 
 
 def time_rotations(ctx: FheContext, level: int, count: int, reps: int = 3) -> float:

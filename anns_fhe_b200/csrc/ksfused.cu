@@ -38,6 +38,10 @@
 // (staged in shared memory behind a barrier across the whole cluster).
 #include <cooperative_groups.h>
 
+#include <map>
+#include <mutex>
+#include <tuple>
+
 #include "internal.h"
 
 namespace cg = cooperative_groups;
@@ -808,7 +812,8 @@ __global__ void key_prep_kernel(const u64* __restrict__ key, ulonglong2* __restr
 
 }  // namespace
 
-int key_switch_fused_capacity(int log_n, int ept, int slice) {
+namespace {
+int capacity_uncached(int log_n, int ept, int slice) {
     if (slice == 12 && (log_n == 14 || log_n == 15))
         return log_n == 14 ? cluster_capacity<2, 8, 12>() : cluster_capacity<3, 8, 12>();
     if (log_n >= 14 && log_n <= 16) {
@@ -849,14 +854,34 @@ int key_switch_fused_capacity(int log_n, int ept, int slice) {
     return per * sms;
 }
 
+}  // namespace
+
+// The occupancy queries behind the capacity cost tens of microseconds, and
+// the options that consult them are set around every batched operator, so the
+// answers are kept per (device, N, values per thread, slice).
+int key_switch_fused_capacity(int log_n, int ept, int slice) {
+    static std::mutex mu;
+    static std::map<std::tuple<int, int, int, int>, int> cache;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    const auto key = std::make_tuple(dev, log_n, ept, slice);
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = cache.find(key);
+        if (it != cache.end()) return it->second;
+    }
+    const int cap = capacity_uncached(log_n, ept, slice);
+    std::lock_guard<std::mutex> lock(mu);
+    cache[key] = cap;
+    return cap;
+}
+
 bool key_switch_fused_supported(int log_n) {
     if (log_n >= 10 && log_n <= 13) return true;
-    switch (log_n) {
-    case 14: return cluster_capacity<1>() > 0;
-    case 15: return cluster_capacity<2>() > 0;
-    case 16: return cluster_capacity<3>() > 0;
-    default: return false;
-    }
+    return log_n <= 16 && key_switch_fused_capacity(log_n, 8, 13) > 0;
 }
 
 size_t ks_fused_scratch_words(uint32_t n, uint32_t sizeQl, uint32_t K) { return (size_t)n * (sizeQl + 2 * K); }

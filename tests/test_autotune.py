@@ -22,6 +22,10 @@ def test_pick_prefers_fastest_then_larger_chunk_then_fused():
     assert A.pick({(True, 148): 0.78, (True, 296): 0.84, (False, 296): 1.49}) == (True, 296)
     # outside it, speed wins
     assert A.pick({(True, 148): 0.70, (True, 296): 0.84}) == (True, 148)
+    # 16 values per thread only where it wins by more than SHAPE_TIE; slices by speed
+    assert A.pick({(True, 296, 8, 13): 1.00, (True, 296, 16, 13): 0.98}) == (True, 296, 8, 13)
+    assert A.pick({(True, 296, 8, 13): 1.00, (True, 296, 16, 13): 0.95}) == (True, 296, 16, 13)
+    assert A.pick({(True, 256, 8, 13): 1.00, (True, 256, 8, 12): 0.98}) == (True, 256, 8, 12)
 
 
 def test_cache_round_trip(tmp_path):
