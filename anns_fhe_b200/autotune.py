@@ -76,7 +76,7 @@ TIE = 0.10   # candidates within this fraction of the fastest count as ties
 # Version of the key-switch kernels a cache was tuned against: a cache from
 # other kernels (e.g. before the one-kernel path existed at this ring degree)
 # is tuned again.
-KERNELS = 7
+KERNELS = 8
 
 
 def ntt_plan_count(log_n: int) -> int:
@@ -217,7 +217,7 @@ def tune(params: CkksParams, levels, lanes: int, device: int = 0, verbose: bool 
         if fused_ok and params.log_n in (14, 15):
             try:
                 ctx.set_option(L.OPT_KS_SLICE, 12)
-                shapes.insert(2, (True, 8, 12))
+                shapes[2:2] = [(True, 8, 12), (True, 16, 12)]
             except L.AfheError:
                 pass                     # two CTAs per SM cannot be placed in clusters here
             ctx.set_option(L.OPT_KS_SLICE, 13)

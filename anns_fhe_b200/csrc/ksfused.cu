@@ -185,6 +185,12 @@ __device__ __forceinline__ void cross_inv(u64* const (&bufs)[NB], const ulonglon
     }
 }
 
+// Radix of a CTA's own transform rounds: 2^4 where 16 values per thread
+// divide the slice's bits into whole rounds (2^12-value slices: three rounds
+// instead of four), else 2^3.
+template <int LOGQ, int E>
+constexpr int round_bits() { return (E == 16 && LOGQ % 4 == 0) ? 4 : 3; }
+
 // Forward NTT of one buffer. On entry this CTA's slice is written (and
 // visible after a CTA barrier); on return the slice holds lazy residues in
 // [0, 4q). Not inlined: each transform gets its own register allocation
@@ -200,7 +206,7 @@ __device__ __noinline__ void fwd_ntt(u64* buf, const PrimeTables pt, uint32_t pr
         cross_fwd<LOGQ, LOGCL, 1, E>(one, tw, pc);
         G::sync_all();
     }
-    ntt_rounds<false, LOGQ, 0, false, 0, E>(buf, tw, pc, G::rank(), G::LOGN, 0, true);
+    ntt_rounds<false, LOGQ, 0, false, 0, E, round_bits<LOGQ, E>()>(buf, tw, pc, G::rank(), G::LOGN, 0, true);
 }
 
 // Inverse NTT of one buffer; on return the slice holds canonical residues.
@@ -208,7 +214,7 @@ template <int LOGQ, int LOGCL, int E>
 __device__ __noinline__ void inv_ntt(u64* buf, const PrimeTables pt, uint32_t prime, const PrimeConst pc) {
     using G = Geo<LOGQ, LOGCL, E>;
     const ulonglong2* itw = pt.itw2 + ((u64)prime << G::LOGN);
-    ntt_rounds<true, LOGQ, 0, false, 0, E>(buf, itw, pc, G::rank(), G::LOGN, 0, LOGCL == 0);
+    ntt_rounds<true, LOGQ, 0, false, 0, E, round_bits<LOGQ, E>()>(buf, itw, pc, G::rank(), G::LOGN, 0, LOGCL == 0);
     if constexpr (LOGCL > 0) {
         u64* const one[1] = {buf};
         G::sync_all();
@@ -228,7 +234,8 @@ __device__ __noinline__ void ntt2(u64* b0, u64* b1, const PrimeTables pt, uint32
         cross_fwd<LOGQ, LOGCL, 2, E>(bufs, tw, pc);
         G::sync_all();
     }
-    ntt_rounds_n<INV, LOGQ, 0, false, 0, E, 2>(bufs, tw, pc, G::rank(), G::LOGN, 0, !INV || LOGCL == 0);
+    ntt_rounds_n<INV, LOGQ, 0, false, 0, E, 2, round_bits<LOGQ, E>()>(bufs, tw, pc, G::rank(), G::LOGN, 0,
+                                                                       !INV || LOGCL == 0);
     if constexpr (INV && LOGCL > 0) {
         G::sync_all();
         cross_inv<LOGQ, LOGCL, 2, E>(bufs, tw, pc);
@@ -758,9 +765,12 @@ cudaError_t launch_fused(const KsFusedArgs& a, uint32_t nz, cudaStream_t st, int
     return a.prep ? launch_fused_v<LOGQ, LOGCL, true, 8>(a, nz, st) : launch_fused_v<LOGQ, LOGCL, false, 8>(a, nz, st);
 }
 
-// 2^12-value slices (clusters of 4 or 8 CTAs, two CTAs per SM), 8 values per thread
+// 2^12-value slices (clusters of 4 or 8 CTAs, two CTAs per SM): 8 values per
+// thread (512 threads, radix-8 rounds) or 16 (256 threads, radix-16 rounds)
 template <int LOGCL>
-cudaError_t launch_slice12(const KsFusedArgs& a, uint32_t nz, cudaStream_t st) {
+cudaError_t launch_slice12(const KsFusedArgs& a, uint32_t nz, cudaStream_t st, int ept) {
+    if (ept == 16)
+        return a.prep ? launch_fused_v<12, LOGCL, true, 16>(a, nz, st) : launch_fused_v<12, LOGCL, false, 16>(a, nz, st);
     return a.prep ? launch_fused_v<12, LOGCL, true, 8>(a, nz, st) : launch_fused_v<12, LOGCL, false, 8>(a, nz, st);
 }
 
@@ -814,8 +824,10 @@ __global__ void key_prep_kernel(const u64* __restrict__ key, ulonglong2* __restr
 
 namespace {
 int capacity_uncached(int log_n, int ept, int slice) {
-    if (slice == 12 && (log_n == 14 || log_n == 15))
+    if (slice == 12 && (log_n == 14 || log_n == 15)) {
+        if (ept == 16) return log_n == 14 ? cluster_capacity<2, 16, 12>() : cluster_capacity<3, 16, 12>();
         return log_n == 14 ? cluster_capacity<2, 8, 12>() : cluster_capacity<3, 8, 12>();
+    }
     if (log_n >= 14 && log_n <= 16) {
         if (ept == 16)
             return log_n == 14 ? cluster_capacity<1, 16>() : log_n == 15 ? cluster_capacity<2, 16>()
@@ -929,8 +941,8 @@ cudaError_t launch_key_switch_fused(int log_n, const OpTabs& t, uint32_t sizeQl,
     case 11: return launch_fused<11, 0>(a, nz, st, ept);
     case 12: return launch_fused<12, 0>(a, nz, st, ept);
     case 13: return launch_fused<13, 0>(a, nz, st, ept);
-    case 14: return slice == 12 ? launch_slice12<2>(a, nz, st) : launch_fused<kLogQ, 1>(a, nz, st, ept);
-    case 15: return slice == 12 ? launch_slice12<3>(a, nz, st) : launch_fused<kLogQ, 2>(a, nz, st, ept);
+    case 14: return slice == 12 ? launch_slice12<2>(a, nz, st, ept) : launch_fused<kLogQ, 1>(a, nz, st, ept);
+    case 15: return slice == 12 ? launch_slice12<3>(a, nz, st, ept) : launch_fused<kLogQ, 2>(a, nz, st, ept);
     case 16: return launch_fused<kLogQ, 3>(a, nz, st, ept);
     default: return cudaErrorInvalidValue;
     }

@@ -241,30 +241,32 @@ struct NttRound {
 
 // All rounds of a pass over NB tiles in shared memory (same prime), each
 // round followed by a barrier: forward takes bits high to low, inverse low to
-// high, in rounds of three (the remainder round is smaller).
-template <bool INV, int P, int LOGC, bool COL, int RD, int EPT, int NB>
+// high, in rounds of R bits (radix 2^R: R = 3, or 4 with 16 values per
+// thread; the remainder round is smaller).
+template <bool INV, int P, int LOGC, bool COL, int RD, int EPT, int NB, int R = 3>
 __device__ __forceinline__ void ntt_rounds_n(u64* const (&sms)[NB], const ulonglong2* tw, const PrimeConst& pc,
                                              uint32_t tile0, int log_n, int lo_bit, bool last_pass) {
-    constexpr int NR = (P + 2) / 3;
+    static_assert((EPT >> R) >= 1, "a round needs 2^R values per thread");
+    constexpr int NR = (P + R - 1) / R;
     if constexpr (RD < NR) {
-        constexpr int HI = P - 3 * RD;                       // forward: bits [.., HI)
-        constexpr int KF = HI >= 3 ? 3 : HI;
+        constexpr int HI = P - R * RD;                       // forward: bits [.., HI)
+        constexpr int KF = HI >= R ? R : HI;
         constexpr int RBF = HI - KF;
-        constexpr int RBI = 3 * RD;                          // inverse: bits [RBI, ..)
-        constexpr int KI = (P - RBI) >= 3 ? 3 : (P - RBI);
+        constexpr int RBI = R * RD;                          // inverse: bits [RBI, ..)
+        constexpr int KI = (P - RBI) >= R ? R : (P - RBI);
         NttRound<INV, P, LOGC, COL, INV ? RBI : RBF, INV ? KI : KF, EPT>::template run_n<NB>(
             sms, tw, pc, tile0, log_n, lo_bit, last_pass);
         __syncthreads();
-        ntt_rounds_n<INV, P, LOGC, COL, RD + 1, EPT, NB>(sms, tw, pc, tile0, log_n, lo_bit, last_pass);
+        ntt_rounds_n<INV, P, LOGC, COL, RD + 1, EPT, NB, R>(sms, tw, pc, tile0, log_n, lo_bit, last_pass);
     }
 }
 
 // One tile.
-template <bool INV, int P, int LOGC, bool COL, int RD, int EPT = 8>
+template <bool INV, int P, int LOGC, bool COL, int RD, int EPT = 8, int R = 3>
 __device__ __forceinline__ void ntt_rounds(u64* sm, const ulonglong2* tw, const PrimeConst& pc, uint32_t tile0,
                                            int log_n, int lo_bit, bool last_pass) {
     u64* const one[1] = {sm};
-    ntt_rounds_n<INV, P, LOGC, COL, RD, EPT, 1>(one, tw, pc, tile0, log_n, lo_bit, last_pass);
+    ntt_rounds_n<INV, P, LOGC, COL, RD, EPT, 1, R>(one, tw, pc, tile0, log_n, lo_bit, last_pass);
 }
 
 // One pass over 2^(P + LOGC)-word tiles: stage the tile in shared memory

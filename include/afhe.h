@@ -200,8 +200,9 @@ int afhe_copy_poly(afhe_ctx* ctx, uint64_t dst_offset, uint64_t src_offset, uint
 /*   AFHE_OPT_KS_SLICE  log2 of the slice each CTA of a cluster holds in the
  *                      one-kernel key switch at N = 2^14 and 2^15: 13 (the
  *                      default: clusters of N / 2^13 CTAs of 1024 threads, one
- *                      per SM) or 12 (clusters of N / 2^12 CTAs of 512 threads,
- *                      two per SM; 8 values per thread). Ignored at other N.
+ *                      per SM) or 12 (clusters of N / 2^12 CTAs, two per SM:
+ *                      512 threads with 8 values each, or 256 threads with 16
+ *                      values each in radix-16 rounds). Ignored at other N.
  *                      Same residues. */
 #define AFHE_OPT_KS_SLICE 6u
 int afhe_ctx_set_option(afhe_ctx* ctx, uint32_t option, int64_t value);

@@ -2,7 +2,8 @@
 per thread (AFHE_OPT_KS_EPT), at every ring degree it runs at: one CTA per
 ciphertext (N = 2^10, 2^13) and clusters of 2, 4 and 8 CTAs (N = 2^14, 2^15,
 2^16); and with 2^12-value slices, clusters of 4 and 8 CTAs two to an SM
-(AFHE_OPT_KS_SLICE 12, N = 2^14 and 2^15). The workload is a rotate-and-sum chain over ciphertexts at mixed
+(AFHE_OPT_KS_SLICE 12, N = 2^14 and 2^15), at 8 values per thread (radix-8
+rounds) and 16 (256 threads, radix-16 rounds). The workload is a rotate-and-sum chain over ciphertexts at mixed
 levels in one launch per step (afhe_eval_rotate_accumulate_levels_batch),
 then a rescale; the 8-value kernel is checked against the oracle by
 test_gpu_ks_paths.py and test_gpu_primitives_n65536.py."""
@@ -34,7 +35,7 @@ def test_values_per_thread_same_residues(shape):
             pytest.skip("the one-kernel key switch does not run on this GPU at this ring degree")
         ksb.ctx.set_option(L.OPT_FUSED_MIN, 1)
         out = {}
-        variants = [(8, 13), (16, 13)] + ([(8, 12)] if log_n in (14, 15) else [])
+        variants = [(8, 13), (16, 13)] + ([(8, 12), (16, 12)] if log_n in (14, 15) else [])
         for ept, sl in variants:
             ksb.ctx.set_option(L.OPT_KS_EPT, ept)
             ksb.ctx.set_option(L.OPT_KS_SLICE, sl)
