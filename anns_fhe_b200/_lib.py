@@ -165,6 +165,7 @@ SIGNATURES = {
     "afhe_ntt_set_plan": (C.c_int, [u32, u32]),
     "afhe_ntt_get_plan": (C.c_int, [u32, P32]),
     "afhe_automorphism_from_map": (C.c_int, [CTX, u64, u64, u64, u32, u32]),
+    "afhe_automorphism_batch": (C.c_int, [CTX, P64, P32, P64, u32, u32]),
     "afhe_encode_batch": (C.c_int, [CTX, C.POINTER(C.c_double), u32, u32, C.c_double, u32, P64]),
     "afhe_pq_create": (C.c_int, [CTX, C.POINTER(PqIndex), C.POINTER(C.c_void_p)]),
     "afhe_pq_destroy": (C.c_int, [C.c_void_p]),

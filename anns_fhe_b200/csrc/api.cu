@@ -455,6 +455,7 @@ int afhe_ctx_destroy(afhe_ctx* ctx) {
     for (DevPrimeSet* s : {&ctx->nat, &ctx->ld}) { fr(s->pc); fr(s->tw); fr(s->itw); fr(s->tw2); fr(s->itw2); }
     fr(ctx->ld_crt); fr(ctx->ld_crt_sh); fr(ctx->ld_mod);
     for (auto& kv : ctx->rot) fr(kv.second.map);
+    for (auto& kv : ctx->auto_maps) fr(kv.second);
     free_key_preps(ctx);
     fr(ctx->ring.dev);
     if (ctx->ring.host) cudaFreeHost(ctx->ring.host);

@@ -716,6 +716,62 @@ int afhe_eval_add_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const afhe_ct_ref* 
     });
 }
 
+int afhe_automorphism_batch(afhe_ctx* ctx, const uint64_t* src, const uint32_t* galois, const uint64_t* dst,
+                            uint32_t count, uint32_t limbs) {
+    if (!ctx || (count && (!src || !galois || !dst))) return fail(ctx, AFHE_E_ARG, "null argument");
+    int rc;
+    if ((rc = check_limbs_ext(ctx, limbs))) return rc;
+    const u64 w = (u64)limbs * ctx->n;
+    std::vector<std::pair<u64, int>> ends;    // interval ends: sources (+1 / -1) and destinations (+2 / -2)
+    for (uint32_t i = 0; i < count; ++i) {
+        if ((rc = check_poly(ctx, src[i], limbs)) || (rc = check_poly(ctx, dst[i], limbs))) return rc;
+        if ((galois[i] & 1u) == 0 || galois[i] >= 2 * ctx->n)
+            return fail(ctx, AFHE_E_ARG, "galois element must be odd and < 2N");
+        ends.push_back({src[i], 1});
+        ends.push_back({src[i] + w, -1});
+        ends.push_back({dst[i], 2});
+        ends.push_back({dst[i] + w, -2});
+    }
+    // a gather cannot run in place: no destination may overlap any source
+    std::sort(ends.begin(), ends.end());
+    int open_src = 0, open_dst = 0;
+    for (const auto& e : ends) {
+        if (e.second == 1) ++open_src;
+        else if (e.second == -1) --open_src;
+        else if (e.second == 2) ++open_dst;
+        else --open_dst;
+        if (open_src > 0 && open_dst > 0) return fail(ctx, AFHE_E_ARG, "a destination overlaps a source");
+    }
+    for (uint32_t i = 0; i < count; ++i)
+        if (!ctx->auto_maps.count(galois[i])) {
+            std::vector<uint32_t> map(ctx->n);
+            automorphism_map(ctx->log_n, galois[i], map.data());
+            uint32_t* d = nullptr;
+            CK(cudaMalloc(&d, (size_t)ctx->n * sizeof(uint32_t)));
+            cudaError_t e = cudaMemcpy(d, map.data(), (size_t)ctx->n * sizeof(uint32_t), cudaMemcpyHostToDevice);
+            if (e != cudaSuccess) {
+                cudaFree(d);
+                return cuda_fail(ctx, e, "automorphism map upload");
+            }
+            ctx->auto_maps[galois[i]] = d;
+        }
+    return for_chunks(ctx, count, [&](uint32_t s, uint32_t m) {
+        Offs S(m), D(m), M(m);
+        for (uint32_t z = 0; z < m; ++z) {
+            S[z] = src[s + z];
+            D[z] = dst[s + z];
+            M[z] = (u64)(uintptr_t)ctx->auto_maps.at(galois[s + z]);
+        }
+        ZBases zb{};
+        ZField maps;
+        ZF(zb.src, S);
+        ZF(zb.out, D);
+        ZF(maps, M);
+        CK(launch_automorphism_z(maps, ctx->poly, ctx->n, limbs, m, zb, ctx->st));
+        return (int)AFHE_OK;
+    });
+}
+
 int afhe_eval_copy_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const afhe_ct_ref* d, uint32_t count, uint32_t limbs) {
     if (!ctx || (count && (!a || !d))) return fail(ctx, AFHE_E_ARG, "null argument");
     int rc;

@@ -129,6 +129,8 @@ struct afhe_ctx {
     afhe::u64 relin_off = 0;
     ulonglong2* relin_prep = nullptr;
     std::map<int32_t, afhe::RotKey> rot;
+    // device automorphism maps by Galois element (afhe_automorphism_batch)
+    std::map<uint32_t, uint32_t*> auto_maps;
 
     // device address of the static working array of afhe_key_switch_noalloc
     // on this context's device, looked up when the context is created (null
@@ -160,6 +162,9 @@ cudaError_t launch_tensor(const PrimeConst* pc, u64* arena, uint32_t n, uint32_t
 // out[l][i] = a[l][map[i]]; map as u32[N] (device) or packed pairs in u64.
 cudaError_t launch_automorphism(const uint32_t* map32, const u64* map64, u64* arena, uint32_t n, uint32_t limbs,
                                 uint32_t nz, const ZBases& zb, cudaStream_t st);
+// out_z = in_z through permutation maps.at(z) (a device address per polynomial)
+cudaError_t launch_automorphism_z(const ZField& maps, u64* arena, uint32_t n, uint32_t limbs, uint32_t nz,
+                                  const ZBases& zb, cudaStream_t st);
 
 // Plain (I)NTT of `limbs` limbs laid out contiguously (limb i at +i*N), table
 // index prime0 + i. src arena -> dst arena, per-z offsets zb.src / zb.out.

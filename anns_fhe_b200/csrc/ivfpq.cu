@@ -18,8 +18,9 @@
 //             -k in one key switch, sum
 //   stage 3   per candidate batch: ct_dim - pt_batch, square, rescale, tree
 //             sum with rotations B, 2B, .., B D/2, mask the batch's slots,
-//             rescale, place it at its slot offset (eval_rotate's steps, or
-//             one key switch per batch when packed), accumulate into the
+//             rescale, place it at its slot offset (eval_rotate's steps; when
+//             packed, the mask itself is moved to the batch's row, since the
+//             tree sum leaves the sums in every row), accumulate into the
 //             query's result ciphertext
 //
 // Plaintexts, masks and working ciphertexts stay resident in poly_gmem at the
@@ -214,9 +215,9 @@ int stage1_packed(afhe_ivfpq* h, const afhe_ivfpq_query* q, const std::vector<ui
         Cts diff(m), sq(m), sel(m), in(m);
         std::vector<u64> pts(m), stride(m, h->masks[Ll][0]);
         for (size_t j = 0; j < m; ++j) {
-            diff[j] = h->work[3 * j];
-            sq[j] = h->work[3 * j + 1];
-            sel[j] = h->work[3 * j + 2];
+            diff[j] = h->work[4 * j];
+            sq[j] = h->work[4 * j + 1];
+            sel[j] = h->work[4 * j + 2];
             in[j] = q[items[c0 + j].first].ct_query;
             pts[j] = h->centroid_cts[items[c0 + j].second];
         }
@@ -245,8 +246,8 @@ int stage1_reference(afhe_ivfpq* h, const afhe_ivfpq_query* q, const std::vector
         Cts diff(m), sq(m), in(m);
         std::vector<u64> pts(m, h->centroid_cts[0]);
         for (size_t j = 0; j < m; ++j) {
-            diff[j] = h->work[3 * j];
-            sq[j] = h->work[3 * j + 1];
+            diff[j] = h->work[4 * j];
+            sq[j] = h->work[4 * j + 1];
             in[j] = q[idx[c0 + j]].ct_query;
         }
         RC(sub_plain(h, in, pts, diff, Ll));
@@ -295,9 +296,9 @@ int stage3_items(afhe_ivfpq* h, const afhe_ivfpq_query* q, const std::vector<Ite
         std::vector<u64> pts(m), prefix(m);
         for (size_t j = 0; j < m; ++j) {
             const Item& it = items[c0 + j];
-            diff[j] = h->work[3 * j];
-            sq[j] = h->work[3 * j + 1];
-            sel[j] = h->work[3 * j + 2];
+            diff[j] = h->work[4 * j];
+            sq[j] = h->work[4 * j + 1];
+            sel[j] = h->work[4 * j + 2];
             in[j] = q[it.qi].ct_dim;
             pts[j] = it.pt;
             auto pm = h->prefix.find({Ll, it.cnt});
@@ -307,15 +308,30 @@ int stage3_items(afhe_ivfpq* h, const afhe_ivfpq_query* q, const std::vector<Ite
         RC(sub_plain(h, in, pts, diff, Ll));
         RC(square(h, diff, sq, Ll));
         for (uint32_t s = B; s < D * B; s <<= 1) RC(rot_acc(h, sq, sq, (int32_t)s, Ll - 1));
-        RC(mult_plain(h, sq, prefix, sel, Ll - 1));
-        std::vector<std::pair<afhe_ct_ref, int32_t>> place;
         std::vector<std::pair<std::pair<afhe_ct_ref, bool>, afhe_ct_ref>> acc;
         for (size_t j = 0; j < m; ++j) {
             const Item& it = items[c0 + j];
-            place.push_back({sel[j], -(int32_t)(it.off % S)});
             acc.push_back({{q[it.qi].results[it.off / S], it.off % S == 0}, sel[j]});
         }
-        RC(h->sh.packed ? rotate_direct(h, place, Ll - 2) : rotate_grouped(h, place, Ll - 2));
+        if (h->sh.packed) {
+            // The tree sum runs over all D rows of B slots, so every row holds
+            // the batch's sums. The prefix mask moved to row t = offset / B
+            // (an automorphism of the plaintext: no key switch) both selects
+            // and places them.
+            std::vector<u64> masks(m);
+            std::vector<uint32_t> gal(m);
+            for (size_t j = 0; j < m; ++j) {
+                masks[j] = h->work[4 * j + 3].c0_offset;
+                gal[j] = afhe_galois_elt(h->ctx->log_n, -(int32_t)(items[c0 + j].off % S));
+            }
+            RC(afhe_automorphism_batch(h->ctx, prefix.data(), gal.data(), masks.data(), (uint32_t)m, Ll - 1));
+            RC(mult_plain(h, sq, masks, sel, Ll - 1));
+        } else {
+            RC(mult_plain(h, sq, prefix, sel, Ll - 1));
+            std::vector<std::pair<afhe_ct_ref, int32_t>> place;
+            for (size_t j = 0; j < m; ++j) place.push_back({sel[j], -(int32_t)(items[c0 + j].off % S)});
+            RC(rotate_grouped(h, place, Ll - 2));
+        }
         RC(accumulate(h, acc, Ll - 2));
     }
     return AFHE_OK;
@@ -389,8 +405,8 @@ int afhe_ivfpq_set_list(afhe_ivfpq* h, uint32_t list, const uint64_t* pts, const
 
 int afhe_ivfpq_set_lanes(afhe_ivfpq* h, const afhe_ct_ref* work, uint32_t lanes, const afhe_ct_ref* cmp) {
     if (!h || !work) return fail_h(h, AFHE_E_ARG, "null argument");
-    if (lanes < h->sh.lanes) return fail_h(h, AFHE_E_ARG, "a diff / sq / sel ciphertext triple for every lane");
-    h->work.assign(work, work + 3 * (size_t)lanes);
+    if (lanes < h->sh.lanes) return fail_h(h, AFHE_E_ARG, "a diff / sq / sel / mask quadruple for every lane");
+    h->work.assign(work, work + 4 * (size_t)lanes);
     if (!h->sh.packed && h->sh.n_list > 1) {
         if (!cmp) return fail_h(h, AFHE_E_ARG, "the reference compaction needs n_list - 1 term ciphertexts per lane");
         h->cmp.assign(cmp, cmp + (size_t)lanes * (h->sh.n_list - 1));

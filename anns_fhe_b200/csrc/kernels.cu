@@ -128,6 +128,27 @@ cudaError_t launch_automorphism(const uint32_t* map32, const u64* map64, u64* ar
     return cudaGetLastError();
 }
 
+// Every polynomial of a batch through its own permutation: maps.at(z) is the
+// device address of polynomial z's map (N indices, each < N).
+__global__ void __launch_bounds__(256) automorphism_z_kernel(const ZField maps, u64* __restrict__ arena, uint32_t n,
+                                                            const ZBases zb) {
+    const uint32_t l = blockIdx.y, z = blockIdx.z;
+    const uint32_t* __restrict__ map = (const uint32_t*)maps.at(z);
+    const u64 off = (u64)l * n;
+    const u64* a = arena + zb.src.at(z) + off;
+    u64* o = arena + zb.out.at(z) + off;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) o[i] = a[__ldg(map + i)];
+}
+
+cudaError_t launch_automorphism_z(const ZField& maps, u64* arena, uint32_t n, uint32_t limbs, uint32_t nz,
+                                  const ZBases& zb, cudaStream_t st) {
+    if (limbs == 0 || nz == 0) return cudaSuccess;
+    dim3 grid((n + 255) / 256, limbs, nz);
+    automorphism_z_kernel<<<grid, 256, 0, st>>>(maps, arena, n, zb);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
 // ---------------------------------------------------------------------------
 // plain transforms
 // ---------------------------------------------------------------------------

@@ -27,10 +27,13 @@ Two compactions:
     ciphertext returns all n_list distances (list k * (slots / D) + c at slot
     c * D + k). That takes n_coarse - 1 key switches per query instead of
     the reference's sum over lists of popcount(i * (D - 1)).
-    The packed chain also places candidates more cheaply: candidate batch t
-    of a query starts at slot (t mod (slots / B)) * B of result t // (slots /
-    B), and its placement rotation is one key switch with a key made for that
-    step, instead of eval_rotate's popcount(offset) power-of-two steps.
+    The packed chain also places candidates without a key switch: candidate
+    batch t of a query starts at slot (t mod (slots / B)) * B of result
+    t // (slots / B). Its tree sum runs over all D rows of B slots, so every
+    row already holds the batch's B sums; the prefix mask moved to row
+    t mod (slots / B) (an automorphism of the plaintext) selects them there,
+    instead of masking row 0 and rotating by the offset with
+    popcount(offset) key switches.
 In the reference chain, candidate distances past `slots` continue in further
 result ciphertexts (position p at slot p mod slots of result p // slots). A
 candidate batch never straddles two results: one that would not fit starts
@@ -55,7 +58,7 @@ import numpy as np
 
 from . import _lib as L
 from .ckks import Encoder, Slots, encode_index_batches, encode_plaintext, encode_plaintexts
-from .driver import FheContext, FHEHostDriver
+from .driver import FheContext, FHEHostDriver, galois_elt
 from .ivfpq import IvfPqIndex
 
 MAX_LANES = 4096
@@ -365,7 +368,7 @@ class InteractiveQueryManager:
                 s <<= 1
         else:
             steps.update(-k for k in range(1, sh.n_coarse))          # coarse packing, one step each
-            steps.update(-B * m for m in range(1, sh.slots // B))    # batch placement, one step each
+            # batch placement moves the plaintext mask instead: no key
         return steps
 
     def new_query(self) -> QueryRecord:
@@ -504,7 +507,7 @@ class InteractiveQueryManager:
             cnts = np.array([b[1] for b in bs] or [0], dtype=np.uint32)
             L.check(lib.afhe_ivfpq_set_list(h, c, self._offs([b[0] for b in bs]), cnts.ctypes.data_as(L.P32),
                                             len(bs)), "ivfpq_set_list")
-        work = self._refs([w[k] for w in self.work[:self.lanes] for k in ("diff", "sq", "sel")])
+        work = self._refs([w[k] for w in self.work[:self.lanes] for k in ("diff", "sq", "sel", "tmp")])
         cmp = self._refs([c for row in self.cmp[:self.lanes] for c in row]) if self.cmp else None
         L.check(lib.afhe_ivfpq_set_lanes(h, work, self.lanes, cmp), "ivfpq_set_lanes")
         for lv, ch in getattr(self, "_tuning", {}).items():
@@ -782,15 +785,21 @@ class InteractiveQueryManager:
             while s < D * B:                 # sq += rot(sq, s)
                 self._rot_acc(sq, sq, s, Ll - 1)
                 s <<= 1
-            self._mult_plain(sq, [self._prefix(x[2], Ll) for x in it], sel, Ll - 1)
-            # rotate each item by -(offset mod slots): eval_rotate's steps,
-            # grouped across items step by step (reference chain), or one key
-            # switch per item (packed chain)
-            place = [(sel[k], -(x[3] % S)) for k, x in enumerate(it)]
+            prefix = [self._prefix(x[2], Ll) for x in it]
             if self.sh.compaction == "packed":
-                self._rotate_direct(place, Ll - 2)
+                # the tree sum leaves the batch's sums in every row: the prefix
+                # mask moved to row offset / B (a plaintext automorphism, no
+                # key switch) selects and places them at once
+                masks = [x["tmp"][0] for x in w]
+                gal = (L.u32 * len(it))(*[galois_elt(self.p.log_n, -(x[3] % S)) for x in it])
+                L.check(self.lib.afhe_automorphism_batch(self.ctx.h, self._offs(prefix), gal, self._offs(masks),
+                                                         len(it), Ll - 1), "automorphism_batch")
+                self._mult_plain(sq, masks, sel, Ll - 1)
             else:
-                self._rotate_grouped(place, Ll - 2)
+                # rotate each item by -(offset mod slots): eval_rotate's steps,
+                # grouped across items step by step
+                self._mult_plain(sq, prefix, sel, Ll - 1)
+                self._rotate_grouped([(sel[k], -(x[3] % S)) for k, x in enumerate(it)], Ll - 2)
             # accumulate into result offset // slots; the item at slot 0 starts it
             self._accumulate([(queries[x[0]].results[x[3] // S], x[3] % S == 0, sel[k]) for k, x in enumerate(it)],
                              Ll - 2)

@@ -376,6 +376,15 @@ int afhe_eval_add_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const afhe_ct_ref* 
  * powers of two). dst[i] may alias in[i]. */
 int afhe_eval_rotate_steps_batch(afhe_ctx* ctx, const afhe_ct_ref* in, const afhe_ct_ref* dst,
                                  const int32_t* steps, uint32_t count, uint32_t limbs);
+/* dst[i] = the Galois automorphism galois[i] of the polynomial src[i] (`limbs`
+ * limbs, evaluation form): a permutation of its coefficients in each limb, the
+ * same gather afhe_automorphism applies, for many polynomials and elements in
+ * one launch. On a plaintext it rotates the slots: the automorphism of an
+ * encoded vector is the encoding of the rotated vector, exactly (a signed
+ * permutation of the rounded coefficients). No destination may overlap a
+ * source. Maps are computed on first use of an element and kept. */
+int afhe_automorphism_batch(afhe_ctx* ctx, const uint64_t* src, const uint32_t* galois, const uint64_t* dst,
+                            uint32_t count, uint32_t limbs);
 /* dst[i] = a[i] (both polynomials, `limbs` limbs): the slot-to-slot copies the
  * reference's host makes between operators (eval_sub_plain's c1 copy,
  * fhe_host_driver.cpp:259-270), for many ciphertexts in one launch. */
@@ -468,8 +477,10 @@ int afhe_ivfpq_set_prefix_mask(afhe_ivfpq* h, uint32_t level, uint32_t count, ui
 /* List `list`'s candidate batches: plaintext offsets and candidates per batch. */
 int afhe_ivfpq_set_list(afhe_ivfpq* h, uint32_t list, const uint64_t* pts, const uint32_t* counts,
                         uint32_t batches);
-/* Working ciphertexts: work[3 j .. 3 j + 2] = lane j's diff, sq, sel;
- * cmp[j (n_list - 1) + i - 1] = lane j's stage-1b term i (reference compaction). */
+/* Working ciphertexts: work[4 j .. 4 j + 3] = lane j's diff, sq, sel and a
+ * scratch slot whose c0 polynomial holds the lane's placed mask (packed
+ * chain); cmp[j (n_list - 1) + i - 1] = lane j's stage-1b term i (reference
+ * compaction). */
 int afhe_ivfpq_set_lanes(afhe_ivfpq* h, const afhe_ct_ref* work, uint32_t lanes, const afhe_ct_ref* cmp);
 /* Key-switch options applied around every operator the stages issue at
  * `level` limbs (afhe_ctx_set_option's AFHE_OPT_KS_FUSED, AFHE_OPT_CHUNK,

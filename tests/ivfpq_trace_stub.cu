@@ -44,6 +44,8 @@ afhe_ctx* trace_ctx_new(uint32_t L, uint32_t n, uint32_t lanes) {
     afhe_ctx* c = new afhe_ctx();
     c->L = L;
     c->n = n;
+    c->log_n = 0;
+    while ((1u << c->log_n) < n) ++c->log_n;
     c->lanes = lanes;
     g_log.clear();
     g_fused = 1;
@@ -120,6 +122,29 @@ int afhe_eval_rotate_accumulate_batch(afhe_ctx*, const afhe_ct_ref* in, const af
     refs(s, in, n), refs(s, acc, n);
     g_log.push_back(s);
     return AFHE_OK;
+}
+int afhe_automorphism_batch(afhe_ctx*, const uint64_t* src, const uint32_t* galois, const uint64_t* dst, uint32_t n,
+                            uint32_t limbs) {
+    std::string s = head("automorphism", limbs, false);
+    words(s, src, n);
+    for (uint32_t i = 0; i < n; ++i) s += " " + std::to_string(galois[i]);
+    s += " |";
+    words(s, dst, n);
+    g_log.push_back(s);
+    return AFHE_OK;
+}
+uint32_t afhe_galois_elt(uint32_t log_n, int32_t step) {
+    // 5^step mod 2N (5^-1 for negative steps), as the library computes it
+    const uint64_t m = 2ull << log_n;
+    uint64_t g = 1, b = 5, e = (uint64_t)(step < 0 ? -(int64_t)step : step) % (m / 4);
+    if (step < 0) {
+        uint64_t inv = 1;
+        for (uint64_t k = 0; k < m / 4 - 1; ++k) inv = inv * 5 % m;   // 5 has order N/2 mod 2N
+        b = inv;
+    }
+    for (; e; e >>= 1, b = b * b % m)
+        if (e & 1) g = g * b % m;
+    return (uint32_t)g;
 }
 int afhe_eval_rotate_steps_batch(afhe_ctx*, const afhe_ct_ref* in, const afhe_ct_ref* d, const int32_t* steps,
                                  uint32_t n, uint32_t limbs) {

@@ -28,6 +28,7 @@ import pytest
 
 from anns_fhe_b200.workloads import SMALL, Workload, WorkloadSpec
 from oracle.composite import OracleCKKS
+from oracle.oracle import tables_py as T
 
 pytestmark = pytest.mark.gpu
 
@@ -92,16 +93,22 @@ def reference_chain(wl, ora, ct, ct_dim, probes, level=None):
     off, acc, t = 0, {}, 0
     for c in probes:
         for pt_off, cnt, _ in iqm.batches[c]:
-            if packed:                  # batch t starts at t * B, placed by one key
+            if packed:                  # batch t starts at t * B, placed by its mask
                 off = t * B
             elif off % S + cnt > S:     # a batch that does not fit starts the next result
                 off = (off // S + 1) * S
             diff = ora.eval_sub_plain(ct_dim, pt(pt_off, L), L)
             sq = tree(ora.eval_mult_relin_rescale(diff, diff, relin, L), B)
-            sel = ora.eval_mult_plain_rescale(sq, pt(iqm._prefix_lv[(cnt, L)], L - 1), L - 1)
-            if off % S:
-                sel = (ora.eval_rotate_single_step(sel, -(off % S), rot, L - 2) if packed
-                       else ora.eval_rotate(sel, -(off % S), rot, L - 2))
+            mask = pt(iqm._prefix_lv[(cnt, L)], L - 1)
+            if packed:
+                # the tree sum leaves the sums in every row; the prefix mask
+                # moved to row t (a plaintext automorphism) selects them there
+                mask = ora.automorphism(mask, T.galois(p.log_n, -(off % S)), L - 1)
+                sel = ora.eval_mult_plain_rescale(sq, mask, L - 1)
+            else:
+                sel = ora.eval_mult_plain_rescale(sq, mask, L - 1)
+                if off % S:
+                    sel = ora.eval_rotate(sel, -(off % S), rot, L - 2)
             r = off // S
             acc[r] = sel if r not in acc else ora.eval_add(acc[r], sel, L - 2)
             off += cnt

@@ -17,6 +17,8 @@ import shutil
 import subprocess
 import zlib
 
+from types import SimpleNamespace
+
 import numpy as np
 import pytest
 
@@ -103,6 +105,11 @@ class FakeLib:
         self.log.append(self._head("rot_acc", limbs, True) + f" {rot} |" + self._refs(a, n) + self._refs(acc, n))
         return 0
 
+    def afhe_automorphism_batch(self, h, src, gal, dst, n, limbs):
+        self.log.append(self._head("automorphism", limbs, False) + self._words(src, n) + self._words(gal, n)
+                        + self._words(dst, n))
+        return 0
+
     def afhe_eval_rotate_steps_batch(self, h, a, d, steps, n, limbs):
         self.log.append(self._head("rotate_steps", limbs, True) + self._words(steps, n) + self._refs(a, n)
                         + self._refs(d, n))
@@ -135,6 +142,7 @@ def build_manager(rng, *, D, n_list, slots, L_top, lanes, compaction, eval_level
     m = object.__new__(InteractiveQueryManager)
     ctx = FakeCtx(ctx_lanes)
     m.ctx, m.sh, m.lanes, m.L, m.native = ctx, sh, lanes, L_top, False
+    m.p = SimpleNamespace(log_n=(2 * slots).bit_length() - 1)
     m.lib = FakeLib(ctx)
     m._nh, m._nh_key, m._nh_ver = None, None, 0
     nxt = iter(range(1000, 10 ** 9, 7))
