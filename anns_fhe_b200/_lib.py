@@ -85,7 +85,7 @@ class IvfpqShape(C.Structure):
 
 
 class IvfpqQuery(C.Structure):
-    _fields_ = [("ct_query", CtRef), ("ct_dim", CtRef), ("compact", CtRef), ("results", C.POINTER(CtRef)),
+    _fields_ = [("ct_query", CtRef), ("ct_dim", CtRef), ("compact", CtRef), ("norm", CtRef), ("results", C.POINTER(CtRef)),
                 ("n_results", u32), ("level", u32), ("probes", C.POINTER(u32)), ("nprobe", u32)]
 
 
@@ -166,10 +166,13 @@ SIGNATURES = {
     "afhe_ntt_get_plan": (C.c_int, [u32, P32]),
     "afhe_automorphism_from_map": (C.c_int, [CTX, u64, u64, u64, u32, u32]),
     "afhe_automorphism_batch": (C.c_int, [CTX, P64, P32, P64, u32, u32]),
+    "afhe_eval_sub_batch": (C.c_int, [CTX, C.POINTER(CtRef), C.POINTER(CtRef), C.POINTER(CtRef), u32, u32]),
+    "afhe_eval_add_plain_batch": (C.c_int, [CTX, C.POINTER(CtRef), P64, C.POINTER(CtRef), u32, u32]),
     "afhe_encode_batch": (C.c_int, [CTX, C.POINTER(C.c_double), u32, u32, C.c_double, u32, P64]),
     "afhe_pq_create": (C.c_int, [CTX, C.POINTER(PqIndex), C.POINTER(C.c_void_p)]),
     "afhe_pq_destroy": (C.c_int, [C.c_void_p]),
     "afhe_pq_encode_batches": (C.c_int, [C.c_void_p, P32, P32, P32, u32, C.c_double, u32, P64]),
+    "afhe_pq_encode_norms": (C.c_int, [C.c_void_p, P32, P32, P32, u32, C.c_double, u32, P64]),
     "afhe_ivfpq_create": (C.c_int, [CTX, C.POINTER(IvfpqShape), C.POINTER(C.c_void_p)]),
     "afhe_ivfpq_destroy": (C.c_int, [C.c_void_p]),
     "afhe_ivfpq_set_centroids": (C.c_int, [C.c_void_p, P64, u32]),
@@ -177,6 +180,7 @@ SIGNATURES = {
     "afhe_ivfpq_set_prefix_mask": (C.c_int, [C.c_void_p, u32, u32, u64]),
     "afhe_ivfpq_set_list": (C.c_int, [C.c_void_p, u32, P64, P32, u32]),
     "afhe_ivfpq_set_lanes": (C.c_int, [C.c_void_p, C.POINTER(CtRef), u32, C.POINTER(CtRef)]),
+    "afhe_ivfpq_set_norms": (C.c_int, [C.c_void_p, u32, P64, u32]),
     "afhe_ivfpq_set_tuning": (C.c_int, [C.c_void_p, u32, C.POINTER(KsOptions)]),
     "afhe_ivfpq_stage1": (C.c_int, [C.c_void_p, C.POINTER(IvfpqQuery), u32]),
     "afhe_ivfpq_stage3": (C.c_int, [C.c_void_p, C.POINTER(IvfpqQuery), u32]),

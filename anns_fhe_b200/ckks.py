@@ -425,11 +425,13 @@ def encode_plaintexts(ctx: FheContext, enc: Encoder, values: np.ndarray, scale: 
                                       float(scale), level, o.ctypes.data_as(L.P64)), "encode_batch")
 
 
-def encode_index_batches(ctx: FheContext, index, vids, first, counts, offs, scale: float, level: int) -> None:
+def encode_index_batches(ctx: FheContext, index, vids, first, counts, offs, scale: float, level: int,
+                         norms: bool = False) -> None:
     """The stage-3 candidate plaintexts built and encoded on the device
     (afhe_pq_*): batch b holds candidates vids[first[b] .. first[b] +
     counts[b]); slot d B + j = component d of candidate j's reconstruction
-    (centroid of its list + its PQ codewords)."""
+    (centroid of its list + its PQ codewords). With `norms`, the batches'
+    squared norms instead: slot d B + j = ||x_j||^2 in every row d."""
     from . import _lib as L
     cent = np.ascontiguousarray(index.centroids, dtype=np.float32)
     books = np.ascontiguousarray(index.codebooks, dtype=np.float32)
@@ -446,9 +448,9 @@ def encode_index_batches(ctx: FheContext, index, vids, first, counts, offs, scal
         f = np.ascontiguousarray(first, dtype=np.uint32)
         c = np.ascontiguousarray(counts, dtype=np.uint32)
         o = np.ascontiguousarray(offs, dtype=np.uint64)
-        L.check(ctx.lib.afhe_pq_encode_batches(h, v.ctypes.data_as(L.P32), f.ctypes.data_as(L.P32),
-                                               c.ctypes.data_as(L.P32), o.size, float(scale), level,
-                                               o.ctypes.data_as(L.P64)), "pq_encode_batches")
+        fn = ctx.lib.afhe_pq_encode_norms if norms else ctx.lib.afhe_pq_encode_batches
+        L.check(fn(h, v.ctypes.data_as(L.P32), f.ctypes.data_as(L.P32), c.ctypes.data_as(L.P32), o.size,
+                   float(scale), level, o.ctypes.data_as(L.P64)), "pq_encode")
     finally:
         ctx.lib.afhe_pq_destroy(h)
 

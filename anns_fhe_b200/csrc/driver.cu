@@ -716,6 +716,46 @@ int afhe_eval_add_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const afhe_ct_ref* 
     });
 }
 
+int afhe_eval_sub_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const afhe_ct_ref* b, const afhe_ct_ref* d,
+                        uint32_t count, uint32_t limbs) {
+    if (!ctx || (count && (!a || !b || !d))) return fail(ctx, AFHE_E_ARG, "null argument");
+    int rc;
+    if ((rc = check_limbs(ctx, limbs, 1)) || (rc = check_cts(ctx, a, count, limbs)) ||
+        (rc = check_cts(ctx, b, count, limbs)) || (rc = check_cts(ctx, d, count, limbs)))
+        return rc;
+    return for_chunks(ctx, count, [&](uint32_t s, uint32_t m) {
+        Offs A(2 * m), B(2 * m), D(2 * m);
+        for (uint32_t z = 0; z < m; ++z) {
+            A[2 * z] = a[s + z].c0_offset; A[2 * z + 1] = a[s + z].c1_offset;
+            B[2 * z] = b[s + z].c0_offset; B[2 * z + 1] = b[s + z].c1_offset;
+            D[2 * z] = d[s + z].c0_offset; D[2 * z + 1] = d[s + z].c1_offset;
+        }
+        return ew_batch(ctx, EW_SUB, A, &B, D, limbs);
+    });
+}
+
+int afhe_eval_add_plain_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const uint64_t* pt, const afhe_ct_ref* d,
+                              uint32_t count, uint32_t limbs) {
+    if (!ctx || (count && (!a || !pt || !d))) return fail(ctx, AFHE_E_ARG, "null argument");
+    int rc;
+    if ((rc = check_limbs(ctx, limbs, 1)) || (rc = check_cts(ctx, a, count, limbs)) || (rc = check_cts(ctx, d, count, limbs)))
+        return rc;
+    for (uint32_t i = 0; i < count; ++i)
+        if ((rc = check_poly(ctx, pt[i], limbs))) return rc;
+    return for_chunks(ctx, count, [&](uint32_t s, uint32_t m) {
+        Offs A(m), P(m), D(m), A2, D2;
+        for (uint32_t z = 0; z < m; ++z) { A[z] = a[s + z].c0_offset; P[z] = pt[s + z]; D[z] = d[s + z].c0_offset; }
+        int r = ew_batch(ctx, EW_ADD, A, &P, D, limbs);
+        if (r != AFHE_OK) return r;
+        for (uint32_t z = 0; z < m; ++z)
+            if (a[s + z].c1_offset != d[s + z].c1_offset) {
+                A2.push_back(a[s + z].c1_offset);
+                D2.push_back(d[s + z].c1_offset);
+            }
+        return A2.empty() ? AFHE_OK : ew_batch(ctx, EW_COPY, A2, nullptr, D2, limbs);
+    });
+}
+
 int afhe_automorphism_batch(afhe_ctx* ctx, const uint64_t* src, const uint32_t* galois, const uint64_t* dst,
                             uint32_t count, uint32_t limbs) {
     if (!ctx || (count && (!src || !galois || !dst))) return fail(ctx, AFHE_E_ARG, "null argument");

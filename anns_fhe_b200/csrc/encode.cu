@@ -220,6 +220,35 @@ __global__ void fft_load_pq(double2* __restrict__ v, uint32_t s, uint32_t dim, u
     }
 }
 
+// The candidates' squared norms, slot d B + j = ||x_j||^2 for every row d
+// (x_j the reconstruction of the batch's candidate j), 0 past the count: the
+// plaintext the expanded distance ||q||^2 - 2 <q, x_j> + ||x_j||^2 adds after
+// the tree sum has left its other two terms in every row.
+__global__ void fft_load_pq_norms(double2* __restrict__ v, uint32_t s, uint32_t dim, uint32_t M, uint32_t K,
+                                  const float* __restrict__ cent, const float* __restrict__ cb,
+                                  const uint8_t* __restrict__ codes, const uint32_t* __restrict__ assign,
+                                  const uint32_t* __restrict__ vids, const uint32_t* __restrict__ first,
+                                  const uint32_t* __restrict__ cnt, uint32_t count) {
+    const uint32_t B = s / dim, sd = dim / M;
+    const u64 total = (u64)count * s;
+    for (u64 t = blockIdx.x * (u64)blockDim.x + threadIdx.x; t < total; t += (u64)gridDim.x * blockDim.x) {
+        const uint32_t z = (uint32_t)(t / s), j = (uint32_t)(t % s) % B;
+        double x2 = 0.0;
+        if (j < cnt[z]) {
+            const uint32_t id = vids[first[z] + j];
+            const float* c = cent + (u64)assign[id] * dim;
+            for (uint32_t m = 0; m < M; ++m) {
+                const float* w = cb + ((u64)m * K + codes[(u64)id * M + m]) * sd;
+                for (uint32_t e = 0; e < sd; ++e) {
+                    const double x = (double)c[m * sd + e] + (double)w[e];
+                    x2 += x * x;
+                }
+            }
+        }
+        v[t] = make_double2(x2, 0.0);
+    }
+}
+
 int grid_for(u64 work) {
     u64 b = (work + 255) / 256;
     return (int)(b < 148ull * 16 ? (b ? b : 1) : 148ull * 16);
@@ -363,8 +392,26 @@ int afhe_pq_destroy(afhe_pq* p) {
     return AFHE_OK;
 }
 
+namespace {
+int pq_encode(afhe_pq* p, const uint32_t* vids, const uint32_t* first, const uint32_t* cnt, uint32_t batches,
+              double scale, uint32_t level, const uint64_t* pt, bool norms);
+}
+
 int afhe_pq_encode_batches(afhe_pq* p, const uint32_t* vids, const uint32_t* first, const uint32_t* cnt,
                            uint32_t batches, double scale, uint32_t level, const uint64_t* pt) {
+    return pq_encode(p, vids, first, cnt, batches, scale, level, pt, false);
+}
+
+int afhe_pq_encode_norms(afhe_pq* p, const uint32_t* vids, const uint32_t* first, const uint32_t* cnt,
+                         uint32_t batches, double scale, uint32_t level, const uint64_t* pt) {
+    return pq_encode(p, vids, first, cnt, batches, scale, level, pt, true);
+}
+
+}  // extern "C"
+
+namespace {
+int pq_encode(afhe_pq* p, const uint32_t* vids, const uint32_t* first, const uint32_t* cnt, uint32_t batches,
+              double scale, uint32_t level, const uint64_t* pt, bool norms) {
     if (!p) return fail(nullptr, AFHE_E_ARG, "null argument");
     afhe_ctx* ctx = p->ctx;
     if (batches && (!vids || !first || !cnt || !pt)) return fail(ctx, AFHE_E_ARG, "null argument");
@@ -397,8 +444,14 @@ int afhe_pq_encode_batches(afhe_pq* p, const uint32_t* vids, const uint32_t* fir
         return cuda_fail(ctx, e, "batch upload");
     }
     auto load = [&](double2* v, uint32_t c0, uint32_t m) -> int {
-        fft_load_pq<<<grid_for((u64)m * s), 256, 0, ctx->st>>>(v, s, p->d, p->M, p->K, p->centroids, p->codebooks,
-                                                               p->codes, p->assign, vids_d, first_d + c0, cnt_d + c0, m);
+        if (norms)
+            fft_load_pq_norms<<<grid_for((u64)m * s), 256, 0, ctx->st>>>(v, s, p->d, p->M, p->K, p->centroids,
+                                                                         p->codebooks, p->codes, p->assign, vids_d,
+                                                                         first_d + c0, cnt_d + c0, m);
+        else
+            fft_load_pq<<<grid_for((u64)m * s), 256, 0, ctx->st>>>(v, s, p->d, p->M, p->K, p->centroids,
+                                                                   p->codebooks, p->codes, p->assign, vids_d,
+                                                                   first_d + c0, cnt_d + c0, m);
         count_launches(1);
         return AFHE_OK;
     };
@@ -406,5 +459,4 @@ int afhe_pq_encode_batches(afhe_pq* p, const uint32_t* vids, const uint32_t* fir
     release();
     return rc;
 }
-
-}  // extern "C"
+}  // namespace

@@ -17,7 +17,9 @@
 //             every centroid slot of coarse ciphertext k, rescale, rotate by
 //             -k in one key switch, sum
 //   stage 3   per candidate batch: ct_dim - pt_batch, square, rescale, tree
-//             sum with rotations B, 2B, .., B D/2, mask the batch's slots,
+//             sum with rotations B, 2B, .., B D/2 (packed, with the norms
+//             registered: ||q||^2 - 2 ct_dim pt_batch, ||q||^2 squared once
+//             per query, then + ||x_j||^2 after the tree sum), mask the batch's slots,
 //             rescale, place it at its slot offset (eval_rotate's steps; when
 //             packed, the mask itself is moved to the batch's row, since the
 //             tree sum leaves the sums in every row), accumulate into the
@@ -43,6 +45,7 @@ struct afhe_ivfpq {
     std::vector<u64> centroid_cts;                      // [n_coarse]
     std::map<uint32_t, std::vector<u64>> masks;         // level -> one-hot [n_list] or stride [1]
     std::map<std::pair<uint32_t, uint32_t>, u64> prefix;   // (level, count) -> mask of the first count slots
+    std::map<uint32_t, std::vector<u64>> norms;         // level -> candidates' squared norms per global batch
     std::vector<std::vector<std::pair<u64, uint32_t>>> lists;   // list -> (plaintext, candidates) per batch
     std::vector<afhe_ct_ref> work;                      // diff, sq, sel per lane
     std::vector<afhe_ct_ref> cmp;                       // (n_list - 1) per lane: reference compaction terms
@@ -286,10 +289,40 @@ struct Item {
     u64 pt;
     uint32_t cnt;
     u64 off;
+    uint32_t gb;      // global batch number (lists in order, then batches)
 };
+
+int sub(afhe_ivfpq* h, const Cts& a, const Cts& b, const Cts& d, uint32_t limbs) {
+    return a.empty() ? AFHE_OK : afhe_eval_sub_batch(h->ctx, a.data(), b.data(), d.data(), (uint32_t)a.size(), limbs);
+}
+
+int add_plain(afhe_ivfpq* h, const Cts& a, const std::vector<u64>& pts, const Cts& d, uint32_t limbs) {
+    return afhe_eval_add_plain_batch(h->ctx, a.data(), pts.data(), d.data(), (uint32_t)a.size(), limbs);
+}
 
 int stage3_items(afhe_ivfpq* h, const afhe_ivfpq_query* q, const std::vector<Item>& items, uint32_t Ll) {
     const uint32_t D = h->sh.D, S = h->sh.slots, B = S / D, lanes = h->sh.lanes;
+    // Expanded distances (packed chain, with the candidates' norms registered
+    // for this level): ||q - x_j||^2 = ||q||^2 - 2 <q, x_j> + ||x_j||^2, the
+    // query's ||q||^2 squared once per query instead of a square per batch.
+    auto nit = h->norms.find(Ll);
+    const bool expand = h->sh.packed && nit != h->norms.end();
+    if (expand) {
+        Cts qin, qnorm;
+        std::vector<bool> seen;
+        for (const Item& it : items) {
+            if (it.qi >= seen.size()) seen.resize(it.qi + 1, false);
+            if (seen[it.qi]) continue;
+            seen[it.qi] = true;
+            qin.push_back(q[it.qi].ct_dim);
+            qnorm.push_back(q[it.qi].norm);
+        }
+        for (size_t c0 = 0; c0 < qin.size(); c0 += lanes) {
+            const size_t m = std::min<size_t>(lanes, qin.size() - c0);
+            RC(square(h, Cts(qin.begin() + c0, qin.begin() + c0 + m), Cts(qnorm.begin() + c0, qnorm.begin() + c0 + m),
+                      Ll));
+        }
+    }
     for (size_t c0 = 0; c0 < items.size(); c0 += lanes) {
         const size_t m = std::min<size_t>(lanes, items.size() - c0);
         Cts diff(m), sq(m), sel(m), in(m);
@@ -305,9 +338,25 @@ int stage3_items(afhe_ivfpq* h, const afhe_ivfpq_query* q, const std::vector<Ite
             if (pm == h->prefix.end()) return fail_h(h, AFHE_E_STATE, "no prefix mask for a candidate count at this level");
             prefix[j] = pm->second;
         }
-        RC(sub_plain(h, in, pts, diff, Ll));
-        RC(square(h, diff, sq, Ll));
-        for (uint32_t s = B; s < D * B; s <<= 1) RC(rot_acc(h, sq, sq, (int32_t)s, Ll - 1));
+        if (expand) {
+            Cts qn(m);
+            std::vector<u64> nx(m);
+            for (size_t j = 0; j < m; ++j) {
+                qn[j] = q[items[c0 + j].qi].norm;
+                if (items[c0 + j].gb >= nit->second.size())
+                    return fail_h(h, AFHE_E_STATE, "no norm plaintext for a candidate batch at this level");
+                nx[j] = nit->second[items[c0 + j].gb];
+            }
+            RC(mult_plain(h, in, pts, diff, Ll));          // <q, x_j> per row (one rescale)
+            RC(sub(h, qn, diff, sq, Ll - 1));              // ||q||^2 - <q, x_j>
+            RC(sub(h, sq, diff, sq, Ll - 1));              //          - <q, x_j>
+            for (uint32_t s = B; s < D * B; s <<= 1) RC(rot_acc(h, sq, sq, (int32_t)s, Ll - 1));
+            RC(add_plain(h, sq, nx, sq, Ll - 1));          // + ||x_j||^2, in every row
+        } else {
+            RC(sub_plain(h, in, pts, diff, Ll));
+            RC(square(h, diff, sq, Ll));
+            for (uint32_t s = B; s < D * B; s <<= 1) RC(rot_acc(h, sq, sq, (int32_t)s, Ll - 1));
+        }
         std::vector<std::pair<std::pair<afhe_ct_ref, bool>, afhe_ct_ref>> acc;
         for (size_t j = 0; j < m; ++j) {
             const Item& it = items[c0 + j];
@@ -414,6 +463,13 @@ int afhe_ivfpq_set_lanes(afhe_ivfpq* h, const afhe_ct_ref* work, uint32_t lanes,
     return AFHE_OK;
 }
 
+int afhe_ivfpq_set_norms(afhe_ivfpq* h, uint32_t level, const uint64_t* pts, uint32_t batches) {
+    if (!h || (batches && !pts)) return fail_h(h, AFHE_E_ARG, "null argument");
+    if (!h->sh.packed) return fail_h(h, AFHE_E_STATE, "expanded distances are for the packed chain");
+    h->norms[level].assign(pts, pts + batches);
+    return AFHE_OK;
+}
+
 int afhe_ivfpq_set_tuning(afhe_ivfpq* h, uint32_t level, const afhe_ks_options* o) {
     if (!h || !o) return fail_h(h, AFHE_E_ARG, "null argument");
     if (o->ept && o->ept != 8 && o->ept != 16) return fail_h(h, AFHE_E_ARG, "values per thread must be 8 or 16");
@@ -436,6 +492,8 @@ int afhe_ivfpq_stage3(afhe_ivfpq* h, const afhe_ivfpq_query* q, uint32_t count) 
     if (!h || (count && !q)) return fail_h(h, AFHE_E_ARG, "null argument");
     if (h->work.empty()) return fail_h(h, AFHE_E_STATE, "lanes not set");
     const uint32_t S = h->sh.slots, B = S / h->sh.D;
+    std::vector<uint32_t> first_batch(h->sh.n_list + 1, 0);      // global number of each list's first batch
+    for (uint32_t c = 0; c < h->sh.n_list; ++c) first_batch[c + 1] = first_batch[c] + (uint32_t)h->lists[c].size();
     std::map<uint32_t, std::vector<Item>> items;
     for (uint32_t qi = 0; qi < count; ++qi) {
         RC(check_query(h, q[qi]));
@@ -446,7 +504,8 @@ int afhe_ivfpq_stage3(afhe_ivfpq* h, const afhe_ivfpq_query* q, uint32_t count) 
         for (uint32_t p = 0; p < q[qi].nprobe; ++p) {
             const uint32_t c = q[qi].probes[p];
             if (c >= h->sh.n_list) return fail_h(h, AFHE_E_RANGE, "probed list out of range");
-            for (auto& b : h->lists[c]) {
+            for (size_t bi = 0; bi < h->lists[c].size(); ++bi) {
+                const auto& b = h->lists[c][bi];
                 u64 at_;
                 if (h->sh.packed) {
                     at_ = (u64)t * B;            // batch t at slot t B
@@ -456,7 +515,7 @@ int afhe_ivfpq_stage3(afhe_ivfpq* h, const afhe_ivfpq_query* q, uint32_t count) 
                     off += b.second;
                 }
                 if (at_ / S >= q[qi].n_results) return fail_h(h, AFHE_E_RANGE, "more candidates than the result ciphertexts hold");
-                lst.push_back({qi, b.first, b.second, at_});
+                lst.push_back({qi, b.first, b.second, at_, first_batch[c] + (uint32_t)bi});
                 ++t;
             }
         }

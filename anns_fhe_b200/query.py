@@ -107,6 +107,7 @@ class QueryRecord:
     results: list = field(default_factory=list)    # every result ciphertext (dists first)
     level: int = 0          # limbs of the encrypted query (0: the top level L)
     nprobe: int = 0         # lists the client selects (0: the shape's nprobe)
+    norm: tuple | None = None   # stage 3 scratch, packed chain: ||q||^2 (at the evaluation level - 1)
 
 
 def batch_offsets(counts, slots: int, align: int | None = None) -> list[int]:
@@ -218,6 +219,14 @@ class InteractiveQueryManager:
         # reconstruction of candidate j: centroid + PQ codewords)
         if boffs:
             encode_index_batches(ctx, index, bvids, bfirst, bcnt, boffs, shape.scale, L)
+        self._bvids, self._bfirst, self._bcnt = bvids, bfirst, bcnt
+        self._first_batch = np.concatenate([[0], np.cumsum([len(b) for b in self.batches])]).astype(int).tolist()
+        # packed chain: the candidates' squared norms per level, for the
+        # expanded distance ||q||^2 - 2 <q, x_j> + ||x_j||^2
+        self._norms: dict[int, list[int]] = {}
+        if shape.compaction == "packed":
+            for lv in self.levels:
+                self._norm_plaintexts(lv)
         self._counts = sorted(counts)
         for lv in self.levels:
             self._prefix_masks(lv)
@@ -257,6 +266,20 @@ class InteractiveQueryManager:
             self._stride[lv] = self.slots.take(1)[0]
             encode_plaintexts(self.ctx, self.enc, m, ms, [self._stride[lv]], lv - 1)
 
+    def _norm_plaintexts(self, lv: int) -> None:
+        """The candidate batches' squared norms at level lv - 1, scale
+        Delta^2 / q_{lv-1} (the scale of <q, x_j> and ||q||^2 after their
+        rescale), packed back to back."""
+        nb = len(self._bcnt)
+        w1 = (lv - 1) * self.p.n
+        base = self.slots.take(self.norm_plaintext_slots(nb, lv, self.p.n, self.slots.w))[0] if nb else 0
+        offs = [base + b * w1 for b in range(nb)]
+        if nb:
+            encode_index_batches(self.ctx, self.index, self._bvids, self._bfirst, self._bcnt, offs,
+                                 self.sh.scale * self.sh.scale / self.p.q[lv - 1], lv - 1, norms=True)
+        self._norms[lv] = offs
+        self._nh_ver += 1
+
     def _prefix_masks(self, lv: int) -> None:
         """Masks of the first `count` slots, for every candidate-batch size."""
         cs = self._counts
@@ -279,6 +302,8 @@ class InteractiveQueryManager:
             if lv not in self.levels:
                 self._level_masks(lv)
                 self._prefix_masks(lv)
+                if self.sh.compaction == "packed":
+                    self._norm_plaintexts(lv)
                 self.levels = sorted(self.levels + [lv])
         self._nh_ver += 1
 
@@ -372,8 +397,21 @@ class InteractiveQueryManager:
         return steps
 
     def new_query(self) -> QueryRecord:
-        s = self.slots.take(8)
-        return QueryRecord((s[0], s[1]), (s[2], s[3]), (s[4], s[5]), (s[6], s[7]), results=[(s[6], s[7])])
+        s = self.slots.take(10 if self.sh.compaction == "packed" else 8)
+        return QueryRecord((s[0], s[1]), (s[2], s[3]), (s[4], s[5]), (s[6], s[7]), results=[(s[6], s[7])],
+                           norm=(s[8], s[9]) if self.sh.compaction == "packed" else None)
+
+    @staticmethod
+    def norm_slots(count: int, L: int, n: int, slot_w: int) -> int:
+        """Slots of the queries' ||q||^2 scratch (packed chain): 2 (L - 1) N
+        words per query, packed back to back."""
+        return -(-2 * count * (L - 1) * n // slot_w)
+
+    @staticmethod
+    def norm_plaintext_slots(batches: int, L: int, n: int, slot_w: int) -> int:
+        """Slots of one level's candidate-norm plaintexts (at most L - 1 limbs
+        each), packed back to back."""
+        return -(-batches * (L - 1) * n // slot_w)
 
     def alloc_queries(self, count: int) -> list[QueryRecord]:
         """Records whose results (compacted coarse distances; n_res candidate
@@ -382,13 +420,17 @@ class InteractiveQueryManager:
         w = self.lvl_out * self.p.n
         comp = self.slots.take(-(-2 * count * w // self.slots.w))[0]
         dist = self.slots.take(-(-2 * count * self.n_res * w // self.slots.w))[0]
+        packed = self.sh.compaction == "packed"
+        w1 = (self.L - 1) * self.p.n
+        nbase = self.slots.take(self.norm_slots(count, self.L, self.p.n, self.slots.w))[0] if packed else 0
         recs = []
         for i in range(count):
             s = self.slots.take(4)
             res = [(dist + 2 * (i * self.n_res + k) * w, dist + (2 * (i * self.n_res + k) + 1) * w)
                    for k in range(self.n_res)]
             recs.append(QueryRecord((s[0], s[1]), (s[2], s[3]),
-                                    (comp + 2 * i * w, comp + (2 * i + 1) * w), res[0], results=res))
+                                    (comp + 2 * i * w, comp + (2 * i + 1) * w), res[0], results=res,
+                                    norm=(nbase + 2 * i * w1, nbase + (2 * i + 1) * w1) if packed else None))
         self._outbox = {"compact": (comp, 1), "dists": (dist, self.n_res)}
         return recs
 
@@ -503,6 +545,8 @@ class InteractiveQueryManager:
             L.check(lib.afhe_ivfpq_set_level_masks(h, lv, self._offs(m), len(m)), "ivfpq_set_level_masks")
         for (cnt, lv), off in self._prefix_lv.items():
             L.check(lib.afhe_ivfpq_set_prefix_mask(h, lv, cnt, off), "ivfpq_set_prefix_mask")
+        for lv, offs in getattr(self, "_norms", {}).items():
+            L.check(lib.afhe_ivfpq_set_norms(h, lv, self._offs(offs), len(offs)), "ivfpq_set_norms")
         for c, bs in enumerate(self.batches):
             cnts = np.array([b[1] for b in bs] or [0], dtype=np.uint32)
             L.check(lib.afhe_ivfpq_set_list(h, c, self._offs([b[0] for b in bs]), cnts.ctypes.data_as(L.P32),
@@ -530,6 +574,8 @@ class InteractiveQueryManager:
         keep = [arr]
         for q, r in zip(arr, queries):
             q.ct_query, q.ct_dim, q.compact = L.CtRef(*r.ct_query), L.CtRef(*r.ct_dim), L.CtRef(*r.compact)
+            if r.norm is not None:
+                q.norm = L.CtRef(*r.norm)
             res = (L.CtRef * len(r.results))(*[L.CtRef(*c) for c in r.results])
             q.results, q.n_results, q.level = res, len(r.results), r.level
             keep.append(res)
@@ -578,6 +624,14 @@ class InteractiveQueryManager:
     def _copy(self, a, d, limbs):
         L.check(self.lib.afhe_eval_copy_batch(self.ctx.h, self._refs(a), self._refs(d), len(a), limbs),
                 "eval_copy_batch")
+
+    def _sub(self, a, b, d, limbs):
+        L.check(self.lib.afhe_eval_sub_batch(self.ctx.h, self._refs(a), self._refs(b), self._refs(d), len(a), limbs),
+                "eval_sub_batch")
+
+    def _add_plain(self, a, pts, d, limbs):
+        L.check(self.lib.afhe_eval_add_plain_batch(self.ctx.h, self._refs(a), self._offs(pts), self._refs(d), len(a),
+                                                   limbs), "eval_add_plain_batch")
 
     def _mult_plain(self, a, pts, d, limbs):
         L.check(self.lib.afhe_eval_mult_plain_rescale_batch(self.ctx.h, self._refs(a), self._offs(pts), self._refs(d),
@@ -751,10 +805,11 @@ class InteractiveQueryManager:
             q.vids, q.pos = [], []
             lst = items.setdefault(self.level_of(q), [])
             bs = [b for c in q.probes for b in self.batches[c]]
+            gbs = [self._first_batch[c] + i for c in q.probes for i in range(len(self.batches[c]))]
             align = self.sh.B if self.sh.compaction == "packed" else None
             offs = batch_offsets([b[1] for b in bs], S, align)
-            for (pt, cnt, vids), off in zip(bs, offs):
-                lst.append((qi, pt, cnt, off))
+            for (pt, cnt, vids), off, gb in zip(bs, offs, gbs):
+                lst.append((qi, pt, cnt, off, gb))
                 q.vids.extend(vids)
             q.pos = (np.concatenate([np.arange(off, off + b[1]) for b, off in zip(bs, offs)]) if bs
                      else np.zeros(0, dtype=np.int64))
@@ -773,18 +828,37 @@ class InteractiveQueryManager:
 
     def _stage3_items(self, queries: list[QueryRecord], items, Ll: int) -> None:
         D, B, S = self.sh.D, self.sh.B, self.sh.slots
+        norms = getattr(self, "_norms", {}).get(Ll) if self.sh.compaction == "packed" else None
+        if norms is not None:
+            # expanded distances: ||q||^2 squared once per query
+            seen, qs = set(), []
+            for x in items:
+                if x[0] not in seen:
+                    seen.add(x[0])
+                    qs.append(queries[x[0]])
+            for c0 in range(0, len(qs), self.lanes):
+                part = qs[c0:c0 + self.lanes]
+                self._square([q.ct_dim for q in part], [q.norm for q in part], Ll)
         for c0 in range(0, len(items), self.lanes):
             it = items[c0:c0 + self.lanes]
             w = self.work[:len(it)]
             diff = [x["diff"] for x in w]
             sq = [x["sq"] for x in w]
             sel = [x["sel"] for x in w]
-            self._sub_plain([queries[x[0]].ct_dim for x in it], [x[1] for x in it], diff, Ll)
-            self._square(diff, sq, Ll)
+            if norms is not None:
+                # ||q||^2 - 2 <q, x_j> in every row, then + ||x_j||^2
+                self._mult_plain([queries[x[0]].ct_dim for x in it], [x[1] for x in it], diff, Ll)
+                self._sub([queries[x[0]].norm for x in it], diff, sq, Ll - 1)
+                self._sub(sq, diff, sq, Ll - 1)
+            else:
+                self._sub_plain([queries[x[0]].ct_dim for x in it], [x[1] for x in it], diff, Ll)
+                self._square(diff, sq, Ll)
             s = B
             while s < D * B:                 # sq += rot(sq, s)
                 self._rot_acc(sq, sq, s, Ll - 1)
                 s <<= 1
+            if norms is not None:
+                self._add_plain(sq, [norms[x[4]] for x in it], sq, Ll - 1)
             prefix = [self._prefix(x[2], Ll) for x in it]
             if self.sh.compaction == "packed":
                 # the tree sum leaves the batch's sums in every row: the prefix

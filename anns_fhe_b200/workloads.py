@@ -150,10 +150,15 @@ class Workload:
         dec_slots = -(-most * 2 * n // slot_w) + -(-most * n // slot_w)
         outbox_slots = -(-2 * max_queries * w_out // slot_w) + -(-2 * max_queries * n_res * w_out // slot_w)
         masks = InteractiveQueryManager.mask_slots(shape, len(lvls) + spare_levels, spec.compaction == "reference")
+        norm_slots = 0
+        if spec.compaction == "packed":     # ||q||^2 scratch per query; the candidates' norms per level
+            norm_slots = (InteractiveQueryManager.norm_slots(max_queries, self.params.L, n, slot_w)
+                          + (len(lvls) + spare_levels)
+                          * InteractiveQueryManager.norm_plaintext_slots(n_batches, self.params.L, n, slot_w))
         n_slots = (16 + shape.n_coarse + masks + n_batches + 8 * lanes + 4 * max_queries + outbox_slots + 64
                    + InteractiveQueryManager.compaction_slots(spec.n_list if spec.compaction == "reference" else 1,
                                                               self.params.L, n, slot_w, lanes)
-                   + dec_slots)
+                   + dec_slots + norm_slots)
         self.ctx = FheContext(self.params, poly_words=n_slots * slot_w,
                               key_words=n_keys * self.params.key_words() + 4096, device=device,
                               max_batch=lanes)

@@ -390,6 +390,12 @@ int afhe_automorphism_batch(afhe_ctx* ctx, const uint64_t* src, const uint32_t* 
  * fhe_host_driver.cpp:259-270), for many ciphertexts in one launch. */
 int afhe_eval_copy_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const afhe_ct_ref* dst, uint32_t count,
                          uint32_t limbs);
+/* dst[i] = a[i] - b[i] (both polynomials) */
+int afhe_eval_sub_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const afhe_ct_ref* b, const afhe_ct_ref* dst,
+                        uint32_t count, uint32_t limbs);
+/* dst[i] = a[i] + pt[i] (c0 + pt, c1 copied), the add counterpart of eval_sub_plain */
+int afhe_eval_add_plain_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const uint64_t* pt, const afhe_ct_ref* dst,
+                              uint32_t count, uint32_t limbs);
 /* pt[i] is the plaintext polynomial offset for ciphertext i */
 int afhe_eval_sub_plain_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const uint64_t* pt, const afhe_ct_ref* dst,
                               uint32_t count, uint32_t limbs);
@@ -434,6 +440,11 @@ int afhe_pq_destroy(afhe_pq* pq);
  * encoded as afhe_encode_batch does into pt[b]. */
 int afhe_pq_encode_batches(afhe_pq* pq, const uint32_t* vids, const uint32_t* first, const uint32_t* count,
                            uint32_t batches, double scale, uint32_t level, const uint64_t* pt);
+/* The same batches' squared norms: slot d' B + j = ||x_j||^2 in every row d',
+ * 0 past the count (the term the expanded distance ||q||^2 - 2 <q, x_j> +
+ * ||x_j||^2 adds after the tree sum). */
+int afhe_pq_encode_norms(afhe_pq* pq, const uint32_t* vids, const uint32_t* first, const uint32_t* count,
+                         uint32_t batches, double scale, uint32_t level, const uint64_t* pt);
 
 /* ---- encrypted IVF-PQ server stages ---------------------------------------- */
 /* InteractiveQueryManager's server stages (cpp_host_model/src/
@@ -459,6 +470,7 @@ typedef struct afhe_ivfpq_query {
     afhe_ct_ref ct_query;        /* the query, repeated every D slots (stage 1 input) */
     afhe_ct_ref ct_dim;          /* the query, dimension d in slots d B .. d B + B - 1 (stage 3 input) */
     afhe_ct_ref compact;         /* stage 1b output: the compacted coarse distances */
+    afhe_ct_ref norm;            /* stage 3 scratch (expanded distances): ||q||^2 at the level - 1 */
     const afhe_ct_ref* results;  /* stage 3 outputs, n_results ciphertexts */
     uint32_t n_results;
     uint32_t level;              /* limbs of the encrypted query (0: the top level) */
@@ -482,6 +494,13 @@ int afhe_ivfpq_set_list(afhe_ivfpq* h, uint32_t list, const uint64_t* pts, const
  * chain); cmp[j (n_list - 1) + i - 1] = lane j's stage-1b term i (reference
  * compaction). */
 int afhe_ivfpq_set_lanes(afhe_ivfpq* h, const afhe_ct_ref* work, uint32_t lanes, const afhe_ct_ref* cmp);
+/* Expanded distances for the packed chain at `level`: pts[g] is the squared
+ * norms plaintext (afhe_pq_encode_norms, level - 1 limbs, scale Delta^2 /
+ * q_{level-1}) of global batch g (lists in order, then their batches). With
+ * them stage 3 computes ||q||^2 - 2 <q, x_j> + ||x_j||^2: ||q||^2 once per
+ * query (one relinearisation into afhe_ivfpq_query.norm), a plaintext
+ * product per batch instead of a square. */
+int afhe_ivfpq_set_norms(afhe_ivfpq* h, uint32_t level, const uint64_t* pts, uint32_t batches);
 /* Key-switch options applied around every operator the stages issue at
  * `level` limbs (afhe_ctx_set_option's AFHE_OPT_KS_FUSED, AFHE_OPT_CHUNK,
  * AFHE_OPT_KS_EPT, AFHE_OPT_KS_SLICE, AFHE_OPT_FUSED_MIN): fused -1 leaves

@@ -82,6 +82,20 @@ int afhe_eval_add_batch(afhe_ctx*, const afhe_ct_ref* a, const afhe_ct_ref* b, c
     g_log.push_back(s);
     return AFHE_OK;
 }
+int afhe_eval_sub_batch(afhe_ctx*, const afhe_ct_ref* a, const afhe_ct_ref* b, const afhe_ct_ref* d, uint32_t n,
+                        uint32_t limbs) {
+    std::string s = head("sub", limbs, false);
+    refs(s, a, n), refs(s, b, n), refs(s, d, n);
+    g_log.push_back(s);
+    return AFHE_OK;
+}
+int afhe_eval_add_plain_batch(afhe_ctx*, const afhe_ct_ref* a, const uint64_t* pt, const afhe_ct_ref* d, uint32_t n,
+                              uint32_t limbs) {
+    std::string s = head("add_plain", limbs, false);
+    refs(s, a, n), words(s, pt, n), refs(s, d, n);
+    g_log.push_back(s);
+    return AFHE_OK;
+}
 int afhe_eval_copy_batch(afhe_ctx*, const afhe_ct_ref* a, const afhe_ct_ref* d, uint32_t n, uint32_t limbs) {
     std::string s = head("copy", limbs, false);
     refs(s, a, n), refs(s, d, n);

@@ -90,15 +90,25 @@ def reference_chain(wl, ora, ct, ct_dim, probes, level=None):
     # stage 3: candidate p lands in result p // slots at slot p mod slots
     S = iqm.sh.slots
     packed = iqm.sh.compaction == "packed"
+    if packed:      # expanded distances: the query's ||q||^2 once
+        qnorm = ora.eval_mult_relin_rescale(ct_dim, ct_dim, relin, L)
     off, acc, t = 0, {}, 0
     for c in probes:
-        for pt_off, cnt, _ in iqm.batches[c]:
+        for bi, (pt_off, cnt, _) in enumerate(iqm.batches[c]):
             if packed:                  # batch t starts at t * B, placed by its mask
                 off = t * B
             elif off % S + cnt > S:     # a batch that does not fit starts the next result
                 off = (off // S + 1) * S
-            diff = ora.eval_sub_plain(ct_dim, pt(pt_off, L), L)
-            sq = tree(ora.eval_mult_relin_rescale(diff, diff, relin, L), B)
+            if packed:
+                # ||q||^2 - 2 <q, x_j> in every row after the tree sum, then + ||x_j||^2
+                cx = ora.eval_mult_plain_rescale(ct_dim, pt(pt_off, L), L)
+                y = tuple(ora.poly("sub", ora.poly("sub", qn, ci, L - 1), ci, L - 1) for qn, ci in zip(qnorm, cx))
+                sq = tree(y, B)
+                nrm = pt(iqm._norms[L][iqm._first_batch[c] + bi], L - 1)
+                sq = (ora.poly("add", sq[0], nrm, L - 1), sq[1])
+            else:
+                diff = ora.eval_sub_plain(ct_dim, pt(pt_off, L), L)
+                sq = tree(ora.eval_mult_relin_rescale(diff, diff, relin, L), B)
             mask = pt(iqm._prefix_lv[(cnt, L)], L - 1)
             if packed:
                 # the tree sum leaves the sums in every row; the prefix mask

@@ -80,6 +80,15 @@ class FakeLib:
         self.log.append(self._head("add", limbs, False) + self._refs(a, n) + self._refs(b, n) + self._refs(d, n))
         return 0
 
+    def afhe_eval_sub_batch(self, h, a, b, d, n, limbs):
+        self.log.append(self._head("sub", limbs, False) + self._refs(a, n) + self._refs(b, n) + self._refs(d, n))
+        return 0
+
+    def afhe_eval_add_plain_batch(self, h, a, pt, d, n, limbs):
+        self.log.append(self._head("add_plain", limbs, False) + self._refs(a, n) + self._words(pt, n)
+                        + self._refs(d, n))
+        return 0
+
     def afhe_eval_copy_batch(self, h, a, d, n, limbs):
         self.log.append(self._head("copy", limbs, False) + self._refs(a, n) + self._refs(d, n))
         return 0
@@ -167,6 +176,10 @@ def build_manager(rng, *, D, n_list, slots, L_top, lanes, compaction, eval_level
             out.append((next(nxt), cnt, list(range(vid, vid + cnt))))
             vid += cnt
         m.batches.append(out)
+    m._first_batch = np.concatenate([[0], np.cumsum([len(b) for b in m.batches])]).astype(int).tolist()
+    nb = m._first_batch[-1]
+    # packed chain: the candidates' norm plaintexts per level (expanded distances)
+    m._norms = {lv: [next(nxt) for _ in range(nb)] for lv in m.levels} if compaction == "packed" else {}
     m.work = [dict(diff=(next(nxt), next(nxt)), sq=(next(nxt), next(nxt)), tmp=(next(nxt), next(nxt)),
                    sel=(next(nxt), next(nxt))) for _ in range(lanes)]
     m.cmp = ([[(next(nxt), next(nxt)) for _ in range(n_list - 1)] for _ in range(lanes)]
@@ -179,7 +192,8 @@ def build_manager(rng, *, D, n_list, slots, L_top, lanes, compaction, eval_level
     for i in range(6):
         res = [(next(nxt), next(nxt)) for _ in range(m.n_res)]
         recs.append(QueryRecord((next(nxt), next(nxt)), (next(nxt), next(nxt)), (next(nxt), next(nxt)), res[0],
-                                results=res, level=int(rng.choice([0] + list(levels)))))
+                                results=res, level=int(rng.choice([0] + list(levels))),
+                                norm=(next(nxt), next(nxt)) if compaction == "packed" else None))
     for r in recs:
         r.probes = [int(c) for c in rng.choice(n_list, size=int(rng.integers(1, 4)), replace=False)]
     return m, recs
