@@ -142,11 +142,12 @@ def profile_ks(lanes: int, workload: str = "small", level: int = 0, ept: int = 8
                                  choice=KsChoice(True, lanes, 0.0, ept, slc))))
 
 
-def profile_step(nq: int, workload: str = "small", lanes: int = 0):
-    """One warm step, then one measured step of `nq` queries. Prints the
+def profile_step(nq: int, workload: str = "small", lanes: int = 0, tune: bool = False):
+    """One warm step, then one measured step of `nq` queries (with `tune`,
+    under the autotuner's options, as the benchmark runs). Prints the
     kernel-launch counts an ncu launch list needs (-s / -c)."""
     from .workloads import LARGE, SMALL, Workload
-    wl = Workload(LARGE if workload == "large" else SMALL, max_queries=nq, lanes=lanes or nq)
+    wl = Workload(LARGE if workload == "large" else SMALL, max_queries=nq, lanes=lanes or nq, tune=tune)
     lib = wl.ctx.lib
     recs = wl.records[:nq]
     wl.encrypt_queries(wl.queries(nq, seed=7), recs)
@@ -340,6 +341,7 @@ def main() -> None:
     a.add_argument("queries", type=int)
     a.add_argument("--workload", default="small", choices=["small", "large"])
     a.add_argument("--lanes", type=int, default=0)
+    a.add_argument("--tune", action="store_true", help="the autotuner's key-switch options (as the benchmark)")
     sub.add_parser("host", help="end-to-end phases and the streamed run's host hotspots")
     a = sub.add_parser("dispatch", help="afhe_dispatch cost per call and op code")
     a.add_argument("--calls", type=int, default=200)
@@ -349,7 +351,7 @@ def main() -> None:
     elif args.what == "ntt":
         profile_ntt(args.polys, args.log_n)
     elif args.what == "step":
-        profile_step(args.queries, args.workload, args.lanes)
+        profile_step(args.queries, args.workload, args.lanes, args.tune)
     elif args.what == "dispatch":
         profile_dispatch(args.calls)
     else:
