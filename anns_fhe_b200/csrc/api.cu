@@ -25,6 +25,10 @@ int fail(afhe_ctx* ctx, int code, const std::string& msg) {
 }
 
 int cuda_fail(afhe_ctx* ctx, cudaError_t e, const char* where) {
+    // a failed runtime call (an out-of-memory cudaMalloc, say) also records
+    // its error as the thread's last error: clear it here, or the launch
+    // check of the next, unrelated call (cudaGetLastError) reports it again
+    (void)cudaGetLastError();
     return fail(ctx, AFHE_E_CUDA, std::string(where) + ": " + cudaGetErrorString(e));
 }
 

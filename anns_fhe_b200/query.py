@@ -62,6 +62,10 @@ from .driver import FheContext, FHEHostDriver, galois_elt
 from .ivfpq import IvfPqIndex
 
 MAX_LANES = 4096
+# HBM for the packed chain's candidate-norm plaintexts (the expanded distance):
+# (l - 1) N words per candidate batch and evaluation level l. Levels are
+# prepared lowest first while they fit; the rest square the difference.
+NORM_BUDGET_BYTES = 32 << 30
 
 
 @dataclass
@@ -144,10 +148,12 @@ class InteractiveQueryManager:
     restricted to its first l limbs is the same plaintext at level l. Masks
     are encoded per level, at scale q_{l-2}, the prime the mask rescale drops.
     `levels` lists the query levels to prepare masks for (default: L only).
-    `max_nprobe` sizes the result ciphertexts (default: the shape's nprobe)."""
+    `max_nprobe` sizes the result ciphertexts (default: the shape's nprobe).
+    `norm_budget`: bytes of candidate-norm plaintexts (packed chain) the
+    slots hold room for (default NORM_BUDGET_BYTES)."""
 
     def __init__(self, ctx: FheContext, index: IvfPqIndex, shape: QueryShape, slots: Slots, lanes: int = MAX_LANES,
-                 levels=None, max_nprobe: int | None = None, native: bool = True):
+                 levels=None, max_nprobe: int | None = None, native: bool = True, norm_budget: int | None = None):
         self.ctx, self.index, self.sh = ctx, index, shape
         self.native = native
         self._nh, self._nh_key, self._nh_ver = None, None, 0
@@ -224,6 +230,7 @@ class InteractiveQueryManager:
         # packed chain: the candidates' squared norms per level, for the
         # expanded distance ||q||^2 - 2 <q, x_j> + ||x_j||^2
         self._norms: dict[int, list[int]] = {}
+        self._norm_left = (NORM_BUDGET_BYTES if norm_budget is None else norm_budget) // 8
         if shape.compaction == "packed":
             for lv in self.levels:
                 self._norm_plaintexts(lv)
@@ -269,10 +276,15 @@ class InteractiveQueryManager:
     def _norm_plaintexts(self, lv: int) -> None:
         """The candidate batches' squared norms at level lv - 1, scale
         Delta^2 / q_{lv-1} (the scale of <q, x_j> and ||q||^2 after their
-        rescale), packed back to back."""
+        rescale), packed back to back. A level they do not fit the budget
+        for keeps the unexpanded distance (the square of the difference)."""
         nb = len(self._bcnt)
         w1 = (lv - 1) * self.p.n
-        base = self.slots.take(self.norm_plaintext_slots(nb, lv, self.p.n, self.slots.w))[0] if nb else 0
+        k = self.norm_plaintext_slots(nb, lv, self.p.n, self.slots.w)
+        if k * self.slots.w > self._norm_left:
+            return
+        self._norm_left -= k * self.slots.w
+        base = self.slots.take(k)[0] if nb else 0
         offs = [base + b * w1 for b in range(nb)]
         if nb:
             encode_index_batches(self.ctx, self.index, self._bvids, self._bfirst, self._bcnt, offs,
@@ -412,6 +424,20 @@ class InteractiveQueryManager:
         """Slots of one level's candidate-norm plaintexts (at most L - 1 limbs
         each), packed back to back."""
         return -(-batches * (L - 1) * n // slot_w)
+
+    @classmethod
+    def norm_reserve_slots(cls, levels, spare: int, batches: int, L: int, n: int, slot_w: int,
+                           budget: int = NORM_BUDGET_BYTES) -> int:
+        """Slots to reserve for the candidate norms of the evaluation `levels`
+        (lowest first) and `spare` more levels (any up to L), within `budget`
+        bytes: what a manager given norm_budget = slots * slot_w * 8 takes."""
+        cap, total = budget // 8 // slot_w, 0
+        for lv in sorted(levels) + [L] * spare:
+            k = cls.norm_plaintext_slots(batches, lv, n, slot_w)
+            if total + k > cap:
+                break
+            total += k
+        return total
 
     def alloc_queries(self, count: int) -> list[QueryRecord]:
         """Records whose results (compacted coarse distances; n_res candidate

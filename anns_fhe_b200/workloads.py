@@ -19,7 +19,7 @@ import numpy as np
 from .ckks import CkksClient, Slots
 from .driver import CkksParams, FheContext
 from .ivfpq import IvfPqIndex, gaussian_mixture, plaintext_coarse, plaintext_search
-from .query import InteractiveQueryManager, QueryRecord, QueryShape
+from .query import NORM_BUDGET_BYTES, InteractiveQueryManager, QueryRecord, QueryShape
 
 
 @dataclass
@@ -120,12 +120,14 @@ def ranked_prefix(vals: np.ndarray, pos, k: int) -> list[np.ndarray]:
 class Workload:
     def __init__(self, spec: WorkloadSpec = SMALL, max_queries: int = 64, lanes: int = 64, device: int = 0,
                  index: IvfPqIndex | None = None, levels=None, max_nprobe: int | None = None,
-                 tune: bool = False, spare_levels: int = 0):
+                 tune: bool = False, spare_levels: int = 0, norm_budget: int = NORM_BUDGET_BYTES):
         """levels: query levels to serve besides the top one (mixed-level
         traffic); max_nprobe: the most lists one query may probe; tune: apply
         the autotuner's key-switch choices (cached per GPU and parameter
         set, measured when absent); spare_levels: room for the masks of that
-        many more evaluation levels (InteractiveQueryManager.set_eval_level)."""
+        many more evaluation levels (InteractiveQueryManager.set_eval_level);
+        norm_budget: HBM bytes for the packed chain's candidate norms (levels
+        beyond it evaluate the unexpanded distance)."""
         self.spec = spec
         t0 = time.time()
         self.X = gaussian_mixture(spec.n_vectors, spec.d, spec.components, spec.sigma, spec.seed)
@@ -150,11 +152,12 @@ class Workload:
         dec_slots = -(-most * 2 * n // slot_w) + -(-most * n // slot_w)
         outbox_slots = -(-2 * max_queries * w_out // slot_w) + -(-2 * max_queries * n_res * w_out // slot_w)
         masks = InteractiveQueryManager.mask_slots(shape, len(lvls) + spare_levels, spec.compaction == "reference")
-        norm_slots = 0
+        norm_slots = norm_reserve = 0
         if spec.compaction == "packed":     # ||q||^2 scratch per query; the candidates' norms per level
-            norm_slots = (InteractiveQueryManager.norm_slots(max_queries, self.params.L, n, slot_w)
-                          + (len(lvls) + spare_levels)
-                          * InteractiveQueryManager.norm_plaintext_slots(n_batches, self.params.L, n, slot_w))
+            evl = sorted({min(x, spec.eval_level or x) for x in lvls})
+            norm_reserve = InteractiveQueryManager.norm_reserve_slots(evl, spare_levels, n_batches, self.params.L,
+                                                                      n, slot_w, norm_budget)
+            norm_slots = InteractiveQueryManager.norm_slots(max_queries, self.params.L, n, slot_w) + norm_reserve
         n_slots = (16 + shape.n_coarse + masks + n_batches + 8 * lanes + 4 * max_queries + outbox_slots + 64
                    + InteractiveQueryManager.compaction_slots(spec.n_list if spec.compaction == "reference" else 1,
                                                               self.params.L, n, slot_w, lanes)
@@ -165,7 +168,7 @@ class Workload:
         self.slots = Slots(self.params, 0, n_slots * slot_w)
         self.client = CkksClient(self.ctx, self.slots, seed=spec.seed + 7)
         self.iqm = InteractiveQueryManager(self.ctx, self.index, shape, self.slots, lanes=lanes, levels=lvls,
-                                           max_nprobe=most_probes)
+                                           max_nprobe=most_probes, norm_budget=norm_reserve * slot_w * 8)
         self.tuning = None
         if tune:
             from .autotune import load_or_tune

@@ -5,7 +5,7 @@ import numpy as np
 
 from anns_fhe_b200.ckks import Encoder, crt_centered, to_rns
 from anns_fhe_b200.ivfpq import IvfPqIndex, gaussian_mixture, plaintext_search
-from anns_fhe_b200.query import pow2_steps
+from anns_fhe_b200.query import InteractiveQueryManager, pow2_steps
 
 
 def coef_automorphism(coef: np.ndarray, k: int) -> np.ndarray:
@@ -117,3 +117,22 @@ def test_decode_real_matches_decode():
     sc = np.array([1.0, 2.0, 4.0, 8.0, 16.0]) * 2.0**30
     got = e.decode_real_batch(coef, sc, 8)
     assert np.allclose(got * sc[:, None] / 2.0**30, e.decode_real_batch(coef, 2.0**30, 8), rtol=0, atol=1e-9)
+
+
+def test_norm_reserve_within_budget():
+    """The candidate-norm plaintexts of the packed chain: levels lowest first,
+    then the spare levels at L, while their slots fit the budget; the large
+    configuration (7,813 batches, N = 2^15, L = 12, slots of 16 N words)."""
+    from anns_fhe_b200.query import NORM_BUDGET_BYTES
+    IQM = InteractiveQueryManager
+    n, L, nb = 1 << 15, 12, 7813
+    w = 16 * n
+    per = {lv: IQM.norm_plaintext_slots(nb, lv, n, w) for lv in range(3, L + 1)}
+    assert per[3] == -(-nb * 2 // 16) and per[12] == -(-nb * 11 // 16)
+    # evaluation at 3 limbs, plus one spare level for the full-level leg
+    assert IQM.norm_reserve_slots([3], 1, nb, L, n, w) == per[3] + per[12]
+    # query levels 6..12 at their own level: 6 and 7 fit 32 GiB, 8 does not
+    r = IQM.norm_reserve_slots(range(6, 13), 0, nb, L, n, w)
+    assert r == per[6] + per[7] and (r + per[8]) * w * 8 > NORM_BUDGET_BYTES >= r * w * 8
+    assert IQM.norm_reserve_slots([3], 0, nb, L, n, w, budget=0) == 0
+    assert IQM.norm_reserve_slots([], 0, nb, L, n, w) == 0

@@ -277,6 +277,23 @@ def test_options_and_limits(ed):
         assert top.get_option(L.OPT_CHUNK) == 4096
 
 
+def test_out_of_memory_leaves_later_calls_clean(ed):
+    """An arena larger than the GPU's memory fails afhe_ctx_create with a CUDA
+    status (cudaMalloc's out of memory, no fault); the next context's first
+    launches do not report that stale error."""
+    small = CkksParams(10, ed.prm.q[:2], ed.prm.p[:1], 1)
+    with pytest.raises(L.AfheError) as ei:
+        FheContext(small, poly_words=1 << 40, key_words=1 << 12)      # 8 TiB
+    assert ei.value.status == L.E_CUDA and "out of memory" in str(ei.value)
+    with FheContext(small, poly_words=1 << 14, key_words=1 << 12) as c:
+        x = uniform_residues(np.random.default_rng(5), small.q[:2], small.n)
+        c.write_poly(0, x)
+        d = FHEHostDriver(c)
+        d.ntt(0, 2 * small.n, 2)
+        d.intt(2 * small.n, 4 * small.n, 2)
+        assert np.array_equal(c.read_poly(4 * small.n, 2 * small.n), x)
+
+
 def test_fences_and_asynchronous_rows(ed):
     lib, h, n = ed.lib, ed.h, ed.n
     c = ed.ct(NQ)
