@@ -70,6 +70,17 @@ class CtRef(C.Structure):
     _fields_ = [("c0_offset", u64), ("c1_offset", u64)]
 
 
+class MacTerm(C.Structure):
+    _fields_ = [("pt", C.c_uint64), ("galois", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class MacGroup(C.Structure):
+    _fields_ = [("src", CtRef), ("first_term", C.c_uint32), ("n_terms", C.c_uint32)]
+
+
+MAC_UNIT = (1 << 64) - 1
+
+
 class PqIndex(C.Structure):
     _fields_ = [("n_list", u32), ("d", u32), ("M", u32), ("K", u32), ("n", u64),
                 ("centroids", C.POINTER(C.c_float)), ("codebooks", C.POINTER(C.c_float)),
@@ -167,12 +178,16 @@ SIGNATURES = {
     "afhe_automorphism_from_map": (C.c_int, [CTX, u64, u64, u64, u32, u32]),
     "afhe_automorphism_batch": (C.c_int, [CTX, P64, P32, P64, u32, u32]),
     "afhe_eval_sub_batch": (C.c_int, [CTX, C.POINTER(CtRef), C.POINTER(CtRef), C.POINTER(CtRef), u32, u32]),
+    "afhe_eval_mac_plain_batch": (C.c_int, [CTX, C.POINTER(CtRef), P32, u32, C.POINTER(MacGroup), C.POINTER(MacTerm),
+                                            u32, u32]),
     "afhe_eval_add_plain_batch": (C.c_int, [CTX, C.POINTER(CtRef), P64, C.POINTER(CtRef), u32, u32]),
     "afhe_encode_batch": (C.c_int, [CTX, C.POINTER(C.c_double), u32, u32, C.c_double, u32, P64]),
     "afhe_pq_create": (C.c_int, [CTX, C.POINTER(PqIndex), C.POINTER(C.c_void_p)]),
     "afhe_pq_destroy": (C.c_int, [C.c_void_p]),
     "afhe_pq_encode_batches": (C.c_int, [C.c_void_p, P32, P32, P32, u32, C.c_double, u32, P64]),
     "afhe_pq_encode_norms": (C.c_int, [C.c_void_p, P32, P32, P32, u32, C.c_double, u32, P64]),
+    "afhe_pq_encode_diagonals": (C.c_int, [C.c_void_p, P32, P32, P32, u32, u32, C.c_double, C.c_double, u32, P64]),
+    "afhe_pq_encode_unit_norms": (C.c_int, [C.c_void_p, P32, P32, P32, u32, C.c_double, u32, P64]),
     "afhe_ivfpq_create": (C.c_int, [CTX, C.POINTER(IvfpqShape), C.POINTER(C.c_void_p)]),
     "afhe_ivfpq_destroy": (C.c_int, [C.c_void_p]),
     "afhe_ivfpq_set_centroids": (C.c_int, [C.c_void_p, P64, u32]),

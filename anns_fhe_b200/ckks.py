@@ -426,12 +426,15 @@ def encode_plaintexts(ctx: FheContext, enc: Encoder, values: np.ndarray, scale: 
 
 
 def encode_index_batches(ctx: FheContext, index, vids, first, counts, offs, scale: float, level: int,
-                         norms: bool = False) -> None:
+                         norms: bool = False, layout: str = "batches", n1: int = 0, coef: float = 1.0) -> None:
     """The stage-3 candidate plaintexts built and encoded on the device
     (afhe_pq_*): batch b holds candidates vids[first[b] .. first[b] +
     counts[b]); slot d B + j = component d of candidate j's reconstruction
     (centroid of its list + its PQ codewords). With `norms`, the batches'
-    squared norms instead: slot d B + j = ||x_j||^2 in every row d."""
+    squared norms instead: slot d B + j = ||x_j||^2 in every row d.
+    layout "diagonals": the diagonal method's D plaintexts per unit (of up to
+    N/2 candidates) into offs[u D + i] (afhe_pq_encode_diagonals, n1 baby
+    steps, values times coef); "unit_norms": slot j = ||x_j||^2 per unit."""
     from . import _lib as L
     cent = np.ascontiguousarray(index.centroids, dtype=np.float32)
     books = np.ascontiguousarray(index.codebooks, dtype=np.float32)
@@ -448,9 +451,17 @@ def encode_index_batches(ctx: FheContext, index, vids, first, counts, offs, scal
         f = np.ascontiguousarray(first, dtype=np.uint32)
         c = np.ascontiguousarray(counts, dtype=np.uint32)
         o = np.ascontiguousarray(offs, dtype=np.uint64)
-        fn = ctx.lib.afhe_pq_encode_norms if norms else ctx.lib.afhe_pq_encode_batches
-        L.check(fn(h, v.ctypes.data_as(L.P32), f.ctypes.data_as(L.P32), c.ctypes.data_as(L.P32), o.size,
-                   float(scale), level, o.ctypes.data_as(L.P64)), "pq_encode")
+        args = (v.ctypes.data_as(L.P32), f.ctypes.data_as(L.P32), c.ctypes.data_as(L.P32))
+        if layout == "diagonals":
+            assert o.size == c.size * cent.shape[1]
+            L.check(ctx.lib.afhe_pq_encode_diagonals(h, *args, c.size, n1, float(coef), float(scale), level,
+                                                     o.ctypes.data_as(L.P64)), "pq_encode_diagonals")
+        elif layout == "unit_norms":
+            L.check(ctx.lib.afhe_pq_encode_unit_norms(h, *args, c.size, float(scale), level,
+                                                      o.ctypes.data_as(L.P64)), "pq_encode_unit_norms")
+        else:
+            fn = ctx.lib.afhe_pq_encode_norms if norms else ctx.lib.afhe_pq_encode_batches
+            L.check(fn(h, *args, o.size, float(scale), level, o.ctypes.data_as(L.P64)), "pq_encode")
     finally:
         ctx.lib.afhe_pq_destroy(h)
 

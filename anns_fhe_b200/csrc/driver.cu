@@ -59,6 +59,28 @@ int check_cts(afhe_ctx* ctx, const afhe_ct_ref* v, uint32_t count, uint32_t limb
     return AFHE_OK;
 }
 
+// The device copy of the evaluation-form automorphism map of `galois`
+// (computed on first use, kept until the context is destroyed).
+int cached_map(afhe_ctx* ctx, uint32_t galois, const uint32_t** out) {
+    auto it = ctx->auto_maps.find(galois);
+    if (it != ctx->auto_maps.end()) {
+        *out = it->second;
+        return AFHE_OK;
+    }
+    std::vector<uint32_t> map(ctx->n);
+    automorphism_map(ctx->log_n, galois, map.data());
+    uint32_t* d = nullptr;
+    CK(cudaMalloc(&d, (size_t)ctx->n * sizeof(uint32_t)));
+    cudaError_t e = cudaMemcpy(d, map.data(), (size_t)ctx->n * sizeof(uint32_t), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+        cudaFree(d);
+        return cuda_fail(ctx, e, "automorphism map upload");
+    }
+    ctx->auto_maps[galois] = d;
+    *out = d;
+    return AFHE_OK;
+}
+
 #define ZF(dst, vec)                                                                    \
     do {                                                                                \
         int _rc = zf_from(ctx, (vec).data(), (uint32_t)(vec).size(), &(dst));           \
@@ -782,19 +804,10 @@ int afhe_automorphism_batch(afhe_ctx* ctx, const uint64_t* src, const uint32_t* 
         else --open_dst;
         if (open_src > 0 && open_dst > 0) return fail(ctx, AFHE_E_ARG, "a destination overlaps a source");
     }
-    for (uint32_t i = 0; i < count; ++i)
-        if (!ctx->auto_maps.count(galois[i])) {
-            std::vector<uint32_t> map(ctx->n);
-            automorphism_map(ctx->log_n, galois[i], map.data());
-            uint32_t* d = nullptr;
-            CK(cudaMalloc(&d, (size_t)ctx->n * sizeof(uint32_t)));
-            cudaError_t e = cudaMemcpy(d, map.data(), (size_t)ctx->n * sizeof(uint32_t), cudaMemcpyHostToDevice);
-            if (e != cudaSuccess) {
-                cudaFree(d);
-                return cuda_fail(ctx, e, "automorphism map upload");
-            }
-            ctx->auto_maps[galois[i]] = d;
-        }
+    for (uint32_t i = 0; i < count; ++i) {
+        const uint32_t* d = nullptr;
+        if ((rc = cached_map(ctx, galois[i], &d))) return rc;
+    }
     return for_chunks(ctx, count, [&](uint32_t s, uint32_t m) {
         Offs S(m), D(m), M(m);
         for (uint32_t z = 0; z < m; ++z) {
@@ -810,6 +823,106 @@ int afhe_automorphism_batch(afhe_ctx* ctx, const uint64_t* src, const uint32_t* 
         CK(launch_automorphism_z(maps, ctx->poly, ctx->n, limbs, m, zb, ctx->st));
         return (int)AFHE_OK;
     });
+}
+
+int afhe_eval_mac_plain_batch(afhe_ctx* ctx, const afhe_ct_ref* out, const uint32_t* first_group, uint32_t count,
+                              const afhe_mac_group* groups, const afhe_mac_term* terms, uint32_t limbs,
+                              uint32_t accumulate) {
+    if (!ctx || (count && (!out || !first_group || !groups || !terms))) return fail(ctx, AFHE_E_ARG, "null argument");
+    int rc;
+    if ((rc = check_limbs(ctx, limbs, 1)) || (rc = check_cts(ctx, out, count, limbs))) return rc;
+    const u64 w = (u64)limbs * ctx->n;
+    // interval ends: operands read (+1 / -1) and outputs (+2 / -2); an output
+    // may overlap nothing else of the call (its own accumulation is read in place)
+    std::vector<std::pair<u64, int>> ends;
+    auto read = [&](u64 off) {
+        ends.push_back({off, 1});
+        ends.push_back({off + w, -1});
+    };
+    for (uint32_t j = 0; j < count; ++j) {
+        if (first_group[j + 1] < first_group[j]) return fail(ctx, AFHE_E_ARG, "group ranges must not decrease");
+        for (uint32_t g = first_group[j]; g < first_group[j + 1]; ++g) {
+            const afhe_mac_group& G = groups[g];
+            if (G.src.c0_offset != AFHE_MAC_UNIT) {
+                if ((rc = check_poly(ctx, G.src.c0_offset, limbs)) || (rc = check_poly(ctx, G.src.c1_offset, limbs)))
+                    return rc;
+                read(G.src.c0_offset);
+                read(G.src.c1_offset);
+            }
+            for (uint32_t t = G.first_term; t < G.first_term + G.n_terms; ++t) {
+                if ((rc = check_poly(ctx, terms[t].pt, limbs))) return rc;
+                if ((terms[t].galois & 1u) == 0 || terms[t].galois >= 2 * ctx->n)
+                    return fail(ctx, AFHE_E_ARG, "galois element must be odd and < 2N");
+                read(terms[t].pt);
+            }
+        }
+        ends.push_back({out[j].c0_offset, 2});
+        ends.push_back({out[j].c0_offset + w, -2});
+        ends.push_back({out[j].c1_offset, 2});
+        ends.push_back({out[j].c1_offset + w, -2});
+    }
+    std::sort(ends.begin(), ends.end());
+    int open_src = 0, open_dst = 0;
+    for (const auto& e : ends) {
+        if (e.second == 1) ++open_src;
+        else if (e.second == -1) --open_src;
+        else if (e.second == 2) ++open_dst;
+        else --open_dst;
+        if (open_dst > 1 || (open_src > 0 && open_dst > 0))
+            return fail(ctx, AFHE_E_ARG, "an output overlaps another output or an operand");
+    }
+    // terms between folds of the 128-bit accumulators: each product < q^2
+    u64 qmax = 0;
+    for (uint32_t l = 0; l < limbs; ++l) qmax = std::max<u64>(qmax, ctx->prm.q[l]);
+    const unsigned __int128 sq = (unsigned __int128)(qmax - 1) * (qmax - 1);
+    const unsigned __int128 room = ~(unsigned __int128)0 / (sq ? sq : 1);
+    const uint32_t reduce_every = room > 0x7fffffff ? 0x7fffffffu : (uint32_t)room;
+    // launches of whole jobs whose descriptors fit one segment of the ring
+    const size_t seg = ctx->ring.seg_words - 96;
+    std::vector<MacJob> J;
+    std::vector<MacGroup> G;
+    std::vector<MacTerm> T;
+    auto words = [&](size_t j, size_t g, size_t t) {
+        return (j * sizeof(MacJob) + g * sizeof(MacGroup) + t * sizeof(MacTerm)) / sizeof(u64);
+    };
+    auto flush = [&]() -> int {
+        if (J.empty()) return AFHE_OK;
+        u64 *dj = nullptr, *dg = nullptr, *dt = nullptr;
+        int r;
+        if ((r = ring_put(ctx, J.data(), J.size() * sizeof(MacJob) / sizeof(u64), &dj))) return r;
+        if ((r = ring_put(ctx, G.data(), std::max<size_t>(G.size(), 1) * sizeof(MacGroup) / sizeof(u64), &dg)))
+            return r;
+        if ((r = ring_put(ctx, T.data(), std::max<size_t>(T.size(), 1) * sizeof(MacTerm) / sizeof(u64), &dt)))
+            return r;
+        CK(launch_mac_plain(ctx->nat.pc, ctx->poly, ctx->n, limbs, (uint32_t)J.size(), (const MacJob*)dj,
+                            (const MacGroup*)dg, (const MacTerm*)dt, reduce_every, accumulate ? 1 : 0, ctx->st));
+        J.clear();
+        G.clear();
+        T.clear();
+        return AFHE_OK;
+    };
+    G.reserve(1);
+    T.reserve(1);
+    for (uint32_t j = 0; j < count; ++j) {
+        size_t ng = first_group[j + 1] - first_group[j], nt = 0;
+        for (uint32_t g = first_group[j]; g < first_group[j + 1]; ++g) nt += groups[g].n_terms;
+        if (words(1, std::max<size_t>(ng, 1), std::max<size_t>(nt, 1)) > seg / 3)
+            return fail(ctx, AFHE_E_ARG, "too many terms in one output for the descriptor ring");
+        if (words(J.size() + 1, G.size() + ng + 1, T.size() + nt + 1) > seg / 3 && (rc = flush())) return rc;
+        MacJob mj{out[j].c0_offset, out[j].c1_offset, (uint32_t)G.size(), (uint32_t)(G.size() + ng)};
+        J.push_back(mj);
+        for (uint32_t g = first_group[j]; g < first_group[j + 1]; ++g) {
+            const afhe_mac_group& src = groups[g];
+            MacGroup mg{src.src.c0_offset, src.src.c1_offset, (uint32_t)T.size(), (uint32_t)(T.size() + src.n_terms)};
+            G.push_back(mg);
+            for (uint32_t t = src.first_term; t < src.first_term + src.n_terms; ++t) {
+                const uint32_t* map = nullptr;
+                if (terms[t].galois != 1 && (rc = cached_map(ctx, terms[t].galois, &map))) return rc;
+                T.push_back(MacTerm{terms[t].pt, map});
+            }
+        }
+    }
+    return flush();
 }
 
 int afhe_eval_copy_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const afhe_ct_ref* d, uint32_t count, uint32_t limbs) {

@@ -223,13 +223,14 @@ __global__ void fft_load_pq(double2* __restrict__ v, uint32_t s, uint32_t dim, u
 // The candidates' squared norms, slot d B + j = ||x_j||^2 for every row d
 // (x_j the reconstruction of the batch's candidate j), 0 past the count: the
 // plaintext the expanded distance ||q||^2 - 2 <q, x_j> + ||x_j||^2 adds after
-// the tree sum has left its other two terms in every row.
+// the tree sum has left its other two terms in every row. With B = N/2 (one
+// row) slot j = ||x_j||^2: a unit of the diagonal method.
 __global__ void fft_load_pq_norms(double2* __restrict__ v, uint32_t s, uint32_t dim, uint32_t M, uint32_t K,
                                   const float* __restrict__ cent, const float* __restrict__ cb,
                                   const uint8_t* __restrict__ codes, const uint32_t* __restrict__ assign,
                                   const uint32_t* __restrict__ vids, const uint32_t* __restrict__ first,
-                                  const uint32_t* __restrict__ cnt, uint32_t count) {
-    const uint32_t B = s / dim, sd = dim / M;
+                                  const uint32_t* __restrict__ cnt, uint32_t B, uint32_t count) {
+    const uint32_t sd = dim / M;
     const u64 total = (u64)count * s;
     for (u64 t = blockIdx.x * (u64)blockDim.x + threadIdx.x; t < total; t += (u64)gridDim.x * blockDim.x) {
         const uint32_t z = (uint32_t)(t / s), j = (uint32_t)(t % s) % B;
@@ -246,6 +247,35 @@ __global__ void fft_load_pq_norms(double2* __restrict__ v, uint32_t s, uint32_t 
             }
         }
         v[t] = make_double2(x2, 0.0);
+    }
+}
+
+// The diagonals of a unit of up to N/2 candidates (the diagonal method's
+// plaintexts): plaintext i = g n1 + b of unit z, slot k, holds coef x_j[(j +
+// i) mod dim] for the candidate j = (k - n1 g) mod (N/2) of the unit (0 past
+// its count). That is diagonal i of the (candidates x dim) matrix, whose
+// slot j multiplies slot j of the query rotated by i, pre-rotated by -n1 g
+// for the giant step that brings it back.
+__global__ void fft_load_pq_diag(double2* __restrict__ v, uint32_t s, uint32_t dim, uint32_t M, uint32_t K,
+                                 const float* __restrict__ cent, const float* __restrict__ cb,
+                                 const uint8_t* __restrict__ codes, const uint32_t* __restrict__ assign,
+                                 const uint32_t* __restrict__ vids, const uint32_t* __restrict__ first,
+                                 const uint32_t* __restrict__ cnt, uint32_t n1, double coef, uint32_t pt0,
+                                 uint32_t count) {
+    const uint32_t sd = dim / M;
+    const u64 total = (u64)count * s;
+    for (u64 t = blockIdx.x * (u64)blockDim.x + threadIdx.x; t < total; t += (u64)gridDim.x * blockDim.x) {
+        const uint32_t z = pt0 + (uint32_t)(t / s), slot = (uint32_t)(t % s);
+        const uint32_t unit = z / dim, i = z % dim, g = i / n1;
+        const uint32_t j = (slot + s - (n1 * g) % s) % s;
+        double x = 0.0;
+        if (j < cnt[unit]) {
+            const uint32_t id = vids[first[unit] + j];
+            const uint32_t d = (j + i) % dim, m = d / sd;
+            x = coef * ((double)cent[(u64)assign[id] * dim + d] +
+                        (double)cb[((u64)m * K + codes[(u64)id * M + m]) * sd + (d - m * sd)]);
+        }
+        v[t] = make_double2(x, 0.0);
     }
 }
 
@@ -393,34 +423,51 @@ int afhe_pq_destroy(afhe_pq* p) {
 }
 
 namespace {
+enum PqLayout { PQ_BATCHES, PQ_NORMS, PQ_DIAGONALS, PQ_UNIT_NORMS };
 int pq_encode(afhe_pq* p, const uint32_t* vids, const uint32_t* first, const uint32_t* cnt, uint32_t batches,
-              double scale, uint32_t level, const uint64_t* pt, bool norms);
+              double scale, uint32_t level, const uint64_t* pt, PqLayout layout, uint32_t n1 = 0, double coef = 1.0);
 }
 
 int afhe_pq_encode_batches(afhe_pq* p, const uint32_t* vids, const uint32_t* first, const uint32_t* cnt,
                            uint32_t batches, double scale, uint32_t level, const uint64_t* pt) {
-    return pq_encode(p, vids, first, cnt, batches, scale, level, pt, false);
+    return pq_encode(p, vids, first, cnt, batches, scale, level, pt, PQ_BATCHES);
 }
 
 int afhe_pq_encode_norms(afhe_pq* p, const uint32_t* vids, const uint32_t* first, const uint32_t* cnt,
                          uint32_t batches, double scale, uint32_t level, const uint64_t* pt) {
-    return pq_encode(p, vids, first, cnt, batches, scale, level, pt, true);
+    return pq_encode(p, vids, first, cnt, batches, scale, level, pt, PQ_NORMS);
+}
+
+int afhe_pq_encode_diagonals(afhe_pq* p, const uint32_t* vids, const uint32_t* first, const uint32_t* cnt,
+                             uint32_t units, uint32_t n1, double coef, double scale, uint32_t level,
+                             const uint64_t* pt) {
+    return pq_encode(p, vids, first, cnt, units, scale, level, pt, PQ_DIAGONALS, n1, coef);
+}
+
+int afhe_pq_encode_unit_norms(afhe_pq* p, const uint32_t* vids, const uint32_t* first, const uint32_t* cnt,
+                              uint32_t units, double scale, uint32_t level, const uint64_t* pt) {
+    return pq_encode(p, vids, first, cnt, units, scale, level, pt, PQ_UNIT_NORMS);
 }
 
 }  // extern "C"
 
 namespace {
 int pq_encode(afhe_pq* p, const uint32_t* vids, const uint32_t* first, const uint32_t* cnt, uint32_t batches,
-              double scale, uint32_t level, const uint64_t* pt, bool norms) {
+              double scale, uint32_t level, const uint64_t* pt, PqLayout layout, uint32_t n1, double coef) {
     if (!p) return fail(nullptr, AFHE_E_ARG, "null argument");
     afhe_ctx* ctx = p->ctx;
     if (batches && (!vids || !first || !cnt || !pt)) return fail(ctx, AFHE_E_ARG, "null argument");
     const uint32_t s = ctx->n / 2;
     if (p->d > s || s % p->d) return fail(ctx, AFHE_E_ARG, "the dimension must divide N/2");
-    const uint32_t B = s / p->d;
+    const bool unit = layout == PQ_DIAGONALS || layout == PQ_UNIT_NORMS;
+    const uint32_t B = unit ? s : s / p->d;
+    if (layout == PQ_DIAGONALS && (n1 == 0 || p->d % n1))
+        return fail(ctx, AFHE_E_ARG, "the baby steps must divide the dimension");
+    if (layout == PQ_DIAGONALS && !std::isfinite(coef)) return fail(ctx, AFHE_E_ARG, "coefficient must be finite");
     uint64_t total = 0;
     for (uint32_t b = 0; b < batches; ++b) {
-        if (cnt[b] > B) return fail(ctx, AFHE_E_ARG, "more candidates in a batch than N / 2d");
+        if (cnt[b] > B) return fail(ctx, AFHE_E_ARG, unit ? "more candidates in a unit than N / 2"
+                                                          : "more candidates in a batch than N / 2d");
         total = std::max<uint64_t>(total, (uint64_t)first[b] + cnt[b]);
     }
     std::vector<uint32_t> ids(vids, vids + total);
@@ -444,10 +491,14 @@ int pq_encode(afhe_pq* p, const uint32_t* vids, const uint32_t* first, const uin
         return cuda_fail(ctx, e, "batch upload");
     }
     auto load = [&](double2* v, uint32_t c0, uint32_t m) -> int {
-        if (norms)
+        if (layout == PQ_NORMS || layout == PQ_UNIT_NORMS)
             fft_load_pq_norms<<<grid_for((u64)m * s), 256, 0, ctx->st>>>(v, s, p->d, p->M, p->K, p->centroids,
                                                                          p->codebooks, p->codes, p->assign, vids_d,
-                                                                         first_d + c0, cnt_d + c0, m);
+                                                                         first_d + c0, cnt_d + c0, B, m);
+        else if (layout == PQ_DIAGONALS)       // plaintexts c0 .. c0 + m - 1 of units x dim
+            fft_load_pq_diag<<<grid_for((u64)m * s), 256, 0, ctx->st>>>(v, s, p->d, p->M, p->K, p->centroids,
+                                                                        p->codebooks, p->codes, p->assign, vids_d,
+                                                                        first_d, cnt_d, n1, coef, c0, m);
         else
             fft_load_pq<<<grid_for((u64)m * s), 256, 0, ctx->st>>>(v, s, p->d, p->M, p->K, p->centroids,
                                                                    p->codebooks, p->codes, p->assign, vids_d,
@@ -455,7 +506,12 @@ int pq_encode(afhe_pq* p, const uint32_t* vids, const uint32_t* first, const uin
         count_launches(1);
         return AFHE_OK;
     };
-    int rc = encode_pipeline(ctx, batches, scale, level, pt, load);
+    const uint64_t n_pts = layout == PQ_DIAGONALS ? (uint64_t)batches * p->d : batches;
+    if (n_pts > 0xffffffffull) {
+        release();
+        return fail(ctx, AFHE_E_ARG, "too many plaintexts in one call");
+    }
+    int rc = encode_pipeline(ctx, (uint32_t)n_pts, scale, level, pt, load);
     release();
     return rc;
 }

@@ -166,6 +166,29 @@ cudaError_t launch_automorphism(const uint32_t* map32, const u64* map64, u64* ar
 cudaError_t launch_automorphism_z(const ZField& maps, u64* arena, uint32_t n, uint32_t limbs, uint32_t nz,
                                   const ZBases& zb, cudaStream_t st);
 
+// Sums of plaintext-ciphertext products (afhe_eval_mac_plain_batch): job z
+// writes out = sum over its groups of sum over the group's terms of
+// pt[map[i]] * src (both polynomials), limbs l < limbs with prime l. A group
+// whose src0 is kMacUnit multiplies by the constant ciphertext (1, 0). Terms
+// are reduced once at the end (128-bit accumulators, folded every
+// reduce_every terms); accumulate adds the existing out.
+constexpr u64 kMacUnit = ~0ull;
+struct MacJob {
+    u64 out0, out1;
+    uint32_t g0, g1;
+};
+struct MacGroup {
+    u64 src0, src1;
+    uint32_t t0, t1;
+};
+struct MacTerm {
+    u64 pt;
+    const uint32_t* map;   // null: identity
+};
+cudaError_t launch_mac_plain(const PrimeConst* pc, u64* arena, uint32_t n, uint32_t limbs, uint32_t jobs,
+                             const MacJob* job, const MacGroup* group, const MacTerm* term, uint32_t reduce_every,
+                             int accumulate, cudaStream_t st);
+
 // Plain (I)NTT of `limbs` limbs laid out contiguously (limb i at +i*N), table
 // index prime0 + i. src arena -> dst arena, per-z offsets zb.src / zb.out.
 cudaError_t launch_ntt_plain(bool inverse, int log_n, const PrimeTables& pt, const LimbJob* jobs, uint32_t limbs,

@@ -150,6 +150,68 @@ cudaError_t launch_automorphism_z(const ZField& maps, u64* arena, uint32_t n, ui
 }
 
 // ---------------------------------------------------------------------------
+// sums of plaintext-ciphertext products, each plaintext read through its own
+// automorphism (the inner products of the diagonal method: a plaintext moved
+// by a slot rotation is a permutation of its evaluation-form coefficients)
+// ---------------------------------------------------------------------------
+AFHE_HD void acc_fold(Acc128& a, const ModConst& m) {
+    a.lo = acc_reduce(a, m);
+    a.hi = 0;
+}
+
+__global__ void __launch_bounds__(256) mac_plain_kernel(const PrimeConst* __restrict__ pc, u64* __restrict__ arena,
+                                                        uint32_t n, const MacJob* __restrict__ jobs,
+                                                        const MacGroup* __restrict__ groups,
+                                                        const MacTerm* __restrict__ terms, uint32_t reduce_every,
+                                                        int accumulate) {
+    const uint32_t l = blockIdx.y;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const MacJob J = jobs[blockIdx.z];
+    const ModConst m = modconst_of(pc[l]);
+    const u64 off = (u64)l * n + i;
+    Acc128 a0, a1;
+    acc_init(a0);
+    acc_init(a1);
+    uint32_t cnt = 0;
+    for (uint32_t g = J.g0; g < J.g1; ++g) {
+        const MacGroup G = groups[g];
+        const bool unit = G.src0 == kMacUnit;
+        const u64 x0 = unit ? 1 : arena[G.src0 + off];
+        const u64 x1 = unit ? 0 : arena[G.src1 + off];
+        for (uint32_t t = G.t0; t < G.t1; ++t) {
+            const MacTerm T = terms[t];
+            const uint32_t j = T.map ? __ldg(T.map + i) : i;
+            const u64 p = arena[T.pt + (u64)l * n + j];
+            acc_mad(a0, p, x0);
+            if (!unit) acc_mad(a1, p, x1);
+            if (++cnt == reduce_every) {
+                acc_fold(a0, m);
+                acc_fold(a1, m);
+                cnt = 1;
+            }
+        }
+    }
+    u64 r0 = acc_reduce(a0, m), r1 = acc_reduce(a1, m);
+    if (accumulate) {
+        r0 = add_mod(r0, arena[J.out0 + off], m.q);
+        r1 = add_mod(r1, arena[J.out1 + off], m.q);
+    }
+    arena[J.out0 + off] = r0;
+    arena[J.out1 + off] = r1;
+}
+
+cudaError_t launch_mac_plain(const PrimeConst* pc, u64* arena, uint32_t n, uint32_t limbs, uint32_t jobs,
+                             const MacJob* job, const MacGroup* group, const MacTerm* term, uint32_t reduce_every,
+                             int accumulate, cudaStream_t st) {
+    if (limbs == 0 || jobs == 0) return cudaSuccess;
+    dim3 grid((n + 255) / 256, limbs, jobs);
+    mac_plain_kernel<<<grid, 256, 0, st>>>(pc, arena, n, job, group, term, reduce_every, accumulate);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
 // plain transforms
 // ---------------------------------------------------------------------------
 cudaError_t launch_ntt_plain(bool inverse, int log_n, const PrimeTables& pt, const LimbJob* jobs, uint32_t limbs,

@@ -385,6 +385,35 @@ int afhe_eval_rotate_steps_batch(afhe_ctx* ctx, const afhe_ct_ref* in, const afh
  * source. Maps are computed on first use of an element and kept. */
 int afhe_automorphism_batch(afhe_ctx* ctx, const uint64_t* src, const uint32_t* galois, const uint64_t* dst,
                             uint32_t count, uint32_t limbs);
+/* Sums of plaintext-ciphertext products, each plaintext moved by its own
+ * Galois automorphism: the inner products of the diagonal (baby-step
+ * giant-step) method, sum_i diag_i * rot(ct, i). Each term is the two
+ * poly_mul_ntt products eval_mult_plain_rescale makes before its rescale
+ * (fhe_host_driver.cpp:308-317) with the plaintext first moved by
+ * FHEHostDriver::automorphism (:230-232); the terms are summed as eval_add
+ * does (:248-257). For each output j:
+ *   out[j] (+)= sum over groups g in [first_group[j], first_group[j + 1]) of
+ *               sum over terms t of g: automorphism(terms[t].pt, terms[t].galois) * groups[g].src
+ * (both polynomials, `limbs` limbs, evaluation form; galois 1 is the identity;
+ * a group whose src.c0_offset is AFHE_MAC_UNIT multiplies by the constant
+ * ciphertext (1, 0), i.e. adds its plaintexts to c0). The sums are reduced
+ * once, so the result is the exact residue of the sum of products: equal to
+ * eval_mult_plain without rescale on every term and eval_add of them all.
+ * With accumulate the existing out is added. No output may overlap another
+ * output or any operand. first_group has count + 1 entries. */
+#define AFHE_MAC_UNIT UINT64_MAX
+typedef struct afhe_mac_term {
+    uint64_t pt;        /* plaintext polynomial offset in poly_gmem */
+    uint32_t galois;    /* odd, < 2N; 1: no automorphism */
+    uint32_t reserved;
+} afhe_mac_term;
+typedef struct afhe_mac_group {
+    afhe_ct_ref src;     /* the ciphertext the group's plaintexts multiply */
+    uint32_t first_term, n_terms;
+} afhe_mac_group;
+int afhe_eval_mac_plain_batch(afhe_ctx* ctx, const afhe_ct_ref* out, const uint32_t* first_group, uint32_t count,
+                              const afhe_mac_group* groups, const afhe_mac_term* terms, uint32_t limbs,
+                              uint32_t accumulate);
 /* dst[i] = a[i] (both polynomials, `limbs` limbs): the slot-to-slot copies the
  * reference's host makes between operators (eval_sub_plain's c1 copy,
  * fhe_host_driver.cpp:259-270), for many ciphertexts in one launch. */
@@ -445,6 +474,19 @@ int afhe_pq_encode_batches(afhe_pq* pq, const uint32_t* vids, const uint32_t* fi
  * ||x_j||^2 adds after the tree sum). */
 int afhe_pq_encode_norms(afhe_pq* pq, const uint32_t* vids, const uint32_t* first, const uint32_t* count,
                          uint32_t batches, double scale, uint32_t level, const uint64_t* pt);
+/* The diagonal method's plaintexts of `units` units of up to N/2 candidates
+ * (unit u: vids[first[u] .. first[u] + count[u])): pt[u dim + i], i = g n1 + b
+ * (n1 divides dim), slot k = coef x_j[(j + i) mod dim] with j = (k - n1 g)
+ * mod N/2 the unit's candidate, 0 past the count. The sum over i of
+ * plaintext i times the query (repeated every dim slots) rotated by b, each
+ * giant-step group g rotated back by n1 g, leaves coef <q, x_j> in slot j. */
+int afhe_pq_encode_diagonals(afhe_pq* pq, const uint32_t* vids, const uint32_t* first, const uint32_t* count,
+                             uint32_t units, uint32_t n1, double coef, double scale, uint32_t level,
+                             const uint64_t* pt);
+/* The units' squared norms: slot j = ||x_j||^2 of the unit's candidate j, 0
+ * past the count, into pt[u]. */
+int afhe_pq_encode_unit_norms(afhe_pq* pq, const uint32_t* vids, const uint32_t* first, const uint32_t* count,
+                              uint32_t units, double scale, uint32_t level, const uint64_t* pt);
 
 /* ---- encrypted IVF-PQ server stages ---------------------------------------- */
 /* InteractiveQueryManager's server stages (cpp_host_model/src/
