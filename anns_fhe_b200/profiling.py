@@ -135,8 +135,8 @@ def profile_ks(lanes: int, workload: str = "small", level: int = 0, ept: int = 8
     level), the one-kernel key switch at `ept` values per thread."""
     from .autotune import KsChoice
     from .driver import CkksParams
-    from .workloads import LARGE, SMALL
-    spec = LARGE if workload == "large" else SMALL
+    from .workloads import WORKLOADS
+    spec = WORKLOADS[workload]
     p = CkksParams.generate(spec.log_n, spec.num_q, spec.q_bits, spec.num_p, spec.p_bits, spec.alpha)
     print(json.dumps(ks_roofline(p, lanes, level=level or spec.eval_level or spec.num_q,
                                  choice=KsChoice(True, lanes, 0.0, ept, slc))))
@@ -146,8 +146,8 @@ def profile_step(nq: int, workload: str = "small", lanes: int = 0, tune: bool = 
     """One warm step, then one measured step of `nq` queries (with `tune`,
     under the autotuner's options, as the benchmark runs). Prints the
     kernel-launch counts an ncu launch list needs (-s / -c)."""
-    from .workloads import LARGE, SMALL, Workload
-    wl = Workload(LARGE if workload == "large" else SMALL, max_queries=nq, lanes=lanes or nq, tune=tune)
+    from .workloads import WORKLOADS, Workload
+    wl = Workload(WORKLOADS[workload], max_queries=nq, lanes=lanes or nq, tune=tune)
     lib = wl.ctx.lib
     recs = wl.records[:nq]
     wl.encrypt_queries(wl.queries(nq, seed=7), recs)
@@ -330,7 +330,7 @@ def main() -> None:
     sub = ap.add_subparsers(dest="what", required=True)
     a = sub.add_parser("ks", help="rotation key switch alone: ciphertexts per call")
     a.add_argument("lanes", type=int)
-    a.add_argument("--workload", default="small", choices=["small", "large"])
+    a.add_argument("--workload", default="small", choices=["small", "large", "large_diag"])
     a.add_argument("--level", type=int, default=0)
     a.add_argument("--ept", type=int, default=8, choices=[8, 16], help="values per thread (one-kernel path)")
     a.add_argument("--slice", type=int, default=13, choices=[12, 13], help="log2 of a cluster CTA's slice")
@@ -339,7 +339,7 @@ def main() -> None:
     a.add_argument("--log-n", type=int, default=13)
     a = sub.add_parser("step", help="one query step: queries per step")
     a.add_argument("queries", type=int)
-    a.add_argument("--workload", default="small", choices=["small", "large"])
+    a.add_argument("--workload", default="small", choices=["small", "large", "large_diag"])
     a.add_argument("--lanes", type=int, default=0)
     a.add_argument("--tune", action="store_true", help="the autotuner's key-switch options (as the benchmark)")
     sub.add_parser("host", help="end-to-end phases and the streamed run's host hotspots")

@@ -17,7 +17,7 @@ the context's max_batch per launch; one lane of context scratch each): several q
 several (query, list, batch) items in stage 3. Each ciphertext's residues are
 the ones the one-at-a-time chain produces. `lanes=1` is the plain path.
 
-Two compactions:
+Three compactions:
   * "reference": the chain above, verbatim, for indexes whose centroids fit
     one ciphertext (n_list * D <= slots);
   * "packed", for larger indexes: the centroids span n_coarse = n_list /
@@ -34,6 +34,21 @@ Two compactions:
     t mod (slots / B) (an automorphism of the plaintext) selects them there,
     instead of masking row 0 and rotating by the offset with
     popcount(offset) key switches.
+  * "diagonal": the inner products by the diagonal method (baby-step
+    giant-step). The query, repeated every D slots, is rotated by b = 1 ..
+    n1 - 1 once per query (the baby steps, kept for stage 3). The distance
+    of the candidate in slot j is ||q||^2 - 2 <q, x_j> + ||x_j||^2 with
+    -2 <q, x_j> = sum over g < n2 of rot(sum over b < n1 of pt_{g,b} *
+    rot(q, b), n1 g), pt_{g,b} the (pre-rotated) diagonal g n1 + b of the
+    candidates x dims matrix: n2 - 1 giant-step key switches per output
+    ciphertext instead of log2 D per candidate batch. Stage 1 treats the
+    centroids as one such matrix (coarse distance of list c in slot c).
+    Stage 3's plaintexts are built once per unit (a list, or N/2 candidates
+    of it) and placed at the unit's output offset, a multiple of D, by an
+    automorphism of the plaintext folded into the product's loads
+    (afhe_eval_mac_plain_batch); ||q||^2 (one square and a tree sum per
+    query) and the placed unit norms are added. Depth 1: results at l - 1
+    limbs. Slots outside the probed units hold ||q||^2 alone.
 In the reference chain, candidate distances past `slots` continue in further
 result ciphertexts (position p at slot p mod slots of result p // slots). A
 candidate batch never straddles two results: one that would not fit starts
@@ -90,11 +105,28 @@ class QueryShape:
 
     @property
     def n_coarse(self) -> int:
+        if self.compaction == "diagonal":
+            return 1
         return -(-self.n_list // self.per_ct)
+
+    @property
+    def n1(self) -> int:
+        """Baby steps of the diagonal method: 2^ceil(log2(D) / 2)."""
+        return 1 << ((self.D.bit_length() - 1 + 1) // 2)
+
+    @property
+    def n2(self) -> int:
+        """Giant steps of the diagonal method: D / n1."""
+        return self.D // self.n1
+
+    @property
+    def depth(self) -> int:
+        """Rescales of the chain (limbs the results lose)."""
+        return 1 if self.compaction == "diagonal" else 2
 
     def coarse_slot(self, lst: int) -> int:
         """Slot of list `lst`'s distance in the compacted coarse ciphertext."""
-        if self.compaction == "reference":
+        if self.compaction in ("reference", "diagonal"):
             return lst
         return (lst % self.per_ct) * self.D + lst // self.per_ct
 
@@ -111,7 +143,9 @@ class QueryRecord:
     results: list = field(default_factory=list)    # every result ciphertext (dists first)
     level: int = 0          # limbs of the encrypted query (0: the top level L)
     nprobe: int = 0         # lists the client selects (0: the shape's nprobe)
-    norm: tuple | None = None   # stage 3 scratch, packed chain: ||q||^2 (at the evaluation level - 1)
+    norm: tuple | None = None   # packed / diagonal chain: ||q||^2 (at the evaluation level - 1)
+    baby: list = field(default_factory=list)       # diagonal chain: the query rotated by 1 .. n1 - 1
+    layout: list = field(default_factory=list)     # diagonal chain: (unit, slot offset) per probed unit
 
 
 def batch_offsets(counts, slots: int, align: int | None = None) -> list[int]:
@@ -128,6 +162,21 @@ def batch_offsets(counts, slots: int, align: int | None = None) -> list[int]:
             off = (off // slots + 1) * slots
         out.append(off)
         off += cnt
+    return out
+
+
+def unit_offsets(counts, slots: int, D: int) -> list[int]:
+    """Slot offsets of consecutive units of the diagonal chain (counts <=
+    slots): each spans its count rounded up to a multiple of D, back to back,
+    except that a unit that would cross a result's end starts the next
+    result."""
+    out, off = [], 0
+    for cnt in counts:
+        span = -(-cnt // D) * D
+        if off % slots + span > slots:
+            off = (off // slots + 1) * slots
+        out.append(off)
+        off += span
     return out
 
 
@@ -166,6 +215,9 @@ class InteractiveQueryManager:
         self.lanes = max(1, min(lanes, MAX_LANES, ctx.max_batch))
         if shape.compaction == "reference":
             assert shape.n_list * shape.D <= shape.slots, "centroids do not fit one ciphertext"
+        elif shape.compaction == "diagonal":
+            assert shape.n_list <= shape.slots, "the centroids must fit one ciphertext"
+            assert shape.D & (shape.D - 1) == 0 and shape.slots % shape.D == 0, "D: a power of two dividing slots"
         else:
             assert shape.compaction == "packed" and shape.n_coarse <= shape.D, "unsupported compaction"
         L, n = self.L, self.p.n
@@ -181,6 +233,10 @@ class InteractiveQueryManager:
         # inside +-q_0 / 2; distances are at most (|q| + |x|)^2 <= 4 max |x|^2
         bound = 4.0 * float(np.max((index.centroids.astype(np.float64) ** 2).sum(1))) * 4.0 + 64.0
         assert bound * self.out_scale * 4 < self.p.q[0] / 2, "results would not decrypt from limb 0"
+        self._bound = bound
+        if shape.compaction == "diagonal":
+            self._init_diagonal(levels, max_nprobe)
+            return
         # ---- resident plaintexts ----
         self.pt_centroid_cts = slots.take(shape.n_coarse)
         self.pt_centroids = self.pt_centroid_cts[0]
@@ -256,6 +312,123 @@ class InteractiveQueryManager:
             self.cmp = [[(base + k * per_lane + 2 * i * w, base + k * per_lane + (2 * i + 1) * w)
                          for i in range(shape.n_list - 1)] for k in range(self.lanes)]
 
+    # ---- the diagonal chain: resident plaintexts ----
+    def _init_diagonal(self, levels, max_nprobe) -> None:
+        """Units (a list, or N/2 candidates of it), then per evaluation level
+        lv the centroids' and every unit's D diagonals (lv limbs, scale Delta,
+        times -2) and squared norms (lv - 1 limbs, scale Delta^2 / q_{lv-1}),
+        all built and encoded on the device; n_res results per query; a pool
+        of `lanes` working ciphertexts for the inner products."""
+        sh, n, S = self.sh, self.p.n, self.sh.slots
+        assert sh.eval_level is None or 2 <= sh.eval_level <= self.L, "eval_level must be in [2, L]"
+        self._query_levels = set(levels or [self.L]) | {self.L}
+        self.levels = sorted({self.eval_at(lv) for lv in self._query_levels})
+        assert all(2 <= lv <= self.L for lv in self.levels), "evaluation levels must be in [2, L]"
+        self._onehot, self._stride, self._prefix_lv, self._counts = {}, {}, {}, []
+        self._norms, self.mask_prefix, self.cmp, self.batches = {}, {}, [], []
+        self.pt_centroid_cts = []
+        self.units: list[tuple[int, list]] = []       # (list, candidate ids)
+        self.list_units: list[list[int]] = []
+        uvids, ufirst, ucnt = [], [], []
+        for c in range(self.index.n_list):
+            vl = [int(v) for v in self.index.lists[c]]
+            us = []
+            for u0 in range(0, len(vl), S):
+                part = vl[u0:u0 + S]
+                us.append(len(self.units))
+                self.units.append((c, part))
+                ufirst.append(len(uvids))
+                ucnt.append(len(part))
+                uvids.extend(part)
+            self.list_units.append(us)
+        self._uvids, self._ufirst, self._ucnt = uvids, ufirst, ucnt
+        self._gal_cache: dict[int, int] = {}
+        self._diag: dict[int, dict] = {}
+        for lv in self.levels:
+            self._diag_plaintexts(lv)
+        self.max_nprobe = max(max_nprobe or sh.nprobe, sh.nprobe)
+        self.n_res = self.results_for(self.index, sh, self.max_nprobe)
+        top = self.levels[-1]
+        self.lvl_out = top - 1                 # results of the highest evaluation level
+        self._baby_limbs = top
+        w = top * n
+        pool = self.inner_pool(self.lanes, sh.n2)
+        base = self.slots.take(-(-2 * pool * w // self.slots.w))[0]
+        self._inner = [(base + 2 * k * w, base + (2 * k + 1) * w) for k in range(pool)]
+        self.work = []
+
+    @staticmethod
+    def diagonal_values(X: np.ndarray, S: int, D: int, n1: int, coef: float = -2.0) -> np.ndarray:
+        """The D pre-rotated diagonals of the (rows x D) matrix X as slot
+        vectors: row i = g n1 + b, slot k = coef X[j, (j + i) mod D] with
+        j = (k - n1 g) mod S, 0 for j >= rows (afhe_pq_encode_diagonals'
+        layout, for matrices given on the host)."""
+        rows = X.shape[0]
+        out = np.zeros((D, S))
+        k = np.arange(S)
+        for i in range(D):
+            j = (k - (i // n1) * n1) % S
+            ok = j < rows
+            jj = j[ok]
+            out[i, ok] = coef * X[jj, (jj + i) % D]
+        return out
+
+    def _diag_plaintexts(self, lv: int) -> None:
+        sh, n, S, D, n1 = self.sh, self.p.n, self.sh.slots, self.sh.D, self.sh.n1
+        sc = sh.scale * sh.scale / self.p.q[lv - 1]
+
+        def region(count: int, limbs: int) -> list[int]:
+            if count == 0:
+                return []
+            base = self.slots.take(-(-count * limbs * n // self.slots.w))[0]
+            return [base + i * limbs * n for i in range(count)]
+
+        cent = self.index.centroids.astype(np.float64)
+        d = dict(cent=region(D, lv), cnorm=region(1, lv - 1)[0],
+                 pts=np.asarray(region(len(self.units) * D, lv), dtype=np.uint64),
+                 norms=np.asarray(region(len(self.units), lv - 1), dtype=np.uint64))
+        encode_plaintexts(self.ctx, self.enc, self.diagonal_values(cent, S, D, n1), sh.scale, d["cent"], lv)
+        cn = np.zeros((1, S))
+        cn[0, :len(cent)] = (cent ** 2).sum(1)
+        encode_plaintexts(self.ctx, self.enc, cn, sc, [d["cnorm"]], lv - 1)
+        if self.units:
+            args = (self.ctx, self.index, self._uvids, self._ufirst, self._ucnt)
+            encode_index_batches(*args, d["pts"], sh.scale, lv, layout="diagonals", n1=n1, coef=-2.0)
+            encode_index_batches(*args, d["norms"], sc, lv - 1, layout="unit_norms")
+        self._diag[lv] = d
+        self._nh_ver += 1
+
+    @staticmethod
+    def diagonal_slots(units: int, D: int, lv: int, n: int, slot_w: int) -> int:
+        """Slots of one evaluation level's diagonal-chain plaintexts (the
+        centroids' D diagonals and norms, the units' D diagonals and norms,
+        each group packed back to back)."""
+        return sum(-(-count * limbs * n // slot_w) for count, limbs in
+                   ((D, lv), (1, lv - 1), (units * D, lv), (units, lv - 1)) if count)
+
+    @staticmethod
+    def inner_pool(lanes: int, n2: int) -> int:
+        """Working ciphertexts of the inner products: the lanes, rounded down
+        to whole outputs of n2 giant steps, at least one output."""
+        return max(n2, lanes // n2 * n2)
+
+    @classmethod
+    def diagonal_scratch_slots(cls, queries: int, lanes: int, n1: int, n2: int, top: int, n: int,
+                               slot_w: int) -> int:
+        """Slots of the queries' baby steps and the inner-product pool (top
+        limbs each)."""
+        return (-(-2 * queries * (n1 - 1) * top * n // slot_w)
+                + -(-2 * cls.inner_pool(lanes, n2) * top * n // slot_w))
+
+    def unit_offsets(self, probes) -> list[tuple[int, int]]:
+        """(unit, slot offset across the results) for a query's probed lists,
+        in probe order: each unit's slots start at a multiple of D (the
+        plaintext placement keeps the diagonals aligned to the query's
+        period), back to back, a unit that would cross a result's end
+        starting the next result."""
+        us = [u for c in probes for u in self.list_units[c]]
+        return list(zip(us, unit_offsets([len(self.units[u][1]) for u in us], self.sh.slots, self.sh.D)))
+
     def _level_masks(self, lv: int) -> None:
         """The compaction masks of level lv, at scale q_{lv-2} (the prime the
         mask rescale drops)."""
@@ -307,7 +480,16 @@ class InteractiveQueryManager:
         """Change the limbs the server evaluates queries at (None: each query's
         own level). Masks for levels not prepared yet are encoded now (the
         Workload reserves their slots). Call it between steps, with no query
-        in flight."""
+        in flight. The diagonal chain only moves between levels prepared at
+        construction (its plaintexts take D limbs per candidate slot and level)."""
+        if self.sh.compaction == "diagonal":
+            old = self.sh.eval_level
+            self.sh.eval_level = level
+            if any(self.eval_at(x) not in self._diag for x in self._query_levels):
+                self.sh.eval_level = old
+                raise ValueError("the diagonal chain has no plaintexts at that evaluation level")
+            self._nh_ver += 1
+            return
         assert level is None or 3 <= level <= self.L, "eval_level must be in [3, L]"
         self.sh.eval_level = level
         for lv in sorted({self.eval_at(x) for x in self._query_levels}):
@@ -335,6 +517,16 @@ class InteractiveQueryManager:
     def results_for(index: IvfPqIndex, shape: QueryShape, nprobe: int) -> int:
         """Result ciphertexts a query probing `nprobe` lists may need."""
         B, S = shape.B, shape.slots
+        if shape.compaction == "diagonal":      # units of <= S candidates, each over a multiple of D slots
+            spans = sorted((-(-min(len(v) - u0, S) // shape.D) * shape.D for v in index.lists
+                            for u0 in range(0, len(v), S)), reverse=True)
+            per_list = sorted((-(-len(v) // S) for v in index.lists), reverse=True)[:nprobe]
+            total = sum(sorted((sum(-(-min(len(v) - u0, S) // shape.D) * shape.D for u0 in range(0, len(v), S))
+                                for v in index.lists), reverse=True)[:nprobe])
+            # a result closes only when the next unit does not fit: it holds
+            # more than S - (largest span) + D slots, and at least one unit
+            widest = spans[0] if spans else shape.D
+            return max(1, min(sum(per_list), -(-total // (S - widest + shape.D))))
         if shape.compaction == "packed":        # aligned batches: S / B per result
             most = sum(sorted((-(-len(v) // B) for v in index.lists), reverse=True)[:nprobe])
             return max(1, -(-most // (S // B)))
@@ -390,6 +582,13 @@ class InteractiveQueryManager:
     def steps_for(sh: QueryShape) -> set[int]:
         """Rotation keys the chain needs."""
         D, B = sh.D, sh.B
+        if sh.compaction == "diagonal":
+            steps = set(range(1, sh.n1)) | {sh.n1 * g for g in range(1, sh.n2)}    # baby and giant steps
+            s = 1
+            while s < D:
+                steps.add(s)        # tree sum of ||q||^2
+                s <<= 1
+            return steps
         steps = set()
         s = 1
         while s < D:
@@ -409,6 +608,8 @@ class InteractiveQueryManager:
         return steps
 
     def new_query(self) -> QueryRecord:
+        if self.sh.compaction == "diagonal":
+            return self.alloc_queries(1)[0]
         s = self.slots.take(10 if self.sh.compaction == "packed" else 8)
         return QueryRecord((s[0], s[1]), (s[2], s[3]), (s[4], s[5]), (s[6], s[7]), results=[(s[6], s[7])],
                            norm=(s[8], s[9]) if self.sh.compaction == "packed" else None)
@@ -446,17 +647,22 @@ class InteractiveQueryManager:
         w = self.lvl_out * self.p.n
         comp = self.slots.take(-(-2 * count * w // self.slots.w))[0]
         dist = self.slots.take(-(-2 * count * self.n_res * w // self.slots.w))[0]
-        packed = self.sh.compaction == "packed"
+        packed = self.sh.compaction in ("packed", "diagonal")
         w1 = (self.L - 1) * self.p.n
         nbase = self.slots.take(self.norm_slots(count, self.L, self.p.n, self.slots.w))[0] if packed else 0
+        nb = self.sh.n1 - 1 if self.sh.compaction == "diagonal" else 0
+        wb = getattr(self, "_baby_limbs", 0) * self.p.n
+        bbase = self.slots.take(-(-2 * count * nb * wb // self.slots.w))[0] if nb else 0
         recs = []
         for i in range(count):
             s = self.slots.take(4)
             res = [(dist + 2 * (i * self.n_res + k) * w, dist + (2 * (i * self.n_res + k) + 1) * w)
                    for k in range(self.n_res)]
+            baby = [(bbase + 2 * (i * nb + b) * wb, bbase + (2 * (i * nb + b) + 1) * wb) for b in range(nb)]
             recs.append(QueryRecord((s[0], s[1]), (s[2], s[3]),
                                     (comp + 2 * i * w, comp + (2 * i + 1) * w), res[0], results=res,
-                                    norm=(nbase + 2 * i * w1, nbase + (2 * i + 1) * w1) if packed else None))
+                                    norm=(nbase + 2 * i * w1, nbase + (2 * i + 1) * w1) if packed else None,
+                                    baby=baby))
         self._outbox = {"compact": (comp, 1), "dists": (dist, self.n_res)}
         return recs
 
@@ -728,6 +934,10 @@ class InteractiveQueryManager:
     # ---- stages ----
     def stage1_coarse(self, queries: list[QueryRecord]) -> None:
         """Stages 1 and 1b for every query (lanes at a time, one level at a time)."""
+        if self.sh.compaction == "diagonal" and not self._native_diagonal():
+            for lv, idx in self._by_level(queries, self.level_of):
+                self._stage1_diagonal([queries[i] for i in idx], lv)
+            return
         if self.native:
             arr, keep = self._native_queries(queries, probes=False)
             L.check(self.lib.afhe_ivfpq_stage1(self._native_handle(), arr, len(queries)), "ivfpq_stage1")
@@ -809,6 +1019,145 @@ class InteractiveQueryManager:
         # per query: comp += sum of its n_list - 1 rotated terms
         self._sum_groups([[comp[k]] + self.cmp[k] for k in range(len(qs))], Ll - 2)
 
+    # ---- the diagonal chain: stages ----
+    def _native_diagonal(self) -> bool:
+        return False
+
+    MAC_GROUP = np.dtype([("c0", "<u8"), ("c1", "<u8"), ("first", "<u4"), ("n", "<u4")])
+    MAC_TERM = np.dtype([("pt", "<u8"), ("galois", "<u4"), ("reserved", "<u4")])
+
+    def _mac(self, outs, first, groups: np.ndarray, terms: np.ndarray, limbs: int, accumulate: bool = False) -> None:
+        """afhe_eval_mac_plain_batch: outs[j] (+)= sum over groups [first[j],
+        first[j + 1]) of the group's placed plaintexts times its ciphertext
+        (c0 = MAC_UNIT: the constant ciphertext (1, 0)). groups / terms are
+        MAC_GROUP / MAC_TERM arrays (the C ABI's afhe_mac_group / afhe_mac_term)."""
+        fg = np.ascontiguousarray(first, dtype=np.uint32)
+        assert fg.size == len(outs) + 1 and groups.dtype == self.MAC_GROUP and terms.dtype == self.MAC_TERM
+        g = np.ascontiguousarray(groups if groups.size else np.zeros(1, self.MAC_GROUP))
+        t = np.ascontiguousarray(terms if terms.size else np.zeros(1, self.MAC_TERM))
+        L.check(self.lib.afhe_eval_mac_plain_batch(self.ctx.h, self._refs(outs), fg.ctypes.data_as(L.P32), len(outs),
+                                                   g.ctypes.data_as(C.POINTER(L.MacGroup)),
+                                                   t.ctypes.data_as(C.POINTER(L.MacTerm)), limbs, int(accumulate)),
+                "eval_mac_plain_batch")
+
+    def _diag_jobs(self, srcs, pts, gals):
+        """Descriptors of inner-product outputs: output k, giant step g has
+        n1 groups b (source srcs[k][b]) whose terms are pts[k][g, b, :] moved
+        by gals[k][:]. pts[k]: (n2, n1, m_k) offsets; gals[k]: (m_k,)."""
+        n1, n2 = self.sh.n1, self.sh.n2
+        G = np.zeros(len(srcs) * n2 * n1, self.MAC_GROUP)
+        sizes = np.repeat([p.shape[2] for p in pts], n2 * n1)
+        G["n"] = sizes
+        G["first"] = np.concatenate([[0], np.cumsum(sizes)[:-1]]) if sizes.size else []
+        src = np.asarray(srcs, dtype=np.uint64).reshape(len(srcs), 1, n1, 2)
+        src = np.broadcast_to(src, (len(srcs), n2, n1, 2)).reshape(-1, 2)
+        G["c0"], G["c1"] = src[:, 0], src[:, 1]
+        T = np.zeros(int(sizes.sum()), self.MAC_TERM)
+        if T.size:
+            T["pt"] = np.concatenate([p.reshape(-1) for p in pts])
+            T["galois"] = np.concatenate([np.tile(np.asarray(g, dtype=np.uint32), n2 * n1) for g in gals])
+        first = np.arange(0, len(srcs) * n2 * n1 + 1, n1)
+        return first, G, T
+
+    def _rescale(self, a, d, in_limbs: int) -> None:
+        L.check(self.lib.afhe_rescale_batch(self.ctx.h, self._refs(a), self._refs(d), len(a), in_limbs),
+                "rescale_batch")
+
+    def _giant(self, inner, jobs, Ll: int) -> None:
+        """Output k of the inner products jobs (_diag_jobs descriptors, giant
+        step g into inner[k n2 + g], Ll limbs): rescaled, giant step g
+        rotated by n1 g, summed into inner[k n2] (Ll - 1 limbs)."""
+        n1, n2 = self.sh.n1, self.sh.n2
+        self._mac(inner, *jobs, Ll)
+        self._rescale(inner, inner, Ll)
+        self._rotate_direct([(inner[j], n1 * (j % n2)) for j in range(len(inner)) if j % n2], Ll - 1)
+        self._sum_groups([inner[k:k + n2] for k in range(0, len(inner), n2)], Ll - 1)
+
+    def _babies(self, q: QueryRecord) -> list:
+        return [q.ct_query] + list(q.baby)
+
+    def _stage1_diagonal(self, queries: list[QueryRecord], Ll: int) -> None:
+        """Baby steps and ||q||^2 of every query, then the coarse distances
+        ||q||^2 - 2 <q, c> + ||c||^2 in slot c of `compact` (Ll - 1 limbs)."""
+        D, n1, n2 = self.sh.D, self.sh.n1, self.sh.n2
+        dg = self._diag[Ll]
+        items = [(q, b) for q in queries for b in range(1, n1)]
+        if items:
+            steps = (L.i32 * len(items))(*[b for _, b in items])
+            self._at(Ll)
+            L.check(self.lib.afhe_eval_rotate_steps_batch(self.ctx.h, self._refs([q.ct_query for q, _ in items]),
+                                                          self._refs([q.baby[b - 1] for q, b in items]), steps,
+                                                          len(items), Ll), "eval_rotate_steps_batch")
+        nrm = [q.norm for q in queries]
+        self._square([q.ct_query for q in queries], nrm, Ll)
+        s = 1
+        while s < D:                         # ||q||^2 in every slot
+            self._rot_acc(nrm, nrm, s, Ll - 1)
+            s <<= 1
+        cent = np.asarray(dg["cent"], dtype=np.uint64).reshape(n2, n1, 1)
+        per = len(self._inner) // n2
+        for c0 in range(0, len(queries), per):
+            qs = queries[c0:c0 + per]
+            inner = self._inner[:len(qs) * n2]
+            self._giant(inner, self._diag_jobs([self._babies(q) for q in qs], [cent] * len(qs),
+                                               [np.ones(1, np.uint32)] * len(qs)), Ll)
+            comp = [q.compact for q in qs]
+            self._add(inner[0::n2], [q.norm for q in qs], comp, Ll - 1)
+            self._add_plain(comp, [dg["cnorm"]] * len(qs), comp, Ll - 1)
+
+    def _stage3_diagonal_layout(self, queries: list[QueryRecord]) -> None:
+        """Each query's units, their offsets, candidate ids and slot positions."""
+        S = self.sh.slots
+        for q in queries:
+            q.layout = self.unit_offsets(q.probes)
+            q.vids = [v for u, _ in q.layout for v in self.units[u][1]]
+            q.pos = (np.concatenate([np.arange(off, off + len(self.units[u][1])) for u, off in q.layout])
+                     if q.layout else np.zeros(0, dtype=np.int64))
+            if q.layout and q.layout[-1][1] // S >= self.n_res:
+                raise ValueError("more candidates than the result ciphertexts hold")
+
+    def _placement_galois(self, off: int) -> int:
+        """Galois element moving a unit's plaintext from slot 0 to `off` (mod slots)."""
+        o = off % self.sh.slots
+        if o not in self._gal_cache:
+            self._gal_cache[o] = galois_elt(self.p.log_n, -o)
+        return self._gal_cache[o]
+
+    def _stage3_diagonal(self, queries: list[QueryRecord], Ll: int) -> None:
+        """Per (query, result ciphertext): the placed units' inner products,
+        the giant steps, + ||q||^2 + the placed unit norms."""
+        D, S, n1, n2 = self.sh.D, self.sh.slots, self.sh.n1, self.sh.n2
+        dg = self._diag[Ll]
+        pts, norms = dg["pts"], dg["norms"]
+        ib = (np.arange(n2)[:, None, None] * n1 + np.arange(n1)[None, :, None])     # (n2, n1, 1)
+        items = []
+        for q in queries:
+            used = q.layout[-1][1] // S + 1 if q.layout else 1
+            lay = np.asarray(q.layout, dtype=np.int64).reshape(-1, 2)
+            for r in range(used):
+                sel = lay[lay[:, 1] // S == r]
+                gal = np.fromiter((self._placement_galois(int(o)) for o in sel[:, 1]), dtype=np.uint32,
+                                  count=len(sel))
+                items.append((q, r, sel[:, 0], gal))
+        per = len(self._inner) // n2
+        for c0 in range(0, len(items), per):
+            it = items[c0:c0 + per]
+            inner = self._inner[:len(it) * n2]
+            jobs = self._diag_jobs([self._babies(q) for q, _, _, _ in it],
+                                   [pts[u[None, None, :] * D + ib] for _, _, u, _ in it], [g for _, _, _, g in it])
+            self._giant(inner, jobs, Ll)
+            outs = [q.results[r] for q, r, _, _ in it]
+            self._add(inner[0::n2], [q.norm for q, _, _, _ in it], outs, Ll - 1)
+            sizes = np.array([len(u) for _, _, u, _ in it], dtype=np.int64)
+            G = np.zeros(len(it), self.MAC_GROUP)
+            G["c0"], G["n"] = L.MAC_UNIT, sizes
+            G["first"] = np.concatenate([[0], np.cumsum(sizes)[:-1]])
+            T = np.zeros(int(sizes.sum()), self.MAC_TERM)
+            if T.size:
+                T["pt"] = np.concatenate([norms[u] for _, _, u, _ in it])
+                T["galois"] = np.concatenate([g for _, _, _, g in it])
+            self._mac(outs, np.arange(len(it) + 1), G, T, Ll - 1, accumulate=True)
+
     def _sum_groups(self, groups, limbs: int) -> None:
         """groups[g][0] += groups[g][1] + ... , all groups side by side, by
         pairwise batched additions (depth log2 of the largest group)."""
@@ -826,6 +1175,12 @@ class InteractiveQueryManager:
         """Stage 3 for every (query, probed list, batch) item, lanes at a time.
         Each query's `probes` must be set (stage 2)."""
         S = self.sh.slots
+        if self.sh.compaction == "diagonal":
+            self._stage3_diagonal_layout(queries)
+            if not self._native_diagonal():
+                for lv, idx in self._by_level(queries, self.level_of):
+                    self._stage3_diagonal([queries[i] for i in idx], lv)
+                return
         items: dict[int, list] = {}
         for qi, q in enumerate(queries):
             q.vids, q.pos = [], []

@@ -12,6 +12,7 @@ special prime, alpha 1 (dnum 3).
 from __future__ import annotations
 
 import time
+import dataclasses
 from dataclasses import dataclass
 
 import numpy as np
@@ -67,6 +68,14 @@ LARGE = WorkloadSpec("ivfpq_1Mx128_nlist1024_N32768_L12", n_vectors=1_000_000, d
                      n_list=1024, M=16, K=256, nprobe=16, top_k=8, log_n=15, num_q=12, q_bits=50, num_p=4,
                      p_bits=60, alpha=4, log_scale=40, compaction="packed", kmeans_iters=8, train_sample=131072,
                      pq_sample=32768, init="farthest", eval_level=3)
+
+# The same database, index and CKKS parameters through the diagonal chain
+# (baby-step giant-step inner products, depth 1): the queries' first 2 limbs
+# suffice, and the 1,024 lists' diagonals (128 plaintexts of 2 limbs per list,
+# 64 GiB) stay resident in HBM.
+LARGE_DIAG = dataclasses.replace(LARGE, name="ivfpq_1Mx128_nlist1024_N32768_L12_diagonal", compaction="diagonal",
+                                 eval_level=2)
+WORKLOADS = {"small": SMALL, "large": LARGE, "large_diag": LARGE_DIAG}
 
 
 def query_layout(q: np.ndarray, sh: QueryShape) -> np.ndarray:
@@ -153,12 +162,24 @@ class Workload:
         outbox_slots = -(-2 * max_queries * w_out // slot_w) + -(-2 * max_queries * n_res * w_out // slot_w)
         masks = InteractiveQueryManager.mask_slots(shape, len(lvls) + spare_levels, spec.compaction == "reference")
         norm_slots = norm_reserve = 0
+        work_slots = 8 * lanes
+        if spec.compaction == "diagonal":   # no batch plaintexts or masks: per-level diagonals, baby steps
+            IQM = InteractiveQueryManager
+            evl = sorted({min(x, spec.eval_level or x) for x in lvls})
+            units = sum(-(-len(v) // slots) for v in self.index.lists)
+            n_batches, masks, work_slots = 0, 0, 0
+            w_out = (self.params.L - 1) * n
+            outbox_slots = -(-2 * max_queries * w_out // slot_w) + -(-2 * max_queries * n_res * w_out // slot_w)
+            norm_slots = (IQM.norm_slots(max_queries, self.params.L, n, slot_w)
+                          + sum(IQM.diagonal_slots(units, spec.d, lv, n, slot_w) for lv in evl)
+                          + IQM.diagonal_scratch_slots(max_queries, min(lanes, 4096), shape.n1, shape.n2, evl[-1], n,
+                                                       slot_w))
         if spec.compaction == "packed":     # ||q||^2 scratch per query; the candidates' norms per level
             evl = sorted({min(x, spec.eval_level or x) for x in lvls})
             norm_reserve = InteractiveQueryManager.norm_reserve_slots(evl, spare_levels, n_batches, self.params.L,
                                                                       n, slot_w, norm_budget)
             norm_slots = InteractiveQueryManager.norm_slots(max_queries, self.params.L, n, slot_w) + norm_reserve
-        n_slots = (16 + shape.n_coarse + masks + n_batches + 8 * lanes + 4 * max_queries + outbox_slots + 64
+        n_slots = (16 + shape.n_coarse + masks + n_batches + work_slots + 4 * max_queries + outbox_slots + 64
                    + InteractiveQueryManager.compaction_slots(spec.n_list if spec.compaction == "reference" else 1,
                                                               self.params.L, n, slot_w, lanes)
                    + dec_slots + norm_slots)
@@ -199,7 +220,8 @@ class Workload:
             lv = levels[i] if levels is not None else self.params.L
             r.level = lv
             self.client.encrypt(query_layout(q, sh), sh.scale, r.ct_query[0], r.ct_query[1], level=lv)
-            self.client.encrypt(dimpack_layout(q, sh), sh.scale, r.ct_dim[0], r.ct_dim[1], level=lv)
+            if sh.compaction != "diagonal":          # the diagonal chain reads ct_query alone
+                self.client.encrypt(dimpack_layout(q, sh), sh.scale, r.ct_dim[0], r.ct_dim[1], level=lv)
 
     def decrypt_many(self, cts, scales, slots: int | None = None) -> np.ndarray:
         """Decrypt result ciphertexts resident on the device from limb 0 (the

@@ -136,3 +136,37 @@ def test_norm_reserve_within_budget():
     assert r == per[6] + per[7] and (r + per[8]) * w * 8 > NORM_BUDGET_BYTES >= r * w * 8
     assert IQM.norm_reserve_slots([3], 0, nb, L, n, w, budget=0) == 0
     assert IQM.norm_reserve_slots([], 0, nb, L, n, w) == 0
+
+
+def test_diagonal_method_algebra():
+    """The diagonal chain's plaintexts and steps, on plaintext slot vectors:
+    sum over g of rot(sum over b of pt_{g,b} * rot(q, b), n1 g) = -2 <q, x_j>
+    in slot j, 0 elsewhere; a unit's plaintexts moved right by a multiple of
+    D (its placement) move the result by the same amount."""
+    from anns_fhe_b200.query import QueryShape
+    rng = np.random.default_rng(0)
+    for S, D, rows in ((512, 16, 70), (1024, 8, 1024), (2048, 64, 300)):
+        sh = QueryShape(D=D, n_list=4, slots=S, nprobe=1, top_k=1, scale=1.0, compaction="diagonal")
+        n1, n2 = sh.n1, sh.n2
+        assert n1 * n2 == D and n1 >= n2
+        X, q = rng.normal(size=(rows, D)), rng.normal(size=D)
+        P = InteractiveQueryManager.diagonal_values(X, S, D, n1)
+        rot = lambda v, r: np.roll(v, -r)      # noqa: E731  slot k <- slot k + r
+        baby = [rot(np.tile(q, S // D), b) for b in range(n1)]
+        for o in {o for o in (0, D, (S - rows) // D * D) if o + rows <= S}:
+            out = sum(rot(sum(rot(P[g * n1 + b], -o) * baby[b] for b in range(n1)), n1 * g) for g in range(n2))
+            assert np.allclose(out[o:o + rows], -2 * X @ q)
+            assert np.allclose(np.delete(out, np.arange(o, o + rows)), 0)
+
+
+def test_unit_offsets():
+    from anns_fhe_b200.query import unit_offsets
+    assert unit_offsets([5, 8, 9], 32, 8) == [0, 8, 16]
+    assert unit_offsets([5, 8, 9, 1], 32, 8) == [0, 8, 16, 32]
+    assert unit_offsets([32, 1, 32], 32, 8) == [0, 32, 64]
+    assert unit_offsets([], 32, 8) == []
+    rng = np.random.default_rng(1)
+    counts = [int(x) for x in rng.integers(1, 513, 300)]
+    offs = unit_offsets(counts, 512, 8)
+    for off, cnt in zip(offs, counts):
+        assert off % 8 == 0 and off // 512 == (off + cnt - 1) // 512
