@@ -14,6 +14,7 @@ both outputs written (4 x l limbs of N words); the rotation key (2 x dnum x
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import time
@@ -165,6 +166,76 @@ def profile_step(nq: int, workload: str = "small", lanes: int = 0, tune: bool = 
     wl.close()
 
 
+def mac_roofline(outputs: int = 64, units: int = 16, limbs: int = 2, reps: int = 10) -> dict:
+    """The diagonal chain's inner-product kernel (afhe_eval_mac_plain_batch)
+    alone, shaped like its stage 3 on the large configuration (N = 2^15, d =
+    128: n1 = 16 baby steps, n2 = 8 giant steps): `outputs` outputs (one per
+    query and giant step), each 16 groups (baby-step ciphertexts) of `units`
+    plaintexts placed at multiples of 1,024 slots; the plaintexts come from
+    `units` units of 128 diagonals at `limbs` limbs (1 GiB at 16 units, more
+    than L2). Timed with CUDA events on the context stream after 3 warm-up
+    calls. Algorithmic bytes: every plaintext read once per output, the
+    outputs written, the 16 sources (2 polynomials) read once."""
+    import numpy as np
+    import torch
+
+    from . import _lib as L
+    from .driver import CkksParams, FheContext, galois_elt
+    from .query import InteractiveQueryManager as IQM
+    p = CkksParams.generate(15, 12, 50, 4, 60, 4)
+    n, D, n1, n2 = p.n, 128, 16, 8
+    torch.cuda.init()
+    w = limbs * n
+    n_pts = units * D
+    srcs = [((n_pts + 2 * b) * w, (n_pts + 2 * b + 1) * w) for b in range(n1)]
+    base = (n_pts + 2 * n1) * w
+    outs = [(base + 2 * o * w, base + (2 * o + 1) * w) for o in range(outputs)]
+    ctx = FheContext(p, poly_words=base + 2 * outputs * w + w, key_words=1024, device=torch.cuda.current_device())
+    try:
+        rng = np.random.default_rng(3)
+        for off in range(0, base, w):       # residues below every prime of the limbs
+            ctx.write_poly(off, rng.integers(0, min(p.q[:limbs]), size=w, dtype=np.uint64))
+        gal = np.array([galois_elt(p.log_n, -1024 * i) for i in range(units)], dtype=np.uint32)
+        ib = np.arange(n2)[:, None, None] * n1 + np.arange(n1)[None, :, None]
+        first, G, T = [0], [], []
+        for o in range(outputs):
+            k, g = divmod(o, n2)
+            u = (k + np.arange(units)) % units
+            pts = (u[None, None, :] * D + ib)[g] * w                       # (n1, units)
+            for b in range(n1):
+                G.append((srcs[b][0], srcs[b][1], len(T), units))
+                T.extend(zip(pts[b].tolist(), gal.tolist(), [0] * units))
+            first.append(len(G))
+        Ga = np.array(G, dtype=IQM.MAC_GROUP)
+        Ta = np.array(T, dtype=IQM.MAC_TERM)
+        fg = np.array(first, dtype=np.uint32)
+        refs = (L.CtRef * outputs)(*[L.CtRef(*c) for c in outs])
+
+        def call():
+            L.check(ctx.lib.afhe_eval_mac_plain_batch(ctx.h, refs, fg.ctypes.data_as(L.P32), outputs,
+                                                      Ga.ctypes.data_as(ctypes.POINTER(L.MacGroup)),
+                                                      Ta.ctypes.data_as(ctypes.POINTER(L.MacTerm)), limbs, 0),
+                    "eval_mac_plain_batch")
+        for _ in range(3):
+            call()
+        ctx.sync()
+        st = torch.cuda.ExternalStream(ctx.lib.afhe_stream(ctx.h), device=torch.cuda.current_device())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(reps):
+            call()
+        e1.record(st)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        alg = (len(T) * w + outputs * 2 * w + n1 * 2 * w) * 8
+        peak, src = load_peaks()
+        return {"profile": "mac_plain", "outputs": outputs, "terms": len(T), "limbs": limbs, "ms": round(ms, 4),
+                "algorithmic_bytes": alg, "achieved_gbs": round(alg / ms / 1e6, 1), "peak_gbs": peak,
+                "frac": round(alg / ms / 1e6 / peak, 3), "peak_source": src}
+    finally:
+        ctx.close()
+
+
 def profile_ntt(polys: int, log_n: int = 13, reps: int = 10):
     """Batched in-place NTT / INTT over `polys` polynomials of 4 limbs (the
     key switch's shape), forward then inverse, `reps` each."""
@@ -218,7 +289,7 @@ def profile_host(batch: int = 296, steps: int = 5):
     recs = wl.records[:batch]
     wl.encrypt_queries(wl.queries(batch, seed=1000), recs)
     Lw = wl.params.L * wl.params.n
-    host = [[torch.from_numpy(wl.ctx.read_poly(o, Lw)).pin_memory().numpy() for o in (*r.ct_query, *r.ct_dim)]
+    host = [[torch.from_numpy(wl.ctx.read_poly(o, Lw)).pin_memory().numpy() for o in wl.iqm.input_polys(r)]
             for r in recs]
     dec = wl.client.decryptor(batch * max(1, iqm.n_res))
     phases: dict = {}
@@ -232,7 +303,7 @@ def profile_host(batch: int = 296, steps: int = 5):
     def phased_step():
         t = time.perf_counter()
         for r, cts in zip(recs, host):
-            for off, a in zip((*r.ct_query, *r.ct_dim), cts):
+            for off, a in zip(wl.iqm.input_polys(r), cts):
                 check(wl.ctx.lib.afhe_write_poly_async(wl.ctx.h, off, a.ctypes.data_as(P64), a.size), "write")
         t = mark("h2d", t)
         iqm.stage1_coarse(recs)
@@ -342,6 +413,9 @@ def main() -> None:
     a.add_argument("--workload", default="small", choices=["small", "large", "large_diag"])
     a.add_argument("--lanes", type=int, default=0)
     a.add_argument("--tune", action="store_true", help="the autotuner's key-switch options (as the benchmark)")
+    a = sub.add_parser("mac", help="the diagonal chain's inner-product kernel alone: outputs per call")
+    a.add_argument("outputs", type=int)
+    a.add_argument("--units", type=int, default=16)
     sub.add_parser("host", help="end-to-end phases and the streamed run's host hotspots")
     a = sub.add_parser("dispatch", help="afhe_dispatch cost per call and op code")
     a.add_argument("--calls", type=int, default=200)
@@ -352,6 +426,8 @@ def main() -> None:
         profile_ntt(args.polys, args.log_n)
     elif args.what == "step":
         profile_step(args.queries, args.workload, args.lanes, args.tune)
+    elif args.what == "mac":
+        print(json.dumps(mac_roofline(args.outputs, args.units)))
     elif args.what == "dispatch":
         profile_dispatch(args.calls)
     else:

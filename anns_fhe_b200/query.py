@@ -1260,6 +1260,13 @@ class InteractiveQueryManager:
                              Ll - 2)
 
     # ---- result transfer ----
+    def input_polys(self, rec: QueryRecord) -> tuple:
+        """Offsets of the polynomials the server reads from a client: ct_query
+        and ct_dim, or ct_query alone (the diagonal chain)."""
+        if self.sh.compaction == "diagonal":
+            return tuple(rec.ct_query)
+        return (*rec.ct_query, *rec.ct_dim)
+
     def read_ct(self, ct: tuple[int, int]) -> tuple[np.ndarray, np.ndarray]:
         w = self.lvl_out * self.p.n
         return self.ctx.read_poly(ct[0], w), self.ctx.read_poly(ct[1], w)

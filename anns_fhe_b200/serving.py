@@ -119,8 +119,8 @@ class WorkloadBackend:
                  pool: list[list[np.ndarray]] | None = None, levels=None, pool_levels=None):
         """Q: query vectors the client encrypts into the pool (query i at
         levels[i] limbs, default the top level); or `pool`: ciphertexts
-        already encrypted, four host arrays (ct_query c0, c1, ct_dim c0, c1)
-        per query, at pool_levels[i] limbs (default the top level)."""
+        already encrypted, the host arrays of iqm.input_polys (ct_query c0,
+        c1, then ct_dim c0, c1 where the chain reads it) per query, at pool_levels[i] limbs (default the top level)."""
         self.wl = wl
         self.iqm = wl.iqm
         self.lib = wl.ctx.lib
@@ -138,13 +138,15 @@ class WorkloadBackend:
             lv = None if levels is None else list(levels[c0:c0 + chunk])
             wl.encrypt_queries(part, recs, lv)
             for r in recs:
-                self.pool.append([wl.ctx.read_poly(o, r.level * self.n) for o in (*r.ct_query, *r.ct_dim)])
+                self.pool.append([wl.ctx.read_poly(o, r.level * self.n) for o in wl.iqm.input_polys(r)])
                 self.pool_level.append(r.level)
         w = self.iqm.lvl_out * self.n
-        # device bytes one in-flight query holds: two encrypted queries at L
-        # limbs, the compacted coarse result and n_res candidate results at
-        # lvl_out limbs
-        self.bytes_per_query = (4 * Lw + 2 * w * (1 + self.iqm.n_res)) * 8
+        # device bytes one in-flight query holds: its encrypted polynomials at
+        # L limbs, the compacted coarse result and n_res candidate results at
+        # lvl_out limbs, and (diagonal chain) its baby steps
+        r0 = wl.records[0]
+        self.bytes_per_query = (len(self.iqm.input_polys(r0)) * Lw + 2 * w * (1 + self.iqm.n_res)
+                                + 2 * len(r0.baby) * getattr(self.iqm, "_baby_limbs", 0) * self.n) * 8
         self._dec = {"dec": None}
         self._pool_ptrs: dict = {}
 
@@ -172,7 +174,7 @@ class WorkloadBackend:
         ptrs = self._pool_ptrs.get(req.payload)
         if ptrs is None:          # pointers made once per pool entry (each keeps its array alive)
             ptrs = self._pool_ptrs[req.payload] = [(a.ctypes.data_as(L.P64), a.size) for a in self.pool[req.payload]]
-        for off, (p, size) in zip((*rec.ct_query, *rec.ct_dim), ptrs):
+        for off, (p, size) in zip(self.iqm.input_polys(rec), ptrs):
             L.check(self.lib.afhe_write_poly_async(self.h, off, p, size), "write_poly_async")
 
     def coarse(self, recs) -> None:

@@ -73,8 +73,7 @@ LARGE = WorkloadSpec("ivfpq_1Mx128_nlist1024_N32768_L12", n_vectors=1_000_000, d
 # (baby-step giant-step inner products, depth 1): the queries' first 2 limbs
 # suffice, and the 1,024 lists' diagonals (128 plaintexts of 2 limbs per list,
 # 64 GiB) stay resident in HBM.
-LARGE_DIAG = dataclasses.replace(LARGE, name="ivfpq_1Mx128_nlist1024_N32768_L12_diagonal", compaction="diagonal",
-                                 eval_level=2)
+LARGE_DIAG = dataclasses.replace(LARGE, compaction="diagonal", eval_level=2)
 WORKLOADS = {"small": SMALL, "large": LARGE, "large_diag": LARGE_DIAG}
 
 
@@ -284,7 +283,7 @@ class Workload:
         lib, h = self.ctx.lib, self.ctx.h
         h2d = 0
         for r, cts in zip(part, hp):
-            for off, a in zip((*r.ct_query, *r.ct_dim), cts):
+            for off, a in zip(self.iqm.input_polys(r), cts):
                 L.check(lib.afhe_write_poly_async(h, off, a.ctypes.data_as(L.P64), a.size), "write_poly_async")
                 h2d += a.nbytes
         self.iqm.stage1_coarse(part)

@@ -79,8 +79,10 @@ def summarize_clocks(samples):
 
 
 def spec_of(workload: str):
-    from anns_fhe_b200.workloads import LARGE, SMALL
-    return LARGE if workload == "large" else SMALL
+    """large: config 4 through the diagonal chain (the headline); large_packed:
+    the same configuration through the packed chain; small: config 1."""
+    from anns_fhe_b200.workloads import LARGE, LARGE_DIAG, SMALL
+    return {"large": LARGE_DIAG, "large_packed": LARGE, "small": SMALL}[workload]
 
 
 def default_batch(spec) -> int:
@@ -97,8 +99,7 @@ def config_of(spec, batch: int) -> dict:
     return {"workload": spec.name, "queries_per_step": batch, "n_vectors": spec.n_vectors, "d": spec.d,
             "n_list": spec.n_list, "nprobe": spec.nprobe, "pq": f"{spec.M}x{spec.K}", "top_k": spec.top_k,
             "ring_degree": n, "q_limbs": spec.num_q, "p_limbs": spec.num_p, "alpha": spec.alpha,
-            "scale_bits": spec.log_scale, "compaction": spec.compaction,
-            "eval_level": spec.eval_level or spec.num_q,
+            "scale_bits": spec.log_scale,
             "l2": f"no flush; inputs larger than L2: {batch * ct_bytes / 1e6:.0f} MB of encrypted queries per step "
                   f"(L2 126 MB)"}
 
@@ -124,9 +125,11 @@ def time_steps(wl, recs, stream, steps: int):
     return out
 
 
-def measure(args, spec, rank: int, world: int, steps: int, warmup: int, batch: int, legs: bool):
+def measure(args, spec, rank: int, world: int, steps: int, warmup: int, batch: int, legs: bool,
+            full_level: bool = False):
     """One workload: device-only steps, the streamed end-to-end run, and (with
-    legs) the full-level sample, serving and roofline. Returns the line."""
+    legs) serving and the roofline; with full_level, the full-level sample.
+    Returns the line."""
     import torch
 
     from anns_fhe_b200 import _lib as L
@@ -139,14 +142,14 @@ def measure(args, spec, rank: int, world: int, steps: int, warmup: int, batch: i
     large = spec.log_n >= 15
     # twice the records of a step: the stream keeps three groups in flight
     wl = Workload(spec, max_queries=2 * batch, lanes=lanes, device=dev, tune=not args.no_tune,
-                  spare_levels=1 if large else 0)
+                  spare_levels=1 if full_level else 0)
     try:
         stream = torch.cuda.ExternalStream(wl.ctx.lib.afhe_stream(wl.ctx.h), device=dev)
         recs = wl.records[:batch]
         Q = wl.queries(batch, seed=query_seed(1000, rank))
         wl.encrypt_queries(Q, recs)            # client work done once: encrypted queries on the host
         Lw = wl.params.L * wl.params.n
-        host = [[torch.from_numpy(wl.ctx.read_poly(o, Lw)).pin_memory() for o in (*r.ct_query, *r.ct_dim)]
+        host = [[torch.from_numpy(wl.ctx.read_poly(o, Lw)).pin_memory() for o in wl.iqm.input_polys(r)]
                 for r in recs]
         host_np = [[t.numpy() for t in cts] for cts in host]
         groups = max(1, args.e2e_groups)
@@ -202,18 +205,21 @@ def measure(args, spec, rank: int, world: int, steps: int, warmup: int, batch: i
                                else None),
                     "lane_scratch_gb": round(wl.ctx.scratch_bytes() / 1e9, 1),
                     "ks_capacity": wl.ctx.get_option(L.OPT_KS_CAPACITY),
-                    "ntt_plan": get_ntt_plan(spec.log_n), "stage_driver": "native" if wl.iqm.native else "python"},
+                    "ntt_plan": get_ntt_plan(spec.log_n), "stage_driver": "native" if wl.iqm.native else "python",
+                    "chain": spec.compaction, "eval_level": spec.eval_level or spec.num_q},
         }
-        if legs and large and not args.skip_full_level:
+        if full_level and not args.skip_full_level:
             line["full_level"] = full_level_leg(wl, stream, rank)
         if legs and not args.skip_serving:
             line["serving"] = serve_leg(args, wl, host_np, rank, line["value"])
     finally:
         wl.close()
     if legs:
-        from anns_fhe_b200.profiling import ks_roofline
+        from anns_fhe_b200.profiling import ks_roofline, mac_roofline
         ev = spec.eval_level or spec.num_q
         line["roofline"] = ks_roofline(wl.params, lanes, level=ev, choice=(wl.tuning or {}).get(ev))
+        if spec.compaction == "diagonal" and large:
+            line["roofline_inner_products"] = mac_roofline(64, 16, ev)
     return line
 
 
@@ -301,9 +307,19 @@ def run_ours(args, rank: int, world: int):
         base = cpu_baseline(args.workload)
     import torch
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", 0)))
-    line = measure(args, spec, rank, world, args.steps, args.warmup, batch, legs=True)
+    line = measure(args, spec, rank, world, args.steps, args.warmup, batch, legs=True,
+                   full_level=args.workload == "large_packed")
     if base:
         line["cpu_baseline"] = base
+    if args.workload == "large" and not args.skip_packed:
+        # the same configuration through the packed chain (tree sums per
+        # candidate batch), with its full-level sample
+        pk = measure(args, spec_of("large_packed"), rank, world, args.steps, args.warmup, batch, legs=False,
+                     full_level=True)
+        line["packed_chain"] = {k: pk[k] for k in ("value", "unit", "ms_per_step", "e2e", "gpu_launches", "run")
+                                if k in pk}
+        if "full_level" in pk:
+            line["packed_chain"]["full_level"] = pk["full_level"]
     if args.workload == "large" and not args.skip_small:
         small = spec_of("small")
         s = measure(args, small, rank, world, max(3, args.steps // 4), 3, default_batch(small), legs=False)
@@ -525,14 +541,16 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="large", choices=["large", "small"],
-                    help="large: 1M x 128, n_list 1024, N=2^15 (default); small: 4,096 x 64, N=2^13")
+    ap.add_argument("--workload", default="large", choices=["large", "large_packed", "small"],
+                    help="large: 1M x 128, n_list 1024, N=2^15, diagonal chain (default); large_packed: the same "
+                         "through the packed chain; small: 4,096 x 64, N=2^13")
     ap.add_argument("--batch", type=int, default=0, help="queries per step (default: 256 large, 296 small)")
     ap.add_argument("--lanes", type=int, default=0, help="ciphertexts per launch (default: the batch)")
     ap.add_argument("--skip-cpu", action="store_true", help="omit the cpu_baseline leg")
     ap.add_argument("--skip-serving", action="store_true", help="omit the serving leg")
     ap.add_argument("--skip-small", action="store_true", help="omit the small configuration's secondary line")
     ap.add_argument("--skip-full-level", action="store_true", help="omit the full-level sample")
+    ap.add_argument("--skip-packed", action="store_true", help="omit the packed chain's secondary line")
     ap.add_argument("--e2e-groups", type=int, default=2,
                     help="e2e: groups of queries per step whose client and server work overlap")
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuner's key-switch choices")

@@ -69,7 +69,7 @@ OP_NTT, OP_INTT, OP_ADD, OP_SUB, OP_MUL, OP_AUTO, OP_KS, OP_RESCALE, OP_LOAD = 1
 def shape(workload: str) -> dict:
     """The CKKS parameters, query shape and per-query work units of a workload."""
     from anns_fhe_b200.workloads import LARGE, SMALL
-    spec = LARGE if workload == "large" else SMALL
+    spec = SMALL if workload == "small" else LARGE      # the reference's own chain on either large form
     log_n, n = spec.log_n, 1 << spec.log_n
     q = T.ntt_primes(log_n, spec.q_bits, spec.num_q)
     p = T.ntt_primes(log_n, spec.p_bits, spec.num_p, q)
