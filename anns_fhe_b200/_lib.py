@@ -180,6 +180,8 @@ SIGNATURES = {
     "afhe_eval_sub_batch": (C.c_int, [CTX, C.POINTER(CtRef), C.POINTER(CtRef), C.POINTER(CtRef), u32, u32]),
     "afhe_eval_mac_plain_batch": (C.c_int, [CTX, C.POINTER(CtRef), P32, u32, C.POINTER(MacGroup), C.POINTER(MacTerm),
                                             u32, u32]),
+    "afhe_eval_diag_inner_batch": (C.c_int, [CTX, C.POINTER(CtRef), u32, C.POINTER(CtRef), u32, P64, P32, P32, u64,
+                                             u32, u32]),
     "afhe_eval_add_plain_batch": (C.c_int, [CTX, C.POINTER(CtRef), P64, C.POINTER(CtRef), u32, u32]),
     "afhe_encode_batch": (C.c_int, [CTX, C.POINTER(C.c_double), u32, u32, C.c_double, u32, P64]),
     "afhe_pq_create": (C.c_int, [CTX, C.POINTER(PqIndex), C.POINTER(C.c_void_p)]),

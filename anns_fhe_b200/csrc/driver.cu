@@ -925,6 +925,94 @@ int afhe_eval_mac_plain_batch(afhe_ctx* ctx, const afhe_ct_ref* out, const uint3
     return flush();
 }
 
+int afhe_eval_diag_inner_batch(afhe_ctx* ctx, const afhe_ct_ref* out, uint32_t count, const afhe_ct_ref* src,
+                               uint32_t nb, const uint64_t* unit_pt, const uint32_t* unit_galois,
+                               const uint32_t* first_unit, uint64_t pt_stride, uint32_t limbs, uint32_t accumulate) {
+    if (!ctx || (count && (!out || !src || !first_unit))) return fail(ctx, AFHE_E_ARG, "null argument");
+    if (nb != 1 && nb != 2 && nb != 4 && nb != 8 && nb != 16) return fail(ctx, AFHE_E_ARG, "nb must be 1, 2, 4, 8 or 16");
+    int rc;
+    if ((rc = check_limbs(ctx, limbs, 1)) || (rc = check_cts(ctx, out, count, limbs)) ||
+        (rc = check_cts(ctx, src, count * nb, limbs)))
+        return rc;
+    const u64 w = (u64)limbs * ctx->n;
+    const u64 span = (u64)(nb - 1) * pt_stride + w;       // a unit's nb plaintexts
+    std::vector<std::pair<u64, int>> ends;
+    auto read = [&](u64 off, u64 len) {
+        ends.push_back({off, 1});
+        ends.push_back({off + len, -1});
+    };
+    for (uint32_t j = 0; j < count; ++j) {
+        if (first_unit[j + 1] < first_unit[j]) return fail(ctx, AFHE_E_ARG, "unit ranges must not decrease");
+        if (first_unit[j + 1] > first_unit[j] && (!unit_pt || !unit_galois)) return fail(ctx, AFHE_E_ARG, "null argument");
+        for (uint32_t k = first_unit[j]; k < first_unit[j + 1]; ++k) {
+            if (!range_ok(unit_pt[k], span, ctx->prm.poly_words)) return fail(ctx, AFHE_E_RANGE, "plaintexts out of poly_gmem");
+            if ((unit_galois[k] & 1u) == 0 || unit_galois[k] >= 2 * ctx->n)
+                return fail(ctx, AFHE_E_ARG, "galois element must be odd and < 2N");
+            read(unit_pt[k], span);
+        }
+        for (uint32_t b = 0; b < nb; ++b) {
+            read(src[(u64)j * nb + b].c0_offset, w);
+            read(src[(u64)j * nb + b].c1_offset, w);
+        }
+        ends.push_back({out[j].c0_offset, 2});
+        ends.push_back({out[j].c0_offset + w, -2});
+        ends.push_back({out[j].c1_offset, 2});
+        ends.push_back({out[j].c1_offset + w, -2});
+    }
+    std::sort(ends.begin(), ends.end());
+    int open_src = 0, open_dst = 0;
+    for (const auto& e : ends) {
+        if (e.second == 1) ++open_src;
+        else if (e.second == -1) --open_src;
+        else if (e.second == 2) ++open_dst;
+        else --open_dst;
+        if (open_dst > 1 || (open_src > 0 && open_dst > 0))
+            return fail(ctx, AFHE_E_ARG, "an output overlaps another output or an operand");
+    }
+    u64 qmax = 0;
+    for (uint32_t l = 0; l < limbs; ++l) qmax = std::max<u64>(qmax, ctx->prm.q[l]);
+    const unsigned __int128 sq = (unsigned __int128)(qmax - 1) * (qmax - 1);
+    const unsigned __int128 room = ~(unsigned __int128)0 / (sq ? sq : 1);
+    const uint32_t reduce_every = room > 0x7fffffff ? 0x7fffffffu : (uint32_t)room;
+    if (reduce_every < nb + 1) return fail(ctx, AFHE_E_ARG, "primes too large for the accumulators; use afhe_eval_mac_plain_batch");
+    const size_t seg = ctx->ring.seg_words - 96;
+    std::vector<DiagJob> J;
+    std::vector<u64> S;
+    std::vector<DiagUnit> U;
+    auto flush = [&]() -> int {
+        if (J.empty()) return AFHE_OK;
+        u64 *dj = nullptr, *ds = nullptr, *du = nullptr;
+        int r;
+        if (U.empty()) U.push_back(DiagUnit{0, nullptr});
+        if ((r = ring_put(ctx, J.data(), J.size() * sizeof(DiagJob) / sizeof(u64), &dj))) return r;
+        if ((r = ring_put(ctx, S.data(), S.size(), &ds))) return r;
+        if ((r = ring_put(ctx, U.data(), U.size() * sizeof(DiagUnit) / sizeof(u64), &du))) return r;
+        CK(launch_diag_inner(ctx->nat.pc, ctx->poly, ctx->n, limbs, (uint32_t)J.size(), nb, (const DiagJob*)dj, ds,
+                             (const DiagUnit*)du, pt_stride, reduce_every, accumulate ? 1 : 0, ctx->st));
+        J.clear();
+        S.clear();
+        U.clear();
+        return AFHE_OK;
+    };
+    for (uint32_t j = 0; j < count; ++j) {
+        const size_t nu = first_unit[j + 1] - first_unit[j];
+        if (3 + 2 * nb + 2 * nu + 2 > seg / 3) return fail(ctx, AFHE_E_ARG, "too many units in one output for the descriptor ring");
+        if ((J.size() + 1) * 3 > seg / 3 || S.size() + 2 * nb > seg / 3 || (U.size() + nu + 1) * 2 > seg / 3)
+            if ((rc = flush())) return rc;
+        J.push_back(DiagJob{out[j].c0_offset, out[j].c1_offset, (uint32_t)U.size(), (uint32_t)(U.size() + nu)});
+        for (uint32_t b = 0; b < nb; ++b) {
+            S.push_back(src[(u64)j * nb + b].c0_offset);
+            S.push_back(src[(u64)j * nb + b].c1_offset);
+        }
+        for (uint32_t k = first_unit[j]; k < first_unit[j + 1]; ++k) {
+            const uint32_t* map = nullptr;
+            if (unit_galois[k] != 1 && (rc = cached_map(ctx, unit_galois[k], &map))) return rc;
+            U.push_back(DiagUnit{unit_pt[k], map});
+        }
+    }
+    return flush();
+}
+
 int afhe_eval_copy_batch(afhe_ctx* ctx, const afhe_ct_ref* a, const afhe_ct_ref* d, uint32_t count, uint32_t limbs) {
     if (!ctx || (count && (!a || !d))) return fail(ctx, AFHE_E_ARG, "null argument");
     int rc;

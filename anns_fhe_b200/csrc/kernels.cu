@@ -201,6 +201,75 @@ __global__ void __launch_bounds__(256) mac_plain_kernel(const PrimeConst* __rest
     arena[J.out1 + off] = r1;
 }
 
+// One coefficient per thread: the nb baby-step ciphertexts' coefficients stay
+// in registers while the job's units stream through; a unit's automorphism
+// index is loaded once for its nb plaintexts, which lie `stride` words apart.
+template <int NB>
+__global__ void __launch_bounds__(256) diag_inner_kernel(const PrimeConst* __restrict__ pc, u64* __restrict__ arena,
+                                                         uint32_t n, const DiagJob* __restrict__ jobs,
+                                                         const u64* __restrict__ srcs,
+                                                         const DiagUnit* __restrict__ units, u64 stride,
+                                                         uint32_t reduce_every, int accumulate) {
+    const uint32_t l = blockIdx.y;
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const DiagJob J = jobs[blockIdx.z];
+    const ModConst m = modconst_of(pc[l]);
+    const u64 off = (u64)l * n;
+    const u64* s = srcs + (u64)blockIdx.z * 2 * NB;
+    u64 x0[NB], x1[NB];
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+        x0[b] = arena[s[2 * b] + off + i];
+        x1[b] = arena[s[2 * b + 1] + off + i];
+    }
+    Acc128 a0, a1;
+    acc_init(a0);
+    acc_init(a1);
+    uint32_t cnt = 0;
+    for (uint32_t k = J.u0; k < J.u1; ++k) {
+        const DiagUnit U = units[k];
+        const uint32_t j = U.map ? __ldg(U.map + i) : i;
+        const u64* p = arena + U.pt + off + j;
+        if (cnt + NB > reduce_every) {
+            acc_fold(a0, m);
+            acc_fold(a1, m);
+            cnt = 1;
+        }
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            const u64 v = p[(u64)b * stride];
+            acc_mad(a0, v, x0[b]);
+            acc_mad(a1, v, x1[b]);
+        }
+        cnt += NB;
+    }
+    u64 r0 = acc_reduce(a0, m), r1 = acc_reduce(a1, m);
+    if (accumulate) {
+        r0 = add_mod(r0, arena[J.out0 + off + i], m.q);
+        r1 = add_mod(r1, arena[J.out1 + off + i], m.q);
+    }
+    arena[J.out0 + off + i] = r0;
+    arena[J.out1 + off + i] = r1;
+}
+
+cudaError_t launch_diag_inner(const PrimeConst* pc, u64* arena, uint32_t n, uint32_t limbs, uint32_t jobs,
+                              uint32_t nb, const DiagJob* job, const u64* srcs, const DiagUnit* unit, u64 stride,
+                              uint32_t reduce_every, int accumulate, cudaStream_t st) {
+    if (limbs == 0 || jobs == 0) return cudaSuccess;
+    dim3 grid((n + 255) / 256, limbs, jobs);
+    switch (nb) {
+    case 1: diag_inner_kernel<1><<<grid, 256, 0, st>>>(pc, arena, n, job, srcs, unit, stride, reduce_every, accumulate); break;
+    case 2: diag_inner_kernel<2><<<grid, 256, 0, st>>>(pc, arena, n, job, srcs, unit, stride, reduce_every, accumulate); break;
+    case 4: diag_inner_kernel<4><<<grid, 256, 0, st>>>(pc, arena, n, job, srcs, unit, stride, reduce_every, accumulate); break;
+    case 8: diag_inner_kernel<8><<<grid, 256, 0, st>>>(pc, arena, n, job, srcs, unit, stride, reduce_every, accumulate); break;
+    case 16: diag_inner_kernel<16><<<grid, 256, 0, st>>>(pc, arena, n, job, srcs, unit, stride, reduce_every, accumulate); break;
+    default: return cudaErrorInvalidValue;
+    }
+    count_launches(1);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_mac_plain(const PrimeConst* pc, u64* arena, uint32_t n, uint32_t limbs, uint32_t jobs,
                              const MacJob* job, const MacGroup* group, const MacTerm* term, uint32_t reduce_every,
                              int accumulate, cudaStream_t st) {

@@ -166,7 +166,7 @@ def profile_step(nq: int, workload: str = "small", lanes: int = 0, tune: bool = 
     wl.close()
 
 
-def mac_roofline(outputs: int = 64, units: int = 16, limbs: int = 2, reps: int = 10) -> dict:
+def mac_roofline(outputs: int = 64, units: int = 16, limbs: int = 2, reps: int = 10, generic: bool = False) -> dict:
     """The diagonal chain's inner-product kernel (afhe_eval_mac_plain_batch)
     alone, shaped like its stage 3 on the large configuration (N = 2^15, d =
     128: n1 = 16 baby steps, n2 = 8 giant steps): `outputs` outputs (one per
@@ -175,7 +175,9 @@ def mac_roofline(outputs: int = 64, units: int = 16, limbs: int = 2, reps: int =
     `units` units of 128 diagonals at `limbs` limbs (1 GiB at 16 units, more
     than L2). Timed with CUDA events on the context stream after 3 warm-up
     calls. Algorithmic bytes: every plaintext read once per output, the
-    outputs written, the 16 sources (2 polynomials) read once."""
+    outputs written, the 16 sources (2 polynomials) read once. The kernel
+    is the diagonal chain's (afhe_eval_diag_inner_batch), or with `generic`
+    afhe_eval_mac_plain_batch on the same terms."""
     import numpy as np
     import torch
 
@@ -210,12 +212,22 @@ def mac_roofline(outputs: int = 64, units: int = 16, limbs: int = 2, reps: int =
         Ta = np.array(T, dtype=IQM.MAC_TERM)
         fg = np.array(first, dtype=np.uint32)
         refs = (L.CtRef * outputs)(*[L.CtRef(*c) for c in outs])
+        # the same terms in the structured form: per output its 16 sources and units
+        dsrc = (L.CtRef * (outputs * n1))(*[L.CtRef(*srcs[b]) for _ in range(outputs) for b in range(n1)])
+        upt = np.concatenate([Ta["pt"][o * n1 * units:o * n1 * units + units] for o in range(outputs)])
+        ugal = np.concatenate([Ta["galois"][o * n1 * units:o * n1 * units + units] for o in range(outputs)])
+        ufirst = np.arange(0, outputs * units + 1, units, dtype=np.uint32)
 
         def call():
-            L.check(ctx.lib.afhe_eval_mac_plain_batch(ctx.h, refs, fg.ctypes.data_as(L.P32), outputs,
-                                                      Ga.ctypes.data_as(ctypes.POINTER(L.MacGroup)),
-                                                      Ta.ctypes.data_as(ctypes.POINTER(L.MacTerm)), limbs, 0),
-                    "eval_mac_plain_batch")
+            if generic:
+                L.check(ctx.lib.afhe_eval_mac_plain_batch(ctx.h, refs, fg.ctypes.data_as(L.P32), outputs,
+                                                          Ga.ctypes.data_as(ctypes.POINTER(L.MacGroup)),
+                                                          Ta.ctypes.data_as(ctypes.POINTER(L.MacTerm)), limbs, 0),
+                        "eval_mac_plain_batch")
+            else:
+                L.check(ctx.lib.afhe_eval_diag_inner_batch(ctx.h, refs, outputs, dsrc, n1, upt.ctypes.data_as(L.P64),
+                                                           ugal.ctypes.data_as(L.P32), ufirst.ctypes.data_as(L.P32),
+                                                           w, limbs, 0), "eval_diag_inner_batch")
         for _ in range(3):
             call()
         ctx.sync()
@@ -229,7 +241,8 @@ def mac_roofline(outputs: int = 64, units: int = 16, limbs: int = 2, reps: int =
         ms = e0.elapsed_time(e1) / reps
         alg = (len(T) * w + outputs * 2 * w + n1 * 2 * w) * 8
         peak, src = load_peaks()
-        return {"profile": "mac_plain", "outputs": outputs, "terms": len(T), "limbs": limbs, "ms": round(ms, 4),
+        return {"profile": "mac_plain" if generic else "diag_inner", "outputs": outputs, "terms": len(T),
+                "limbs": limbs, "ms": round(ms, 4),
                 "algorithmic_bytes": alg, "achieved_gbs": round(alg / ms / 1e6, 1), "peak_gbs": peak,
                 "frac": round(alg / ms / 1e6 / peak, 3), "peak_source": src}
     finally:
@@ -416,6 +429,7 @@ def main() -> None:
     a = sub.add_parser("mac", help="the diagonal chain's inner-product kernel alone: outputs per call")
     a.add_argument("outputs", type=int)
     a.add_argument("--units", type=int, default=16)
+    a.add_argument("--generic", action="store_true", help="afhe_eval_mac_plain_batch instead of the structured kernel")
     sub.add_parser("host", help="end-to-end phases and the streamed run's host hotspots")
     a = sub.add_parser("dispatch", help="afhe_dispatch cost per call and op code")
     a.add_argument("--calls", type=int, default=200)
@@ -427,7 +441,7 @@ def main() -> None:
     elif args.what == "step":
         profile_step(args.queries, args.workload, args.lanes, args.tune)
     elif args.what == "mac":
-        print(json.dumps(mac_roofline(args.outputs, args.units)))
+        print(json.dumps(mac_roofline(args.outputs, args.units, generic=args.generic)))
     elif args.what == "dispatch":
         profile_dispatch(args.calls)
     else:

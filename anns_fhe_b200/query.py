@@ -1063,12 +1063,29 @@ class InteractiveQueryManager:
         L.check(self.lib.afhe_rescale_batch(self.ctx.h, self._refs(a), self._refs(d), len(a), in_limbs),
                 "rescale_batch")
 
-    def _giant(self, inner, jobs, Ll: int) -> None:
-        """Output k of the inner products jobs (_diag_jobs descriptors, giant
-        step g into inner[k n2 + g], Ll limbs): rescaled, giant step g
-        rotated by n1 g, summed into inner[k n2] (Ll - 1 limbs)."""
+    def _giant(self, inner, srcs, bases, gals, Ll: int) -> None:
+        """Output k (of len(srcs)): giant step g's inner product into
+        inner[k n2 + g] (Ll limbs): sum over units m and b < n1 of the unit's
+        plaintext bases[k][g, m] + b Ll N moved by gals[k][m] times srcs[k][b];
+        then rescaled, giant step g rotated by n1 g, summed into inner[k n2]
+        (Ll - 1 limbs)."""
         n1, n2 = self.sh.n1, self.sh.n2
-        self._mac(inner, *jobs, Ll)
+        stride = Ll * self.p.n
+        if n1 in (1, 2, 4, 8, 16):
+            sizes = np.repeat([b.shape[1] for b in bases], n2)
+            first = np.concatenate([[0], np.cumsum(sizes)]).astype(np.uint32)
+            upt = np.ascontiguousarray(np.concatenate([b.reshape(-1) for b in bases]) if bases else
+                                       np.zeros(1), dtype=np.uint64)
+            ugal = np.ascontiguousarray(np.concatenate([np.tile(np.asarray(g, dtype=np.uint32), n2) for g in gals])
+                                        if gals else np.zeros(1), dtype=np.uint32)
+            src = [c for k in range(len(srcs)) for _ in range(n2) for c in srcs[k]]
+            L.check(self.lib.afhe_eval_diag_inner_batch(self.ctx.h, self._refs(inner), len(inner), self._refs(src), n1,
+                                                        upt.ctypes.data_as(L.P64) if upt.size else None,
+                                                        ugal.ctypes.data_as(L.P32), first.ctypes.data_as(L.P32),
+                                                        stride, Ll, 0), "eval_diag_inner_batch")
+        else:
+            pts = [bs[:, None, :] + np.arange(n1, dtype=np.uint64)[None, :, None] * np.uint64(stride) for bs in bases]
+            self._mac(inner, *self._diag_jobs(srcs, pts, gals), Ll)
         self._rescale(inner, inner, Ll)
         self._rotate_direct([(inner[j], n1 * (j % n2)) for j in range(len(inner)) if j % n2], Ll - 1)
         self._sum_groups([inner[k:k + n2] for k in range(0, len(inner), n2)], Ll - 1)
@@ -1094,13 +1111,13 @@ class InteractiveQueryManager:
         while s < D:                         # ||q||^2 in every slot
             self._rot_acc(nrm, nrm, s, Ll - 1)
             s <<= 1
-        cent = np.asarray(dg["cent"], dtype=np.uint64).reshape(n2, n1, 1)
+        cent = np.asarray(dg["cent"], dtype=np.uint64)[np.arange(n2) * n1].reshape(n2, 1)
         per = len(self._inner) // n2
         for c0 in range(0, len(queries), per):
             qs = queries[c0:c0 + per]
             inner = self._inner[:len(qs) * n2]
-            self._giant(inner, self._diag_jobs([self._babies(q) for q in qs], [cent] * len(qs),
-                                               [np.ones(1, np.uint32)] * len(qs)), Ll)
+            self._giant(inner, [self._babies(q) for q in qs], [cent] * len(qs), [np.ones(1, np.uint32)] * len(qs),
+                        Ll)
             comp = [q.compact for q in qs]
             self._add(inner[0::n2], [q.norm for q in qs], comp, Ll - 1)
             self._add_plain(comp, [dg["cnorm"]] * len(qs), comp, Ll - 1)
@@ -1129,7 +1146,7 @@ class InteractiveQueryManager:
         D, S, n1, n2 = self.sh.D, self.sh.slots, self.sh.n1, self.sh.n2
         dg = self._diag[Ll]
         pts, norms = dg["pts"], dg["norms"]
-        ib = (np.arange(n2)[:, None, None] * n1 + np.arange(n1)[None, :, None])     # (n2, n1, 1)
+        g0 = np.arange(n2)[:, None] * n1          # diagonal g n1 (b = 0) of each giant step
         items = []
         for q in queries:
             used = q.layout[-1][1] // S + 1 if q.layout else 1
@@ -1143,9 +1160,8 @@ class InteractiveQueryManager:
         for c0 in range(0, len(items), per):
             it = items[c0:c0 + per]
             inner = self._inner[:len(it) * n2]
-            jobs = self._diag_jobs([self._babies(q) for q, _, _, _ in it],
-                                   [pts[u[None, None, :] * D + ib] for _, _, u, _ in it], [g for _, _, _, g in it])
-            self._giant(inner, jobs, Ll)
+            self._giant(inner, [self._babies(q) for q, _, _, _ in it], [pts[u[None, :] * D + g0] for _, _, u, _ in it],
+                        [g for _, _, _, g in it], Ll)
             outs = [q.results[r] for q, r, _, _ in it]
             self._add(inner[0::n2], [q.norm for q, _, _, _ in it], outs, Ll - 1)
             sizes = np.array([len(u) for _, _, u, _ in it], dtype=np.int64)

@@ -414,6 +414,18 @@ typedef struct afhe_mac_group {
 int afhe_eval_mac_plain_batch(afhe_ctx* ctx, const afhe_ct_ref* out, const uint32_t* first_group, uint32_t count,
                               const afhe_mac_group* groups, const afhe_mac_term* terms, uint32_t limbs,
                               uint32_t accumulate);
+/* The diagonal method's inner products in a fixed shape, the form the
+ * diagonal chain issues: for output j,
+ *   out[j] (+)= sum over units k in [first_unit[j], first_unit[j + 1]) of
+ *               sum over b < nb of automorphism(pt at unit_pt[k] + b pt_stride, unit_galois[k]) * src[j nb + b]
+ * (nb = 1, 2, 4, 8 or 16 baby steps; a unit's nb plaintexts lie pt_stride
+ * words apart). Equal to afhe_eval_mac_plain_batch with one group per baby
+ * step and one term per unit; the baby-step ciphertexts stay in registers and
+ * a unit's automorphism index is read once for its nb plaintexts. No output
+ * may overlap another output or any operand; first_unit has count + 1 entries. */
+int afhe_eval_diag_inner_batch(afhe_ctx* ctx, const afhe_ct_ref* out, uint32_t count, const afhe_ct_ref* src,
+                               uint32_t nb, const uint64_t* unit_pt, const uint32_t* unit_galois,
+                               const uint32_t* first_unit, uint64_t pt_stride, uint32_t limbs, uint32_t accumulate);
 /* dst[i] = a[i] (both polynomials, `limbs` limbs): the slot-to-slot copies the
  * reference's host makes between operators (eval_sub_plain's c1 copy,
  * fhe_host_driver.cpp:259-270), for many ciphertexts in one launch. */

@@ -100,3 +100,45 @@ def test_mac_plain_matches_host(q_bits):
         assert call(ctx, [src[6], src[6]], [[], []], limbs) == L.E_ARG
     finally:
         ctx.close()
+
+
+@pytest.mark.parametrize("nb", [1, 4, 16])
+def test_diag_inner_equals_mac_plain(nb):
+    """afhe_eval_diag_inner_batch equals afhe_eval_mac_plain_batch with one
+    group per baby step and one term per unit, units at pt + b * stride."""
+    log_n, limbs = 11, 2
+    q, p = primes_for(log_n, limbs, 50, 1, 60)
+    n = 1 << log_n
+    w = limbs * n
+    ctx = FheContext(CkksParams(log_n, q, p, 1), poly_words=600 * w, key_words=1024)
+    try:
+        rng = np.random.default_rng(nb)
+        ctx.write_poly(0, np.concatenate([uniform_residues(rng, q, n) for _ in range(500)]))
+        stride = 3 * w                                   # a unit's plaintexts 3 polynomials apart
+        srcs = [(2 * i * w, (2 * i + 1) * w) for i in range(32)]        # [0, 64 w)
+        units = [64 * w + k * w for k in range(48)]                     # plaintexts in [64 w, 64 w + 48 w + 45 stride)
+        gals = [1, galois_elt(log_n, -64), galois_elt(log_n, -256), galois_elt(log_n, 5)]
+        jobs = [(list(range(0, 5)), 0), (list(range(7, 9)), 1), ([], 2)]    # (units, first source)
+        outs_a = [((520 + 4 * j) * w, (521 + 4 * j) * w) for j in range(len(jobs))]
+        outs_b = [((522 + 4 * j) * w, (523 + 4 * j) * w) for j in range(len(jobs))]
+        src = (L.CtRef * (len(jobs) * nb))(*[L.CtRef(*srcs[(s + b) % 32]) for _, s in jobs for b in range(nb)])
+        upt = np.array([units[k] for ks, _ in jobs for k in ks] or [0], dtype=np.uint64)
+        ugal = np.array([gals[k % 4] for ks, _ in jobs for k in ks] or [1], dtype=np.uint32)
+        first = np.concatenate([[0], np.cumsum([len(ks) for ks, _ in jobs])]).astype(np.uint32)
+        oa = (L.CtRef * len(jobs))(*[L.CtRef(*c) for c in outs_a])
+        rc = ctx.lib.afhe_eval_diag_inner_batch(ctx.h, oa, len(jobs), src, nb, upt.ctypes.data_as(L.P64),
+                                                ugal.ctypes.data_as(L.P32), first.ctypes.data_as(L.P32), stride,
+                                                limbs, 0)
+        assert rc == L.OK, L.load().afhe_last_error()
+        mac_jobs = [[(srcs[(s + b) % 32], [(units[k] + b * stride, gals[k % 4]) for k in ks]) for b in range(nb)]
+                    for ks, s in jobs]
+        assert call(ctx, outs_b, mac_jobs, limbs) == L.OK
+        for a, b in zip(outs_a, outs_b):
+            assert np.array_equal(ctx.read_poly(a[0], w), ctx.read_poly(b[0], w))
+            assert np.array_equal(ctx.read_poly(a[1], w), ctx.read_poly(b[1], w))
+        # nb must be a power of two up to 16
+        assert ctx.lib.afhe_eval_diag_inner_batch(ctx.h, oa, 1, src, 3, upt.ctypes.data_as(L.P64),
+                                                  ugal.ctypes.data_as(L.P32), first.ctypes.data_as(L.P32), stride,
+                                                  limbs, 0) == L.E_ARG
+    finally:
+        ctx.close()
