@@ -97,7 +97,8 @@ class IvfpqShape(C.Structure):
 
 class IvfpqQuery(C.Structure):
     _fields_ = [("ct_query", CtRef), ("ct_dim", CtRef), ("compact", CtRef), ("norm", CtRef), ("results", C.POINTER(CtRef)),
-                ("n_results", u32), ("level", u32), ("probes", C.POINTER(u32)), ("nprobe", u32)]
+                ("n_results", u32), ("level", u32), ("probes", C.POINTER(u32)), ("nprobe", u32),
+                ("baby", C.POINTER(CtRef)), ("n_baby", u32)]
 
 
 CTX = C.c_void_p
@@ -180,6 +181,9 @@ SIGNATURES = {
     "afhe_eval_sub_batch": (C.c_int, [CTX, C.POINTER(CtRef), C.POINTER(CtRef), C.POINTER(CtRef), u32, u32]),
     "afhe_eval_mac_plain_batch": (C.c_int, [CTX, C.POINTER(CtRef), P32, u32, C.POINTER(MacGroup), C.POINTER(MacTerm),
                                             u32, u32]),
+    "afhe_ivfpq_set_units": (C.c_int, [C.c_void_p, P32, P32, u32]),
+    "afhe_ivfpq_set_diagonals": (C.c_int, [C.c_void_p, u32, u64, u64, P64, P64, u32]),
+    "afhe_ivfpq_set_scratch": (C.c_int, [C.c_void_p, C.POINTER(CtRef), u32]),
     "afhe_eval_diag_inner_batch": (C.c_int, [CTX, C.POINTER(CtRef), u32, C.POINTER(CtRef), u32, P64, P32, P32, u64,
                                              u32, u32]),
     "afhe_eval_add_plain_batch": (C.c_int, [CTX, C.POINTER(CtRef), P64, C.POINTER(CtRef), u32, u32]),

@@ -24,6 +24,15 @@
 //             packed, the mask itself is moved to the batch's row, since the
 //             tree sum leaves the sums in every row), accumulate into the
 //             query's result ciphertext
+//   diagonal  (shape.packed = 2) stage 1: the query rotated by 1 .. n1 - 1
+//             (baby steps, kept for stage 3), ||q||^2 (square, tree sum),
+//             the centroids' inner products by their diagonals (one
+//             afhe_eval_diag_inner_batch per giant step group), rescale,
+//             giant-step rotations by n1 g, sum, + ||q||^2 + ||c||^2;
+//             stage 3: the same per result ciphertext over the query's units,
+//             each unit's diagonals placed at its slot offset (a multiple of
+//             D) by an automorphism folded into the product's loads, then
+//             + ||q||^2 + the placed unit norms
 //
 // Plaintexts, masks and working ciphertexts stay resident in poly_gmem at the
 // offsets the caller registers (anns_fhe_b200/query.py encodes them). Modular
@@ -51,6 +60,15 @@ struct afhe_ivfpq {
     std::vector<afhe_ct_ref> cmp;                       // (n_list - 1) per lane: reference compaction terms
     std::map<uint32_t, afhe_ks_options> tuning;        // level -> key-switch options
     bool fused_ok = false;                              // the one-kernel key switch was on at creation
+    // diagonal chain
+    struct Diag {
+        u64 cent = 0, cnorm = 0;                        // centroids' first diagonal, their norms
+        std::vector<u64> unit_pts, unit_norms;          // per unit: first diagonal, norms
+    };
+    std::map<uint32_t, Diag> diag;                      // level -> plaintexts
+    std::vector<uint32_t> list_first_unit;              // [n_list + 1]
+    std::vector<uint32_t> unit_count;                   // candidates per unit
+    std::vector<afhe_ct_ref> scratch;                   // inner-product ciphertexts
 };
 
 namespace {
@@ -60,8 +78,18 @@ typedef std::vector<afhe_ct_ref> Cts;
 int fail_h(afhe_ivfpq* h, int code, const char* msg) { return fail(h ? h->ctx : nullptr, code, msg); }
 
 uint32_t n_coarse(const afhe_ivfpq_shape& s) {
+    if (s.packed == 2) return 1;
     const uint32_t per = s.slots / s.D;
     return (s.n_list + per - 1) / per;
+}
+
+bool diagonal(const afhe_ivfpq* h) { return h->sh.packed == 2; }
+
+// Baby steps of the diagonal method: 2^ceil(log2(D) / 2); giant steps D / n1.
+uint32_t baby_steps(uint32_t D) {
+    uint32_t lg = 0;
+    while ((1u << lg) < D) ++lg;
+    return 1u << ((lg + 1) / 2);
 }
 
 uint32_t eval_at(const afhe_ivfpq* h, uint32_t level) {
@@ -386,7 +414,181 @@ int stage3_items(afhe_ivfpq* h, const afhe_ivfpq_query* q, const std::vector<Ite
     return AFHE_OK;
 }
 
+// ---- the diagonal chain ----------------------------------------------------
+// One output of the inner products: its baby-step sources (n1 ciphertexts)
+// and its placed units (first diagonal of the unit at giant step 0, galois).
+struct InnerOut {
+    const afhe_ct_ref* query;              // the query (baby step 0)
+    const afhe_ct_ref* baby;               // baby steps 1 .. n1 - 1
+    std::vector<std::pair<u64, uint32_t>> units;
+};
+
+// For each output k: giant step g's inner product into scr[k n2 + g] (Ll
+// limbs), the sum over its units and b < n1 of diagonal g n1 + b (unit base +
+// (g n1 + b) Ll N) moved by the unit's automorphism, times baby step b; then
+// rescaled, giant step g rotated by n1 g, summed into scr[k n2] (Ll - 1 limbs).
+int giant(afhe_ivfpq* h, const std::vector<InnerOut>& outs, const Cts& scr, uint32_t Ll) {
+    const uint32_t n1 = baby_steps(h->sh.D), n2 = h->sh.D / n1;
+    const u64 stride = (u64)Ll * h->ctx->n;
+    const uint32_t count = (uint32_t)outs.size() * n2;
+    Cts inner(scr.begin(), scr.begin() + count), src;
+    std::vector<u64> upt;
+    std::vector<uint32_t> ugal, first{0};
+    for (const auto& o : outs)
+        for (uint32_t g = 0; g < n2; ++g) {
+            src.push_back(*o.query);
+            for (uint32_t b = 1; b < n1; ++b) src.push_back(o.baby[b - 1]);
+            for (const auto& u : o.units) {
+                upt.push_back(u.first + (u64)g * n1 * stride);
+                ugal.push_back(u.second);
+            }
+            first.push_back((uint32_t)upt.size());
+        }
+    if (n1 <= 16) {
+        RC(afhe_eval_diag_inner_batch(h->ctx, inner.data(), count, src.data(), n1, upt.data(), ugal.data(),
+                                      first.data(), stride, Ll, 0));
+    } else {                                          // the generic form: one group per baby step
+        std::vector<afhe_mac_group> G;
+        std::vector<afhe_mac_term> T;
+        std::vector<uint32_t> fg{0};
+        for (uint32_t j = 0; j < count; ++j) {
+            for (uint32_t b = 0; b < n1; ++b) {
+                G.push_back(afhe_mac_group{src[(size_t)j * n1 + b], (uint32_t)T.size(), first[j + 1] - first[j]});
+                for (uint32_t k = first[j]; k < first[j + 1]; ++k) T.push_back(afhe_mac_term{upt[k] + b * stride, ugal[k], 0});
+            }
+            fg.push_back((uint32_t)G.size());
+        }
+        RC(afhe_eval_mac_plain_batch(h->ctx, inner.data(), fg.data(), count, G.data(), T.data(), Ll, 0));
+    }
+    RC(afhe_rescale_batch(h->ctx, inner.data(), inner.data(), count, Ll));
+    std::vector<std::pair<afhe_ct_ref, int32_t>> rot;
+    std::vector<Cts> groups;
+    for (size_t k = 0; k < outs.size(); ++k) {
+        groups.push_back(Cts(inner.begin() + k * n2, inner.begin() + (k + 1) * n2));
+        for (uint32_t g = 1; g < n2; ++g) rot.push_back({inner[k * n2 + g], (int32_t)(n1 * g)});
+    }
+    RC(rotate_direct(h, rot, Ll - 1));
+    return sum_groups(h, groups, Ll - 1);
+}
+
+int stage1_diagonal(afhe_ivfpq* h, const afhe_ivfpq_query* q, const std::vector<uint32_t>& idx, uint32_t Ll) {
+    const uint32_t D = h->sh.D, n1 = baby_steps(D), n2 = D / n1;
+    const afhe_ivfpq::Diag& dg = h->diag.at(Ll);
+    Cts src, dst, cq, nrm;
+    std::vector<int32_t> steps;
+    for (uint32_t i : idx) {
+        for (uint32_t b = 1; b < n1; ++b) {
+            src.push_back(q[i].ct_query);
+            dst.push_back(q[i].baby[b - 1]);
+            steps.push_back((int32_t)b);
+        }
+        cq.push_back(q[i].ct_query);
+        nrm.push_back(q[i].norm);
+    }
+    if (!src.empty()) {
+        at(h, Ll);
+        RC(afhe_eval_rotate_steps_batch(h->ctx, src.data(), dst.data(), steps.data(), (uint32_t)src.size(), Ll));
+    }
+    RC(square(h, cq, nrm, Ll));                           // ||q||^2 in every slot: square, tree sum
+    for (uint32_t s = 1; s < D; s <<= 1) RC(rot_acc(h, nrm, nrm, (int32_t)s, Ll - 1));
+    const size_t per = h->scratch.size() / n2;
+    for (size_t c0 = 0; c0 < idx.size(); c0 += per) {
+        const size_t m = std::min(per, idx.size() - c0);
+        std::vector<InnerOut> outs;
+        Cts heads, norms, comp;
+        for (size_t k = 0; k < m; ++k) {
+            const afhe_ivfpq_query& x = q[idx[c0 + k]];
+            outs.push_back(InnerOut{&x.ct_query, x.baby, {{dg.cent, 1u}}});
+            heads.push_back(h->scratch[k * n2]);
+            norms.push_back(x.norm);
+            comp.push_back(x.compact);
+        }
+        RC(giant(h, outs, h->scratch, Ll));
+        RC(add(h, heads, norms, comp, Ll - 1));
+        RC(add_plain(h, comp, std::vector<u64>(m, dg.cnorm), comp, Ll - 1));
+    }
+    return AFHE_OK;
+}
+
+// The slot offsets of a query's units (probe order): spans of count rounded
+// up to a multiple of D, back to back, a unit that would cross a result's end
+// starting the next result. Returns false on a list out of range.
+bool unit_layout(const afhe_ivfpq* h, const afhe_ivfpq_query& q, std::vector<std::pair<uint32_t, u64>>& out) {
+    const u64 S = h->sh.slots, D = h->sh.D;
+    u64 off = 0;
+    out.clear();
+    for (uint32_t p = 0; p < q.nprobe; ++p) {
+        const uint32_t c = q.probes[p];
+        if (c >= h->sh.n_list) return false;
+        for (uint32_t u = h->list_first_unit[c]; u < h->list_first_unit[c + 1]; ++u) {
+            const u64 span = (h->unit_count[u] + D - 1) / D * D;
+            if (off % S + span > S) off = (off / S + 1) * S;
+            out.push_back({u, off});
+            off += span;
+        }
+    }
+    return true;
+}
+
+int stage3_diagonal(afhe_ivfpq* h, const afhe_ivfpq_query* q, const std::vector<uint32_t>& idx, uint32_t Ll) {
+    const uint32_t D = h->sh.D, n1 = baby_steps(D), n2 = D / n1;
+    const u64 S = h->sh.slots;
+    const afhe_ivfpq::Diag& dg = h->diag.at(Ll);
+    struct It {
+        uint32_t qi, r;
+        std::vector<std::pair<uint32_t, uint32_t>> units;     // (unit, galois)
+    };
+    std::vector<It> items;
+    std::vector<std::pair<uint32_t, u64>> lay;
+    for (uint32_t i : idx) {
+        unit_layout(h, q[i], lay);
+        const uint32_t used = lay.empty() ? 1u : (uint32_t)(lay.back().second / S) + 1;
+        for (uint32_t r = 0; r < used; ++r) {
+            It it{i, r, {}};
+            for (const auto& u : lay)
+                if (u.second / S == r)
+                    it.units.push_back({u.first, afhe_galois_elt((uint32_t)h->ctx->log_n, -(int32_t)(u.second % S))});
+            items.push_back(std::move(it));
+        }
+    }
+    const size_t per = h->scratch.size() / n2;
+    for (size_t c0 = 0; c0 < items.size(); c0 += per) {
+        const size_t m = std::min(per, items.size() - c0);
+        std::vector<InnerOut> outs;
+        Cts heads, norms, res;
+        std::vector<afhe_mac_group> G;
+        std::vector<afhe_mac_term> T;
+        std::vector<uint32_t> fg{0};
+        for (size_t k = 0; k < m; ++k) {
+            const It& it = items[c0 + k];
+            const afhe_ivfpq_query& x = q[it.qi];
+            InnerOut o{&x.ct_query, x.baby, {}};
+            G.push_back(afhe_mac_group{afhe_ct_ref{AFHE_MAC_UNIT, 0}, (uint32_t)T.size(), (uint32_t)it.units.size()});
+            for (const auto& u : it.units) {
+                o.units.push_back({dg.unit_pts[u.first], u.second});
+                T.push_back(afhe_mac_term{dg.unit_norms[u.first], u.second, 0});
+            }
+            fg.push_back((uint32_t)G.size());
+            outs.push_back(std::move(o));
+            heads.push_back(h->scratch[k * n2]);
+            norms.push_back(x.norm);
+            res.push_back(x.results[it.r]);
+        }
+        RC(giant(h, outs, h->scratch, Ll));
+        RC(add(h, heads, norms, res, Ll - 1));            // + ||q||^2, then + the placed unit norms
+        RC(afhe_eval_mac_plain_batch(h->ctx, res.data(), fg.data(), (uint32_t)m, G.data(), T.data(), Ll - 1, 1));
+    }
+    return AFHE_OK;
+}
+
 int check_query(afhe_ivfpq* h, const afhe_ivfpq_query& q) {
+    if (diagonal(h)) {
+        if (q.level > h->ctx->L || (q.level && q.level < 2)) return fail_h(h, AFHE_E_LEVEL, "query level outside [2, L]");
+        if (!h->diag.count(eval_at(h, q.level))) return fail_h(h, AFHE_E_STATE, "no diagonals for the query's level");
+        if (q.n_baby != baby_steps(h->sh.D) - 1 || (q.n_baby && !q.baby))
+            return fail_h(h, AFHE_E_ARG, "a query needs n1 - 1 baby-step ciphertexts");
+        return AFHE_OK;
+    }
     if (q.level > h->ctx->L || (q.level && q.level < 3)) return fail_h(h, AFHE_E_LEVEL, "query level outside [3, L]");
     if (!h->masks.count(eval_at(h, q.level))) return fail_h(h, AFHE_E_STATE, "no masks for the query's level");
     return AFHE_OK;
@@ -402,9 +604,13 @@ int afhe_ivfpq_create(afhe_ctx* ctx, const afhe_ivfpq_shape* shape, afhe_ivfpq**
     if (s.D < 2 || (s.D & (s.D - 1)) || s.slots != ctx->n / 2 || s.D > s.slots || s.n_list < 1 || s.lanes < 1 ||
         s.lanes > ctx->lanes)
         return fail(ctx, AFHE_E_ARG, "ivfpq shape: D a power of two <= N/2, slots = N/2, lanes in [1, context lanes]");
-    if (!s.packed && s.n_list * s.D > s.slots) return fail(ctx, AFHE_E_ARG, "centroids do not fit one ciphertext");
-    if (s.packed && n_coarse(s) > s.D) return fail(ctx, AFHE_E_ARG, "packed compaction needs n_coarse <= D");
-    if (s.eval_level && (s.eval_level < 3 || s.eval_level > ctx->L)) return fail(ctx, AFHE_E_LEVEL, "eval_level in [3, L]");
+    if (s.packed > 2) return fail(ctx, AFHE_E_ARG, "compaction: 0 reference, 1 packed, 2 diagonal");
+    if (s.packed == 0 && s.n_list * s.D > s.slots) return fail(ctx, AFHE_E_ARG, "centroids do not fit one ciphertext");
+    if (s.packed == 1 && n_coarse(s) > s.D) return fail(ctx, AFHE_E_ARG, "packed compaction needs n_coarse <= D");
+    if (s.packed == 2 && s.n_list > s.slots) return fail(ctx, AFHE_E_ARG, "the diagonal chain needs n_list <= N/2");
+    const uint32_t min_level = s.packed == 2 ? 2 : 3;     // the chain's depth + 1
+    if (s.eval_level && (s.eval_level < min_level || s.eval_level > ctx->L))
+        return fail(ctx, AFHE_E_LEVEL, "eval_level in [depth + 1, L]");
     afhe_ivfpq* h = new afhe_ivfpq();
     h->ctx = ctx;
     h->sh = s;
@@ -479,8 +685,58 @@ int afhe_ivfpq_set_tuning(afhe_ivfpq* h, uint32_t level, const afhe_ks_options* 
     return AFHE_OK;
 }
 
+int afhe_ivfpq_set_units(afhe_ivfpq* h, const uint32_t* list_first_unit, const uint32_t* counts, uint32_t units) {
+    if (!h || !list_first_unit || (units && !counts)) return fail_h(h, AFHE_E_ARG, "null argument");
+    if (!diagonal(h)) return fail_h(h, AFHE_E_STATE, "units are for the diagonal chain");
+    if (list_first_unit[0] != 0 || list_first_unit[h->sh.n_list] != units)
+        return fail_h(h, AFHE_E_ARG, "list_first_unit must run from 0 to units");
+    for (uint32_t c = 0; c < h->sh.n_list; ++c)
+        if (list_first_unit[c + 1] < list_first_unit[c]) return fail_h(h, AFHE_E_ARG, "unit ranges must not decrease");
+    for (uint32_t u = 0; u < units; ++u)
+        if (counts[u] < 1 || counts[u] > h->sh.slots) return fail_h(h, AFHE_E_ARG, "unit count outside [1, N/2]");
+    h->list_first_unit.assign(list_first_unit, list_first_unit + h->sh.n_list + 1);
+    h->unit_count.assign(counts, counts + units);
+    return AFHE_OK;
+}
+
+int afhe_ivfpq_set_diagonals(afhe_ivfpq* h, uint32_t level, uint64_t centroids, uint64_t centroid_norms,
+                             const uint64_t* unit_pts, const uint64_t* unit_norms, uint32_t units) {
+    if (!h || (units && (!unit_pts || !unit_norms))) return fail_h(h, AFHE_E_ARG, "null argument");
+    if (!diagonal(h)) return fail_h(h, AFHE_E_STATE, "diagonals are for the diagonal chain");
+    if (level < 2 || level > h->ctx->L) return fail_h(h, AFHE_E_LEVEL, "level in [2, L]");
+    if (units != h->unit_count.size()) return fail_h(h, AFHE_E_ARG, "one set of diagonals per unit (set the units first)");
+    const u64 w = (u64)level * h->ctx->n, span = (u64)h->sh.D * w;
+    if (!range_ok(centroids, span, h->ctx->prm.poly_words) ||
+        !range_ok(centroid_norms, (u64)(level - 1) * h->ctx->n, h->ctx->prm.poly_words))
+        return fail_h(h, AFHE_E_RANGE, "centroid plaintexts out of poly_gmem");
+    for (uint32_t u = 0; u < units; ++u)
+        if (!range_ok(unit_pts[u], span, h->ctx->prm.poly_words) ||
+            !range_ok(unit_norms[u], (u64)(level - 1) * h->ctx->n, h->ctx->prm.poly_words))
+            return fail_h(h, AFHE_E_RANGE, "unit plaintexts out of poly_gmem");
+    afhe_ivfpq::Diag& d = h->diag[level];
+    d.cent = centroids;
+    d.cnorm = centroid_norms;
+    d.unit_pts.assign(unit_pts, unit_pts + units);
+    d.unit_norms.assign(unit_norms, unit_norms + units);
+    return AFHE_OK;
+}
+
+int afhe_ivfpq_set_scratch(afhe_ivfpq* h, const afhe_ct_ref* cts, uint32_t count) {
+    if (!h || (count && !cts)) return fail_h(h, AFHE_E_ARG, "null argument");
+    const uint32_t n2 = h->sh.D / baby_steps(h->sh.D);
+    if (count < n2) return fail_h(h, AFHE_E_ARG, "at least D / n1 working ciphertexts");
+    h->scratch.assign(cts, cts + count / n2 * n2);
+    return AFHE_OK;
+}
+
 int afhe_ivfpq_stage1(afhe_ivfpq* h, const afhe_ivfpq_query* q, uint32_t count) {
     if (!h || (count && !q)) return fail_h(h, AFHE_E_ARG, "null argument");
+    if (diagonal(h)) {
+        if (h->scratch.empty()) return fail_h(h, AFHE_E_STATE, "scratch not set");
+        for (uint32_t i = 0; i < count; ++i) RC(check_query(h, q[i]));
+        for (auto& g : by_level(h, q, count)) RC(stage1_diagonal(h, q, g.second, g.first));
+        return AFHE_OK;
+    }
     if (h->work.empty() || h->centroid_cts.empty()) return fail_h(h, AFHE_E_STATE, "lanes and centroids not set");
     for (uint32_t i = 0; i < count; ++i) RC(check_query(h, q[i]));
     for (auto& g : by_level(h, q, count))
@@ -490,6 +746,19 @@ int afhe_ivfpq_stage1(afhe_ivfpq* h, const afhe_ivfpq_query* q, uint32_t count) 
 
 int afhe_ivfpq_stage3(afhe_ivfpq* h, const afhe_ivfpq_query* q, uint32_t count) {
     if (!h || (count && !q)) return fail_h(h, AFHE_E_ARG, "null argument");
+    if (diagonal(h)) {
+        if (h->scratch.empty() || h->list_first_unit.empty()) return fail_h(h, AFHE_E_STATE, "scratch and units not set");
+        std::vector<std::pair<uint32_t, u64>> lay;
+        for (uint32_t i = 0; i < count; ++i) {
+            RC(check_query(h, q[i]));
+            if (q[i].nprobe && !q[i].probes) return fail_h(h, AFHE_E_ARG, "null probes");
+            if (!unit_layout(h, q[i], lay)) return fail_h(h, AFHE_E_RANGE, "probed list out of range");
+            if (!lay.empty() && lay.back().second / h->sh.slots >= q[i].n_results)
+                return fail_h(h, AFHE_E_RANGE, "more candidates than the result ciphertexts hold");
+        }
+        for (auto& g : by_level(h, q, count)) RC(stage3_diagonal(h, q, g.second, g.first));
+        return AFHE_OK;
+    }
     if (h->work.empty()) return fail_h(h, AFHE_E_STATE, "lanes not set");
     const uint32_t S = h->sh.slots, B = S / h->sh.D;
     std::vector<uint32_t> first_batch(h->sh.n_list + 1, 0);      // global number of each list's first batch

@@ -764,12 +764,24 @@ class InteractiveQueryManager:
             return self._nh
         self.close_native()
         sh = self.sh
-        shape = L.IvfpqShape(sh.D, sh.n_list, sh.slots, self.lanes, int(sh.compaction == "packed"),
-                             sh.eval_level or 0)
+        kind = {"reference": 0, "packed": 1, "diagonal": 2}[sh.compaction]
+        shape = L.IvfpqShape(sh.D, sh.n_list, sh.slots, self.lanes, kind, sh.eval_level or 0)
         h = C.c_void_p()
         L.check(self.lib.afhe_ivfpq_create(self.ctx.h, C.byref(shape), C.byref(h)), "ivfpq_create")
         self._nh = h
         lib = self.lib
+        if kind == 2:
+            first = np.concatenate([[0], np.cumsum([len(u) for u in self.list_units])]).astype(np.uint32)
+            cnt = np.asarray(self._ucnt or [0], dtype=np.uint32)
+            L.check(lib.afhe_ivfpq_set_units(h, first.ctypes.data_as(L.P32), cnt.ctypes.data_as(L.P32),
+                                             len(self.units)), "ivfpq_set_units")
+            for lv, d in self._diag.items():
+                L.check(lib.afhe_ivfpq_set_diagonals(h, lv, int(d["cent"][0]), int(d["cnorm"]), self._offs(d["pts"][::sh.D]),
+                                                     self._offs(d["norms"]), len(self.units)), "ivfpq_set_diagonals")
+            L.check(lib.afhe_ivfpq_set_scratch(h, self._refs(self._inner), len(self._inner)), "ivfpq_set_scratch")
+            self._native_tuning(h)
+            self._nh_key = key
+            return h
         L.check(lib.afhe_ivfpq_set_centroids(h, self._offs(self.pt_centroid_cts), len(self.pt_centroid_cts)),
                 "ivfpq_set_centroids")
         for lv in self.levels:
@@ -786,12 +798,15 @@ class InteractiveQueryManager:
         work = self._refs([w[k] for w in self.work[:self.lanes] for k in ("diff", "sq", "sel", "tmp")])
         cmp = self._refs([c for row in self.cmp[:self.lanes] for c in row]) if self.cmp else None
         L.check(lib.afhe_ivfpq_set_lanes(h, work, self.lanes, cmp), "ivfpq_set_lanes")
+        self._native_tuning(h)
+        self._nh_key = key
+        return h
+
+    def _native_tuning(self, h) -> None:
         for lv, ch in getattr(self, "_tuning", {}).items():
             o = L.KsOptions(int(ch.fused), int(ch.chunk), int(getattr(ch, "ept", 8)), int(getattr(ch, "slice", 13)),
                             int(getattr(ch, "fused_min", 0)))
-            L.check(lib.afhe_ivfpq_set_tuning(h, lv, C.byref(o)), "ivfpq_set_tuning")
-        self._nh_key = key
-        return h
+            L.check(self.lib.afhe_ivfpq_set_tuning(h, lv, C.byref(o)), "ivfpq_set_tuning")
 
     def close_native(self) -> None:
         if self._nh is not None:
@@ -815,6 +830,10 @@ class InteractiveQueryManager:
                 pr = (C.c_uint32 * max(1, len(r.probes)))(*[int(c) for c in r.probes])
                 q.probes, q.nprobe = pr, len(r.probes)
                 keep.append(pr)
+            if r.baby:
+                bb = (L.CtRef * len(r.baby))(*[L.CtRef(*c) for c in r.baby])
+                q.baby, q.n_baby = bb, len(r.baby)
+                keep.append(bb)
         return arr, keep
 
     # ---- batched C-ABI helpers ----
@@ -1021,7 +1040,7 @@ class InteractiveQueryManager:
 
     # ---- the diagonal chain: stages ----
     def _native_diagonal(self) -> bool:
-        return False
+        return self.native
 
     MAC_GROUP = np.dtype([("c0", "<u8"), ("c1", "<u8"), ("first", "<u4"), ("n", "<u4")])
     MAC_TERM = np.dtype([("pt", "<u8"), ("galois", "<u4"), ("reserved", "<u4")])
@@ -1197,6 +1216,10 @@ class InteractiveQueryManager:
                 for lv, idx in self._by_level(queries, self.level_of):
                     self._stage3_diagonal([queries[i] for i in idx], lv)
                 return
+            arr, keep = self._native_queries(queries, probes=True)
+            L.check(self.lib.afhe_ivfpq_stage3(self._native_handle(), arr, len(queries)), "ivfpq_stage3")
+            self._opt_now = None
+            return
         items: dict[int, list] = {}
         for qi, q in enumerate(queries):
             q.vids, q.pos = [], []

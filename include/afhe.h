@@ -517,7 +517,9 @@ typedef struct afhe_ivfpq_shape {
     uint32_t lanes;       /* ciphertexts per batched call, <= the context's lanes */
     uint32_t packed;      /* 0: the reference's compaction (one-hot masks, eval_rotate's
                              power-of-two steps); 1: centroids over ceil(n_list / (slots / D))
-                             ciphertexts, one stride mask, one key switch per placement */
+                             ciphertexts, one stride mask, one key switch per placement;
+                             2: the diagonal chain (baby-step giant-step inner products,
+                             afhe_ivfpq_set_units / _set_diagonals / _set_scratch) */
     uint32_t eval_level;  /* limbs the chain runs at (0: each query's own level) */
 } afhe_ivfpq_shape;
 typedef struct afhe_ivfpq_query {
@@ -530,6 +532,9 @@ typedef struct afhe_ivfpq_query {
     uint32_t level;              /* limbs of the encrypted query (0: the top level) */
     const uint32_t* probes;      /* stage 3: the lists the client selected, in order */
     uint32_t nprobe;
+    const afhe_ct_ref* baby;     /* diagonal chain: the query rotated by 1 .. n1 - 1 (stage 1 output,
+                                    stage 3 input), n1 - 1 ciphertexts */
+    uint32_t n_baby;
 } afhe_ivfpq_query;
 int afhe_ivfpq_create(afhe_ctx* ctx, const afhe_ivfpq_shape* shape, afhe_ivfpq** out);
 int afhe_ivfpq_destroy(afhe_ivfpq* h);
@@ -564,6 +569,21 @@ typedef struct afhe_ks_options {
     uint32_t chunk, ept, slice, fused_min;
 } afhe_ks_options;
 int afhe_ivfpq_set_tuning(afhe_ivfpq* h, uint32_t level, const afhe_ks_options* opts);
+/* Diagonal chain (shape.packed = 2). Units: list c holds units
+ * [list_first_unit[c], list_first_unit[c + 1]), unit u counts[u] candidates
+ * (<= N/2); a query's units are placed in probe order at multiples of D,
+ * starting a new result ciphertext where one would not fit. */
+int afhe_ivfpq_set_units(afhe_ivfpq* h, const uint32_t* list_first_unit, const uint32_t* counts, uint32_t units);
+/* The plaintexts of queries evaluated at `level` limbs: the centroids' D
+ * diagonals from `centroids` (stride level N words) and their squared norms
+ * (level - 1 limbs); per unit its D diagonals from unit_pts[u] (stride level
+ * N) and its squared norms unit_norms[u] (afhe_pq_encode_diagonals,
+ * afhe_pq_encode_unit_norms). */
+int afhe_ivfpq_set_diagonals(afhe_ivfpq* h, uint32_t level, uint64_t centroids, uint64_t centroid_norms,
+                             const uint64_t* unit_pts, const uint64_t* unit_norms, uint32_t units);
+/* Working ciphertexts of the inner products (at least D / n1, a multiple of it
+ * used at a time), each with room for the highest evaluation level. */
+int afhe_ivfpq_set_scratch(afhe_ivfpq* h, const afhe_ct_ref* cts, uint32_t count);
 int afhe_ivfpq_stage1(afhe_ivfpq* h, const afhe_ivfpq_query* queries, uint32_t count);
 int afhe_ivfpq_stage3(afhe_ivfpq* h, const afhe_ivfpq_query* queries, uint32_t count);
 

@@ -47,6 +47,7 @@ afhe_ctx* trace_ctx_new(uint32_t L, uint32_t n, uint32_t lanes) {
     c->log_n = 0;
     while ((1u << c->log_n) < n) ++c->log_n;
     c->lanes = lanes;
+    c->prm.poly_words = 1ull << 60;      // every recorded offset is in range
     g_log.clear();
     g_fused = 1;
     g_chunk = 0;
@@ -166,6 +167,42 @@ int afhe_eval_rotate_steps_batch(afhe_ctx*, const afhe_ct_ref* in, const afhe_ct
     for (uint32_t i = 0; i < n; ++i) s += " " + std::to_string(steps[i]);
     s += " |";
     refs(s, in, n), refs(s, d, n);
+    g_log.push_back(s);
+    return AFHE_OK;
+}
+
+int afhe_rescale_batch(afhe_ctx*, const afhe_ct_ref* a, const afhe_ct_ref* d, uint32_t n, uint32_t limbs) {
+    std::string s = head("rescale", limbs, false);
+    refs(s, a, n), refs(s, d, n);
+    g_log.push_back(s);
+    return AFHE_OK;
+}
+int afhe_eval_diag_inner_batch(afhe_ctx*, const afhe_ct_ref* out, uint32_t n, const afhe_ct_ref* src, uint32_t nb,
+                               const uint64_t* upt, const uint32_t* ugal, const uint32_t* first, uint64_t stride,
+                               uint32_t limbs, uint32_t accumulate) {
+    std::string s = head("diag_inner", limbs, false) + " nb=" + std::to_string(nb) + " stride=" +
+                    std::to_string(stride) + " acc=" + std::to_string(accumulate) + " |";
+    refs(s, out, n), refs(s, src, n * nb);
+    for (uint32_t j = 0; j < n; ++j) {
+        for (uint32_t k = first[j]; k < first[j + 1]; ++k) s += " " + std::to_string(upt[k]) + "@" + std::to_string(ugal[k]);
+        s += " ;";
+    }
+    g_log.push_back(s);
+    return AFHE_OK;
+}
+int afhe_eval_mac_plain_batch(afhe_ctx*, const afhe_ct_ref* out, const uint32_t* first, uint32_t n,
+                              const afhe_mac_group* g, const afhe_mac_term* t, uint32_t limbs, uint32_t accumulate) {
+    std::string s = head("mac", limbs, false) + " acc=" + std::to_string(accumulate) + " |";
+    refs(s, out, n);
+    for (uint32_t j = 0; j < n; ++j) {
+        for (uint32_t k = first[j]; k < first[j + 1]; ++k) {
+            s += " [" + std::to_string(g[k].src.c0_offset) + ":" + std::to_string(g[k].src.c1_offset);
+            for (uint32_t x = g[k].first_term; x < g[k].first_term + g[k].n_terms; ++x)
+                s += " " + std::to_string(t[x].pt) + "@" + std::to_string(t[x].galois);
+            s += "]";
+        }
+        s += " ;";
+    }
     g_log.push_back(s);
     return AFHE_OK;
 }

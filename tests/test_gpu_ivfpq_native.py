@@ -2,8 +2,8 @@
 
 InteractiveQueryManager runs stages 1/1b and 3 in C++ by default
 (afhe_ivfpq_stage1 / afhe_ivfpq_stage3, csrc/ivfpq.cu); native=False runs
-them from Python over the batched C ABI. For the reference compaction, the
-packed compaction, mixed query levels and a reduced evaluation level, every
+them from Python over the batched C ABI. For the reference, packed and
+diagonal chains, mixed query levels and a reduced evaluation level, every
 word of every compacted coarse ciphertext and result ciphertext must be
 equal. (test_gpu_chain_parity.py checks the native path against the oracle's
 one-ciphertext-at-a-time chain; test_ivfpq_native_trace.py checks the two
@@ -15,6 +15,7 @@ import pytest
 
 from anns_fhe_b200.workloads import SMALL, Workload
 from tests.test_gpu_chain_parity import TINY, TINY_PACKED
+from tests.test_gpu_diagonal_chain import TINY_DIAG, TINY_UNITS
 
 pytestmark = pytest.mark.gpu
 
@@ -53,7 +54,11 @@ def both_ways(wl, Q, levels=None, nprobes=None):
     (dataclasses.replace(TINY_PACKED, name="ivfpq_2048x8_nlist128_N1024_L5_eval3", num_q=5, eval_level=3),
      [5, 4, 3], [2, 3, 4], 4),
     (SMALL, None, None, 64),
-], ids=["tiny", "tiny_lanes3_probes", "tiny_packed_levels", "tiny_packed_eval3", "small"])
+    (TINY_DIAG, [4, 3, 4], [30, 40, 12], 16),
+    (dataclasses.replace(TINY_UNITS, eval_level=2), [4, 3], None, 3),
+    (dataclasses.replace(SMALL, name=SMALL.name + "_diag", compaction="diagonal", eval_level=2), None, None, 64),
+], ids=["tiny", "tiny_lanes3_probes", "tiny_packed_levels", "tiny_packed_eval3", "small", "tiny_diagonal_levels",
+        "tiny_diagonal_units_eval2", "small_diagonal"])
 def test_native_equals_python(spec, levels, nprobes, lanes):
     n = len(levels) if levels else 5
     wl = Workload(spec, max_queries=n, lanes=lanes, levels=sorted(set(levels or [])) or None,

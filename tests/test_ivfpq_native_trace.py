@@ -47,6 +47,7 @@ def trace(tmp_path_factory):
     lib.trace_line.restype, lib.trace_line.argtypes = C.c_char_p, [C.c_uint32]
     for name in ("afhe_ivfpq_create", "afhe_ivfpq_destroy", "afhe_ivfpq_set_centroids", "afhe_ivfpq_set_level_masks",
                  "afhe_ivfpq_set_prefix_mask", "afhe_ivfpq_set_list", "afhe_ivfpq_set_lanes", "afhe_ivfpq_set_tuning",
+                 "afhe_ivfpq_set_units", "afhe_ivfpq_set_diagonals", "afhe_ivfpq_set_scratch",
                  "afhe_ivfpq_stage1", "afhe_ivfpq_stage3"):
         fn = getattr(lib, name)
         fn.restype, fn.argtypes = L.SIGNATURES[name]
@@ -124,6 +125,29 @@ class FakeLib:
                         + self._refs(d, n))
         return 0
 
+    def afhe_rescale_batch(self, h, a, d, n, limbs):
+        self.log.append(self._head("rescale", limbs, False) + self._refs(a, n) + self._refs(d, n))
+        return 0
+
+    def afhe_eval_diag_inner_batch(self, h, out, n, src, nb, upt, ugal, first, stride, limbs, acc):
+        s = self._head("diag_inner", limbs, False) + f" nb={nb} stride={stride} acc={acc} |"
+        s += self._refs(out, n) + self._refs(src, n * nb)
+        for j in range(n):
+            s += "".join(f" {int(upt[k])}@{int(ugal[k])}" for k in range(first[j], first[j + 1])) + " ;"
+        self.log.append(s)
+        return 0
+
+    def afhe_eval_mac_plain_batch(self, h, out, first, n, g, t, limbs, acc):
+        s = self._head("mac", limbs, False) + f" acc={acc} |" + self._refs(out, n)
+        for j in range(n):
+            for k in range(first[j], first[j + 1]):
+                s += f" [{g[k].src.c0_offset}:{g[k].src.c1_offset}"
+                s += "".join(f" {t[x].pt}@{t[x].galois}" for x in range(g[k].first_term, g[k].first_term + g[k].n_terms))
+                s += "]"
+            s += " ;"
+        self.log.append(s)
+        return 0
+
 
 class FakeCtx:
     def __init__(self, lanes):
@@ -151,13 +175,15 @@ def build_manager(rng, *, D, n_list, slots, L_top, lanes, compaction, eval_level
     m = object.__new__(InteractiveQueryManager)
     ctx = FakeCtx(ctx_lanes)
     m.ctx, m.sh, m.lanes, m.L, m.native = ctx, sh, lanes, L_top, False
-    m.p = SimpleNamespace(log_n=(2 * slots).bit_length() - 1)
+    m.p = SimpleNamespace(log_n=(2 * slots).bit_length() - 1, n=2 * slots)
     m.lib = FakeLib(ctx)
     m._nh, m._nh_key, m._nh_ver = None, None, 0
     nxt = iter(range(1000, 10 ** 9, 7))
     m.pt_centroid_cts = [next(nxt) for _ in range(sh.n_coarse)]
     m.pt_centroids = m.pt_centroid_cts[0]
     m.levels = sorted({min(lv, eval_level or lv) for lv in levels})
+    if compaction == "diagonal":
+        return build_diagonal(m, rng, nxt, levels, tuning)
     m._onehot, m._stride, m._prefix_lv = {}, {}, {}
     B = sh.B
     for lv in m.levels:
@@ -199,6 +225,50 @@ def build_manager(rng, *, D, n_list, slots, L_top, lanes, compaction, eval_level
     return m, recs
 
 
+def build_diagonal(m, rng, nxt, levels, tuning):
+    """The diagonal chain's state: units of up to `slots` candidates (at most
+    two per list), per level the centroid and unit diagonals (D plaintexts
+    `lv N` words apart) and norms, the inner-product pool, records with
+    their baby-step ciphertexts."""
+    sh = m.sh
+    n = 2 * sh.slots
+    m.units, m.list_units, m._ucnt, m._gal_cache = [], [], [], {}
+    vid = 0
+    for c in range(sh.n_list):
+        us = []
+        for _ in range(int(rng.integers(0, 3))):
+            cnt = int(rng.integers(1, sh.slots + 1))
+            us.append(len(m.units))
+            m.units.append((c, list(range(vid, vid + cnt))))
+            m._ucnt.append(cnt)
+            vid += cnt
+        m.list_units.append(us)
+    m._diag = {}
+    for lv in m.levels:
+        base = next(nxt) * 1000
+        cent = [base + i * lv * n for i in range(sh.D)]
+        pts = np.array([base + (1 + u) * sh.D * lv * n + i * lv * n for u in range(len(m.units))
+                        for i in range(sh.D)], dtype=np.uint64)
+        m._diag[lv] = dict(cent=cent, cnorm=next(nxt), pts=pts,
+                           norms=np.array([next(nxt) for _ in m.units], dtype=np.uint64))
+    m._inner = [(next(nxt), next(nxt)) for _ in range(InteractiveQueryManager.inner_pool(m.lanes, sh.n2))]
+    m._query_levels = set(levels)
+    m._bcnt, m.batches, m.cmp, m.work = [], [], [], []
+    m.n_res = 8
+    m._tuning = {lv: Choice(*t) for lv, t in tuning.items()}
+    m._opt_now = None
+    m._fused_ok = True
+    recs = []
+    for i in range(6):
+        res = [(next(nxt), next(nxt)) for _ in range(m.n_res)]
+        recs.append(QueryRecord((next(nxt), next(nxt)), (next(nxt), next(nxt)), (next(nxt), next(nxt)), res[0],
+                                results=res, level=int(rng.choice([0] + list(levels))),
+                                norm=(next(nxt), next(nxt)), baby=[(next(nxt), next(nxt)) for _ in range(sh.n1 - 1)]))
+    for r in recs:
+        r.probes = [int(c) for c in rng.choice(sh.n_list, size=int(rng.integers(1, 4)), replace=False)]
+    return m, recs
+
+
 def run_native(trace, m, recs, L_top, n, ctx_lanes, stage):
     """Register the manager's state through its own code (what the product
     runs) with the stubbed library, then run the stage natively."""
@@ -226,6 +296,13 @@ CASES = {
                               levels=[7, 6], tuning={4: (1, 4, 8, 12), 3: (0, 2), 2: (1, 4)}),
     "packed_mixed_levels": dict(D=4, n_list=30, slots=32, L_top=6, lanes=5, compaction="packed", eval_level=None,
                                 levels=[6, 5, 3], tuning={5: (1, 5), 4: (1, 1)}),
+    "diagonal_mixed_levels": dict(D=16, n_list=40, slots=64, L_top=5, lanes=9, compaction="diagonal",
+                                  eval_level=None, levels=[5, 3, 2], tuning={}),
+    "diagonal_eval_level": dict(D=64, n_list=50, slots=64, L_top=6, lanes=16, compaction="diagonal", eval_level=2,
+                                levels=[6, 4], tuning={2: (1, 8, 8, 12), 1: (0, 4)}),
+    # 32 baby steps: the generic sums of products
+    "diagonal_generic": dict(D=1024, n_list=20, slots=1024, L_top=4, lanes=32, compaction="diagonal",
+                             eval_level=3, levels=[4], tuning={}),
 }
 
 
