@@ -284,7 +284,7 @@ def profile_ntt(polys: int, log_n: int = 13, reps: int = 10):
     ctx.close()
 
 
-def profile_host(batch: int = 296, steps: int = 5):
+def profile_host(batch: int = 296, steps: int = 5, workload: str = "small"):
     """The end-to-end path on the host: (1) one batch through the protocol one
     phase at a time, each phase followed by a synchronisation, its wall time
     averaged over `steps` steps; (2) the streamed end-to-end run under
@@ -296,8 +296,8 @@ def profile_host(batch: int = 296, steps: int = 5):
     import torch
 
     from ._lib import P64, check
-    from .workloads import SMALL, Workload
-    wl = Workload(SMALL, max_queries=2 * batch, lanes=batch)
+    from .workloads import WORKLOADS, Workload
+    wl = Workload(WORKLOADS[workload], max_queries=2 * batch, lanes=batch, tune=workload != "small")
     iqm = wl.iqm
     recs = wl.records[:batch]
     wl.encrypt_queries(wl.queries(batch, seed=1000), recs)
@@ -430,7 +430,9 @@ def main() -> None:
     a.add_argument("outputs", type=int)
     a.add_argument("--units", type=int, default=16)
     a.add_argument("--generic", action="store_true", help="afhe_eval_mac_plain_batch instead of the structured kernel")
-    sub.add_parser("host", help="end-to-end phases and the streamed run's host hotspots")
+    a = sub.add_parser("host", help="end-to-end phases and the streamed run's host hotspots")
+    a.add_argument("--workload", default="small", choices=["small", "large", "large_diag"])
+    a.add_argument("--batch", type=int, default=296)
     a = sub.add_parser("dispatch", help="afhe_dispatch cost per call and op code")
     a.add_argument("--calls", type=int, default=200)
     args = ap.parse_args()
@@ -445,7 +447,7 @@ def main() -> None:
     elif args.what == "dispatch":
         profile_dispatch(args.calls)
     else:
-        profile_host()
+        profile_host(args.batch, workload=args.workload)
 
 
 if __name__ == "__main__":
