@@ -975,7 +975,6 @@ int afhe_eval_diag_inner_batch(afhe_ctx* ctx, const afhe_ct_ref* out, uint32_t c
     const unsigned __int128 room = ~(unsigned __int128)0 / (sq ? sq : 1);
     const uint32_t reduce_every = room > 0x7fffffff ? 0x7fffffffu : (uint32_t)room;
     if (reduce_every < nb + 1) return fail(ctx, AFHE_E_ARG, "primes too large for the accumulators; use afhe_eval_mac_plain_batch");
-    const bool split = qmax < (1ull << 50);          // 25-bit split products
     const size_t seg = ctx->ring.seg_words - 96;
     std::vector<DiagJob> J;
     std::vector<u64> S;
@@ -989,7 +988,7 @@ int afhe_eval_diag_inner_batch(afhe_ctx* ctx, const afhe_ct_ref* out, uint32_t c
         if ((r = ring_put(ctx, S.data(), S.size(), &ds))) return r;
         if ((r = ring_put(ctx, U.data(), U.size() * sizeof(DiagUnit) / sizeof(u64), &du))) return r;
         CK(launch_diag_inner(ctx->nat.pc, ctx->poly, ctx->n, limbs, (uint32_t)J.size(), nb, (const DiagJob*)dj, ds,
-                             (const DiagUnit*)du, pt_stride, reduce_every, accumulate ? 1 : 0, split, ctx->st));
+                             (const DiagUnit*)du, pt_stride, reduce_every, accumulate ? 1 : 0, ctx->st));
         J.clear();
         S.clear();
         U.clear();

@@ -188,7 +188,6 @@ struct MacTerm {
 // The diagonal method's inner products (afhe_eval_diag_inner_batch): job z
 // writes out = sum over its units k of sum over b < nb of
 // pt_k[b stride + map_k[i]] * src_{z, b}, srcs[z nb + b] = (c0, c1) offsets.
-// split: every prime of the limbs is below 2^50 (25-bit split products).
 struct DiagJob {
     u64 out0, out1;
     uint32_t u0, u1;
@@ -199,7 +198,7 @@ struct DiagUnit {
 };
 cudaError_t launch_diag_inner(const PrimeConst* pc, u64* arena, uint32_t n, uint32_t limbs, uint32_t jobs,
                               uint32_t nb, const DiagJob* job, const u64* srcs, const DiagUnit* unit, u64 stride,
-                              uint32_t reduce_every, int accumulate, bool split, cudaStream_t st);
+                              uint32_t reduce_every, int accumulate, cudaStream_t st);
 cudaError_t launch_mac_plain(const PrimeConst* pc, u64* arena, uint32_t n, uint32_t limbs, uint32_t jobs,
                              const MacJob* job, const MacGroup* group, const MacTerm* term, uint32_t reduce_every,
                              int accumulate, cudaStream_t st);

@@ -204,40 +204,7 @@ __global__ void __launch_bounds__(256) mac_plain_kernel(const PrimeConst* __rest
 // One coefficient per thread: the nb baby-step ciphertexts' coefficients stay
 // in registers while the job's units stream through; a unit's automorphism
 // index is loaded once for its nb plaintexts, which lie `stride` words apart.
-// Residues below 2^50 (every prime of the launch's limbs): each operand splits
-// into 25-bit halves, x = x1 2^25 + x0, and a product's three partial sums
-// x0 y0, x0 y1 + x1 y0 and x1 y1 accumulate in 64-bit registers (one
-// 32 x 32 + 64 multiply-add each; products of halves < 2^50, so 4,096 of
-// them fit before a fold). The sum is recombined in 128 bits once.
-constexpr uint32_t kSplitBits = 25;
-constexpr uint32_t kSplitFold = 4096;    // products between folds (s01 < 2^51 each)
-
-struct Split3 {
-    u64 s00, s01, s11;
-};
-__device__ __forceinline__ void split_mad(Split3& a, uint32_t v0, uint32_t v1, uint32_t x0, uint32_t x1) {
-    a.s00 += (u64)v0 * x0;
-    a.s01 += (u64)v0 * x1 + (u64)v1 * x0;
-    a.s11 += (u64)v1 * x1;
-}
-__device__ __forceinline__ u64 split_reduce(const Split3& a, const ModConst& m) {
-    // s00 + s01 2^25 + s11 2^50 in 128 bits
-    u64 lo = a.s00, hi = 0;
-    u64 t = a.s01 << kSplitBits;
-    lo += t;
-    hi += (lo < t ? 1 : 0) + (a.s01 >> (64 - kSplitBits));
-    t = a.s11 << (2 * kSplitBits);
-    lo += t;
-    hi += (lo < t ? 1 : 0) + (a.s11 >> (64 - 2 * kSplitBits));
-    return reduce128(hi, lo, m);
-}
-
-// One coefficient per thread: the nb baby-step ciphertexts' coefficients stay
-// in registers while the job's units stream through; a unit's automorphism
-// index is loaded once for its nb plaintexts, which lie `stride` words apart.
-// SPLIT: the 25-bit split products above (all primes < 2^50); otherwise
-// 128-bit accumulators folded every reduce_every products.
-template <int NB, bool SPLIT>
+template <int NB>
 __global__ void __launch_bounds__(256) diag_inner_kernel(const PrimeConst* __restrict__ pc, u64* __restrict__ arena,
                                                          uint32_t n, const DiagJob* __restrict__ jobs,
                                                          const u64* __restrict__ srcs,
@@ -250,71 +217,34 @@ __global__ void __launch_bounds__(256) diag_inner_kernel(const PrimeConst* __res
     const ModConst m = modconst_of(pc[l]);
     const u64 off = (u64)l * n;
     const u64* s = srcs + (u64)blockIdx.z * 2 * NB;
-    u64 r0, r1;
-    if (SPLIT) {
-        constexpr uint32_t mask = (1u << kSplitBits) - 1;
-        uint32_t a0[NB], a1[NB], b0[NB], b1[NB];
+    u64 x0[NB], x1[NB];
 #pragma unroll
-        for (int b = 0; b < NB; ++b) {
-            const u64 x = arena[s[2 * b] + off + i], y = arena[s[2 * b + 1] + off + i];
-            a0[b] = (uint32_t)x & mask;
-            a1[b] = (uint32_t)(x >> kSplitBits);
-            b0[b] = (uint32_t)y & mask;
-            b1[b] = (uint32_t)(y >> kSplitBits);
-        }
-        Split3 c0{0, 0, 0}, c1{0, 0, 0};
-        uint32_t cnt = 0;
-        for (uint32_t k = J.u0; k < J.u1; ++k) {
-            const DiagUnit U = units[k];
-            const uint32_t j = U.map ? __ldg(U.map + i) : i;
-            const u64* p = arena + U.pt + off + j;
-            if (cnt + NB > kSplitFold) {
-                c0 = Split3{split_reduce(c0, m), 0, 0};
-                c1 = Split3{split_reduce(c1, m), 0, 0};
-                cnt = 1;
-            }
-#pragma unroll
-            for (int b = 0; b < NB; ++b) {
-                const u64 v = p[(u64)b * stride];
-                const uint32_t v0 = (uint32_t)v & mask, v1 = (uint32_t)(v >> kSplitBits);
-                split_mad(c0, v0, v1, a0[b], a1[b]);
-                split_mad(c1, v0, v1, b0[b], b1[b]);
-            }
-            cnt += NB;
-        }
-        r0 = split_reduce(c0, m);
-        r1 = split_reduce(c1, m);
-    } else {
-        u64 x0[NB], x1[NB];
-#pragma unroll
-        for (int b = 0; b < NB; ++b) {
-            x0[b] = arena[s[2 * b] + off + i];
-            x1[b] = arena[s[2 * b + 1] + off + i];
-        }
-        Acc128 a0, a1;
-        acc_init(a0);
-        acc_init(a1);
-        uint32_t cnt = 0;
-        for (uint32_t k = J.u0; k < J.u1; ++k) {
-            const DiagUnit U = units[k];
-            const uint32_t j = U.map ? __ldg(U.map + i) : i;
-            const u64* p = arena + U.pt + off + j;
-            if (cnt + NB > reduce_every) {
-                acc_fold(a0, m);
-                acc_fold(a1, m);
-                cnt = 1;
-            }
-#pragma unroll
-            for (int b = 0; b < NB; ++b) {
-                const u64 v = p[(u64)b * stride];
-                acc_mad(a0, v, x0[b]);
-                acc_mad(a1, v, x1[b]);
-            }
-            cnt += NB;
-        }
-        r0 = acc_reduce(a0, m);
-        r1 = acc_reduce(a1, m);
+    for (int b = 0; b < NB; ++b) {
+        x0[b] = arena[s[2 * b] + off + i];
+        x1[b] = arena[s[2 * b + 1] + off + i];
     }
+    Acc128 a0, a1;
+    acc_init(a0);
+    acc_init(a1);
+    uint32_t cnt = 0;
+    for (uint32_t k = J.u0; k < J.u1; ++k) {
+        const DiagUnit U = units[k];
+        const uint32_t j = U.map ? __ldg(U.map + i) : i;
+        const u64* p = arena + U.pt + off + j;
+        if (cnt + NB > reduce_every) {
+            acc_fold(a0, m);
+            acc_fold(a1, m);
+            cnt = 1;
+        }
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            const u64 v = p[(u64)b * stride];
+            acc_mad(a0, v, x0[b]);
+            acc_mad(a1, v, x1[b]);
+        }
+        cnt += NB;
+    }
+    u64 r0 = acc_reduce(a0, m), r1 = acc_reduce(a1, m);
     if (accumulate) {
         r0 = add_mod(r0, arena[J.out0 + off + i], m.q);
         r1 = add_mod(r1, arena[J.out1 + off + i], m.q);
@@ -325,27 +255,17 @@ __global__ void __launch_bounds__(256) diag_inner_kernel(const PrimeConst* __res
 
 cudaError_t launch_diag_inner(const PrimeConst* pc, u64* arena, uint32_t n, uint32_t limbs, uint32_t jobs,
                               uint32_t nb, const DiagJob* job, const u64* srcs, const DiagUnit* unit, u64 stride,
-                              uint32_t reduce_every, int accumulate, bool split, cudaStream_t st) {
+                              uint32_t reduce_every, int accumulate, cudaStream_t st) {
     if (limbs == 0 || jobs == 0) return cudaSuccess;
     dim3 grid((n + 255) / 256, limbs, jobs);
-#define DIAG_CASE(NBV)                                                                                      \
-    case NBV:                                                                                               \
-        if (split)                                                                                          \
-            diag_inner_kernel<NBV, true><<<grid, 256, 0, st>>>(pc, arena, n, job, srcs, unit, stride,       \
-                                                               reduce_every, accumulate);                   \
-        else                                                                                                \
-            diag_inner_kernel<NBV, false><<<grid, 256, 0, st>>>(pc, arena, n, job, srcs, unit, stride,      \
-                                                                reduce_every, accumulate);                  \
-        break;
     switch (nb) {
-        DIAG_CASE(1)
-        DIAG_CASE(2)
-        DIAG_CASE(4)
-        DIAG_CASE(8)
-        DIAG_CASE(16)
+    case 1: diag_inner_kernel<1><<<grid, 256, 0, st>>>(pc, arena, n, job, srcs, unit, stride, reduce_every, accumulate); break;
+    case 2: diag_inner_kernel<2><<<grid, 256, 0, st>>>(pc, arena, n, job, srcs, unit, stride, reduce_every, accumulate); break;
+    case 4: diag_inner_kernel<4><<<grid, 256, 0, st>>>(pc, arena, n, job, srcs, unit, stride, reduce_every, accumulate); break;
+    case 8: diag_inner_kernel<8><<<grid, 256, 0, st>>>(pc, arena, n, job, srcs, unit, stride, reduce_every, accumulate); break;
+    case 16: diag_inner_kernel<16><<<grid, 256, 0, st>>>(pc, arena, n, job, srcs, unit, stride, reduce_every, accumulate); break;
     default: return cudaErrorInvalidValue;
     }
-#undef DIAG_CASE
     count_launches(1);
     return cudaGetLastError();
 }
