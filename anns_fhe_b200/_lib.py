@@ -192,6 +192,7 @@ SIGNATURES = {
     "afhe_pq_destroy": (C.c_int, [C.c_void_p]),
     "afhe_pq_encode_batches": (C.c_int, [C.c_void_p, P32, P32, P32, u32, C.c_double, u32, P64]),
     "afhe_pq_encode_norms": (C.c_int, [C.c_void_p, P32, P32, P32, u32, C.c_double, u32, P64]),
+    "afhe_decode_batch": (C.c_int, [CTX, P64, C.POINTER(C.c_double), u32, u32, C.POINTER(C.c_double)]),
     "afhe_pq_encode_diagonals": (C.c_int, [C.c_void_p, P32, P32, P32, u32, u32, C.c_double, C.c_double, u32, P64]),
     "afhe_pq_encode_unit_norms": (C.c_int, [C.c_void_p, P32, P32, P32, u32, C.c_double, u32, P64]),
     "afhe_ivfpq_create": (C.c_int, [CTX, C.POINTER(IvfpqShape), C.POINTER(C.c_void_p)]),

@@ -327,6 +327,13 @@ class CkksClient:
                                    self.ctx.staging.get("dec_coef", count * level * n)).reshape(count, level * n)
         return centred_coefficients(limbs, self.p.q, level)
 
+    def decrypt_decode(self, cts, scales, slots: int) -> np.ndarray:
+        """Decrypt ciphertexts resident in poly_gmem from limb 0 and decode
+        them on the device (afhe_decrypt_batch, afhe_decode_batch): (count,
+        slots) real slot values, row i at scales[i]."""
+        return _decrypt_decode(self.ctx, cts, self.s_slot, self._region("dec_out", len(cts) * self.p.n), scales,
+                               slots)
+
     def decryptor(self, max_count: int, max_level: int = 1) -> "CkksDecryptor":
         """This client's decryption on a device context of its own (see
         CkksDecryptor); closed with close_decryptors()."""
@@ -405,8 +412,36 @@ class CkksDecryptor:
         limbs = self.ctx.read_poly(self.out_off, count * w, self.ctx.staging.get("dec_coef", count * w))
         return centred_coefficients(limbs.reshape(count, w), self.p.q, level)
 
+    def decrypt_decode_host(self, cts: np.ndarray, scales, slots: int) -> np.ndarray:
+        """Ciphertexts received as a host array (count, 2, N) (limb 0) ->
+        (count, slots) real slot values, row i at scales[i]: decryption and
+        decoding on the device (afhe_decode_batch)."""
+        n, count = self.p.n, cts.shape[0]
+        if count > self.max_count:
+            raise ValueError(f"{count} ciphertexts: the decryptor holds {self.max_count}")
+        self.ctx.write_poly(self.in_off, np.ascontiguousarray(cts).reshape(-1))
+        refs = [(self.in_off + 2 * i * n, self.in_off + (2 * i + 1) * n) for i in range(count)]
+        return _decrypt_decode(self.ctx, refs, self.s_off, self.out_off, scales, slots)
+
     def close(self) -> None:
         self.ctx.close()
+
+
+def _decrypt_decode(ctx: FheContext, cts, s_off: int, out: int, scales, slots: int) -> np.ndarray:
+    """m = c0 + c1 s of each ciphertext (limb 0) into out + i N, then its
+    slots decoded on the device into page-locked staging."""
+    from . import _lib as L
+    n, count = ctx.params.n, len(cts)
+    arr = (L.CtRef * max(count, 1))()
+    for i, (a, b) in enumerate(cts):
+        arr[i].c0_offset, arr[i].c1_offset = a, b
+    L.check(ctx.lib.afhe_decrypt_batch(ctx.h, arr, count, s_off, out, 1), "decrypt_batch")
+    coef = np.arange(count, dtype=np.uint64) * np.uint64(n) + np.uint64(out)
+    sc = np.ascontiguousarray(np.broadcast_to(np.asarray(scales, dtype=np.float64), (count,)))
+    res = ctx.staging.get("decoded", count * slots).view(np.float64).reshape(count, slots)
+    L.check(ctx.lib.afhe_decode_batch(ctx.h, coef.ctypes.data_as(L.P64), sc.ctypes.data_as(C.POINTER(C.c_double)),
+                                      count, slots, res.ctypes.data_as(C.POINTER(C.c_double))), "decode_batch")
+    return res
 
 
 def encode_plaintexts(ctx: FheContext, enc: Encoder, values: np.ndarray, scale: float, offs, level: int) -> None:

@@ -307,6 +307,81 @@ int finish_chunk(afhe_ctx* ctx, const FftTables& tb, double2* v, uint32_t count,
 }
 
 // Shared driver: `load(v, c0, m)` fills v with plaintexts [c0, c0 + m).
+// ---- decoding (the client's side): the forward special FFT ----------------
+// Slot j of m = sum c_k X^k is m(zeta^(5^j)). With v_i = (c_i + i c_{i+N/2}) /
+// scale, the encoder's transform inverted: bit reversal, then the stages of
+// block length 2 .. N/2, each (a, b) -> (a + w b, a - w b) with w =
+// ksi^((5^j mod 4 len) 2N / (4 len)); slot j is then v_j.
+__device__ __forceinline__ void special_bfly_fwd(double2& a, double2& b, uint32_t j, uint32_t len, uint32_t m,
+                                                 const double2* __restrict__ ksi, const uint32_t* __restrict__ rot) {
+    const uint32_t lenq = len << 2;
+    const uint32_t idx = (__ldg(rot + j) & (lenq - 1)) * (m / lenq);
+    const double2 t = cmul(b, __ldg(ksi + idx));
+    b = make_double2(a.x - t.x, a.y - t.y);
+    a = make_double2(a.x + t.x, a.y + t.y);
+}
+
+// limb 0 of each decrypted polynomial (coefficient form), centred mod q_0,
+// / scale, paired (c_i, c_{i+N/2}) at the bit-reversed position of i
+__global__ void dec_load(double2* __restrict__ v, const u64* __restrict__ arena, const u64* __restrict__ coef,
+                         const double* __restrict__ scales, u64 q0, uint32_t log_s, uint32_t count) {
+    const uint32_t s = 1u << log_s;
+    const u64 total = (u64)count * s;
+    for (u64 t = blockIdx.x * (u64)blockDim.x + threadIdx.x; t < total; t += (u64)gridDim.x * blockDim.x) {
+        const uint32_t z = (uint32_t)(t >> log_s), i = (uint32_t)(t & (s - 1));
+        const u64* c = arena + coef[z];
+        const u64 a = c[i], b = c[i + s];
+        const double inv = 1.0 / scales[z];
+        const double re = (double)(a > q0 / 2 ? -(long long)(q0 - a) : (long long)a) * inv;
+        const double im = (double)(b > q0 / 2 ? -(long long)(q0 - b) : (long long)b) * inv;
+        v[(u64)z * s + (__brev(i) >> (32 - log_s))] = make_double2(re, im);
+    }
+}
+
+// the stages of block length 2 .. tile in shared memory, one tile per CTA
+__global__ void __launch_bounds__(kTileThreads) dec_tile_stages(double2* __restrict__ v, uint32_t s, uint32_t tile,
+                                                                const double2* __restrict__ ksi,
+                                                                const uint32_t* __restrict__ rot) {
+    extern __shared__ double2 sm2[];
+    const uint32_t m = 4 * s;
+    double2* g = v + (u64)blockIdx.y * s + (u64)blockIdx.x * tile;
+    for (uint32_t e = threadIdx.x; e < tile; e += blockDim.x) sm2[e] = g[e];
+    __syncthreads();
+    for (uint32_t len = 2; len <= tile; len <<= 1) {
+        const uint32_t lenh = len >> 1;
+        for (uint32_t b = threadIdx.x; b < tile / 2; b += blockDim.x) {
+            const uint32_t blk = b / lenh, j = b % lenh;
+            special_bfly_fwd(sm2[blk * len + j], sm2[blk * len + j + lenh], j, len, m, ksi, rot);
+        }
+        __syncthreads();
+    }
+    for (uint32_t e = threadIdx.x; e < tile; e += blockDim.x) g[e] = sm2[e];
+}
+
+// one stage of block length above a tile, in global memory
+__global__ void dec_global_stage(double2* __restrict__ v, uint32_t s, uint32_t len, uint32_t count,
+                                 const double2* __restrict__ ksi, const uint32_t* __restrict__ rot) {
+    const uint32_t half = s / 2, lenh = len >> 1, m = 4 * s;
+    const u64 total = (u64)count * half;
+    for (u64 t = blockIdx.x * (u64)blockDim.x + threadIdx.x; t < total; t += (u64)gridDim.x * blockDim.x) {
+        const uint32_t z = (uint32_t)(t / half), b = (uint32_t)(t % half);
+        const uint32_t blk = b / lenh, j = b % lenh;
+        double2* p = v + (u64)z * s + (u64)blk * len + j;
+        double2 a = p[0], c = p[lenh];
+        special_bfly_fwd(a, c, j, len, m, ksi, rot);
+        p[0] = a;
+        p[lenh] = c;
+    }
+}
+
+// the real parts of slots 0 .. slots - 1
+__global__ void dec_store(const double2* __restrict__ v, double* __restrict__ out, uint32_t s, uint32_t slots,
+                          uint32_t count) {
+    const u64 total = (u64)count * slots;
+    for (u64 t = blockIdx.x * (u64)blockDim.x + threadIdx.x; t < total; t += (u64)gridDim.x * blockDim.x)
+        out[t] = v[(t / slots) * s + t % slots].x;
+}
+
 template <class Load>
 int encode_pipeline(afhe_ctx* ctx, uint32_t count, double scale, uint32_t level, const uint64_t* pt, Load load) {
     if (!(scale > 0.0) || !std::isfinite(scale)) return fail(ctx, AFHE_E_ARG, "scale must be positive and finite");
@@ -356,6 +431,62 @@ int encode_pipeline(afhe_ctx* ctx, uint32_t count, double scale, uint32_t level,
 }  // namespace afhe
 
 extern "C" {
+
+int afhe_decode_batch(afhe_ctx* ctx, const uint64_t* coef, const double* scales, uint32_t count, uint32_t slots,
+                      double* out) {
+    if (!ctx || (count && (!coef || !scales || !out))) return fail(ctx, AFHE_E_ARG, "null argument");
+    const uint32_t s = ctx->n / 2;
+    if (slots < 1 || slots > s) return fail(ctx, AFHE_E_ARG, "slots must be in [1, N/2]");
+    if (ctx->prm.q[0] >= (1ull << 53)) return fail(ctx, AFHE_E_ARG, "q_0 must be below 2^53 (exact doubles)");
+    for (uint32_t i = 0; i < count; ++i) {
+        if (!range_ok(coef[i], ctx->n, ctx->prm.poly_words)) return fail(ctx, AFHE_E_RANGE, "polynomial out of range");
+        if (!(scales[i] > 0.0) || !std::isfinite(scales[i])) return fail(ctx, AFHE_E_ARG, "scales must be positive");
+    }
+    if (count == 0) return AFHE_OK;
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return fail(ctx, AFHE_E_CUDA, "cudaSetDevice");
+    FftTables tb;
+    CK(fft_tables(ctx->device, ctx->n, ctx->st, &tb));
+    uint32_t log_s = 0;
+    while ((1u << log_s) < s) ++log_s;
+    const uint32_t chunk = count < kChunkPts ? count : kChunkPts, tile = s < kTile ? s : kTile;
+    double2* v = nullptr;
+    double *sc = nullptr, *res = nullptr;
+    u64* cf = nullptr;
+    int rc = AFHE_OK;
+    cudaError_t e = cudaMalloc(&v, (size_t)chunk * s * sizeof(double2));
+    if (e == cudaSuccess) e = cudaMalloc(&sc, (size_t)count * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&cf, (size_t)count * sizeof(u64));
+    if (e == cudaSuccess) e = cudaMalloc(&res, (size_t)chunk * slots * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(sc, scales, (size_t)count * sizeof(double), cudaMemcpyHostToDevice, ctx->st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(cf, coef, (size_t)count * sizeof(u64), cudaMemcpyHostToDevice, ctx->st);
+    if (e != cudaSuccess) rc = cuda_fail(ctx, e, "decode buffers");
+    const size_t smem = tile * sizeof(double2);
+    if (rc == AFHE_OK) {
+        e = cudaFuncSetAttribute(dec_tile_stages, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) rc = cuda_fail(ctx, e, "decode smem");
+    }
+    for (uint32_t c0 = 0; rc == AFHE_OK && c0 < count; c0 += chunk) {
+        const uint32_t m = count - c0 < chunk ? count - c0 : chunk;
+        dec_load<<<grid_for((u64)m * s), 256, 0, ctx->st>>>(v, ctx->poly, cf + c0, sc + c0, ctx->prm.q[0], log_s, m);
+        dec_tile_stages<<<dim3(s / tile, m), kTileThreads, smem, ctx->st>>>(v, s, tile, tb.ksi, tb.rot);
+        for (uint32_t len = 2 * tile; len <= s; len <<= 1)
+            dec_global_stage<<<grid_for((u64)m * s / 2), 256, 0, ctx->st>>>(v, s, len, m, tb.ksi, tb.rot);
+        dec_store<<<grid_for((u64)m * slots), 256, 0, ctx->st>>>(v, res, s, slots, m);
+        count_launches(3 + (s > tile ? log_s - (31 - __builtin_clz(tile)) : 0));
+        e = cudaGetLastError();
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(out + (size_t)c0 * slots, res, (size_t)m * slots * sizeof(double),
+                                cudaMemcpyDeviceToHost, ctx->st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->st);    // res is reused by the next chunk
+        if (e != cudaSuccess) rc = cuda_fail(ctx, e, "decode");
+    }
+    cudaStreamSynchronize(ctx->st);
+    cudaFree(v);
+    cudaFree(sc);
+    cudaFree(cf);
+    cudaFree(res);
+    return rc;
+}
 
 int afhe_encode_batch(afhe_ctx* ctx, const double* values, uint32_t count, uint32_t slots, double scale,
                       uint32_t level, const uint64_t* pt) {

@@ -1144,11 +1144,16 @@ class InteractiveQueryManager:
     def _stage3_diagonal_layout(self, queries: list[QueryRecord]) -> None:
         """Each query's units, their offsets, candidate ids and slot positions."""
         S = self.sh.slots
+        if getattr(self, "_unit_arrays", None) is None:
+            self._unit_arrays = [np.asarray(v, dtype=np.int64) for _, v in self.units]
+        ua, ar = self._unit_arrays, np.arange(S, dtype=np.int64)
         for q in queries:
             q.layout = self.unit_offsets(q.probes)
-            q.vids = [v for u, _ in q.layout for v in self.units[u][1]]
-            q.pos = (np.concatenate([np.arange(off, off + len(self.units[u][1])) for u, off in q.layout])
-                     if q.layout else np.zeros(0, dtype=np.int64))
+            if q.layout:
+                q.vids = np.concatenate([ua[u] for u, _ in q.layout]).tolist()
+                q.pos = np.concatenate([ar[:len(ua[u])] + off for u, off in q.layout])
+            else:
+                q.vids, q.pos = [], np.zeros(0, dtype=np.int64)
             if q.layout and q.layout[-1][1] // S >= self.n_res:
                 raise ValueError("more candidates than the result ciphertexts hold")
 

@@ -218,35 +218,36 @@ class WorkloadBackend:
 
     def receive(self, h: dict) -> dict:
         """A request's results to the client: wait for its copy, then the
-        device part of the client's decryption ("coef", one row of N
-        coefficients per ciphertext), on the client's own context, so it does
-        not wait for the server's work enqueued since the request."""
+        client's decryption and decoding ("vals", the slots each query
+        needs: its coarse distances, or up to its last candidate), on the
+        client's own context, so they do not wait for the server's work
+        enqueued since the request."""
         self.wl.ctx.fence_wait(h["fence"])
-        box = h["box"][:, :h.get("need", 1)]
-        coef = self._decryptor(box.shape[0] * box.shape[1]).decrypt_host_batch_coef(box.reshape(-1, 2, self.n), 1)
-        got = dict(h, box=box, coef=coef.reshape(h["count"], -1))
-        return got
+        need = h.get("need", 1)
+        box = h["box"][:, :need]
+        if h["kind"] == "compact":
+            slots = self.iqm.coarse_slots_needed()
+        else:
+            last = max((int(p[-1]) + 1 if len(p) else 1) for p in h["pos"])
+            slots = min(self.iqm.sh.slots, last) if need == 1 else self.iqm.sh.slots
+        vals = self._decryptor(box.shape[0] * box.shape[1]).decrypt_decode_host(
+            box.reshape(-1, 2, self.n), np.repeat(h["scale"], need), slots)
+        return dict(h, box=box, vals=vals.reshape(h["count"], -1).copy())
 
     def select(self, recs, got: dict) -> None:
-        """Stage 2 on the host: decode the coarse distances, keep the nprobe nearest lists."""
+        """Stage 2 on the host: keep the nprobe nearest lists."""
         wl = self.wl
-        vals = wl.client.enc.decode_real_batch(got["coef"], got["scale"], self.iqm.coarse_slots_needed())
+        vals = got["vals"]
         from .workloads import nearest_lists
         for r, pr in zip(recs, nearest_lists(self.iqm.coarse_from_slots(vals),
                                              [r.nprobe or wl.spec.nprobe for r in recs])):
             r.probes = pr
 
     def topk(self, recs, got: dict) -> list[list[int]]:
-        """Stage 4 on the host: decode the candidate distances, rank them."""
+        """Stage 4 on the host: rank the candidate distances."""
         wl = self.wl
         vids = got["vids"]
-        count = len(vids)
-        coef = got["coef"].reshape(-1, self.n)               # one row per result ciphertext
-        per = coef.shape[0] // count
-        # one result each: decode only up to the last candidate slot
-        slots = (min(self.iqm.sh.slots, max((int(p[-1]) + 1 if len(p) else 1) for p in got["pos"]))
-                 if per == 1 else None)
-        d = wl.client.enc.decode_real_batch(coef, np.repeat(got["scale"], per), slots).reshape(count, -1)
+        d = got["vals"]
         from .workloads import ranked_prefix
         return [[v[i] for i in top] for v, top in zip(vids, ranked_prefix(d, got["pos"], wl.spec.top_k))]
 

@@ -226,8 +226,8 @@ class Workload:
         """Decrypt result ciphertexts resident on the device from limb 0 (the
         messages are far below q_0 / 2; the query manager checks the bound);
         row i is decoded at scales[i]."""
-        coef = self.client.decrypt_batch_coef(cts, 1)
-        return self.client.enc.decode_real_batch(coef, np.asarray(scales, dtype=np.float64), slots)
+        return self.client.decrypt_decode(cts, np.asarray(scales, dtype=np.float64),
+                                          slots or self.iqm.sh.slots).copy()
 
     def coarse(self, recs) -> np.ndarray:
         """(count, n_list) decrypted coarse distances."""
@@ -299,8 +299,7 @@ class Workload:
         iqm = self.iqm
         self.ctx.fence_wait(fence)
         scales = np.array([iqm.out_scale_at(iqm.level_of(r)) for r in part])
-        vals = dec.enc.decode_real_batch(dec.decrypt_host_batch_coef(box[:, 0], 1), scales,
-                                         iqm.coarse_slots_needed())
+        vals = dec.decrypt_decode_host(box[:, 0], scales, iqm.coarse_slots_needed())
         for r, pr in zip(part, nearest_lists(iqm.coarse_from_slots(vals),
                                              [r.nprobe or self.spec.nprobe for r in part])):
             r.probes = pr
@@ -319,8 +318,8 @@ class Workload:
         last = max((int(p[-1]) + 1 if len(p) else 1) for p in pos)
         need = -(-last // S)                      # result ciphertexts that hold candidates
         scales = np.repeat([iqm.out_scale_at(iqm.level_of(r)) for r in part], need)
-        coef = dec.decrypt_host_batch_coef(box[:, :need].reshape(-1, 2, n), 1)
-        vals = dec.enc.decode_real_batch(coef, scales, min(S, last) if need == 1 else None).reshape(len(part), -1)
+        vals = dec.decrypt_decode_host(box[:, :need].reshape(-1, 2, n), scales,
+                                       min(S, last) if need == 1 else S).reshape(len(part), -1)
         return [[r.vids[i] for i in top] for r, top in zip(part, ranked_prefix(vals, pos, self.spec.top_k))], box.nbytes
 
     def run_host_pipelined(self, recs: list[QueryRecord], host_cts, dec, groups: int = 2):

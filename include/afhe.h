@@ -474,6 +474,16 @@ typedef struct afhe_pq_index {
     const uint32_t* assignments;  /* n: the list of each vector */
 } afhe_pq_index;
 typedef struct afhe_pq afhe_pq;
+/* The client's decoding on the device, the inverse of afhe_encode_batch's
+ * transform: polynomial i (coefficient form, e.g. afhe_decrypt_batch's
+ * output, limb 0 at poly_gmem offset coef[i], centred mod q_0 < 2^53) to the
+ * real parts of slots 0 .. slots - 1, m(zeta^(5^j)) / scales[i], into host
+ * `out` (count x slots doubles, row-major; page-locked memory copies
+ * fastest). Double-precision special FFT; the reference's client decodes
+ * with OpenFHE (Decrypt + GetRealPackedValue,
+ * fhe_core/fhe_context_manager.cpp:505-507). */
+int afhe_decode_batch(afhe_ctx* ctx, const uint64_t* coef, const double* scales, uint32_t count, uint32_t slots,
+                      double* out);
 int afhe_pq_create(afhe_ctx* ctx, const afhe_pq_index* index, afhe_pq** out);
 int afhe_pq_destroy(afhe_pq* pq);
 /* Batch b: candidates vids[first[b] .. first[b] + count[b]) (count <= N / 2d);

@@ -92,3 +92,47 @@ def test_pq_batches_equal_encode_of_reconstructions():
             assert np.array_equal(ctx.read_poly(a[i], prm.L * n), ctx.read_poly(b[i], prm.L * n)), f"batch {i}"
     finally:
         ctx.close()
+
+
+@pytest.mark.parametrize("log_n", [10, 13, 15])
+def test_decode_batch_matches_host(log_n):
+    """afhe_decode_batch (the client's decoding on the device) against the
+    host decoder (Encoder.decode_real_batch) on random centred coefficients
+    of up to 2^45 in limb 0: equal to 1e-9 relative to the largest slot, for
+    every slot and for a prefix of slots; and the round trip through
+    afhe_encode_batch returns the encoded values."""
+    from anns_fhe_b200.driver import find_ntt_primes
+    q = find_ntt_primes(log_n, 50, 2, [])
+    p = find_ntt_primes(log_n, 60, 1, q)
+    prm = CkksParams(log_n, q, p, 1)
+    n = prm.n
+    ctx = FheContext(prm, poly_words=128 * n, key_words=1024)
+    try:
+        rng = np.random.default_rng(log_n)
+        enc = Encoder(log_n)
+        c = rng.integers(-(1 << 45), 1 << 45, size=(6, n), dtype=np.int64)
+        offs = np.arange(6, dtype=np.uint64) * np.uint64(2 * n)
+        for i in range(6):
+            ctx.write_poly(int(offs[i]), np.mod(c[i], q[0]).astype(np.uint64))
+        scales = np.array([2.0 ** 30, 2.0 ** 40, 1.0, 3.5, 2.0 ** 20, 7.0])
+        for slots in (n // 2, 37):
+            out = np.zeros((6, slots))
+            L.check(ctx.lib.afhe_decode_batch(ctx.h, offs.ctypes.data_as(L.P64),
+                                              scales.ctypes.data_as(L.C.POINTER(L.C.c_double)), 6, slots,
+                                              out.ctypes.data_as(L.C.POINTER(L.C.c_double))), "decode_batch")
+            want = enc.decode_real_batch(c.astype(np.float64), scales, slots)
+            assert np.max(np.abs(out - want) / np.max(np.abs(want), axis=1, keepdims=True)) < 1e-9
+        # encode then decode (coefficient form via the INTT) returns the values
+        vals = rng.normal(size=(3, n // 2)) * 100
+        pts = [int(12 * 2 * n + 2 * i * n) for i in range(3)]
+        encode_plaintexts(ctx, enc, vals, 2.0 ** 40, pts, 1)
+        for i, off in enumerate(pts):
+            ctx.write_poly(off, coefficients(ctx, off, 1)[0])
+        out = np.zeros((3, n // 2))
+        po = np.array(pts, dtype=np.uint64)
+        sc = np.full(3, 2.0 ** 40)
+        L.check(ctx.lib.afhe_decode_batch(ctx.h, po.ctypes.data_as(L.P64), sc.ctypes.data_as(L.C.POINTER(L.C.c_double)),
+                                          3, n // 2, out.ctypes.data_as(L.C.POINTER(L.C.c_double))), "decode_batch")
+        assert np.max(np.abs(out - vals)) < 1e-6
+    finally:
+        ctx.close()
