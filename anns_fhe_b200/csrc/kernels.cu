@@ -227,10 +227,20 @@ __global__ void __launch_bounds__(256) diag_inner_kernel(const PrimeConst* __res
     acc_init(a0);
     acc_init(a1);
     uint32_t cnt = 0;
+    // the next unit's descriptor and automorphism index are loaded while the
+    // current unit's plaintexts are read and multiplied
+    DiagUnit Un{};
+    uint32_t jn = i;
+    if (J.u0 < J.u1) {
+        Un = units[J.u0];
+        jn = Un.map ? __ldg(Un.map + i) : i;
+    }
     for (uint32_t k = J.u0; k < J.u1; ++k) {
-        const DiagUnit U = units[k];
-        const uint32_t j = U.map ? __ldg(U.map + i) : i;
-        const u64* p = arena + U.pt + off + j;
+        const u64* p = arena + Un.pt + off + jn;
+        if (k + 1 < J.u1) {
+            Un = units[k + 1];
+            jn = Un.map ? __ldg(Un.map + i) : i;
+        }
         if (cnt + NB > reduce_every) {
             acc_fold(a0, m);
             acc_fold(a1, m);
