@@ -460,6 +460,7 @@ int afhe_ctx_destroy(afhe_ctx* ctx) {
     fr(ctx->ld_crt); fr(ctx->ld_crt_sh); fr(ctx->ld_mod);
     for (auto& kv : ctx->rot) fr(kv.second.map);
     for (auto& kv : ctx->auto_maps) fr(kv.second);
+    fr(ctx->dec_ws);
     free_key_preps(ctx);
     fr(ctx->ring.dev);
     if (ctx->ring.host) cudaFreeHost(ctx->ring.host);

@@ -448,16 +448,30 @@ int afhe_decode_batch(afhe_ctx* ctx, const uint64_t* coef, const double* scales,
     CK(fft_tables(ctx->device, ctx->n, ctx->st, &tb));
     uint32_t log_s = 0;
     while ((1u << log_s) < s) ++log_s;
-    const uint32_t chunk = count < kChunkPts ? count : kChunkPts, tile = s < kTile ? s : kTile;
-    double2* v = nullptr;
-    double *sc = nullptr, *res = nullptr;
-    u64* cf = nullptr;
+    const uint32_t chunk = kChunkPts, tile = s < kTile ? s : kTile;
+    // one workspace per context, grown on demand: v (chunk x s), res (chunk
+    // x slots), the scales and offsets of the call
+    const size_t need = (size_t)chunk * s * sizeof(double2) + (size_t)chunk * s * sizeof(double) +
+                        (size_t)count * (sizeof(double) + sizeof(u64));
     int rc = AFHE_OK;
-    cudaError_t e = cudaMalloc(&v, (size_t)chunk * s * sizeof(double2));
-    if (e == cudaSuccess) e = cudaMalloc(&sc, (size_t)count * sizeof(double));
-    if (e == cudaSuccess) e = cudaMalloc(&cf, (size_t)count * sizeof(u64));
-    if (e == cudaSuccess) e = cudaMalloc(&res, (size_t)chunk * slots * sizeof(double));
-    if (e == cudaSuccess) e = cudaMemcpyAsync(sc, scales, (size_t)count * sizeof(double), cudaMemcpyHostToDevice, ctx->st);
+    cudaError_t e = cudaSuccess;
+    if (ctx->dec_ws_bytes < need) {
+        if (ctx->dec_ws) {
+            cudaStreamSynchronize(ctx->st);
+            cudaFree(ctx->dec_ws);
+            ctx->dec_ws = nullptr;
+            ctx->dec_ws_bytes = 0;
+        }
+        const size_t grow = std::max(need, 2 * ctx->dec_ws_bytes);
+        e = cudaMalloc(&ctx->dec_ws, grow);
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "decode workspace");
+        ctx->dec_ws_bytes = grow;
+    }
+    double2* v = (double2*)ctx->dec_ws;
+    double* res = (double*)(v + (size_t)chunk * s);
+    double* sc = res + (size_t)chunk * s;
+    u64* cf = (u64*)(sc + count);
+    e = cudaMemcpyAsync(sc, scales, (size_t)count * sizeof(double), cudaMemcpyHostToDevice, ctx->st);
     if (e == cudaSuccess) e = cudaMemcpyAsync(cf, coef, (size_t)count * sizeof(u64), cudaMemcpyHostToDevice, ctx->st);
     if (e != cudaSuccess) rc = cuda_fail(ctx, e, "decode buffers");
     const size_t smem = tile * sizeof(double2);
@@ -480,11 +494,7 @@ int afhe_decode_batch(afhe_ctx* ctx, const uint64_t* coef, const double* scales,
         if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->st);    // res is reused by the next chunk
         if (e != cudaSuccess) rc = cuda_fail(ctx, e, "decode");
     }
-    cudaStreamSynchronize(ctx->st);
-    cudaFree(v);
-    cudaFree(sc);
-    cudaFree(cf);
-    cudaFree(res);
+    if (rc != AFHE_OK) cudaStreamSynchronize(ctx->st);
     return rc;
 }
 

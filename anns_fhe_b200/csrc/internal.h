@@ -131,6 +131,10 @@ struct afhe_ctx {
     std::map<int32_t, afhe::RotKey> rot;
     // device automorphism maps by Galois element (afhe_automorphism_batch)
     std::map<uint32_t, uint32_t*> auto_maps;
+    // afhe_decode_batch's working memory, grown on demand and kept (a
+    // cudaFree per call would wait for every stream of the device)
+    void* dec_ws = nullptr;
+    size_t dec_ws_bytes = 0;
 
     // device address of the static working array of afhe_key_switch_noalloc
     // on this context's device, looked up when the context is created (null

@@ -814,27 +814,55 @@ class InteractiveQueryManager:
             self._nh, self._nh_key = None, None
 
     @staticmethod
-    def _native_queries(queries, probes: bool):
-        """An afhe_ivfpq_query array for the records; the arrays it points to
-        are kept alive by the returned list."""
-        arr = (L.IvfpqQuery * max(1, len(queries)))()
-        keep = [arr]
-        for q, r in zip(arr, queries):
-            q.ct_query, q.ct_dim, q.compact = L.CtRef(*r.ct_query), L.CtRef(*r.ct_dim), L.CtRef(*r.compact)
-            if r.norm is not None:
-                q.norm = L.CtRef(*r.norm)
-            res = (L.CtRef * len(r.results))(*[L.CtRef(*c) for c in r.results])
-            q.results, q.n_results, q.level = res, len(r.results), r.level
-            keep.append(res)
-            if probes:
-                pr = (C.c_uint32 * max(1, len(r.probes)))(*[int(c) for c in r.probes])
-                q.probes, q.nprobe = pr, len(r.probes)
-                keep.append(pr)
-            if r.baby:
-                bb = (L.CtRef * len(r.baby))(*[L.CtRef(*c) for c in r.baby])
-                q.baby, q.n_baby = bb, len(r.baby)
-                keep.append(bb)
-        return arr, keep
+    def _query_dtype() -> np.dtype:
+        """afhe_ivfpq_query as a numpy record (offsets from the ctypes struct)."""
+        f = L.IvfpqQuery
+        names = [n for n, _ in f._fields_]
+        kinds = {"ct_query": ("<u8", (2,)), "ct_dim": ("<u8", (2,)), "compact": ("<u8", (2,)),
+                 "norm": ("<u8", (2,)), "results": ("<u8", ()), "probes": ("<u8", ()), "baby": ("<u8", ())}
+        return np.dtype({"names": names,
+                         "formats": [kinds[n] if n in kinds else "<u4" for n in names],
+                         "offsets": [getattr(f, n).offset for n in names], "itemsize": C.sizeof(f)})
+
+    @classmethod
+    def _native_queries(cls, queries, probes: bool):
+        """An afhe_ivfpq_query array for the records, built with numpy (the
+        arrays it points to are kept alive by the returned list)."""
+        m = len(queries)
+        dt = getattr(cls, "_qdt", None)
+        if dt is None:
+            dt = cls._qdt = cls._query_dtype()
+        a = np.zeros(max(1, m), dtype=dt)
+        if m:
+            a["ct_query"] = [r.ct_query for r in queries]
+            a["ct_dim"] = [r.ct_dim for r in queries]
+            a["compact"] = [r.compact for r in queries]
+            a["norm"] = [r.norm if r.norm is not None else (0, 0) for r in queries]
+            a["level"] = [r.level for r in queries]
+        keep = [a]
+
+        def pointers(field, count_field, rows, width):
+            """rows: per query a list of (c0, c1) pairs or ints, all `width`
+            long except where shorter; one contiguous array, one pointer each."""
+            if not width:
+                return
+            flat = np.zeros((m, width) + ((2,) if field != "probes" else ()), dtype=np.uint64 if field != "probes"
+                            else np.uint32)
+            n = np.zeros(m, dtype=np.uint32)
+            for i, row in enumerate(rows):
+                if len(row):
+                    flat[i, :len(row)] = row
+                n[i] = len(row)
+            keep.append(flat)
+            a[field] = flat.ctypes.data + np.arange(m, dtype=np.uint64) * np.uint64(flat.strides[0])
+            a[count_field] = n
+        pointers("results", "n_results", [r.results for r in queries], max((len(r.results) for r in queries),
+                                                                            default=0))
+        if probes:
+            pointers("probes", "nprobe", [[int(c) for c in r.probes] for r in queries],
+                     max((len(r.probes) for r in queries), default=0))
+        pointers("baby", "n_baby", [r.baby for r in queries], max((len(r.baby) for r in queries), default=0))
+        return a.ctypes.data_as(C.POINTER(L.IvfpqQuery)), keep
 
     # ---- batched C-ABI helpers ----
     @staticmethod
@@ -1150,7 +1178,7 @@ class InteractiveQueryManager:
         for q in queries:
             q.layout = self.unit_offsets(q.probes)
             if q.layout:
-                q.vids = np.concatenate([ua[u] for u, _ in q.layout]).tolist()
+                q.vids = np.concatenate([ua[u] for u, _ in q.layout])
                 q.pos = np.concatenate([ar[:len(ua[u])] + off for u, off in q.layout])
             else:
                 q.vids, q.pos = [], np.zeros(0, dtype=np.int64)

@@ -203,7 +203,7 @@ class WorkloadBackend:
              "scale": np.array([self.iqm.out_scale_at(self.iqm.level_of(r)) for r in recs])}
         if kind == "dists":     # only the result ciphertexts that hold candidates
             h["need"] = max(1, -(-max((int(r.pos[-1]) + 1 if len(r.pos) else 1) for r in recs) // self.iqm.sh.slots))
-            h["vids"] = [list(r.vids) for r in recs]
+            h["vids"] = [r.vids for r in recs]     # a record's next stage 3 builds new ones
             h["pos"] = [np.asarray(r.pos, dtype=np.int64) for r in recs]
         return h
 
@@ -249,7 +249,7 @@ class WorkloadBackend:
         vids = got["vids"]
         d = got["vals"]
         from .workloads import ranked_prefix
-        return [[v[i] for i in top] for v, top in zip(vids, ranked_prefix(d, got["pos"], wl.spec.top_k))]
+        return [[int(v[i]) for i in top] for v, top in zip(vids, ranked_prefix(d, got["pos"], wl.spec.top_k))]
 
 
 class ServingLoop:

@@ -270,7 +270,7 @@ class Workload:
         self.iqm.stage3_fine(recs)
         for r, o, d in zip(recs, out, self.candidates(recs)):
             order = np.argsort(d, kind="stable")[:self.spec.top_k]
-            o.update(dists=d, vids=list(r.vids), topk=[r.vids[i] for i in order])
+            o.update(dists=d, vids=[int(v) for v in r.vids], topk=[int(r.vids[i]) for i in order])
         return out
 
     # ---- protocol from host buffers, in groups of queries ----
@@ -320,7 +320,8 @@ class Workload:
         scales = np.repeat([iqm.out_scale_at(iqm.level_of(r)) for r in part], need)
         vals = dec.decrypt_decode_host(box[:, :need].reshape(-1, 2, n), scales,
                                        min(S, last) if need == 1 else S).reshape(len(part), -1)
-        return [[r.vids[i] for i in top] for r, top in zip(part, ranked_prefix(vals, pos, self.spec.top_k))], box.nbytes
+        return [[int(r.vids[i]) for i in top] for r, top in zip(part, ranked_prefix(vals, pos, self.spec.top_k))], \
+            box.nbytes
 
     def run_host_pipelined(self, recs: list[QueryRecord], host_cts, dec, groups: int = 2):
         """The interactive protocol for `recs` through the C ABI from host
