@@ -25,10 +25,11 @@
 //             tree sum leaves the sums in every row), accumulate into the
 //             query's result ciphertext
 //   diagonal  (shape.packed = 2) stage 1: the query rotated by 1 .. n1 - 1
-//             (baby steps, kept for stage 3), ||q||^2 (square, tree sum),
-//             the centroids' inner products by their diagonals (one
+//             (baby steps, kept for stage 3), the centroids' inner products
+//             by their diagonals (one
 //             afhe_eval_diag_inner_batch per giant step group), rescale,
-//             giant-step rotations by n1 g, sum, + ||q||^2 + ||c||^2;
+//             giant-step rotations by n1 g, sum, + ||q||^2 (the client's
+//             ciphertext in ct_dim) + ||c||^2;
 //             stage 3: the same per result ciphertext over the query's units,
 //             each unit's diagonals placed at its slot offset (a multiple of
 //             D) by an automorphism folded into the product's loads, then
@@ -474,23 +475,18 @@ int giant(afhe_ivfpq* h, const std::vector<InnerOut>& outs, const Cts& scr, uint
 int stage1_diagonal(afhe_ivfpq* h, const afhe_ivfpq_query* q, const std::vector<uint32_t>& idx, uint32_t Ll) {
     const uint32_t D = h->sh.D, n1 = baby_steps(D), n2 = D / n1;
     const afhe_ivfpq::Diag& dg = h->diag.at(Ll);
-    Cts src, dst, cq, nrm;
+    Cts src, dst;
     std::vector<int32_t> steps;
-    for (uint32_t i : idx) {
+    for (uint32_t i : idx)
         for (uint32_t b = 1; b < n1; ++b) {
             src.push_back(q[i].ct_query);
             dst.push_back(q[i].baby[b - 1]);
             steps.push_back((int32_t)b);
         }
-        cq.push_back(q[i].ct_query);
-        nrm.push_back(q[i].norm);
-    }
     if (!src.empty()) {
         at(h, Ll);
         RC(afhe_eval_rotate_steps_batch(h->ctx, src.data(), dst.data(), steps.data(), (uint32_t)src.size(), Ll));
     }
-    RC(square(h, cq, nrm, Ll));                           // ||q||^2 in every slot: square, tree sum
-    for (uint32_t s = 1; s < D; s <<= 1) RC(rot_acc(h, nrm, nrm, (int32_t)s, Ll - 1));
     const size_t per = h->scratch.size() / n2;
     for (size_t c0 = 0; c0 < idx.size(); c0 += per) {
         const size_t m = std::min(per, idx.size() - c0);
@@ -500,7 +496,7 @@ int stage1_diagonal(afhe_ivfpq* h, const afhe_ivfpq_query* q, const std::vector<
             const afhe_ivfpq_query& x = q[idx[c0 + k]];
             outs.push_back(InnerOut{&x.ct_query, x.baby, {{dg.cent, 1u}}});
             heads.push_back(h->scratch[k * n2]);
-            norms.push_back(x.norm);
+            norms.push_back(x.ct_dim);                    // ||q||^2, the client's
             comp.push_back(x.compact);
         }
         RC(giant(h, outs, h->scratch, Ll));
@@ -571,7 +567,7 @@ int stage3_diagonal(afhe_ivfpq* h, const afhe_ivfpq_query* q, const std::vector<
             fg.push_back((uint32_t)G.size());
             outs.push_back(std::move(o));
             heads.push_back(h->scratch[k * n2]);
-            norms.push_back(x.norm);
+            norms.push_back(x.ct_dim);
             res.push_back(x.results[it.r]);
         }
         RC(giant(h, outs, h->scratch, Ll));

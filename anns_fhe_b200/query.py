@@ -46,9 +46,9 @@ Three compactions:
     Stage 3's plaintexts are built once per unit (a list, or N/2 candidates
     of it) and placed at the unit's output offset, a multiple of D, by an
     automorphism of the plaintext folded into the product's loads
-    (afhe_eval_mac_plain_batch); ||q||^2 (one square and a tree sum per
-    query) and the placed unit norms are added. Depth 1: results at l - 1
-    limbs. Slots outside the probed units hold ||q||^2 alone.
+    (afhe_eval_mac_plain_batch); ||q||^2 (the client's ciphertext, sent in
+    place of ct_dim) and the placed unit norms are added. Depth 1: results
+    at l - 1 limbs. Slots outside the probed units hold ||q||^2 alone.
 In the reference chain, candidate distances past `slots` continue in further
 result ciphertexts (position p at slot p mod slots of result p // slots). A
 candidate batch never straddles two results: one that would not fit starts
@@ -134,7 +134,7 @@ class QueryShape:
 @dataclass
 class QueryRecord:
     ct_query: tuple[int, int]
-    ct_dim: tuple[int, int]
+    ct_dim: tuple[int, int]        # diagonal chain: ||q||^2 in every slot (the client's), evaluation level - 1
     compact: tuple[int, int]
     dists: tuple[int, int]                          # the first result ciphertext
     probes: list = field(default_factory=list)
@@ -143,7 +143,7 @@ class QueryRecord:
     results: list = field(default_factory=list)    # every result ciphertext (dists first)
     level: int = 0          # limbs of the encrypted query (0: the top level L)
     nprobe: int = 0         # lists the client selects (0: the shape's nprobe)
-    norm: tuple | None = None   # packed / diagonal chain: ||q||^2 (at the evaluation level - 1)
+    norm: tuple | None = None   # packed chain: ||q||^2 (at the evaluation level - 1)
     baby: list = field(default_factory=list)       # diagonal chain: the query rotated by 1 .. n1 - 1
     layout: list = field(default_factory=list)     # diagonal chain: (unit, slot offset) per probed unit
 
@@ -583,12 +583,7 @@ class InteractiveQueryManager:
         """Rotation keys the chain needs."""
         D, B = sh.D, sh.B
         if sh.compaction == "diagonal":
-            steps = set(range(1, sh.n1)) | {sh.n1 * g for g in range(1, sh.n2)}    # baby and giant steps
-            s = 1
-            while s < D:
-                steps.add(s)        # tree sum of ||q||^2
-                s <<= 1
-            return steps
+            return set(range(1, sh.n1)) | {sh.n1 * g for g in range(1, sh.n2)}     # baby and giant steps
         steps = set()
         s = 1
         while s < D:
@@ -647,7 +642,7 @@ class InteractiveQueryManager:
         w = self.lvl_out * self.p.n
         comp = self.slots.take(-(-2 * count * w // self.slots.w))[0]
         dist = self.slots.take(-(-2 * count * self.n_res * w // self.slots.w))[0]
-        packed = self.sh.compaction in ("packed", "diagonal")
+        packed = self.sh.compaction == "packed"
         w1 = (self.L - 1) * self.p.n
         nbase = self.slots.take(self.norm_slots(count, self.L, self.p.n, self.slots.w))[0] if packed else 0
         nb = self.sh.n1 - 1 if self.sh.compaction == "diagonal" else 0
@@ -1141,8 +1136,9 @@ class InteractiveQueryManager:
         return [q.ct_query] + list(q.baby)
 
     def _stage1_diagonal(self, queries: list[QueryRecord], Ll: int) -> None:
-        """Baby steps and ||q||^2 of every query, then the coarse distances
-        ||q||^2 - 2 <q, c> + ||c||^2 in slot c of `compact` (Ll - 1 limbs)."""
+        """Baby steps of every query, then the coarse distances ||q||^2 -
+        2 <q, c> + ||c||^2 in slot c of `compact` (Ll - 1 limbs); ||q||^2 is
+        the client's ciphertext in ct_dim."""
         D, n1, n2 = self.sh.D, self.sh.n1, self.sh.n2
         dg = self._diag[Ll]
         items = [(q, b) for q in queries for b in range(1, n1)]
@@ -1152,12 +1148,6 @@ class InteractiveQueryManager:
             L.check(self.lib.afhe_eval_rotate_steps_batch(self.ctx.h, self._refs([q.ct_query for q, _ in items]),
                                                           self._refs([q.baby[b - 1] for q, b in items]), steps,
                                                           len(items), Ll), "eval_rotate_steps_batch")
-        nrm = [q.norm for q in queries]
-        self._square([q.ct_query for q in queries], nrm, Ll)
-        s = 1
-        while s < D:                         # ||q||^2 in every slot
-            self._rot_acc(nrm, nrm, s, Ll - 1)
-            s <<= 1
         cent = np.asarray(dg["cent"], dtype=np.uint64)[np.arange(n2) * n1].reshape(n2, 1)
         per = len(self._inner) // n2
         for c0 in range(0, len(queries), per):
@@ -1166,7 +1156,7 @@ class InteractiveQueryManager:
             self._giant(inner, [self._babies(q) for q in qs], [cent] * len(qs), [np.ones(1, np.uint32)] * len(qs),
                         Ll)
             comp = [q.compact for q in qs]
-            self._add(inner[0::n2], [q.norm for q in qs], comp, Ll - 1)
+            self._add(inner[0::n2], [q.ct_dim for q in qs], comp, Ll - 1)     # + ||q||^2 (the client's)
             self._add_plain(comp, [dg["cnorm"]] * len(qs), comp, Ll - 1)
 
     def _stage3_diagonal_layout(self, queries: list[QueryRecord]) -> None:
@@ -1215,7 +1205,7 @@ class InteractiveQueryManager:
             self._giant(inner, [self._babies(q) for q, _, _, _ in it], [pts[u[None, :] * D + g0] for _, _, u, _ in it],
                         [g for _, _, _, g in it], Ll)
             outs = [q.results[r] for q, r, _, _ in it]
-            self._add(inner[0::n2], [q.norm for q, _, _, _ in it], outs, Ll - 1)
+            self._add(inner[0::n2], [q.ct_dim for q, _, _, _ in it], outs, Ll - 1)
             sizes = np.array([len(u) for _, _, u, _ in it], dtype=np.int64)
             G = np.zeros(len(it), self.MAC_GROUP)
             G["c0"], G["n"] = L.MAC_UNIT, sizes
@@ -1334,9 +1324,7 @@ class InteractiveQueryManager:
     # ---- result transfer ----
     def input_polys(self, rec: QueryRecord) -> tuple:
         """Offsets of the polynomials the server reads from a client: ct_query
-        and ct_dim, or ct_query alone (the diagonal chain)."""
-        if self.sh.compaction == "diagonal":
-            return tuple(rec.ct_query)
+        and ct_dim (the diagonal chain: ct_dim holds ||q||^2)."""
         return (*rec.ct_query, *rec.ct_dim)
 
     def read_ct(self, ct: tuple[int, int]) -> tuple[np.ndarray, np.ndarray]:

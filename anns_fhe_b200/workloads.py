@@ -169,8 +169,7 @@ class Workload:
             n_batches, masks, work_slots = 0, 0, 0
             w_out = (self.params.L - 1) * n
             outbox_slots = -(-2 * max_queries * w_out // slot_w) + -(-2 * max_queries * n_res * w_out // slot_w)
-            norm_slots = (IQM.norm_slots(max_queries, self.params.L, n, slot_w)
-                          + sum(IQM.diagonal_slots(units, spec.d, lv, n, slot_w) for lv in evl)
+            norm_slots = (sum(IQM.diagonal_slots(units, spec.d, lv, n, slot_w) for lv in evl)
                           + IQM.diagonal_scratch_slots(max_queries, min(lanes, 4096), shape.n1, shape.n2, evl[-1], n,
                                                        slot_w))
         if spec.compaction == "packed":     # ||q||^2 scratch per query; the candidates' norms per level
@@ -212,14 +211,22 @@ class Workload:
 
     # ---- client side ----
     def encrypt_queries(self, Q: np.ndarray, recs: list[QueryRecord], levels=None) -> None:
-        """Encrypt each query (both layouts) into its record, at levels[i]
-        limbs (default: the top level)."""
+        """Encrypt each query (both layouts; the diagonal chain: the query
+        and its squared norm) into its record, at levels[i] limbs (default:
+        the top level)."""
         sh = self.iqm.sh
         for i, (q, r) in enumerate(zip(Q, recs)):
             lv = levels[i] if levels is not None else self.params.L
             r.level = lv
             self.client.encrypt(query_layout(q, sh), sh.scale, r.ct_query[0], r.ct_query[1], level=lv)
-            if sh.compaction != "diagonal":          # the diagonal chain reads ct_query alone
+            if sh.compaction == "diagonal":
+                # ||q||^2 in every slot, at the scale and level the server's
+                # inner products reach after their rescale
+                ll = self.iqm.eval_at(lv)
+                n2 = float(np.dot(np.asarray(q, dtype=np.float64), np.asarray(q, dtype=np.float64)))
+                self.client.encrypt(np.full(sh.slots, n2), sh.scale * sh.scale / self.params.q[ll - 1],
+                                    r.ct_dim[0], r.ct_dim[1], level=ll - 1)
+            else:
                 self.client.encrypt(dimpack_layout(q, sh), sh.scale, r.ct_dim[0], r.ct_dim[1], level=lv)
 
     def decrypt_many(self, cts, scales, slots: int | None = None) -> np.ndarray:

@@ -534,9 +534,11 @@ typedef struct afhe_ivfpq_shape {
 } afhe_ivfpq_shape;
 typedef struct afhe_ivfpq_query {
     afhe_ct_ref ct_query;        /* the query, repeated every D slots (stage 1 input) */
-    afhe_ct_ref ct_dim;          /* the query, dimension d in slots d B .. d B + B - 1 (stage 3 input) */
+    afhe_ct_ref ct_dim;          /* the query, dimension d in slots d B .. d B + B - 1 (stage 3 input);
+                                    diagonal chain: ||q||^2 in every slot, encrypted by the client at the
+                                    evaluation level - 1 and scale Delta^2 / q_{level-1} */
     afhe_ct_ref compact;         /* stage 1b output: the compacted coarse distances */
-    afhe_ct_ref norm;            /* stage 3 scratch (expanded distances): ||q||^2 at the level - 1 */
+    afhe_ct_ref norm;            /* packed chain, stage 3 scratch (expanded distances): ||q||^2 at the level - 1 */
     const afhe_ct_ref* results;  /* stage 3 outputs, n_results ciphertexts */
     uint32_t n_results;
     uint32_t level;              /* limbs of the encrypted query (0: the top level) */

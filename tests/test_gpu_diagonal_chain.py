@@ -3,12 +3,11 @@
 * residues: every compacted coarse ciphertext and every result ciphertext
   equals a one-ciphertext-at-a-time replay on the CPU oracle (the C
   restatement of the reference's HLS kernels) of the same chain: the baby
-  steps as single-step rotations (eval_rotate_single_step), ||q||^2 as
-  eval_mult_relin_rescale and an eval_rotate tree sum, each inner product as
+  steps as single-step rotations (eval_rotate_single_step), each inner product as
   poly_mul_ntt products of the plaintexts (moved by FHEHostDriver's
   automorphism) summed with eval_add, then rescale, the giant-step rotation
-  and eval_add; the keys, plaintexts and encrypted queries are read back
-  from the device;
+  and eval_add, + the client's ||q||^2 ciphertext + the placed norms; the
+  keys, plaintexts and encrypted queries are read back from the device;
 * decrypted coarse and candidate distances match the plaintext IVF-PQ
   search within the CKKS tolerance, probes and top-k ids are identical;
 * the batched server and the one-lane server give identical ciphertexts.
@@ -37,9 +36,10 @@ TINY_UNITS = dataclasses.replace(TINY_DIAG, name="ivfpq_2048x8_nlist2_N1024_L4_d
                                  nprobe=2)
 
 
-def diagonal_replay(wl, ora, ct, probes, lv):
+def diagonal_replay(wl, ora, ct, nrm, probes, lv):
     """One query through the diagonal chain, one ciphertext at a time, on
-    the oracle, at `lv` limbs: (compact, [result ciphertexts used])."""
+    the oracle, at `lv` limbs (nrm: the client's ||q||^2 ciphertext at lv - 1
+    limbs): (compact, [result ciphertexts used])."""
     iqm, p = wl.iqm, wl.params
     n, sh = p.n, iqm.sh
     D, S, n1, n2 = sh.D, sh.slots, sh.n1, sh.n2
@@ -49,7 +49,6 @@ def diagonal_replay(wl, ora, ct, probes, lv):
     def key(off):
         k = wl.ctx.read_key(off, kw)
         return k[:half], k[half:]
-    relin = key(0)
     where = {s: kw * (1 + i) for i, s in enumerate(sorted(wl.steps))}
 
     class Keys(dict):
@@ -95,11 +94,6 @@ def diagonal_replay(wl, ora, ct, probes, lv):
         return total
 
     babies = [ct] + [ora.eval_rotate_single_step(ct, b, rot, lv) for b in range(1, n1)]
-    nrm = ora.eval_mult_relin_rescale(ct, ct, relin, lv)
-    s = 1
-    while s < D:
-        nrm = ora.eval_add(nrm, ora.eval_rotate(nrm, s, rot, lv - 1), lv - 1)
-        s <<= 1
     comp = giant([[(babies[b], dg["cent"][g * n1 + b], 1) for b in range(n1)] for g in range(n2)])
     comp = ora.eval_add(comp, nrm, lv - 1)
     comp = (ora.poly("add", comp[0], pt(dg["cnorm"], lv - 1), lv - 1), comp[1])
@@ -126,14 +120,17 @@ def replay_and_compare(spec, nq, lanes, orc, levels=None):
         wl.encrypt_queries(wl.queries(nq, seed=21), recs, levels)
         ins = [(wl.ctx.read_poly(r.ct_query[0], r.level * n), wl.ctx.read_poly(r.ct_query[1], r.level * n))
                for r in recs]
+        lvs = [wl.iqm.level_of(r) for r in recs]
+        nrms = [(wl.ctx.read_poly(r.ct_dim[0], (lv - 1) * n), wl.ctx.read_poly(r.ct_dim[1], (lv - 1) * n))
+                for r, lv in zip(recs, lvs)]
         wl.iqm.stage1_coarse(recs)
         wl.select(recs)
         wl.iqm.stage3_fine(recs)
         ora = OracleCKKS(p.log_n, p.q, p.p, p.alpha, orc)
         used = set()
-        for r, ct in zip(recs, ins):
+        for r, ct, nrm in zip(recs, ins, nrms):
             lv = wl.iqm.level_of(r)
-            comp, results = diagonal_replay(wl, ora, (ct[0][:lv * n], ct[1][:lv * n]), r.probes, lv)
+            comp, results = diagonal_replay(wl, ora, (ct[0][:lv * n], ct[1][:lv * n]), nrm, r.probes, lv)
             w = (lv - 1) * n
             got = [a[:w] for a in wl.iqm.read_ct(r.compact)]
             assert np.array_equal(got[0], comp[0]) and np.array_equal(got[1], comp[1]), "coarse ciphertext differs"
