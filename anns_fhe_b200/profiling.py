@@ -301,8 +301,8 @@ def profile_host(batch: int = 296, steps: int = 5, workload: str = "small"):
     iqm = wl.iqm
     recs = wl.records[:batch]
     wl.encrypt_queries(wl.queries(batch, seed=1000), recs)
-    Lw = wl.params.L * wl.params.n
-    host = [[torch.from_numpy(wl.ctx.read_poly(o, Lw)).pin_memory().numpy() for o in wl.iqm.input_polys(r)]
+    host = [[torch.from_numpy(wl.ctx.read_poly(o, w)).pin_memory().numpy()
+             for o, w in zip(wl.iqm.input_polys(r), wl.iqm.input_words(r))]
             for r in recs]
     dec = wl.client.decryptor(batch * max(1, iqm.n_res))
     phases: dict = {}

@@ -1327,6 +1327,14 @@ class InteractiveQueryManager:
         and ct_dim (the diagonal chain: ct_dim holds ||q||^2)."""
         return (*rec.ct_query, *rec.ct_dim)
 
+    def input_words(self, rec: QueryRecord) -> tuple:
+        """Words of each of input_polys: the query's level; the diagonal
+        chain's ||q||^2 ciphertext is at the evaluation level - 1."""
+        lv = rec.level or self.L
+        wq, n = lv * self.p.n, self.p.n
+        wd = (self.eval_at(lv) - 1) * n if self.sh.compaction == "diagonal" else wq
+        return (wq, wq, wd, wd)
+
     def read_ct(self, ct: tuple[int, int]) -> tuple[np.ndarray, np.ndarray]:
         w = self.lvl_out * self.p.n
         return self.ctx.read_poly(ct[0], w), self.ctx.read_poly(ct[1], w)

@@ -138,7 +138,7 @@ class WorkloadBackend:
             lv = None if levels is None else list(levels[c0:c0 + chunk])
             wl.encrypt_queries(part, recs, lv)
             for r in recs:
-                self.pool.append([wl.ctx.read_poly(o, r.level * self.n) for o in wl.iqm.input_polys(r)])
+                self.pool.append([wl.ctx.read_poly(o, w) for o, w in zip(wl.iqm.input_polys(r), wl.iqm.input_words(r))])
                 self.pool_level.append(r.level)
         w = self.iqm.lvl_out * self.n
         # device bytes one in-flight query holds: its encrypted polynomials at

@@ -148,8 +148,8 @@ def measure(args, spec, rank: int, world: int, steps: int, warmup: int, batch: i
         recs = wl.records[:batch]
         Q = wl.queries(batch, seed=query_seed(1000, rank))
         wl.encrypt_queries(Q, recs)            # client work done once: encrypted queries on the host
-        Lw = wl.params.L * wl.params.n
-        host = [[torch.from_numpy(wl.ctx.read_poly(o, Lw)).pin_memory() for o in wl.iqm.input_polys(r)]
+        host = [[torch.from_numpy(wl.ctx.read_poly(o, w)).pin_memory()
+                 for o, w in zip(wl.iqm.input_polys(r), wl.iqm.input_words(r))]
                 for r in recs]
         host_np = [[t.numpy() for t in cts] for cts in host]
         groups = max(1, args.e2e_groups)
