@@ -76,7 +76,10 @@ int cached_map(afhe_ctx* ctx, uint32_t galois, const uint32_t** out) {
         cudaFree(d);
         return cuda_fail(ctx, e, "automorphism map upload");
     }
+    bool local = true;
+    for (uint32_t i = 0; i < ctx->n && local; ++i) local = (map[i] >> 8) == (i >> 8);
     ctx->auto_maps[galois] = d;
+    ctx->auto_map_local[galois] = local;
     *out = d;
     return AFHE_OK;
 }
@@ -975,6 +978,18 @@ int afhe_eval_diag_inner_batch(afhe_ctx* ctx, const afhe_ct_ref* out, uint32_t c
     const unsigned __int128 room = ~(unsigned __int128)0 / (sq ? sq : 1);
     const uint32_t reduce_every = room > 0x7fffffff ? 0x7fffffffu : (uint32_t)room;
     if (reduce_every < nb + 1) return fail(ctx, AFHE_E_ARG, "primes too large for the accumulators; use afhe_eval_mac_plain_batch");
+    // the shared-memory form: tiles of 256 words stay put under every map,
+    // 16-byte aligned plaintext tiles
+    bool staged = ctx->n % 256 == 0 && pt_stride % 2 == 0;
+    for (uint32_t j = 0; j < count && staged; ++j)
+        for (uint32_t k = first_unit[j]; k < first_unit[j + 1] && staged; ++k) {
+            const uint32_t* map = nullptr;
+            if (unit_pt[k] % 2) staged = false;
+            else if (unit_galois[k] != 1) {
+                if ((rc = cached_map(ctx, unit_galois[k], &map))) return rc;
+                staged = ctx->auto_map_local[unit_galois[k]];
+            }
+        }
     const size_t seg = ctx->ring.seg_words - 96;
     std::vector<DiagJob> J;
     std::vector<u64> S;
@@ -988,7 +1003,7 @@ int afhe_eval_diag_inner_batch(afhe_ctx* ctx, const afhe_ct_ref* out, uint32_t c
         if ((r = ring_put(ctx, S.data(), S.size(), &ds))) return r;
         if ((r = ring_put(ctx, U.data(), U.size() * sizeof(DiagUnit) / sizeof(u64), &du))) return r;
         CK(launch_diag_inner(ctx->nat.pc, ctx->poly, ctx->n, limbs, (uint32_t)J.size(), nb, (const DiagJob*)dj, ds,
-                             (const DiagUnit*)du, pt_stride, reduce_every, accumulate ? 1 : 0, ctx->st));
+                             (const DiagUnit*)du, pt_stride, reduce_every, accumulate ? 1 : 0, staged, ctx->st));
         J.clear();
         S.clear();
         U.clear();

@@ -131,6 +131,8 @@ struct afhe_ctx {
     std::map<int32_t, afhe::RotKey> rot;
     // device automorphism maps by Galois element (afhe_automorphism_batch)
     std::map<uint32_t, uint32_t*> auto_maps;
+    // whether a map keeps every 256-word tile within itself (by Galois element)
+    std::map<uint32_t, bool> auto_map_local;
     // afhe_decode_batch's working memory, grown on demand and kept (a
     // cudaFree per call would wait for every stream of the device)
     void* dec_ws = nullptr;
@@ -192,6 +194,9 @@ struct MacTerm {
 // The diagonal method's inner products (afhe_eval_diag_inner_batch): job z
 // writes out = sum over its units k of sum over b < nb of
 // pt_k[b stride + map_k[i]] * src_{z, b}, srcs[z nb + b] = (c0, c1) offsets.
+// staged: every map keeps 256-word tiles within themselves, every plaintext
+// offset and the stride are even and N is a multiple of 256 (the
+// shared-memory form).
 struct DiagJob {
     u64 out0, out1;
     uint32_t u0, u1;
@@ -202,7 +207,7 @@ struct DiagUnit {
 };
 cudaError_t launch_diag_inner(const PrimeConst* pc, u64* arena, uint32_t n, uint32_t limbs, uint32_t jobs,
                               uint32_t nb, const DiagJob* job, const u64* srcs, const DiagUnit* unit, u64 stride,
-                              uint32_t reduce_every, int accumulate, cudaStream_t st);
+                              uint32_t reduce_every, int accumulate, bool staged, cudaStream_t st);
 cudaError_t launch_mac_plain(const PrimeConst* pc, u64* arena, uint32_t n, uint32_t limbs, uint32_t jobs,
                              const MacJob* job, const MacGroup* group, const MacTerm* term, uint32_t reduce_every,
                              int accumulate, cudaStream_t st);

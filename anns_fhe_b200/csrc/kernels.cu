@@ -263,10 +263,120 @@ __global__ void __launch_bounds__(256) diag_inner_kernel(const PrimeConst* __res
     arena[J.out1 + off + i] = r1;
 }
 
+// The same sums with the plaintexts staged through shared memory: every
+// placement map of the launch keeps each 256-coefficient tile within itself
+// (a slot rotation by a multiple of D permutes the evaluation form inside
+// blocks of N / 2D words), so a CTA copies the tile of all nb plaintexts of
+// its next unit with cp.async while it multiplies the current one
+// (double-buffered), and gathers from shared memory. One coefficient per
+// thread, 256 threads: tile t = coefficients [256 t, 256 t + 256).
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int K>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(K) : "memory"); }
+
+constexpr uint32_t kDiagTile = 256;
+
+template <int NB>
+__global__ void __launch_bounds__(kDiagTile) diag_inner_staged_kernel(
+    const PrimeConst* __restrict__ pc, u64* __restrict__ arena, uint32_t n, const DiagJob* __restrict__ jobs,
+    const u64* __restrict__ srcs, const DiagUnit* __restrict__ units, u64 stride, uint32_t reduce_every,
+    int accumulate) {
+    extern __shared__ u64 stage[];          // 2 buffers x NB plaintexts x kDiagTile words
+    const uint32_t l = blockIdx.y, tid = threadIdx.x;
+    const uint32_t base = blockIdx.x * kDiagTile, i = base + tid;
+    const DiagJob J = jobs[blockIdx.z];
+    const ModConst m = modconst_of(pc[l]);
+    const u64 off = (u64)l * n;
+    const u64* s = srcs + (u64)blockIdx.z * 2 * NB;
+    u64 x0[NB], x1[NB];
+#pragma unroll
+    for (int b = 0; b < NB; ++b) {
+        x0[b] = arena[s[2 * b] + off + i];
+        x1[b] = arena[s[2 * b + 1] + off + i];
+    }
+    // unit k's tile of its NB plaintexts into buffer `buf`: NB x 128 chunks of 16 bytes
+    auto issue = [&](uint32_t k, uint32_t buf) {
+        const u64* g = arena + units[k].pt + off + base;
+        u64* d = stage + (size_t)buf * NB * kDiagTile;
+        for (uint32_t c = tid; c < NB * (kDiagTile / 2); c += kDiagTile) {
+            const uint32_t b = c / (kDiagTile / 2), w = (c % (kDiagTile / 2)) * 2;
+            cp_async16(d + b * kDiagTile + w, g + (u64)b * stride + w);
+        }
+        cp_async_commit();
+    };
+    Acc128 a0, a1;
+    acc_init(a0);
+    acc_init(a1);
+    uint32_t cnt = 0;
+    if (J.u0 < J.u1) issue(J.u0, 0);
+    for (uint32_t k = J.u0; k < J.u1; ++k) {
+        const uint32_t buf = (k - J.u0) & 1u;
+        const uint32_t* map = units[k].map;
+        const uint32_t j = (map ? __ldg(map + i) : i) - base;
+        if (k + 1 < J.u1) {
+            issue(k + 1, buf ^ 1u);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        if (cnt + NB > reduce_every) {
+            acc_fold(a0, m);
+            acc_fold(a1, m);
+            cnt = 1;
+        }
+        const u64* t = stage + (size_t)buf * NB * kDiagTile + j;
+#pragma unroll
+        for (int b = 0; b < NB; ++b) {
+            const u64 v = t[b * kDiagTile];
+            acc_mad(a0, v, x0[b]);
+            acc_mad(a1, v, x1[b]);
+        }
+        cnt += NB;
+        __syncthreads();                    // the buffer is refilled two units later
+    }
+    u64 r0 = acc_reduce(a0, m), r1 = acc_reduce(a1, m);
+    if (accumulate) {
+        r0 = add_mod(r0, arena[J.out0 + off + i], m.q);
+        r1 = add_mod(r1, arena[J.out1 + off + i], m.q);
+    }
+    arena[J.out0 + off + i] = r0;
+    arena[J.out1 + off + i] = r1;
+}
+
 cudaError_t launch_diag_inner(const PrimeConst* pc, u64* arena, uint32_t n, uint32_t limbs, uint32_t jobs,
                               uint32_t nb, const DiagJob* job, const u64* srcs, const DiagUnit* unit, u64 stride,
-                              uint32_t reduce_every, int accumulate, cudaStream_t st) {
+                              uint32_t reduce_every, int accumulate, bool staged, cudaStream_t st) {
     if (limbs == 0 || jobs == 0) return cudaSuccess;
+    if (staged) {
+        if (n % kDiagTile) return cudaErrorInvalidValue;
+        dim3 grid(n / kDiagTile, limbs, jobs);
+        const size_t smem = 2ull * nb * kDiagTile * sizeof(u64);
+#define DIAG_STAGED(NBV)                                                                                       \
+    case NBV: {                                                                                                \
+        cudaError_t e = cudaFuncSetAttribute(diag_inner_staged_kernel<NBV>,                                    \
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);          \
+        if (e != cudaSuccess) return e;                                                                        \
+        diag_inner_staged_kernel<NBV><<<grid, kDiagTile, smem, st>>>(pc, arena, n, job, srcs, unit, stride,    \
+                                                                     reduce_every, accumulate);                \
+        break;                                                                                                 \
+    }
+        switch (nb) {
+            DIAG_STAGED(1)
+            DIAG_STAGED(2)
+            DIAG_STAGED(4)
+            DIAG_STAGED(8)
+            DIAG_STAGED(16)
+        default: return cudaErrorInvalidValue;
+        }
+#undef DIAG_STAGED
+        count_launches(1);
+        return cudaGetLastError();
+    }
     dim3 grid((n + 255) / 256, limbs, jobs);
     switch (nb) {
     case 1: diag_inner_kernel<1><<<grid, 256, 0, st>>>(pc, arena, n, job, srcs, unit, stride, reduce_every, accumulate); break;

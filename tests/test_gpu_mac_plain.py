@@ -102,12 +102,16 @@ def test_mac_plain_matches_host(q_bits):
         ctx.close()
 
 
-@pytest.mark.parametrize("nb", [1, 4, 16])
-def test_diag_inner_equals_mac_plain(nb):
+@pytest.mark.parametrize("nb,q_bits,local", [(1, 50, True), (4, 50, True), (16, 50, True), (16, 60, True),
+                                              (16, 50, False), (4, 60, False)])
+def test_diag_inner_equals_mac_plain(nb, q_bits, local):
     """afhe_eval_diag_inner_batch equals afhe_eval_mac_plain_batch with one
-    group per baby step and one term per unit, units at pt + b * stride."""
+    group per baby step and one term per unit, units at pt + b * stride.
+    With `local`, every placement is a rotation by a multiple of 64 slots,
+    whose map keeps 256-word tiles in place (the shared-memory form of the
+    kernel); otherwise a rotation by 5 is among them (the register form)."""
     log_n, limbs = 11, 2
-    q, p = primes_for(log_n, limbs, 50, 1, 60)
+    q, p = primes_for(log_n, limbs, q_bits, 1, 61 if q_bits == 60 else 60)
     n = 1 << log_n
     w = limbs * n
     ctx = FheContext(CkksParams(log_n, q, p, 1), poly_words=600 * w, key_words=1024)
@@ -117,7 +121,8 @@ def test_diag_inner_equals_mac_plain(nb):
         stride = 3 * w                                   # a unit's plaintexts 3 polynomials apart
         srcs = [(2 * i * w, (2 * i + 1) * w) for i in range(32)]        # [0, 64 w)
         units = [64 * w + k * w for k in range(48)]                     # plaintexts in [64 w, 64 w + 48 w + 45 stride)
-        gals = [1, galois_elt(log_n, -64), galois_elt(log_n, -256), galois_elt(log_n, 5)]
+        gals = [1, galois_elt(log_n, -64), galois_elt(log_n, -256),
+                galois_elt(log_n, 128) if local else galois_elt(log_n, 5)]
         jobs = [(list(range(0, 5)), 0), (list(range(7, 9)), 1), ([], 2)]    # (units, first source)
         outs_a = [((520 + 4 * j) * w, (521 + 4 * j) * w) for j in range(len(jobs))]
         outs_b = [((522 + 4 * j) * w, (523 + 4 * j) * w) for j in range(len(jobs))]
