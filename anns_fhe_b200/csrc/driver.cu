@@ -1003,7 +1003,8 @@ int afhe_eval_diag_inner_batch(afhe_ctx* ctx, const afhe_ct_ref* out, uint32_t c
         if ((r = ring_put(ctx, S.data(), S.size(), &ds))) return r;
         if ((r = ring_put(ctx, U.data(), U.size() * sizeof(DiagUnit) / sizeof(u64), &du))) return r;
         CK(launch_diag_inner(ctx->nat.pc, ctx->poly, ctx->n, limbs, (uint32_t)J.size(), nb, (const DiagJob*)dj, ds,
-                             (const DiagUnit*)du, pt_stride, reduce_every, accumulate ? 1 : 0, staged, ctx->st));
+                             (const DiagUnit*)du, pt_stride, reduce_every, accumulate ? 1 : 0, staged,
+                             qmax < (1ull << 50), ctx->st));
         J.clear();
         S.clear();
         U.clear();

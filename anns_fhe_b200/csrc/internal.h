@@ -196,7 +196,8 @@ struct MacTerm {
 // pt_k[b stride + map_k[i]] * src_{z, b}, srcs[z nb + b] = (c0, c1) offsets.
 // staged: every map keeps 256-word tiles within themselves, every plaintext
 // offset and the stride are even and N is a multiple of 256 (the
-// shared-memory form).
+// shared-memory form); halves (staged only): every prime is below 2^50
+// (25-bit split products).
 struct DiagJob {
     u64 out0, out1;
     uint32_t u0, u1;
@@ -207,7 +208,7 @@ struct DiagUnit {
 };
 cudaError_t launch_diag_inner(const PrimeConst* pc, u64* arena, uint32_t n, uint32_t limbs, uint32_t jobs,
                               uint32_t nb, const DiagJob* job, const u64* srcs, const DiagUnit* unit, u64 stride,
-                              uint32_t reduce_every, int accumulate, bool staged, cudaStream_t st);
+                              uint32_t reduce_every, int accumulate, bool staged, bool halves, cudaStream_t st);
 cudaError_t launch_mac_plain(const PrimeConst* pc, u64* arena, uint32_t n, uint32_t limbs, uint32_t jobs,
                              const MacJob* job, const MacGroup* group, const MacTerm* term, uint32_t reduce_every,
                              int accumulate, cudaStream_t st);

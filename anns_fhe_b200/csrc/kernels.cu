@@ -280,7 +280,34 @@ __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_gr
 
 constexpr uint32_t kDiagTile = 256;
 
-template <int NB>
+// Residues below 2^50: operands split into 25-bit halves, x = x1 2^25 + x0;
+// the partial sums x0 y0, x0 y1 + x1 y0, x1 y1 of the products accumulate
+// in 64-bit registers by single 32 x 32 + 64 multiply-adds (products of
+// halves < 2^50: 4,096 products fit between folds); recombined in 128 bits.
+constexpr uint32_t kHalfBits = 25, kHalfMask = (1u << kHalfBits) - 1, kHalfFold = 4096;
+__device__ __forceinline__ void mad_wide(u64& acc, uint32_t a, uint32_t b) {
+    asm("mad.wide.u32 %0, %1, %2, %0;" : "+l"(acc) : "r"(a), "r"(b));
+}
+struct Halves {
+    u64 s00, s01, s11;
+};
+__device__ __forceinline__ void halves_mad(Halves& h, uint32_t v0, uint32_t v1, uint32_t x0, uint32_t x1) {
+    mad_wide(h.s00, v0, x0);
+    mad_wide(h.s01, v0, x1);
+    mad_wide(h.s01, v1, x0);
+    mad_wide(h.s11, v1, x1);
+}
+__device__ __forceinline__ u64 halves_reduce(const Halves& h, const ModConst& m) {
+    u64 lo = h.s00, hi = 0;
+    const u64 t1 = h.s01 << kHalfBits, t2 = h.s11 << (2 * kHalfBits);
+    lo += t1;
+    hi += (lo < t1 ? 1 : 0) + (h.s01 >> (64 - kHalfBits));
+    lo += t2;
+    hi += (lo < t2 ? 1 : 0) + (h.s11 >> (64 - 2 * kHalfBits));
+    return reduce128(hi, lo, m);
+}
+
+template <int NB, bool HALVES>
 __global__ void __launch_bounds__(kDiagTile) diag_inner_staged_kernel(
     const PrimeConst* __restrict__ pc, u64* __restrict__ arena, uint32_t n, const DiagJob* __restrict__ jobs,
     const u64* __restrict__ srcs, const DiagUnit* __restrict__ units, u64 stride, uint32_t reduce_every,
@@ -292,11 +319,20 @@ __global__ void __launch_bounds__(kDiagTile) diag_inner_staged_kernel(
     const ModConst m = modconst_of(pc[l]);
     const u64 off = (u64)l * n;
     const u64* s = srcs + (u64)blockIdx.z * 2 * NB;
-    u64 x0[NB], x1[NB];
+    u64 x0[HALVES ? 1 : NB], x1[HALVES ? 1 : NB];
+    uint32_t h00[HALVES ? NB : 1], h01[HALVES ? NB : 1], h10[HALVES ? NB : 1], h11[HALVES ? NB : 1];
 #pragma unroll
     for (int b = 0; b < NB; ++b) {
-        x0[b] = arena[s[2 * b] + off + i];
-        x1[b] = arena[s[2 * b + 1] + off + i];
+        const u64 y0 = arena[s[2 * b] + off + i], y1 = arena[s[2 * b + 1] + off + i];
+        if (HALVES) {
+            h00[b] = (uint32_t)y0 & kHalfMask;
+            h01[b] = (uint32_t)(y0 >> kHalfBits);
+            h10[b] = (uint32_t)y1 & kHalfMask;
+            h11[b] = (uint32_t)(y1 >> kHalfBits);
+        } else {
+            x0[b] = y0;
+            x1[b] = y1;
+        }
     }
     // unit k's tile of its NB plaintexts into buffer `buf`: NB x 128 chunks of 16 bytes
     auto issue = [&](uint32_t k, uint32_t buf) {
@@ -311,6 +347,7 @@ __global__ void __launch_bounds__(kDiagTile) diag_inner_staged_kernel(
     Acc128 a0, a1;
     acc_init(a0);
     acc_init(a1);
+    Halves c0{0, 0, 0}, c1{0, 0, 0};
     uint32_t cnt = 0;
     if (J.u0 < J.u1) issue(J.u0, 0);
     for (uint32_t k = J.u0; k < J.u1; ++k) {
@@ -324,22 +361,38 @@ __global__ void __launch_bounds__(kDiagTile) diag_inner_staged_kernel(
             cp_async_wait<0>();
         }
         __syncthreads();
-        if (cnt + NB > reduce_every) {
-            acc_fold(a0, m);
-            acc_fold(a1, m);
-            cnt = 1;
-        }
         const u64* t = stage + (size_t)buf * NB * kDiagTile + j;
+        if (HALVES) {
+            if (cnt + NB > kHalfFold) {
+                c0 = Halves{halves_reduce(c0, m), 0, 0};
+                c1 = Halves{halves_reduce(c1, m), 0, 0};
+                cnt = 1;
+            }
 #pragma unroll
-        for (int b = 0; b < NB; ++b) {
-            const u64 v = t[b * kDiagTile];
-            acc_mad(a0, v, x0[b]);
-            acc_mad(a1, v, x1[b]);
+            for (int b = 0; b < NB; ++b) {
+                const u64 v = t[b * kDiagTile];
+                const uint32_t v0 = (uint32_t)v & kHalfMask, v1 = (uint32_t)(v >> kHalfBits);
+                halves_mad(c0, v0, v1, h00[b], h01[b]);
+                halves_mad(c1, v0, v1, h10[b], h11[b]);
+            }
+        } else {
+            if (cnt + NB > reduce_every) {
+                acc_fold(a0, m);
+                acc_fold(a1, m);
+                cnt = 1;
+            }
+#pragma unroll
+            for (int b = 0; b < NB; ++b) {
+                const u64 v = t[b * kDiagTile];
+                acc_mad(a0, v, x0[b]);
+                acc_mad(a1, v, x1[b]);
+            }
         }
         cnt += NB;
         __syncthreads();                    // the buffer is refilled two units later
     }
-    u64 r0 = acc_reduce(a0, m), r1 = acc_reduce(a1, m);
+    u64 r0 = HALVES ? halves_reduce(c0, m) : acc_reduce(a0, m);
+    u64 r1 = HALVES ? halves_reduce(c1, m) : acc_reduce(a1, m);
     if (accumulate) {
         r0 = add_mod(r0, arena[J.out0 + off + i], m.q);
         r1 = add_mod(r1, arena[J.out1 + off + i], m.q);
@@ -350,21 +403,27 @@ __global__ void __launch_bounds__(kDiagTile) diag_inner_staged_kernel(
 
 cudaError_t launch_diag_inner(const PrimeConst* pc, u64* arena, uint32_t n, uint32_t limbs, uint32_t jobs,
                               uint32_t nb, const DiagJob* job, const u64* srcs, const DiagUnit* unit, u64 stride,
-                              uint32_t reduce_every, int accumulate, bool staged, cudaStream_t st) {
+                              uint32_t reduce_every, int accumulate, bool staged, bool halves, cudaStream_t st) {
     if (limbs == 0 || jobs == 0) return cudaSuccess;
     if (staged) {
         if (n % kDiagTile) return cudaErrorInvalidValue;
         dim3 grid(n / kDiagTile, limbs, jobs);
         const size_t smem = 2ull * nb * kDiagTile * sizeof(u64);
-#define DIAG_STAGED(NBV)                                                                                       \
-    case NBV: {                                                                                                \
-        cudaError_t e = cudaFuncSetAttribute(diag_inner_staged_kernel<NBV>,                                    \
+#define DIAG_STAGED_H(NBV, H)                                                                                  \
+    {                                                                                                          \
+        cudaError_t e = cudaFuncSetAttribute(diag_inner_staged_kernel<NBV, H>,                                 \
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);          \
         if (e != cudaSuccess) return e;                                                                        \
-        diag_inner_staged_kernel<NBV><<<grid, kDiagTile, smem, st>>>(pc, arena, n, job, srcs, unit, stride,    \
-                                                                     reduce_every, accumulate);                \
-        break;                                                                                                 \
+        diag_inner_staged_kernel<NBV, H><<<grid, kDiagTile, smem, st>>>(pc, arena, n, job, srcs, unit, stride, \
+                                                                        reduce_every, accumulate);             \
     }
+#define DIAG_STAGED(NBV)                \
+    case NBV:                           \
+        if (halves)                     \
+            DIAG_STAGED_H(NBV, true)    \
+        else                            \
+            DIAG_STAGED_H(NBV, false)   \
+        break;
         switch (nb) {
             DIAG_STAGED(1)
             DIAG_STAGED(2)
@@ -374,6 +433,7 @@ cudaError_t launch_diag_inner(const PrimeConst* pc, u64* arena, uint32_t n, uint
         default: return cudaErrorInvalidValue;
         }
 #undef DIAG_STAGED
+#undef DIAG_STAGED_H
         count_launches(1);
         return cudaGetLastError();
     }
