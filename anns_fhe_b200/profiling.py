@@ -36,6 +36,9 @@ KS_CAPTURES: dict = {
     # clusters of 8 CTAs of 2^12-value slices, two per SM; 66 = two full waves
     (32768, 3, 4, 12): {"kernel": "ks_fused_kernel<12, 3, 1, 8>", "ciphertexts": 66, "dram_bytes": 715.8e6,
                         "pipe": "alu", "util": 0.370},
+    # the diagonal chain's evaluation level (2 + 4 limbs), same shape
+    (32768, 2, 4, 12): {"kernel": "ks_fused_kernel<12, 3, 1, 8>", "ciphertexts": 66, "dram_bytes": 522.2e6,
+                        "pipe": "alu", "util": 0.371},
 }
 
 
