@@ -1328,11 +1328,14 @@ class InteractiveQueryManager:
         return (*rec.ct_query, *rec.ct_dim)
 
     def input_words(self, rec: QueryRecord) -> tuple:
-        """Words of each of input_polys: the query's level; the diagonal
-        chain's ||q||^2 ciphertext is at the evaluation level - 1."""
-        lv = rec.level or self.L
-        wq, n = lv * self.p.n, self.p.n
-        wd = (self.eval_at(lv) - 1) * n if self.sh.compaction == "diagonal" else wq
+        """Words of each of input_polys a client sends: the limbs the server
+        evaluates the query at (a ciphertext's first l limbs are the same
+        message mod Q_l, so the client drops the rest before sending, as the
+        server would on arrival); the diagonal chain's ||q||^2 ciphertext is
+        at the evaluation level - 1."""
+        lv, n = self.eval_at(rec.level or self.L), self.p.n
+        wq = lv * n
+        wd = (lv - 1) * n if self.sh.compaction == "diagonal" else wq
         return (wq, wq, wd, wd)
 
     def read_ct(self, ct: tuple[int, int]) -> tuple[np.ndarray, np.ndarray]:
