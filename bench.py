@@ -99,7 +99,7 @@ def config_of(spec, batch: int) -> dict:
     return {"workload": spec.name, "queries_per_step": batch, "n_vectors": spec.n_vectors, "d": spec.d,
             "n_list": spec.n_list, "nprobe": spec.nprobe, "pq": f"{spec.M}x{spec.K}", "top_k": spec.top_k,
             "ring_degree": n, "q_limbs": spec.num_q, "p_limbs": spec.num_p, "alpha": spec.alpha,
-            "scale_bits": spec.log_scale,
+            "scale_bits": spec.log_scale, "chain": spec.compaction, "eval_level": spec.eval_level or spec.num_q,
             "l2": f"no flush; inputs larger than L2: {batch * ct_bytes / 1e6:.0f} MB of encrypted queries per step "
                   f"(L2 126 MB)"}
 

@@ -538,7 +538,8 @@ def reference_rate(workload: str = "large", steps: int = 3, warmup: int = 1, wor
     rate = fractions / wall
     kind = "reference" if kinds == {"reference"} else "port"
     what = ("the reference's HLS C-simulation rebuilt at N = %d over its SimMemoryBus, in FHEHostDriver's "
-            "operator sequence" % sh["n"]) if kind == "reference" else "the C restatement (oracle port)"
+            "operator sequence of the reference's chain (%s compaction, depth 2, evaluated at %d limbs)"
+            % (sh["n"], sh["compaction"], sh["L"])) if kind == "reference" else "the C restatement (oracle port)"
     return {"value": rate, "unit": "queries/s", "cores": workers, "kind": kind, "workload": sh["name"],
             "units_per_query": U, "seconds": wall, "ms_per_step": 1e3 * wall / max(1, steps),
             "sample": (f"{steps} timed steps after {warmup} warm-up; each step {workers} processes x "
