@@ -408,9 +408,10 @@ class InteractiveQueryManager:
 
     @staticmethod
     def inner_pool(lanes: int, n2: int) -> int:
-        """Working ciphertexts of the inner products: the lanes, rounded down
-        to whole outputs of n2 giant steps, at least one output."""
-        return max(n2, lanes // n2 * n2)
+        """Working ciphertexts of the inner products: n2 giant steps for each
+        of `lanes` outputs, so that a batched call covers as many outputs as
+        a launch holds ciphertexts."""
+        return max(1, lanes) * n2
 
     @classmethod
     def diagonal_scratch_slots(cls, queries: int, lanes: int, n1: int, n2: int, top: int, n: int,
