@@ -170,3 +170,23 @@ def test_unit_offsets():
     offs = unit_offsets(counts, 512, 8)
     for off, cnt in zip(offs, counts):
         assert off % 8 == 0 and off // 512 == (off + cnt - 1) // 512
+
+
+def test_diagonal_results_bound():
+    """results_for (diagonal chain) covers every probe set of up to nprobe
+    lists: random list sizes (some longer than the slots), random probes."""
+    from types import SimpleNamespace
+
+    from anns_fhe_b200.query import QueryShape, unit_offsets
+    rng = np.random.default_rng(7)
+    for S, D, nprobe in ((512, 8, 40), (16384, 128, 16), (4096, 64, 4)):
+        sizes = [int(x) for x in rng.integers(0, 3 * S // 2, 200)]
+        index = SimpleNamespace(lists=[list(range(k)) for k in sizes])
+        sh = QueryShape(D=D, n_list=200, slots=S, nprobe=nprobe, top_k=1, scale=1.0, compaction="diagonal")
+        bound = InteractiveQueryManager.results_for(index, sh, nprobe)
+        for _ in range(300):
+            probes = rng.choice(200, size=int(rng.integers(1, nprobe + 1)), replace=False)
+            counts = [min(S, sizes[c] - u0) for c in probes for u0 in range(0, sizes[c], S)]
+            offs = unit_offsets(counts, S, D)
+            used = offs[-1] // S + 1 if offs else 1
+            assert used <= bound
