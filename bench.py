@@ -4,10 +4,14 @@ Headline workload (default, --workload large): the largest single-GPU
 configuration, 1,000,000 x 128 float32 vectors from a 1,024-component
 Gaussian mixture (sigma 0.15), IVF n_list 1024, PQ 16 x 256, nprobe 16;
 CKKS N = 2^15, scale 2^40, 12 x 50-bit Q primes + 4 x 60-bit special primes,
-alpha 4 (dnum 3). Queries are encrypted at 12 limbs; the depth-2 chain runs
-on their first 3 limbs (`eval_level` 3), which is the same message at the
-same scale. A step is 256 queries through the server's operator chain
-(stage 1/1b, then stage 3 after the client's list selection).
+alpha 4 (dnum 3). Queries are encrypted at 12 limbs; the server runs the
+diagonal chain (baby-step giant-step inner products, depth 1) on their first
+2 limbs (`eval_level` 2), which is the same message at the same scale. A
+step is 256 queries through the server's operator chain (stage 1, then
+stage 3 after the client's list selection). `packed_chain` is the same
+configuration through the packed chain (per-batch tree sums, depth 2, 3
+limbs), with its `full_level` sample (--workload large_packed makes it the
+headline).
 
 * value: queries / device time of the server stages, inputs (encrypted
   queries) resident in HBM, CUDA events on the context stream.
@@ -18,14 +22,15 @@ same scale. A step is 256 queries through the server's operator chain
   (--e2e-groups per step) whose client and server work overlap
   (Workload.run_host_stream); the client decrypts on a device context of
   its own. Every step's queries are copied in and its results out.
-* roofline: the step's dominant operation, the rotation key switch at the
-  chain's evaluation shape, timed alone (anns_fhe_b200/profiling.py).
+* roofline: the step's largest operation, the rotation key switch at the
+  chain's evaluation shape, timed alone (anns_fhe_b200/profiling.py);
+  roofline_inner_products: the diagonal chain's inner-product kernel.
 * cpu_baseline and --impl reference: the same chain on the host's cores,
   the reference's own HLS C-simulation rebuilt at this ring degree, driven in
   FHEHostDriver's operator sequence (oracle/refchain.py), in work units of a
   query.
-* secondary keys: `full_level` (the same queries evaluated at their 12
-  limbs, a sample of 64 queries), `small` (the small interactive
+* secondary keys: `packed_chain` (with `full_level`: the same queries
+  evaluated at their 12 limbs, a sample of 64 queries), `small` (the small interactive
   configuration: 4,096 x 64, n_list 32, nprobe 4, N = 2^13, 3 + 1 limbs,
   296 queries per step), and `serving` (p50/p99 of the plain path and of
   the continuous-batching server on a Poisson trace).
