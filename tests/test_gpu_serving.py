@@ -11,20 +11,26 @@ database, n_list 32, nprobe 4).
   far inside the CKKS tolerance of 1e-2 used for the plaintext comparison.
 * Probes and top-k equal the plaintext IVF-PQ search.
 * A short real-time Poisson trace completes every request.
+Both for the reference's chain and for the diagonal chain (the client's
+||q||^2 ciphertext travels with the query).
 """
+import dataclasses
+
 import numpy as np
 import pytest
 
 from anns_fhe_b200.serving import (Request, ServingLoop, WorkloadBackend, make_trace, poisson_arrivals,
                                    summarize)
-from anns_fhe_b200.workloads import Workload
+from anns_fhe_b200.workloads import SMALL, Workload
 
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture(scope="module")
-def served():
-    wl = Workload(max_queries=12, lanes=8)
+@pytest.fixture(scope="module", params=["reference_chain", "diagonal_chain"])
+def served(request):
+    spec = SMALL if request.param == "reference_chain" else \
+        dataclasses.replace(SMALL, name=SMALL.name + "_diag", compaction="diagonal", eval_level=2)
+    wl = Workload(spec, max_queries=12, lanes=8)
     Q = wl.queries(10, seed=11)
     be = WorkloadBackend(wl, Q)
     yield wl, Q, be
