@@ -326,12 +326,12 @@ def profile_host(batch: int = 296, steps: int = 5, workload: str = "small"):
         t = mark("stage1", t)
         box = iqm.read_results("compact", recs, staged=True)[:, 0]
         t = mark("d2h_coarse", t)
-        coef = dec.decrypt_host_batch_coef(box, 1)
-        t = mark("client_decrypt_coarse", t)
-        vals = dec.enc.decode_real_batch(coef, iqm.out_scale, iqm.coarse_slots_needed())
+        scales = np.array([iqm.out_scale_at(iqm.level_of(r)) for r in recs])
+        vals = dec.decrypt_decode_host(box, scales, iqm.coarse_slots_needed())
+        t = mark("client_decrypt_decode_coarse", t)
         for r, c in zip(recs, iqm.coarse_from_slots(vals)):
             r.probes = list(np.argsort(c, kind="stable")[:wl.spec.nprobe])
-        t = mark("client_decode_select", t)
+        t = mark("client_select", t)
         iqm.stage3_fine(recs)
         t = mark("stage3", t)
         fbox = iqm.read_results("dists", recs, staged=True)
