@@ -313,12 +313,15 @@ __global__ void __launch_bounds__(kDiagTile) diag_inner_staged_kernel(
     const u64* __restrict__ srcs, const DiagUnit* __restrict__ units, u64 stride, uint32_t reduce_every,
     int accumulate) {
     extern __shared__ u64 stage[];          // 2 buffers x NB plaintexts x kDiagTile words
-    const uint32_t l = blockIdx.y, tid = threadIdx.x;
-    const uint32_t base = blockIdx.x * kDiagTile, i = base + tid;
-    const DiagJob J = jobs[blockIdx.z];
+    // jobs vary fastest across the grid: consecutive CTAs are other outputs
+    // of the same tile, so outputs that share their baby steps (one query's
+    // giant steps) read them from L2
+    const uint32_t z = blockIdx.x, l = blockIdx.z, tid = threadIdx.x;
+    const uint32_t base = blockIdx.y * kDiagTile, i = base + tid;
+    const DiagJob J = jobs[z];
     const ModConst m = modconst_of(pc[l]);
     const u64 off = (u64)l * n;
-    const u64* s = srcs + (u64)blockIdx.z * 2 * NB;
+    const u64* s = srcs + (u64)z * 2 * NB;
     u64 x0[HALVES ? 1 : NB], x1[HALVES ? 1 : NB];
     uint32_t h00[HALVES ? NB : 1], h01[HALVES ? NB : 1], h10[HALVES ? NB : 1], h11[HALVES ? NB : 1];
 #pragma unroll
@@ -407,7 +410,8 @@ cudaError_t launch_diag_inner(const PrimeConst* pc, u64* arena, uint32_t n, uint
     if (limbs == 0 || jobs == 0) return cudaSuccess;
     if (staged) {
         if (n % kDiagTile) return cudaErrorInvalidValue;
-        dim3 grid(n / kDiagTile, limbs, jobs);
+        if (n / kDiagTile > 65535 || limbs > 65535) return cudaErrorInvalidValue;
+        dim3 grid(jobs, n / kDiagTile, limbs);
         const size_t smem = 2ull * nb * kDiagTile * sizeof(u64);
 #define DIAG_STAGED_H(NBV, H)                                                                                  \
     {                                                                                                          \
