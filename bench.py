@@ -100,13 +100,18 @@ def default_batch(spec) -> int:
 def config_of(spec, batch: int) -> dict:
     """The workload named by what it is; the same dict on both arms."""
     n = 1 << spec.log_n
-    ct_bytes = 4 * spec.num_q * n * 8
+    ev = spec.eval_level or spec.num_q
+    # the encrypted queries the server reads (at the evaluated limbs) and the
+    # resident plaintexts it streams per step
+    q_bytes = batch * (2 * ev + (2 * (ev - 1) if spec.compaction == "diagonal" else 2 * ev)) * n * 8
+    streamed = ("the units' diagonal plaintexts (64 GiB resident)" if spec.compaction == "diagonal"
+                else "the candidate-batch plaintexts")
     return {"workload": spec.name, "queries_per_step": batch, "n_vectors": spec.n_vectors, "d": spec.d,
             "n_list": spec.n_list, "nprobe": spec.nprobe, "pq": f"{spec.M}x{spec.K}", "top_k": spec.top_k,
             "ring_degree": n, "q_limbs": spec.num_q, "p_limbs": spec.num_p, "alpha": spec.alpha,
             "scale_bits": spec.log_scale, "chain": spec.compaction, "eval_level": spec.eval_level or spec.num_q,
-            "l2": f"no flush; inputs larger than L2: {batch * ct_bytes / 1e6:.0f} MB of encrypted queries per step "
-                  f"(L2 126 MB)"}
+            "l2": f"no flush; inputs larger than L2: {q_bytes / 1e6:.0f} MB of encrypted queries per step and "
+                  f"{streamed} (L2 126 MB)"}
 
 
 def time_steps(wl, recs, stream, steps: int):
